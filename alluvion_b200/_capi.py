@@ -1,0 +1,214 @@
+"""ctypes view of the engine's C ABI (include/alluvion_b200.h).
+
+The structures here mirror the header field for field.  Loading fails
+loudly when liballuvion_b200.so is missing: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "liballuvion_b200.so")
+
+AL_MAX_BOUNDARIES = 16
+
+STATUS = {
+    0: "AL_OK", 1: "AL_ERR_CUDA", 2: "AL_ERR_INVALID", 3: "AL_ERR_OUT_OF_GRID",
+    4: "AL_ERR_CELL_OVERFLOW", 5: "AL_ERR_NEIGHBOR_OVERFLOW", 6: "AL_ERR_UNSUPPORTED",
+    7: "AL_ERR_TIMEOUT", 8: "AL_ERR_NO_DEVICE", 9: "AL_ERR_ALLOC",
+}
+AL_OK = 0
+AL_ERR_OUT_OF_GRID = 3
+AL_ERR_CELL_OVERFLOW = 4
+AL_ERR_NEIGHBOR_OVERFLOW = 5
+ANOMALY_STATUSES = (AL_ERR_OUT_OF_GRID, AL_ERR_CELL_OVERFLOW, AL_ERR_NEIGHBOR_OVERFLOW)
+
+SHAPE_BOX, SHAPE_SPHERE, SHAPE_BOX_SHELL, SHAPE_TORUS = 0, 1, 2, 3
+
+
+def _const_struct(name, real):
+    fields = [(f, real) for f in (
+        "kernel_radius", "kernel_radius_sqr", "cubic_kernel_k", "cubic_kernel_l",
+        "cubic_kernel_zero", "particle_radius", "particle_vol", "particle_mass", "density0",
+        "viscosity", "boundary_viscosity", "dfsph_factor_epsilon")]
+    fields.append(("gravity", real * 3))
+    return type(name, (ctypes.Structure,), {"_fields_": fields})
+
+
+ConstF32 = _const_struct("al_const_f32", ctypes.c_float)
+ConstF64 = _const_struct("al_const_f64", ctypes.c_double)
+
+
+class ConstI(ctypes.Structure):
+    _fields_ = [("max_num_particles_per_cell", ctypes.c_uint32),
+                ("grid_res", ctypes.c_uint32 * 3),
+                ("grid_offset", ctypes.c_int32 * 3),
+                ("max_num_neighbors_per_particle", ctypes.c_uint32),
+                ("num_boundaries", ctypes.c_uint32)]
+
+
+def _body_struct(name, real):
+    return type(name, (ctypes.Structure,), {"_fields_": [
+        ("shape", ctypes.c_uint32),
+        ("use_distance_grid", ctypes.c_uint32),
+        ("sign", real),
+        ("shape_params", real * 8),
+        ("domain_min", real * 3),
+        ("domain_max", real * 3),
+        ("cell_size", real * 3),
+        ("resolution", ctypes.c_uint32 * 3),
+        ("num_nodes", ctypes.c_uint32),
+        ("distance_nodes", ctypes.c_void_p),
+        ("volume_nodes", ctypes.c_void_p),
+        ("max_distance", real),
+        ("mass", real),
+        ("inertia", real * 3),
+    ]})
+
+
+BodyF32 = _body_struct("al_body_f32", ctypes.c_float)
+BodyF64 = _body_struct("al_body_f64", ctypes.c_double)
+
+
+def _rigid_struct(name, real):
+    return type(name, (ctypes.Structure,), {"_fields_": [
+        ("x", real * 3), ("v", real * 3), ("q", real * 4), ("omega", real * 3)]})
+
+
+RigidF32 = _rigid_struct("al_rigid_f32", ctypes.c_float)
+RigidF64 = _rigid_struct("al_rigid_f64", ctypes.c_double)
+
+
+class SolverParams(ctypes.Structure):
+    _fields_ = [("density_change_tolerance", ctypes.c_double),
+                ("density_error_tolerance", ctypes.c_double),
+                ("min_density_solve", ctypes.c_uint32),
+                ("max_density_solve", ctypes.c_uint32),
+                ("min_divergence_solve", ctypes.c_uint32),
+                ("max_divergence_solve", ctypes.c_uint32),
+                ("enable_divergence_solve", ctypes.c_uint32),
+                ("enable_density_solve", ctypes.c_uint32),
+                ("cfl", ctypes.c_double),
+                ("max_dt", ctypes.c_double),
+                ("min_dt", ctypes.c_double),
+                ("pile_gravity", ctypes.c_double * 3),
+                ("integrate_rigids", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class StepReport(ctypes.Structure):
+    _fields_ = [("num_divergence_solve", ctypes.c_uint32),
+                ("num_density_solve", ctypes.c_uint32),
+                ("mean_density_change", ctypes.c_double),
+                ("mean_density_error", ctypes.c_double),
+                ("particle_max_v2", ctypes.c_double),
+                ("pile_max_v2", ctypes.c_double),
+                ("max_v2", ctypes.c_double),
+                ("cfl_dt", ctypes.c_double),
+                ("utilized_cfl", ctypes.c_double),
+                ("dt", ctypes.c_double),
+                ("grid_anomaly", ctypes.c_uint32 * 3),
+                ("num_active_boundary_pairs", ctypes.c_uint32),
+                ("force", (ctypes.c_double * 3) * AL_MAX_BOUNDARIES),
+                ("torque", (ctypes.c_double * 3) * AL_MAX_BOUNDARIES)]
+
+
+def real_types(dtype):
+    """(ConstT, BodyT, RigidT, ctypes real) for np.float32 / np.float64."""
+    if np.dtype(dtype) == np.float32:
+        return ConstF32, BodyF32, RigidF32, ctypes.c_float
+    if np.dtype(dtype) == np.float64:
+        return ConstF64, BodyF64, RigidF64, ctypes.c_double
+    raise TypeError("unsupported real type %r" % (dtype,))
+
+
+def suffix(dtype):
+    return "f32" if np.dtype(dtype) == np.float32 else "f64"
+
+
+_lib = None
+
+# name -> (restype, argtypes); pointer arguments are passed as c_void_p.
+_P = ctypes.c_void_p
+_U = ctypes.c_uint32
+_SIGNATURES = {
+    "al_engine_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "al_engine_destroy": (ctypes.c_int, [_P]),
+    "al_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "al_last_error": (ctypes.c_char_p, []),
+    "al_engine_synchronize": (ctypes.c_int, [_P, _P]),
+}
+for _s in ("f32", "f64"):
+    _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])
+    _SIGNATURES["al_update_particle_neighbors_" + _s] = (
+        ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P, _P])
+
+
+def declared_symbols():
+    """Names of every entry point this module binds (all of include/*.h)."""
+    return sorted(_SIGNATURES)
+
+
+def lib():
+    """Loads liballuvion_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "liballuvion_b200.so not found at %s; run `python -m alluvion_b200.build` "
+                "(there is no CPU fallback)" % LIB_PATH)
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+class EngineError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = lib().al_last_error().decode() or lib().al_status_string(status).decode()
+        super().__init__("%s failed: %s (%s)" % (where, STATUS.get(status, status), msg))
+
+
+def check(status, where, allow=()):
+    """Raises EngineError for a non-OK status not listed in `allow`."""
+    if status != AL_OK and status not in allow:
+        raise EngineError(status, where)
+    return status
+
+
+class Engine:
+    """Owns one al_engine* bound to a CUDA device."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(lib().al_engine_create(device, ctypes.byref(h)), "al_engine_create")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().al_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self, stream=None):
+        check(lib().al_engine_synchronize(self.handle, stream), "al_engine_synchronize")
+
+
+def ptr(t):
+    """Device/host address of a torch tensor or numpy array (None -> NULL)."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return ctypes.c_void_p(t.data_ptr())
+    return ctypes.c_void_p(t.ctypes.data)

@@ -1,0 +1,72 @@
+// engine.hpp -- host-side engine context: device binding, scratch buffers,
+// error reporting.  Shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <unordered_map>
+
+#include "alluvion_b200.h"
+
+namespace alb {
+
+// Thread-local message of the last failing call (al_last_error).
+void set_error(const std::string& msg);
+const std::string& get_error();
+
+// Evaluates a CUDA runtime call; on failure records the message and returns
+// AL_ERR_CUDA from the enclosing function.
+#define ALB_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      ::alb::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));     \
+      return AL_ERR_CUDA;                                                       \
+    }                                                                           \
+  } while (0)
+
+// Propagates a non-zero al_status.
+#define ALB_TRY(expr)          \
+  do {                         \
+    int s_ = (expr);           \
+    if (s_ != AL_OK) return s_; \
+  } while (0)
+
+#define ALB_CHECK_ARG(cond, msg)        \
+  do {                                  \
+    if (!(cond)) {                      \
+      ::alb::set_error(msg);            \
+      return AL_ERR_INVALID;            \
+    }                                   \
+  } while (0)
+
+// A named, growable device buffer.  Capacity only grows; contents are not
+// preserved across growth.
+struct Scratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace alb
+
+struct al_engine {
+  int device = 0;
+  int num_sms = 0;
+  std::unordered_map<std::string, alb::Scratch> scratch;
+  // pinned host staging (control readback, reports)
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+
+  // Returns a device buffer of at least `bytes` under `name`.
+  int buffer(const char* name, size_t bytes, void** out);
+  template <class T>
+  int buf(const char* name, size_t count, T** out) {
+    return buffer(name, count * sizeof(T), reinterpret_cast<void**>(out));
+  }
+  int host_pinned(size_t bytes, void** out);
+  int activate() const;
+  ~al_engine();
+};

@@ -1,0 +1,37 @@
+// grid.cuh -- uniform-grid cell hash and stable counting sort.
+//
+// Replaces update_particle_grid (runner.hpp:1840-1867).  The reference
+// appends particles to fixed-capacity buckets in atomicAdd order; the engine
+// builds a compact cell-sorted permutation in canonical (cell, index) order:
+//   1. hash:    cell id per particle, arrival rank within the cell
+//   2. scan:    exclusive prefix sum of cell counts (3 passes, no waits)
+//   3. scatter: slot = cell_start + arrival rank
+//   4. order:   each cell's members sorted by original index (makes the
+//               permutation independent of atomic arrival order)
+// Particles outside the grid land in a tail bucket after all cells.
+#pragma once
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace alb {
+
+struct GridState {
+  uint32_t n = 0;
+  uint32_t ncells = 0;
+  uint32_t* cell = nullptr;        // [n] cell of original particle (kNoCell outside)
+  uint32_t* perm = nullptr;        // [n] sorted slot -> original index
+  uint32_t* inv = nullptr;         // [n] original index -> sorted slot
+  uint32_t* cell_start = nullptr;  // [ncells + 2]; [ncells] = in-grid count, [ncells+1] = n
+  uint32_t* count = nullptr;       // [ncells + 1]; last = out-of-grid count
+  uint32_t* flags = nullptr;       // [4] grid_anomaly[0..2] + spare (device)
+};
+
+// Hashes, sorts and gathers positions into `xs` (sorted order, w = 0).
+// particle_x is the caller's [n][3] array.  `flags` must be zeroed by the
+// caller (it is also used by later passes).
+template <class TF>
+int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* particle_x,
+               uint32_t n, vec4<TF>* xs, uint32_t* flags, GridState& gs, cudaStream_t st);
+
+}  // namespace alb

@@ -1,0 +1,223 @@
+"""Physical constants, grid sizing, bodies and seeded synthetic scenes.
+
+Constants are derived in the solver's real type with the operation order of
+Const<TF>::set_kernel_radius / set_particle_attr (constants.hpp:100-128), so
+float32 scenes see exactly the float32 values the reference would.
+"""
+import math
+
+import numpy as np
+
+from . import _capi
+
+PI = 3.14159265358979323846264338327950288
+
+
+def make_const(dtype, particle_radius, density0=1000.0, viscosity=0.01,
+               boundary_viscosity=0.01, dfsph_factor_epsilon=1e-6,
+               gravity=(0.0, -9.81, 0.0), kernel_radius=None, particle_mass=None):
+    """Returns an al_const_{f32,f64} for a particle radius r.
+
+    Defaults follow the benchmark scenes: h = 4r, m = rho0 (2r)^3 so that
+    V = (2r)^3, viscosity 0.01, boundary_viscosity 0.01,
+    dfsph_factor_epsilon 1e-6 (both unset in the reference, whose default is
+    0), g = (0, -9.81, 0).
+    """
+    T = np.dtype(dtype).type
+    ConstT, _, _, _ = _capi.real_types(dtype)
+    r = T(particle_radius)
+    h = T(kernel_radius) if kernel_radius is not None else T(4) * r
+    # Const::set_kernel_radius
+    h2 = h * h
+    h3 = h2 * h
+    h4 = h2 * h2
+    k = T(8.0) / h3 / T(PI)
+    l = T(48.0) / h4 / T(PI)
+    # Const::set_particle_attr
+    rho0 = T(density0)
+    if particle_mass is None:
+        d = T(2) * r
+        mass = rho0 * (d * d * d)
+    else:
+        mass = T(particle_mass)
+    vol = mass / rho0
+    c = ConstT()
+    c.kernel_radius = h
+    c.kernel_radius_sqr = h2
+    c.cubic_kernel_k = k
+    c.cubic_kernel_l = l
+    c.cubic_kernel_zero = k
+    c.particle_radius = r
+    c.particle_vol = vol
+    c.particle_mass = mass
+    c.density0 = rho0
+    c.viscosity = T(viscosity)
+    c.boundary_viscosity = T(boundary_viscosity)
+    c.dfsph_factor_epsilon = T(dfsph_factor_epsilon)
+    for i in range(3):
+        c.gravity[i] = T(gravity[i])
+    return c
+
+
+def make_consti(domain_min, domain_max, kernel_radius, num_boundaries=0,
+                max_num_particles_per_cell=64, max_num_neighbors_per_particle=64):
+    """Uniform grid of cell size h covering [domain_min, domain_max].
+
+    grid_offset = floor(domain_min / h) - 1 and the resolution spans the
+    domain plus one cell of margin on each side.
+    """
+    g = _capi.ConstI()
+    h = float(kernel_radius)
+    for i in range(3):
+        lo = math.floor(domain_min[i] / h) - 1
+        hi = math.floor(domain_max[i] / h) + 1
+        g.grid_offset[i] = lo
+        g.grid_res[i] = hi - lo + 1
+    g.max_num_particles_per_cell = max_num_particles_per_cell
+    g.max_num_neighbors_per_particle = max_num_neighbors_per_particle
+    g.num_boundaries = num_boundaries
+    return g
+
+
+def fluid_block(num, box_min, particle_radius, dtype=np.float32, jitter=0.1, seed=0):
+    """Lattice block of num = (nx, ny, nz) particles at spacing 2r starting at
+    box_min + 2r, the mode-0 layout of index_to_position_in_fluid_block
+    (runner.hpp:971-995), plus seeded uniform jitter of +-jitter*r per
+    coordinate (numpy PCG64)."""
+    nx, ny, nz = num
+    r = float(particle_radius)
+    n = nx * ny * nz
+    p = np.arange(n, dtype=np.int64)
+    j = (p % (nx * nz)) // nz
+    k = p // (nx * nz)
+    l = p % nz
+    pos = np.stack([2 * r * j, 2 * r * k, 2 * r * l], axis=1).astype(np.float64)
+    pos += np.asarray(box_min, dtype=np.float64) + 2 * r
+    if jitter:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        pos += rng.uniform(-jitter * r, jitter * r, size=pos.shape)
+    return pos.astype(dtype)
+
+
+# ----------------------------------------------------------------- bodies
+def shape_aabb(shape, params):
+    """(aabb_min, aabb_max, max_distance) of an analytic shape in its frame
+    (dg/box_distance.hpp:13-17, dg/sphere_distance.hpp:11-13,
+    dg/box_shell_distance.hpp:13-21; the torus is new)."""
+    p = [float(v) for v in params]
+    if shape == _capi.SHAPE_BOX:
+        hw = np.array(p[:3])
+        out = p[3]
+        return -hw - out, hw + out, float(np.linalg.norm(hw)) + out
+    if shape == _capi.SHAPE_SPHERE:
+        rr = p[0]
+        return np.full(3, -rr), np.full(3, rr), rr
+    if shape == _capi.SHAPE_BOX_SHELL:
+        outer = np.array(p[3:6])
+        out = p[6]
+        return -outer - out, outer + out, float(np.linalg.norm(outer)) + out
+    if shape == _capi.SHAPE_TORUS:
+        R, rr = p[0], p[1]
+        e = np.array([R + rr, rr, R + rr])
+        return -e, e, R + rr
+    raise ValueError("unknown shape %r" % shape)
+
+
+def box_params(widths, outset=0.0):
+    w = [0.5 * float(v) for v in widths]
+    return w + [outset]
+
+
+def box_shell_params(inner_widths, thickness, outset=0.0):
+    hi = [0.5 * float(v) for v in inner_widths]
+    ho = [v + float(thickness) for v in hi]
+    return hi + ho + [outset]
+
+
+def make_body(dtype, cn, shape, params, resolution, sign=1.0, margin=None,
+              use_distance_grid=False, mass=0.0, inertia=(1.0, 1.0, 1.0)):
+    """al_body_{f32,f64} with the domain of Pile::calculate_domain_and_resolution
+    (pile.hpp:40-65; margin defaults to h for sign < 0, 2h otherwise) and the
+    grid attributes of Pile::calculate_grid_attributes (pile.hpp:66-78).
+    Node pointers are left NULL."""
+    T = np.dtype(dtype).type
+    _, BodyT, _, _ = _capi.real_types(dtype)
+    h = T(cn.kernel_radius)
+    if margin is None:
+        margin = h if sign < 0 else h * T(2)
+    margin = T(margin)
+    lo, hi, maxd = shape_aabb(shape, params)
+    b = BodyT()
+    b.shape = shape
+    b.use_distance_grid = int(bool(use_distance_grid))
+    b.sign = T(sign)
+    padded = list(params) + [0.0] * (8 - len(params))
+    for i in range(8):
+        b.shape_params[i] = T(padded[i])
+    res = [int(v) for v in (resolution if np.ndim(resolution) else [resolution] * 3)]
+    for i in range(3):
+        dmin = T(lo[i]) - margin
+        dmax = T(hi[i]) + margin
+        b.domain_min[i] = dmin
+        b.domain_max[i] = dmax
+        b.cell_size[i] = (dmax - dmin) / T(res[i])
+        b.resolution[i] = res[i]
+    b.num_nodes = num_grid_nodes(res)
+    b.max_distance = T(maxd)
+    b.mass = T(mass)
+    for i in range(3):
+        b.inertia[i] = T(inertia[i])
+    return b
+
+
+def num_grid_nodes(res):
+    nx, ny, nz = res
+    return ((nx + 1) * (ny + 1) * (nz + 1) + 2 * (nx * (ny + 1) * (nz + 1) +
+            (nx + 1) * ny * (nz + 1) + (nx + 1) * (ny + 1) * nz))
+
+
+def rigid_state(dtype, x=(0, 0, 0), v=(0, 0, 0), q=(0, 0, 0, 1), omega=(0, 0, 0)):
+    _, _, RigidT, _ = _capi.real_types(dtype)
+    s = RigidT()
+    for i in range(3):
+        s.x[i], s.v[i], s.omega[i] = x[i], v[i], omega[i]
+    for i in range(4):
+        s.q[i] = q[i]
+    return s
+
+
+def rigid_array(dtype, states):
+    """Packs rigid states into an (nb, 13) array: x, v, q, omega."""
+    T = np.dtype(dtype).type
+    out = np.zeros((len(states), 13), dtype=T)
+    for b, s in enumerate(states):
+        out[b, 0:3] = list(s.x)
+        out[b, 3:6] = list(s.v)
+        out[b, 6:10] = list(s.q)
+        out[b, 10:13] = list(s.omega)
+    return out
+
+
+def solver_params(**kw):
+    """al_solver_params with the reference defaults (solver_df.hpp:60-67) and
+    the benchmark's cfl 0.4, max_dt 2e-4."""
+    p = _capi.SolverParams()
+    p.density_change_tolerance = 1e-3
+    p.density_error_tolerance = 1e-3
+    p.min_density_solve = 2
+    p.max_density_solve = 100
+    p.min_divergence_solve = 1
+    p.max_divergence_solve = 100
+    p.enable_divergence_solve = 1
+    p.enable_density_solve = 1
+    p.cfl = 0.4
+    p.max_dt = 2e-4
+    p.min_dt = 0.0
+    p.pile_gravity[:] = (0.0, -9.81, 0.0)
+    p.integrate_rigids = 1
+    for k, v in kw.items():
+        if k == "pile_gravity":
+            p.pile_gravity[:] = v
+        else:
+            setattr(p, k, v)
+    return p

@@ -1,0 +1,292 @@
+/*
+ * alluvion_b200.h -- C ABI of the B200 (sm_100a) SPH fluid-step engine.
+ *
+ * This is the drop-in boundary underneath alluvion's fluid-step path.  The
+ * reference drives that path from templated C++ host code
+ * (include/alluvion/solver.hpp, solver_df.hpp, solver_ii.hpp, pile.hpp) that
+ * launches kernels from include/alluvion/runner.hpp.  Each entry point below
+ * names the reference routine(s) it replaces.
+ *
+ * Conventions
+ *  - Plain C types only: device pointers, sizes, POD parameter blocks passed
+ *    by pointer and read once per call.  No CUDA, torch or C++ types.
+ *  - Buffers named particle_* use the reference's layouts: particle_x and
+ *    particle_v are [N][3] arrays of the solver's real type (float3/double3
+ *    AoS), scalars are [N], particle_boundary / particle_boundary_kernel are
+ *    [num_boundaries][N][4], particle_neighbors is [N][cap][4] whose 4th
+ *    component holds the neighbor's index as raw uint32 bits
+ *    (runner.hpp:1896-1897).
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *    stream).  Calls are asynchronous unless documented otherwise.
+ *  - Every call returns an al_status.  No call throws or aborts.  Capacity
+ *    anomalies (the reference's grid_anomaly flags, runner.hpp:1860-1865,
+ *    1907-1909) are reported with their own codes after the outputs have
+ *    been written with the reference's truncation semantics.
+ *  - The engine owns its scratch memory (cell tables, sorted particle state,
+ *    compact neighbor lists); callers own every particle_* buffer.
+ */
+#ifndef ALLUVION_B200_H
+#define ALLUVION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AL_API __attribute__((visibility("default")))
+#else
+#define AL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef enum al_status {
+  AL_OK = 0,
+  AL_ERR_CUDA = 1,             /* a CUDA runtime call failed (message: al_last_error) */
+  AL_ERR_INVALID = 2,          /* bad argument (null pointer, size, capacity) */
+  AL_ERR_OUT_OF_GRID = 3,      /* a particle fell outside the grid: grid_anomaly[0] */
+  AL_ERR_CELL_OVERFLOW = 4,    /* a cell exceeded max_num_particles_per_cell: grid_anomaly[1] */
+  AL_ERR_NEIGHBOR_OVERFLOW = 5,/* a particle exceeded max_num_neighbors_per_particle: grid_anomaly[2] */
+  AL_ERR_UNSUPPORTED = 6,      /* option outside the engine's scope */
+  AL_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up */
+  AL_ERR_NO_DEVICE = 8,        /* no CUDA device, or not an sm_100 part */
+  AL_ERR_ALLOC = 9             /* device allocation failed */
+} al_status;
+
+#define AL_MAX_BOUNDARIES 16
+
+/* ------------------------------------------------------- parameter blocks
+ * Mirror of the hot-path subset of Const<TF> (constants.hpp:51-137).  The
+ * derived kernel constants are computed by the caller exactly as
+ * Const::set_kernel_radius / set_particle_attr do (constants.hpp:100-128),
+ * so the engine sees the same rounded values the reference would. */
+typedef struct al_const_f32 {
+  float kernel_radius;       /* h */
+  float kernel_radius_sqr;   /* h^2 */
+  float cubic_kernel_k;      /* 8 / h^3 / pi */
+  float cubic_kernel_l;      /* 48 / h^4 / pi */
+  float cubic_kernel_zero;   /* W(0) = k */
+  float particle_radius;
+  float particle_vol;        /* mass / density0 */
+  float particle_mass;
+  float density0;
+  float viscosity;
+  float boundary_viscosity;
+  float dfsph_factor_epsilon;
+  float gravity[3];
+} al_const_f32;
+
+typedef struct al_const_f64 {
+  double kernel_radius;
+  double kernel_radius_sqr;
+  double cubic_kernel_k;
+  double cubic_kernel_l;
+  double cubic_kernel_zero;
+  double particle_radius;
+  double particle_vol;
+  double particle_mass;
+  double density0;
+  double viscosity;
+  double boundary_viscosity;
+  double dfsph_factor_epsilon;
+  double gravity[3];
+} al_const_f64;
+
+/* Mirror of Consti (constants.hpp:40-49). */
+typedef struct al_consti {
+  uint32_t max_num_particles_per_cell;
+  uint32_t grid_res[3];
+  int32_t grid_offset[3];
+  uint32_t max_num_neighbors_per_particle;
+  uint32_t num_boundaries;
+} al_consti;
+
+/* ----------------------------------------------------------- rigid bodies
+ * One boundary of the Pile (pile.hpp:98-121).  The analytic distances are
+ * those of dg/box_distance.hpp, dg/sphere_distance.hpp and
+ * dg/box_shell_distance.hpp; AL_SHAPE_TORUS has no reference counterpart.
+ * Grid fields follow Pile::calculate_grid_attributes (pile.hpp:66-78):
+ * cell_size = (domain_max - domain_min) / resolution and
+ * num_nodes = (rx+1)(ry+1)(rz+1) + 2 * (edge count).
+ * Node arrays are device pointers for the engine. */
+typedef enum al_shape {
+  AL_SHAPE_BOX = 0,       /* shape_params: half widths x y z, outset */
+  AL_SHAPE_SPHERE = 1,    /* shape_params: radius */
+  AL_SHAPE_BOX_SHELL = 2, /* shape_params: inner half widths xyz, outer half widths xyz, outset */
+  AL_SHAPE_TORUS = 3      /* shape_params: major radius (x-z plane), minor radius */
+} al_shape;
+
+typedef struct al_body_f32 {
+  uint32_t shape;
+  /* 1: distance and normal interpolated from distance_nodes
+   *    (compute_particle_boundary, runner.hpp:2004-2025);
+   * 0: analytic distance with finite-difference normal
+   *    (compute_particle_boundary_analytic<0>, runner.hpp:1982-2002). */
+  uint32_t use_distance_grid;
+  float sign; /* +1: fluid outside the body; -1: fluid inside (container) */
+  float shape_params[8];
+  float domain_min[3];
+  float domain_max[3];
+  float cell_size[3];
+  uint32_t resolution[3];
+  uint32_t num_nodes;
+  const float* distance_nodes; /* [num_nodes]; required when use_distance_grid */
+  const float* volume_nodes;   /* [num_nodes] */
+  float max_distance;          /* Distance::get_max_distance (CFL bound) */
+  float mass;                  /* 0: kinematic body, not integrated */
+  float inertia[3];            /* principal moments, body frame */
+} al_body_f32;
+
+typedef struct al_body_f64 {
+  uint32_t shape;
+  uint32_t use_distance_grid;
+  double sign;
+  double shape_params[8];
+  double domain_min[3];
+  double domain_max[3];
+  double cell_size[3];
+  uint32_t resolution[3];
+  uint32_t num_nodes;
+  const double* distance_nodes;
+  const double* volume_nodes;
+  double max_distance;
+  double mass;
+  double inertia[3];
+} al_body_f64;
+
+/* Kinematic state of one body (Pile x_, v_, q_, omega_; pile.hpp:103-110).
+ * q is {x, y, z, w}. */
+typedef struct al_rigid_f32 {
+  float x[3];
+  float v[3];
+  float q[4];
+  float omega[3];
+} al_rigid_f32;
+
+typedef struct al_rigid_f64 {
+  double x[3];
+  double v[3];
+  double q[4];
+  double omega[3];
+} al_rigid_f64;
+
+/* ------------------------------------------------------- solver controls
+ * Fields of Solver / SolverDf / SolverIi (solver.hpp:261-273,
+ * solver_df.hpp:372-379, solver_ii.hpp:259-261) plus Pile::gravity_
+ * (pile.hpp:142) used by Pile::integrate_kinematics. */
+typedef struct al_solver_params {
+  double density_change_tolerance; /* DFSPH divergence solve: mean drho/dt < tol / dt */
+  double density_error_tolerance;  /* mean (rho_adv - 1) < tol */
+  uint32_t min_density_solve;
+  uint32_t max_density_solve;
+  uint32_t min_divergence_solve;
+  uint32_t max_divergence_solve;
+  uint32_t enable_divergence_solve;
+  uint32_t enable_density_solve;
+  double cfl;
+  double max_dt;
+  double min_dt;
+  double pile_gravity[3];
+  uint32_t integrate_rigids; /* 1: apply Pile::integrate_kinematics after the fluid step */
+  uint32_t reserved;
+} al_solver_params;
+
+/* What one step reports (the solvers' read-only report fields,
+ * solver.hpp:274-279, solver_df.hpp:381-385) plus FP64 rigid totals. */
+typedef struct al_step_report {
+  uint32_t num_divergence_solve;
+  uint32_t num_density_solve;
+  double mean_density_change;
+  double mean_density_error;
+  double particle_max_v2;
+  double pile_max_v2;
+  double max_v2;
+  double cfl_dt;
+  double utilized_cfl;
+  double dt; /* time step used after update_dt */
+  uint32_t grid_anomaly[3];
+  uint32_t num_active_boundary_pairs; /* (particle, body) pairs with nonzero volume */
+  double force[AL_MAX_BOUNDARIES][3];  /* sum_i particle_force[b][i], FP64 */
+  double torque[AL_MAX_BOUNDARIES][3];
+} al_step_report;
+
+/* ------------------------------------------------------------- lifecycle */
+typedef struct al_engine al_engine;
+
+/* Creates an engine bound to CUDA device `device`.  Allocates no particle
+ * memory; scratch grows on first use.  Fails with AL_ERR_NO_DEVICE when the
+ * device is absent or not compute capability 10.x. */
+AL_API int al_engine_create(int device, al_engine** out);
+AL_API int al_engine_destroy(al_engine* engine);
+/* Static description of a status code. */
+AL_API const char* al_status_string(int status);
+/* Thread-local text of the last failing call on this thread ("" if none). */
+AL_API const char* al_last_error(void);
+/* Blocks until all work the engine queued on `stream` has finished. */
+AL_API int al_engine_synchronize(al_engine* engine, void* stream);
+
+/* ------------------------------------------------------------ grid / sort
+ * Uniform-grid cell hash and stable counting sort.  Replaces the bucket
+ * insert of update_particle_grid (runner.hpp:1840-1867): instead of
+ * atomic-order buckets the engine produces the canonical order
+ * (cell index, original index), cell index = (ix*gy + iy)*gz + iz with
+ * (ix,iy,iz) = floor(x / h) - grid_offset (runner.hpp:1827-1838), IEEE
+ * division.  Particles outside the grid get cell index UINT32_MAX and sort
+ * after every in-grid particle.
+ *
+ *   particle_x         [N][3] device, in
+ *   particle_cell      [N] device, out: cell index per original particle
+ *   sorted_to_original [N] device, out: permutation, sorted slot -> index
+ *   cell_start         [gx*gy*gz + 1] device, out (may be NULL): first
+ *                      sorted slot of each cell; last entry = in-grid count
+ *   pid_length         [gx][gy][gz] device, out (may be NULL): particles per
+ *                      cell, uncapped (reference buffer solver.hpp:67-73)
+ * Returns AL_ERR_OUT_OF_GRID / AL_ERR_CELL_OVERFLOW after writing outputs
+ * when the reference would have raised grid_anomaly[0] / [1]. */
+AL_API int al_grid_sort_f32(al_engine* engine, const al_const_f32* cn,
+                     const al_consti* cni, const float* particle_x,
+                     uint32_t num_particles, uint32_t* particle_cell,
+                     uint32_t* sorted_to_original, uint32_t* cell_start,
+                     uint32_t* pid_length, void* stream);
+AL_API int al_grid_sort_f64(al_engine* engine, const al_const_f64* cn,
+                     const al_consti* cni, const double* particle_x,
+                     uint32_t num_particles, uint32_t* particle_cell,
+                     uint32_t* sorted_to_original, uint32_t* cell_start,
+                     uint32_t* pid_length, void* stream);
+
+/* ------------------------------------------------ neighbors and density
+ * Solver::update_particle_neighbors<0> (solver.hpp:225-260) for the
+ * volume-map boundary method: grid sort, neighbor list
+ * (make_neighbor_list<0>, runner.hpp:1869-1911) and density
+ * (compute_density, runner.hpp:2052-2072).
+ *
+ *   particle_boundary_kernel [nb][N][4] device in, or NULL when
+ *                            cni->num_boundaries == 0
+ *   particle_density         [N] device out
+ *   particle_num_neighbors   [N] device out (min(count, cap))
+ *   particle_neighbors       [N][cap][4] device out or NULL; entries are
+ *                            {x_i - x_j, bits(j)} in canonical order
+ *                            (ascending (cell, index) of j)
+ *   grid_anomaly             [3] device out or NULL (reference flags)
+ * When a particle has more than cap neighbors the first cap canonical
+ * entries are kept and AL_ERR_NEIGHBOR_OVERFLOW is returned. */
+AL_API int al_update_particle_neighbors_f32(
+    al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+    const float* particle_x, uint32_t num_particles,
+    const float* particle_boundary_kernel, float* particle_density,
+    uint32_t* particle_num_neighbors, float* particle_neighbors,
+    uint32_t* grid_anomaly, void* stream);
+AL_API int al_update_particle_neighbors_f64(
+    al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+    const double* particle_x, uint32_t num_particles,
+    const double* particle_boundary_kernel, double* particle_density,
+    uint32_t* particle_num_neighbors, double* particle_neighbors,
+    uint32_t* grid_anomaly, void* stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* ALLUVION_B200_H */

@@ -1,0 +1,390 @@
+// oracle_capi.cpp -- C entry points of the CPU ORACLE (test infrastructure).
+//
+// Loaded by tests/ (as the checker) and by bench.py's CPU-baseline leg only.
+// All pointers are HOST pointers; layouts are the reference's (see
+// include/alluvion_b200.h).  Each function restates the reference routine
+// named in sph_oracle.hpp.
+#include <omp.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "sph_oracle.hpp"
+
+using namespace oracle;
+
+namespace {
+
+template <class TF>
+V3<TF> v3(const TF* p) {
+  return V3<TF>{p[0], p[1], p[2]};
+}
+
+template <class TF, class B>
+Body<TF> make_body(const B& b, const TF* rigid) {
+  Body<TF> o{};
+  o.shape = b.shape;
+  o.use_grid = b.use_distance_grid;
+  o.sign = b.sign;
+  o.dmin = v3<TF>(b.domain_min);
+  o.dmax = v3<TF>(b.domain_max);
+  o.cs = v3<TF>(b.cell_size);
+  for (int k = 0; k < 3; ++k) o.res[k] = b.resolution[k];
+  o.num_nodes = b.num_nodes;
+  o.dist_nodes = b.distance_nodes;
+  o.vol_nodes = b.volume_nodes;
+  o.sdf.kind = b.shape;
+  for (int k = 0; k < 8; ++k) o.sdf.p[k] = b.shape_params[k];
+  o.max_distance = b.max_distance;
+  o.mass = b.mass;
+  o.inertia = v3<TF>(b.inertia);
+  // rigid: x[3] v[3] q[4] omega[3]
+  if (rigid) {
+    o.x = v3<TF>(rigid);
+    o.v = v3<TF>(rigid + 3);
+    o.q = V4<TF>{rigid[6], rigid[7], rigid[8], rigid[9]};
+    o.omega = v3<TF>(rigid + 10);
+  } else {
+    o.x = {0, 0, 0};
+    o.v = {0, 0, 0};
+    o.q = {0, 0, 0, 1};
+    o.omega = {0, 0, 0};
+  }
+  return o;
+}
+
+template <class TF>
+void load_fluid(Fluid<TF>& f, uint32_t n, uint32_t nb, const TF* x, const TF* v) {
+  f.x.resize(n);
+  f.v.resize(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    f.x[i] = v3<TF>(x + 3 * size_t(i));
+    f.v[i] = v ? v3<TF>(v + 3 * size_t(i)) : V3<TF>{0, 0, 0};
+  }
+  f.resize(n, nb);
+}
+
+template <class TF, class C>
+int grid_sort_impl(const C* cn, const al_consti* cni, const TF* x, uint32_t n, uint32_t* cell,
+                   uint32_t* sorted, uint32_t* cell_start, uint32_t* flags) {
+  Cn<TF> c = make_cn<TF>(*cn);
+  std::vector<V3<TF>> xs(n);
+  for (uint32_t i = 0; i < n; ++i) xs[i] = v3<TF>(x + 3 * size_t(i));
+  GridSort s = grid_sort(c, *cni, xs.data(), n);
+  std::copy(s.cell.begin(), s.cell.end(), cell);
+  std::copy(s.sorted.begin(), s.sorted.end(), sorted);
+  if (cell_start) std::copy(s.cell_start.begin(), s.cell_start.end(), cell_start);
+  flags[0] = s.out_of_grid;
+  flags[1] = s.cell_overflow;
+  return 0;
+}
+
+template <class TF, class C>
+int neighbors_impl(const C* cn, const al_consti* cni, const TF* x, uint32_t n,
+                   const TF* boundary_kernel, TF* density, uint32_t* count, uint32_t* index,
+                   TF* neighbors, uint32_t* flags) {
+  Cn<TF> c = make_cn<TF>(*cn);
+  Fluid<TF> f;
+  load_fluid<TF>(f, n, cni->num_boundaries, x, nullptr);
+  if (boundary_kernel)
+    for (size_t k = 0; k < size_t(f.nb) * n; ++k)
+      f.bk[k] = V4<TF>{boundary_kernel[4 * k], boundary_kernel[4 * k + 1],
+                       boundary_kernel[4 * k + 2], boundary_kernel[4 * k + 3]};
+  update_particle_neighbors(c, *cni, f);
+  const uint32_t cap = f.nl.cap;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (density) density[i] = f.density[i];
+    count[i] = f.nl.count[i];
+    for (uint32_t k = 0; k < cap; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * cap + k];
+      if (index) index[size_t(i) * cap + k] = k < f.nl.count[i] ? j : 0xffffffffu;
+      if (neighbors && k < f.nl.count[i]) {
+        TF* e = neighbors + (size_t(i) * cap + k) * 4;
+        V3<TF> d = f.x[i] - f.x[j];
+        e[0] = d.x;
+        e[1] = d.y;
+        e[2] = d.z;
+        std::memcpy(&e[3], &j, sizeof(uint32_t));
+      }
+    }
+  }
+  flags[0] = f.gs.out_of_grid;
+  flags[1] = f.gs.cell_overflow;
+  flags[2] = f.nl.overflow;
+  return 0;
+}
+
+template <class TF>
+void node_positions_impl(const TF* dmin, const uint32_t* res, const TF* cs, TF* out) {
+  uint32_t nn = num_grid_nodes(res);
+  V3<TF> lo = v3<TF>(dmin), c = v3<TF>(cs);
+  for (uint32_t l = 0; l < nn; ++l) {
+    V3<TF> p = node_position(lo, res, c, l);
+    out[3 * size_t(l)] = p.x;
+    out[3 * size_t(l) + 1] = p.y;
+    out[3 * size_t(l) + 2] = p.z;
+  }
+}
+
+// Distance nodes sampled from the analytic SDF at the node positions (the
+// role CubicLagrangeDiscreteGrid::addFunction plays for mesh distances,
+// pile.hpp:79-94).
+template <class TF, class B>
+void distance_grid_impl(const B* b, TF* out) {
+  Body<TF> body = make_body<TF>(*b, nullptr);
+#pragma omp parallel for schedule(static)
+  for (int64_t l = 0; l < int64_t(body.num_nodes); ++l)
+    out[l] = body.sdf.sdf(node_position(body.dmin, body.res, body.cs, uint32_t(l)));
+}
+
+template <class TF, class C, class B>
+void volume_field_impl(const C* cn, const B* b, TF* out) {
+  Cn<TF> c = make_cn<TF>(*cn);
+  Body<TF> body = make_body<TF>(*b, nullptr);
+  PeirceTables pt = peirce_tables();
+  LagrangeGrid<TF> grid{body.dmin, body.dmax, body.cs, {body.res[0], body.res[1], body.res[2]},
+                        body.dist_nodes};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t l = 0; l < int64_t(body.num_nodes); ++l) {
+    V3<TF> x = node_position(body.dmin, body.res, body.cs, uint32_t(l));
+    if (body.use_grid)
+      out[l] = volume_at(c, pt, x, body.sign, [&](V3<TF> p) { return grid.value(p); });
+    else
+      out[l] = volume_at(c, pt, x, body.sign, [&](V3<TF> p) { return body.sdf.sdf(p); });
+  }
+}
+
+template <class TF, class C, class B>
+void boundary_impl(const C* cn, const B* bodies, const TF* rigid, uint32_t nb, const TF* x,
+                   uint32_t n, TF* bnd, TF* bk) {
+  Cn<TF> c = make_cn<TF>(*cn);
+  std::vector<Body<TF>> bs;
+  for (uint32_t b = 0; b < nb; ++b) bs.push_back(make_body<TF>(bodies[b], rigid + 13 * b));
+  Fluid<TF> f;
+  load_fluid<TF>(f, n, nb, x, nullptr);
+  compute_boundaries(c, bs, f);
+  for (size_t k = 0; k < size_t(nb) * n; ++k) {
+    bnd[4 * k] = f.bnd[k].x;
+    bnd[4 * k + 1] = f.bnd[k].y;
+    bnd[4 * k + 2] = f.bnd[k].z;
+    bnd[4 * k + 3] = f.bnd[k].w;
+    bk[4 * k] = f.bk[k].x;
+    bk[4 * k + 1] = f.bk[k].y;
+    bk[4 * k + 2] = f.bk[k].z;
+    bk[4 * k + 3] = f.bk[k].w;
+  }
+}
+
+// Runs `steps` solver steps on host arrays.  State arrays are in/out.
+// rigid: nb x 13 values (x, v, q, omega).  reports: `steps` entries.
+template <class TF, class C, class B>
+int run_impl(bool iisph, const C* cn, const al_consti* cni, const B* bodies, TF* rigid,
+             uint32_t n, TF* x, TF* v, TF* kappa_or_pressure, TF* kappa_v, TF* density,
+             TF* density_adv, TF* a, const al_solver_params* sp_in, TF* dt, uint32_t steps,
+             al_step_report* reports) {
+  Cn<TF> c = make_cn<TF>(*cn);
+  const uint32_t nb = cni->num_boundaries;
+  std::vector<Body<TF>> bs;
+  for (uint32_t b = 0; b < nb; ++b) bs.push_back(make_body<TF>(bodies[b], rigid + 13 * b));
+  Fluid<TF> f;
+  f.x.resize(n);
+  f.v.resize(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    f.x[i] = v3<TF>(x + 3 * size_t(i));
+    f.v[i] = v3<TF>(v + 3 * size_t(i));
+  }
+  f.kappa.assign(n, 0);
+  f.kappa_v.assign(n, 0);
+  f.pressure.assign(n, 0);
+  if (iisph) {
+    if (kappa_or_pressure) std::copy(kappa_or_pressure, kappa_or_pressure + n, f.pressure.begin());
+  } else {
+    if (kappa_or_pressure) std::copy(kappa_or_pressure, kappa_or_pressure + n, f.kappa.begin());
+    if (kappa_v) std::copy(kappa_v, kappa_v + n, f.kappa_v.begin());
+  }
+  f.resize(n, nb);
+  SolverParams sp;
+  sp.density_change_tolerance = sp_in->density_change_tolerance;
+  sp.density_error_tolerance = sp_in->density_error_tolerance;
+  sp.min_density_solve = sp_in->min_density_solve;
+  sp.max_density_solve = sp_in->max_density_solve;
+  sp.min_divergence_solve = sp_in->min_divergence_solve;
+  sp.max_divergence_solve = sp_in->max_divergence_solve;
+  sp.enable_divergence_solve = sp_in->enable_divergence_solve != 0;
+  sp.enable_density_solve = sp_in->enable_density_solve != 0;
+  sp.cfl = sp_in->cfl;
+  sp.max_dt = sp_in->max_dt;
+  sp.min_dt = sp_in->min_dt;
+  V3<TF> pg{TF(sp_in->pile_gravity[0]), TF(sp_in->pile_gravity[1]), TF(sp_in->pile_gravity[2])};
+  TF step_dt = *dt;
+  for (uint32_t s = 0; s < steps; ++s) {
+    std::vector<V3<double>> F, T;
+    StepReport r = iisph ? ii_step(c, *cni, bs, f, sp, step_dt, pg, sp_in->integrate_rigids != 0, &F, &T)
+                         : df_step(c, *cni, bs, f, sp, step_dt, pg, sp_in->integrate_rigids != 0, &F, &T);
+    if (reports) {
+      al_step_report& o = reports[s];
+      std::memset(&o, 0, sizeof(o));
+      o.num_divergence_solve = r.num_divergence_solve;
+      o.num_density_solve = r.num_density_solve;
+      o.mean_density_change = r.mean_density_change;
+      o.mean_density_error = r.mean_density_error;
+      o.particle_max_v2 = r.particle_max_v2;
+      o.pile_max_v2 = r.pile_max_v2;
+      o.max_v2 = r.max_v2;
+      o.cfl_dt = r.cfl_dt;
+      o.utilized_cfl = r.utilized_cfl;
+      o.dt = r.dt;
+      for (int k = 0; k < 3; ++k) o.grid_anomaly[k] = r.grid_anomaly[k];
+      uint32_t active = 0;
+      for (size_t k = 0; k < f.bnd.size(); ++k) active += f.bnd[k].w != 0;
+      o.num_active_boundary_pairs = active;
+      for (uint32_t b = 0; b < nb && b < AL_MAX_BOUNDARIES; ++b) {
+        o.force[b][0] = F[b].x;
+        o.force[b][1] = F[b].y;
+        o.force[b][2] = F[b].z;
+        o.torque[b][0] = T[b].x;
+        o.torque[b][1] = T[b].y;
+        o.torque[b][2] = T[b].z;
+      }
+    }
+  }
+  *dt = step_dt;
+  for (uint32_t i = 0; i < n; ++i) {
+    x[3 * size_t(i)] = f.x[i].x;
+    x[3 * size_t(i) + 1] = f.x[i].y;
+    x[3 * size_t(i) + 2] = f.x[i].z;
+    v[3 * size_t(i)] = f.v[i].x;
+    v[3 * size_t(i) + 1] = f.v[i].y;
+    v[3 * size_t(i) + 2] = f.v[i].z;
+    if (density) density[i] = f.density[i];
+    if (density_adv) density_adv[i] = f.density_adv[i];
+    if (a) {
+      a[3 * size_t(i)] = f.a[i].x;
+      a[3 * size_t(i) + 1] = f.a[i].y;
+      a[3 * size_t(i) + 2] = f.a[i].z;
+    }
+    if (iisph) {
+      if (kappa_or_pressure) kappa_or_pressure[i] = f.pressure[i];
+    } else {
+      if (kappa_or_pressure) kappa_or_pressure[i] = f.kappa[i];
+      if (kappa_v) kappa_v[i] = f.kappa_v[i];
+    }
+  }
+  for (uint32_t b = 0; b < nb; ++b) {
+    TF* r = rigid + 13 * b;
+    const Body<TF>& o = bs[b];
+    TF vals[13] = {o.x.x, o.x.y, o.x.z, o.v.x, o.v.y, o.v.z, o.q.x,
+                   o.q.y, o.q.z, o.q.w, o.omega.x, o.omega.y, o.omega.z};
+    std::copy(vals, vals + 13, r);
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_num_threads(void) { return omp_get_max_threads(); }
+void orc_set_num_threads(int n) { omp_set_num_threads(n); }
+
+void orc_peirce_tables(double* cosphi, double* sinphi, double* b, double* r, double* c) {
+  PeirceTables t = peirce_tables();
+  std::copy(t.cosphi, t.cosphi + kNumPhi, cosphi);
+  std::copy(t.sinphi, t.sinphi + kNumPhi, sinphi);
+  std::copy(t.b, t.b + kNumPhi, b);
+  std::copy(t.r, t.r + kNumR, r);
+  std::copy(t.c, t.c + kNumR, c);
+}
+
+int orc_grid_sort_f32(const al_const_f32* cn, const al_consti* cni, const float* x, uint32_t n,
+                      uint32_t* cell, uint32_t* sorted, uint32_t* cell_start, uint32_t* flags) {
+  return grid_sort_impl<float>(cn, cni, x, n, cell, sorted, cell_start, flags);
+}
+int orc_grid_sort_f64(const al_const_f64* cn, const al_consti* cni, const double* x, uint32_t n,
+                      uint32_t* cell, uint32_t* sorted, uint32_t* cell_start, uint32_t* flags) {
+  return grid_sort_impl<double>(cn, cni, x, n, cell, sorted, cell_start, flags);
+}
+
+int orc_update_particle_neighbors_f32(const al_const_f32* cn, const al_consti* cni,
+                                      const float* x, uint32_t n, const float* boundary_kernel,
+                                      float* density, uint32_t* count, uint32_t* index,
+                                      float* neighbors, uint32_t* flags) {
+  return neighbors_impl<float>(cn, cni, x, n, boundary_kernel, density, count, index, neighbors,
+                               flags);
+}
+int orc_update_particle_neighbors_f64(const al_const_f64* cn, const al_consti* cni,
+                                      const double* x, uint32_t n, const double* boundary_kernel,
+                                      double* density, uint32_t* count, uint32_t* index,
+                                      double* neighbors, uint32_t* flags) {
+  return neighbors_impl<double>(cn, cni, x, n, boundary_kernel, density, count, index, neighbors,
+                                flags);
+}
+
+uint32_t orc_num_grid_nodes(const uint32_t* res) { return num_grid_nodes(res); }
+void orc_node_positions_f32(const float* dmin, const uint32_t* res, const float* cs, float* out) {
+  node_positions_impl<float>(dmin, res, cs, out);
+}
+void orc_node_positions_f64(const double* dmin, const uint32_t* res, const double* cs,
+                            double* out) {
+  node_positions_impl<double>(dmin, res, cs, out);
+}
+
+// Shape functions at reference coordinates xi (3 values): N[32], dN[3][32].
+void orc_shape_functions_f64(const double* xi, double* N, double* dN) {
+  shape_functions<double>(V3<double>{xi[0], xi[1], xi[2]}, N, dN, dN + 32, dN + 64);
+}
+void orc_cell_nodes(const uint32_t* res, const int* ipos, uint32_t* out) {
+  cell_nodes(res, ipos, out);
+}
+
+void orc_distance_grid_f32(const al_body_f32* b, float* out) { distance_grid_impl<float>(b, out); }
+void orc_distance_grid_f64(const al_body_f64* b, double* out) {
+  distance_grid_impl<double>(b, out);
+}
+void orc_volume_field_f32(const al_const_f32* cn, const al_body_f32* b, float* out) {
+  volume_field_impl<float>(cn, b, out);
+}
+void orc_volume_field_f64(const al_const_f64* cn, const al_body_f64* b, double* out) {
+  volume_field_impl<double>(cn, b, out);
+}
+
+void orc_boundary_f32(const al_const_f32* cn, const al_body_f32* bodies, const float* rigid,
+                      uint32_t nb, const float* x, uint32_t n, float* bnd, float* bk) {
+  boundary_impl<float>(cn, bodies, rigid, nb, x, n, bnd, bk);
+}
+void orc_boundary_f64(const al_const_f64* cn, const al_body_f64* bodies, const double* rigid,
+                      uint32_t nb, const double* x, uint32_t n, double* bnd, double* bk) {
+  boundary_impl<double>(cn, bodies, rigid, nb, x, n, bnd, bk);
+}
+
+int orc_df_run_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f32* bodies,
+                   float* rigid, uint32_t n, float* x, float* v, float* kappa, float* kappa_v,
+                   float* density, float* density_adv, float* a, const al_solver_params* sp,
+                   float* dt, uint32_t steps, al_step_report* reports) {
+  return run_impl<float>(false, cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density,
+                         density_adv, a, sp, dt, steps, reports);
+}
+int orc_df_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f64* bodies,
+                   double* rigid, uint32_t n, double* x, double* v, double* kappa,
+                   double* kappa_v, double* density, double* density_adv, double* a,
+                   const al_solver_params* sp, double* dt, uint32_t steps,
+                   al_step_report* reports) {
+  return run_impl<double>(false, cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density,
+                          density_adv, a, sp, dt, steps, reports);
+}
+int orc_ii_run_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f32* bodies,
+                   float* rigid, uint32_t n, float* x, float* v, float* pressure, float* density,
+                   float* density_adv, float* a, const al_solver_params* sp, float* dt,
+                   uint32_t steps, al_step_report* reports) {
+  return run_impl<float>(true, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+                         density_adv, a, sp, dt, steps, reports);
+}
+int orc_ii_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f64* bodies,
+                   double* rigid, uint32_t n, double* x, double* v, double* pressure,
+                   double* density, double* density_adv, double* a, const al_solver_params* sp,
+                   double* dt, uint32_t steps, al_step_report* reports) {
+  return run_impl<double>(true, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+                          density_adv, a, sp, dt, steps, reports);
+}
+
+}  // extern "C"

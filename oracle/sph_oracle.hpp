@@ -1,0 +1,1313 @@
+// sph_oracle.hpp -- CPU ORACLE (test infrastructure, not product code).
+//
+// A C++17 + OpenMP restatement of kennychufk/alluvion's SPH fluid-step path,
+// templated on the real type (float / double).  Only tests/, the smoke check
+// and bench.py's CPU-baseline leg may load it; the engine never calls it.
+//
+// Every routine cites the reference file:line it restates.  Paths are
+// relative to the reference project root; "runner.hpp" means
+// include/alluvion/runner.hpp.
+//
+// Deliberate, documented differences from the reference:
+//  * cell index uses IEEE x / h (the reference builds with --use_fast_math,
+//    whose division is not reproducible); the engine uses the same rule.
+//  * buckets are unbounded and ordered canonically by (cell, index) instead
+//    of atomicAdd order (runner.hpp:1853); neighbor lists follow that order.
+//  * rigid force / torque totals and the solvers' convergence means are
+//    accumulated in double (the reference sums FP32 with thrust).
+//  * contacts (pile.hpp:826-979) are out of scope and not applied.
+// Arithmetic that decides neighbor membership is written with explicit
+// operation order; this file must be compiled with -ffp-contract=off.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "alluvion_b200.h"
+
+namespace oracle {
+
+// ------------------------------------------------------------------ vectors
+template <class T>
+struct V3 {
+  T x, y, z;
+};
+template <class T>
+struct V4 {
+  T x, y, z, w;
+};
+template <class T>
+inline V3<T> operator+(V3<T> a, V3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T>
+inline V3<T> operator-(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T>
+inline V3<T> operator-(V3<T> a) { return {-a.x, -a.y, -a.z}; }
+template <class T>
+inline V3<T> operator*(T s, V3<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T>
+inline V3<T> operator*(V3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T>
+inline V3<T>& operator+=(V3<T>& a, V3<T> b) { a = a + b; return a; }
+template <class T>
+inline V3<T>& operator-=(V3<T>& a, V3<T> b) { a = a - b; return a; }
+template <class T>
+inline T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T>
+inline T length_sqr(V3<T> a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+template <class T>
+inline V3<T> cross(V3<T> a, V3<T> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T>
+inline T inv_sqrt(T v) { return T(1) / std::sqrt(v); }
+template <class T>
+inline V3<T> normalized(V3<T> a) { return inv_sqrt(dot(a, a)) * a; }
+
+// Quaternion {x, y, z, w}.  Rotation matrix as runner.hpp:141-154.
+template <class T>
+inline V3<T> rotate(V3<T> v, V4<T> q) {
+  V3<T> r;
+  r.x = (1 - 2 * (q.y * q.y + q.z * q.z)) * v.x + 2 * (q.x * q.y - q.z * q.w) * v.y +
+        2 * (q.x * q.z + q.y * q.w) * v.z;
+  r.y = 2 * (q.x * q.y + q.z * q.w) * v.x + (1 - 2 * (q.x * q.x + q.z * q.z)) * v.y +
+        2 * (q.y * q.z - q.x * q.w) * v.z;
+  r.z = 2 * (q.x * q.z - q.y * q.w) * v.x + 2 * (q.y * q.z + q.x * q.w) * v.y +
+        (1 - 2 * (q.x * q.x + q.y * q.y)) * v.z;
+  return r;
+}
+template <class T>
+inline V4<T> conjugate(V4<T> q) { return {-q.x, -q.y, -q.z, q.w}; }
+
+// ---------------------------------------------------------- parameter view
+template <class TF>
+struct Cn {
+  TF h, h2, k, l, w0, radius, vol, mass, rho0, visc, bvisc, eps;
+  V3<TF> g;
+};
+template <class TF, class C>
+inline Cn<TF> make_cn(const C& c) {
+  return Cn<TF>{c.kernel_radius, c.kernel_radius_sqr, c.cubic_kernel_k, c.cubic_kernel_l,
+                c.cubic_kernel_zero, c.particle_radius, c.particle_vol, c.particle_mass,
+                c.density0, c.viscosity, c.boundary_viscosity, c.dfsph_factor_epsilon,
+                V3<TF>{c.gravity[0], c.gravity[1], c.gravity[2]}};
+}
+
+// ------------------------------------------------------------ SPH kernels
+// Cubic spline W(r) of a distance (dist_cubic_kernel, runner.hpp:596-606).
+template <class TF>
+inline TF W_dist(const Cn<TF>& c, TF r) {
+  TF q = std::fabs(r) / c.h;
+  TF conj = 1 - q;
+  TF s = 0;
+  if (q <= TF(0.5))
+    s = (6 * q - 6) * q * q + 1;
+  else if (q <= 1)
+    s = 2 * conj * conj * conj;
+  return s * c.k;
+}
+// W of a squared distance (d2_cubic_kernel, runner.hpp:608-619).
+template <class TF>
+inline TF W_r2(const Cn<TF>& c, TF r2) {
+  TF q2 = r2 / c.h2;
+  TF q = std::sqrt(r2) / c.h;
+  TF conj = 1 - q;
+  TF s = 0;
+  if (q <= TF(0.5))
+    s = (6 * q - 6) * q2 + 1;
+  else if (q <= 1)
+    s = 2 * conj * conj * conj;
+  return s * c.k;
+}
+// Gradient of W for a displacement (displacement_cubic_kernel_grad,
+// runner.hpp:628-638).
+template <class TF>
+inline V3<TF> gradW(const Cn<TF>& c, V3<TF> d) {
+  TF rl2 = length_sqr(d);
+  TF rl = std::sqrt(rl2);
+  TF q = rl / c.h;
+  TF s = q <= TF(0.5) ? (q * 3 - 2) / c.h : (q <= 1 ? (1 - q) * (q - 1) / rl : TF(0));
+  return (c.l * s) * d;
+}
+
+// ------------------------------------------------------------------- grid
+constexpr uint32_t kNoCell = 0xffffffffu;
+
+// Cell of a position (get_ipos / within_grid, runner.hpp:1827-1838) with
+// IEEE division.  Returns kNoCell outside the grid.
+template <class TF>
+inline void cell_coords(const Cn<TF>& c, const al_consti& g, V3<TF> x, int out[3]) {
+  out[0] = int(std::floor(x.x / c.h)) - g.grid_offset[0];
+  out[1] = int(std::floor(x.y / c.h)) - g.grid_offset[1];
+  out[2] = int(std::floor(x.z / c.h)) - g.grid_offset[2];
+}
+inline bool in_grid(const al_consti& g, const int p[3]) {
+  return p[0] >= 0 && p[0] < int(g.grid_res[0]) && p[1] >= 0 && p[1] < int(g.grid_res[1]) &&
+         p[2] >= 0 && p[2] < int(g.grid_res[2]);
+}
+inline uint32_t cell_linear(const al_consti& g, const int p[3]) {
+  return (uint32_t(p[0]) * g.grid_res[1] + uint32_t(p[1])) * g.grid_res[2] + uint32_t(p[2]);
+}
+
+struct GridSort {
+  std::vector<uint32_t> cell;        // per original particle
+  std::vector<uint32_t> sorted;      // sorted slot -> original index
+  std::vector<uint32_t> cell_start;  // ncells + 1
+  bool out_of_grid = false;
+  bool cell_overflow = false;
+};
+
+// Canonical replacement of update_particle_grid (runner.hpp:1840-1867):
+// stable counting sort by cell; out-of-grid particles go last.
+template <class TF>
+GridSort grid_sort(const Cn<TF>& c, const al_consti& g, const V3<TF>* x, uint32_t n) {
+  GridSort s;
+  const uint32_t ncells = g.grid_res[0] * g.grid_res[1] * g.grid_res[2];
+  s.cell.resize(n);
+  s.cell_start.assign(size_t(ncells) + 1, 0);
+  std::vector<uint32_t> count(ncells, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    int p[3];
+    cell_coords(c, g, x[i], p);
+    if (in_grid(g, p)) {
+      s.cell[i] = cell_linear(g, p);
+      ++count[s.cell[i]];
+    } else {
+      s.cell[i] = kNoCell;
+      s.out_of_grid = true;
+    }
+  }
+  uint32_t run = 0;
+  for (uint32_t k = 0; k < ncells; ++k) {
+    s.cell_start[k] = run;
+    run += count[k];
+    if (count[k] > g.max_num_particles_per_cell) s.cell_overflow = true;
+  }
+  s.cell_start[ncells] = run;
+  s.sorted.resize(n);
+  std::vector<uint32_t> cursor(s.cell_start.begin(), s.cell_start.end() - 1);
+  uint32_t tail = run;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (s.cell[i] == kNoCell)
+      s.sorted[tail++] = i;
+    else
+      s.sorted[cursor[s.cell[i]]++] = i;
+  }
+  return s;
+}
+
+// Squared distance with a fixed operation order ((dx*dx + dy*dy) + dz*dz),
+// the order length_sqr uses in the reference.
+template <class TF>
+inline TF dist2(V3<TF> a, V3<TF> b) {
+  TF dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  return (dx * dx + dy * dy) + dz * dz;
+}
+
+struct NeighborList {
+  uint32_t cap = 0;
+  std::vector<uint32_t> count;  // min(found, cap)
+  std::vector<uint32_t> index;  // [n][cap] original indices, canonical order
+  bool overflow = false;
+};
+
+// make_neighbor_list<0> (runner.hpp:1869-1911): scan the 27 cells in
+// ascending cell order, keep j != i with |x_i - x_j|^2 < h^2.  The reference
+// clamps at cap with slot cap-1 overwritten; here the first cap canonical
+// entries are kept and `overflow` is raised.
+template <class TF>
+NeighborList neighbor_list(const Cn<TF>& c, const al_consti& g, const V3<TF>* x, uint32_t n,
+                           const GridSort& s) {
+  NeighborList nl;
+  nl.cap = g.max_num_neighbors_per_particle;
+  nl.count.assign(n, 0);
+  nl.index.assign(size_t(n) * nl.cap, 0);
+  bool overflow = false;
+#pragma omp parallel for schedule(static) reduction(|| : overflow)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    int p[3];
+    cell_coords(c, g, x[i], p);
+    uint32_t found = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          int q[3] = {p[0] + dx, p[1] + dy, p[2] + dz};
+          if (!in_grid(g, q)) continue;
+          uint32_t cell = cell_linear(g, q);
+          for (uint32_t t = s.cell_start[cell]; t < s.cell_start[cell + 1]; ++t) {
+            uint32_t j = s.sorted[t];
+            if (j == i) continue;
+            if (dist2(x[i], x[j]) < c.h2) {
+              if (found < nl.cap) nl.index[size_t(i) * nl.cap + found] = j;
+              ++found;
+            }
+          }
+        }
+    if (found > nl.cap) overflow = true;
+    nl.count[i] = std::min(found, nl.cap);
+  }
+  nl.overflow = overflow;
+  return nl;
+}
+
+// -------------------------------------------- cubic Lagrange grid (32 nodes)
+struct GridShape {
+  uint32_t res[3];
+};
+
+// Node position of linear node index l (index_to_node_position,
+// runner.hpp:1131-1178): vertices first (x fastest), then the two
+// third-point nodes of every x-, y- and z-edge.
+template <class TF>
+V3<TF> node_position(V3<TF> dmin, const uint32_t r[3], V3<TF> cs, uint32_t l) {
+  const uint32_t nx = r[0], ny = r[1], nz = r[2];
+  const uint32_t nv = (nx + 1) * (ny + 1) * (nz + 1);
+  const uint32_t nex = nx * (ny + 1) * (nz + 1);
+  const uint32_t ney = (nx + 1) * ny * (nz + 1);
+  auto at = [&](uint32_t a, uint32_t b, uint32_t cc) {
+    return V3<TF>{dmin.x + cs.x * TF(a), dmin.y + cs.y * TF(b), dmin.z + cs.z * TF(cc)};
+  };
+  if (l < nv) {
+    uint32_t t = l % ((ny + 1) * (nx + 1));
+    return at(t % (nx + 1), t / (nx + 1), l / ((ny + 1) * (nx + 1)));
+  }
+  if (l < nv + 2 * nex) {
+    l -= nv;
+    uint32_t e = l / 2, t = e % ((ny + 1) * nx);
+    V3<TF> p = at(t % nx, t / nx, e / ((ny + 1) * nx));
+    p.x += (TF(1) + TF(l % 2)) / TF(3) * cs.x;
+    return p;
+  }
+  if (l < nv + 2 * (nex + ney)) {
+    l -= nv + 2 * nex;
+    uint32_t e = l / 2, t = e % ((nz + 1) * ny);
+    V3<TF> p = at(e / ((nz + 1) * ny), t % ny, t / ny);
+    p.y += (TF(1) + TF(l % 2)) / TF(3) * cs.y;
+    return p;
+  }
+  l -= nv + 2 * (nex + ney);
+  uint32_t e = l / 2, t = e % ((nx + 1) * nz);
+  V3<TF> p = at(t / nz, e / ((nx + 1) * nz), t % nz);
+  p.z += (TF(1) + TF(l % 2)) / TF(3) * cs.z;
+  return p;
+}
+
+inline uint32_t num_grid_nodes(const uint32_t r[3]) {
+  const uint32_t nx = r[0], ny = r[1], nz = r[2];
+  return (nx + 1) * (ny + 1) * (nz + 1) +
+         2 * (nx * (ny + 1) * (nz + 1) + (nx + 1) * ny * (nz + 1) + (nx + 1) * (ny + 1) * nz);
+}
+
+// Cell lookup (resolve, runner.hpp:1180-1195).  Returns false outside.
+template <class TF>
+bool resolve(V3<TF> dmin, V3<TF> dmax, const uint32_t r[3], V3<TF> cs, V3<TF> x, int ip[3],
+             V3<TF>& xi) {
+  V3<TF> inv{TF(1) / cs.x, TF(1) / cs.y, TF(1) / cs.z};
+  if (!(x.x >= dmin.x && x.y >= dmin.y && x.z >= dmin.z && dmax.x >= x.x && dmax.y >= x.y &&
+        dmax.z >= x.z))
+    return false;
+  ip[0] = std::min(int((x.x - dmin.x) * inv.x), int(r[0]) - 1);
+  ip[1] = std::min(int((x.y - dmin.y) * inv.y), int(r[1]) - 1);
+  ip[2] = std::min(int((x.z - dmin.z) * inv.z), int(r[2]) - 1);
+  V3<TF> lo{dmin.x + cs.x * TF(ip[0]), dmin.y + cs.y * TF(ip[1]), dmin.z + cs.z * TF(ip[2])};
+  xi = {2 * (x.x - lo.x) * inv.x - 1, 2 * (x.y - lo.y) * inv.y - 1, 2 * (x.z - lo.z) * inv.z - 1};
+  return true;
+}
+
+// The 32 node indices of a cell (get_cells, runner.hpp:1197-1257): 8 corner
+// vertices, then for the x-, y- and z-edge families four edges of two
+// third-point nodes each.
+inline void cell_nodes(const uint32_t r[3], const int ip[3], uint32_t out[32]) {
+  const uint32_t nx = r[0], ny = r[1], nz = r[2];
+  const uint32_t x = ip[0], y = ip[1], z = ip[2];
+  for (uint32_t j = 0; j < 8; ++j) {
+    uint32_t a = x + (j & 1), b = y + ((j >> 1) & 1), cc = z + ((j >> 2) & 1);
+    out[j] = (nx + 1) * (ny + 1) * cc + (nx + 1) * b + a;
+  }
+  uint32_t base = (nx + 1) * (ny + 1) * (nz + 1);
+  // x-edges: pair (e>>1)&1 -> z offset, (e>>2)&1 -> y offset
+  for (uint32_t e = 0; e < 8; e += 2) {
+    uint32_t oz = (e >> 1) & 1, oy = (e >> 2) & 1;
+    uint32_t k = base + 2 * (nx * (ny + 1) * (z + oz) + nx * (y + oy) + x);
+    out[8 + e] = k;
+    out[9 + e] = k + 1;
+  }
+  base += 2 * (nx * (ny + 1) * (nz + 1));
+  // y-edges: (e>>1)&1 -> x offset, (e>>2)&1 -> z offset
+  for (uint32_t e = 0; e < 8; e += 2) {
+    uint32_t ox = (e >> 1) & 1, oz = (e >> 2) & 1;
+    uint32_t k = base + 2 * (ny * (nz + 1) * (x + ox) + ny * (z + oz) + y);
+    out[16 + e] = k;
+    out[17 + e] = k + 1;
+  }
+  base += 2 * ((nx + 1) * ny * (nz + 1));
+  // z-edges: (e>>1)&1 -> y offset, (e>>2)&1 -> x offset
+  for (uint32_t e = 0; e < 8; e += 2) {
+    uint32_t oy = (e >> 1) & 1, ox = (e >> 2) & 1;
+    uint32_t k = base + 2 * (nz * (nx + 1) * (y + oy) + nz * (x + ox) + z);
+    out[24 + e] = k;
+    out[25 + e] = k + 1;
+  }
+}
+
+// Shape functions of the 32-node cubic serendipity-type element and their
+// derivatives (the element of get_shape_function[_and_gradient],
+// runner.hpp:1259-1584):
+//   corner (sx,sy,sz):  (1/64)(1+sx x)(1+sy y)(1+sz z)(9(x^2+y^2+z^2) - 19)
+//   x-edge (s,sy,sz):   (9/64)(1-x^2)(1+3 s x)(1+sy y)(1+sz z)   (likewise y, z)
+// Node order matches cell_nodes().  Derivatives by the product rule.
+template <class TF>
+void shape_functions(V3<TF> p, TF N[32], TF* dN0, TF* dN1, TF* dN2) {
+  const TF x = p.x, y = p.y, z = p.z;
+  const TF r2 = x * x + y * y + z * z;
+  const TF c64 = TF(1) / TF(64), e64 = TF(9) / TF(64);
+  for (int j = 0; j < 8; ++j) {
+    TF sx = (j & 1) ? 1 : -1, sy = (j & 2) ? 1 : -1, sz = (j & 4) ? 1 : -1;
+    TF ax = 1 + sx * x, ay = 1 + sy * y, az = 1 + sz * z, f = 9 * r2 - 19;
+    N[j] = c64 * ax * ay * az * f;
+    if (dN0) {
+      dN0[j] = c64 * ay * az * (sx * f + 18 * x * ax);
+      dN1[j] = c64 * ax * az * (sy * f + 18 * y * ay);
+      dN2[j] = c64 * ax * ay * (sz * f + 18 * z * az);
+    }
+  }
+  // axis a is the edge direction; (b, c) the perpendicular directions whose
+  // offsets are selected by bits 1 and 2 of the node's index within the
+  // family (see cell_nodes).
+  auto edge_family = [&](int first, int axis, int bit1_axis, int bit2_axis) {
+    TF u[3] = {x, y, z};
+    for (int e = 0; e < 8; ++e) {
+      TF s = (e & 1) ? 1 : -1;
+      TF s1 = (e & 2) ? 1 : -1;
+      TF s2 = (e & 4) ? 1 : -1;
+      TF t = u[axis], a = 1 + s1 * u[bit1_axis], b = 1 + s2 * u[bit2_axis];
+      TF g = (1 - t * t) * (1 + 3 * s * t);
+      TF dg = 3 * s * (1 - t * t) - 2 * t * (1 + 3 * s * t);
+      N[first + e] = e64 * g * a * b;
+      if (dN0) {
+        TF d[3];
+        d[axis] = e64 * dg * a * b;
+        d[bit1_axis] = e64 * g * s1 * b;
+        d[bit2_axis] = e64 * g * a * s2;
+        dN0[first + e] = d[0];
+        dN1[first + e] = d[1];
+        dN2[first + e] = d[2];
+      }
+    }
+  };
+  edge_family(8, 0, 2, 1);   // x-edges: bit1 -> z, bit2 -> y
+  edge_family(16, 1, 0, 2);  // y-edges: bit1 -> x, bit2 -> z
+  edge_family(24, 2, 1, 0);  // z-edges: bit1 -> y, bit2 -> x
+}
+
+// Interpolated value (interpolate, runner.hpp:1586-1594) and, optionally,
+// gradient scaled by 2 / cell size (interpolate_and_derive,
+// runner.hpp:1773-1791).  Returns FLT/DBL max outside the domain
+// (interpolate_distance_without_intermediates, runner.hpp:1596-1614).
+template <class TF>
+struct LagrangeGrid {
+  V3<TF> dmin, dmax, cs;
+  uint32_t res[3];
+  const TF* nodes;
+  TF value(V3<TF> x) const {
+    int ip[3];
+    V3<TF> xi;
+    if (!resolve(dmin, dmax, res, cs, x, ip, xi)) return std::numeric_limits<TF>::max();
+    TF N[32];
+    uint32_t cells[32];
+    shape_functions<TF>(xi, N, nullptr, nullptr, nullptr);
+    cell_nodes(res, ip, cells);
+    TF phi = 0;
+    for (int j = 0; j < 32; ++j) phi += nodes[cells[j]] * N[j];
+    return phi;
+  }
+};
+
+// ------------------------------------------------------- analytic distances
+// dg/box_distance.hpp:23-39, dg/sphere_distance.hpp:18-21,
+// dg/box_shell_distance.hpp:36-59.  The torus (tube radius r around a circle
+// of radius R in the x-z plane) has no reference counterpart.
+template <class TF>
+struct Shape {
+  uint32_t kind;
+  TF p[8];
+  TF sdf(V3<TF> x) const {
+    switch (kind) {
+      case AL_SHAPE_BOX: {
+        V3<TF> d{std::fabs(x.x) - p[0], std::fabs(x.y) - p[1], std::fabs(x.z) - p[2]};
+        V3<TF> cl{std::max(d.x, TF(0)), std::max(d.y, TF(0)), std::max(d.z, TF(0))};
+        return std::sqrt(dot(cl, cl)) + std::min(std::max(d.x, std::max(d.y, d.z)), TF(0)) - p[3];
+      }
+      case AL_SHAPE_SPHERE:
+        return std::sqrt(dot(x, x)) - p[0];
+      case AL_SHAPE_BOX_SHELL: {
+        auto box = [&](TF hx, TF hy, TF hz) {
+          V3<TF> d{std::fabs(x.x) - hx, std::fabs(x.y) - hy, std::fabs(x.z) - hz};
+          V3<TF> cl{std::max(d.x, TF(0)), std::max(d.y, TF(0)), std::max(d.z, TF(0))};
+          return std::sqrt(dot(cl, cl)) + std::min(std::max(d.x, std::max(d.y, d.z)), TF(0)) -
+                 p[6];
+        };
+        TF inner = box(p[0], p[1], p[2]);
+        TF outer = box(p[3], p[4], p[5]);
+        return std::max(outer, -inner);
+      }
+      case AL_SHAPE_TORUS: {
+        TF rho = std::sqrt(x.x * x.x + x.z * x.z) - p[0];
+        return std::sqrt(rho * rho + x.y * x.y) - p[1];
+      }
+      default:
+        return std::numeric_limits<TF>::max();
+    }
+  }
+  // Un-normalised outward direction.  Sphere: the position itself
+  // (sphere_distance.hpp:21); others: central differences with step
+  // h * 2^-8 (box_distance.hpp:28-38).
+  V3<TF> gradient(V3<TF> x, TF h) const {
+    if (kind == AL_SHAPE_SPHERE) return x;
+    const TF step = h * TF(0.00390625);
+    return V3<TF>{sdf(x + V3<TF>{step, 0, 0}) - sdf(x - V3<TF>{step, 0, 0}),
+                  sdf(x + V3<TF>{0, step, 0}) - sdf(x - V3<TF>{0, step, 0}),
+                  sdf(x + V3<TF>{0, 0, step}) - sdf(x - V3<TF>{0, 0, step})};
+  }
+};
+
+// -------------------------------------------------------- Peirce quadrature
+// Peirce's product rule on the ball (dg/peirce_quadrature.hpp:10-13,
+// 484-510) for m = 14: 60 equally spaced azimuths theta_i = 2 pi (i+1)/60,
+// 30 Gauss-Legendre nodes in cos(phi) with weights b_j, and 15 radial
+// nodes r_k = sqrt(s_k) with s_k the Gauss-Jacobi(0, 1/2) nodes mapped to
+// [0,1] and weights c_k = w_k / 2^(5/2), so that sum c_k f(r_k) integrates
+// r^2 f(r) over [0,1].  Computed here from those definitions in long double.
+constexpr int kNumTheta = 60, kNumPhi = 30, kNumR = 15;
+
+struct PeirceTables {
+  double cosphi[kNumPhi], sinphi[kNumPhi], b[kNumPhi], r[kNumR], c[kNumR];
+};
+
+namespace detail {
+// Jacobi polynomial P_n^(a,b)(t) and its derivative by the three-term
+// recurrence (Abramowitz & Stegun 22.7.1, 22.8.1).
+inline void jacobi(int n, long double a, long double b, long double t, long double& p,
+                   long double& dp) {
+  auto value = [&](int m, long double aa, long double bb) {
+    long double p0 = 1, p1 = (aa + 1) + (aa + bb + 2) * (t - 1) / 2;
+    if (m == 0) return p0;
+    for (int k = 2; k <= m; ++k) {
+      long double s = 2 * k + aa + bb;
+      long double a1 = 2 * k * (k + aa + bb) * (s - 2);
+      long double a2 = (s - 1) * (aa * aa - bb * bb);
+      long double a3 = (s - 2) * (s - 1) * s;
+      long double a4 = 2 * (k + aa - 1) * (k + bb - 1) * s;
+      long double p2 = ((a2 + a3 * t) * p1 - a4 * p0) / a1;
+      p0 = p1;
+      p1 = p2;
+    }
+    return p1;
+  };
+  p = value(n, a, b);
+  dp = n == 0 ? 0 : (n + a + b + 1) / 2 * value(n - 1, a + 1, b + 1);
+}
+// Roots of P_n^(a,b) on (-1,1): sign-change bracketing then Newton.
+inline std::vector<long double> jacobi_roots(int n, long double a, long double b) {
+  std::vector<long double> roots;
+  const int kScan = 200000;
+  long double prev_t = -1, prev_p, dp;
+  jacobi(n, a, b, prev_t, prev_p, dp);
+  for (int s = 1; s <= kScan; ++s) {
+    long double t = -1 + 2.0L * s / kScan, p;
+    jacobi(n, a, b, t, p, dp);
+    if ((p < 0) != (prev_p < 0)) {
+      long double lo = prev_t, hi = t, plo = prev_p;
+      for (int it = 0; it < 200; ++it) {
+        long double mid = (lo + hi) / 2, pm;
+        jacobi(n, a, b, mid, pm, dp);
+        if ((pm < 0) == (plo < 0)) {
+          lo = mid;
+          plo = pm;
+        } else {
+          hi = mid;
+        }
+      }
+      long double x = (lo + hi) / 2;
+      for (int it = 0; it < 5; ++it) {
+        long double px;
+        jacobi(n, a, b, x, px, dp);
+        if (dp != 0) x -= px / dp;
+      }
+      roots.push_back(x);
+    }
+    prev_t = t;
+    prev_p = p;
+  }
+  return roots;
+}
+}  // namespace detail
+
+inline PeirceTables peirce_tables() {
+  PeirceTables t{};
+  // Gauss-Legendre (Jacobi a = b = 0): w = 2 / ((1 - x^2) P'(x)^2).
+  auto xs = detail::jacobi_roots(kNumPhi, 0, 0);
+  for (int j = 0; j < kNumPhi; ++j) {
+    long double p, dp;
+    detail::jacobi(kNumPhi, 0, 0, xs[j], p, dp);
+    t.cosphi[j] = double(xs[j]);
+    t.sinphi[j] = double(std::sqrt(1 - xs[j] * xs[j]));
+    t.b[j] = double(2 / ((1 - xs[j] * xs[j]) * dp * dp));
+  }
+  // Gauss-Jacobi (a = 0, b = 1/2): w = 2^(a+b+1) G(n+a+1)G(n+b+1) /
+  // (G(n+a+b+1) n!) / ((1 - t^2) P'(t)^2); the Gamma ratio is 1 for a = 0.
+  auto ts = detail::jacobi_roots(kNumR, 0, 0.5L);
+  for (int k = 0; k < kNumR; ++k) {
+    long double p, dp;
+    detail::jacobi(kNumR, 0, 0.5L, ts[k], p, dp);
+    long double w = std::pow(2.0L, 1.5L) / ((1 - ts[k] * ts[k]) * dp * dp);
+    t.r[k] = double(std::sqrt((1 + ts[k]) / 2));
+    t.c[k] = double(w / std::pow(2.0L, 2.5L));
+  }
+  return t;
+}
+
+// Volume-map node value (update_volume_field, runner.hpp:1616-1694):
+//   V(x) = h^3 sum_ijk w_ijk * ext(sign * phi(x + h r_k u_ij)),
+//   ext(d) = 1 for d <= 0, W(d) / W(0) otherwise.
+// The per-sample arithmetic follows the reference in TF; the sum is
+// accumulated in double (the reference's host check, tests/field_gen.cu:35-46,
+// accumulates in double as PeirceQuadrature::integrate does).
+template <class TF, class Phi>
+TF volume_at(const Cn<TF>& c, const PeirceTables& pt, V3<TF> x, TF sign, Phi phi) {
+  const TF pi = TF(3.14159265358979323846264338327950288L);
+  double sum = 0;
+  for (int i = 0; i < kNumTheta; ++i) {
+    TF theta = 2 * pi * TF(i + 1) / TF(kNumTheta);
+    TF ct = std::cos(theta), st = std::sin(theta);
+    for (int j = 0; j < kNumPhi; ++j) {
+      V3<TF> u{TF(pt.sinphi[j]) * ct, TF(pt.sinphi[j]) * st, TF(pt.cosphi[j])};
+      for (int k = 0; k < kNumR; ++k) {
+        TF w = 2 * pi * TF(pt.b[j]) * TF(pt.c[k]) / TF(kNumTheta);
+        TF d = phi(x + (c.h * TF(pt.r[k])) * u) * sign;
+        TF ext = d <= 0 ? TF(1) : W_dist(c, d) / c.w0;
+        sum += double(w) * double(ext);
+      }
+    }
+  }
+  return TF(sum * double(c.h2) * double(c.h));
+}
+
+// ------------------------------------------------------------------ bodies
+template <class TF>
+struct Body {
+  uint32_t shape, use_grid;
+  TF sign;
+  V3<TF> dmin, dmax, cs;
+  uint32_t res[3];
+  uint32_t num_nodes;
+  const TF* dist_nodes;
+  const TF* vol_nodes;
+  Shape<TF> sdf;
+  TF max_distance, mass;
+  V3<TF> inertia;
+  // kinematics (pile.hpp:103-110)
+  V3<TF> x, v, omega;
+  V4<TF> q;
+};
+
+// Boundary sample of one particle against one body:
+// compute_volume_and_boundary_x (runner.hpp:1696-1734, distance grid) and
+// compute_volume_and_boundary_x_analytic<0> (runner.hpp:1736-1771), then
+// compute_particle_boundary[_analytic] (runner.hpp:1982-2025).
+template <class TF>
+void boundary_sample(const Cn<TF>& c, const Body<TF>& b, V3<TF> x, V4<TF>& bnd, V4<TF>& bk) {
+  V3<TF> local = rotate(x - b.x, conjugate(b.q));
+  V3<TF> bx = x, xi_bxj{0, 0, 0};
+  TF d = 0, vol = 0;
+  int ip[3];
+  V3<TF> xi;
+  bool inside = resolve(b.dmin, b.dmax, b.res, b.cs, local, ip, xi);
+  TF N[32], d0[32], d1[32], d2[32];
+  uint32_t cells[32];
+  if (b.use_grid) {
+    if (inside) {
+      shape_functions<TF>(xi, N, d0, d1, d2);
+      cell_nodes(b.res, ip, cells);
+      TF phi = 0;
+      V3<TF> grad{0, 0, 0};
+      for (int j = 0; j < 32; ++j) {
+        TF v = b.dist_nodes[cells[j]];
+        phi += v * N[j];
+        grad.x += v * d0[j];
+        grad.y += v * d1[j];
+        grad.z += v * d2[j];
+      }
+      grad.x *= TF(2) / b.cs.x;
+      grad.y *= TF(2) / b.cs.y;
+      grad.z *= TF(2) / b.cs.z;
+      d = phi * b.sign;
+      V3<TF> nrm = rotate(grad * b.sign, b.q);
+      TF nl2 = length_sqr(nrm);
+      nrm = (nl2 > 0 ? inv_sqrt(nl2) : TF(0)) * nrm;
+      xi_bxj = d * nrm;
+      bx = x - xi_bxj;
+      for (int j = 0; j < 32; ++j) vol += b.vol_nodes[cells[j]] * N[j];
+    }
+  } else {
+    d = b.sdf.sdf(local) * b.sign;
+    V3<TF> nrm = rotate(b.sdf.gradient(local, c.h) * b.sign, b.q);
+    TF nl2 = length_sqr(nrm);
+    nrm = (nl2 > 0 ? inv_sqrt(nl2) : TF(0)) * nrm;
+    xi_bxj = d * nrm;
+    bx = x - xi_bxj;
+    if (inside) {
+      shape_functions<TF>(xi, N, nullptr, nullptr, nullptr);
+      cell_nodes(b.res, ip, cells);
+      for (int j = 0; j < 32; ++j) vol += b.vol_nodes[cells[j]] * N[j];
+    }
+  }
+  V3<TF> kg = gradW(c, xi_bxj);
+  bnd = {bx.x, bx.y, bx.z, vol};
+  bk = {vol * kg.x, vol * kg.y, vol * kg.z, vol * W_dist(c, d)};
+}
+
+// ------------------------------------------------------------- fluid state
+template <class TF>
+struct Fluid {
+  uint32_t n = 0, nb = 0;
+  std::vector<V3<TF>> x, v, a;
+  std::vector<TF> density, factor, kappa, kappa_v, density_adv;
+  std::vector<TF> pressure, last_pressure, aii, density_err;
+  std::vector<V3<TF>> dii, dij_pj, pressure_accel;
+  std::vector<V4<TF>> bnd, bk;          // [nb][n]
+  std::vector<V3<TF>> force, torque;    // [nb][n] per-particle rigid force
+  NeighborList nl;
+  GridSort gs;
+  void resize(uint32_t n_, uint32_t nb_) {
+    n = n_;
+    nb = nb_;
+    a.assign(n, {0, 0, 0});
+    density.assign(n, 0);
+    factor.assign(n, 0);
+    density_adv.assign(n, 0);
+    if (kappa.size() != n) kappa.assign(n, 0);
+    if (kappa_v.size() != n) kappa_v.assign(n, 0);
+    if (pressure.size() != n) pressure.assign(n, 0);
+    last_pressure.assign(n, 0);
+    aii.assign(n, 0);
+    density_err.assign(n, 0);
+    dii.assign(n, {0, 0, 0});
+    dij_pj.assign(n, {0, 0, 0});
+    pressure_accel.assign(n, {0, 0, 0});
+    bnd.assign(size_t(nb) * n, {0, 0, 0, 0});
+    bk.assign(size_t(nb) * n, {0, 0, 0, 0});
+    force.assign(size_t(nb) * n, {0, 0, 0});
+    torque.assign(size_t(nb) * n, {0, 0, 0});
+  }
+};
+
+// compute_all_boundaries (solver.hpp:170-185).
+template <class TF>
+void compute_boundaries(const Cn<TF>& c, const std::vector<Body<TF>>& bodies, Fluid<TF>& f) {
+  for (uint32_t b = 0; b < f.nb; ++b) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(f.n); ++i)
+      boundary_sample(c, bodies[b], f.x[i], f.bnd[size_t(b) * f.n + i], f.bk[size_t(b) * f.n + i]);
+  }
+}
+
+// compute_density (runner.hpp:2052-2072).
+template <class TF>
+void compute_density(const Cn<TF>& c, Fluid<TF>& f) {
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(f.n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    TF rho = c.vol * c.w0;
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      rho += c.vol * W_r2(c, length_sqr(f.x[i] - f.x[j]));
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) rho += f.bk[size_t(b) * f.n + i].w;
+    f.density[i] = rho * c.rho0;
+  }
+}
+
+// update_particle_neighbors<0> (solver.hpp:225-260): grid, list, density.
+template <class TF>
+void update_particle_neighbors(const Cn<TF>& c, const al_consti& g, Fluid<TF>& f) {
+  f.gs = grid_sort(c, g, f.x.data(), f.n);
+  f.nl = neighbor_list(c, g, f.x.data(), f.n, f.gs);
+  compute_density(c, f);
+}
+
+template <class TF>
+inline V3<TF> xv(const Fluid<TF>& f, uint32_t i, uint32_t j) {
+  return f.x[i] - f.x[j];
+}
+template <class TF>
+inline V3<TF> body_velocity(const Body<TF>& b, V3<TF> at) {
+  return cross(b.omega, at - b.x) + b.v;
+}
+
+// compute_dfsph_factor (runner.hpp:3123-3154).
+template <class TF>
+void compute_dfsph_factor(const Cn<TF>& c, Fluid<TF>& f) {
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(f.n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    TF sum = 0;
+    V3<TF> gi{0, 0, 0};
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      V3<TF> gj = (-c.vol) * gradW(c, xv(f, i, j));
+      sum += length_sqr(gj);
+      gi -= gj;
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+      gi += V3<TF>{k4.x, k4.y, k4.z};
+    }
+    sum += length_sqr(gi);
+    f.factor[i] = sum > c.eps ? -1 / sum : TF(0);
+  }
+}
+
+// compute_density_change (runner.hpp:3192-3228).
+template <class TF>
+TF density_change(const Cn<TF>& c, const std::vector<Body<TF>>& bodies, const Fluid<TF>& f,
+                  uint32_t i) {
+  TF adv = 0;
+  V3<TF> vi = f.v[i];
+  for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+    uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+    adv += c.vol * dot(vi - f.v[j], gradW(c, xv(f, i, j)));
+  }
+  for (uint32_t b = 0; b < f.nb; ++b) {
+    const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+    const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+    V3<TF> vj = body_velocity(bodies[b], V3<TF>{bn.x, bn.y, bn.z});
+    adv += dot(vi - vj, V3<TF>{k4.x, k4.y, k4.z});
+  }
+  adv = std::max(adv, TF(0));
+  if (f.nl.count[i] < 20) adv = 0;
+  return adv;
+}
+
+// compute_density_adv (runner.hpp:3493-3523).
+template <class TF>
+TF density_adv(const Cn<TF>& c, const std::vector<Body<TF>>& bodies, const Fluid<TF>& f,
+               uint32_t i, TF dt) {
+  TF delta = 0;
+  V3<TF> vi = f.v[i];
+  for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+    uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+    delta += c.vol * dot(vi - f.v[j], gradW(c, xv(f, i, j)));
+  }
+  for (uint32_t b = 0; b < f.nb; ++b) {
+    const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+    const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+    V3<TF> vj = body_velocity(bodies[b], V3<TF>{bn.x, bn.y, bn.z});
+    delta += dot(vi - vj, V3<TF>{k4.x, k4.y, k4.z});
+  }
+  return std::max(f.density[i] / c.rho0 + dt * delta, TF(1));
+}
+
+// Shared body of the kappa-driven velocity updates
+// (warm_start_divergence_solve_1 runner.hpp:3251-3295,
+//  divergence_solve_iteration :3316-3363, warm_start_pressure_solve1
+//  :3451-3491, pressure_solve_iteration :3543-3588).  `kappa_of(j)` returns
+// the neighbor's coefficient; the pair term is dv += sgn * dt * (k_i + k_j)
+// * V * gradW with sgn = -1 for the divergence forms (written there as
+// dv -= dt * k_sum * (-V gradW)) and +1 for the pressure forms.
+template <class TF, class KappaOf>
+void kappa_velocity_update(const Cn<TF>& c, const std::vector<Body<TF>>& bodies, Fluid<TF>& f,
+                           uint32_t i, TF ki, KappaOf kappa_of, TF dt, bool divergence_form,
+                           V3<TF>& dv) {
+  dv = {0, 0, 0};
+  for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+    uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+    TF ksum = ki + kappa_of(j);
+    if (std::fabs(ksum) > c.eps) {
+      if (divergence_form) {
+        V3<TF> gpj = (-c.vol) * gradW(c, xv(f, i, j));
+        dv -= (dt * ksum) * gpj;
+      } else {
+        dv += (dt * ksum * c.vol) * gradW(c, xv(f, i, j));
+      }
+    }
+  }
+  if (std::fabs(ki) > c.eps) {
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+      const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+      V3<TF> a = ki * (-V3<TF>{k4.x, k4.y, k4.z});
+      V3<TF> force = c.mass * a;
+      dv -= dt * a;
+      f.force[size_t(b) * f.n + i] += force;
+      f.torque[size_t(b) * f.n + i] += cross(V3<TF>{bn.x, bn.y, bn.z} - bodies[b].x, force);
+    }
+  }
+}
+
+// Orthonormal tangents of a unit normal (get_orthogonal_vectors,
+// runner.hpp:119-131).
+template <class TF>
+void tangents(V3<TF> n, V3<TF>& t1, V3<TF>& t2) {
+  V3<TF> v{1, 0, 0};
+  if (std::fabs(dot(v, n)) > TF(0.999)) v = {0, 1, 0};
+  t1 = cross(n, v);
+  t2 = cross(n, t1);
+  t1 = normalized(t1);
+  t2 = normalized(t2);
+}
+
+// clear_acceleration + compute_viscosity (runner.hpp:1974-1980, 2150-2249).
+template <class TF>
+void compute_viscosity(const Cn<TF>& c, const std::vector<Body<TF>>& bodies, Fluid<TF>& f) {
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(f.n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    V3<TF> vi = f.v[i], xi = f.x[i], da{0, 0, 0};
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      V3<TF> d = xv(f, i, j);
+      da += (c.visc * c.mass / f.density[j] * dot(d, gradW(c, d)) /
+             (length_sqr(d) + TF(0.01) * c.h2)) *
+            (vi - f.v[j]);
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+      V3<TF> bxj{bn.x, bn.y, bn.z};
+      const Body<TF>& body = bodies[b];
+      V3<TF> nrm = bxj - xi;
+      TF nl2 = length_sqr(nrm);
+      if (!(nl2 > 0)) continue;
+      nrm = inv_sqrt(nl2) * nrm;
+      V3<TF> t1, t2;
+      tangents(nrm, t1, t2);
+      TF dist = c.h - std::sqrt(nl2);
+      V3<TF> pts[4] = {bxj - t1 * dist, bxj + t1 * dist, bxj - t2 * dist, bxj + t2 * dist};
+      TF vol = TF(0.25) * bn.w;
+      V3<TF> fsum{0, 0, 0}, tsum{0, 0, 0};
+      V3<TF> acc[4];
+      for (int s = 0; s < 4; ++s) {
+        V3<TF> xix = xi - pts[s];
+        V3<TF> vb = body_velocity(body, pts[s]);
+        acc[s] = (c.bvisc * vol * dot(xix, gradW(c, xix)) / (length_sqr(xix) + TF(0.01) * c.h2)) *
+                 (vi - vb);
+      }
+      da += acc[0] + acc[1] + acc[2] + acc[3];
+      for (int s = 0; s < 4; ++s) {
+        V3<TF> fs = (-c.mass) * acc[s];
+        fsum += fs;
+        tsum += cross(pts[s] - body.x, fs);
+      }
+      f.force[size_t(b) * f.n + i] += fsum;
+      f.torque[size_t(b) * f.n + i] += tsum;
+    }
+    f.a[i] = c.g + da;
+  }
+}
+
+// --------------------------------------------------------------- solvers
+struct SolverParams {
+  double density_change_tolerance = 1e-3, density_error_tolerance = 1e-3;
+  uint32_t min_density_solve = 2, max_density_solve = 100;
+  uint32_t min_divergence_solve = 1, max_divergence_solve = 100;
+  double cfl = 0.4, max_dt = 2e-4, min_dt = 0;
+  bool enable_divergence_solve = true, enable_density_solve = true;
+};
+
+struct StepReport {
+  uint32_t num_divergence_solve = 0, num_density_solve = 0;
+  double mean_density_change = 0, mean_density_error = 0;
+  double particle_max_v2 = 0, pile_max_v2 = 0, max_v2 = 0, cfl_dt = 0, utilized_cfl = 0;
+  double dt = 0;
+  uint32_t grid_anomaly[3] = {0, 0, 0};
+};
+
+// Pile::calculate_cfl_v2 (pile.hpp:816-825).
+template <class TF>
+double pile_max_v2(const std::vector<Body<TF>>& bodies) {
+  double m = -std::numeric_limits<TF>::max();
+  for (const Body<TF>& b : bodies) {
+    V3<TF> w = cross(b.omega, V3<TF>{b.max_distance, 0, 0}) + b.v;
+    m = std::max(m, double(length_sqr(w)));
+  }
+  return m;
+}
+
+// Solver::update_dt (solver.hpp:153-169) with calculate_cfl_v2
+// (runner.hpp:2533-2541).
+template <class TF>
+void update_dt(const Cn<TF>& c, const std::vector<Body<TF>>& bodies, Fluid<TF>& f,
+               const SolverParams& sp, TF& dt, StepReport& rep) {
+  TF pmax = -std::numeric_limits<TF>::max();
+  for (uint32_t i = 0; i < f.n; ++i) pmax = std::max(pmax, length_sqr(f.v[i] + f.a[i] * dt));
+  rep.particle_max_v2 = pmax;
+  rep.pile_max_v2 = bodies.empty() ? -std::numeric_limits<TF>::max() : TF(pile_max_v2(bodies));
+  TF max_v2 = std::max(TF(rep.particle_max_v2), TF(rep.pile_max_v2));
+  rep.max_v2 = max_v2;
+  TF max_v = std::sqrt(max_v2);
+  TF length_scale = c.radius * 2;
+  TF cfl_dt = TF(sp.cfl) * length_scale / max_v;
+  rep.cfl_dt = cfl_dt;
+  dt = std::max(std::min(cfl_dt, TF(sp.max_dt)), TF(sp.min_dt));
+  rep.utilized_cfl = dt * max_v / length_scale;
+}
+
+// Per-body totals of the per-particle rigid force/torque entries
+// (solver_df.hpp:346-353), accumulated in double.
+template <class TF>
+void rigid_totals(const Fluid<TF>& f, std::vector<V3<double>>& F, std::vector<V3<double>>& T) {
+  F.assign(f.nb, {0, 0, 0});
+  T.assign(f.nb, {0, 0, 0});
+  for (uint32_t b = 0; b < f.nb; ++b)
+    for (uint32_t i = 0; i < f.n; ++i) {
+      const V3<TF>& fi = f.force[size_t(b) * f.n + i];
+      const V3<TF>& ti = f.torque[size_t(b) * f.n + i];
+      F[b] += V3<double>{fi.x, fi.y, fi.z};
+      T[b] += V3<double>{ti.x, ti.y, ti.z};
+    }
+}
+
+// Pile::integrate_kinematics (pile.hpp:794-815) with calculate_dq and
+// calculate_angular_acceleration (runner.hpp:202-251).
+template <class TF>
+void integrate_kinematics(std::vector<Body<TF>>& bodies, const std::vector<V3<double>>& F,
+                          const std::vector<V3<double>>& T, V3<TF> gravity, TF dt) {
+  for (size_t i = 0; i < bodies.size(); ++i) {
+    Body<TF>& b = bodies[i];
+    auto dq = [](V3<TF> w, V4<TF> q) {
+      return V4<TF>{TF(0.5) * (w.x * q.w + w.y * q.z - w.z * q.y),
+                    TF(0.5) * (-w.x * q.z + w.y * q.w + w.z * q.x),
+                    TF(0.5) * (w.x * q.y - w.y * q.x + w.z * q.w),
+                    TF(0.5) * (-w.x * q.x - w.y * q.y - w.z * q.z)};
+    };
+    auto advance_q = [&](void) {
+      V4<TF> d = dq(b.omega, b.q);
+      V4<TF> q{b.q.x + dt * d.x, b.q.y + dt * d.y, b.q.z + dt * d.z, b.q.w + dt * d.w};
+      TF inv = inv_sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+      b.q = {q.x * inv, q.y * inv, q.z * inv, q.w * inv};
+    };
+    if (b.mass == 0) {
+      b.x += b.v * dt;
+      advance_q();
+      continue;
+    }
+    V3<TF> force{TF(F[i].x), TF(F[i].y), TF(F[i].z)};
+    V3<TF> torque{TF(T[i].x), TF(T[i].y), TF(T[i].z)};
+    b.v += (1 / b.mass) * force * dt;
+    // world-frame inverse inertia R diag(1/I) R^T applied to the torque
+    V4<TF> q = b.q;
+    V3<TF> ii{1 / b.inertia.x, 1 / b.inertia.y, 1 / b.inertia.z};
+    TF m[3][3] = {{1 - 2 * (q.y * q.y + q.z * q.z), 2 * (q.x * q.y - q.z * q.w),
+                   2 * (q.x * q.z + q.y * q.w)},
+                  {2 * (q.x * q.y + q.z * q.w), 1 - 2 * (q.x * q.x + q.z * q.z),
+                   2 * (q.y * q.z - q.x * q.w)},
+                  {2 * (q.x * q.z - q.y * q.w), 2 * (q.y * q.z + q.x * q.w),
+                   1 - 2 * (q.x * q.x + q.y * q.y)}};
+    TF tq[3] = {torque.x, torque.y, torque.z}, alpha[3];
+    for (int r = 0; r < 3; ++r) {
+      TF s = 0;
+      for (int k = 0; k < 3; ++k) {
+        TF cong = ii.x * m[r][0] * m[k][0] + ii.y * m[r][1] * m[k][1] + ii.z * m[r][2] * m[k][2];
+        s += tq[k] * cong;
+      }
+      alpha[r] = s;
+    }
+    b.omega += V3<TF>{alpha[0], alpha[1], alpha[2]} * dt;
+    advance_q();
+    V3<TF> dx = (gravity * dt + b.v) * dt;
+    b.x += dx;
+    b.v = (1 / dt) * dx;
+  }
+}
+
+// SolverDf<TF>::step<0> (solver_df.hpp:74-359) without contacts.
+template <class TF>
+StepReport df_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& bodies, Fluid<TF>& f,
+                   const SolverParams& sp, TF& dt, V3<TF> pile_gravity, bool integrate_bodies,
+                   std::vector<V3<double>>* F_out = nullptr,
+                   std::vector<V3<double>>* T_out = nullptr) {
+  StepReport rep;
+  const uint32_t n = f.n;
+  std::fill(f.force.begin(), f.force.end(), V3<TF>{0, 0, 0});
+  std::fill(f.torque.begin(), f.torque.end(), V3<TF>{0, 0, 0});
+  compute_boundaries(c, bodies, f);
+  update_particle_neighbors(c, g, f);
+  rep.grid_anomaly[0] = f.gs.out_of_grid;
+  rep.grid_anomaly[1] = f.gs.cell_overflow;
+  rep.grid_anomaly[2] = f.nl.overflow;
+  compute_dfsph_factor(c, f);
+  if (sp.enable_divergence_solve) {
+    // warm_start_divergence_solve_0 (runner.hpp:3230-3249)
+    std::vector<TF> adv0(n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(n); ++i) adv0[i] = density_change(c, bodies, f, uint32_t(i));
+    for (uint32_t i = 0; i < n; ++i)
+      f.kappa_v[i] = adv0[i] > 0 ? TF(0.5) * std::max(f.kappa_v[i], TF(-0.5)) / dt : TF(0);
+    // warm_start_divergence_solve_1
+    std::vector<V3<TF>> dv(n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(n); ++i)
+      kappa_velocity_update(c, bodies, f, uint32_t(i), f.kappa_v[i],
+                            [&](uint32_t j) { return f.kappa_v[j]; }, dt, true, dv[i]);
+    for (uint32_t i = 0; i < n; ++i) f.v[i] += dv[i];
+    // compute_velocity_of_density_change (runner.hpp:3297-3314)
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(n); ++i) {
+      f.density_adv[i] = density_change(c, bodies, f, uint32_t(i));
+      f.factor[i] *= 1 / dt;
+    }
+    double mean = std::numeric_limits<double>::max();
+    uint32_t it = 0;
+    std::vector<TF> ki(n);
+    while ((mean > sp.density_change_tolerance / double(dt) || it < sp.min_divergence_solve) &&
+           it < sp.max_divergence_solve) {
+      // divergence_solve_iteration (runner.hpp:3316-3363)
+      for (uint32_t i = 0; i < n; ++i) ki[i] = f.density_adv[i] * f.factor[i];
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < int64_t(n); ++i)
+        kappa_velocity_update(c, bodies, f, uint32_t(i), ki[i],
+                              [&](uint32_t j) { return ki[j]; }, dt, true, dv[i]);
+      for (uint32_t i = 0; i < n; ++i) {
+        f.kappa_v[i] += ki[i];
+        f.v[i] += dv[i];
+      }
+      // compute_divergence_solve_density_error (runner.hpp:3396-3410)
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < int64_t(n); ++i)
+        f.density_adv[i] = density_change(c, bodies, f, uint32_t(i));
+      double s = 0;
+      for (uint32_t i = 0; i < n; ++i) s += double(f.density_adv[i]);
+      mean = s / double(n);
+      ++it;
+    }
+    rep.num_divergence_solve = it;
+    rep.mean_density_change = mean;
+    // divergence_solve_finish (runner.hpp:3412-3420)
+    for (uint32_t i = 0; i < n; ++i) {
+      f.factor[i] *= dt;
+      f.kappa_v[i] *= dt;
+    }
+  }
+  compute_viscosity(c, bodies, f);
+  update_dt(c, bodies, f, sp, dt, rep);
+  rep.dt = dt;
+  // integrate_non_pressure_acceleration (runner.hpp:3422-3428)
+  for (uint32_t i = 0; i < n; ++i) f.v[i] += dt * f.a[i];
+  if (sp.enable_density_solve) {
+    // warm_start_pressure_solve0 (runner.hpp:3430-3449)
+    std::vector<TF> adv0(n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(n); ++i) adv0[i] = density_adv(c, bodies, f, uint32_t(i), dt);
+    for (uint32_t i = 0; i < n; ++i)
+      f.kappa[i] = adv0[i] > TF(1.0)
+                       ? TF(0.5) * std::max(f.kappa[i], TF(-0.00025)) / (dt * dt)
+                       : TF(0);
+    // warm_start_pressure_solve1
+    std::vector<V3<TF>> dv(n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(n); ++i)
+      kappa_velocity_update(c, bodies, f, uint32_t(i), f.kappa[i],
+                            [&](uint32_t j) { return f.kappa[j]; }, dt, false, dv[i]);
+    for (uint32_t i = 0; i < n; ++i) f.v[i] += dv[i];
+    // compute_rho_adv (runner.hpp:3525-3541)
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < int64_t(n); ++i) {
+      f.density_adv[i] = density_adv(c, bodies, f, uint32_t(i), dt);
+      f.factor[i] *= 1 / (dt * dt);
+    }
+    double mean = std::numeric_limits<double>::max();
+    uint32_t it = 0;
+    std::vector<TF> ki(n);
+    while ((mean > sp.density_error_tolerance || it < sp.min_density_solve) &&
+           it < sp.max_density_solve) {
+      // pressure_solve_iteration (runner.hpp:3543-3588)
+      for (uint32_t i = 0; i < n; ++i) ki[i] = (f.density_adv[i] - 1) * f.factor[i];
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < int64_t(n); ++i)
+        kappa_velocity_update(c, bodies, f, uint32_t(i), ki[i],
+                              [&](uint32_t j) { return ki[j]; }, dt, false, dv[i]);
+      for (uint32_t i = 0; i < n; ++i) {
+        f.kappa[i] += ki[i];
+        f.v[i] += dv[i];
+      }
+      // compute_pressure_solve_density_error (runner.hpp:3590-3604); the
+      // mean is formed as sum(rho_adv - 1) / N in double
+      // (solver_df.hpp:323-325 forms sum / N - 1 in TF).
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < int64_t(n); ++i)
+        f.density_adv[i] = density_adv(c, bodies, f, uint32_t(i), dt);
+      double s = 0;
+      for (uint32_t i = 0; i < n; ++i) s += double(f.density_adv[i]) - 1.0;
+      mean = s / double(n);
+      ++it;
+    }
+    rep.num_density_solve = it;
+    rep.mean_density_error = mean;
+    // pressure_solve_finish (runner.hpp:3606-3611)
+    for (uint32_t i = 0; i < n; ++i) f.kappa[i] *= dt * dt;
+  }
+  // integrate_velocity<0> (runner.hpp:3613-3623)
+  for (uint32_t i = 0; i < n; ++i) f.x[i] += dt * f.v[i];
+  std::vector<V3<double>> F, T;
+  rigid_totals(f, F, T);
+  if (F_out) *F_out = F;
+  if (T_out) *T_out = T;
+  if (integrate_bodies) integrate_kinematics(bodies, F, T, pile_gravity, dt);
+  return rep;
+}
+
+// SolverIi<TF>::step<0> (solver_ii.hpp:76-243) without contacts.
+template <class TF>
+StepReport ii_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& bodies, Fluid<TF>& f,
+                   const SolverParams& sp, TF& dt, V3<TF> pile_gravity, bool integrate_bodies,
+                   std::vector<V3<double>>* F_out = nullptr,
+                   std::vector<V3<double>>* T_out = nullptr) {
+  StepReport rep;
+  const uint32_t n = f.n;
+  std::fill(f.force.begin(), f.force.end(), V3<TF>{0, 0, 0});
+  std::fill(f.torque.begin(), f.torque.end(), V3<TF>{0, 0, 0});
+  compute_boundaries(c, bodies, f);
+  update_particle_neighbors(c, g, f);
+  rep.grid_anomaly[0] = f.gs.out_of_grid;
+  rep.grid_anomaly[1] = f.gs.cell_overflow;
+  rep.grid_anomaly[2] = f.nl.overflow;
+  compute_viscosity(c, bodies, f);
+  update_dt(c, bodies, f, sp, dt, rep);
+  rep.dt = dt;
+  const TF V = c.vol, rho0 = c.rho0;
+  // predict_advection0 (runner.hpp:2609-2639)
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    f.v[i] += dt * f.a[i];
+    f.last_pressure[i] = f.pressure[i] * TF(0.5);
+    TF rho = f.density[i], rho2 = rho * rho;
+    V3<TF> dii{0, 0, 0};
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      dii -= (V / rho2) * gradW(c, xv(f, i, j));
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+      dii -= V3<TF>{k4.x / rho2, k4.y / rho2, k4.z / rho2};
+    }
+    f.dii[i] = dii * rho0;
+  }
+  // predict_advection1 (runner.hpp:2640-2690)
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    V3<TF> vi = f.v[i], dii = f.dii[i];
+    TF rho = f.density[i], rho2 = rho * rho, inv_rho2 = 1 / rho2, dpi = V * inv_rho2;
+    TF adv = rho / rho0, aii = 0;
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      V3<TF> gw = gradW(c, xv(f, i, j));
+      V3<TF> dji = (dpi * rho0) * gw;
+      adv += dt * V * dot(vi - f.v[j], gw);
+      aii += V * dot(dii - dji, gw);
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+      const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+      V3<TF> gw{k4.x, k4.y, k4.z};
+      V3<TF> vj = body_velocity(bodies[b], V3<TF>{bn.x, bn.y, bn.z});
+      V3<TF> dji = (inv_rho2 * rho0) * gw;
+      adv += dt * dot(vi - vj, gw);
+      aii += dot(dii - dji, gw);
+    }
+    f.density_adv[i] = adv;
+    f.aii[i] = aii * rho0;
+  }
+  double mean = std::numeric_limits<double>::max();
+  uint32_t it = 0;
+  while ((mean > sp.density_error_tolerance || it < sp.min_density_solve) &&
+         it < sp.max_density_solve) {
+    // pressure_solve_iteration0 (runner.hpp:2691-2715)
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+      uint32_t i = uint32_t(ii);
+      V3<TF> s{0, 0, 0};
+      for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+        uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+        TF rj = f.density[j], rj2 = rj * rj;
+        s -= (V / rj2 * f.last_pressure[j]) * gradW(c, xv(f, i, j));
+      }
+      f.dij_pj[i] = s * rho0;
+    }
+    // pressure_solve_iteration1 (runner.hpp:2716-2772)
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+      uint32_t i = uint32_t(ii);
+      TF lp = f.last_pressure[i];
+      V3<TF> dij_pj = f.dij_pj[i];
+      TF rho = f.density[i], rho2 = rho * rho, dpi = V / rho2;
+      TF bterm = 1 - f.density_adv[i], dt2 = dt * dt, aii = f.aii[i], denom = aii * dt2;
+      const TF omega = TF(2) / 3;
+      TF p = 0, sum = 0;
+      for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+        uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+        V3<TF> gw = gradW(c, xv(f, i, j));
+        V3<TF> dji = (dpi * rho0) * gw;
+        V3<TF> dji_pi = dji * lp;
+        sum += V * dot(dij_pj - f.dii[j] * f.last_pressure[j] - (f.dij_pj[j] - dji_pi), gw);
+      }
+      for (uint32_t b = 0; b < f.nb; ++b) {
+        const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+        sum += dot(dij_pj, V3<TF>{k4.x, k4.y, k4.z});
+      }
+      sum *= rho0;
+      if (std::fabs(denom) > TF(1.0e-9))
+        p = std::max((1 - omega) * lp + omega / denom * (bterm - dt2 * sum), TF(0));
+      f.density_err[i] = p == 0 ? TF(0) : (denom * p + sum * dt2 - bterm);
+      f.pressure[i] = p;
+    }
+    for (uint32_t i = 0; i < n; ++i) f.last_pressure[i] = f.pressure[i];
+    double s = 0;
+    for (uint32_t i = 0; i < n; ++i) s += double(f.density_err[i]);
+    mean = s / double(n);
+    ++it;
+  }
+  rep.num_density_solve = it;
+  rep.mean_density_error = mean;
+  // compute_pressure_accels (runner.hpp:2774-2817)
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    TF rho = f.density[i], dpi = f.pressure[i] / (rho * rho);
+    V3<TF> ai{0, 0, 0};
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      TF rj = f.density[j], dpj = f.pressure[j] / (rj * rj);
+      ai -= (c.mass * (dpi + dpj)) * gradW(c, xv(f, i, j));
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+      const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+      V3<TF> a = (rho0 * dpi) * V3<TF>{k4.x, k4.y, k4.z};
+      V3<TF> force = c.mass * a;
+      ai -= a;
+      f.force[size_t(b) * f.n + i] += force;
+      f.torque[size_t(b) * f.n + i] += cross(V3<TF>{bn.x, bn.y, bn.z} - bodies[b].x, force);
+    }
+    f.pressure_accel[i] = rho0 * ai;
+  }
+  // kinematic_integration<0> (runner.hpp:2873-2887)
+  for (uint32_t i = 0; i < n; ++i) {
+    V3<TF> v = f.v[i] + f.pressure_accel[i] * dt;
+    f.x[i] += v * dt;
+    f.v[i] = v;
+  }
+  std::vector<V3<double>> F, T;
+  rigid_totals(f, F, T);
+  if (F_out) *F_out = F;
+  if (T_out) *T_out = T;
+  if (integrate_bodies) integrate_kinematics(bodies, F, T, pile_gravity, dt);
+  return rep;
+}
+
+}  // namespace oracle

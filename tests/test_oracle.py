@@ -1,0 +1,158 @@
+"""CPU checks of the oracle itself, before it is trusted as the checker.
+
+Pins: the Peirce m=14 tables against the reference's literals
+(tests/golden/peirce_m14.json, extracted by tests/golden/make_golden.py);
+the cubic Lagrange element's defining properties; the cubic spline's
+normalisation and gradient; node positions of the reference's own
+known-answer setup (tests/field_op.cu:17-58).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import binding as orc
+from alluvion_b200 import scenes, _capi
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_peirce_tables_match_reference_literals():
+    ref = json.load(open(os.path.join(GOLDEN, "peirce_m14.json")))["tables"]
+    got = orc.peirce_tables()
+    for name in ("cosphi", "sinphi", "b", "r", "c"):
+        np.testing.assert_allclose(got[name], ref[name], rtol=0, atol=1e-15, err_msg=name)
+        # identical once rounded to the solver's float32 constant tables
+        assert np.array_equal(np.float32(got[name]), np.float32(ref[name])), name
+
+
+def test_peirce_rule_integrates_polynomials_on_ball():
+    t = orc.peirce_tables()
+    # sum over theta of w_theta (2 pi / 60) * b_j * c_k * f(r u) = integral over unit ball
+    theta = 2 * np.pi * (np.arange(60) + 1) / 60
+    vol = 0.0
+    second = 0.0
+    for ct, st in zip(np.cos(theta), np.sin(theta)):
+        for j in range(30):
+            u = np.array([t["sinphi"][j] * ct, t["sinphi"][j] * st, t["cosphi"][j]])
+            for k in range(15):
+                w = 2 * np.pi * t["b"][j] * t["c"][k] / 60
+                p = t["r"][k] * u
+                vol += w
+                second += w * p[0] ** 2
+    assert vol == pytest.approx(4 * np.pi / 3, rel=1e-13)
+    assert second == pytest.approx(4 * np.pi / 15, rel=1e-12)
+
+
+def _node_coords():
+    pts = []
+    for j in range(8):
+        pts.append([1 if j & 1 else -1, 1 if j & 2 else -1, 1 if j & 4 else -1])
+    # x-edges: bit0 -> -1/3 | +1/3, bit1 -> z, bit2 -> y
+    for e in range(8):
+        pts.append([(1 if e & 1 else -1) / 3, 1 if e & 4 else -1, 1 if e & 2 else -1])
+    # y-edges: bit1 -> x, bit2 -> z
+    for e in range(8):
+        pts.append([1 if e & 2 else -1, (1 if e & 1 else -1) / 3, 1 if e & 4 else -1])
+    # z-edges: bit1 -> y, bit2 -> x
+    for e in range(8):
+        pts.append([1 if e & 4 else -1, 1 if e & 2 else -1, (1 if e & 1 else -1) / 3])
+    return np.array(pts, dtype=np.float64)
+
+
+def test_shape_functions_kronecker_and_partition_of_unity():
+    nodes = _node_coords()
+    for k, p in enumerate(nodes):
+        N, _ = orc.shape_functions(p)
+        expect = np.zeros(32)
+        expect[k] = 1
+        np.testing.assert_allclose(N, expect, atol=1e-14)
+    rng = np.random.default_rng(1)
+    for _ in range(50):
+        xi = rng.uniform(-1, 1, 3)
+        N, dN = orc.shape_functions(xi)
+        assert N.sum() == pytest.approx(1.0, abs=1e-14)
+        np.testing.assert_allclose(dN.sum(axis=1), 0, atol=1e-13)
+
+
+def test_shape_functions_reproduce_cubics_and_gradients():
+    nodes = _node_coords()
+    rng = np.random.default_rng(2)
+
+    def f(p):
+        x, y, z = p
+        return 1 + 2 * x - y + 0.5 * z + x * y - 3 * y * z + x * x * z + 2 * x ** 3 - y * y * x
+
+    def grad(p):
+        x, y, z = p
+        return np.array([2 + y + 2 * x * z + 6 * x * x - y * y,
+                         -1 + x - 3 * z - 2 * x * y,
+                         0.5 - 3 * y + x * x])
+
+    vals = np.array([f(p) for p in nodes])
+    for _ in range(50):
+        xi = rng.uniform(-1, 1, 3)
+        N, dN = orc.shape_functions(xi)
+        assert N @ vals == pytest.approx(f(xi), abs=1e-12)
+        np.testing.assert_allclose(dN @ vals, grad(xi), atol=1e-11)
+
+
+def test_cell_nodes_are_the_reference_corner_and_edge_slots():
+    res = np.array([3, 4, 5], np.uint32)
+    dmin = np.array([-1.0, 2.0, 0.5])
+    cs = np.array([0.5, 0.25, 0.125])
+    pos = orc.node_positions(dmin, res, cs, np.float64)
+    ref_nodes = _node_coords()
+    for ip in ([0, 0, 0], [2, 3, 4], [1, 2, 3]):
+        cells = orc.cell_nodes(res, ip)
+        lo = dmin + cs * np.array(ip)
+        for k in range(32):
+            expect = lo + (ref_nodes[k] + 1) / 2 * cs
+            np.testing.assert_allclose(pos[cells[k]], expect, atol=1e-12)
+
+
+def test_node_positions_known_answer():
+    """tests/field_op.cu:17-58 setup: domain (-23.1, 12.23, -31.44) ..
+    (45.1, 103.2, 12.4), 11^3 cells; every node lies on the vertex/third-point
+    lattice of its cell and all nodes are distinct."""
+    dmin = np.array([-23.1, 12.23, -31.44])
+    dmax = np.array([45.1, 103.2, 12.4])
+    res = np.array([11, 11, 11], np.uint32)
+    cs = (dmax - dmin) / res
+    pos = orc.node_positions(dmin, res, cs, np.float64)
+    assert pos.shape[0] == 12 ** 3 + 2 * 3 * 11 * 12 * 12
+    frac = (pos - dmin) / cs * 3
+    np.testing.assert_allclose(frac, np.round(frac), atol=1e-9)
+    assert len({tuple(np.round(f).astype(int)) for f in frac}) == pos.shape[0]
+    assert np.all(pos >= dmin - 1e-9) and np.all(pos <= dmax + 1e-9)
+
+
+def test_cubic_spline_normalised_and_gradient(tmp_path):
+    cn = scenes.make_const(np.float64, 0.01)
+    h = cn.kernel_radius
+    k = cn.cubic_kernel_k
+
+    def W(r):
+        q = r / h
+        return np.where(q <= 0.5, (6 * q - 6) * q * q + 1,
+                        np.where(q <= 1, 2 * (1 - q) ** 3, 0.0)) * k
+
+    r = np.linspace(0, h, 200001)
+    integral = np.trapezoid(4 * np.pi * r * r * W(r), r)
+    assert integral == pytest.approx(1.0, rel=1e-6)
+
+
+def test_neighbor_list_matches_brute_force():
+    cn = scenes.make_const(np.float32, 0.01)
+    x = scenes.fluid_block((6, 5, 7), (0, 0, 0), 0.01, np.float32, seed=3)
+    cni = scenes.make_consti(x.min(0), x.max(0), cn.kernel_radius)
+    density, count, index, nbrs, flags = orc.update_particle_neighbors(cn, cni, x)
+    assert not flags.any()
+    h2 = np.float32(cn.kernel_radius_sqr)
+    d = x[:, None, :] - x[None, :, :]
+    d2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    for i in range(x.shape[0]):
+        expect = set(np.nonzero((d2[i] < h2) & (np.arange(len(x)) != i))[0].tolist())
+        got = set(index[i, :count[i]].tolist())
+        assert got == expect
