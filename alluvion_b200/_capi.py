@@ -114,6 +114,30 @@ class StepReport(ctypes.Structure):
                 ("torque", (ctypes.c_double * 3) * AL_MAX_BOUNDARIES)]
 
 
+_FLUID_PTRS = ("particle_x", "particle_v", "particle_a", "particle_density",
+               "particle_dfsph_factor", "particle_kappa", "particle_kappa_v",
+               "particle_density_adv", "particle_pressure", "particle_boundary",
+               "particle_boundary_kernel")
+
+
+class Fluid(ctypes.Structure):
+    """al_fluid_f32 / al_fluid_f64 (identical layout: pointers)."""
+    _fields_ = [("num_particles", ctypes.c_uint32), ("reserved", ctypes.c_uint32)] + \
+               [(name, ctypes.c_void_p) for name in _FLUID_PTRS]
+
+
+def make_fluid(num_particles, **buffers):
+    """al_fluid from device buffers (torch tensors or raw addresses)."""
+    f = Fluid()
+    f.num_particles = num_particles
+    for name, t in buffers.items():
+        assert name in _FLUID_PTRS, name
+        if t is None:
+            continue
+        setattr(f, name, t if isinstance(t, int) else t.data_ptr())
+    return f
+
+
 def real_types(dtype):
     """(ConstT, BodyT, RigidT, ctypes real) for np.float32 / np.float64."""
     if np.dtype(dtype) == np.float32:
@@ -143,6 +167,13 @@ for _s in ("f32", "f64"):
     _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])
     _SIGNATURES["al_update_particle_neighbors_" + _s] = (
         ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P, _P])
+    _SIGNATURES["al_compute_particle_boundary_" + _s] = (
+        ctypes.c_int, [_P, _P, _U, _P, _P, _P, _U, _P, _P, _P])
+    _SIGNATURES["al_build_volume_field_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _P])
+    _SIGNATURES["al_build_distance_grid_" + _s] = (ctypes.c_int, [_P, _P, _P, _P])
+    _SIGNATURES["al_node_positions_" + _s] = (ctypes.c_int, [_P, _P, _P, _P])
+    _SIGNATURES["al_df_step_" + _s] = (ctypes.c_int, [_P] * 10)
+    _SIGNATURES["al_ii_step_" + _s] = (ctypes.c_int, [_P] * 10)
 
 
 def declared_symbols():
@@ -206,9 +237,11 @@ class Engine:
 
 
 def ptr(t):
-    """Device/host address of a torch tensor or numpy array (None -> NULL)."""
+    """Address of a torch tensor, numpy array or ctypes object (None -> NULL)."""
     if t is None:
         return None
+    if isinstance(t, (ctypes.Structure, ctypes.Array)):
+        return ctypes.cast(ctypes.pointer(t), ctypes.c_void_p)
     if hasattr(t, "data_ptr"):
         return ctypes.c_void_p(t.data_ptr())
     return ctypes.c_void_p(t.ctypes.data)

@@ -1,0 +1,478 @@
+// boundary.cu -- Lagrange-grid / analytic boundary sampling, volume maps,
+// distance grids.
+#include <cmath>
+
+#include "boundary.cuh"
+#include "peirce_tables.h"
+
+namespace alb {
+
+namespace {
+
+inline uint32_t blocks_for(uint32_t n, int block) { return (n + block - 1) / block; }
+
+// Quadrature tables in constant memory: per azimuth i cos/sin(theta_i), per
+// polar node j sin/cos(phi_j), per (j, k) the weight 2 pi b_j c_k / 60, per
+// k the radius.
+template <class T>
+struct PeirceTab {
+  T ct[peirce::kNumTheta], st[peirce::kNumTheta];
+  T sp[peirce::kNumPhi], cp[peirce::kNumPhi];
+  T w[peirce::kNumPhi * peirce::kNumR];
+  T r[peirce::kNumR];
+};
+using PeirceDev = PeirceTab<float>;
+using PeirceDevD = PeirceTab<double>;
+__constant__ PeirceDev c_peirce_f;
+__constant__ PeirceDevD c_peirce_d;
+
+template <class TF>
+struct PeirceSel;
+template <>
+struct PeirceSel<float> {
+  __device__ static const PeirceDev& get() { return c_peirce_f; }
+};
+template <>
+struct PeirceSel<double> {
+  __device__ static const PeirceDevD& get() { return c_peirce_d; }
+};
+
+// ------------------------------------------------------------- geometry
+template <class TF>
+__device__ __forceinline__ vec3<TF> rotate(vec3<TF> v, vec4<TF> q) {
+  vec3<TF> r;
+  r.x = (TF(1) - TF(2) * (q.y * q.y + q.z * q.z)) * v.x + TF(2) * (q.x * q.y - q.z * q.w) * v.y +
+        TF(2) * (q.x * q.z + q.y * q.w) * v.z;
+  r.y = TF(2) * (q.x * q.y + q.z * q.w) * v.x + (TF(1) - TF(2) * (q.x * q.x + q.z * q.z)) * v.y +
+        TF(2) * (q.y * q.z - q.x * q.w) * v.z;
+  r.z = TF(2) * (q.x * q.z - q.y * q.w) * v.x + TF(2) * (q.y * q.z + q.x * q.w) * v.y +
+        (TF(1) - TF(2) * (q.x * q.x + q.y * q.y)) * v.z;
+  return r;
+}
+
+template <class TF>
+__device__ __forceinline__ TF box_sdf(vec3<TF> x, TF hx, TF hy, TF hz, TF outset) {
+  vec3<TF> d{fabs(x.x) - hx, fabs(x.y) - hy, fabs(x.z) - hz};
+  vec3<TF> cl{fmax(d.x, TF(0)), fmax(d.y, TF(0)), fmax(d.z, TF(0))};
+  return sqrt(length_sqr(cl)) + fmin(fmax(d.x, fmax(d.y, d.z)), TF(0)) - outset;
+}
+
+// Analytic signed distances (dg/box_distance.hpp:23-30,
+// dg/sphere_distance.hpp:18-20, dg/box_shell_distance.hpp:36-47) and the
+// torus |(|x_xz| - R, y)| - r.
+template <class TF>
+__device__ __forceinline__ TF shape_sdf(const BodyDev<TF>& b, vec3<TF> x) {
+  switch (b.shape) {
+    case AL_SHAPE_BOX:
+      return box_sdf(x, b.p[0], b.p[1], b.p[2], b.p[3]);
+    case AL_SHAPE_SPHERE:
+      return sqrt(length_sqr(x)) - b.p[0];
+    case AL_SHAPE_BOX_SHELL: {
+      TF inner = box_sdf(x, b.p[0], b.p[1], b.p[2], b.p[6]);
+      TF outer = box_sdf(x, b.p[3], b.p[4], b.p[5], b.p[6]);
+      return fmax(outer, -inner);
+    }
+    default: {
+      TF rho = sqrt(x.x * x.x + x.z * x.z) - b.p[0];
+      return sqrt(rho * rho + x.y * x.y) - b.p[1];
+    }
+  }
+}
+
+// Un-normalised outward direction: the position for a sphere
+// (sphere_distance.hpp:21), central differences with step h/256 otherwise
+// (box_distance.hpp:28-38).
+template <class TF>
+__device__ __forceinline__ vec3<TF> shape_gradient(const BodyDev<TF>& b, vec3<TF> x, TF h) {
+  if (b.shape == AL_SHAPE_SPHERE) return x;
+  const TF s = h * TF(0.00390625);
+  return vec3<TF>{shape_sdf(b, vec3<TF>{x.x + s, x.y, x.z}) - shape_sdf(b, vec3<TF>{x.x - s, x.y, x.z}),
+                  shape_sdf(b, vec3<TF>{x.x, x.y + s, x.z}) - shape_sdf(b, vec3<TF>{x.x, x.y - s, x.z}),
+                  shape_sdf(b, vec3<TF>{x.x, x.y, x.z + s}) - shape_sdf(b, vec3<TF>{x.x, x.y, x.z - s})};
+}
+
+// resolve (runner.hpp:1180-1195): cell of x and reference coordinates.
+template <class TF>
+__device__ __forceinline__ bool resolve(const BodyDev<TF>& b, vec3<TF> x, int ip[3],
+                                        vec3<TF>& xi) {
+  if (!(x.x >= b.dmin.x && x.y >= b.dmin.y && x.z >= b.dmin.z && b.dmax.x >= x.x &&
+        b.dmax.y >= x.y && b.dmax.z >= x.z))
+    return false;
+  const vec3<TF> inv{TF(1) / b.cs.x, TF(1) / b.cs.y, TF(1) / b.cs.z};
+  ip[0] = min(int((x.x - b.dmin.x) * inv.x), int(b.res[0]) - 1);
+  ip[1] = min(int((x.y - b.dmin.y) * inv.y), int(b.res[1]) - 1);
+  ip[2] = min(int((x.z - b.dmin.z) * inv.z), int(b.res[2]) - 1);
+  const vec3<TF> lo{b.dmin.x + b.cs.x * TF(ip[0]), b.dmin.y + b.cs.y * TF(ip[1]),
+                    b.dmin.z + b.cs.z * TF(ip[2])};
+  xi = vec3<TF>{TF(2) * (x.x - lo.x) * inv.x - TF(1), TF(2) * (x.y - lo.y) * inv.y - TF(1),
+                TF(2) * (x.z - lo.z) * inv.z - TF(1)};
+  return true;
+}
+
+// Linear index of the j-th node of cell ip (get_cells, runner.hpp:1197-1257):
+// 8 vertices, then per x-, y-, z-edge family four edges of two third-point
+// nodes.
+__device__ __forceinline__ uint32_t lagrange_node(const uint32_t r[3], uint32_t x, uint32_t y,
+                                                  uint32_t z, int j) {
+  const uint32_t nx = r[0], ny = r[1], nz = r[2];
+  if (j < 8)
+    return (nx + 1) * (ny + 1) * (z + ((j >> 2) & 1)) + (nx + 1) * (y + ((j >> 1) & 1)) + x +
+           (j & 1);
+  uint32_t base = (nx + 1) * (ny + 1) * (nz + 1);
+  if (j < 16) {
+    const int e = j - 8;
+    return base + 2 * (nx * (ny + 1) * (z + ((e >> 1) & 1)) + nx * (y + ((e >> 2) & 1)) + x) +
+           (e & 1);
+  }
+  base += 2 * nx * (ny + 1) * (nz + 1);
+  if (j < 24) {
+    const int e = j - 16;
+    return base + 2 * (ny * (nz + 1) * (x + ((e >> 1) & 1)) + ny * (z + ((e >> 2) & 1)) + y) +
+           (e & 1);
+  }
+  base += 2 * (nx + 1) * ny * (nz + 1);
+  const int e = j - 24;
+  return base + 2 * (nz * (nx + 1) * (y + ((e >> 1) & 1)) + nz * (x + ((e >> 2) & 1)) + z) +
+         (e & 1);
+}
+
+// Shape function j of the 32-node element at reference point p and,
+// if GRAD, its derivatives (the element of get_shape_function_and_gradient,
+// runner.hpp:1354-1584):
+//   corner: (1/64)(1+sx x)(1+sy y)(1+sz z)(9|p|^2 - 19)
+//   edge:   (9/64)(1-t^2)(1+3 s t)(1+s1 u)(1+s2 w)
+template <class TF, bool GRAD>
+__device__ __forceinline__ void shape_j(int j, vec3<TF> p, TF r2, TF& N, vec3<TF>& dN) {
+  const TF c64 = TF(1) / TF(64), e64 = TF(9) / TF(64);
+  if (j < 8) {
+    const TF sx = (j & 1) ? TF(1) : TF(-1), sy = (j & 2) ? TF(1) : TF(-1),
+             sz = (j & 4) ? TF(1) : TF(-1);
+    const TF ax = TF(1) + sx * p.x, ay = TF(1) + sy * p.y, az = TF(1) + sz * p.z;
+    const TF f = TF(9) * r2 - TF(19);
+    N = c64 * ax * ay * az * f;
+    if (GRAD) {
+      dN.x = c64 * ay * az * (sx * f + TF(18) * p.x * ax);
+      dN.y = c64 * ax * az * (sy * f + TF(18) * p.y * ay);
+      dN.z = c64 * ax * ay * (sz * f + TF(18) * p.z * az);
+    }
+    return;
+  }
+  // family: axis of the edge, and the axes selected by bits 1 and 2
+  int axis, a1, a2, e;
+  if (j < 16) {
+    e = j - 8;
+    axis = 0;
+    a1 = 2;
+    a2 = 1;
+  } else if (j < 24) {
+    e = j - 16;
+    axis = 1;
+    a1 = 0;
+    a2 = 2;
+  } else {
+    e = j - 24;
+    axis = 2;
+    a1 = 1;
+    a2 = 0;
+  }
+  const TF u[3] = {p.x, p.y, p.z};
+  const TF s = (e & 1) ? TF(1) : TF(-1), s1 = (e & 2) ? TF(1) : TF(-1),
+           s2 = (e & 4) ? TF(1) : TF(-1);
+  const TF t = u[axis], A = TF(1) + s1 * u[a1], B = TF(1) + s2 * u[a2];
+  const TF g = (TF(1) - t * t) * (TF(1) + TF(3) * s * t);
+  N = e64 * g * A * B;
+  if (GRAD) {
+    const TF dg = TF(3) * s * (TF(1) - t * t) - TF(2) * t * (TF(1) + TF(3) * s * t);
+    TF d[3];
+    d[axis] = e64 * dg * A * B;
+    d[a1] = e64 * g * s1 * B;
+    d[a2] = e64 * g * A * s2;
+    dN = vec3<TF>{d[0], d[1], d[2]};
+  }
+}
+
+// Interpolated value of `nodes` at x (interpolate_distance_without_
+// intermediates, runner.hpp:1596-1614): +max outside the domain.
+template <class TF>
+__device__ __forceinline__ TF interpolate_grid(const BodyDev<TF>& b, const TF* __restrict__ nodes,
+                                               vec3<TF> x) {
+  int ip[3];
+  vec3<TF> xi;
+  if (!resolve(b, x, ip, xi)) return max_value<TF>();
+  const TF r2 = xi.x * xi.x + xi.y * xi.y + xi.z * xi.z;
+  TF phi = 0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    TF N;
+    vec3<TF> dN;
+    shape_j<TF, false>(j, xi, r2, N, dN);
+    phi += __ldg(nodes + lagrange_node(b.res, ip[0], ip[1], ip[2], j)) * N;
+  }
+  return phi;
+}
+
+// Boundary sample of one particle against one body
+// (compute_volume_and_boundary_x[_analytic], runner.hpp:1696-1771, and the
+// writes of compute_particle_boundary[_analytic], runner.hpp:1982-2025).
+template <class TF>
+__device__ __forceinline__ void sample_body(const Cn<TF>& c, const BodyDev<TF>& b,
+                                            const RigidDev<TF>& r, vec3<TF> x, vec4<TF>& bnd,
+                                            vec4<TF>& bk) {
+  const vec4<TF> qc{-r.q.x, -r.q.y, -r.q.z, r.q.w};
+  const vec3<TF> local = rotate(x - r.x, qc);
+  vec3<TF> bx = x, xi_bxj{0, 0, 0};
+  TF d = 0, vol = 0;
+  int ip[3];
+  vec3<TF> xi;
+  const bool inside = resolve(b, local, ip, xi);
+  if (b.use_grid) {
+    if (inside) {
+      const TF r2 = xi.x * xi.x + xi.y * xi.y + xi.z * xi.z;
+      TF phi = 0;
+      vec3<TF> grad{0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        TF N;
+        vec3<TF> dN;
+        shape_j<TF, true>(j, xi, r2, N, dN);
+        const uint32_t node = lagrange_node(b.res, ip[0], ip[1], ip[2], j);
+        const TF dv = __ldg(b.dist + node);
+        phi += dv * N;
+        grad.x += dv * dN.x;
+        grad.y += dv * dN.y;
+        grad.z += dv * dN.z;
+        vol += __ldg(b.vol + node) * N;
+      }
+      grad.x *= TF(2) / b.cs.x;
+      grad.y *= TF(2) / b.cs.y;
+      grad.z *= TF(2) / b.cs.z;
+      d = phi * b.sign;
+      vec3<TF> nrm = rotate(grad * b.sign, r.q);
+      const TF nl2 = length_sqr(nrm);
+      nrm = (nl2 > TF(0) ? rsqrt_(nl2) : TF(0)) * nrm;
+      xi_bxj = d * nrm;
+      bx = x - xi_bxj;
+    }
+  } else {
+    d = shape_sdf(b, local) * b.sign;
+    vec3<TF> nrm = rotate(shape_gradient(b, local, c.h) * b.sign, r.q);
+    const TF nl2 = length_sqr(nrm);
+    nrm = (nl2 > TF(0) ? rsqrt_(nl2) : TF(0)) * nrm;
+    xi_bxj = d * nrm;
+    bx = x - xi_bxj;
+    if (inside) {
+      const TF r2 = xi.x * xi.x + xi.y * xi.y + xi.z * xi.z;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        TF N;
+        vec3<TF> dN;
+        shape_j<TF, false>(j, xi, r2, N, dN);
+        vol += __ldg(b.vol + lagrange_node(b.res, ip[0], ip[1], ip[2], j)) * N;
+      }
+    }
+  }
+  const vec3<TF> kg = gradW(c, xi_bxj);
+  bnd = vec4<TF>{bx.x, bx.y, bx.z, vol};
+  bk = vec4<TF>{vol * kg.x, vol * kg.y, vol * kg.z, vol * W_dist(c, d)};
+}
+
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_sample_boundaries(Cn<TF> c, const BodyDev<TF>* __restrict__ bodies,
+                        const RigidDev<TF>* __restrict__ rigid, uint32_t nb,
+                        const vec4<TF>* __restrict__ xs, const uint32_t* __restrict__ perm,
+                        uint32_t n, uint32_t* __restrict__ mask, vec4<TF>* __restrict__ bx,
+                        vec4<TF>* __restrict__ bk, TF* __restrict__ ref_b,
+                        TF* __restrict__ ref_k) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const vec3<TF> x = xyz(xs[s]);
+  const uint32_t i = perm ? perm[s] : s;
+  uint32_t m = 0;
+  for (uint32_t b = 0; b < nb; ++b) {
+    vec4<TF> bnd, kk;
+    sample_body(c, bodies[b], rigid[b], x, bnd, kk);
+    if (bnd.w != TF(0)) {
+      m |= 1u << b;
+      if (bx) {
+        bx[size_t(b) * n + s] = bnd;
+        bk[size_t(b) * n + s] = kk;
+      }
+    }
+    if (ref_b) {
+      TF* o = ref_b + (size_t(b) * n + i) * 4;
+      o[0] = bnd.x;
+      o[1] = bnd.y;
+      o[2] = bnd.z;
+      o[3] = bnd.w;
+      TF* k = ref_k + (size_t(b) * n + i) * 4;
+      k[0] = kk.x;
+      k[1] = kk.y;
+      k[2] = kk.z;
+      k[3] = kk.w;
+    }
+  }
+  if (mask) mask[s] = m;
+}
+
+// index_to_node_position (runner.hpp:1131-1178).
+template <class TF>
+__device__ __forceinline__ vec3<TF> node_position(const BodyDev<TF>& b, uint32_t l) {
+  const uint32_t nx = b.res[0], ny = b.res[1], nz = b.res[2];
+  const uint32_t nv = (nx + 1) * (ny + 1) * (nz + 1);
+  const uint32_t nex = nx * (ny + 1) * (nz + 1);
+  const uint32_t ney = (nx + 1) * ny * (nz + 1);
+  auto at = [&](uint32_t a, uint32_t bb, uint32_t cc) {
+    return vec3<TF>{b.dmin.x + b.cs.x * TF(a), b.dmin.y + b.cs.y * TF(bb),
+                    b.dmin.z + b.cs.z * TF(cc)};
+  };
+  if (l < nv) {
+    const uint32_t t = l % ((ny + 1) * (nx + 1));
+    return at(t % (nx + 1), t / (nx + 1), l / ((ny + 1) * (nx + 1)));
+  }
+  if (l < nv + 2 * nex) {
+    l -= nv;
+    const uint32_t e = l / 2, t = e % ((ny + 1) * nx);
+    vec3<TF> p = at(t % nx, t / nx, e / ((ny + 1) * nx));
+    p.x += (TF(1) + TF(l % 2)) / TF(3) * b.cs.x;
+    return p;
+  }
+  if (l < nv + 2 * (nex + ney)) {
+    l -= nv + 2 * nex;
+    const uint32_t e = l / 2, t = e % ((nz + 1) * ny);
+    vec3<TF> p = at(e / ((nz + 1) * ny), t % ny, t / ny);
+    p.y += (TF(1) + TF(l % 2)) / TF(3) * b.cs.y;
+    return p;
+  }
+  l -= nv + 2 * (nex + ney);
+  const uint32_t e = l / 2, t = e % ((nx + 1) * nz);
+  vec3<TF> p = at(t / nz, e / ((nx + 1) * nz), t % nz);
+  p.z += (TF(1) + TF(l % 2)) / TF(3) * b.cs.z;
+  return p;
+}
+
+template <class TF>
+__global__ void k_node_positions(BodyDev<TF> b, TF* __restrict__ out) {
+  const uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= b.num_nodes) return;
+  st3(out, l, node_position(b, l));
+}
+
+template <class TF>
+__global__ void k_distance_grid(BodyDev<TF> b, TF* __restrict__ out) {
+  const uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= b.num_nodes) return;
+  out[l] = shape_sdf(b, node_position(b, l));
+}
+
+// update_volume_field: one warp per node; lanes stride over the 27,000
+// (theta, phi, r) samples and accumulate in double; the warp sum is the
+// node's integral times h^3.
+template <class TF>
+__global__ void __launch_bounds__(256)
+    k_volume_field(Cn<TF> c, BodyDev<TF> b, TF* __restrict__ out) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= b.num_nodes) return;
+  const auto& pt = PeirceSel<TF>::get();
+  const vec3<TF> x = node_position(b, warp);
+  constexpr int kDirs = peirce::kNumTheta * peirce::kNumPhi;
+  double sum = 0;
+  for (int f = lane; f < kDirs * peirce::kNumR; f += 32) {
+    const int k = f % peirce::kNumR;
+    const int dir = f / peirce::kNumR;  // dir = i * kNumPhi + j
+    const int j = dir % peirce::kNumPhi;
+    const int i = dir / peirce::kNumPhi;
+    const TF rr = c.h * pt.r[k];
+    const TF ux = pt.sp[j] * pt.ct[i], uy = pt.sp[j] * pt.st[i], uz = pt.cp[j];
+    const vec3<TF> p{x.x + rr * ux, x.y + rr * uy, x.z + rr * uz};
+    const TF dist = b.use_grid ? interpolate_grid(b, b.dist, p) : shape_sdf(b, p);
+    const TF dm = dist * b.sign;
+    const TF ext = dm <= TF(0) ? TF(1) : W_dist(c, dm) / c.w0;
+    sum += double(pt.w[j * peirce::kNumR + k]) * double(ext);
+  }
+  sum = warp_sum(sum);
+  if (lane == 0) out[warp] = TF(sum * double(c.h2) * double(c.h));
+}
+
+}  // namespace
+
+int upload_peirce_tables(cudaStream_t st) {
+  static PeirceDev tf;
+  static PeirceDevD td;
+  const double pi = 3.14159265358979323846264338327950288;
+  for (int i = 0; i < peirce::kNumTheta; ++i) {
+    const double theta = 2 * pi * (i + 1) / peirce::kNumTheta;
+    td.ct[i] = std::cos(theta);
+    td.st[i] = std::sin(theta);
+    tf.ct[i] = float(td.ct[i]);
+    tf.st[i] = float(td.st[i]);
+  }
+  for (int j = 0; j < peirce::kNumPhi; ++j) {
+    td.sp[j] = peirce::k_sinphi[j];
+    td.cp[j] = peirce::k_cosphi[j];
+    tf.sp[j] = float(td.sp[j]);
+    tf.cp[j] = float(td.cp[j]);
+  }
+  for (int j = 0; j < peirce::kNumPhi; ++j)
+    for (int k = 0; k < peirce::kNumR; ++k) {
+      td.w[j * peirce::kNumR + k] =
+          2 * pi * peirce::k_b[j] * peirce::k_c[k] / peirce::kNumTheta;
+      tf.w[j * peirce::kNumR + k] = float(td.w[j * peirce::kNumR + k]);
+    }
+  for (int k = 0; k < peirce::kNumR; ++k) {
+    td.r[k] = peirce::k_r[k];
+    tf.r[k] = float(td.r[k]);
+  }
+  ALB_CUDA(cudaMemcpyToSymbolAsync(c_peirce_f, &tf, sizeof(tf), 0, cudaMemcpyHostToDevice, st));
+  ALB_CUDA(cudaMemcpyToSymbolAsync(c_peirce_d, &td, sizeof(td), 0, cudaMemcpyHostToDevice, st));
+  ALB_CUDA(cudaStreamSynchronize(st));
+  return AL_OK;
+}
+
+template <class TF>
+int sample_boundaries(const Cn<TF>& c, const BodyDev<TF>* bodies_dev, const RigidDev<TF>* rigid_dev,
+                      uint32_t nb, const vec4<TF>* xs, const uint32_t* perm, uint32_t n,
+                      const BoundaryState<TF>& bs, TF* ref_boundary, TF* ref_kernel,
+                      cudaStream_t st) {
+  if (n == 0) return AL_OK;
+  k_sample_boundaries<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(
+      c, bodies_dev, rigid_dev, nb, xs, perm, n, bs.mask, bs.bx, bs.bk, ref_boundary, ref_kernel);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+template <class TF>
+int build_volume_field(const Cn<TF>& c, const BodyDev<TF>& b, TF* out, cudaStream_t st) {
+  const uint64_t threads = uint64_t(b.num_nodes) * 32;
+  k_volume_field<TF><<<uint32_t((threads + 255) / 256), 256, 0, st>>>(c, b, out);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+template <class TF>
+int build_distance_grid(const BodyDev<TF>& b, TF* out, cudaStream_t st) {
+  k_distance_grid<TF><<<blocks_for(b.num_nodes, 256), 256, 0, st>>>(b, out);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+template <class TF>
+int node_positions(const BodyDev<TF>& b, TF* out, cudaStream_t st) {
+  k_node_positions<TF><<<blocks_for(b.num_nodes, 256), 256, 0, st>>>(b, out);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+#define ALB_INST(TF)                                                                          \
+  template int sample_boundaries<TF>(const Cn<TF>&, const BodyDev<TF>*, const RigidDev<TF>*,  \
+                                     uint32_t, const vec4<TF>*, const uint32_t*, uint32_t,     \
+                                     const BoundaryState<TF>&, TF*, TF*, cudaStream_t);        \
+  template int build_volume_field<TF>(const Cn<TF>&, const BodyDev<TF>&, TF*, cudaStream_t); \
+  template int build_distance_grid<TF>(const BodyDev<TF>&, TF*, cudaStream_t);               \
+  template int node_positions<TF>(const BodyDev<TF>&, TF*, cudaStream_t);
+ALB_INST(float)
+ALB_INST(double)
+#undef ALB_INST
+
+}  // namespace alb

@@ -2,6 +2,7 @@
 // engine lifecycle, grid sort and the standalone neighbor update.
 #include <string>
 
+#include "boundary.cuh"
 #include "engine.hpp"
 #include "grid.cuh"
 #include "neighbors.cuh"
@@ -99,6 +100,8 @@ int al_engine_create(int device, al_engine** out) {
               "; this build targets sm_100a");
     return AL_ERR_NO_DEVICE;
   }
+  ALB_CUDA(cudaSetDevice(device));
+  ALB_TRY(upload_peirce_tables(nullptr));
   al_engine* e = new al_engine();
   e->device = device;
   e->num_sms = prop.multiProcessorCount;
@@ -150,8 +153,8 @@ template <class TF, class C>
 int grid_sort_impl(al_engine* e, const C* cn, const al_consti* cni, const TF* x, uint32_t n,
                    uint32_t* particle_cell, uint32_t* sorted_to_original, uint32_t* cell_start,
                    uint32_t* pid_length, void* stream) {
-  ALB_CHECK_ARG(e && cn && x, "al_grid_sort: null argument");
-  ALB_CHECK_ARG(particle_cell && sorted_to_original, "al_grid_sort: null output");
+  ALB_CHECK_ARG(e && cn && (x || n == 0), "al_grid_sort: null argument");
+  ALB_CHECK_ARG(n == 0 || (particle_cell && sorted_to_original), "al_grid_sort: null output");
   ALB_TRY(check_consti(cni));
   ALB_TRY(e->activate());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -164,9 +167,12 @@ int grid_sort_impl(al_engine* e, const C* cn, const al_consti* cni, const TF* x,
   ALB_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), st));
   GridState gs;
   ALB_TRY(grid_build<TF>(e, c, g, x, n, xs, flags, gs, st));
-  ALB_CUDA(cudaMemcpyAsync(particle_cell, gs.cell, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
-  ALB_CUDA(cudaMemcpyAsync(sorted_to_original, gs.perm, size_t(n) * 4, cudaMemcpyDeviceToDevice,
-                           st));
+  if (n > 0) {
+    ALB_CUDA(
+        cudaMemcpyAsync(particle_cell, gs.cell, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(sorted_to_original, gs.perm, size_t(n) * 4,
+                             cudaMemcpyDeviceToDevice, st));
+  }
   if (cell_start)
     ALB_CUDA(cudaMemcpyAsync(cell_start, gs.cell_start, (size_t(g.ncells) + 1) * 4,
                              cudaMemcpyDeviceToDevice, st));
@@ -180,7 +186,8 @@ template <class TF, class C>
 int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const TF* x,
                           uint32_t n, const TF* boundary_kernel, TF* density, uint32_t* num_nbr,
                           TF* neighbors, uint32_t* grid_anomaly, void* stream) {
-  ALB_CHECK_ARG(e && cn && x && num_nbr, "al_update_particle_neighbors: null argument");
+  ALB_CHECK_ARG(e && cn && ((x && num_nbr) || n == 0),
+                "al_update_particle_neighbors: null argument");
   ALB_TRY(check_consti(cni));
   ALB_CHECK_ARG(cni->num_boundaries == 0 || boundary_kernel != nullptr,
                 "al_update_particle_neighbors: boundary kernel required when num_boundaries > 0");
@@ -200,7 +207,7 @@ int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const
   GridState gs;
   ALB_TRY(grid_build<TF>(e, c, g, x, n, xs, flags, gs, st));
   RefBoundaryKernel<TF> bk{boundary_kernel, gs.perm, n, g.nb};
-  ALB_TRY(build_neighbors_density<TF>(c, g, gs, xs, bk, nbr, ncount, rho, st));
+  ALB_TRY(build_neighbors_density<TF>(c, g, gs, xs, bk, nbr, ncount, rho, nullptr, st));
   ALB_TRY(export_neighbors<TF>(g, gs, xs, nbr, ncount, rho, neighbors, num_nbr, density, st));
   if (grid_anomaly)
     ALB_CUDA(cudaMemcpyAsync(grid_anomaly, flags, 3 * sizeof(uint32_t), cudaMemcpyDeviceToDevice,

@@ -77,6 +77,17 @@ __host__ __device__ __forceinline__ vec3<TF> cross(vec3<TF> a, vec3<TF> b) {
   return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
 
+template <class TF>
+__host__ __device__ __forceinline__ constexpr TF max_value();
+template <>
+__host__ __device__ __forceinline__ constexpr float max_value<float>() {
+  return 3.40282346638528859811704183484516925e+38f;
+}
+template <>
+__host__ __device__ __forceinline__ constexpr double max_value<double>() {
+  return 1.79769313486231570814527423731704357e+308;
+}
+
 __device__ __forceinline__ float rsqrt_(float v) { return rsqrtf(v); }
 __device__ __forceinline__ double rsqrt_(double v) { return rsqrt(v); }
 

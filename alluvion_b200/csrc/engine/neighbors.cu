@@ -8,12 +8,13 @@ namespace {
 
 inline uint32_t blocks_for(uint32_t n, int block) { return (n + block - 1) / block; }
 
-template <class TF, class BK>
+template <class TF, class BK, bool FACTOR>
 __global__ void __launch_bounds__(kBlock)
     k_build_neighbors(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
                       const vec4<TF>* __restrict__ xs, uint32_t n, BK bk,
                       uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount,
-                      TF* __restrict__ rho, uint32_t* __restrict__ flags) {
+                      TF* __restrict__ rho, TF* __restrict__ alpha,
+                      uint32_t* __restrict__ flags) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const vec3<TF> xi = xyz(xs[s]);
@@ -23,6 +24,8 @@ __global__ void __launch_bounds__(kBlock)
   const int z1 = min(ip[2] + 1, int(g.res[2]) - 1);
   uint32_t cnt = 0;
   TF density = c.vol * c.w0;
+  TF sum_grad = 0;
+  vec3<TF> grad_i{0, 0, 0};
   if (z0 <= z1) {
     for (int dx = -1; dx <= 1; ++dx) {
       const int cx = ip[0] + dx;
@@ -40,6 +43,12 @@ __global__ void __launch_bounds__(kBlock)
             if (cnt < g.cap_nbr) {
               nbr[size_t(cnt) * n + s] = t;
               density += c.vol * W_r2(c, d2);
+              if (FACTOR) {
+                const vec3<TF> d{sub_rn(xi.x, xj.x), sub_rn(xi.y, xj.y), sub_rn(xi.z, xj.z)};
+                const vec3<TF> gpj = (-c.vol) * gradW(c, d);
+                sum_grad += length_sqr(gpj);
+                grad_i -= gpj;
+              }
             }
             ++cnt;
           }
@@ -54,6 +63,11 @@ __global__ void __launch_bounds__(kBlock)
   ncount[s] = cnt;
   density += bk.density_term(s);
   rho[s] = density * c.rho0;
+  if (FACTOR) {
+    grad_i += bk.grad_term(s);
+    sum_grad += length_sqr(grad_i);
+    alpha[s] = sum_grad > c.eps ? TF(-1) / sum_grad : TF(0);
+  }
 }
 
 template <class TF>
@@ -93,10 +107,14 @@ __global__ void k_export_neighbors(uint32_t cap, uint32_t n, const uint32_t* __r
 template <class TF, class BK>
 int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState& gs,
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
-                            TF* rho, cudaStream_t st) {
+                            TF* rho, TF* alpha, cudaStream_t st) {
   if (gs.n == 0) return AL_OK;
-  k_build_neighbors<TF, BK><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
-      c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, gs.flags);
+  if (alpha)
+    k_build_neighbors<TF, BK, true><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
+        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, gs.flags);
+  else
+    k_build_neighbors<TF, BK, false><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
+        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, gs.flags);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }
@@ -114,12 +132,15 @@ int export_neighbors(const GridDims& g, const GridState& gs, const vec4<TF>* xs,
   return AL_OK;
 }
 
-template int build_neighbors_density<float, RefBoundaryKernel<float>>(
-    const Cn<float>&, const GridDims&, const GridState&, const vec4<float>*,
-    const RefBoundaryKernel<float>&, uint32_t*, uint32_t*, float*, cudaStream_t);
-template int build_neighbors_density<double, RefBoundaryKernel<double>>(
-    const Cn<double>&, const GridDims&, const GridState&, const vec4<double>*,
-    const RefBoundaryKernel<double>&, uint32_t*, uint32_t*, double*, cudaStream_t);
+#define ALB_INST(TF, BK)                                                                  \
+  template int build_neighbors_density<TF, BK<TF>>(                                       \
+      const Cn<TF>&, const GridDims&, const GridState&, const vec4<TF>*, const BK<TF>&,    \
+      uint32_t*, uint32_t*, TF*, TF*, cudaStream_t);
+ALB_INST(float, RefBoundaryKernel)
+ALB_INST(double, RefBoundaryKernel)
+ALB_INST(float, SortedBoundaryKernel)
+ALB_INST(double, SortedBoundaryKernel)
+#undef ALB_INST
 template int export_neighbors<float>(const GridDims&, const GridState&, const vec4<float>*,
                                      const uint32_t*, const uint32_t*, const float*, float*,
                                      uint32_t*, float*, cudaStream_t);

@@ -34,15 +34,48 @@ struct RefBoundaryKernel {
     }
     return sum;
   }
+  __device__ __forceinline__ vec3<TF> grad_term(uint32_t s) const {
+    vec3<TF> g{0, 0, 0};
+    if (bk) {
+      const uint32_t i = perm[s];
+      for (uint32_t b = 0; b < nb; ++b) {
+        const TF* e = bk + (size_t(b) * n + i) * 4;
+        g += vec3<TF>{e[0], e[1], e[2]};
+      }
+    }
+    return g;
+  }
+};
+
+// The engine's sparse boundary state in sorted order: only bodies whose bit
+// is set in mask[s] contribute (their volume is non-zero; the others'
+// terms are exactly zero).  Bodies are visited in ascending order, as the
+// reference's boundary loops do.
+template <class TF>
+struct SortedBoundaryKernel {
+  const uint32_t* mask;
+  const vec4<TF>* bk;
+  uint32_t n;
+  __device__ __forceinline__ TF density_term(uint32_t s) const {
+    TF sum = 0;
+    for (uint32_t m = mask[s]; m; m &= m - 1) sum += bk[size_t(__ffs(m) - 1) * n + s].w;
+    return sum;
+  }
+  __device__ __forceinline__ vec3<TF> grad_term(uint32_t s) const {
+    vec3<TF> g{0, 0, 0};
+    for (uint32_t m = mask[s]; m; m &= m - 1) g += xyz(bk[size_t(__ffs(m) - 1) * n + s]);
+    return g;
+  }
 };
 
 // Builds nbr / ncount for all n sorted slots and the density
-// rho_s = rho0 (V W(0) + sum_j V W(x_sj) + boundary).  Raises flags[2] on
-// neighbor overflow.
+// rho_s = rho0 (V W(0) + sum_j V W(x_sj) + boundary).  When `alpha` is
+// non-null also the DFSPH factor of compute_dfsph_factor
+// (runner.hpp:3123-3154).  Raises flags[2] on neighbor overflow.
 template <class TF, class BK>
 int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState& gs,
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
-                            TF* rho, cudaStream_t st);
+                            TF* rho, TF* alpha, cudaStream_t st);
 
 // Writes reference-layout outputs in original particle order:
 // particle_neighbors [N][cap][4] {x_i - x_j, bits(j)} (if non-null),

@@ -1,0 +1,1009 @@
+// solver.cu -- DFSPH / IISPH step kernels and their orchestration.
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+#include "neighbors.cuh"
+#include "solver.cuh"
+
+namespace alb {
+
+namespace {
+
+inline uint32_t blocks_for(uint32_t n, int block) { return (n + block - 1) / block; }
+
+template <class TF>
+__device__ __forceinline__ vec3<TF> body_velocity(const RigidDev<TF>& r, vec3<TF> at) {
+  return cross(r.omega, at - r.x) + r.v;
+}
+
+template <class TF>
+__device__ __forceinline__ vec3<TF> ldx(const vec4<TF>* p, uint32_t i) {
+  return xyz(__ldg(p + i));
+}
+
+// Adds the block's contributions (f, t) for body b to the block's rigid
+// force/torque slot: warp trees, then warp partials in warp order.  All
+// threads of the block call it.  Deterministic.
+template <class TF>
+__device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b, vec3<TF> f,
+                                             vec3<TF> t) {
+  __shared__ double part[6][kBlock / 32];
+  double v[6] = {double(f.x), double(f.y), double(f.z), double(t.x), double(t.y), double(t.z)};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = warp_sum(v[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) part[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0;
+    for (int w = 0; w < kBlock / 32; ++w) s += part[threadIdx.x][w];
+    S.ft[(size_t(blockIdx.x) * S.nb + b) * 6 + threadIdx.x] += s;
+  }
+  __syncthreads();
+}
+
+// Deterministic grid-wide double sum: every block writes its block sum to
+// red[blockIdx]; the last block to finish (ticket) sums the partials in
+// block order.  Returns true in the last block, with the total in thread 0.
+__device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_t* ticket,
+                                              double* total) {
+  __shared__ bool last;
+  const double bsum = block_sum_double(value);
+  if (threadIdx.x == 0) {
+    red[blockIdx.x] = bsum;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double s = 0;
+  for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) s += __ldcg(red + k);
+  s = block_sum_double(s);
+  if (threadIdx.x == 0) {
+    *total = s;
+    *ticket = 0;
+  }
+  return true;
+}
+
+// Sum over neighbors of V (v_i - v_j) . grad W_ij plus the boundary terms
+// (v_i - v_b) . (grad W V)_b: the shared body of compute_density_change
+// (runner.hpp:3192-3228) and compute_density_adv (runner.hpp:3493-3523).
+template <class TF>
+__device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepState<TF>& S,
+                                                  uint32_t s, vec3<TF> xi, vec3<TF> vi,
+                                                  uint32_t cnt) {
+  TF acc = 0;
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const vec3<TF> d = xi - ldx(S.x, t);
+    acc += c.vol * dot(vi - ldx(S.v, t), gradW(c, d));
+  }
+  for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+    const uint32_t b = __ffs(m) - 1;
+    const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+    const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+    const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
+    acc += dot(vi - vj, xyz(kg));
+  }
+  return acc;
+}
+
+template <class TF>
+__device__ __forceinline__ TF density_change(const Cn<TF>& c, const StepState<TF>& S, uint32_t s) {
+  const uint32_t cnt = S.ncount[s];
+  TF adv = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), cnt);
+  adv = fmax(adv, TF(0));
+  if (cnt < 20) adv = 0;
+  return adv;
+}
+
+template <class TF>
+__device__ __forceinline__ TF density_adv(const Cn<TF>& c, const StepState<TF>& S, uint32_t s,
+                                          TF dt) {
+  const TF delta = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), S.ncount[s]);
+  return fmax(S.rho[s] / c.rho0 + dt * delta, TF(1));
+}
+
+// ------------------------------------------------------------- kernels
+template <class TF>
+__global__ void k_step_init(StepState<TF> S) {
+  Ctrl<TF>& C = *S.ctrl;
+  if (threadIdx.x == 0) {
+    C.ticket = 0;
+    C.vmax_bits = 0;
+    C.it = 0;
+    C.keep_going = 0;
+    C.mean = 0;
+    al_step_report& r = C.rep;
+    r.num_divergence_solve = 0;
+    r.num_density_solve = 0;
+    r.mean_density_change = DBL_MAX;
+    r.mean_density_error = DBL_MAX;
+    r.num_active_boundary_pairs = 0;
+    for (int k = 0; k < AL_MAX_BOUNDARIES; ++k)
+      for (int j = 0; j < 3; ++j) r.force[k][j] = r.torque[k][j] = 0;
+    // Pile::calculate_cfl_v2 (pile.hpp:816-825)
+    TF m = -max_value<TF>();
+    for (uint32_t b = 0; b < S.nb; ++b) {
+      const RigidDev<TF>& rg = S.rigid[b];
+      const vec3<TF> w = cross(rg.omega, vec3<TF>{S.bodies[b].max_distance, TF(0), TF(0)}) + rg.v;
+      m = fmax(m, length_sqr(w));
+    }
+    r.pile_max_v2 = double(m);
+  }
+}
+
+template <class TF, bool DF>
+__global__ void k_gather_state(StepState<TF> S, const TF* __restrict__ v_ref,
+                               const TF* __restrict__ k_ref, const TF* __restrict__ kv_ref) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const uint32_t i = S.perm[s];
+  const vec3<TF> v = ld3(v_ref, i);
+  S.v[s] = vec4<TF>{v.x, v.y, v.z, TF(0)};
+  S.kappa[s] = k_ref ? k_ref[i] : TF(0);
+  if (DF) S.kappa_v[s] = kv_ref ? kv_ref[i] : TF(0);
+}
+
+// warm_start_divergence_solve_0 (runner.hpp:3230-3249).
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_df_warm0(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF adv = density_change(c, S, s);
+  const TF dt = S.ctrl->dt;
+  const TF kv = S.kappa_v[s];
+  S.kappa_v[s] = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
+}
+
+enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
+
+// The kappa-driven velocity updates: warm_start_divergence_solve_1
+// (runner.hpp:3251-3295), divergence_solve_iteration (:3316-3363),
+// warm_start_pressure_solve1 (:3451-3491), pressure_solve_iteration
+// (:3543-3588).  Boundary reaction forces go to the per-block rigid slots.
+template <class TF, int MODE>
+__global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
+  constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = s < S.n;
+  const TF* __restrict__ ksrc =
+      MODE == kDivWarm ? S.kappa_v : (MODE == kPressWarm ? S.kappa : S.kk);
+  const TF dt = S.ctrl->dt;
+  TF ki = 0;
+  vec3<TF> dv{0, 0, 0};
+  uint32_t m = 0;
+  if (act) {
+    ki = ksrc[s];
+    const vec3<TF> xi = xyz(S.x[s]);
+    const uint32_t cnt = S.ncount[s];
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const TF ksum = ki + __ldg(ksrc + t);
+      if (fabs(ksum) > c.eps) {
+        const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+        if (kDiv) {
+          const vec3<TF> gpj = (-c.vol) * gw;
+          dv -= (dt * ksum) * gpj;
+        } else {
+          dv += (dt * ksum * c.vol) * gw;
+        }
+      }
+    }
+    if (fabs(ki) > c.eps) m = S.mask[s];
+  }
+  for (uint32_t b = 0; b < S.nb; ++b) {
+    const bool mine = (m >> b) & 1u;
+    if (!__syncthreads_or(mine)) continue;
+    vec3<TF> f{0, 0, 0}, tq{0, 0, 0};
+    if (mine) {
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+      const vec3<TF> a = ki * (-xyz(kg));
+      f = c.mass * a;
+      dv -= dt * a;
+      tq = cross(xyz(bn) - S.rigid[b].x, f);
+    }
+    block_add_ft(S, b, f, tq);
+  }
+  if (act) {
+    if (MODE == kDivIter) S.kappa_v[s] += ki;
+    if (MODE == kPressIter) S.kappa[s] += ki;
+    vec4<TF> v = S.v[s];
+    S.v[s] = vec4<TF>{v.x + dv.x, v.y + dv.y, v.z + dv.z, v.w};
+  }
+}
+
+// compute_velocity_of_density_change (runner.hpp:3297-3314); also forms
+// k = rho_adv * alpha for the first divergence iteration.
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF adv = density_change(c, S, s);
+  const TF dt = S.ctrl->dt;
+  const TF alpha = S.alpha[s] * (TF(1) / dt);
+  S.rho_adv[s] = adv;
+  S.alpha[s] = alpha;
+  S.kk[s] = adv * alpha;
+}
+
+template <class TF>
+__global__ void k_loop_begin(StepState<TF> S, int density_solve,
+                             cudaGraphConditionalHandle handle, int use_handle) {
+  Ctrl<TF>& C = *S.ctrl;
+  C.it = 0;
+  C.ticket = 0;
+  const uint32_t mx = density_solve ? C.max_den : C.max_div;
+  C.keep_going = mx > 0;
+  if (use_handle) cudaGraphSetConditional(handle, C.keep_going);
+}
+
+// Loop decision of solver_df.hpp:131-133 / 296-298 and solver_ii.hpp:181-183.
+template <class TF>
+__device__ __forceinline__ void finish_iteration(Ctrl<TF>& C, double total, uint32_t n,
+                                                 int which, cudaGraphConditionalHandle handle,
+                                                 int use_handle) {
+  C.mean = total / double(n);
+  C.it += 1;
+  bool go;
+  if (which == 0) {
+    go = (C.mean > C.tol_div / double(C.dt) || C.it < C.min_div) && C.it < C.max_div;
+    C.rep.num_divergence_solve = C.it;
+    C.rep.mean_density_change = C.mean;
+  } else {
+    go = (C.mean > C.tol_den || C.it < C.min_den) && C.it < C.max_den;
+    C.rep.num_density_solve = C.it;
+    C.rep.mean_density_error = C.mean;
+  }
+  C.keep_going = go;
+  if (use_handle) cudaGraphSetConditional(handle, go);
+}
+
+// compute_divergence_solve_density_error (runner.hpp:3396-3410) with the
+// mean of solver_df.hpp:160-161 reduced in double on the device.
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_df_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  double val = 0;
+  if (s < S.n) {
+    const TF adv = density_change(c, S, s);
+    S.rho_adv[s] = adv;
+    S.kk[s] = adv * S.alpha[s];
+    val = double(adv);
+  }
+  double total;
+  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total) && threadIdx.x == 0)
+    finish_iteration(*S.ctrl, total, S.n, 0, handle, use_handle);
+}
+
+// clear_acceleration + compute_viscosity (runner.hpp:1974-1980, 2150-2249),
+// divergence_solve_finish (runner.hpp:3412-3420) when `finish_div`, and
+// calculate_cfl_v2 (runner.hpp:2533-2541) reduced to the global max; the
+// last block applies Solver::update_dt (solver.hpp:153-169).
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_viscosity(Cn<TF> c, StepState<TF> S, int finish_div) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = s < S.n;
+  const TF dt = S.ctrl->dt;
+  vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, da{0, 0, 0};
+  uint32_t m = 0;
+  if (act) {
+    xi = xyz(S.x[s]);
+    vi = xyz(S.v[s]);
+    const uint32_t cnt = S.ncount[s];
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const vec3<TF> d = xi - ldx(S.x, t);
+      da += (c.visc * c.mass / __ldg(S.rho + t) * dot(d, gradW(c, d)) /
+             (length_sqr(d) + TF(0.01) * c.h2)) *
+            (vi - ldx(S.v, t));
+    }
+    m = S.mask[s];
+  }
+  for (uint32_t b = 0; b < S.nb; ++b) {
+    const bool mine = (m >> b) & 1u;
+    if (!__syncthreads_or(mine)) continue;
+    vec3<TF> fsum{0, 0, 0}, tsum{0, 0, 0};
+    if (mine) {
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+      const vec3<TF> bxj = xyz(bn);
+      const RigidDev<TF> rg = S.rigid[b];
+      vec3<TF> nrm = bxj - xi;
+      const TF nl2 = length_sqr(nrm);
+      if (nl2 > TF(0)) {
+        nrm = rsqrt_(nl2) * nrm;
+        // get_orthogonal_vectors (runner.hpp:119-131)
+        vec3<TF> ref{TF(1), TF(0), TF(0)};
+        if (fabs(dot(ref, nrm)) > TF(0.999)) ref = vec3<TF>{TF(0), TF(1), TF(0)};
+        vec3<TF> t1 = cross(nrm, ref);
+        vec3<TF> t2 = cross(nrm, t1);
+        t1 = rsqrt_(dot(t1, t1)) * t1;
+        t2 = rsqrt_(dot(t2, t2)) * t2;
+        const TF dist = c.h - sqrt(nl2);
+        const vec3<TF> pts[4] = {bxj - t1 * dist, bxj + t1 * dist, bxj - t2 * dist,
+                                 bxj + t2 * dist};
+        const TF vol = TF(0.25) * bn.w;
+        vec3<TF> acc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const vec3<TF> xix = xi - pts[q];
+          const vec3<TF> vb = body_velocity(rg, pts[q]);
+          acc[q] = (c.bvisc * vol * dot(xix, gradW(c, xix)) /
+                    (length_sqr(xix) + TF(0.01) * c.h2)) *
+                   (vi - vb);
+        }
+        da += acc[0] + acc[1] + acc[2] + acc[3];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const vec3<TF> fq = (-c.mass) * acc[q];
+          fsum += fq;
+          tsum += cross(pts[q] - rg.x, fq);
+        }
+      }
+    }
+    block_add_ft(S, b, fsum, tsum);
+  }
+  TF v2 = 0;
+  if (act) {
+    const vec3<TF> a = c.g + da;
+    S.a[s] = vec4<TF>{a.x, a.y, a.z, TF(0)};
+    if (finish_div) {
+      S.alpha[s] *= dt;
+      S.kappa_v[s] *= dt;
+    }
+    v2 = length_sqr(vi + a * dt);
+  }
+  // block max, then one ordered-bits atomicMax per block
+  __shared__ TF wmax[kBlock / 32];
+  __shared__ bool last;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    TF bm = wmax[0];
+    for (int w = 1; w < kBlock / 32; ++w) bm = fmax(bm, wmax[w]);
+    unsigned long long bits;
+    if constexpr (sizeof(TF) == 4)
+      bits = __float_as_uint(bm);
+    else
+      bits = (unsigned long long)__double_as_longlong(bm);
+    atomicMax(&S.ctrl->vmax_bits, bits);
+    __threadfence();
+    last = atomicAdd(&S.ctrl->ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    Ctrl<TF>& C = *S.ctrl;
+    __threadfence();
+    const unsigned long long bits = atomicAdd(&C.vmax_bits, 0ull);
+    TF pmax;
+    if constexpr (sizeof(TF) == 4)
+      pmax = __uint_as_float(uint32_t(bits));
+    else
+      pmax = __longlong_as_double((long long)bits);
+    const TF pile = TF(C.rep.pile_max_v2);
+    const TF max_v2 = fmax(pmax, pile);
+    const TF max_v = sqrt(max_v2);
+    const TF cfl_dt = C.cfl * C.length_scale / max_v;
+    const TF ndt = fmax(fmin(cfl_dt, C.max_dt), C.min_dt);
+    C.rep.particle_max_v2 = double(pmax);
+    C.rep.max_v2 = double(max_v2);
+    C.rep.cfl_dt = double(cfl_dt);
+    C.rep.utilized_cfl = double(ndt * max_v / C.length_scale);
+    C.rep.dt = double(ndt);
+    C.dt = ndt;
+    C.ticket = 0;
+  }
+}
+
+// integrate_non_pressure_acceleration (runner.hpp:3422-3428).
+template <class TF>
+__global__ void k_integrate_np(StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF dt = S.ctrl->dt;
+  const vec4<TF> a = S.a[s];
+  vec4<TF> v = S.v[s];
+  S.v[s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
+}
+
+// warm_start_pressure_solve0 (runner.hpp:3430-3449).
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_p_warm0(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF dt = S.ctrl->dt;
+  const TF adv = density_adv(c, S, s, dt);
+  const TF kp = S.kappa[s];
+  S.kappa[s] = adv > TF(1) ? TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt) : TF(0);
+}
+
+// compute_rho_adv (runner.hpp:3525-3541); also k for the first iteration.
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF dt = S.ctrl->dt;
+  const TF adv = density_adv(c, S, s, dt);
+  const TF alpha = S.alpha[s] * (TF(1) / (dt * dt));
+  S.rho_adv[s] = adv;
+  S.alpha[s] = alpha;
+  S.kk[s] = (adv - TF(1)) * alpha;
+}
+
+// compute_pressure_solve_density_error (runner.hpp:3590-3604); the mean is
+// sum(rho_adv - 1) / N in double (solver_df.hpp:323-325 forms sum/N - 1).
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_p_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  double val = 0;
+  if (s < S.n) {
+    const TF adv = density_adv(c, S, s, S.ctrl->dt);
+    S.rho_adv[s] = adv;
+    S.kk[s] = (adv - TF(1)) * S.alpha[s];
+    val = double(adv) - 1.0;
+  }
+  double total;
+  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total) && threadIdx.x == 0)
+    finish_iteration(*S.ctrl, total, S.n, 1, handle, use_handle);
+}
+
+// pressure_solve_finish + integrate_velocity<0> (runner.hpp:3606-3623),
+// written straight back to the caller's buffers in original order.
+template <class TF>
+__global__ void k_df_finish(StepState<TF> S, int density_solve, TF* __restrict__ x_ref,
+                            TF* __restrict__ v_ref, TF* __restrict__ a_ref,
+                            TF* __restrict__ rho_ref, TF* __restrict__ alpha_ref,
+                            TF* __restrict__ kappa_ref, TF* __restrict__ kappa_v_ref,
+                            TF* __restrict__ rho_adv_ref) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const uint32_t i = S.perm[s];
+  const TF dt = S.ctrl->dt;
+  const vec3<TF> v = xyz(S.v[s]);
+  const vec3<TF> x = xyz(S.x[s]);
+  st3(x_ref, i, x + dt * v);
+  st3(v_ref, i, v);
+  if (a_ref) st3(a_ref, i, xyz(S.a[s]));
+  if (rho_ref) rho_ref[i] = S.rho[s];
+  if (alpha_ref) alpha_ref[i] = S.alpha[s];
+  TF kp = S.kappa[s];
+  if (density_solve) kp *= dt * dt;
+  if (kappa_ref) kappa_ref[i] = kp;
+  if (kappa_v_ref) kappa_v_ref[i] = S.kappa_v[s];
+  if (rho_adv_ref) rho_adv_ref[i] = S.rho_adv[s];
+}
+
+// ------------------------------------------------------------------ IISPH
+// predict_advection0 (runner.hpp:2609-2639).  kappa holds the pressure,
+// kappa_v the last pressure.
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF dt = S.ctrl->dt;
+  const vec4<TF> a = S.a[s];
+  vec4<TF> v = S.v[s];
+  S.v[s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
+  S.kappa_v[s] = S.kappa[s] * TF(0.5);
+  const vec3<TF> xi = xyz(S.x[s]);
+  const TF rho = S.rho[s], rho2 = rho * rho;
+  vec3<TF> dii{0, 0, 0};
+  const uint32_t cnt = S.ncount[s];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    dii -= (c.vol / rho2) * gradW(c, xi - ldx(S.x, t));
+  }
+  for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+    const uint32_t b = __ffs(m) - 1;
+    const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+    dii -= vec3<TF>{kg.x / rho2, kg.y / rho2, kg.z / rho2};
+  }
+  dii = dii * c.rho0;
+  S.dii[s] = vec4<TF>{dii.x, dii.y, dii.z, TF(0)};
+}
+
+// predict_advection1 (runner.hpp:2640-2690).  aii goes to kk.
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF dt = S.ctrl->dt;
+  const vec3<TF> xi = xyz(S.x[s]), vi = xyz(S.v[s]), dii = xyz(S.dii[s]);
+  const TF rho = S.rho[s], rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
+  TF adv = rho / c.rho0, aii = 0;
+  const uint32_t cnt = S.ncount[s];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+    const vec3<TF> dji = (dpi * c.rho0) * gw;
+    adv += dt * c.vol * dot(vi - ldx(S.v, t), gw);
+    aii += c.vol * dot(dii - dji, gw);
+  }
+  for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+    const uint32_t b = __ffs(m) - 1;
+    const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+    const vec3<TF> gw = xyz(S.bk[size_t(b) * S.n + s]);
+    const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
+    const vec3<TF> dji = (inv_rho2 * c.rho0) * gw;
+    adv += dt * dot(vi - vj, gw);
+    aii += dot(dii - dji, gw);
+  }
+  S.rho_adv[s] = adv;
+  S.kk[s] = aii * c.rho0;
+}
+
+// pressure_solve_iteration0 (runner.hpp:2691-2715).  On iterations after
+// the first, also performs the reference's last_pressure <- pressure copy
+// (solver_ii.hpp:204) for the own particle; this kernel reads the
+// neighbors' pressure (equal to their last pressure after that copy).
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const bool first = S.ctrl->it == 0;
+  const TF* __restrict__ src = first ? S.kappa_v : S.kappa;
+  if (!first) S.kappa_v[s] = S.kappa[s];
+  const vec3<TF> xi = xyz(S.x[s]);
+  vec3<TF> acc{0, 0, 0};
+  const uint32_t cnt = S.ncount[s];
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const TF rj = __ldg(S.rho + t), rj2 = rj * rj;
+    acc -= (c.vol / rj2 * src[t]) * gradW(c, xi - ldx(S.x, t));
+  }
+  acc = acc * c.rho0;
+  S.dij_pj[s] = vec4<TF>{acc.x, acc.y, acc.z, TF(0)};
+}
+
+// pressure_solve_iteration1 (runner.hpp:2716-2772) and the mean of
+// solver_ii.hpp:205-206 (double, on the device).
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_ii_iter1(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  double val = 0;
+  if (s < S.n) {
+    const TF dt = S.ctrl->dt;
+    const vec3<TF> xi = xyz(S.x[s]);
+    const TF lp = S.kappa_v[s];
+    const vec3<TF> dij_pj = xyz(S.dij_pj[s]);
+    const TF rho = S.rho[s], rho2 = rho * rho, dpi = c.vol / rho2;
+    const TF bterm = TF(1) - S.rho_adv[s];
+    const TF dt2 = dt * dt;
+    const TF denom = S.kk[s] * dt2;
+    const TF omega = TF(2) / TF(3);
+    TF p = 0, sum = 0;
+    const uint32_t cnt = S.ncount[s];
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+      const vec3<TF> dji = (dpi * c.rho0) * gw;
+      const vec3<TF> dji_pi = dji * lp;
+      sum += c.vol * dot(dij_pj - ldx(S.dii, t) * __ldg(S.kappa_v + t) -
+                             (ldx(S.dij_pj, t) - dji_pi),
+                         gw);
+    }
+    for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+      const uint32_t b = __ffs(m) - 1;
+      sum += dot(dij_pj, xyz(S.bk[size_t(b) * S.n + s]));
+    }
+    sum *= c.rho0;
+    if (fabs(denom) > TF(1.0e-9))
+      p = fmax((TF(1) - omega) * lp + omega / denom * (bterm - dt2 * sum), TF(0));
+    const TF err = p == TF(0) ? TF(0) : (denom * p + sum * dt2 - bterm);
+    S.err[s] = err;
+    S.kappa[s] = p;
+    val = double(err);
+  }
+  double total;
+  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total) && threadIdx.x == 0)
+    finish_iteration(*S.ctrl, total, S.n, 1, handle, use_handle);
+}
+
+// compute_pressure_accels (runner.hpp:2774-2817) + kinematic_integration<0>
+// (runner.hpp:2873-2887), written back in original order.
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_ii_accel_finish(Cn<TF> c, StepState<TF> S, TF* __restrict__ x_ref, TF* __restrict__ v_ref,
+                      TF* __restrict__ a_ref, TF* __restrict__ rho_ref, TF* __restrict__ p_ref,
+                      TF* __restrict__ rho_adv_ref) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = s < S.n;
+  vec3<TF> ai{0, 0, 0}, xi{0, 0, 0};
+  TF dpi = 0;
+  uint32_t m = 0;
+  if (act) {
+    xi = xyz(S.x[s]);
+    const TF rho = S.rho[s];
+    dpi = S.kappa[s] / (rho * rho);
+    const uint32_t cnt = S.ncount[s];
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const TF rj = __ldg(S.rho + t);
+      const TF dpj = __ldg(S.kappa + t) / (rj * rj);
+      ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldx(S.x, t));
+    }
+    m = S.mask[s];
+  }
+  for (uint32_t b = 0; b < S.nb; ++b) {
+    const bool mine = (m >> b) & 1u;
+    if (!__syncthreads_or(mine)) continue;
+    vec3<TF> f{0, 0, 0}, tq{0, 0, 0};
+    if (mine) {
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+      const vec3<TF> a = (c.rho0 * dpi) * xyz(S.bk[size_t(b) * S.n + s]);
+      f = c.mass * a;
+      ai -= a;
+      tq = cross(xyz(bn) - S.rigid[b].x, f);
+    }
+    block_add_ft(S, b, f, tq);
+  }
+  if (!act) return;
+  const TF dt = S.ctrl->dt;
+  const vec3<TF> ap = c.rho0 * ai;
+  const vec3<TF> v = xyz(S.v[s]) + ap * dt;
+  const uint32_t i = S.perm[s];
+  st3(x_ref, i, xi + v * dt);
+  st3(v_ref, i, v);
+  if (a_ref) st3(a_ref, i, xyz(S.a[s]));
+  if (rho_ref) rho_ref[i] = S.rho[s];
+  if (p_ref) p_ref[i] = S.kappa[s];
+  if (rho_adv_ref) rho_adv_ref[i] = S.rho_adv[s];
+}
+
+// Per-body totals of the rigid slots (solver_df.hpp:346-353) in double and
+// Pile::integrate_kinematics (pile.hpp:794-815).  One block per body.
+template <class TF>
+__global__ void k_rigid_finish(StepState<TF> S) {
+  const uint32_t b = blockIdx.x;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t g = threadIdx.x; g < S.grid; g += blockDim.x) {
+    const double* slot = S.ft + (size_t(g) * S.nb + b) * 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] += slot[k];
+  }
+  double tot[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) tot[k] = block_sum_double(acc[k]);
+  if (threadIdx.x != 0) return;
+  Ctrl<TF>& C = *S.ctrl;
+  for (int k = 0; k < 3; ++k) {
+    C.rep.force[b][k] = tot[k];
+    C.rep.torque[b][k] = tot[3 + k];
+  }
+  if (!C.integrate_rigids) return;
+  const TF dt = C.dt;
+  const BodyDev<TF>& body = S.bodies[b];
+  RigidDev<TF> r = S.rigid[b];
+  auto advance_q = [&]() {
+    const vec3<TF> w = r.omega;
+    const vec4<TF> q = r.q;
+    const vec4<TF> dq{TF(0.5) * (w.x * q.w + w.y * q.z - w.z * q.y),
+                      TF(0.5) * (-w.x * q.z + w.y * q.w + w.z * q.x),
+                      TF(0.5) * (w.x * q.y - w.y * q.x + w.z * q.w),
+                      TF(0.5) * (-w.x * q.x - w.y * q.y - w.z * q.z)};
+    vec4<TF> nq{q.x + dt * dq.x, q.y + dt * dq.y, q.z + dt * dq.z, q.w + dt * dq.w};
+    const TF inv = rsqrt_(nq.x * nq.x + nq.y * nq.y + nq.z * nq.z + nq.w * nq.w);
+    r.q = vec4<TF>{nq.x * inv, nq.y * inv, nq.z * inv, nq.w * inv};
+  };
+  if (body.mass == TF(0)) {
+    r.x += r.v * dt;
+    advance_q();
+  } else {
+    const vec3<TF> force{TF(tot[0]), TF(tot[1]), TF(tot[2])};
+    const vec3<TF> torque{TF(tot[3]), TF(tot[4]), TF(tot[5])};
+    r.v += (TF(1) / body.mass) * force * dt;
+    // calculate_angular_acceleration (runner.hpp:202-239)
+    const vec4<TF> q = r.q;
+    const vec3<TF> ii{TF(1) / body.inertia.x, TF(1) / body.inertia.y, TF(1) / body.inertia.z};
+    const TF m[3][3] = {{TF(1) - TF(2) * (q.y * q.y + q.z * q.z), TF(2) * (q.x * q.y - q.z * q.w),
+                         TF(2) * (q.x * q.z + q.y * q.w)},
+                        {TF(2) * (q.x * q.y + q.z * q.w), TF(1) - TF(2) * (q.x * q.x + q.z * q.z),
+                         TF(2) * (q.y * q.z - q.x * q.w)},
+                        {TF(2) * (q.x * q.z - q.y * q.w), TF(2) * (q.y * q.z + q.x * q.w),
+                         TF(1) - TF(2) * (q.x * q.x + q.y * q.y)}};
+    const TF tqa[3] = {torque.x, torque.y, torque.z};
+    TF alpha[3];
+    for (int row = 0; row < 3; ++row) {
+      TF sacc = 0;
+      for (int k = 0; k < 3; ++k) {
+        const TF cong = ii.x * m[row][0] * m[k][0] + ii.y * m[row][1] * m[k][1] +
+                        ii.z * m[row][2] * m[k][2];
+        sacc += tqa[k] * cong;
+      }
+      alpha[row] = sacc;
+    }
+    r.omega += vec3<TF>{alpha[0], alpha[1], alpha[2]} * dt;
+    advance_q();
+    const vec3<TF> g{C.pile_gravity[0], C.pile_gravity[1], C.pile_gravity[2]};
+    const vec3<TF> dx = (g * dt + r.v) * dt;
+    r.x += dx;
+    r.v = (TF(1) / dt) * dx;
+  }
+  S.rigid[b] = r;
+}
+
+// ------------------------------------------------------------ host side
+template <class TF>
+struct FluidT;
+template <>
+struct FluidT<float> {
+  using type = al_fluid_f32;
+  using body = al_body_f32;
+  using rigid = al_rigid_f32;
+  using cn = al_const_f32;
+};
+template <>
+struct FluidT<double> {
+  using type = al_fluid_f64;
+  using body = al_body_f64;
+  using rigid = al_rigid_f64;
+  using cn = al_const_f64;
+};
+
+template <class TF>
+int check_step_args(const typename FluidT<TF>::type* f, const al_consti* cni,
+                    const typename FluidT<TF>::body* bodies, const void* rigid,
+                    const al_solver_params* sp, const TF* dt) {
+  ALB_CHECK_ARG(f && cni && sp && dt, "step: null argument");
+  ALB_CHECK_ARG(f->num_particles == 0 || (f->particle_x && f->particle_v),
+                "step: particle_x / particle_v are null");
+  ALB_CHECK_ARG(cni->num_boundaries == 0 || (bodies && rigid), "step: bodies / rigid are null");
+  ALB_CHECK_ARG(cni->num_boundaries <= AL_MAX_BOUNDARIES, "step: too many boundaries");
+  ALB_CHECK_ARG(cni->grid_res[0] > 0 && cni->grid_res[1] > 0 && cni->grid_res[2] > 0,
+                "step: grid_res must be positive");
+  ALB_CHECK_ARG(uint64_t(cni->grid_res[0]) * cni->grid_res[1] * cni->grid_res[2] < (1ull << 31),
+                "step: grid has too many cells");
+  ALB_CHECK_ARG(cni->max_num_neighbors_per_particle > 0, "step: neighbor capacity is 0");
+  ALB_CHECK_ARG(*dt > TF(0), "step: dt must be positive");
+  return AL_OK;
+}
+
+// Reads the loop flag (eager mode: one small readback per iteration).
+template <class TF>
+int read_keep_going(const StepState<TF>& S, uint32_t* pinned, cudaStream_t st, bool* go) {
+  ALB_CUDA(cudaMemcpyAsync(pinned, &S.ctrl->keep_going, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           st));
+  ALB_CUDA(cudaStreamSynchronize(st));
+  *go = *pinned != 0;
+  return AL_OK;
+}
+
+template <class TF>
+int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
+             const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
+             typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
+             al_step_report* report, cudaStream_t st) {
+  ALB_TRY(check_step_args<TF>(f, cni, bodies, rigid, sp, dt));
+  ALB_TRY(e->activate());
+  const Cn<TF> c = to_cn<TF>(*cn);
+  const GridDims g = to_dims(*cni);
+  const uint32_t n = f->num_particles;
+  const uint32_t nb = g.nb;
+  StepState<TF> S;
+  S.n = n;
+  S.nb = nb;
+  S.cap = g.cap_nbr;
+  S.grid = blocks_for(n, kBlock) > 0 ? blocks_for(n, kBlock) : 1;
+  // ---- buffers
+  uint32_t* flags = nullptr;
+  BodyDev<TF>* bodies_dev = nullptr;
+  ALB_TRY(e->buf("flags", 4, &flags));
+  ALB_TRY(e->buf("sorted.x", n, &S.x));
+  ALB_TRY(e->buf("sorted.v", n, &S.v));
+  ALB_TRY(e->buf("sorted.a", n, &S.a));
+  ALB_TRY(e->buf("sorted.rho", n, &S.rho));
+  ALB_TRY(e->buf("sorted.alpha", n, &S.alpha));
+  ALB_TRY(e->buf("sorted.rho_adv", n, &S.rho_adv));
+  ALB_TRY(e->buf("sorted.kappa", n, &S.kappa));
+  ALB_TRY(e->buf("sorted.kappa_v", n, &S.kappa_v));
+  ALB_TRY(e->buf("sorted.kk", n, &S.kk));
+  if (iisph) {
+    ALB_TRY(e->buf("sorted.err", n, &S.err));
+    ALB_TRY(e->buf("sorted.dii", n, &S.dii));
+    ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
+  }
+  ALB_TRY(e->buf("nbr.list", size_t(n) * g.cap_nbr, &S.nbr));
+  ALB_TRY(e->buf("nbr.count", n, &S.ncount));
+  ALB_TRY(e->buf("bnd.mask", n, &S.mask));
+  ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
+  ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
+  ALB_TRY(e->buf("bodies", nb ? nb : 1, &bodies_dev));
+  ALB_TRY(e->buf("rigid", nb ? nb : 1, &S.rigid));
+  ALB_TRY(e->buf("ft", size_t(S.grid) * (nb ? nb : 1) * 6, &S.ft));
+  ALB_TRY(e->buf("red", S.grid, &S.red));
+  ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
+  S.bodies = bodies_dev;
+  // ---- host staging: bodies, rigid state, control block
+  void* pinned = nullptr;
+  const size_t stage_bytes = sizeof(Ctrl<TF>) + (sizeof(BodyDev<TF>) + sizeof(RigidDev<TF>)) *
+                                 AL_MAX_BOUNDARIES + 64;
+  ALB_TRY(e->host_pinned(stage_bytes, &pinned));
+  Ctrl<TF>* hc = reinterpret_cast<Ctrl<TF>*>(pinned);
+  BodyDev<TF>* hb = reinterpret_cast<BodyDev<TF>*>(hc + 1);
+  RigidDev<TF>* hr = reinterpret_cast<RigidDev<TF>*>(hb + AL_MAX_BOUNDARIES);
+  uint32_t* hflag = reinterpret_cast<uint32_t*>(hr + AL_MAX_BOUNDARIES);
+  std::memset(hc, 0, sizeof(Ctrl<TF>));
+  hc->dt = *dt;
+  hc->length_scale = c.radius * TF(2);
+  hc->cfl = TF(sp->cfl);
+  hc->max_dt = TF(sp->max_dt);
+  hc->min_dt = TF(sp->min_dt);
+  hc->tol_div = double(TF(sp->density_change_tolerance));
+  hc->tol_den = double(TF(sp->density_error_tolerance));
+  hc->min_div = sp->min_divergence_solve;
+  hc->max_div = sp->max_divergence_solve;
+  hc->min_den = sp->min_density_solve;
+  hc->max_den = sp->max_density_solve;
+  hc->integrate_rigids = sp->integrate_rigids;
+  for (int k = 0; k < 3; ++k) hc->pile_gravity[k] = TF(sp->pile_gravity[k]);
+  for (uint32_t b = 0; b < nb; ++b) {
+    hb[b] = to_body_dev<TF>(bodies[b]);
+    ALB_TRY(validate_body(hb[b], true, true));
+    hr[b] = to_rigid_dev<TF>(rigid[b]);
+  }
+  ALB_CUDA(cudaMemcpyAsync(S.ctrl, hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
+  if (nb) {
+    ALB_CUDA(cudaMemcpyAsync(bodies_dev, hb, sizeof(BodyDev<TF>) * nb, cudaMemcpyHostToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(S.rigid, hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice, st));
+  }
+  ALB_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), st));
+  ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
+  k_step_init<TF><<<1, 32, 0, st>>>(S);
+  // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
+  GridState gs;
+  ALB_TRY(grid_build<TF>(e, c, g, f->particle_x, n, S.x, flags, gs, st));
+  S.perm = gs.perm;
+  const uint32_t blocks = blocks_for(n, kBlock);
+  if (n > 0) {
+    const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
+    if (iisph)
+      k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref, nullptr);
+    else
+      k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                          f->particle_kappa_v);
+  }
+  BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk};
+  if (nb)
+    ALB_TRY(sample_boundaries<TF>(c, bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
+                                  f->particle_boundary, f->particle_boundary_kernel, st));
+  else if (n)
+    ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
+  SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
+  ALB_TRY(build_neighbors_density<TF>(c, g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+                                      iisph ? nullptr : S.alpha, st));
+  const bool div = !iisph && sp->enable_divergence_solve;
+  const bool den = iisph || sp->enable_density_solve;
+  bool go = false;
+  if (n > 0) {
+    if (div) {
+      k_df_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S);
+      k_kappa<TF, kDivWarm><<<blocks, kBlock, 0, st>>>(c, S);
+      k_df_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S);
+      k_loop_begin<TF><<<1, 1, 0, st>>>(S, 0, 0, 0);
+      go = sp->max_divergence_solve > 0;
+      while (go) {
+        k_kappa<TF, kDivIter><<<blocks, kBlock, 0, st>>>(c, S);
+        k_df_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0);
+        ALB_TRY(read_keep_going(S, hflag, st, &go));
+      }
+    }
+    k_viscosity<TF><<<blocks, kBlock, 0, st>>>(c, S, div ? 1 : 0);
+    if (!iisph) {
+      k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S);
+      if (den) {
+        k_p_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S);
+        k_kappa<TF, kPressWarm><<<blocks, kBlock, 0, st>>>(c, S);
+        k_p_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S);
+        k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0);
+        go = sp->max_density_solve > 0;
+        while (go) {
+          k_kappa<TF, kPressIter><<<blocks, kBlock, 0, st>>>(c, S);
+          k_p_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0);
+          ALB_TRY(read_keep_going(S, hflag, st, &go));
+        }
+      }
+      k_df_finish<TF><<<blocks, kBlock, 0, st>>>(
+          S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+          f->particle_dfsph_factor, f->particle_kappa, f->particle_kappa_v,
+          f->particle_density_adv);
+    } else {
+      k_ii_predict0<TF><<<blocks, kBlock, 0, st>>>(c, S);
+      k_ii_predict1<TF><<<blocks, kBlock, 0, st>>>(c, S);
+      k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0);
+      go = sp->max_density_solve > 0;
+      while (go) {
+        k_ii_iter0<TF><<<blocks, kBlock, 0, st>>>(c, S);
+        k_ii_iter1<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0);
+        ALB_TRY(read_keep_going(S, hflag, st, &go));
+      }
+      k_ii_accel_finish<TF><<<blocks, kBlock, 0, st>>>(
+          c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+          f->particle_pressure, f->particle_density_adv);
+    }
+  }
+  if (nb) k_rigid_finish<TF><<<nb, 256, 0, st>>>(S);
+  ALB_CUDA(cudaGetLastError());
+  // ---- read back: report, rigid state, anomaly flags
+  uint32_t hf[4];
+  ALB_CUDA(cudaMemcpyAsync(hc, S.ctrl, sizeof(Ctrl<TF>), cudaMemcpyDeviceToHost, st));
+  if (nb)
+    ALB_CUDA(cudaMemcpyAsync(hr, S.rigid, sizeof(RigidDev<TF>) * nb, cudaMemcpyDeviceToHost, st));
+  ALB_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+  ALB_CUDA(cudaStreamSynchronize(st));
+  al_step_report rep = hc->rep;
+  for (int k = 0; k < 3; ++k) rep.grid_anomaly[k] = hf[k];
+  if (n == 0) rep.dt = double(*dt);
+  *dt = TF(rep.dt);
+  for (uint32_t b = 0; b < nb; ++b) {
+    for (int k = 0; k < 3; ++k) {
+      rigid[b].x[k] = (&hr[b].x.x)[k];
+      rigid[b].v[k] = (&hr[b].v.x)[k];
+      rigid[b].omega[k] = (&hr[b].omega.x)[k];
+    }
+    rigid[b].q[0] = hr[b].q.x;
+    rigid[b].q[1] = hr[b].q.y;
+    rigid[b].q[2] = hr[b].q.z;
+    rigid[b].q[3] = hr[b].q.w;
+  }
+  if (report) *report = rep;
+  if (hf[0]) return AL_ERR_OUT_OF_GRID;
+  if (hf[1]) return AL_ERR_CELL_OVERFLOW;
+  if (hf[2]) return AL_ERR_NEIGHBOR_OVERFLOW;
+  return AL_OK;
+}
+
+}  // namespace
+
+}  // namespace alb
+
+using namespace alb;
+
+extern "C" {
+
+int al_df_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                   const al_fluid_f32* fluid, const al_body_f32* bodies, al_rigid_f32* rigid,
+                   const al_solver_params* params, float* dt, al_step_report* report,
+                   void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_df_step: null argument");
+  return run_step<float>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
+                         static_cast<cudaStream_t>(stream));
+}
+int al_df_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                   const al_fluid_f64* fluid, const al_body_f64* bodies, al_rigid_f64* rigid,
+                   const al_solver_params* params, double* dt, al_step_report* report,
+                   void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_df_step: null argument");
+  return run_step<double>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
+                          static_cast<cudaStream_t>(stream));
+}
+int al_ii_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                   const al_fluid_f32* fluid, const al_body_f32* bodies, al_rigid_f32* rigid,
+                   const al_solver_params* params, float* dt, al_step_report* report,
+                   void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_ii_step: null argument");
+  return run_step<float>(engine, true, cn, cni, fluid, bodies, rigid, params, dt, report,
+                         static_cast<cudaStream_t>(stream));
+}
+int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                   const al_fluid_f64* fluid, const al_body_f64* bodies, al_rigid_f64* rigid,
+                   const al_solver_params* params, double* dt, al_step_report* report,
+                   void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_ii_step: null argument");
+  return run_step<double>(engine, true, cn, cni, fluid, bodies, rigid, params, dt, report,
+                          static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

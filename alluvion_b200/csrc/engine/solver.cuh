@@ -1,0 +1,76 @@
+// solver.cuh -- DFSPH and IISPH steps over the cell-sorted particle state.
+//
+// Replaces SolverDf<TF>::step<0> (solver_df.hpp:74-359) and
+// SolverIi<TF>::step<0> (solver_ii.hpp:76-243) with the kernels they launch
+// (runner.hpp:1974-2249, 2533-2541, 2609-2887, 3123-3623) and the rigid
+// force/torque sums and Pile::integrate_kinematics (pile.hpp:794-815).
+//
+// Differences in mechanism (same arithmetic per particle):
+//  * all passes run on cell-sorted state (gathered once per step, scattered
+//    back to the caller's buffers at the end);
+//  * the solvers' convergence means are reduced on the device in double,
+//    deterministically (fixed block partition, fixed summation order), and
+//    the loop decision is taken on the device; the host reads one flag per
+//    iteration (eager mode) or nothing at all (graph mode);
+//  * rigid force/torque contributions are reduced per block into per-block
+//    slots (no atomics) and summed per body in double at the end of the
+//    step; per-particle [nb][N] force arrays are not materialised.
+#pragma once
+
+#include "boundary.cuh"
+#include "common.cuh"
+#include "engine.hpp"
+#include "grid.cuh"
+
+namespace alb {
+
+// Device control block of one step.
+template <class TF>
+struct Ctrl {
+  TF dt;            // time step in use by the kernels
+  TF length_scale;  // 2 r
+  TF cfl, max_dt, min_dt;
+  TF pad0;
+  double tol_div;   // density_change_tolerance
+  double tol_den;   // density_error_tolerance
+  uint32_t min_div, max_div, min_den, max_den;
+  uint32_t it;          // iterations done by the running solve
+  uint32_t keep_going;  // 1 while the running solve must iterate again
+  uint32_t ticket;      // last-block ticket of grid reductions
+  uint32_t integrate_rigids;
+  double mean;          // latest mean of the running solve
+  unsigned long long vmax_bits;  // max |v + a dt|^2 as ordered bits
+  TF pile_gravity[3];
+  TF pad1;
+  al_step_report rep;
+};
+
+template <class TF>
+struct StepState {
+  uint32_t n = 0, nb = 0, cap = 0, grid = 0;
+  vec4<TF>* x = nullptr;
+  vec4<TF>* v = nullptr;
+  vec4<TF>* a = nullptr;
+  TF* rho = nullptr;
+  TF* alpha = nullptr;
+  TF* rho_adv = nullptr;
+  TF* kappa = nullptr;    // DFSPH kappa, IISPH pressure
+  TF* kappa_v = nullptr;  // DFSPH kappa_v, IISPH last pressure
+  TF* kk = nullptr;       // per-iteration k = b * alpha (DFSPH), aii (IISPH)
+  TF* err = nullptr;      // IISPH density error
+  vec4<TF>* dii = nullptr;
+  vec4<TF>* dij_pj = nullptr;
+  uint32_t* nbr = nullptr;
+  uint32_t* ncount = nullptr;
+  uint32_t* mask = nullptr;
+  vec4<TF>* bx = nullptr;
+  vec4<TF>* bk = nullptr;
+  const BodyDev<TF>* bodies = nullptr;
+  RigidDev<TF>* rigid = nullptr;
+  double* ft = nullptr;   // [grid][nb][6] rigid force/torque partials
+  double* red = nullptr;  // [grid] reduction partials
+  Ctrl<TF>* ctrl = nullptr;
+  const uint32_t* perm = nullptr;
+};
+
+}  // namespace alb

@@ -198,6 +198,197 @@ def rigid_array(dtype, states):
     return out
 
 
+def sphere_inertia(mass, radius):
+    i = 0.4 * mass * radius * radius
+    return (i, i, i)
+
+
+def box_inertia(mass, widths):
+    wx, wy, wz = widths
+    return (mass * (wy * wy + wz * wz) / 12, mass * (wx * wx + wz * wz) / 12,
+            mass * (wx * wx + wy * wy) / 12)
+
+
+class DeviceScene:
+    """A seeded scene held on one CUDA device: constants, grid dimensions,
+    bodies with device-built distance grids and volume maps, and the
+    reference-layout particle buffers.  Steps go through the C ABI.
+
+    bodies: list of dicts with keys shape, params, sign, resolution,
+    use_distance_grid, mass, inertia, x, q (optional v, omega, margin).
+    """
+
+    def __init__(self, engine, dtype, cn, cni, x, bodies=(), device="cuda",
+                 pile_gravity=(0.0, -9.81, 0.0)):
+        import torch
+        self.torch = torch
+        self.engine = engine
+        self.dtype = np.dtype(dtype)
+        self.tdtype = torch.float32 if self.dtype == np.float32 else torch.float64
+        self.sfx = _capi.suffix(dtype)
+        self.cn = cn
+        self.cni = cni
+        self.device = device
+        self.n = int(x.shape[0])
+        zeros = lambda *s: torch.zeros(*s, dtype=self.tdtype, device=device)
+        self.x = torch.from_numpy(np.ascontiguousarray(x, dtype=self.dtype)).to(device)
+        self.v = zeros(self.n, 3)
+        self.a = zeros(self.n, 3)
+        self.density = zeros(self.n)
+        self.dfsph_factor = zeros(self.n)
+        self.kappa = zeros(self.n)
+        self.kappa_v = zeros(self.n)
+        self.density_adv = zeros(self.n)
+        self.pressure = zeros(self.n)
+        self.pile_gravity = pile_gravity
+        self.body_specs = list(bodies)
+        self.distance_nodes = []
+        self.volume_nodes = []
+        _, BodyT, RigidT, _ = _capi.real_types(dtype)
+        nb = len(self.body_specs)
+        self.bodies = (BodyT * max(nb, 1))()
+        self.rigid = (RigidT * max(nb, 1))()
+        for b, spec in enumerate(self.body_specs):
+            body = make_body(dtype, cn, spec["shape"], spec["params"], spec["resolution"],
+                             sign=spec.get("sign", 1.0), margin=spec.get("margin"),
+                             use_distance_grid=spec.get("use_distance_grid", False),
+                             mass=spec.get("mass", 0.0), inertia=spec.get("inertia", (1, 1, 1)))
+            dist = zeros(body.num_nodes) if body.use_distance_grid else None
+            vol = zeros(body.num_nodes)
+            if dist is not None:
+                body.distance_nodes = dist.data_ptr()
+                _capi.check(getattr(_capi.lib(), "al_build_distance_grid_" + self.sfx)(
+                    engine.handle, _capi.ptr(body), _capi.ptr(dist), None),
+                    "al_build_distance_grid")
+            body.volume_nodes = vol.data_ptr()
+            _capi.check(getattr(_capi.lib(), "al_build_volume_field_" + self.sfx)(
+                engine.handle, _capi.ptr(cn), _capi.ptr(body), _capi.ptr(vol), None),
+                "al_build_volume_field")
+            self.bodies[b] = body
+            self.distance_nodes.append(dist)
+            self.volume_nodes.append(vol)
+            self.rigid[b] = rigid_state(dtype, x=spec.get("x", (0, 0, 0)),
+                                        v=spec.get("v", (0, 0, 0)),
+                                        q=spec.get("q", (0, 0, 0, 1)),
+                                        omega=spec.get("omega", (0, 0, 0)))
+        self.cni.num_boundaries = nb
+        torch.cuda.synchronize()
+
+    @property
+    def num_boundaries(self):
+        return len(self.body_specs)
+
+    def fluid(self, export_boundary=None):
+        bufs = dict(particle_x=self.x, particle_v=self.v, particle_a=self.a,
+                    particle_density=self.density, particle_dfsph_factor=self.dfsph_factor,
+                    particle_kappa=self.kappa, particle_kappa_v=self.kappa_v,
+                    particle_density_adv=self.density_adv, particle_pressure=self.pressure)
+        if export_boundary is not None:
+            bufs["particle_boundary"], bufs["particle_boundary_kernel"] = export_boundary
+        return _capi.make_fluid(self.n, **bufs)
+
+    def step(self, method, sp, dt, report=None, stream=None, allow=()):
+        """One DFSPH ('df') or IISPH ('ii') step; returns (dt_out, report)."""
+        T = self.dtype.type
+        dt_c = (ctypes_real(self.dtype))(T(dt))
+        rep = report if report is not None else _capi.StepReport()
+        fluid = self.fluid()
+        fn = getattr(_capi.lib(), "al_%s_step_%s" % (method, self.sfx))
+        status = fn(self.engine.handle, _capi.ptr(self.cn), _capi.ptr(self.cni), _capi.ptr(fluid),
+                    _capi.ptr(self.bodies) if self.num_boundaries else None,
+                    _capi.ptr(self.rigid) if self.num_boundaries else None,
+                    _capi.ptr(sp), _capi.ptr(dt_c), _capi.ptr(rep), stream)
+        _capi.check(status, "al_%s_step" % method, allow=allow)
+        return float(dt_c.value), rep
+
+    def host_bodies(self):
+        """(bodies with HOST node pointers, keep-alive arrays, rigid (nb,13))
+        for CPU consumers of the same grids."""
+        _, BodyT, _, _ = _capi.real_types(self.dtype)
+        nb = self.num_boundaries
+        hb = (BodyT * max(nb, 1))()
+        keep = []
+        for b in range(nb):
+            src = self.bodies[b]
+            ctypes_copy(hb, b, src)
+            vol = self.volume_nodes[b].cpu().numpy()
+            keep.append(vol)
+            hb[b].volume_nodes = vol.ctypes.data
+            if self.distance_nodes[b] is not None:
+                dist = self.distance_nodes[b].cpu().numpy()
+                keep.append(dist)
+                hb[b].distance_nodes = dist.ctypes.data
+        rigid = rigid_array(self.dtype, [self.rigid[b] for b in range(nb)])
+        return hb, keep, rigid
+
+    def state(self):
+        """Host copies of the particle state."""
+        g = lambda t: t.cpu().numpy()
+        return {"x": g(self.x), "v": g(self.v), "a": g(self.a), "density": g(self.density),
+                "kappa": g(self.kappa), "kappa_v": g(self.kappa_v),
+                "density_adv": g(self.density_adv), "pressure": g(self.pressure),
+                "dfsph_factor": g(self.dfsph_factor)}
+
+
+def ctypes_real(dtype):
+    import ctypes
+    return ctypes.c_float if np.dtype(dtype) == np.float32 else ctypes.c_double
+
+
+def ctypes_copy(dst_array, index, src):
+    import ctypes
+    ctypes.memmove(ctypes.addressof(dst_array) + index * ctypes.sizeof(src),
+                   ctypes.addressof(src), ctypes.sizeof(src))
+
+
+def dam_break(engine, dtype, lattice, particle_radius, container, bodies=(), seed=0,
+              volume_resolution=64, jitter=0.1, max_num_particles_per_cell=64,
+              max_num_neighbors_per_particle=64, **const_kw):
+    """Dam break: a jittered lattice block in the low corner of a box
+    container (analytic box distance, sign -1, fluid inside) centred at
+    container/2, plus extra bodies.  Returns a DeviceScene."""
+    cn = make_const(dtype, particle_radius, **const_kw)
+    box_min = (0.0, 0.0, 0.0)
+    x = fluid_block(lattice, box_min, particle_radius, dtype, jitter=jitter, seed=seed)
+    size = np.asarray(container, dtype=np.float64)
+    cont = dict(shape=_capi.SHAPE_BOX, params=box_params(size), sign=-1.0,
+                resolution=volume_resolution, use_distance_grid=False, mass=0.0,
+                x=tuple(size / 2))
+    all_bodies = [cont] + list(bodies)
+    h = float(cn.kernel_radius)
+    cni = make_consti(-0.5 * h * np.ones(3), size + 0.5 * h, h, len(all_bodies),
+                      max_num_particles_per_cell, max_num_neighbors_per_particle)
+    return DeviceScene(engine, dtype, cn, cni, x, all_bodies)
+
+
+def seeded_rigid_bodies(seed, container, particle_radius, spheres=2, boxes=2,
+                        sphere_radius=0.05, box_side=0.08, resolution=64,
+                        y_range=(0.7, 0.9), density_range=(500.0, 2000.0)):
+    """Rigid spheres and boxes at seeded positions above the fluid block,
+    densities uniform in density_range, analytic mass and inertia, sampled
+    onto cubic-Lagrange distance grids (use_distance_grid)."""
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    size = np.asarray(container, dtype=np.float64)
+    out = []
+    for k in range(spheres + boxes):
+        rho = rng.uniform(*density_range)
+        pos = (rng.uniform(0.2, 0.8) * size[0], rng.uniform(*y_range) * size[1],
+               rng.uniform(0.2, 0.8) * size[2])
+        if k < spheres:
+            r = sphere_radius
+            mass = rho * 4.0 / 3.0 * PI * r ** 3
+            out.append(dict(shape=_capi.SHAPE_SPHERE, params=[r], sign=1.0,
+                            resolution=resolution, use_distance_grid=True, mass=mass,
+                            inertia=sphere_inertia(mass, r), x=pos))
+        else:
+            w = (box_side,) * 3
+            mass = rho * box_side ** 3
+            out.append(dict(shape=_capi.SHAPE_BOX, params=box_params(w), sign=1.0,
+                            resolution=resolution, use_distance_grid=True, mass=mass,
+                            inertia=box_inertia(mass, w), x=pos))
+    return out
+
+
 def solver_params(**kw):
     """al_solver_params with the reference defaults (solver_df.hpp:60-67) and
     the benchmark's cfl 0.4, max_dt 2e-4."""

@@ -285,6 +285,118 @@ AL_API int al_update_particle_neighbors_f64(
     uint32_t* particle_num_neighbors, double* particle_neighbors,
     uint32_t* grid_anomaly, void* stream);
 
+/* ------------------------------------------------------ boundary sampling
+ * compute_all_boundaries (solver.hpp:170-185): for every body b and
+ * particle i, {x_b, V} into particle_boundary[b][i] and
+ * {grad W(x_i - x_b) V, W(d) V} into particle_boundary_kernel[b][i]
+ * (compute_particle_boundary / _analytic<0>, runner.hpp:1982-2025).
+ *   bodies  host array [num_boundaries]; node arrays are device pointers
+ *   rigid   host array [num_boundaries] (pose at this step) */
+AL_API int al_compute_particle_boundary_f32(
+    al_engine* engine, const al_const_f32* cn, uint32_t num_boundaries,
+    const al_body_f32* bodies, const al_rigid_f32* rigid, const float* particle_x,
+    uint32_t num_particles, float* particle_boundary, float* particle_boundary_kernel,
+    void* stream);
+AL_API int al_compute_particle_boundary_f64(
+    al_engine* engine, const al_const_f64* cn, uint32_t num_boundaries,
+    const al_body_f64* bodies, const al_rigid_f64* rigid, const double* particle_x,
+    uint32_t num_particles, double* particle_boundary, double* particle_boundary_kernel,
+    void* stream);
+
+/* Volume-map nodes of one body (update_volume_field, runner.hpp:1616-1694,
+ * launched by Pile::build_grid, pile.hpp:523-622): Peirce m = 14 ball
+ * quadrature (27,000 samples per node) of the body's distance -- from
+ * body->distance_nodes when use_distance_grid, else the analytic shape.
+ * volume_nodes: device [body->num_nodes] out. */
+AL_API int al_build_volume_field_f32(al_engine* engine, const al_const_f32* cn,
+                                     const al_body_f32* body, float* volume_nodes,
+                                     void* stream);
+AL_API int al_build_volume_field_f64(al_engine* engine, const al_const_f64* cn,
+                                     const al_body_f64* body, double* volume_nodes,
+                                     void* stream);
+
+/* Distance nodes sampled from the body's analytic shape at the Lagrange
+ * node positions -- the role of Pile::construct_distance_grid
+ * (pile.hpp:79-94) for mesh bodies.  distance_nodes: device out. */
+AL_API int al_build_distance_grid_f32(al_engine* engine, const al_body_f32* body,
+                                      float* distance_nodes, void* stream);
+AL_API int al_build_distance_grid_f64(al_engine* engine, const al_body_f64* body,
+                                      double* distance_nodes, void* stream);
+
+/* Node positions of the body's grid (index_to_node_position,
+ * runner.hpp:1131-1178).  positions: device [num_nodes][3] out. */
+AL_API int al_node_positions_f32(al_engine* engine, const al_body_f32* body, float* positions,
+                                 void* stream);
+AL_API int al_node_positions_f64(al_engine* engine, const al_body_f64* body, double* positions,
+                                 void* stream);
+
+/* ------------------------------------------------------------ fluid steps
+ * The caller-owned particle buffers of one solver (solver.hpp:286-305,
+ * solver_df.hpp:367-370, solver_ii.hpp:250-257).  Required: particle_x,
+ * particle_v.  Every other pointer may be NULL (not read / not written).
+ *   in/out: particle_x, particle_v, particle_kappa, particle_kappa_v
+ *           (DFSPH warm-start state), particle_pressure (IISPH)
+ *   out:    particle_a (non-pressure acceleration), particle_density,
+ *           particle_dfsph_factor, particle_density_adv,
+ *           particle_boundary / particle_boundary_kernel ([nb][N][4]) */
+typedef struct al_fluid_f32 {
+  uint32_t num_particles;
+  uint32_t reserved;
+  float* particle_x;
+  float* particle_v;
+  float* particle_a;
+  float* particle_density;
+  float* particle_dfsph_factor;
+  float* particle_kappa;
+  float* particle_kappa_v;
+  float* particle_density_adv;
+  float* particle_pressure;
+  float* particle_boundary;
+  float* particle_boundary_kernel;
+} al_fluid_f32;
+
+typedef struct al_fluid_f64 {
+  uint32_t num_particles;
+  uint32_t reserved;
+  double* particle_x;
+  double* particle_v;
+  double* particle_a;
+  double* particle_density;
+  double* particle_dfsph_factor;
+  double* particle_kappa;
+  double* particle_kappa_v;
+  double* particle_density_adv;
+  double* particle_pressure;
+  double* particle_boundary;
+  double* particle_boundary_kernel;
+} al_fluid_f64;
+
+/* One DFSPH step: SolverDf<TF>::step<0> (solver_df.hpp:74-359) without
+ * contacts (pile.hpp:826-979).  bodies: host [num_boundaries]; rigid: host
+ * [num_boundaries] in/out (integrated when params->integrate_rigids);
+ * dt: host in/out (in: step's initial dt, out: dt after update_dt);
+ * report: host out, may be NULL.  Synchronous: returns after the step has
+ * completed on `stream`. */
+AL_API int al_df_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                          const al_fluid_f32* fluid, const al_body_f32* bodies,
+                          al_rigid_f32* rigid, const al_solver_params* params, float* dt,
+                          al_step_report* report, void* stream);
+AL_API int al_df_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                          const al_fluid_f64* fluid, const al_body_f64* bodies,
+                          al_rigid_f64* rigid, const al_solver_params* params, double* dt,
+                          al_step_report* report, void* stream);
+
+/* One IISPH step: SolverIi<TF>::step<0> (solver_ii.hpp:76-243) without
+ * contacts.  Same conventions as al_df_step; uses particle_pressure. */
+AL_API int al_ii_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                          const al_fluid_f32* fluid, const al_body_f32* bodies,
+                          al_rigid_f32* rigid, const al_solver_params* params, float* dt,
+                          al_step_report* report, void* stream);
+AL_API int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                          const al_fluid_f64* fluid, const al_body_f64* bodies,
+                          al_rigid_f64* rigid, const al_solver_params* params, double* dt,
+                          al_step_report* report, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
