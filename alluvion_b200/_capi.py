@@ -162,6 +162,10 @@ _SIGNATURES = {
     "al_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "al_last_error": (ctypes.c_char_p, []),
     "al_engine_synchronize": (ctypes.c_int, [_P, _P]),
+    "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
+    "al_engine_reset_stats": (ctypes.c_int, [_P]),
+    "al_engine_launch_count": (ctypes.c_int, [_P, _P]),
+    "al_engine_kernel_stat": (ctypes.c_int, [_P, _U, ctypes.c_char_p, ctypes.c_size_t, _P, _P]),
 }
 for _s in ("f32", "f64"):
     _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])
@@ -235,12 +239,36 @@ class Engine:
     def synchronize(self, stream=None):
         check(lib().al_engine_synchronize(self.handle, stream), "al_engine_synchronize")
 
+    def set_profiling(self, enable):
+        check(lib().al_engine_set_profiling(self.handle, int(bool(enable))), "set_profiling")
+
+    def reset_stats(self):
+        check(lib().al_engine_reset_stats(self.handle), "al_engine_reset_stats")
+
+    def launch_count(self):
+        c = ctypes.c_uint64()
+        check(lib().al_engine_launch_count(self.handle, ctypes.byref(c)), "launch_count")
+        return c.value
+
+    def kernel_stats(self):
+        """{launch group name: (total_ms, count)} recorded while profiling."""
+        out = {}
+        buf = ctypes.create_string_buffer(128)
+        ms = ctypes.c_double()
+        cnt = ctypes.c_uint64()
+        i = 0
+        while lib().al_engine_kernel_stat(self.handle, i, buf, 128, ctypes.byref(ms),
+                                          ctypes.byref(cnt)) == AL_OK:
+            out[buf.value.decode()] = (ms.value, cnt.value)
+            i += 1
+        return out
+
 
 def ptr(t):
     """Address of a torch tensor, numpy array or ctypes object (None -> NULL)."""
     if t is None:
         return None
-    if isinstance(t, (ctypes.Structure, ctypes.Array)):
+    if isinstance(t, (ctypes.Structure, ctypes.Array, ctypes._SimpleCData)):
         return ctypes.cast(ctypes.pointer(t), ctypes.c_void_p)
     if hasattr(t, "data_ptr"):
         return ctypes.c_void_p(t.data_ptr())

@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kBlock)
                         const vec4<TF>* __restrict__ xs, const uint32_t* __restrict__ perm,
                         uint32_t n, uint32_t* __restrict__ mask, vec4<TF>* __restrict__ bx,
                         vec4<TF>* __restrict__ bk, TF* __restrict__ ref_b,
-                        TF* __restrict__ ref_k) {
+                        TF* __restrict__ ref_k, uint32_t* __restrict__ active) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const vec3<TF> x = xyz(xs[s]);
@@ -313,6 +313,12 @@ __global__ void __launch_bounds__(kBlock)
     }
   }
   if (mask) mask[s] = m;
+  if (active) {
+    // warp-aggregated count of active (particle, body) pairs
+    const unsigned live = __activemask();
+    const unsigned tot = __reduce_add_sync(live, unsigned(__popc(m)));
+    if ((threadIdx.x & 31) == unsigned(__ffs(live) - 1) && tot) atomicAdd(active, tot);
+  }
 }
 
 // index_to_node_position (runner.hpp:1131-1178).
@@ -437,7 +443,8 @@ int sample_boundaries(const Cn<TF>& c, const BodyDev<TF>* bodies_dev, const Rigi
                       cudaStream_t st) {
   if (n == 0) return AL_OK;
   k_sample_boundaries<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(
-      c, bodies_dev, rigid_dev, nb, xs, perm, n, bs.mask, bs.bx, bs.bk, ref_boundary, ref_kernel);
+      c, bodies_dev, rigid_dev, nb, xs, perm, n, bs.mask, bs.bx, bs.bk, ref_boundary, ref_kernel,
+      bs.active);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }

@@ -90,6 +90,7 @@ struct BoundaryState {
   uint32_t* mask = nullptr;  // [n] bit b set: V_b != 0
   vec4<TF>* bx = nullptr;    // [nb][n] {x_b, V}
   vec4<TF>* bk = nullptr;    // [nb][n] {grad W * V, W * V}
+  uint32_t* active = nullptr;  // optional counter += number of set mask bits
 };
 
 // Samples every body for every sorted particle (positions xs).  When

@@ -56,11 +56,66 @@ int al_engine::host_pinned(size_t bytes, void** out) {
   return AL_OK;
 }
 
+cudaEvent_t al_engine::take_event() {
+  if (!event_pool.empty()) {
+    cudaEvent_t ev = event_pool.back();
+    event_pool.pop_back();
+    return ev;
+  }
+  cudaEvent_t ev = nullptr;
+  if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+  return ev;
+}
+
+int al_engine::flush_stats() {
+  for (Pending& p : pending) {
+    float ms = 0;
+    cudaError_t err = cudaEventElapsedTime(&ms, p.start, p.stop);
+    event_pool.push_back(p.start);
+    event_pool.push_back(p.stop);
+    if (err != cudaSuccess) continue;
+    Stat* s = nullptr;
+    for (auto& kv : stats)
+      if (kv.first == p.name) s = &kv.second;
+    if (!s) {
+      stats.emplace_back(p.name, Stat{});
+      s = &stats.back().second;
+    }
+    s->total_ms += ms;
+    s->count += 1;
+  }
+  pending.clear();
+  return AL_OK;
+}
+
+namespace alb {
+LaunchScope::LaunchScope(al_engine* e_, const char* name_, cudaStream_t st_, int kernels)
+    : e(e_), name(name_), st(st_) {
+  e->launches += uint64_t(kernels);
+  if (e->profiling) {
+    start = e->take_event();
+    if (start) cudaEventRecord(start, st);
+  }
+}
+LaunchScope::~LaunchScope() {
+  if (!start) return;
+  cudaEvent_t stop = e->take_event();
+  if (!stop) return;
+  cudaEventRecord(stop, st);
+  e->pending.push_back(al_engine::Pending{name, start, stop});
+}
+}  // namespace alb
+
 al_engine::~al_engine() {
   cudaSetDevice(device);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);
+  for (Pending& p : pending) {
+    cudaEventDestroy(p.start);
+    cudaEventDestroy(p.stop);
+  }
+  for (cudaEvent_t ev : event_pool) cudaEventDestroy(ev);
 }
 
 extern "C" {
@@ -118,6 +173,44 @@ int al_engine_synchronize(al_engine* engine, void* stream) {
   ALB_CHECK_ARG(engine != nullptr, "al_engine_synchronize: engine is null");
   ALB_TRY(engine->activate());
   ALB_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  return engine->flush_stats();
+}
+
+int al_engine_set_profiling(al_engine* engine, int enable) {
+  ALB_CHECK_ARG(engine != nullptr, "al_engine_set_profiling: engine is null");
+  engine->profiling = enable != 0;
+  return AL_OK;
+}
+
+int al_engine_reset_stats(al_engine* engine) {
+  ALB_CHECK_ARG(engine != nullptr, "al_engine_reset_stats: engine is null");
+  ALB_TRY(engine->activate());
+  ALB_CUDA(cudaDeviceSynchronize());
+  engine->flush_stats();
+  engine->stats.clear();
+  engine->launches = 0;
+  return AL_OK;
+}
+
+int al_engine_launch_count(al_engine* engine, uint64_t* count) {
+  ALB_CHECK_ARG(engine && count, "al_engine_launch_count: null argument");
+  *count = engine->launches;
+  return AL_OK;
+}
+
+int al_engine_kernel_stat(al_engine* engine, uint32_t index, char* name, size_t name_len,
+                          double* total_ms, uint64_t* count) {
+  ALB_CHECK_ARG(engine && name && name_len && total_ms && count,
+                "al_engine_kernel_stat: null argument");
+  engine->flush_stats();
+  if (index >= engine->stats.size()) {
+    set_error("al_engine_kernel_stat: index past the last entry");
+    return AL_ERR_INVALID;
+  }
+  const auto& kv = engine->stats[index];
+  std::snprintf(name, name_len, "%s", kv.first.c_str());
+  *total_ms = kv.second.total_ms;
+  *count = kv.second.count;
   return AL_OK;
 }
 

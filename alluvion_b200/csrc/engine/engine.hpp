@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <string>
 #include <unordered_map>
+#include <utility>
+#include <vector>
 
 #include "alluvion_b200.h"
 
@@ -52,10 +54,48 @@ struct Scratch {
 
 }  // namespace alb
 
+struct al_engine;
+
+namespace alb {
+// Records one named launch group (`kernels` launches) on `st`: counts the
+// launches and, while profiling is on, brackets them with CUDA events.
+struct LaunchScope {
+  al_engine* e;
+  const char* name;
+  cudaStream_t st;
+  cudaEvent_t start = nullptr;
+  LaunchScope(al_engine* e_, const char* name_, cudaStream_t st_, int kernels);
+  ~LaunchScope();
+};
+}  // namespace alb
+
+#define ALB_LAUNCH(eng, name, nk, st, ...)           \
+  do {                                               \
+    ::alb::LaunchScope ls_((eng), (name), (st), (nk)); \
+    __VA_ARGS__;                                     \
+  } while (0)
+
 struct al_engine {
   int device = 0;
   int num_sms = 0;
   std::unordered_map<std::string, alb::Scratch> scratch;
+  // launch statistics (al_engine_set_profiling / al_engine_kernel_stat)
+  struct Stat {
+    double total_ms = 0;
+    uint64_t count = 0;
+  };
+  bool profiling = false;
+  uint64_t launches = 0;
+  std::vector<std::pair<std::string, Stat>> stats;  // insertion order
+  struct Pending {
+    const char* name;
+    cudaEvent_t start, stop;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
+  cudaEvent_t take_event();
+  // Accumulates the elapsed times of recorded launches (after a sync).
+  int flush_stats();
   // pinned host staging (control readback, reports)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

@@ -861,80 +861,99 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   }
   ALB_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), st));
   ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
-  k_step_init<TF><<<1, 32, 0, st>>>(S);
+  ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
   // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
   GridState gs;
-  ALB_TRY(grid_build<TF>(e, c, g, f->particle_x, n, S.x, flags, gs, st));
+  ALB_LAUNCH(e, "grid_sort", 7, st,
+             ALB_TRY(grid_build<TF>(e, c, g, f->particle_x, n, S.x, flags, gs, st)));
   S.perm = gs.perm;
   const uint32_t blocks = blocks_for(n, kBlock);
   if (n > 0) {
     const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
     if (iisph)
-      k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref, nullptr);
+      ALB_LAUNCH(e, "gather_state", 1, st,
+                 k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                                      nullptr));
     else
-      k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
-                                                          f->particle_kappa_v);
+      ALB_LAUNCH(e, "gather_state", 1, st,
+                 k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                                     f->particle_kappa_v));
   }
-  BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk};
+  BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk, &S.ctrl->rep.num_active_boundary_pairs};
   if (nb)
-    ALB_TRY(sample_boundaries<TF>(c, bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
-                                  f->particle_boundary, f->particle_boundary_kernel, st));
+    ALB_LAUNCH(e, "boundary", 1, st,
+               ALB_TRY(sample_boundaries<TF>(c, bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
+                                             f->particle_boundary, f->particle_boundary_kernel,
+                                             st)));
   else if (n)
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
-  ALB_TRY(build_neighbors_density<TF>(c, g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
-                                      iisph ? nullptr : S.alpha, st));
+  ALB_LAUNCH(e, "neighbors", 1, st,
+             ALB_TRY(build_neighbors_density<TF>(c, g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+                                                 iisph ? nullptr : S.alpha, st)));
   const bool div = !iisph && sp->enable_divergence_solve;
   const bool den = iisph || sp->enable_density_solve;
   bool go = false;
   if (n > 0) {
     if (div) {
-      k_df_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S);
-      k_kappa<TF, kDivWarm><<<blocks, kBlock, 0, st>>>(c, S);
-      k_df_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S);
-      k_loop_begin<TF><<<1, 1, 0, st>>>(S, 0, 0, 0);
+      ALB_LAUNCH(e, "div_warm0", 1, st, k_df_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "div_warm1", 1, st,
+                 k_kappa<TF, kDivWarm><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "div_rho_adv", 1, st,
+                 k_df_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 0, 0, 0));
       go = sp->max_divergence_solve > 0;
       while (go) {
-        k_kappa<TF, kDivIter><<<blocks, kBlock, 0, st>>>(c, S);
-        k_df_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0);
+        ALB_LAUNCH(e, "div_iter", 1, st,
+                   k_kappa<TF, kDivIter><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "div_residual", 1, st,
+                   k_df_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0));
         ALB_TRY(read_keep_going(S, hflag, st, &go));
       }
     }
-    k_viscosity<TF><<<blocks, kBlock, 0, st>>>(c, S, div ? 1 : 0);
+    ALB_LAUNCH(e, "viscosity", 1, st,
+               k_viscosity<TF><<<blocks, kBlock, 0, st>>>(c, S, div ? 1 : 0));
     if (!iisph) {
-      k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S);
+      ALB_LAUNCH(e, "integrate_np", 1, st, k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S));
       if (den) {
-        k_p_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S);
-        k_kappa<TF, kPressWarm><<<blocks, kBlock, 0, st>>>(c, S);
-        k_p_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S);
-        k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0);
+        ALB_LAUNCH(e, "press_warm0", 1, st, k_p_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "press_warm1", 1, st,
+                   k_kappa<TF, kPressWarm><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "press_rho_adv", 1, st,
+                   k_p_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0));
         go = sp->max_density_solve > 0;
         while (go) {
-          k_kappa<TF, kPressIter><<<blocks, kBlock, 0, st>>>(c, S);
-          k_p_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0);
+          ALB_LAUNCH(e, "press_iter", 1, st,
+                     k_kappa<TF, kPressIter><<<blocks, kBlock, 0, st>>>(c, S));
+          ALB_LAUNCH(e, "press_residual", 1, st,
+                     k_p_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0));
           ALB_TRY(read_keep_going(S, hflag, st, &go));
         }
       }
-      k_df_finish<TF><<<blocks, kBlock, 0, st>>>(
-          S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-          f->particle_dfsph_factor, f->particle_kappa, f->particle_kappa_v,
-          f->particle_density_adv);
+      ALB_LAUNCH(e, "finish", 1, st,
+                 k_df_finish<TF><<<blocks, kBlock, 0, st>>>(
+                     S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                     f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
+                     f->particle_kappa_v, f->particle_density_adv));
     } else {
-      k_ii_predict0<TF><<<blocks, kBlock, 0, st>>>(c, S);
-      k_ii_predict1<TF><<<blocks, kBlock, 0, st>>>(c, S);
-      k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0);
+      ALB_LAUNCH(e, "ii_predict0", 1, st, k_ii_predict0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "ii_predict1", 1, st, k_ii_predict1<TF><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0));
       go = sp->max_density_solve > 0;
       while (go) {
-        k_ii_iter0<TF><<<blocks, kBlock, 0, st>>>(c, S);
-        k_ii_iter1<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0);
+        ALB_LAUNCH(e, "ii_iter0", 1, st, k_ii_iter0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "ii_iter1", 1, st,
+                   k_ii_iter1<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0));
         ALB_TRY(read_keep_going(S, hflag, st, &go));
       }
-      k_ii_accel_finish<TF><<<blocks, kBlock, 0, st>>>(
-          c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-          f->particle_pressure, f->particle_density_adv);
+      ALB_LAUNCH(e, "finish", 1, st,
+                 k_ii_accel_finish<TF><<<blocks, kBlock, 0, st>>>(
+                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                     f->particle_pressure, f->particle_density_adv));
     }
   }
-  if (nb) k_rigid_finish<TF><<<nb, 256, 0, st>>>(S);
+  if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(S));
   ALB_CUDA(cudaGetLastError());
   // ---- read back: report, rigid state, anomaly flags
   uint32_t hf[4];
@@ -943,6 +962,7 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     ALB_CUDA(cudaMemcpyAsync(hr, S.rigid, sizeof(RigidDev<TF>) * nb, cudaMemcpyDeviceToHost, st));
   ALB_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
   ALB_CUDA(cudaStreamSynchronize(st));
+  e->flush_stats();
   al_step_report rep = hc->rep;
   for (int k = 0; k < 3; ++k) rep.grid_anomaly[k] = hf[k];
   if (n == 0) rep.dt = double(*dt);

@@ -227,6 +227,20 @@ AL_API const char* al_last_error(void);
 /* Blocks until all work the engine queued on `stream` has finished. */
 AL_API int al_engine_synchronize(al_engine* engine, void* stream);
 
+/* Launch statistics, the counterpart of Runner's per-kernel event timing
+ * (launch_stat_dict_, runner.hpp:4835-4859, 6306-6308).  While profiling
+ * is on, every launch group is bracketed with CUDA events on its stream and
+ * its elapsed time accumulated under its name; off by default (the
+ * reference synchronises after every launch; the engine never does).
+ * al_engine_launch_count counts kernel launches whether or not profiling
+ * is on.  al_engine_kernel_stat returns AL_ERR_INVALID past the last
+ * entry. */
+AL_API int al_engine_set_profiling(al_engine* engine, int enable);
+AL_API int al_engine_reset_stats(al_engine* engine);
+AL_API int al_engine_launch_count(al_engine* engine, uint64_t* count);
+AL_API int al_engine_kernel_stat(al_engine* engine, uint32_t index, char* name,
+                                 size_t name_len, double* total_ms, uint64_t* count);
+
 /* ------------------------------------------------------------ grid / sort
  * Uniform-grid cell hash and stable counting sort.  Replaces the bucket
  * insert of update_particle_grid (runner.hpp:1840-1867): instead of

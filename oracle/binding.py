@@ -34,8 +34,10 @@ def lib():
             sig["orc_distance_grid_" + s] = (None, [_P, _P])
             sig["orc_volume_field_" + s] = (None, [_P, _P, _P])
             sig["orc_boundary_" + s] = (None, [_P, _P, _P, _U, _P, _U, _P, _P])
-            sig["orc_df_run_" + s] = (ctypes.c_int, [_P, _P, _P, _P, _U] + [_P] * 8 + [_U, _P])
-            sig["orc_ii_run_" + s] = (ctypes.c_int, [_P, _P, _P, _P, _U] + [_P] * 7 + [_U, _P])
+            # cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density, density_adv, a,
+            # params, dt, steps, reports (IISPH: pressure instead of kappa, kappa_v)
+            sig["orc_df_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 9 + [_U, _P])
+            sig["orc_ii_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 8 + [_U, _P])
         for name, (res, args) in sig.items():
             fn = getattr(handle, name)
             fn.restype = res
@@ -47,7 +49,7 @@ def lib():
 def _p(a):
     if a is None:
         return None
-    if isinstance(a, ctypes.Structure) or isinstance(a, ctypes.Array):
+    if isinstance(a, (ctypes.Structure, ctypes.Array, ctypes._SimpleCData)):
         return ctypes.cast(ctypes.pointer(a), ctypes.c_void_p)
     assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
     return ctypes.c_void_p(a.ctypes.data)
