@@ -828,13 +828,19 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   S.bodies = bodies_dev;
   // ---- host staging: bodies, rigid state, control block
   void* pinned = nullptr;
-  const size_t stage_bytes = sizeof(Ctrl<TF>) + (sizeof(BodyDev<TF>) + sizeof(RigidDev<TF>)) *
-                                 AL_MAX_BOUNDARIES + 64;
+  // staging layout: every section starts on a 64-byte boundary (RigidDev
+  // holds 32-byte-aligned vectors for double)
+  auto up64 = [](size_t b) { return (b + 63) & ~size_t(63); };
+  const size_t off_b = up64(sizeof(Ctrl<TF>));
+  const size_t off_r = off_b + up64(sizeof(BodyDev<TF>) * AL_MAX_BOUNDARIES);
+  const size_t off_f = off_r + up64(sizeof(RigidDev<TF>) * AL_MAX_BOUNDARIES);
+  const size_t stage_bytes = off_f + 64;
   ALB_TRY(e->host_pinned(stage_bytes, &pinned));
-  Ctrl<TF>* hc = reinterpret_cast<Ctrl<TF>*>(pinned);
-  BodyDev<TF>* hb = reinterpret_cast<BodyDev<TF>*>(hc + 1);
-  RigidDev<TF>* hr = reinterpret_cast<RigidDev<TF>*>(hb + AL_MAX_BOUNDARIES);
-  uint32_t* hflag = reinterpret_cast<uint32_t*>(hr + AL_MAX_BOUNDARIES);
+  char* base = static_cast<char*>(pinned);  // cudaMallocHost: page aligned
+  Ctrl<TF>* hc = reinterpret_cast<Ctrl<TF>*>(base);
+  BodyDev<TF>* hb = reinterpret_cast<BodyDev<TF>*>(base + off_b);
+  RigidDev<TF>* hr = reinterpret_cast<RigidDev<TF>*>(base + off_r);
+  uint32_t* hflag = reinterpret_cast<uint32_t*>(base + off_f);
   std::memset(hc, 0, sizeof(Ctrl<TF>));
   hc->dt = *dt;
   hc->length_scale = c.radius * TF(2);

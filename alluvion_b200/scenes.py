@@ -346,16 +346,22 @@ def dam_break(engine, dtype, lattice, particle_radius, container, bodies=(), see
               max_num_neighbors_per_particle=64, **const_kw):
     """Dam break: a jittered lattice block in the low corner of a box
     container (analytic box distance, sign -1, fluid inside) centred at
-    container/2, plus extra bodies.  Returns a DeviceScene."""
+    container/2, plus extra bodies.  Returns a DeviceScene.
+
+    The block's outer particles start one kernel radius h from the three
+    walls.  (The reference's mode-0 block starts 2r = h/2 from its box; with
+    the volume-map boundary term, runner.hpp:1982-2072, a particle at h/2
+    from a wall sees rho ~ 2 rho0, so that layout starts far from
+    equilibrium.  At h the wall term is exactly zero.)"""
     cn = make_const(dtype, particle_radius, **const_kw)
-    box_min = (0.0, 0.0, 0.0)
-    x = fluid_block(lattice, box_min, particle_radius, dtype, jitter=jitter, seed=seed)
+    h = float(cn.kernel_radius)
+    gap = h - 2 * float(particle_radius)
+    x = fluid_block(lattice, (gap, gap, gap), particle_radius, dtype, jitter=jitter, seed=seed)
     size = np.asarray(container, dtype=np.float64)
     cont = dict(shape=_capi.SHAPE_BOX, params=box_params(size), sign=-1.0,
                 resolution=volume_resolution, use_distance_grid=False, mass=0.0,
                 x=tuple(size / 2))
     all_bodies = [cont] + list(bodies)
-    h = float(cn.kernel_radius)
     cni = make_consti(-0.5 * h * np.ones(3), size + 0.5 * h, h, len(all_bodies),
                       max_num_particles_per_cell, max_num_neighbors_per_particle)
     return DeviceScene(engine, dtype, cn, cni, x, all_bodies)
@@ -363,7 +369,7 @@ def dam_break(engine, dtype, lattice, particle_radius, container, bodies=(), see
 
 def seeded_rigid_bodies(seed, container, particle_radius, spheres=2, boxes=2,
                         sphere_radius=0.05, box_side=0.08, resolution=64,
-                        y_range=(0.7, 0.9), density_range=(500.0, 2000.0)):
+                        y_range=(0.75, 0.9), density_range=(500.0, 2000.0)):
     """Rigid spheres and boxes at seeded positions above the fluid block,
     densities uniform in density_range, analytic mass and inertia, sampled
     onto cubic-Lagrange distance grids (use_distance_grid)."""
