@@ -166,6 +166,7 @@ _SIGNATURES = {
     "al_engine_reset_stats": (ctypes.c_int, [_P]),
     "al_engine_launch_count": (ctypes.c_int, [_P, _P]),
     "al_engine_kernel_stat": (ctypes.c_int, [_P, _U, ctypes.c_char_p, ctypes.c_size_t, _P, _P]),
+    "al_grid_sort_noalloc_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P, _P]),
 }
 for _s in ("f32", "f64"):
     _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])

@@ -232,6 +232,37 @@ int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* parti
   return AL_OK;
 }
 
+uint32_t grid_scan_tiles(uint32_t len) { return (len + kScanTile - 1) / kScanTile; }
+
+template <class TF>
+int grid_sort_into(const Cn<TF>& c, const GridDims& g, const TF* particle_x, uint32_t n,
+                   uint32_t* cell, uint32_t* perm, const GridSortScratch& sc, cudaStream_t st) {
+  const uint32_t len = g.ncells + 1;
+  ALB_CUDA(cudaMemsetAsync(sc.count, 0, size_t(len) * sizeof(uint32_t), st));
+  ALB_CUDA(cudaMemsetAsync(sc.flags, 0, 4 * sizeof(uint32_t), st));
+  if (n == 0) {
+    ALB_CUDA(cudaMemsetAsync(sc.start, 0, (size_t(len) + 1) * sizeof(uint32_t), st));
+    return AL_OK;
+  }
+  k_hash<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(particle_x, n, c.h, g, cell, sc.rank,
+                                                       sc.count, sc.flags);
+  const uint32_t ntiles = grid_scan_tiles(len);
+  k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(sc.count, sc.start, len, sc.sums, g.ncells,
+                                                 g.cap_cell, sc.flags);
+  k_scan_sums<<<1, 1024, 0, st>>>(sc.sums, ntiles, sc.start, len);
+  if (ntiles > 1) k_scan_add<<<blocks_for(len, 256), 256, 0, st>>>(sc.start, len, sc.sums);
+  k_scatter<<<blocks_for(n, kBlock), kBlock, 0, st>>>(cell, sc.rank, sc.start, n, g.ncells,
+                                                      perm);
+  k_order_cells<<<blocks_for(g.ncells, kBlock), kBlock, 0, st>>>(sc.start, g.ncells, perm);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+template int grid_sort_into<float>(const Cn<float>&, const GridDims&, const float*, uint32_t,
+                                   uint32_t*, uint32_t*, const GridSortScratch&, cudaStream_t);
+template int grid_sort_into<double>(const Cn<double>&, const GridDims&, const double*, uint32_t,
+                                    uint32_t*, uint32_t*, const GridSortScratch&, cudaStream_t);
+
 template int grid_build<float>(al_engine*, const Cn<float>&, const GridDims&, const float*,
                                uint32_t, vec4<float>*, uint32_t*, GridState&, cudaStream_t);
 template int grid_build<double>(al_engine*, const Cn<double>&, const GridDims&, const double*,

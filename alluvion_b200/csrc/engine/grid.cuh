@@ -34,4 +34,23 @@ template <class TF>
 int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* particle_x,
                uint32_t n, vec4<TF>* xs, uint32_t* flags, GridState& gs, cudaStream_t st);
 
+// Scratch for grid_sort_into, all supplied by the caller.
+struct GridSortScratch {
+  uint32_t* rank;   // [n]
+  uint32_t* count;  // [ncells + 1], zeroed by grid_sort_into
+  uint32_t* start;  // [ncells + 2]
+  uint32_t* sums;   // [grid_scan_tiles(ncells + 1)]
+  uint32_t* flags;  // [4], zeroed by grid_sort_into
+};
+
+// Number of scan tiles for `len` entries.
+uint32_t grid_scan_tiles(uint32_t len);
+
+// The same hash / scan / scatter / per-cell ordering as grid_build, writing
+// the per-particle cell and the permutation straight into cell / perm and
+// using only the given scratch: no allocation of any kind.
+template <class TF>
+int grid_sort_into(const Cn<TF>& c, const GridDims& g, const TF* particle_x, uint32_t n,
+                   uint32_t* cell, uint32_t* perm, const GridSortScratch& sc, cudaStream_t st);
+
 }  // namespace alb

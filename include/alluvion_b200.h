@@ -270,6 +270,24 @@ AL_API int al_grid_sort_f64(al_engine* engine, const al_const_f64* cn,
                      uint32_t* sorted_to_original, uint32_t* cell_start,
                      uint32_t* pid_length, void* stream);
 
+/* The grid sort of al_grid_sort_f32 for callers that must not let the
+ * library allocate device memory (a host capturing its frame into a CUDA
+ * graph, a renderer or game engine that owns the memory budget, a real-time
+ * loop avoiding allocation stalls).  No counterpart in the reference.
+ * Allocates nothing: all scratch is one static device array of 12.6 MiB
+ * that every GPU loading the library keeps until exit.  Limits: at most
+ * 1,048,576 particles and 1,048,576 grid cells; larger problems return
+ * AL_ERR_INVALID.  Uses the current device.  Its first call on a device
+ * looks up the array's device address, so make that first call before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU
+ * race, so order them.  Synchronises `stream` before returning (it reads
+ * the anomaly flags); returns AL_ERR_OUT_OF_GRID / AL_ERR_CELL_OVERFLOW
+ * like al_grid_sort_f32. */
+AL_API int al_grid_sort_noalloc_f32(const al_const_f32* cn, const al_consti* cni,
+                                    const float* particle_x, uint32_t num_particles,
+                                    uint32_t* particle_cell, uint32_t* sorted_to_original,
+                                    uint32_t* cell_start, uint32_t* pid_length, void* stream);
+
 /* ------------------------------------------------ neighbors and density
  * Solver::update_particle_neighbors<0> (solver.hpp:225-260) for the
  * volume-map boundary method: grid sort, neighbor list
