@@ -151,6 +151,7 @@ template <class TF>
 struct Cn {
   TF h, h2, k, l, w0, radius, vol, mass, rho0, visc, bvisc, eps;
   vec3<TF> g;
+  TF inv_h, inv_h2;  // 1 / h and 1 / h^2, rounded once on the host
 };
 
 template <class TF, class C>
@@ -169,6 +170,8 @@ inline Cn<TF> to_cn(const C& c) {
   o.bvisc = c.boundary_viscosity;
   o.eps = c.dfsph_factor_epsilon;
   o.g = vec3<TF>{c.gravity[0], c.gravity[1], c.gravity[2]};
+  o.inv_h = TF(1) / o.h;
+  o.inv_h2 = TF(1) / o.h2;
   return o;
 }
 
@@ -207,6 +210,20 @@ __device__ __forceinline__ TF W_dist(const Cn<TF>& c, TF r) {
 }
 
 // Cubic spline of a squared distance (d2_cubic_kernel, runner.hpp:608-619).
+// float: q from the hardware reciprocal square root and 1/h, no IEEE
+// division or square-root sequence (the reference is built with
+// --use_fast_math, whose division and sqrt are approximate as well).
+__device__ __forceinline__ float W_r2(const Cn<float>& c, float r2) {
+  const float q2 = r2 * c.inv_h2;
+  const float q = r2 > 0.f ? r2 * rsqrtf(r2) * c.inv_h : 0.f;
+  const float conj = 1.f - q;
+  float s = 0.f;
+  if (q <= 0.5f)
+    s = (6.f * q - 6.f) * q2 + 1.f;
+  else if (q <= 1.f)
+    s = 2.f * conj * conj * conj;
+  return s * c.k;
+}
 template <class TF>
 __device__ __forceinline__ TF W_r2(const Cn<TF>& c, TF r2) {
   TF q2 = r2 / c.h2;
@@ -221,7 +238,17 @@ __device__ __forceinline__ TF W_r2(const Cn<TF>& c, TF r2) {
 }
 
 // Kernel gradient of a displacement (displacement_cubic_kernel_grad,
-// runner.hpp:628-638).
+// runner.hpp:628-638).  float: one hardware reciprocal square root gives
+// both |d| and 1/|d|.
+__device__ __forceinline__ vec3<float> gradW(const Cn<float>& c, vec3<float> d) {
+  const float rl2 = length_sqr(d);
+  const float inv_rl = rl2 > 0.f ? rsqrtf(rl2) : 0.f;
+  const float rl = rl2 * inv_rl;
+  const float q = rl * c.inv_h;
+  const float s = q <= 0.5f ? (q * 3.f - 2.f) * c.inv_h
+                            : (q <= 1.f ? (1.f - q) * (q - 1.f) * inv_rl : 0.f);
+  return (c.l * s) * d;
+}
 template <class TF>
 __device__ __forceinline__ vec3<TF> gradW(const Cn<TF>& c, vec3<TF> d) {
   TF rl2 = length_sqr(d);

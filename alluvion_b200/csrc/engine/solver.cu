@@ -79,8 +79,9 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
                                                   uint32_t s, vec3<TF> xi, vec3<TF> vi,
                                                   uint32_t cnt) {
   TF acc = 0;
+  #pragma unroll 4
   for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
     const vec3<TF> d = xi - ldx(S.x, t);
     acc += c.vol * dot(vi - ldx(S.v, t), gradW(c, d));
   }
@@ -183,8 +184,9 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
     ki = ksrc[s];
     const vec3<TF> xi = xyz(S.x[s]);
     const uint32_t cnt = S.ncount[s];
+    #pragma unroll 4
     for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
       const TF ksum = ki + __ldg(ksrc + t);
       if (fabs(ksum) > c.eps) {
         const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
@@ -300,8 +302,9 @@ __global__ void __launch_bounds__(kBlock)
     xi = xyz(S.x[s]);
     vi = xyz(S.v[s]);
     const uint32_t cnt = S.ncount[s];
+    #pragma unroll 4
     for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
       const vec3<TF> d = xi - ldx(S.x, t);
       da += (c.visc * c.mass / __ldg(S.rho + t) * dot(d, gradW(c, d)) /
              (length_sqr(d) + TF(0.01) * c.h2)) *
@@ -501,8 +504,9 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
   const TF rho = S.rho[s], rho2 = rho * rho;
   vec3<TF> dii{0, 0, 0};
   const uint32_t cnt = S.ncount[s];
+  #pragma unroll 4
   for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
     dii -= (c.vol / rho2) * gradW(c, xi - ldx(S.x, t));
   }
   for (uint32_t m = S.mask[s]; m; m &= m - 1) {
@@ -524,8 +528,9 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
   const TF rho = S.rho[s], rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
   TF adv = rho / c.rho0, aii = 0;
   const uint32_t cnt = S.ncount[s];
+  #pragma unroll 4
   for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
     const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
     adv += dt * c.vol * dot(vi - ldx(S.v, t), gw);
@@ -558,8 +563,9 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
   const vec3<TF> xi = xyz(S.x[s]);
   vec3<TF> acc{0, 0, 0};
   const uint32_t cnt = S.ncount[s];
+  #pragma unroll 4
   for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
     const TF rj = __ldg(S.rho + t), rj2 = rj * rj;
     acc -= (c.vol / rj2 * src[t]) * gradW(c, xi - ldx(S.x, t));
   }
@@ -586,8 +592,9 @@ __global__ void __launch_bounds__(kBlock)
     const TF omega = TF(2) / TF(3);
     TF p = 0, sum = 0;
     const uint32_t cnt = S.ncount[s];
+    #pragma unroll 4
     for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
       const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
       const vec3<TF> dji = (dpi * c.rho0) * gw;
       const vec3<TF> dji_pi = dji * lp;
@@ -629,8 +636,9 @@ __global__ void __launch_bounds__(kBlock)
     const TF rho = S.rho[s];
     dpi = S.kappa[s] / (rho * rho);
     const uint32_t cnt = S.ncount[s];
+    #pragma unroll 4
     for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldg(S.nbr + size_t(k) * S.n + s);
+      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
       const TF rj = __ldg(S.rho + t);
       const TF dpj = __ldg(S.kappa + t) / (rj * rj);
       ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldx(S.x, t));

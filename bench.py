@@ -74,6 +74,10 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=20.0,
                    help="budget of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--rigid-bodies", type=int, default=4, choices=[0, 4],
+                   help="0 drops the 4 rigid bodies (profiling case)")
+    p.add_argument("--container-resolution", type=int, default=64,
+                   help="volume-map resolution of the container")
     return p.parse_args()
 
 
@@ -139,11 +143,13 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_scene(engine, dtype=np.float32):
+def build_scene(engine, dtype=np.float32, rigid_bodies=4, container_resolution=64):
     from alluvion_b200 import scenes
-    bodies = scenes.seeded_rigid_bodies(SEED, CONTAINER, RADIUS, resolution=64)
+    bodies = []
+    if rigid_bodies:
+        bodies = scenes.seeded_rigid_bodies(SEED, CONTAINER, RADIUS, resolution=64)
     return scenes.dam_break(engine, dtype, LATTICE, RADIUS, CONTAINER, bodies, seed=SEED,
-                            volume_resolution=64)
+                            volume_resolution=container_resolution)
 
 
 def measured_peaks():
@@ -235,7 +241,8 @@ def engine_arm(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     engine = _capi.Engine(local)
-    scene = build_scene(engine)
+    scene = build_scene(engine, rigid_bodies=args.rigid_bodies,
+                        container_resolution=args.container_resolution)
     sp = scenes.solver_params()
     dt = float(sp.max_dt)
     host_state = scene.state() if rank == 0 and world == 1 else None
@@ -312,12 +319,16 @@ def engine_arm(args):
                 "algorithmic_bytes_per_launch": int(alg_bytes),
                 "launch_ms": round(per_launch[dominant], 4)}
     steps_reps = reps
+    workload = WORKLOAD
+    if args.rigid_bodies == 0 or args.container_resolution != 64:
+        workload += " [variant: %d rigid bodies, %d^3 container map]" % (
+            args.rigid_bodies, args.container_resolution)
     result = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded jittered lattice, seeded rigid bodies)",
-        "config": {"workload": WORKLOAD, "particles_per_gpu": n, "global_particles":
+        "config": {"workload": workload, "particles_per_gpu": n, "global_particles":
                    total_particles, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
                    "mean_divergence_iterations": round(sum(r[0] for r in steps_reps) /
