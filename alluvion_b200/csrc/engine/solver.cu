@@ -77,14 +77,12 @@ __device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_
 template <class TF>
 __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepState<TF>& S,
                                                   uint32_t s, vec3<TF> xi, vec3<TF> vi,
-                                                  uint32_t cnt) {
+                                                  uint64_t desc) {
   TF acc = 0;
-  #pragma unroll 4
-  for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
     const vec3<TF> d = xi - ldx(S.x, t);
     acc += c.vol * dot(vi - ldx(S.v, t), gradW(c, d));
-  }
+  });
   for (uint32_t m = S.mask[s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
     const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
@@ -97,17 +95,17 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
 
 template <class TF>
 __device__ __forceinline__ TF density_change(const Cn<TF>& c, const StepState<TF>& S, uint32_t s) {
-  const uint32_t cnt = S.ncount[s];
-  TF adv = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), cnt);
+  const uint64_t desc = S.desc[s];
+  TF adv = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), desc);
   adv = fmax(adv, TF(0));
-  if (cnt < 20) adv = 0;
+  if (neighbor_total(desc) < 20) adv = 0;
   return adv;
 }
 
 template <class TF>
 __device__ __forceinline__ TF density_adv(const Cn<TF>& c, const StepState<TF>& S, uint32_t s,
                                           TF dt) {
-  const TF delta = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), S.ncount[s]);
+  const TF delta = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), S.desc[s]);
   return fmax(S.rho[s] / c.rho0 + dt * delta, TF(1));
 }
 
@@ -183,10 +181,8 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   if (act) {
     ki = ksrc[s];
     const vec3<TF> xi = xyz(S.x[s]);
-    const uint32_t cnt = S.ncount[s];
-    #pragma unroll 4
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+    const uint64_t desc = S.desc[s];
+    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
       const TF ksum = ki + __ldg(ksrc + t);
       if (fabs(ksum) > c.eps) {
         const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
@@ -197,7 +193,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
           dv += (dt * ksum * c.vol) * gw;
         }
       }
-    }
+    });
     if (fabs(ki) > c.eps) m = S.mask[s];
   }
   for (uint32_t b = 0; b < S.nb; ++b) {
@@ -301,15 +297,13 @@ __global__ void __launch_bounds__(kBlock)
   if (act) {
     xi = xyz(S.x[s]);
     vi = xyz(S.v[s]);
-    const uint32_t cnt = S.ncount[s];
-    #pragma unroll 4
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+    const uint64_t desc = S.desc[s];
+    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
       const vec3<TF> d = xi - ldx(S.x, t);
       da += (c.visc * c.mass / __ldg(S.rho + t) * dot(d, gradW(c, d)) /
              (length_sqr(d) + TF(0.01) * c.h2)) *
             (vi - ldx(S.v, t));
-    }
+    });
     m = S.mask[s];
   }
   for (uint32_t b = 0; b < S.nb; ++b) {
@@ -503,12 +497,10 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
   const vec3<TF> xi = xyz(S.x[s]);
   const TF rho = S.rho[s], rho2 = rho * rho;
   vec3<TF> dii{0, 0, 0};
-  const uint32_t cnt = S.ncount[s];
-  #pragma unroll 4
-  for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+  const uint64_t desc = S.desc[s];
+  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
     dii -= (c.vol / rho2) * gradW(c, xi - ldx(S.x, t));
-  }
+  });
   for (uint32_t m = S.mask[s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
     const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
@@ -527,15 +519,13 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
   const vec3<TF> xi = xyz(S.x[s]), vi = xyz(S.v[s]), dii = xyz(S.dii[s]);
   const TF rho = S.rho[s], rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
   TF adv = rho / c.rho0, aii = 0;
-  const uint32_t cnt = S.ncount[s];
-  #pragma unroll 4
-  for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+  const uint64_t desc = S.desc[s];
+  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
     const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
     adv += dt * c.vol * dot(vi - ldx(S.v, t), gw);
     aii += c.vol * dot(dii - dji, gw);
-  }
+  });
   for (uint32_t m = S.mask[s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
     const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
@@ -562,13 +552,11 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
   if (!first) S.kappa_v[s] = S.kappa[s];
   const vec3<TF> xi = xyz(S.x[s]);
   vec3<TF> acc{0, 0, 0};
-  const uint32_t cnt = S.ncount[s];
-  #pragma unroll 4
-  for (uint32_t k = 0; k < cnt; ++k) {
-    const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+  const uint64_t desc = S.desc[s];
+  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
     const TF rj = __ldg(S.rho + t), rj2 = rj * rj;
     acc -= (c.vol / rj2 * src[t]) * gradW(c, xi - ldx(S.x, t));
-  }
+  });
   acc = acc * c.rho0;
   S.dij_pj[s] = vec4<TF>{acc.x, acc.y, acc.z, TF(0)};
 }
@@ -591,17 +579,15 @@ __global__ void __launch_bounds__(kBlock)
     const TF denom = S.kk[s] * dt2;
     const TF omega = TF(2) / TF(3);
     TF p = 0, sum = 0;
-    const uint32_t cnt = S.ncount[s];
-    #pragma unroll 4
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+    const uint64_t desc = S.desc[s];
+    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
       const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
       const vec3<TF> dji = (dpi * c.rho0) * gw;
       const vec3<TF> dji_pi = dji * lp;
       sum += c.vol * dot(dij_pj - ldx(S.dii, t) * __ldg(S.kappa_v + t) -
                              (ldx(S.dij_pj, t) - dji_pi),
                          gw);
-    }
+    });
     for (uint32_t m = S.mask[s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
       sum += dot(dij_pj, xyz(S.bk[size_t(b) * S.n + s]));
@@ -635,14 +621,12 @@ __global__ void __launch_bounds__(kBlock)
     xi = xyz(S.x[s]);
     const TF rho = S.rho[s];
     dpi = S.kappa[s] / (rho * rho);
-    const uint32_t cnt = S.ncount[s];
-    #pragma unroll 4
-    for (uint32_t k = 0; k < cnt; ++k) {
-      const uint32_t t = __ldcs(S.nbr + size_t(k) * S.n + s);
+    const uint64_t desc = S.desc[s];
+    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
       const TF rj = __ldg(S.rho + t);
       const TF dpj = __ldg(S.kappa + t) / (rj * rj);
       ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldx(S.x, t));
-    }
+    });
     m = S.mask[s];
   }
   for (uint32_t b = 0; b < S.nb; ++b) {
@@ -775,6 +759,14 @@ int check_step_args(const typename FluidT<TF>::type* f, const al_consti* cni,
   ALB_CHECK_ARG(uint64_t(cni->grid_res[0]) * cni->grid_res[1] * cni->grid_res[2] < (1ull << 31),
                 "step: grid has too many cells");
   ALB_CHECK_ARG(cni->max_num_neighbors_per_particle > 0, "step: neighbor capacity is 0");
+  // compact lists: a neighbor's offset within its 3-cell row must fit a byte,
+  // and a row count must fit 7 bits
+  if (cni->max_num_particles_per_cell > (kMaxRowOffset + 1) / 3 ||
+      cni->max_num_neighbors_per_particle >= (1u << kRowBits)) {
+    set_error("step: max_num_particles_per_cell must be <= 85 and "
+              "max_num_neighbors_per_particle < 128");
+    return AL_ERR_UNSUPPORTED;
+  }
   ALB_CHECK_ARG(*dt > TF(0), "step: dt must be positive");
   return AL_OK;
 }
@@ -823,8 +815,8 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     ALB_TRY(e->buf("sorted.dii", n, &S.dii));
     ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
   }
-  ALB_TRY(e->buf("nbr.list", size_t(n) * g.cap_nbr, &S.nbr));
-  ALB_TRY(e->buf("nbr.count", n, &S.ncount));
+  ALB_TRY(e->buf("nbr.desc", n, &S.desc));
+  ALB_TRY(e->buf("nbr.off", size_t(n) * g.cap_nbr, &S.off));
   ALB_TRY(e->buf("bnd.mask", n, &S.mask));
   ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
   ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
@@ -881,6 +873,7 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   ALB_LAUNCH(e, "grid_sort", 7, st,
              ALB_TRY(grid_build<TF>(e, c, g, f->particle_x, n, S.x, flags, gs, st)));
   S.perm = gs.perm;
+  S.rows = NeighborRows{S.desc, S.off, gs.cell_start, n, g};
   const uint32_t blocks = blocks_for(n, kBlock);
   if (n > 0) {
     const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
@@ -903,7 +896,7 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
   ALB_LAUNCH(e, "neighbors", 1, st,
-             ALB_TRY(build_neighbors_density<TF>(c, g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+             ALB_TRY(build_compact_neighbors<TF>(c, g, gs, S.x, sbk, S.desc, S.off, S.rho,
                                                  iisph ? nullptr : S.alpha, st)));
   const bool div = !iisph && sp->enable_divergence_solve;
   const bool den = iisph || sp->enable_density_solve;
