@@ -70,73 +70,6 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// Compact-list variant of k_build_neighbors: same candidates, same order,
-// same density / factor arithmetic; stores row counts and byte offsets.
-template <class TF, class BK, bool FACTOR>
-__global__ void __launch_bounds__(kBlock)
-    k_build_compact(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
-                    const vec4<TF>* __restrict__ xs, uint32_t n, BK bk,
-                    uint64_t* __restrict__ desc_out, uint8_t* __restrict__ off_out,
-                    TF* __restrict__ rho, TF* __restrict__ alpha, uint32_t* __restrict__ flags) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const vec3<TF> xi = xyz(xs[s]);
-  int ip[3];
-  cell_coords(c.h, g, xi, ip);
-  const int z0 = max(ip[2] - 1, 0);
-  const int z1 = min(ip[2] + 1, int(g.res[2]) - 1);
-  uint32_t cnt = 0, stored = 0;
-  uint64_t desc = 0;
-  bool off_overflow = false;
-  TF density = c.vol * c.w0;
-  TF sum_grad = 0;
-  vec3<TF> grad_i{0, 0, 0};
-  if (z0 <= z1) {
-    for (int r = 0; r < 9; ++r) {
-      const int cx = ip[0] + r / 3 - 1, cy = ip[1] + r % 3 - 1;
-      if (cx < 0 || cx >= int(g.res[0]) || cy < 0 || cy >= int(g.res[1])) continue;
-      const uint32_t b = cell_start[cell_linear(g, cx, cy, z0)];
-      const uint32_t e = cell_start[cell_linear(g, cx, cy, z1) + 1];
-      uint32_t cr = 0;
-      for (uint32_t t = b; t < e; ++t) {
-        if (t == s) continue;
-        const vec3<TF> xj = xyz(xs[t]);
-        const TF d2 = dist2_rn(xi, xj);
-        if (d2 < c.h2) {
-          if (cnt < g.cap_nbr) {
-            if (t - b > kMaxRowOffset) {
-              off_overflow = true;
-            } else {
-              off_out[size_t(stored) * n + s] = uint8_t(t - b);
-              ++stored;
-              ++cr;
-              density += c.vol * W_r2(c, d2);
-              if (FACTOR) {
-                const vec3<TF> d{sub_rn(xi.x, xj.x), sub_rn(xi.y, xj.y), sub_rn(xi.z, xj.z)};
-                const vec3<TF> gpj = (-c.vol) * gradW(c, d);
-                sum_grad += length_sqr(gpj);
-                grad_i -= gpj;
-              }
-            }
-          }
-          ++cnt;
-        }
-      }
-      desc |= uint64_t(cr) << (kRowBits * r);
-    }
-  }
-  if (cnt > g.cap_nbr) flags[2] = 1u;
-  if (off_overflow) flags[1] = 1u;
-  desc_out[s] = desc;
-  density += bk.density_term(s);
-  rho[s] = density * c.rho0;
-  if (FACTOR) {
-    grad_i += bk.grad_term(s);
-    sum_grad += length_sqr(grad_i);
-    alpha[s] = sum_grad > c.eps ? TF(-1) / sum_grad : TF(0);
-  }
-}
-
 template <class TF>
 __global__ void k_export_neighbors(uint32_t cap, uint32_t n, const uint32_t* __restrict__ perm,
                                    const uint32_t* __restrict__ inv,
@@ -186,21 +119,6 @@ int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState&
   return AL_OK;
 }
 
-template <class TF, class BK>
-int build_compact_neighbors(const Cn<TF>& c, const GridDims& g, const GridState& gs,
-                            const vec4<TF>* xs, const BK& bk, uint64_t* desc, uint8_t* off,
-                            TF* rho, TF* alpha, cudaStream_t st) {
-  if (gs.n == 0) return AL_OK;
-  if (alpha)
-    k_build_compact<TF, BK, true><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, bk, desc, off, rho, alpha, gs.flags);
-  else
-    k_build_compact<TF, BK, false><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, bk, desc, off, rho, alpha, gs.flags);
-  ALB_CUDA(cudaGetLastError());
-  return AL_OK;
-}
-
 template <class TF>
 int export_neighbors(const GridDims& g, const GridState& gs, const vec4<TF>* xs,
                      const uint32_t* nbr, const uint32_t* ncount, const TF* rho_sorted,
@@ -223,12 +141,6 @@ ALB_INST(double, RefBoundaryKernel)
 ALB_INST(float, SortedBoundaryKernel)
 ALB_INST(double, SortedBoundaryKernel)
 #undef ALB_INST
-template int build_compact_neighbors<float, SortedBoundaryKernel<float>>(
-    const Cn<float>&, const GridDims&, const GridState&, const vec4<float>*,
-    const SortedBoundaryKernel<float>&, uint64_t*, uint8_t*, float*, float*, cudaStream_t);
-template int build_compact_neighbors<double, SortedBoundaryKernel<double>>(
-    const Cn<double>&, const GridDims&, const GridState&, const vec4<double>*,
-    const SortedBoundaryKernel<double>&, uint64_t*, uint8_t*, double*, double*, cudaStream_t);
 template int export_neighbors<float>(const GridDims&, const GridState&, const vec4<float>*,
                                      const uint32_t*, const uint32_t*, const float*, float*,
                                      uint32_t*, float*, cudaStream_t);

@@ -77,66 +77,6 @@ int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState&
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
                             TF* rho, TF* alpha, cudaStream_t st);
 
-// ----------------------------------------------------------- compact lists
-// The step's neighbor lists.  In canonical order the neighbors of a
-// particle lie in the 9 (dx, dy) cell rows around its cell, each row one
-// contiguous range of sorted slots starting at cell_start of the row's
-// first cell.  A particle's list is stored as
-//   desc[s]          9 row counts of 7 bits each (row r = 3 * (dx + 1) + (dy + 1))
-//   off[k * N + s]   offset of the k-th neighbor from its row's first slot
-// so a neighbor costs 1 byte instead of 4 and the list is rebuilt from the
-// particle's own cell coordinates.  Rows hold at most 3 cells; an offset
-// above 255 (only possible when cells overflow their capacity) is dropped
-// and raises the cell-overflow flag.
-constexpr int kRowBits = 7;
-constexpr uint32_t kMaxRowOffset = 255;
-
-struct NeighborRows {
-  const uint64_t* desc;
-  const uint8_t* off;
-  const uint32_t* cell_start;
-  uint32_t n;
-  GridDims g;
-};
-
-__device__ __forceinline__ uint32_t row_count(uint64_t desc, int r) {
-  return uint32_t(desc >> (kRowBits * r)) & ((1u << kRowBits) - 1u);
-}
-__device__ __forceinline__ uint32_t neighbor_total(uint64_t desc) {
-  uint32_t c = 0;
-#pragma unroll
-  for (int r = 0; r < 9; ++r) c += row_count(desc, r);
-  return c;
-}
-
-// Calls f(t) for every neighbor slot t of sorted particle s (position xi),
-// in canonical order.
-template <class TF, class F>
-__device__ __forceinline__ void for_each_neighbor(const NeighborRows& L, TF h, uint32_t s,
-                                                  vec3<TF> xi, uint64_t desc, F&& f) {
-  int ip[3];
-  cell_coords(h, L.g, xi, ip);
-  const int z0 = max(ip[2] - 1, 0);
-  uint32_t k = 0;
-#pragma unroll
-  for (int r = 0; r < 9; ++r) {
-    const uint32_t cr = row_count(desc, r);
-    if (cr == 0) continue;
-    const uint32_t base =
-        __ldg(L.cell_start + cell_linear(L.g, ip[0] + r / 3 - 1, ip[1] + r % 3 - 1, z0));
-    for (uint32_t j = 0; j < cr; ++j, ++k)
-      f(base + uint32_t(__ldg(L.off + size_t(k) * L.n + s)));
-  }
-}
-
-// Builds the compact lists of all n sorted slots, the density and, when
-// `alpha` is non-null, the DFSPH factor (same arithmetic and order as
-// build_neighbors_density).
-template <class TF, class BK>
-int build_compact_neighbors(const Cn<TF>& c, const GridDims& g, const GridState& gs,
-                            const vec4<TF>* xs, const BK& bk, uint64_t* desc, uint8_t* off,
-                            TF* rho, TF* alpha, cudaStream_t st);
-
 // Writes reference-layout outputs in original particle order:
 // particle_neighbors [N][cap][4] {x_i - x_j, bits(j)} (if non-null),
 // particle_num_neighbors [N], particle_density [N] (if non-null).

@@ -71,42 +71,96 @@ __device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_
   return true;
 }
 
+// Pair passes run kTPP threads per particle: lane `sub` of a particle's
+// group walks neighbors sub, sub + kTPP, ...; the group combines its partial
+// sums with warp shuffles (fixed order, deterministic) and lane 0 applies
+// the boundary terms and writes the results.  Shorter dependent-load chains
+// per thread keep more gathers in flight than one thread per particle.
+constexpr int kTPP = 4;
+
+struct Lane {
+  uint32_t s, sub;
+  bool act;
+  __device__ __forceinline__ bool lead() const { return act && sub == 0; }
+};
+
+__device__ __forceinline__ Lane pair_lane(uint32_t n) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  Lane l;
+  l.s = g / kTPP;
+  l.sub = g % kTPP;
+  l.act = l.s < n;
+  return l;
+}
+
+inline uint32_t pair_blocks(uint32_t n) {
+  return uint32_t((uint64_t(n) * kTPP + kBlock - 1) / kBlock);
+}
+
+template <class T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+  for (int o = kTPP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <class TF>
+__device__ __forceinline__ vec3<TF> group_sum(vec3<TF> v) {
+  return vec3<TF>{group_sum(v.x), group_sum(v.y), group_sum(v.z)};
+}
+
+template <class TF>
+__device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, uint32_t s) {
+  return __ldcs(S.nbr + size_t(k) * S.n + s);
+}
+
 // Sum over neighbors of V (v_i - v_j) . grad W_ij plus the boundary terms
 // (v_i - v_b) . (grad W V)_b: the shared body of compute_density_change
 // (runner.hpp:3192-3228) and compute_density_adv (runner.hpp:3493-3523).
+// Every lane of the group calls it and receives the full sum.
 template <class TF>
 __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepState<TF>& S,
-                                                  uint32_t s, vec3<TF> xi, vec3<TF> vi,
-                                                  uint64_t desc) {
+                                                  const Lane& L, vec3<TF> xi, vec3<TF> vi,
+                                                  uint32_t cnt) {
   TF acc = 0;
-  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
     const vec3<TF> d = xi - ldx(S.x, t);
     acc += c.vol * dot(vi - ldx(S.v, t), gradW(c, d));
-  });
-  for (uint32_t m = S.mask[s]; m; m &= m - 1) {
-    const uint32_t b = __ffs(m) - 1;
-    const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
-    const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
-    const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
-    acc += dot(vi - vj, xyz(kg));
+  }
+  acc = group_sum(acc);
+  if (L.act) {
+    for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
+      const uint32_t b = __ffs(m) - 1;
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
+      const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
+      acc += dot(vi - vj, xyz(kg));
+    }
   }
   return acc;
 }
 
 template <class TF>
-__device__ __forceinline__ TF density_change(const Cn<TF>& c, const StepState<TF>& S, uint32_t s) {
-  const uint64_t desc = S.desc[s];
-  TF adv = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), desc);
+__device__ __forceinline__ TF density_change(const Cn<TF>& c, const StepState<TF>& S,
+                                             const Lane& L) {
+  const uint32_t cnt = L.act ? S.ncount[L.s] : 0u;
+  const vec3<TF> xi = L.act ? xyz(S.x[L.s]) : vec3<TF>{0, 0, 0};
+  const vec3<TF> vi = L.act ? xyz(S.v[L.s]) : vec3<TF>{0, 0, 0};
+  TF adv = velocity_divergence(c, S, L, xi, vi, cnt);
   adv = fmax(adv, TF(0));
-  if (neighbor_total(desc) < 20) adv = 0;
+  if (cnt < 20) adv = 0;
   return adv;
 }
 
 template <class TF>
-__device__ __forceinline__ TF density_adv(const Cn<TF>& c, const StepState<TF>& S, uint32_t s,
+__device__ __forceinline__ TF density_adv(const Cn<TF>& c, const StepState<TF>& S, const Lane& L,
                                           TF dt) {
-  const TF delta = velocity_divergence(c, S, s, xyz(S.x[s]), xyz(S.v[s]), S.desc[s]);
-  return fmax(S.rho[s] / c.rho0 + dt * delta, TF(1));
+  const uint32_t cnt = L.act ? S.ncount[L.s] : 0u;
+  const vec3<TF> xi = L.act ? xyz(S.x[L.s]) : vec3<TF>{0, 0, 0};
+  const vec3<TF> vi = L.act ? xyz(S.v[L.s]) : vec3<TF>{0, 0, 0};
+  const TF delta = velocity_divergence(c, S, L, xi, vi, cnt);
+  const TF rho = L.act ? S.rho[L.s] : c.rho0;
+  return fmax(rho / c.rho0 + dt * delta, TF(1));
 }
 
 // ------------------------------------------------------------- kernels
@@ -131,7 +185,8 @@ __global__ void k_step_init(StepState<TF> S) {
     TF m = -max_value<TF>();
     for (uint32_t b = 0; b < S.nb; ++b) {
       const RigidDev<TF>& rg = S.rigid[b];
-      const vec3<TF> w = cross(rg.omega, vec3<TF>{S.bodies[b].max_distance, TF(0), TF(0)}) + rg.v;
+      const vec3<TF> w =
+          cross(rg.omega, vec3<TF>{S.bodies[b].max_distance, TF(0), TF(0)}) + rg.v;
       m = fmax(m, length_sqr(w));
     }
     r.pile_max_v2 = double(m);
@@ -153,12 +208,12 @@ __global__ void k_gather_state(StepState<TF> S, const TF* __restrict__ v_ref,
 // warm_start_divergence_solve_0 (runner.hpp:3230-3249).
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_df_warm0(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  const TF adv = density_change(c, S, s);
+  const Lane L = pair_lane(S.n);
+  const TF adv = density_change(c, S, L);
+  if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
-  const TF kv = S.kappa_v[s];
-  S.kappa_v[s] = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
+  const TF kv = S.kappa_v[L.s];
+  S.kappa_v[L.s] = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
 }
 
 enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
@@ -170,39 +225,41 @@ enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 template <class TF, int MODE>
 __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = s < S.n;
+  const Lane L = pair_lane(S.n);
   const TF* __restrict__ ksrc =
       MODE == kDivWarm ? S.kappa_v : (MODE == kPressWarm ? S.kappa : S.kk);
   const TF dt = S.ctrl->dt;
   TF ki = 0;
   vec3<TF> dv{0, 0, 0};
-  uint32_t m = 0;
-  if (act) {
-    ki = ksrc[s];
-    const vec3<TF> xi = xyz(S.x[s]);
-    const uint64_t desc = S.desc[s];
-    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
-      const TF ksum = ki + __ldg(ksrc + t);
-      if (fabs(ksum) > c.eps) {
-        const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
-        if (kDiv) {
-          const vec3<TF> gpj = (-c.vol) * gw;
-          dv -= (dt * ksum) * gpj;
-        } else {
-          dv += (dt * ksum * c.vol) * gw;
-        }
-      }
-    });
-    if (fabs(ki) > c.eps) m = S.mask[s];
+  uint32_t cnt = 0;
+  vec3<TF> xi{0, 0, 0};
+  if (L.act) {
+    ki = ksrc[L.s];
+    xi = xyz(S.x[L.s]);
+    cnt = S.ncount[L.s];
   }
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
+    const TF ksum = ki + __ldg(ksrc + t);
+    if (fabs(ksum) > c.eps) {
+      const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+      if (kDiv) {
+        const vec3<TF> gpj = (-c.vol) * gw;
+        dv -= (dt * ksum) * gpj;
+      } else {
+        dv += (dt * ksum * c.vol) * gw;
+      }
+    }
+  }
+  dv = group_sum(dv);
+  const uint32_t m = (L.lead() && fabs(ki) > c.eps) ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
     if (!__syncthreads_or(mine)) continue;
     vec3<TF> f{0, 0, 0}, tq{0, 0, 0};
     if (mine) {
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
-      const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
       const vec3<TF> a = ki * (-xyz(kg));
       f = c.mass * a;
       dv -= dt * a;
@@ -210,11 +267,11 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
     }
     block_add_ft(S, b, f, tq);
   }
-  if (act) {
-    if (MODE == kDivIter) S.kappa_v[s] += ki;
-    if (MODE == kPressIter) S.kappa[s] += ki;
-    vec4<TF> v = S.v[s];
-    S.v[s] = vec4<TF>{v.x + dv.x, v.y + dv.y, v.z + dv.z, v.w};
+  if (L.lead()) {
+    if (MODE == kDivIter) S.kappa_v[L.s] += ki;
+    if (MODE == kPressIter) S.kappa[L.s] += ki;
+    const vec4<TF> v = S.v[L.s];
+    S.v[L.s] = vec4<TF>{v.x + dv.x, v.y + dv.y, v.z + dv.z, v.w};
   }
 }
 
@@ -222,14 +279,14 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
 // k = rho_adv * alpha for the first divergence iteration.
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  const TF adv = density_change(c, S, s);
+  const Lane L = pair_lane(S.n);
+  const TF adv = density_change(c, S, L);
+  if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
-  const TF alpha = S.alpha[s] * (TF(1) / dt);
-  S.rho_adv[s] = adv;
-  S.alpha[s] = alpha;
-  S.kk[s] = adv * alpha;
+  const TF alpha = S.alpha[L.s] * (TF(1) / dt);
+  S.rho_adv[L.s] = adv;
+  S.alpha[L.s] = alpha;
+  S.kk[L.s] = adv * alpha;
 }
 
 template <class TF>
@@ -269,12 +326,12 @@ __device__ __forceinline__ void finish_iteration(Ctrl<TF>& C, double total, uint
 template <class TF>
 __global__ void __launch_bounds__(kBlock)
     k_df_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const Lane L = pair_lane(S.n);
+  const TF adv = density_change(c, S, L);
   double val = 0;
-  if (s < S.n) {
-    const TF adv = density_change(c, S, s);
-    S.rho_adv[s] = adv;
-    S.kk[s] = adv * S.alpha[s];
+  if (L.lead()) {
+    S.rho_adv[L.s] = adv;
+    S.kk[L.s] = adv * S.alpha[L.s];
     val = double(adv);
   }
   double total;
@@ -289,29 +346,30 @@ __global__ void __launch_bounds__(kBlock)
 template <class TF>
 __global__ void __launch_bounds__(kBlock)
     k_viscosity(Cn<TF> c, StepState<TF> S, int finish_div) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = s < S.n;
+  const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, da{0, 0, 0};
-  uint32_t m = 0;
-  if (act) {
-    xi = xyz(S.x[s]);
-    vi = xyz(S.v[s]);
-    const uint64_t desc = S.desc[s];
-    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
-      const vec3<TF> d = xi - ldx(S.x, t);
-      da += (c.visc * c.mass / __ldg(S.rho + t) * dot(d, gradW(c, d)) /
-             (length_sqr(d) + TF(0.01) * c.h2)) *
-            (vi - ldx(S.v, t));
-    });
-    m = S.mask[s];
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(S.x[L.s]);
+    vi = xyz(S.v[L.s]);
+    cnt = S.ncount[L.s];
   }
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
+    const vec3<TF> d = xi - ldx(S.x, t);
+    da += (c.visc * c.mass / __ldg(S.rho + t) * dot(d, gradW(c, d)) /
+           (length_sqr(d) + TF(0.01) * c.h2)) *
+          (vi - ldx(S.v, t));
+  }
+  da = group_sum(da);
+  const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
     if (!__syncthreads_or(mine)) continue;
     vec3<TF> fsum{0, 0, 0}, tsum{0, 0, 0};
     if (mine) {
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
       const vec3<TF> bxj = xyz(bn);
       const RigidDev<TF> rg = S.rigid[b];
       vec3<TF> nrm = bxj - xi;
@@ -350,12 +408,12 @@ __global__ void __launch_bounds__(kBlock)
     block_add_ft(S, b, fsum, tsum);
   }
   TF v2 = 0;
-  if (act) {
+  if (L.lead()) {
     const vec3<TF> a = c.g + da;
-    S.a[s] = vec4<TF>{a.x, a.y, a.z, TF(0)};
+    S.a[L.s] = vec4<TF>{a.x, a.y, a.z, TF(0)};
     if (finish_div) {
-      S.alpha[s] *= dt;
-      S.kappa_v[s] *= dt;
+      S.alpha[L.s] *= dt;
+      S.kappa_v[L.s] *= dt;
     }
     v2 = length_sqr(vi + a * dt);
   }
@@ -410,32 +468,32 @@ __global__ void k_integrate_np(StepState<TF> S) {
   if (s >= S.n) return;
   const TF dt = S.ctrl->dt;
   const vec4<TF> a = S.a[s];
-  vec4<TF> v = S.v[s];
+  const vec4<TF> v = S.v[s];
   S.v[s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
 }
 
 // warm_start_pressure_solve0 (runner.hpp:3430-3449).
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_p_warm0(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
+  const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
-  const TF adv = density_adv(c, S, s, dt);
-  const TF kp = S.kappa[s];
-  S.kappa[s] = adv > TF(1) ? TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt) : TF(0);
+  const TF adv = density_adv(c, S, L, dt);
+  if (!L.lead()) return;
+  const TF kp = S.kappa[L.s];
+  S.kappa[L.s] = adv > TF(1) ? TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt) : TF(0);
 }
 
 // compute_rho_adv (runner.hpp:3525-3541); also k for the first iteration.
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
+  const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
-  const TF adv = density_adv(c, S, s, dt);
-  const TF alpha = S.alpha[s] * (TF(1) / (dt * dt));
-  S.rho_adv[s] = adv;
-  S.alpha[s] = alpha;
-  S.kk[s] = (adv - TF(1)) * alpha;
+  const TF adv = density_adv(c, S, L, dt);
+  if (!L.lead()) return;
+  const TF alpha = S.alpha[L.s] * (TF(1) / (dt * dt));
+  S.rho_adv[L.s] = adv;
+  S.alpha[L.s] = alpha;
+  S.kk[L.s] = (adv - TF(1)) * alpha;
 }
 
 // compute_pressure_solve_density_error (runner.hpp:3590-3604); the mean is
@@ -443,12 +501,12 @@ __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<T
 template <class TF>
 __global__ void __launch_bounds__(kBlock)
     k_p_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const Lane L = pair_lane(S.n);
+  const TF adv = density_adv(c, S, L, S.ctrl->dt);
   double val = 0;
-  if (s < S.n) {
-    const TF adv = density_adv(c, S, s, S.ctrl->dt);
-    S.rho_adv[s] = adv;
-    S.kk[s] = (adv - TF(1)) * S.alpha[s];
+  if (L.lead()) {
+    S.rho_adv[L.s] = adv;
+    S.kk[L.s] = (adv - TF(1)) * S.alpha[L.s];
     val = double(adv) - 1.0;
   }
   double total;
@@ -487,56 +545,76 @@ __global__ void k_df_finish(StepState<TF> S, int density_solve, TF* __restrict__
 // kappa_v the last pressure.
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  const TF dt = S.ctrl->dt;
-  const vec4<TF> a = S.a[s];
-  vec4<TF> v = S.v[s];
-  S.v[s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
-  S.kappa_v[s] = S.kappa[s] * TF(0.5);
-  const vec3<TF> xi = xyz(S.x[s]);
-  const TF rho = S.rho[s], rho2 = rho * rho;
+  const Lane L = pair_lane(S.n);
+  vec3<TF> xi{0, 0, 0};
+  TF rho2 = 1;
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(S.x[L.s]);
+    const TF rho = S.rho[L.s];
+    rho2 = rho * rho;
+    cnt = S.ncount[L.s];
+  }
   vec3<TF> dii{0, 0, 0};
-  const uint64_t desc = S.desc[s];
-  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
     dii -= (c.vol / rho2) * gradW(c, xi - ldx(S.x, t));
-  });
-  for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+  }
+  dii = group_sum(dii);
+  if (!L.lead()) return;
+  const TF dt = S.ctrl->dt;
+  const vec4<TF> a = S.a[L.s];
+  const vec4<TF> v = S.v[L.s];
+  S.v[L.s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
+  S.kappa_v[L.s] = S.kappa[L.s] * TF(0.5);
+  for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
-    const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+    const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
     dii -= vec3<TF>{kg.x / rho2, kg.y / rho2, kg.z / rho2};
   }
   dii = dii * c.rho0;
-  S.dii[s] = vec4<TF>{dii.x, dii.y, dii.z, TF(0)};
+  S.dii[L.s] = vec4<TF>{dii.x, dii.y, dii.z, TF(0)};
 }
 
 // predict_advection1 (runner.hpp:2640-2690).  aii goes to kk.
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
+  const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
-  const vec3<TF> xi = xyz(S.x[s]), vi = xyz(S.v[s]), dii = xyz(S.dii[s]);
-  const TF rho = S.rho[s], rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
-  TF adv = rho / c.rho0, aii = 0;
-  const uint64_t desc = S.desc[s];
-  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
+  vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, dii{0, 0, 0};
+  TF rho = c.rho0;
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(S.x[L.s]);
+    vi = xyz(S.v[L.s]);
+    dii = xyz(S.dii[L.s]);
+    rho = S.rho[L.s];
+    cnt = S.ncount[L.s];
+  }
+  const TF rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
+  TF adv = 0, aii = 0;
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
     const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
     adv += dt * c.vol * dot(vi - ldx(S.v, t), gw);
     aii += c.vol * dot(dii - dji, gw);
-  });
-  for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+  }
+  adv = group_sum(adv);
+  aii = group_sum(aii);
+  if (!L.lead()) return;
+  adv += rho / c.rho0;
+  for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
-    const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
-    const vec3<TF> gw = xyz(S.bk[size_t(b) * S.n + s]);
+    const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
+    const vec3<TF> gw = xyz(S.bk[size_t(b) * S.n + L.s]);
     const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
     const vec3<TF> dji = (inv_rho2 * c.rho0) * gw;
     adv += dt * dot(vi - vj, gw);
     aii += dot(dii - dji, gw);
   }
-  S.rho_adv[s] = adv;
-  S.kk[s] = aii * c.rho0;
+  S.rho_adv[L.s] = adv;
+  S.kk[L.s] = aii * c.rho0;
 }
 
 // pressure_solve_iteration0 (runner.hpp:2691-2715).  On iterations after
@@ -545,20 +623,26 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
 // neighbors' pressure (equal to their last pressure after that copy).
 template <class TF>
 __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
+  const Lane L = pair_lane(S.n);
   const bool first = S.ctrl->it == 0;
   const TF* __restrict__ src = first ? S.kappa_v : S.kappa;
-  if (!first) S.kappa_v[s] = S.kappa[s];
-  const vec3<TF> xi = xyz(S.x[s]);
+  vec3<TF> xi{0, 0, 0};
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(S.x[L.s]);
+    cnt = S.ncount[L.s];
+  }
   vec3<TF> acc{0, 0, 0};
-  const uint64_t desc = S.desc[s];
-  for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
     const TF rj = __ldg(S.rho + t), rj2 = rj * rj;
     acc -= (c.vol / rj2 * src[t]) * gradW(c, xi - ldx(S.x, t));
-  });
+  }
+  acc = group_sum(acc);
+  if (!L.lead()) return;
+  if (!first) S.kappa_v[L.s] = S.kappa[L.s];
   acc = acc * c.rho0;
-  S.dij_pj[s] = vec4<TF>{acc.x, acc.y, acc.z, TF(0)};
+  S.dij_pj[L.s] = vec4<TF>{acc.x, acc.y, acc.z, TF(0)};
 }
 
 // pressure_solve_iteration1 (runner.hpp:2716-2772) and the mean of
@@ -566,38 +650,46 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
 template <class TF>
 __global__ void __launch_bounds__(kBlock)
     k_ii_iter1(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const Lane L = pair_lane(S.n);
+  const TF dt = S.ctrl->dt;
+  vec3<TF> xi{0, 0, 0}, dij_pj{0, 0, 0};
+  TF lp = 0, rho = c.rho0;
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(S.x[L.s]);
+    lp = S.kappa_v[L.s];
+    dij_pj = xyz(S.dij_pj[L.s]);
+    rho = S.rho[L.s];
+    cnt = S.ncount[L.s];
+  }
+  const TF rho2 = rho * rho, dpi = c.vol / rho2;
+  TF sum = 0;
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
+    const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+    const vec3<TF> dji = (dpi * c.rho0) * gw;
+    const vec3<TF> dji_pi = dji * lp;
+    sum += c.vol *
+           dot(dij_pj - ldx(S.dii, t) * __ldg(S.kappa_v + t) - (ldx(S.dij_pj, t) - dji_pi), gw);
+  }
+  sum = group_sum(sum);
   double val = 0;
-  if (s < S.n) {
-    const TF dt = S.ctrl->dt;
-    const vec3<TF> xi = xyz(S.x[s]);
-    const TF lp = S.kappa_v[s];
-    const vec3<TF> dij_pj = xyz(S.dij_pj[s]);
-    const TF rho = S.rho[s], rho2 = rho * rho, dpi = c.vol / rho2;
-    const TF bterm = TF(1) - S.rho_adv[s];
-    const TF dt2 = dt * dt;
-    const TF denom = S.kk[s] * dt2;
-    const TF omega = TF(2) / TF(3);
-    TF p = 0, sum = 0;
-    const uint64_t desc = S.desc[s];
-    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
-      const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
-      const vec3<TF> dji = (dpi * c.rho0) * gw;
-      const vec3<TF> dji_pi = dji * lp;
-      sum += c.vol * dot(dij_pj - ldx(S.dii, t) * __ldg(S.kappa_v + t) -
-                             (ldx(S.dij_pj, t) - dji_pi),
-                         gw);
-    });
-    for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+  if (L.lead()) {
+    for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
-      sum += dot(dij_pj, xyz(S.bk[size_t(b) * S.n + s]));
+      sum += dot(dij_pj, xyz(S.bk[size_t(b) * S.n + L.s]));
     }
     sum *= c.rho0;
+    const TF bterm = TF(1) - S.rho_adv[L.s];
+    const TF dt2 = dt * dt;
+    const TF denom = S.kk[L.s] * dt2;
+    const TF omega = TF(2) / TF(3);
+    TF p = 0;
     if (fabs(denom) > TF(1.0e-9))
       p = fmax((TF(1) - omega) * lp + omega / denom * (bterm - dt2 * sum), TF(0));
     const TF err = p == TF(0) ? TF(0) : (denom * p + sum * dt2 - bterm);
-    S.err[s] = err;
-    S.kappa[s] = p;
+    S.err[L.s] = err;
+    S.kappa[L.s] = p;
     val = double(err);
   }
   double total;
@@ -612,47 +704,48 @@ __global__ void __launch_bounds__(kBlock)
     k_ii_accel_finish(Cn<TF> c, StepState<TF> S, TF* __restrict__ x_ref, TF* __restrict__ v_ref,
                       TF* __restrict__ a_ref, TF* __restrict__ rho_ref, TF* __restrict__ p_ref,
                       TF* __restrict__ rho_adv_ref) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool act = s < S.n;
+  const Lane L = pair_lane(S.n);
   vec3<TF> ai{0, 0, 0}, xi{0, 0, 0};
   TF dpi = 0;
-  uint32_t m = 0;
-  if (act) {
-    xi = xyz(S.x[s]);
-    const TF rho = S.rho[s];
-    dpi = S.kappa[s] / (rho * rho);
-    const uint64_t desc = S.desc[s];
-    for_each_neighbor(S.rows, c.h, s, xi, desc, [&](const uint32_t t) {
-      const TF rj = __ldg(S.rho + t);
-      const TF dpj = __ldg(S.kappa + t) / (rj * rj);
-      ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldx(S.x, t));
-    });
-    m = S.mask[s];
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(S.x[L.s]);
+    const TF rho = S.rho[L.s];
+    dpi = S.kappa[L.s] / (rho * rho);
+    cnt = S.ncount[L.s];
   }
+  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
+    const uint32_t t = nbr_at(S, k, L.s);
+    const TF rj = __ldg(S.rho + t);
+    const TF dpj = __ldg(S.kappa + t) / (rj * rj);
+    ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldx(S.x, t));
+  }
+  ai = group_sum(ai);
+  const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
     if (!__syncthreads_or(mine)) continue;
     vec3<TF> f{0, 0, 0}, tq{0, 0, 0};
     if (mine) {
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
-      const vec3<TF> a = (c.rho0 * dpi) * xyz(S.bk[size_t(b) * S.n + s]);
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
+      const vec3<TF> a = (c.rho0 * dpi) * xyz(S.bk[size_t(b) * S.n + L.s]);
       f = c.mass * a;
       ai -= a;
       tq = cross(xyz(bn) - S.rigid[b].x, f);
     }
     block_add_ft(S, b, f, tq);
   }
-  if (!act) return;
+  if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
   const vec3<TF> ap = c.rho0 * ai;
-  const vec3<TF> v = xyz(S.v[s]) + ap * dt;
-  const uint32_t i = S.perm[s];
+  const vec3<TF> v = xyz(S.v[L.s]) + ap * dt;
+  const uint32_t i = S.perm[L.s];
   st3(x_ref, i, xi + v * dt);
   st3(v_ref, i, v);
-  if (a_ref) st3(a_ref, i, xyz(S.a[s]));
-  if (rho_ref) rho_ref[i] = S.rho[s];
-  if (p_ref) p_ref[i] = S.kappa[s];
-  if (rho_adv_ref) rho_adv_ref[i] = S.rho_adv[s];
+  if (a_ref) st3(a_ref, i, xyz(S.a[L.s]));
+  if (rho_ref) rho_ref[i] = S.rho[L.s];
+  if (p_ref) p_ref[i] = S.kappa[L.s];
+  if (rho_adv_ref) rho_adv_ref[i] = S.rho_adv[L.s];
 }
 
 // Per-body totals of the rigid slots (solver_df.hpp:346-353) in double and
@@ -759,14 +852,6 @@ int check_step_args(const typename FluidT<TF>::type* f, const al_consti* cni,
   ALB_CHECK_ARG(uint64_t(cni->grid_res[0]) * cni->grid_res[1] * cni->grid_res[2] < (1ull << 31),
                 "step: grid has too many cells");
   ALB_CHECK_ARG(cni->max_num_neighbors_per_particle > 0, "step: neighbor capacity is 0");
-  // compact lists: a neighbor's offset within its 3-cell row must fit a byte,
-  // and a row count must fit 7 bits
-  if (cni->max_num_particles_per_cell > (kMaxRowOffset + 1) / 3 ||
-      cni->max_num_neighbors_per_particle >= (1u << kRowBits)) {
-    set_error("step: max_num_particles_per_cell must be <= 85 and "
-              "max_num_neighbors_per_particle < 128");
-    return AL_ERR_UNSUPPORTED;
-  }
   ALB_CHECK_ARG(*dt > TF(0), "step: dt must be positive");
   return AL_OK;
 }
@@ -796,7 +881,7 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   S.n = n;
   S.nb = nb;
   S.cap = g.cap_nbr;
-  S.grid = blocks_for(n, kBlock) > 0 ? blocks_for(n, kBlock) : 1;
+  S.grid = pair_blocks(n) > 0 ? pair_blocks(n) : 1;  // grid of the pair passes
   // ---- buffers
   uint32_t* flags = nullptr;
   BodyDev<TF>* bodies_dev = nullptr;
@@ -815,8 +900,8 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     ALB_TRY(e->buf("sorted.dii", n, &S.dii));
     ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
   }
-  ALB_TRY(e->buf("nbr.desc", n, &S.desc));
-  ALB_TRY(e->buf("nbr.off", size_t(n) * g.cap_nbr, &S.off));
+  ALB_TRY(e->buf("nbr.list", size_t(n) * g.cap_nbr, &S.nbr));
+  ALB_TRY(e->buf("nbr.count", n, &S.ncount));
   ALB_TRY(e->buf("bnd.mask", n, &S.mask));
   ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
   ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
@@ -873,8 +958,8 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   ALB_LAUNCH(e, "grid_sort", 7, st,
              ALB_TRY(grid_build<TF>(e, c, g, f->particle_x, n, S.x, flags, gs, st)));
   S.perm = gs.perm;
-  S.rows = NeighborRows{S.desc, S.off, gs.cell_start, n, g};
   const uint32_t blocks = blocks_for(n, kBlock);
+  const uint32_t pblocks = pair_blocks(n);
   if (n > 0) {
     const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
     if (iisph)
@@ -896,45 +981,45 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
   ALB_LAUNCH(e, "neighbors", 1, st,
-             ALB_TRY(build_compact_neighbors<TF>(c, g, gs, S.x, sbk, S.desc, S.off, S.rho,
+             ALB_TRY(build_neighbors_density<TF>(c, g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
                                                  iisph ? nullptr : S.alpha, st)));
   const bool div = !iisph && sp->enable_divergence_solve;
   const bool den = iisph || sp->enable_density_solve;
   bool go = false;
   if (n > 0) {
     if (div) {
-      ALB_LAUNCH(e, "div_warm0", 1, st, k_df_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "div_warm0", 1, st, k_df_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "div_warm1", 1, st,
-                 k_kappa<TF, kDivWarm><<<blocks, kBlock, 0, st>>>(c, S));
+                 k_kappa<TF, kDivWarm><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "div_rho_adv", 1, st,
-                 k_df_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S));
+                 k_df_rho_adv_init<TF><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 0, 0, 0));
       go = sp->max_divergence_solve > 0;
       while (go) {
         ALB_LAUNCH(e, "div_iter", 1, st,
-                   k_kappa<TF, kDivIter><<<blocks, kBlock, 0, st>>>(c, S));
+                   k_kappa<TF, kDivIter><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "div_residual", 1, st,
-                   k_df_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0));
+                   k_df_residual<TF><<<pblocks, kBlock, 0, st>>>(c, S, 0, 0));
         ALB_TRY(read_keep_going(S, hflag, st, &go));
       }
     }
     ALB_LAUNCH(e, "viscosity", 1, st,
-               k_viscosity<TF><<<blocks, kBlock, 0, st>>>(c, S, div ? 1 : 0));
+               k_viscosity<TF><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0));
     if (!iisph) {
       ALB_LAUNCH(e, "integrate_np", 1, st, k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S));
       if (den) {
-        ALB_LAUNCH(e, "press_warm0", 1, st, k_p_warm0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "press_warm0", 1, st, k_p_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "press_warm1", 1, st,
-                   k_kappa<TF, kPressWarm><<<blocks, kBlock, 0, st>>>(c, S));
+                   k_kappa<TF, kPressWarm><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "press_rho_adv", 1, st,
-                   k_p_rho_adv_init<TF><<<blocks, kBlock, 0, st>>>(c, S));
+                   k_p_rho_adv_init<TF><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0));
         go = sp->max_density_solve > 0;
         while (go) {
           ALB_LAUNCH(e, "press_iter", 1, st,
-                     k_kappa<TF, kPressIter><<<blocks, kBlock, 0, st>>>(c, S));
+                     k_kappa<TF, kPressIter><<<pblocks, kBlock, 0, st>>>(c, S));
           ALB_LAUNCH(e, "press_residual", 1, st,
-                     k_p_residual<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0));
+                     k_p_residual<TF><<<pblocks, kBlock, 0, st>>>(c, S, 0, 0));
           ALB_TRY(read_keep_going(S, hflag, st, &go));
         }
       }
@@ -944,18 +1029,18 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
                      f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
                      f->particle_kappa_v, f->particle_density_adv));
     } else {
-      ALB_LAUNCH(e, "ii_predict0", 1, st, k_ii_predict0<TF><<<blocks, kBlock, 0, st>>>(c, S));
-      ALB_LAUNCH(e, "ii_predict1", 1, st, k_ii_predict1<TF><<<blocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "ii_predict0", 1, st, k_ii_predict0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "ii_predict1", 1, st, k_ii_predict1<TF><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0));
       go = sp->max_density_solve > 0;
       while (go) {
-        ALB_LAUNCH(e, "ii_iter0", 1, st, k_ii_iter0<TF><<<blocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "ii_iter0", 1, st, k_ii_iter0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "ii_iter1", 1, st,
-                   k_ii_iter1<TF><<<blocks, kBlock, 0, st>>>(c, S, 0, 0));
+                   k_ii_iter1<TF><<<pblocks, kBlock, 0, st>>>(c, S, 0, 0));
         ALB_TRY(read_keep_going(S, hflag, st, &go));
       }
       ALB_LAUNCH(e, "finish", 1, st,
-                 k_ii_accel_finish<TF><<<blocks, kBlock, 0, st>>>(
+                 k_ii_accel_finish<TF><<<pblocks, kBlock, 0, st>>>(
                      c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
                      f->particle_pressure, f->particle_density_adv));
     }

@@ -21,7 +21,6 @@
 #include "common.cuh"
 #include "engine.hpp"
 #include "grid.cuh"
-#include "neighbors.cuh"
 
 namespace alb {
 
@@ -61,9 +60,8 @@ struct StepState {
   TF* err = nullptr;      // IISPH density error
   vec4<TF>* dii = nullptr;
   vec4<TF>* dij_pj = nullptr;
-  uint64_t* desc = nullptr;  // compact neighbor lists (see NeighborRows)
-  uint8_t* off = nullptr;
-  NeighborRows rows{};
+  uint32_t* nbr = nullptr;
+  uint32_t* ncount = nullptr;
   uint32_t* mask = nullptr;
   vec4<TF>* bx = nullptr;
   vec4<TF>* bk = nullptr;
