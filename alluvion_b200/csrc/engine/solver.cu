@@ -76,7 +76,7 @@ __device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_
 // sums with warp shuffles (fixed order, deterministic) and lane 0 applies
 // the boundary terms and writes the results.  Shorter dependent-load chains
 // per thread keep more gathers in flight than one thread per particle.
-constexpr int kTPP = 4;
+constexpr int kTPP = 2;
 
 struct Lane {
   uint32_t s, sub;
