@@ -162,6 +162,8 @@ _SIGNATURES = {
     "al_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "al_last_error": (ctypes.c_char_p, []),
     "al_engine_synchronize": (ctypes.c_int, [_P, _P]),
+    "al_engine_set_graph_mode": (ctypes.c_int, [_P, ctypes.c_int]),
+    "al_engine_graph_stats": (ctypes.c_int, [_P, _P, _P]),
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_engine_reset_stats": (ctypes.c_int, [_P]),
     "al_engine_launch_count": (ctypes.c_int, [_P, _P]),
@@ -239,6 +241,17 @@ class Engine:
 
     def synchronize(self, stream=None):
         check(lib().al_engine_synchronize(self.handle, stream), "al_engine_synchronize")
+
+    def set_graph_mode(self, enable):
+        """Replay captured step graphs for repeated step configurations."""
+        check(lib().al_engine_set_graph_mode(self.handle, int(bool(enable))), "set_graph_mode")
+
+    def graph_stats(self):
+        """(step graphs captured, steps run by replaying one)."""
+        c, r = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().al_engine_graph_stats(self.handle, ctypes.byref(c), ctypes.byref(r)),
+              "graph_stats")
+        return c.value, r.value
 
     def set_profiling(self, enable):
         check(lib().al_engine_set_profiling(self.handle, int(bool(enable))), "set_profiling")

@@ -39,6 +39,7 @@ int al_engine::buffer(const char* name, size_t bytes, void** out) {
       return AL_ERR_ALLOC;
     }
     s.bytes = want;
+    ++generation;  // captured graphs hold the old pointers
   }
   *out = s.ptr;
   return AL_OK;
@@ -51,6 +52,7 @@ int al_engine::host_pinned(size_t bytes, void** out) {
     pinned_bytes = 0;
     ALB_CUDA(cudaMallocHost(&pinned, bytes));
     pinned_bytes = bytes;
+    ++generation;
   }
   *out = pinned;
   return AL_OK;
@@ -106,8 +108,25 @@ LaunchScope::~LaunchScope() {
 }
 }  // namespace alb
 
+int al_engine::capture_streams() {
+  if (!capture_stream)
+    ALB_CUDA(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking));
+  if (!body_stream) ALB_CUDA(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
+  return AL_OK;
+}
+
+void al_engine::drop_graphs() {
+  for (Graph& g : graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  graphs.clear();
+  seen_keys.clear();
+}
+
 al_engine::~al_engine() {
   cudaSetDevice(device);
+  drop_graphs();
+  if (capture_stream) cudaStreamDestroy(capture_stream);
+  if (body_stream) cudaStreamDestroy(body_stream);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);
@@ -174,6 +193,19 @@ int al_engine_synchronize(al_engine* engine, void* stream) {
   ALB_TRY(engine->activate());
   ALB_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
   return engine->flush_stats();
+}
+
+int al_engine_set_graph_mode(al_engine* engine, int enable) {
+  ALB_CHECK_ARG(engine != nullptr, "al_engine_set_graph_mode: engine is null");
+  engine->graph_mode = enable != 0;
+  return AL_OK;
+}
+
+int al_engine_graph_stats(al_engine* engine, uint64_t* captures, uint64_t* replays) {
+  ALB_CHECK_ARG(engine && captures && replays, "al_engine_graph_stats: null argument");
+  *captures = engine->graph_captures;
+  *replays = engine->graph_replays;
+  return AL_OK;
 }
 
 int al_engine_set_profiling(al_engine* engine, int enable) {

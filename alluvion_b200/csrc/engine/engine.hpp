@@ -96,6 +96,24 @@ struct al_engine {
   cudaEvent_t take_event();
   // Accumulates the elapsed times of recorded launches (after a sync).
   int flush_stats();
+
+  // Captured step graphs (al_engine_set_graph_mode).  `generation` counts
+  // scratch reallocations; a graph whose key (sizes, caller pointers,
+  // generation) no longer matches is recaptured.
+  struct Graph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t fixed_launches = 0;
+  };
+  bool graph_mode = true;
+  uint64_t generation = 0;
+  uint64_t graph_captures = 0, graph_replays = 0;
+  std::vector<std::vector<uint64_t>> seen_keys;  // keys run eagerly once
+  std::vector<Graph> graphs;
+  cudaStream_t capture_stream = nullptr;
+  cudaStream_t body_stream = nullptr;
+  int capture_streams();  // creates the two capture streams on first use
+  void drop_graphs();
   // pinned host staging (control readback, reports)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

@@ -866,97 +866,109 @@ int read_keep_going(const StepState<TF>& S, uint32_t* pinned, cudaStream_t st, b
   return AL_OK;
 }
 
+// Pinned host staging of one step: control block, body descriptors, rigid
+// state, the eager loop flag and the grid anomaly flags.  Every section
+// starts on a 64-byte boundary (RigidDev<double> holds 32-byte-aligned
+// vectors).  A captured graph copies from and to these addresses.
 template <class TF>
-int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
-             const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
-             typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
-             al_step_report* report, cudaStream_t st) {
-  ALB_TRY(check_step_args<TF>(f, cni, bodies, rigid, sp, dt));
-  ALB_TRY(e->activate());
-  const Cn<TF> c = to_cn<TF>(*cn);
-  const GridDims g = to_dims(*cni);
-  const uint32_t n = f->num_particles;
-  const uint32_t nb = g.nb;
-  StepState<TF> S;
-  S.n = n;
-  S.nb = nb;
-  S.cap = g.cap_nbr;
-  S.grid = pair_blocks(n) > 0 ? pair_blocks(n) : 1;  // grid of the pair passes
-  // ---- buffers
-  uint32_t* flags = nullptr;
-  BodyDev<TF>* bodies_dev = nullptr;
-  ALB_TRY(e->buf("flags", 4, &flags));
-  ALB_TRY(e->buf("sorted.x", n, &S.x));
-  ALB_TRY(e->buf("sorted.v", n, &S.v));
-  ALB_TRY(e->buf("sorted.a", n, &S.a));
-  ALB_TRY(e->buf("sorted.rho", n, &S.rho));
-  ALB_TRY(e->buf("sorted.alpha", n, &S.alpha));
-  ALB_TRY(e->buf("sorted.rho_adv", n, &S.rho_adv));
-  ALB_TRY(e->buf("sorted.kappa", n, &S.kappa));
-  ALB_TRY(e->buf("sorted.kappa_v", n, &S.kappa_v));
-  ALB_TRY(e->buf("sorted.kk", n, &S.kk));
-  if (iisph) {
-    ALB_TRY(e->buf("sorted.err", n, &S.err));
-    ALB_TRY(e->buf("sorted.dii", n, &S.dii));
-    ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
-  }
-  ALB_TRY(e->buf("nbr.list", size_t(n) * g.cap_nbr, &S.nbr));
-  ALB_TRY(e->buf("nbr.count", n, &S.ncount));
-  ALB_TRY(e->buf("bnd.mask", n, &S.mask));
-  ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
-  ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
-  ALB_TRY(e->buf("bodies", nb ? nb : 1, &bodies_dev));
-  ALB_TRY(e->buf("rigid", nb ? nb : 1, &S.rigid));
-  ALB_TRY(e->buf("ft", size_t(S.grid) * (nb ? nb : 1) * 6, &S.ft));
-  ALB_TRY(e->buf("red", S.grid, &S.red));
-  ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
-  S.bodies = bodies_dev;
-  // ---- host staging: bodies, rigid state, control block
-  void* pinned = nullptr;
-  // staging layout: every section starts on a 64-byte boundary (RigidDev
-  // holds 32-byte-aligned vectors for double)
+struct Staging {
+  Ctrl<TF>* hc = nullptr;
+  BodyDev<TF>* hb = nullptr;
+  RigidDev<TF>* hr = nullptr;
+  uint32_t* hflag = nullptr;
+  uint32_t* hf = nullptr;  // [4]
+};
+
+template <class TF>
+int staging(al_engine* e, Staging<TF>* out) {
   auto up64 = [](size_t b) { return (b + 63) & ~size_t(63); };
   const size_t off_b = up64(sizeof(Ctrl<TF>));
   const size_t off_r = off_b + up64(sizeof(BodyDev<TF>) * AL_MAX_BOUNDARIES);
   const size_t off_f = off_r + up64(sizeof(RigidDev<TF>) * AL_MAX_BOUNDARIES);
-  const size_t stage_bytes = off_f + 64;
-  ALB_TRY(e->host_pinned(stage_bytes, &pinned));
+  void* pinned = nullptr;
+  ALB_TRY(e->host_pinned(off_f + 128, &pinned));
   char* base = static_cast<char*>(pinned);  // cudaMallocHost: page aligned
-  Ctrl<TF>* hc = reinterpret_cast<Ctrl<TF>*>(base);
-  BodyDev<TF>* hb = reinterpret_cast<BodyDev<TF>*>(base + off_b);
-  RigidDev<TF>* hr = reinterpret_cast<RigidDev<TF>*>(base + off_r);
-  uint32_t* hflag = reinterpret_cast<uint32_t*>(base + off_f);
-  std::memset(hc, 0, sizeof(Ctrl<TF>));
-  hc->dt = *dt;
-  hc->length_scale = c.radius * TF(2);
-  hc->cfl = TF(sp->cfl);
-  hc->max_dt = TF(sp->max_dt);
-  hc->min_dt = TF(sp->min_dt);
-  hc->tol_div = double(TF(sp->density_change_tolerance));
-  hc->tol_den = double(TF(sp->density_error_tolerance));
-  hc->min_div = sp->min_divergence_solve;
-  hc->max_div = sp->max_divergence_solve;
-  hc->min_den = sp->min_density_solve;
-  hc->max_den = sp->max_density_solve;
-  hc->integrate_rigids = sp->integrate_rigids;
-  for (int k = 0; k < 3; ++k) hc->pile_gravity[k] = TF(sp->pile_gravity[k]);
-  for (uint32_t b = 0; b < nb; ++b) {
-    hb[b] = to_body_dev<TF>(bodies[b]);
-    ALB_TRY(validate_body(hb[b], true, true));
-    hr[b] = to_rigid_dev<TF>(rigid[b]);
-  }
-  ALB_CUDA(cudaMemcpyAsync(S.ctrl, hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
+  out->hc = reinterpret_cast<Ctrl<TF>*>(base);
+  out->hb = reinterpret_cast<BodyDev<TF>*>(base + off_b);
+  out->hr = reinterpret_cast<RigidDev<TF>*>(base + off_r);
+  out->hflag = reinterpret_cast<uint32_t*>(base + off_f);
+  out->hf = reinterpret_cast<uint32_t*>(base + off_f + 64);
+  return AL_OK;
+}
+
+// Everything one step launches, resolved on the host.
+template <class TF>
+struct StepPlan {
+  bool iisph = false, div = false, den = false;
+  Cn<TF> c;
+  GridDims g;
+  const typename FluidT<TF>::type* f = nullptr;
+  StepState<TF> S;
+  uint32_t* flags = nullptr;
+  BodyDev<TF>* bodies_dev = nullptr;
+  Staging<TF> io;
+};
+
+// Adds a device-driven WHILE loop at the current end of the capture on
+// `st`: `begin(h)` launches the kernel that sets the first condition,
+// `body(stream, h, 1)` launches one iteration whose last kernel sets the
+// next.  The body is captured on the engine's second stream into the
+// conditional node's own graph.
+template <class Begin, class Body>
+int capture_while(al_engine* e, cudaStream_t st, Begin&& begin, Body&& body) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  ALB_CUDA(cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps));
+  cudaGraphConditionalHandle h;
+  ALB_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault));
+  ALB_TRY(begin(h));
+  ALB_CUDA(cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  ALB_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
+  ALB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaStream_t bs = e->body_stream;
+  ALB_CUDA(cudaStreamBeginCaptureToGraph(bs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  const int rc = body(bs, h, 1);
+  cudaGraph_t captured = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(bs, &captured);
+  ALB_TRY(rc);
+  ALB_CUDA(end);
+  return AL_OK;
+}
+
+// Enqueues one whole step on `st`: staging uploads, grid, boundaries,
+// neighbors, the solves, write-back and the report readback.  With
+// `capture` the solver loops become conditional WHILE nodes (and `loops`
+// counts them); otherwise the host reads the loop flag every iteration.
+template <class TF>
+int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, int* loops) {
+  StepState<TF>& S = P.S;
+  const Cn<TF>& c = P.c;
+  const auto* f = P.f;
+  const uint32_t n = S.n, nb = S.nb;
+  const bool iisph = P.iisph, div = P.div, den = P.den;
+  ALB_CUDA(cudaMemcpyAsync(S.ctrl, P.io.hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
   if (nb) {
-    ALB_CUDA(cudaMemcpyAsync(bodies_dev, hb, sizeof(BodyDev<TF>) * nb, cudaMemcpyHostToDevice, st));
-    ALB_CUDA(cudaMemcpyAsync(S.rigid, hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(P.bodies_dev, P.io.hb, sizeof(BodyDev<TF>) * nb,
+                             cudaMemcpyHostToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(S.rigid, P.io.hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice,
+                             st));
   }
-  ALB_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), st));
+  ALB_CUDA(cudaMemsetAsync(P.flags, 0, 4 * sizeof(uint32_t), st));
   ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
   ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
   // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
   GridState gs;
   ALB_LAUNCH(e, "grid_sort", 7, st,
-             ALB_TRY(grid_build<TF>(e, c, g, f->particle_x, n, S.x, flags, gs, st)));
+             ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
   S.perm = gs.perm;
   const uint32_t blocks = blocks_for(n, kBlock);
   const uint32_t pblocks = pair_blocks(n);
@@ -974,18 +986,37 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk, &S.ctrl->rep.num_active_boundary_pairs};
   if (nb)
     ALB_LAUNCH(e, "boundary", 1, st,
-               ALB_TRY(sample_boundaries<TF>(c, bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
+               ALB_TRY(sample_boundaries<TF>(c, P.bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
                                              f->particle_boundary, f->particle_boundary_kernel,
                                              st)));
   else if (n)
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
   ALB_LAUNCH(e, "neighbors", 1, st,
-             ALB_TRY(build_neighbors_density<TF>(c, g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+             ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
                                                  iisph ? nullptr : S.alpha, st)));
-  const bool div = !iisph && sp->enable_divergence_solve;
-  const bool den = iisph || sp->enable_density_solve;
-  bool go = false;
+  // One solver loop: kernel `k_loop_begin` sets the first condition, `body`
+  // launches one iteration on the given stream.
+  auto solve = [&](int density_solve, uint32_t max_iter, auto&& body) -> int {
+    if (capture) {
+      ++*loops;
+      return capture_while(
+          e, st,
+          [&](cudaGraphConditionalHandle h) -> int {
+            ALB_LAUNCH(e, "loop_begin", 1, st,
+                       k_loop_begin<TF><<<1, 1, 0, st>>>(S, density_solve, h, 1));
+            return AL_OK;
+          },
+          body);
+    }
+    ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, density_solve, 0, 0));
+    bool go = max_iter > 0;
+    while (go) {
+      ALB_TRY(body(st, cudaGraphConditionalHandle(0), 0));
+      ALB_TRY(read_keep_going(S, P.io.hflag, st, &go));
+    }
+    return AL_OK;
+  };
   if (n > 0) {
     if (div) {
       ALB_LAUNCH(e, "div_warm0", 1, st, k_df_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
@@ -993,15 +1024,14 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
                  k_kappa<TF, kDivWarm><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "div_rho_adv", 1, st,
                  k_df_rho_adv_init<TF><<<pblocks, kBlock, 0, st>>>(c, S));
-      ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 0, 0, 0));
-      go = sp->max_divergence_solve > 0;
-      while (go) {
-        ALB_LAUNCH(e, "div_iter", 1, st,
-                   k_kappa<TF, kDivIter><<<pblocks, kBlock, 0, st>>>(c, S));
-        ALB_LAUNCH(e, "div_residual", 1, st,
-                   k_df_residual<TF><<<pblocks, kBlock, 0, st>>>(c, S, 0, 0));
-        ALB_TRY(read_keep_going(S, hflag, st, &go));
-      }
+      ALB_TRY(solve(0, P.io.hc->max_div,
+                    [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+                      ALB_LAUNCH(e, "div_iter", 1, s,
+                                 k_kappa<TF, kDivIter><<<pblocks, kBlock, 0, s>>>(c, S));
+                      ALB_LAUNCH(e, "div_residual", 1, s,
+                                 k_df_residual<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                      return AL_OK;
+                    }));
     }
     ALB_LAUNCH(e, "viscosity", 1, st,
                k_viscosity<TF><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0));
@@ -1013,15 +1043,14 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
                    k_kappa<TF, kPressWarm><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "press_rho_adv", 1, st,
                    k_p_rho_adv_init<TF><<<pblocks, kBlock, 0, st>>>(c, S));
-        ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0));
-        go = sp->max_density_solve > 0;
-        while (go) {
-          ALB_LAUNCH(e, "press_iter", 1, st,
-                     k_kappa<TF, kPressIter><<<pblocks, kBlock, 0, st>>>(c, S));
-          ALB_LAUNCH(e, "press_residual", 1, st,
-                     k_p_residual<TF><<<pblocks, kBlock, 0, st>>>(c, S, 0, 0));
-          ALB_TRY(read_keep_going(S, hflag, st, &go));
-        }
+        ALB_TRY(solve(1, P.io.hc->max_den,
+                      [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+                        ALB_LAUNCH(e, "press_iter", 1, s,
+                                   k_kappa<TF, kPressIter><<<pblocks, kBlock, 0, s>>>(c, S));
+                        ALB_LAUNCH(e, "press_residual", 1, s,
+                                   k_p_residual<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                        return AL_OK;
+                      }));
       }
       ALB_LAUNCH(e, "finish", 1, st,
                  k_df_finish<TF><<<blocks, kBlock, 0, st>>>(
@@ -1031,14 +1060,14 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     } else {
       ALB_LAUNCH(e, "ii_predict0", 1, st, k_ii_predict0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "ii_predict1", 1, st, k_ii_predict1<TF><<<pblocks, kBlock, 0, st>>>(c, S));
-      ALB_LAUNCH(e, "loop_begin", 1, st, k_loop_begin<TF><<<1, 1, 0, st>>>(S, 1, 0, 0));
-      go = sp->max_density_solve > 0;
-      while (go) {
-        ALB_LAUNCH(e, "ii_iter0", 1, st, k_ii_iter0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
-        ALB_LAUNCH(e, "ii_iter1", 1, st,
-                   k_ii_iter1<TF><<<pblocks, kBlock, 0, st>>>(c, S, 0, 0));
-        ALB_TRY(read_keep_going(S, hflag, st, &go));
-      }
+      ALB_TRY(solve(1, P.io.hc->max_den,
+                    [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+                      ALB_LAUNCH(e, "ii_iter0", 1, s,
+                                 k_ii_iter0<TF><<<pblocks, kBlock, 0, s>>>(c, S));
+                      ALB_LAUNCH(e, "ii_iter1", 1, s,
+                                 k_ii_iter1<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                      return AL_OK;
+                    }));
       ALB_LAUNCH(e, "finish", 1, st,
                  k_ii_accel_finish<TF><<<pblocks, kBlock, 0, st>>>(
                      c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
@@ -1048,17 +1077,187 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(S));
   ALB_CUDA(cudaGetLastError());
   // ---- read back: report, rigid state, anomaly flags
-  uint32_t hf[4];
-  ALB_CUDA(cudaMemcpyAsync(hc, S.ctrl, sizeof(Ctrl<TF>), cudaMemcpyDeviceToHost, st));
+  ALB_CUDA(cudaMemcpyAsync(P.io.hc, S.ctrl, sizeof(Ctrl<TF>), cudaMemcpyDeviceToHost, st));
   if (nb)
-    ALB_CUDA(cudaMemcpyAsync(hr, S.rigid, sizeof(RigidDev<TF>) * nb, cudaMemcpyDeviceToHost, st));
-  ALB_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    ALB_CUDA(cudaMemcpyAsync(P.io.hr, S.rigid, sizeof(RigidDev<TF>) * nb, cudaMemcpyDeviceToHost,
+                             st));
+  ALB_CUDA(cudaMemcpyAsync(P.io.hf, P.flags, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  return AL_OK;
+}
+
+// Captures one step into an executable graph.  Sets `*exec` to null (and
+// returns AL_OK) when a scratch buffer moved during the capture.
+template <class TF>
+int capture_step(al_engine* e, StepPlan<TF>& P, cudaGraphExec_t* exec, uint32_t* fixed) {
+  *exec = nullptr;
+  ALB_TRY(e->capture_streams());
+  cudaStream_t cs = e->capture_stream;
+  const uint64_t launches0 = e->launches;
+  const uint64_t gen0 = e->generation;
+  ALB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int loops = 0;
+  const int rc = enqueue_step<TF>(e, P, cs, true, &loops);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(cs, &graph);
+  const uint64_t captured = e->launches - launches0;
+  e->launches = launches0;
+  if (rc != AL_OK || end != cudaSuccess || e->generation != gen0) {
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != AL_OK) return rc;
+    ALB_CUDA(end);
+    return AL_OK;
+  }
+  const cudaError_t inst = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) *exec = nullptr;
+  ALB_CUDA(inst);
+  *fixed = uint32_t(captured - 2u * uint32_t(loops));
+  return AL_OK;
+}
+
+// Graph cache key: precision, method, enabled solves, scratch generation
+// and the raw bytes of the constants, grid descriptor and fluid buffer
+// table (their fields carry no padding).
+template <class TF>
+std::vector<uint64_t> step_key(const al_engine* e, const StepPlan<TF>& P,
+                               const typename FluidT<TF>::cn* cn, const al_consti* cni) {
+  std::vector<uint64_t> k{sizeof(TF), uint64_t(P.iisph), uint64_t(P.div), uint64_t(P.den),
+                          e->generation};
+  auto add = [&k](const void* p, size_t bytes) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < bytes; i += 8) {
+      uint64_t w = 0;
+      std::memcpy(&w, b + i, bytes - i < 8 ? bytes - i : 8);
+      k.push_back(w);
+    }
+  };
+  add(cn, sizeof(*cn));
+  add(cni, sizeof(*cni));
+  add(P.f, sizeof(*P.f));
+  return k;
+}
+
+constexpr size_t kMaxGraphs = 8;
+
+template <class TF>
+int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
+             const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
+             typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
+             al_step_report* report, cudaStream_t st) {
+  ALB_TRY(check_step_args<TF>(f, cni, bodies, rigid, sp, dt));
+  ALB_TRY(e->activate());
+  StepPlan<TF> P;
+  P.iisph = iisph;
+  P.div = !iisph && sp->enable_divergence_solve;
+  P.den = iisph || sp->enable_density_solve;
+  P.c = to_cn<TF>(*cn);
+  P.g = to_dims(*cni);
+  P.f = f;
+  const uint32_t n = f->num_particles;
+  const uint32_t nb = P.g.nb;
+  StepState<TF>& S = P.S;
+  S.n = n;
+  S.nb = nb;
+  S.cap = P.g.cap_nbr;
+  S.grid = pair_blocks(n) > 0 ? pair_blocks(n) : 1;  // grid of the pair passes
+  // ---- buffers
+  ALB_TRY(e->buf("flags", 4, &P.flags));
+  ALB_TRY(e->buf("sorted.x", n, &S.x));
+  ALB_TRY(e->buf("sorted.v", n, &S.v));
+  ALB_TRY(e->buf("sorted.a", n, &S.a));
+  ALB_TRY(e->buf("sorted.rho", n, &S.rho));
+  ALB_TRY(e->buf("sorted.alpha", n, &S.alpha));
+  ALB_TRY(e->buf("sorted.rho_adv", n, &S.rho_adv));
+  ALB_TRY(e->buf("sorted.kappa", n, &S.kappa));
+  ALB_TRY(e->buf("sorted.kappa_v", n, &S.kappa_v));
+  ALB_TRY(e->buf("sorted.kk", n, &S.kk));
+  if (iisph) {
+    ALB_TRY(e->buf("sorted.err", n, &S.err));
+    ALB_TRY(e->buf("sorted.dii", n, &S.dii));
+    ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
+  }
+  ALB_TRY(e->buf("nbr.list", size_t(n) * P.g.cap_nbr, &S.nbr));
+  ALB_TRY(e->buf("nbr.count", n, &S.ncount));
+  ALB_TRY(e->buf("bnd.mask", n, &S.mask));
+  ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
+  ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
+  ALB_TRY(e->buf("bodies", nb ? nb : 1, &P.bodies_dev));
+  ALB_TRY(e->buf("rigid", nb ? nb : 1, &S.rigid));
+  ALB_TRY(e->buf("ft", size_t(S.grid) * (nb ? nb : 1) * 6, &S.ft));
+  ALB_TRY(e->buf("red", S.grid, &S.red));
+  ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
+  S.bodies = P.bodies_dev;
+  // ---- host staging: control block, bodies, rigid state
+  ALB_TRY(staging<TF>(e, &P.io));
+  Ctrl<TF>* hc = P.io.hc;
+  std::memset(hc, 0, sizeof(Ctrl<TF>));
+  hc->dt = *dt;
+  hc->length_scale = P.c.radius * TF(2);
+  hc->cfl = TF(sp->cfl);
+  hc->max_dt = TF(sp->max_dt);
+  hc->min_dt = TF(sp->min_dt);
+  hc->tol_div = double(TF(sp->density_change_tolerance));
+  hc->tol_den = double(TF(sp->density_error_tolerance));
+  hc->min_div = sp->min_divergence_solve;
+  hc->max_div = sp->max_divergence_solve;
+  hc->min_den = sp->min_density_solve;
+  hc->max_den = sp->max_density_solve;
+  hc->integrate_rigids = sp->integrate_rigids;
+  for (int k = 0; k < 3; ++k) hc->pile_gravity[k] = TF(sp->pile_gravity[k]);
+  for (uint32_t b = 0; b < nb; ++b) {
+    P.io.hb[b] = to_body_dev<TF>(bodies[b]);
+    ALB_TRY(validate_body(P.io.hb[b], true, true));
+    P.io.hr[b] = to_rigid_dev<TF>(rigid[b]);
+  }
+  // ---- launch: a cached graph when this configuration ran before, else
+  // eagerly (the first run of a configuration sizes every scratch buffer)
+  const bool use_graph = e->graph_mode && !e->profiling && n > 0;
+  al_engine::Graph* graph = nullptr;
+  std::vector<uint64_t> key;
+  if (use_graph) {
+    key = step_key<TF>(e, P, cn, cni);
+    for (al_engine::Graph& gr : e->graphs)
+      if (gr.key == key) graph = &gr;
+    bool seen = false;
+    for (const auto& k : e->seen_keys) seen = seen || k == key;
+    if (!graph && seen) {
+      al_engine::Graph gr;
+      gr.key = key;
+      ALB_TRY(capture_step<TF>(e, P, &gr.exec, &gr.fixed_launches));
+      if (gr.exec) {
+        if (e->graphs.size() >= kMaxGraphs) {
+          cudaGraphExecDestroy(e->graphs.front().exec);
+          e->graphs.erase(e->graphs.begin());
+        }
+        e->graphs.push_back(std::move(gr));
+        graph = &e->graphs.back();
+        ++e->graph_captures;
+      }
+    }
+  }
+  if (graph) {
+    ALB_CUDA(cudaGraphLaunch(graph->exec, st));
+    ++e->graph_replays;
+  } else {
+    ALB_TRY(enqueue_step<TF>(e, P, st, false, nullptr));
+  }
   ALB_CUDA(cudaStreamSynchronize(st));
   e->flush_stats();
+  if (use_graph && !graph) {
+    // remember the configuration with the scratch generation it left
+    key = step_key<TF>(e, P, cn, cni);
+    if (e->seen_keys.size() >= 2 * kMaxGraphs) e->seen_keys.erase(e->seen_keys.begin());
+    e->seen_keys.push_back(std::move(key));
+  }
   al_step_report rep = hc->rep;
+  if (graph)
+    e->launches += graph->fixed_launches +
+                   2ull * (uint64_t(rep.num_divergence_solve) + rep.num_density_solve);
+  const uint32_t* hf = P.io.hf;
   for (int k = 0; k < 3; ++k) rep.grid_anomaly[k] = hf[k];
   if (n == 0) rep.dt = double(*dt);
   *dt = TF(rep.dt);
+  const RigidDev<TF>* hr = P.io.hr;
   for (uint32_t b = 0; b < nb; ++b) {
     for (int k = 0; k < 3; ++k) {
       rigid[b].x[k] = (&hr[b].x.x)[k];

@@ -78,6 +78,8 @@ def parse_args():
                    help="0 drops the 4 rigid bodies (profiling case)")
     p.add_argument("--container-resolution", type=int, default=64,
                    help="volume-map resolution of the container")
+    p.add_argument("--eager", action="store_true",
+                   help="launch every kernel from the host (no captured step graph)")
     return p.parse_args()
 
 
@@ -246,6 +248,7 @@ def engine_arm(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     engine = _capi.Engine(local)
+    engine.set_graph_mode(not args.eager)
     scene = build_scene(engine, rigid_bodies=args.rigid_bodies,
                         container_resolution=args.container_resolution)
     sp = scenes.solver_params()
@@ -260,8 +263,10 @@ def engine_arm(args):
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = engine.launch_count()
+    graphs0 = engine.graph_stats()
     ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch)
     launches = engine.launch_count() - launches0
+    graphs1 = engine.graph_stats()
     clk = clocks.stop()
     barrier(world)
     ms = max_over_ranks(ms, world, torch)
@@ -341,6 +346,8 @@ def engine_arm(args):
                    "mean_density_iterations": round(sum(r[1] for r in steps_reps) /
                                                     len(steps_reps), 3),
                    "active_boundary_pairs": int(pairs),
+                   "launch": "eager" if args.eager else "step graph (conditional WHILE loops)",
+                   "graph_replays_timed": graphs1[1] - graphs0[1],
                    "pass_ms_per_step": {k: round(v, 4) for k, v in pass_ms.items()}},
         "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},

@@ -227,6 +227,22 @@ AL_API const char* al_last_error(void);
 /* Blocks until all work the engine queued on `stream` has finished. */
 AL_API int al_engine_synchronize(al_engine* engine, void* stream);
 
+/* Step graphs.  With graph mode on (the default), the second and later
+ * al_*_step calls with the same constants, grid descriptor, fluid buffer
+ * table, body count and enabled solves replay one captured CUDA graph: the
+ * divergence and density loops are conditional WHILE nodes whose condition
+ * the residual kernels set on the device, so a step costs one graph launch
+ * and one synchronisation instead of one flag readback per solver
+ * iteration.  Body descriptors, rigid state, dt and the solver parameters
+ * are staged through pinned host memory on every call, so they may change
+ * between calls; changing any keyed argument (or a scratch buffer growing)
+ * makes the next call eager and the one after it capture again.  Steps run
+ * eagerly while profiling is on.  No reference counterpart (the reference
+ * launches every kernel from the host). */
+AL_API int al_engine_set_graph_mode(al_engine* engine, int enable);
+/* Number of step graphs captured and of steps run by replaying one. */
+AL_API int al_engine_graph_stats(al_engine* engine, uint64_t* captures, uint64_t* replays);
+
 /* Launch statistics, the counterpart of Runner's per-kernel event timing
  * (launch_stat_dict_, runner.hpp:4835-4859, 6306-6308).  While profiling
  * is on, every launch group is bracketed with CUDA events on its stream and
