@@ -332,7 +332,7 @@ int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const
   GridState gs;
   ALB_TRY(grid_build<TF>(e, c, g, x, n, xs, flags, gs, st));
   RefBoundaryKernel<TF> bk{boundary_kernel, gs.perm, n, g.nb};
-  ALB_TRY(build_neighbors_density<TF>(c, g, gs, xs, bk, nbr, ncount, rho, nullptr, st));
+  ALB_TRY(build_neighbors_density<TF>(c, g, gs, xs, bk, nbr, ncount, rho, nullptr, nullptr, st));
   ALB_TRY(export_neighbors<TF>(g, gs, xs, nbr, ncount, rho, neighbors, num_nbr, density, st));
   if (grid_anomaly)
     ALB_CUDA(cudaMemcpyAsync(grid_anomaly, flags, 3 * sizeof(uint32_t), cudaMemcpyDeviceToDevice,

@@ -68,14 +68,19 @@ struct SortedBoundaryKernel {
   }
 };
 
+// Element stride of the density copy `rho_rec` (the step's particle
+// records hold 8 reals per particle).
+constexpr size_t kRecStride = 8;
+
 // Builds nbr / ncount for all n sorted slots and the density
 // rho_s = rho0 (V W(0) + sum_j V W(x_sj) + boundary).  When `alpha` is
 // non-null also the DFSPH factor of compute_dfsph_factor
-// (runner.hpp:3123-3154).  Raises flags[2] on neighbor overflow.
+// (runner.hpp:3123-3154); when `rho_rec` is non-null also writes the
+// density to rho_rec[s * kRecStride].  Raises flags[2] on neighbor overflow.
 template <class TF, class BK>
 int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState& gs,
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
-                            TF* rho, TF* alpha, cudaStream_t st);
+                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st);
 
 // Writes reference-layout outputs in original particle order:
 // particle_neighbors [N][cap][4] {x_i - x_j, bits(j)} (if non-null),

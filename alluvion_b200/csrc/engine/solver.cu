@@ -22,6 +22,25 @@ __device__ __forceinline__ vec3<TF> ldx(const vec4<TF>* p, uint32_t i) {
   return xyz(__ldg(p + i));
 }
 
+// Record halves of particle s (see StepState::rec).
+template <class TF>
+__device__ __forceinline__ vec4<TF>& RX(const StepState<TF>& S, uint32_t s) {
+  return S.rec[2 * size_t(s)];
+}
+template <class TF>
+__device__ __forceinline__ vec4<TF>& RV(const StepState<TF>& S, uint32_t s) {
+  return S.rec[2 * size_t(s) + 1];
+}
+// Neighbor loads of the two halves through the read-only path.
+template <class TF>
+__device__ __forceinline__ vec4<TF> gX(const StepState<TF>& S, uint32_t t) {
+  return __ldg(S.rec + 2 * size_t(t));
+}
+template <class TF>
+__device__ __forceinline__ vec4<TF> gV(const StepState<TF>& S, uint32_t t) {
+  return __ldg(S.rec + 2 * size_t(t) + 1);
+}
+
 // Adds the block's contributions (f, t) for body b to the block's rigid
 // force/torque slot: warp trees, then warp partials in warp order.  All
 // threads of the block call it.  Deterministic.
@@ -113,6 +132,37 @@ __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, u
   return __ldcs(S.nbr + size_t(k) * S.n + s);
 }
 
+// Visits the lane's neighbors k = sub, sub + kTPP, ... < cnt in batches of
+// B: the batch's list entries are loaded first, then all their records,
+// then `f(t, x_j, v_j)` runs for each in list order (the order of a plain
+// loop, so sums are bit-identical to one).  Batching keeps B dependent
+// index -> record chains in flight per lane; it pays in the passes with
+// much arithmetic per neighbor (measured on the 1M-particle dam break:
+// B = 4 for k_kappa and viscosity; the velocity-divergence passes, with
+// little arithmetic per neighbor, run fastest unbatched).  `v_j` is loaded
+// only when V.
+template <int B, bool V, class TF, class F>
+__device__ __forceinline__ void for_each_neighbor(const StepState<TF>& S, const Lane& L,
+                                                  uint32_t cnt, F&& f) {
+  for (uint32_t k0 = L.sub; k0 < cnt; k0 += B * kTPP) {
+    uint32_t t[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const uint32_t k = k0 + b * kTPP;
+      t[b] = k < cnt ? nbr_at(S, k, L.s) : L.s;  // own slot: a valid address
+    }
+    vec4<TF> xj[B], vj[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      xj[b] = gX(S, t[b]);
+      vj[b] = V ? gV(S, t[b]) : vec4<TF>{0, 0, 0, 0};
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+      if (k0 + b * kTPP < cnt) f(t[b], xj[b], vj[b]);
+  }
+}
+
 // Sum over neighbors of V (v_i - v_j) . grad W_ij plus the boundary terms
 // (v_i - v_b) . (grad W V)_b: the shared body of compute_density_change
 // (runner.hpp:3192-3228) and compute_density_adv (runner.hpp:3493-3523).
@@ -122,11 +172,10 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
                                                   const Lane& L, vec3<TF> xi, vec3<TF> vi,
                                                   uint32_t cnt) {
   TF acc = 0;
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const vec3<TF> d = xi - ldx(S.x, t);
-    acc += c.vol * dot(vi - ldx(S.v, t), gradW(c, d));
-  }
+  for_each_neighbor<1, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const vec3<TF> d = xi - xyz(xj);
+    acc += c.vol * dot(vi - xyz(vj), gradW(c, d));
+  });
   acc = group_sum(acc);
   if (L.act) {
     for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
@@ -144,8 +193,8 @@ template <class TF>
 __device__ __forceinline__ TF density_change(const Cn<TF>& c, const StepState<TF>& S,
                                              const Lane& L) {
   const uint32_t cnt = L.act ? S.ncount[L.s] : 0u;
-  const vec3<TF> xi = L.act ? xyz(S.x[L.s]) : vec3<TF>{0, 0, 0};
-  const vec3<TF> vi = L.act ? xyz(S.v[L.s]) : vec3<TF>{0, 0, 0};
+  const vec3<TF> xi = L.act ? xyz(RX(S, L.s)) : vec3<TF>{0, 0, 0};
+  const vec3<TF> vi = L.act ? xyz(RV(S, L.s)) : vec3<TF>{0, 0, 0};
   TF adv = velocity_divergence(c, S, L, xi, vi, cnt);
   adv = fmax(adv, TF(0));
   if (cnt < 20) adv = 0;
@@ -156,8 +205,8 @@ template <class TF>
 __device__ __forceinline__ TF density_adv(const Cn<TF>& c, const StepState<TF>& S, const Lane& L,
                                           TF dt) {
   const uint32_t cnt = L.act ? S.ncount[L.s] : 0u;
-  const vec3<TF> xi = L.act ? xyz(S.x[L.s]) : vec3<TF>{0, 0, 0};
-  const vec3<TF> vi = L.act ? xyz(S.v[L.s]) : vec3<TF>{0, 0, 0};
+  const vec3<TF> xi = L.act ? xyz(RX(S, L.s)) : vec3<TF>{0, 0, 0};
+  const vec3<TF> vi = L.act ? xyz(RV(S, L.s)) : vec3<TF>{0, 0, 0};
   const TF delta = velocity_divergence(c, S, L, xi, vi, cnt);
   const TF rho = L.act ? S.rho[L.s] : c.rho0;
   return fmax(rho / c.rho0 + dt * delta, TF(1));
@@ -200,7 +249,8 @@ __global__ void k_gather_state(StepState<TF> S, const TF* __restrict__ v_ref,
   if (s >= S.n) return;
   const uint32_t i = S.perm[s];
   const vec3<TF> v = ld3(v_ref, i);
-  S.v[s] = vec4<TF>{v.x, v.y, v.z, TF(0)};
+  RX(S, s) = vec4<TF>{S.x[s].x, S.x[s].y, S.x[s].z, TF(0)};
+  RV(S, s) = vec4<TF>{v.x, v.y, v.z, TF(0)};  // rho follows from the build
   S.kappa[s] = k_ref ? k_ref[i] : TF(0);
   if (DF) S.kappa_v[s] = kv_ref ? kv_ref[i] : TF(0);
 }
@@ -213,7 +263,9 @@ __global__ void __launch_bounds__(kBlock) k_df_warm0(Cn<TF> c, StepState<TF> S) 
   if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
   const TF kv = S.kappa_v[L.s];
-  S.kappa_v[L.s] = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
+  const TF w = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
+  S.kappa_v[L.s] = w;
+  RX(S, L.s).w = w;
 }
 
 enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
@@ -226,23 +278,21 @@ template <class TF, int MODE>
 __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
   const Lane L = pair_lane(S.n);
-  const TF* __restrict__ ksrc =
-      MODE == kDivWarm ? S.kappa_v : (MODE == kPressWarm ? S.kappa : S.kk);
   const TF dt = S.ctrl->dt;
   TF ki = 0;
   vec3<TF> dv{0, 0, 0};
   uint32_t cnt = 0;
   vec3<TF> xi{0, 0, 0};
   if (L.act) {
-    ki = ksrc[L.s];
-    xi = xyz(S.x[L.s]);
+    const vec4<TF> r = RX(S, L.s);
+    ki = r.w;
+    xi = xyz(r);
     cnt = S.ncount[L.s];
   }
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const TF ksum = ki + __ldg(ksrc + t);
+  for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
+    const TF ksum = ki + xj.w;
     if (fabs(ksum) > c.eps) {
-      const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+      const vec3<TF> gw = gradW(c, xi - xyz(xj));
       if (kDiv) {
         const vec3<TF> gpj = (-c.vol) * gw;
         dv -= (dt * ksum) * gpj;
@@ -250,7 +300,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
         dv += (dt * ksum * c.vol) * gw;
       }
     }
-  }
+  });
   dv = group_sum(dv);
   const uint32_t m = (L.lead() && fabs(ki) > c.eps) ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
@@ -270,8 +320,8 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   if (L.lead()) {
     if (MODE == kDivIter) S.kappa_v[L.s] += ki;
     if (MODE == kPressIter) S.kappa[L.s] += ki;
-    const vec4<TF> v = S.v[L.s];
-    S.v[L.s] = vec4<TF>{v.x + dv.x, v.y + dv.y, v.z + dv.z, v.w};
+    const vec4<TF> v = RV(S, L.s);
+    RV(S, L.s) = vec4<TF>{v.x + dv.x, v.y + dv.y, v.z + dv.z, v.w};
   }
 }
 
@@ -286,7 +336,7 @@ __global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<
   const TF alpha = S.alpha[L.s] * (TF(1) / dt);
   S.rho_adv[L.s] = adv;
   S.alpha[L.s] = alpha;
-  S.kk[L.s] = adv * alpha;
+  RX(S, L.s).w = adv * alpha;
 }
 
 template <class TF>
@@ -331,7 +381,7 @@ __global__ void __launch_bounds__(kBlock)
   double val = 0;
   if (L.lead()) {
     S.rho_adv[L.s] = adv;
-    S.kk[L.s] = adv * S.alpha[L.s];
+    RX(S, L.s).w = adv * S.alpha[L.s];
     val = double(adv);
   }
   double total;
@@ -351,17 +401,16 @@ __global__ void __launch_bounds__(kBlock)
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, da{0, 0, 0};
   uint32_t cnt = 0;
   if (L.act) {
-    xi = xyz(S.x[L.s]);
-    vi = xyz(S.v[L.s]);
+    xi = xyz(RX(S, L.s));
+    vi = xyz(RV(S, L.s));
     cnt = S.ncount[L.s];
   }
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const vec3<TF> d = xi - ldx(S.x, t);
-    da += (c.visc * c.mass / __ldg(S.rho + t) * dot(d, gradW(c, d)) /
+  for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const vec3<TF> d = xi - xyz(xj);  // vj = {v, rho}
+    da += (c.visc * c.mass / vj.w * dot(d, gradW(c, d)) /
            (length_sqr(d) + TF(0.01) * c.h2)) *
-          (vi - ldx(S.v, t));
-  }
+          (vi - xyz(vj));
+  });
   da = group_sum(da);
   const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
@@ -468,8 +517,8 @@ __global__ void k_integrate_np(StepState<TF> S) {
   if (s >= S.n) return;
   const TF dt = S.ctrl->dt;
   const vec4<TF> a = S.a[s];
-  const vec4<TF> v = S.v[s];
-  S.v[s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
+  const vec4<TF> v = RV(S, s);
+  RV(S, s) = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
 }
 
 // warm_start_pressure_solve0 (runner.hpp:3430-3449).
@@ -480,7 +529,9 @@ __global__ void __launch_bounds__(kBlock) k_p_warm0(Cn<TF> c, StepState<TF> S) {
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
   const TF kp = S.kappa[L.s];
-  S.kappa[L.s] = adv > TF(1) ? TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt) : TF(0);
+  const TF w = adv > TF(1) ? TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt) : TF(0);
+  S.kappa[L.s] = w;
+  RX(S, L.s).w = w;
 }
 
 // compute_rho_adv (runner.hpp:3525-3541); also k for the first iteration.
@@ -493,7 +544,7 @@ __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<T
   const TF alpha = S.alpha[L.s] * (TF(1) / (dt * dt));
   S.rho_adv[L.s] = adv;
   S.alpha[L.s] = alpha;
-  S.kk[L.s] = (adv - TF(1)) * alpha;
+  RX(S, L.s).w = (adv - TF(1)) * alpha;
 }
 
 // compute_pressure_solve_density_error (runner.hpp:3590-3604); the mean is
@@ -506,7 +557,7 @@ __global__ void __launch_bounds__(kBlock)
   double val = 0;
   if (L.lead()) {
     S.rho_adv[L.s] = adv;
-    S.kk[L.s] = (adv - TF(1)) * S.alpha[L.s];
+    RX(S, L.s).w = (adv - TF(1)) * S.alpha[L.s];
     val = double(adv) - 1.0;
   }
   double total;
@@ -526,8 +577,8 @@ __global__ void k_df_finish(StepState<TF> S, int density_solve, TF* __restrict__
   if (s >= S.n) return;
   const uint32_t i = S.perm[s];
   const TF dt = S.ctrl->dt;
-  const vec3<TF> v = xyz(S.v[s]);
-  const vec3<TF> x = xyz(S.x[s]);
+  const vec3<TF> v = xyz(RV(S, s));
+  const vec3<TF> x = xyz(RX(S, s));
   st3(x_ref, i, x + dt * v);
   st3(v_ref, i, v);
   if (a_ref) st3(a_ref, i, xyz(S.a[s]));
@@ -550,23 +601,24 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
   TF rho2 = 1;
   uint32_t cnt = 0;
   if (L.act) {
-    xi = xyz(S.x[L.s]);
+    xi = xyz(RX(S, L.s));
     const TF rho = S.rho[L.s];
     rho2 = rho * rho;
     cnt = S.ncount[L.s];
   }
   vec3<TF> dii{0, 0, 0};
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    dii -= (c.vol / rho2) * gradW(c, xi - ldx(S.x, t));
-  }
+  for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
+    dii -= (c.vol / rho2) * gradW(c, xi - xyz(xj));
+  });
   dii = group_sum(dii);
   if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
   const vec4<TF> a = S.a[L.s];
-  const vec4<TF> v = S.v[L.s];
-  S.v[L.s] = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
-  S.kappa_v[L.s] = S.kappa[L.s] * TF(0.5);
+  const vec4<TF> v = RV(S, L.s);
+  RV(S, L.s) = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
+  const TF lp = S.kappa[L.s] * TF(0.5);
+  S.kappa_v[L.s] = lp;
+  RX(S, L.s).w = lp;  // pressure read by the first iteration
   for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
     const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
@@ -585,21 +637,20 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
   TF rho = c.rho0;
   uint32_t cnt = 0;
   if (L.act) {
-    xi = xyz(S.x[L.s]);
-    vi = xyz(S.v[L.s]);
+    xi = xyz(RX(S, L.s));
+    vi = xyz(RV(S, L.s));
     dii = xyz(S.dii[L.s]);
     rho = S.rho[L.s];
     cnt = S.ncount[L.s];
   }
   const TF rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
   TF adv = 0, aii = 0;
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+  for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const vec3<TF> gw = gradW(c, xi - xyz(xj));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
-    adv += dt * c.vol * dot(vi - ldx(S.v, t), gw);
+    adv += dt * c.vol * dot(vi - xyz(vj), gw);
     aii += c.vol * dot(dii - dji, gw);
-  }
+  });
   adv = group_sum(adv);
   aii = group_sum(aii);
   if (!L.lead()) return;
@@ -625,19 +676,19 @@ template <class TF>
 __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
   const Lane L = pair_lane(S.n);
   const bool first = S.ctrl->it == 0;
-  const TF* __restrict__ src = first ? S.kappa_v : S.kappa;
   vec3<TF> xi{0, 0, 0};
   uint32_t cnt = 0;
   if (L.act) {
-    xi = xyz(S.x[L.s]);
+    xi = xyz(RX(S, L.s));
     cnt = S.ncount[L.s];
   }
+  // the payload holds the last pressure on the first iteration
+  // (k_ii_predict0) and the pressure afterwards (k_ii_iter1)
   vec3<TF> acc{0, 0, 0};
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const TF rj = __ldg(S.rho + t), rj2 = rj * rj;
-    acc -= (c.vol / rj2 * src[t]) * gradW(c, xi - ldx(S.x, t));
-  }
+  for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const TF rj = vj.w, rj2 = rj * rj;
+    acc -= (c.vol / rj2 * xj.w) * gradW(c, xi - xyz(xj));
+  });
   acc = group_sum(acc);
   if (!L.lead()) return;
   if (!first) S.kappa_v[L.s] = S.kappa[L.s];
@@ -656,7 +707,7 @@ __global__ void __launch_bounds__(kBlock)
   TF lp = 0, rho = c.rho0;
   uint32_t cnt = 0;
   if (L.act) {
-    xi = xyz(S.x[L.s]);
+    xi = xyz(RX(S, L.s));
     lp = S.kappa_v[L.s];
     dij_pj = xyz(S.dij_pj[L.s]);
     rho = S.rho[L.s];
@@ -664,14 +715,13 @@ __global__ void __launch_bounds__(kBlock)
   }
   const TF rho2 = rho * rho, dpi = c.vol / rho2;
   TF sum = 0;
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const vec3<TF> gw = gradW(c, xi - ldx(S.x, t));
+  for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t t, const vec4<TF>& xj, const vec4<TF>&) {
+    const vec3<TF> gw = gradW(c, xi - xyz(xj));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
     const vec3<TF> dji_pi = dji * lp;
     sum += c.vol *
            dot(dij_pj - ldx(S.dii, t) * __ldg(S.kappa_v + t) - (ldx(S.dij_pj, t) - dji_pi), gw);
-  }
+  });
   sum = group_sum(sum);
   double val = 0;
   if (L.lead()) {
@@ -690,6 +740,7 @@ __global__ void __launch_bounds__(kBlock)
     const TF err = p == TF(0) ? TF(0) : (denom * p + sum * dt2 - bterm);
     S.err[L.s] = err;
     S.kappa[L.s] = p;
+    RX(S, L.s).w = p;  // pressure read by the next iteration
     val = double(err);
   }
   double total;
@@ -709,17 +760,16 @@ __global__ void __launch_bounds__(kBlock)
   TF dpi = 0;
   uint32_t cnt = 0;
   if (L.act) {
-    xi = xyz(S.x[L.s]);
+    xi = xyz(RX(S, L.s));
     const TF rho = S.rho[L.s];
     dpi = S.kappa[L.s] / (rho * rho);
     cnt = S.ncount[L.s];
   }
-  for (uint32_t k = L.sub; k < cnt; k += kTPP) {
-    const uint32_t t = nbr_at(S, k, L.s);
-    const TF rj = __ldg(S.rho + t);
+  for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const TF rj = vj.w;
     const TF dpj = __ldg(S.kappa + t) / (rj * rj);
-    ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldx(S.x, t));
-  }
+    ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - xyz(xj));
+  });
   ai = group_sum(ai);
   const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
@@ -738,7 +788,7 @@ __global__ void __launch_bounds__(kBlock)
   if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
   const vec3<TF> ap = c.rho0 * ai;
-  const vec3<TF> v = xyz(S.v[L.s]) + ap * dt;
+  const vec3<TF> v = xyz(RV(S, L.s)) + ap * dt;
   const uint32_t i = S.perm[L.s];
   st3(x_ref, i, xi + v * dt);
   st3(v_ref, i, v);
@@ -993,8 +1043,9 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
   ALB_LAUNCH(e, "neighbors", 1, st,
-             ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
-                                                 iisph ? nullptr : S.alpha, st)));
+             ALB_TRY(build_neighbors_density<TF>(
+                 c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho, iisph ? nullptr : S.alpha,
+                 reinterpret_cast<TF*>(S.rec) + 7, st)));
   // One solver loop: kernel `k_loop_begin` sets the first condition, `body`
   // launches one iteration on the given stream.
   auto solve = [&](int density_solve, uint32_t max_iter, auto&& body) -> int {
@@ -1163,15 +1214,15 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   // ---- buffers
   ALB_TRY(e->buf("flags", 4, &P.flags));
   ALB_TRY(e->buf("sorted.x", n, &S.x));
-  ALB_TRY(e->buf("sorted.v", n, &S.v));
+  ALB_TRY(e->buf("sorted.rec", size_t(n) * 2, &S.rec));
   ALB_TRY(e->buf("sorted.a", n, &S.a));
   ALB_TRY(e->buf("sorted.rho", n, &S.rho));
   ALB_TRY(e->buf("sorted.alpha", n, &S.alpha));
   ALB_TRY(e->buf("sorted.rho_adv", n, &S.rho_adv));
   ALB_TRY(e->buf("sorted.kappa", n, &S.kappa));
   ALB_TRY(e->buf("sorted.kappa_v", n, &S.kappa_v));
-  ALB_TRY(e->buf("sorted.kk", n, &S.kk));
   if (iisph) {
+    ALB_TRY(e->buf("sorted.kk", n, &S.kk));
     ALB_TRY(e->buf("sorted.err", n, &S.err));
     ALB_TRY(e->buf("sorted.dii", n, &S.dii));
     ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));

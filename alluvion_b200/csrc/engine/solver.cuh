@@ -48,15 +48,22 @@ struct Ctrl {
 template <class TF>
 struct StepState {
   uint32_t n = 0, nb = 0, cap = 0, grid = 0;
-  vec4<TF>* x = nullptr;
-  vec4<TF>* v = nullptr;
+  vec4<TF>* x = nullptr;    // sorted positions (grid sort, boundaries, build)
+  // Interleaved particle records of the pair passes: rec[2s] = {x, payload},
+  // rec[2s + 1] = {v, rho}.  One 32-byte sector (float) holds all a
+  // neighbor contributes to any DFSPH pass.  `payload` is the scalar the
+  // next k_kappa pass reads from its neighbors (the kappa_v / kappa warm
+  // start, or k = b alpha of the running iteration); the kernels that write
+  // it read only x from the same half, so the 4-byte store never races
+  // with a value another thread uses.
+  vec4<TF>* rec = nullptr;
   vec4<TF>* a = nullptr;
   TF* rho = nullptr;
   TF* alpha = nullptr;
   TF* rho_adv = nullptr;
   TF* kappa = nullptr;    // DFSPH kappa, IISPH pressure
   TF* kappa_v = nullptr;  // DFSPH kappa_v, IISPH last pressure
-  TF* kk = nullptr;       // per-iteration k = b * alpha (DFSPH), aii (IISPH)
+  TF* kk = nullptr;       // IISPH aii
   TF* err = nullptr;      // IISPH density error
   vec4<TF>* dii = nullptr;
   vec4<TF>* dij_pj = nullptr;
