@@ -1,0 +1,122 @@
+// build_kernel.cuh -- the neighbor-list build kernel with fused density
+// and DFSPH factor, shared by the standalone neighbor update and the solver
+// step (which adds a per-neighbor term through the EX hook).  Internal
+// linkage: each translation unit that launches it compiles its own copy.
+#pragma once
+
+#include "neighbors.cuh"
+
+namespace alb {
+
+// EX hook of k_build_neighbors that adds nothing.
+template <class TF>
+struct NoExtra {
+  static constexpr bool kOn = false;
+  __device__ __forceinline__ vec3<TF> self_v(uint32_t) const { return vec3<TF>{0, 0, 0}; }
+  __device__ __forceinline__ vec3<TF> vj(uint32_t) const { return vec3<TF>{0, 0, 0}; }
+  __device__ __forceinline__ void finish(uint32_t, uint32_t, TF, vec3<TF>) const {}
+};
+
+namespace {
+
+// Two phases per particle.  Phase 1 walks the 3x3 rows of z-contiguous
+// cells around the particle's cell and appends every candidate closer than
+// h to the list, in ascending sorted index; its accept branch is a store and
+// an increment, so the warp pays little when its lanes accept different
+// candidates (about 1 in 7 is accepted).  Phase 2 walks the compact list in
+// the same order and evaluates W (and grad W for the DFSPH factor) only
+// for neighbors, four list entries in flight at a time.  Both phases form
+// d and |d|^2 with the same rounded operations, so phase 2 sees the
+// distances phase 1 accepted.
+//
+// `EX` adds one more sum over the list to phase 2 (EX::kOn): it supplies
+// the particle's and the neighbors' velocities and receives
+// sum_j V (v_i - v_j) . grad W_ij, in list order, at the end.
+template <class TF, class BK, bool FACTOR, class EX>
+__global__ void __launch_bounds__(kBlock)
+    k_build_neighbors(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
+                      const vec4<TF>* __restrict__ xs, uint32_t n, BK bk,
+                      uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount,
+                      TF* __restrict__ rho, TF* __restrict__ alpha, TF* __restrict__ rho_rec,
+                      uint32_t* __restrict__ flags, EX ex) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const vec3<TF> xi = xyz(xs[s]);
+  int ip[3];
+  cell_coords(c.h, g, xi, ip);
+  const int z0 = max(ip[2] - 1, 0);
+  const int z1 = min(ip[2] + 1, int(g.res[2]) - 1);
+  uint32_t cnt = 0;
+  // ---- phase 1: candidates -> list
+  if (z0 <= z1) {
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int cx = ip[0] + dx;
+      if (cx < 0 || cx >= int(g.res[0])) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int cy = ip[1] + dy;
+        if (cy < 0 || cy >= int(g.res[1])) continue;
+        const uint32_t b = cell_start[cell_linear(g, cx, cy, z0)];
+        const uint32_t e = cell_start[cell_linear(g, cx, cy, z1) + 1];
+        for (uint32_t t = b; t < e; ++t) {
+          const TF d2 = dist2_rn(xi, xyz(__ldg(xs + t)));
+          if (d2 < c.h2 && t != s) {
+            if (cnt < g.cap_nbr) nbr[size_t(cnt) * n + s] = t;
+            ++cnt;
+          }
+        }
+      }
+    }
+  }
+  if (cnt > g.cap_nbr) {
+    flags[2] = 1u;
+    cnt = g.cap_nbr;
+  }
+  ncount[s] = cnt;
+  // ---- phase 2: density (+ factor, + EX) over the list, in list order
+  TF density = c.vol * c.w0;
+  TF sum_grad = 0;
+  vec3<TF> grad_i{0, 0, 0};
+  TF div = 0;
+  const vec3<TF> vi = ex.self_v(s);
+  constexpr uint32_t kB = 4;
+  for (uint32_t k0 = 0; k0 < cnt; k0 += kB) {
+    uint32_t t[kB];
+#pragma unroll
+    for (uint32_t q = 0; q < kB; ++q)  // this thread's own stores: plain loads
+      t[q] = k0 + q < cnt ? nbr[size_t(k0 + q) * n + s] : s;
+    vec3<TF> xj[kB], vj[kB];
+#pragma unroll
+    for (uint32_t q = 0; q < kB; ++q) {
+      xj[q] = xyz(__ldg(xs + t[q]));
+      vj[q] = ex.vj(t[q]);
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kB; ++q) {
+      if (k0 + q >= cnt) break;
+      density += c.vol * W_r2(c, dist2_rn(xi, xj[q]));
+      if (FACTOR || EX::kOn) {
+        const vec3<TF> d{sub_rn(xi.x, xj[q].x), sub_rn(xi.y, xj[q].y), sub_rn(xi.z, xj[q].z)};
+        const vec3<TF> gw = gradW(c, d);
+        if (FACTOR) {
+          const vec3<TF> gpj = (-c.vol) * gw;
+          sum_grad += length_sqr(gpj);
+          grad_i -= gpj;
+        }
+        if (EX::kOn) div += c.vol * dot(vi - vj[q], gw);
+      }
+    }
+  }
+  density += bk.density_term(s);
+  rho[s] = density * c.rho0;
+  if (rho_rec) rho_rec[size_t(s) * kRecStride] = density * c.rho0;
+  if (FACTOR) {
+    grad_i += bk.grad_term(s);
+    sum_grad += length_sqr(grad_i);
+    alpha[s] = sum_grad > c.eps ? TF(-1) / sum_grad : TF(0);
+  }
+  if (EX::kOn) ex.finish(s, cnt, div, vi);
+}
+
+}  // namespace
+
+}  // namespace alb

@@ -3,6 +3,7 @@
 #include <cstring>
 #include <vector>
 
+#include "build_kernel.cuh"
 #include "neighbors.cuh"
 #include "solver.cuh"
 
@@ -255,18 +256,33 @@ __global__ void k_gather_state(StepState<TF> S, const TF* __restrict__ v_ref,
   if (DF) S.kappa_v[s] = kv_ref ? kv_ref[i] : TF(0);
 }
 
-// warm_start_divergence_solve_0 (runner.hpp:3230-3249).
+// warm_start_divergence_solve_0 (runner.hpp:3230-3249), fused into the
+// neighbor build: the build's phase 2 sums the velocity divergence
+// sum_j V (v_i - v_j) . grad W_ij over the list; finish() adds the boundary
+// terms (compute_density_change, runner.hpp:3192-3228) and applies the
+// warm start.  The result also becomes the payload read by k_kappa.
 template <class TF>
-__global__ void __launch_bounds__(kBlock) k_df_warm0(Cn<TF> c, StepState<TF> S) {
-  const Lane L = pair_lane(S.n);
-  const TF adv = density_change(c, S, L);
-  if (!L.lead()) return;
-  const TF dt = S.ctrl->dt;
-  const TF kv = S.kappa_v[L.s];
-  const TF w = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
-  S.kappa_v[L.s] = w;
-  RX(S, L.s).w = w;
-}
+struct WarmDivergence {
+  static constexpr bool kOn = true;
+  StepState<TF> S;
+  __device__ __forceinline__ vec3<TF> self_v(uint32_t s) const { return xyz(RV(S, s)); }
+  __device__ __forceinline__ vec3<TF> vj(uint32_t t) const { return xyz(gV(S, t)); }
+  __device__ __forceinline__ void finish(uint32_t s, uint32_t cnt, TF acc, vec3<TF> vi) const {
+    for (uint32_t m = S.mask[s]; m; m &= m - 1) {
+      const uint32_t b = __ffs(m) - 1;
+      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+      acc += dot(vi - body_velocity(S.rigid[b], xyz(bn)), xyz(kg));
+    }
+    TF adv = fmax(acc, TF(0));
+    if (cnt < 20) adv = 0;
+    const TF dt = S.ctrl->dt;
+    const TF kv = S.kappa_v[s];
+    const TF w = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
+    S.kappa_v[s] = w;
+    RX(S, s).w = w;
+  }
+};
 
 enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 
@@ -1042,10 +1058,18 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   else if (n)
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
-  ALB_LAUNCH(e, "neighbors", 1, st,
-             ALB_TRY(build_neighbors_density<TF>(
-                 c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho, iisph ? nullptr : S.alpha,
-                 reinterpret_cast<TF*>(S.rec) + 7, st)));
+  TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
+  if (div && n > 0)
+    ALB_LAUNCH(e, "neighbors", 1, st,
+               (k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>>
+                <<<blocks_for(n, kBlock), kBlock, 0, st>>>(c, P.g, gs.cell_start, S.x, n, sbk,
+                                                           S.nbr, S.ncount, S.rho, S.alpha,
+                                                           rho_rec, gs.flags,
+                                                           WarmDivergence<TF>{S})));
+  else
+    ALB_LAUNCH(e, "neighbors", 1, st,
+               ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+                                                   iisph ? nullptr : S.alpha, rho_rec, st)));
   // One solver loop: kernel `k_loop_begin` sets the first condition, `body`
   // launches one iteration on the given stream.
   auto solve = [&](int density_solve, uint32_t max_iter, auto&& body) -> int {
@@ -1070,7 +1094,6 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   };
   if (n > 0) {
     if (div) {
-      ALB_LAUNCH(e, "div_warm0", 1, st, k_df_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "div_warm1", 1, st,
                  k_kappa<TF, kDivWarm><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "div_rho_adv", 1, st,
