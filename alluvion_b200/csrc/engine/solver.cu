@@ -42,6 +42,30 @@ __device__ __forceinline__ vec4<TF> gV(const StepState<TF>& S, uint32_t t) {
   return __ldg(S.rec + 2 * size_t(t) + 1);
 }
 
+// Both halves of record t through the read-only path with 256-bit loads
+// (sm_100): one load instruction per float record, two per double record,
+// instead of one per 16 bytes.  Records start on 32-byte (float) and
+// 64-byte (double) boundaries: the buffer is cudaMalloc-aligned and a
+// record is 2 x vec4.
+__device__ __forceinline__ void gXV(const StepState<float>& S, uint32_t t, vec4<float>& x,
+                                    vec4<float>& v) {
+  const vec4<float>* p = S.rec + 2 * size_t(t);
+  asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(v.x), "=f"(v.y), "=f"(v.z),
+                 "=f"(v.w)
+               : "l"(p));
+}
+__device__ __forceinline__ void gXV(const StepState<double>& S, uint32_t t, vec4<double>& x,
+                                    vec4<double>& v) {
+  const vec4<double>* p = S.rec + 2 * size_t(t);
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(x.x), "=d"(x.y), "=d"(x.z), "=d"(x.w)
+               : "l"(p));
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+               : "l"(p + 1));
+}
+
 // Adds the block's contributions (f, t) for body b to the block's rigid
 // force/torque slot: warp trees, then warp partials in warp order.  All
 // threads of the block call it.  Deterministic.
@@ -139,8 +163,8 @@ __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, u
 // loop, so sums are bit-identical to one).  Batching keeps B dependent
 // index -> record chains in flight per lane; it pays in the passes with
 // much arithmetic per neighbor (measured on the 1M-particle dam break:
-// B = 4 for k_kappa and viscosity; the velocity-divergence passes, with
-// little arithmetic per neighbor, run fastest unbatched).  `v_j` is loaded
+// B = 4 for k_kappa and viscosity, B = 2 for the velocity-divergence
+// passes, which have little arithmetic per neighbor).  `v_j` is loaded
 // only when V.
 template <int B, bool V, class TF, class F>
 __device__ __forceinline__ void for_each_neighbor(const StepState<TF>& S, const Lane& L,
@@ -155,8 +179,12 @@ __device__ __forceinline__ void for_each_neighbor(const StepState<TF>& S, const 
     vec4<TF> xj[B], vj[B];
 #pragma unroll
     for (int b = 0; b < B; ++b) {
-      xj[b] = gX(S, t[b]);
-      vj[b] = V ? gV(S, t[b]) : vec4<TF>{0, 0, 0, 0};
+      if (V) {
+        gXV(S, t[b], xj[b], vj[b]);
+      } else {
+        xj[b] = gX(S, t[b]);
+        vj[b] = vec4<TF>{0, 0, 0, 0};
+      }
     }
 #pragma unroll
     for (int b = 0; b < B; ++b)
@@ -173,7 +201,7 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
                                                   const Lane& L, vec3<TF> xi, vec3<TF> vi,
                                                   uint32_t cnt) {
   TF acc = 0;
-  for_each_neighbor<1, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
+  for_each_neighbor<2, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
     const vec3<TF> d = xi - xyz(xj);
     acc += c.vol * dot(vi - xyz(vj), gradW(c, d));
   });
