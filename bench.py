@@ -6,8 +6,13 @@ radius 0.05 m, 2 boxes of side 0.08 m, seeded, 64^3 cubic-Lagrange distance
 grids and volume maps), at 0.1 % density / divergence tolerance.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                  [--workload dambreak-1m|dambreak-32k|dambreak-8m] [--method df|ii]
 
-One step = one SolverDf step (solver_df.hpp:74-359) over the whole scene.
+One step = one SolverDf step (solver_df.hpp:74-359), or one SolverIi step
+(solver_ii.hpp:76-243) with --method ii, over the whole scene.  The default
+workload is the 1M-particle scene; dambreak-32k (32^3 lattice, r = 0.01 m,
+no rigid bodies) and dambreak-8m (256 x 128 x 256 lattice, r = 0.0025 m,
+sphere + box + torus with 128^3 grids) are the small and large variants.
 Multi-GPU runs are independent replicas of the scene (weak scaling): the
 step has no data-path exchange.  Rank 0 prints one JSON line.
 """
@@ -27,13 +32,29 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s at 0.1% avg density error"
 UNIT = "particle-steps/s"
-WORKLOAD = ("DFSPH dam break, 1,048,576 particles (128x64x128 lattice, r=0.005 m) in a "
-            "2x1x2 m box, 4 rigid bodies (2 spheres r=0.05, 2 boxes 0.08 m) with 64^3 "
-            "cubic-Lagrange SDF + volume maps, two-way coupled")
-LATTICE = (128, 64, 128)
-RADIUS = 0.005
-CONTAINER = (2.0, 1.0, 2.0)
 SEED = 0
+# Seeded synthetic dam breaks (a jittered lattice block in a box container
+# with two-way coupled rigid bodies above it); no dataset is involved.
+WORKLOADS = {
+    "dambreak-1m": dict(
+        lattice=(128, 64, 128), radius=0.005, container=(2.0, 1.0, 2.0), bodies="2s2b",
+        grid_resolution=64, container_resolution=64,
+        desc="dam break, 1,048,576 particles (128x64x128 lattice, r=0.005 m) in a 2x1x2 m box, "
+             "4 rigid bodies (2 spheres r=0.05, 2 boxes 0.08 m) with 64^3 cubic-Lagrange SDF + "
+             "volume maps, two-way coupled"),
+    "dambreak-32k": dict(
+        lattice=(32, 32, 32), radius=0.01, container=(1.0, 0.7, 0.7), bodies="none",
+        grid_resolution=64, container_resolution=64,
+        desc="dam break, 32,768 particles (32^3 lattice, r=0.01 m) in a 1.0x0.7x0.7 m box with "
+             "a 64^3 volume map"),
+    "dambreak-8m": dict(
+        lattice=(256, 128, 256), radius=0.0025, container=(2.0, 1.0, 2.0), bodies="sbt",
+        grid_resolution=128, container_resolution=128,
+        desc="dam break, 8,388,608 particles (256x128x256 lattice, r=0.0025 m) in a 2x1x2 m "
+             "tank, sphere r=0.1 + box 0.16 m + torus R=0.1 r=0.04 with 128^3 cubic-Lagrange "
+             "SDF + volume maps, two-way coupled"),
+}
+METHOD_NAME = {"df": "DFSPH", "ii": "IISPH"}
 
 # Compulsory per-particle state traffic per pass, float32 ("Model A": every
 # per-particle array read/written once per pass, neighbor gathers served
@@ -50,6 +71,14 @@ MODEL_A = {
     "press_warm": (110, 32),     # pressure warm start + rho_adv
     "press_iteration": (72, 32),  # pressure iteration (fused residual)
     "finish": (48, 0),           # integrate x
+    # IISPH, the same accounting: predict_advection0 reads x, rho, a, v, p and
+    # writes v, p_last, d_ii (92 B + 16 B per pair); predict_advection1 reads
+    # x, v, d_ii, rho and writes rho_adv, a_ii (60 B + 32 B per pair); one
+    # Jacobi iteration (both kernels fused) ~110 B; pressure accelerations +
+    # integration read x, rho, p, v, a and write x, v (80 B + 32 B per pair)
+    "ii_predict": (152, 48),
+    "ii_iteration": (110, 16),
+    "ii_finish": (80, 32),
 }
 # engine launch groups -> Model A pass
 GROUP_PASS = {
@@ -59,9 +88,11 @@ GROUP_PASS = {
     "viscosity": "viscosity", "integrate_np": "cfl_integrate", "press_warm0": "press_warm",
     "press_warm1": "press_warm", "press_rho_adv": "press_warm", "press_iter": "press_iteration",
     "press_residual": "press_iteration", "finish": "finish",
+    "ii_predict0": "ii_predict", "ii_predict1": "ii_predict", "ii_iter0": "ii_iteration",
+    "ii_iter1": "ii_iteration",
 }
 # how many times a pass runs per step: iteration passes once per iteration
-PASS_PER_STEP = {"div_iteration": "div", "press_iteration": "den"}
+PASS_PER_STEP = {"div_iteration": "div", "press_iteration": "den", "ii_iteration": "den"}
 
 
 def parse_args():
@@ -74,12 +105,14 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=20.0,
                    help="budget of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--rigid-bodies", type=int, default=4, choices=[0, 4],
-                   help="0 drops the 4 rigid bodies (profiling case)")
-    p.add_argument("--container-resolution", type=int, default=64,
-                   help="volume-map resolution of the container")
+    p.add_argument("--rigid-bodies", type=int, default=None, choices=[0],
+                   help="0 drops the workload's rigid bodies (profiling case)")
+    p.add_argument("--container-resolution", type=int, default=None,
+                   help="volume-map resolution of the container (default: the workload's)")
     p.add_argument("--eager", action="store_true",
                    help="launch every kernel from the host (no captured step graph)")
+    p.add_argument("--workload", choices=sorted(WORKLOADS), default="dambreak-1m")
+    p.add_argument("--method", choices=["df", "ii"], default="df")
     return p.parse_args()
 
 
@@ -150,13 +183,63 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_scene(engine, dtype=np.float32, rigid_bodies=4, container_resolution=64):
+def workload_bodies(wl):
+    """Rigid bodies of a workload (seeded positions above the fluid block)."""
+    from alluvion_b200 import _capi, scenes
+    if wl["bodies"] == "2s2b":
+        return scenes.seeded_rigid_bodies(SEED, wl["container"], wl["radius"],
+                                          resolution=wl["grid_resolution"])
+    if wl["bodies"] == "sbt":
+        rng = np.random.Generator(np.random.PCG64(SEED + 2000))
+        size = np.asarray(wl["container"], dtype=np.float64)
+        res = wl["grid_resolution"]
+        out = []
+        for k in range(3):
+            rho = rng.uniform(500.0, 2000.0)
+            pos = (rng.uniform(0.25, 0.75) * size[0], rng.uniform(0.75, 0.85) * size[1],
+                   rng.uniform(0.25, 0.75) * size[2])
+            if k == 0:
+                r = 0.1
+                mass = rho * 4.0 / 3.0 * np.pi * r ** 3
+                out.append(dict(shape=_capi.SHAPE_SPHERE, params=[r], sign=1.0, resolution=res,
+                                use_distance_grid=True, mass=mass,
+                                inertia=scenes.sphere_inertia(mass, r), x=pos))
+            elif k == 1:
+                w = (0.16,) * 3
+                mass = rho * 0.16 ** 3
+                out.append(dict(shape=_capi.SHAPE_BOX, params=scenes.box_params(w), sign=1.0,
+                                resolution=res, use_distance_grid=True, mass=mass,
+                                inertia=scenes.box_inertia(mass, w), x=pos))
+            else:
+                R, r = 0.1, 0.04
+                mass = rho * 2.0 * np.pi ** 2 * R * r * r
+                iy = mass * (R * R + 0.75 * r * r)
+                ixz = mass * (0.5 * R * R + 0.625 * r * r)
+                out.append(dict(shape=_capi.SHAPE_TORUS, params=[R, r], sign=1.0,
+                                resolution=res, use_distance_grid=True, mass=mass,
+                                inertia=(ixz, iy, ixz), x=pos))
+        return out
+    return []
+
+
+def build_scene(engine, workload="dambreak-1m", dtype=np.float32, rigid_bodies=None,
+                container_resolution=None):
     from alluvion_b200 import scenes
-    bodies = []
-    if rigid_bodies:
-        bodies = scenes.seeded_rigid_bodies(SEED, CONTAINER, RADIUS, resolution=64)
-    return scenes.dam_break(engine, dtype, LATTICE, RADIUS, CONTAINER, bodies, seed=SEED,
-                            volume_resolution=container_resolution)
+    wl = WORKLOADS[workload]
+    bodies = [] if rigid_bodies == 0 else workload_bodies(wl)
+    res = container_resolution or wl["container_resolution"]
+    return scenes.dam_break(engine, dtype, wl["lattice"], wl["radius"], wl["container"], bodies,
+                            seed=SEED, volume_resolution=res)
+
+
+def workload_name(args):
+    wl = WORKLOADS[args.workload]
+    name = METHOD_NAME[args.method] + " " + wl["desc"]
+    if args.rigid_bodies == 0 or args.container_resolution:
+        name += " [variant: %s rigid bodies, %d^3 container map]" % (
+            "no" if args.rigid_bodies == 0 else "with",
+            args.container_resolution or wl["container_resolution"])
+    return name
 
 
 def measured_peaks():
@@ -178,25 +261,45 @@ def committed_traffic():
     return None
 
 
-def timed_steps(scene, sp, dt, steps, torch, on_step=None):
+L2_BYTES = 126 * 2 ** 20
+# device bytes a step touches per particle (records, positions, scalars,
+# ~33-entry neighbor list, boundary state); below L2 the bench flushes
+STEP_BYTES_PER_PARTICLE = 300
+
+
+def timed_steps(scene, sp, dt, steps, torch, on_step=None, method="df", flush=None):
     """Runs `steps` steps between CUDA events on the launching (default)
-    stream, synchronised on both sides.  Returns (ms, dt, reports)."""
+    stream, synchronised on both sides.  With `flush` (a device buffer
+    larger than L2), every step is timed alone after the buffer is
+    rewritten (untimed), so no step starts with the previous one's data in
+    L2.  Returns (ms, dt, reports)."""
     reps = []
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
-    start.record()
+    total = 0.0
+    if flush is None:
+        start.record()
     for _ in range(steps):
+        if flush is not None:
+            flush.add_(1)
+            start.record()
         if on_step:
             on_step("before")
-        dt, rep = scene.step("df", sp, dt)
+        dt, rep = scene.step(method, sp, dt)
         if on_step:
             on_step("after")
+        if flush is not None:
+            stop.record()
+            torch.cuda.synchronize()
+            total += start.elapsed_time(stop)
         reps.append((rep.num_divergence_solve, rep.num_density_solve,
                      rep.mean_density_error, rep.num_active_boundary_pairs))
-    stop.record()
-    torch.cuda.synchronize()
-    return start.elapsed_time(stop), dt, reps
+    if flush is None:
+        stop.record()
+        torch.cuda.synchronize()
+        total = start.elapsed_time(stop)
+    return total, dt, reps
 
 
 def max_over_ranks(value, world, torch):
@@ -214,20 +317,28 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline(scene, sp, dt, budget_s, host_state, host_bodies):
-    """The oracle's DFSPH step on the host cores on a bounded sample of the
-    same scene (same initial state and grids)."""
+# per-particle state a step reads and writes besides x and v
+STATE = {"df": ("kappa", "kappa_v"), "ii": ("pressure",)}
+
+
+def oracle_state(host_state, method):
+    keys = ("x", "v", "density", "density_adv", "a") + STATE[method]
+    return {k: np.ascontiguousarray(host_state[k]).copy() for k in keys}
+
+
+def cpu_baseline(scene, sp, dt, budget_s, host_state, host_bodies, method="df"):
+    """The oracle's step on the host cores on a bounded sample of the same
+    scene (same initial state and grids)."""
     from oracle import binding as orc
     hb, keep, rigid = host_bodies
     nb = scene.num_boundaries
     bodies = (type(hb[0]) * nb)(*[hb[b] for b in range(nb)])
-    state = {k: np.ascontiguousarray(host_state[k]).copy()
-             for k in ("x", "v", "kappa", "kappa_v", "density", "density_adv", "a")}
+    state = oracle_state(host_state, method)
     rig = rigid.copy()
     steps = 0
     t0 = time.perf_counter()
     while True:
-        dt, _ = orc.run("df", scene.cn, scene.cni, bodies, rig, state, sp, dt, 1)
+        dt, _ = orc.run(method, scene.cn, scene.cni, bodies, rig, state, sp, dt, 1)
         steps += 1
         el = time.perf_counter() - t0
         # stop at the budget, or before a step that would overrun it by half
@@ -235,8 +346,9 @@ def cpu_baseline(scene, sp, dt, budget_s, host_state, host_bodies):
             break
     return {"value": scene.n * steps / el, "unit": UNIT, "cores": orc.num_threads(),
             "kind": "port",
-            "sample": "%d step(s) of the 1,048,576-particle scene from the same initial state "
-                      "(grids built by the engine, untimed), %.1f s" % (steps, el)}
+            "sample": "%d step(s) of the %s-particle scene from the same initial state "
+                      "(grids built by the engine, untimed), %.1f s" % (steps, format(scene.n, ","),
+                                                                      el)}
 
 
 def engine_arm(args):
@@ -250,7 +362,7 @@ def engine_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     engine = _capi.Engine(local)
     engine.set_graph_mode(not args.eager)
-    scene = build_scene(engine, rigid_bodies=args.rigid_bodies,
+    scene = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
                         container_resolution=args.container_resolution)
     sp = scenes.solver_params()
     dt = float(sp.max_dt)
@@ -258,14 +370,17 @@ def engine_arm(args):
     host_bodies = scene.host_bodies() if host_state is not None else None
     # warm-up
     for _ in range(args.warmup):
-        dt, _ = scene.step("df", sp, dt)
+        dt, _ = scene.step(args.method, sp, dt)
     # ---- device-resident timed region (value)
     barrier(world)
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = engine.launch_count()
     graphs0 = engine.graph_stats()
-    ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch)
+    flush = None
+    if scene.n * STEP_BYTES_PER_PARTICLE < L2_BYTES:
+        flush = torch.zeros(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch, method=args.method, flush=flush)
     launches = engine.launch_count() - launches0
     graphs1 = engine.graph_stats()
     clk = clocks.stop()
@@ -276,22 +391,23 @@ def engine_arm(args):
     # ---- end to end: host buffers in pinned memory, H2D + step + D2H per step
     n = scene.n
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    hx, hv = pin(scene.x.cpu().numpy()), pin(scene.v.cpu().numpy())
-    hk, hkv = pin(scene.kappa.cpu().numpy()), pin(scene.kappa_v.cpu().numpy())
-    h2d = (hx.numel() + hv.numel() + hk.numel() + hkv.numel()) * 4
-    d2h = (hx.numel() + hv.numel()) * 4
+    # host copies of the step's inputs (x, v and the warm-start state) in
+    # pinned memory: uploaded before and x, v read back after every step
+    dev_in = [scene.x, scene.v] + [getattr(scene, k) for k in STATE[args.method]]
+    host_in = [pin(t.cpu().numpy()) for t in dev_in]
+    h2d = sum(t.numel() * t.element_size() for t in host_in)
+    d2h = sum(t.numel() * t.element_size() for t in host_in[:2])
 
     def io(phase):
         if phase == "before":
-            scene.x.copy_(hx, non_blocking=True)
-            scene.v.copy_(hv, non_blocking=True)
-            scene.kappa.copy_(hk, non_blocking=True)
-            scene.kappa_v.copy_(hkv, non_blocking=True)
+            for d, h in zip(dev_in, host_in):
+                d.copy_(h, non_blocking=True)
         else:
-            hx.copy_(scene.x, non_blocking=True)
-            hv.copy_(scene.v, non_blocking=True)
+            for d, h in zip(dev_in[:2], host_in[:2]):
+                h.copy_(d, non_blocking=True)
     barrier(world)
-    ms_e2e, dt, _ = timed_steps(scene, sp, dt, args.steps, torch, on_step=io)
+    ms_e2e, dt, _ = timed_steps(scene, sp, dt, args.steps, torch, on_step=io,
+                                method=args.method, flush=flush)
     barrier(world)
     ms_e2e = max_over_ranks(ms_e2e, world, torch)
     e2e = total_particles * args.steps / (ms_e2e / 1e3)
@@ -299,7 +415,7 @@ def engine_arm(args):
     engine.reset_stats()
     engine.set_profiling(True)
     prof_steps = 3
-    _, dt, preps = timed_steps(scene, sp, dt, prof_steps, torch)
+    _, dt, preps = timed_steps(scene, sp, dt, prof_steps, torch, method=args.method)
     engine.set_profiling(False)
     stats = engine.kernel_stats()
     iters_div = sum(r[0] for r in preps) / prof_steps
@@ -322,7 +438,9 @@ def engine_arm(args):
     achieved = alg_bytes / (per_launch[dominant] / 1e3) / 1e9
     traffic = committed_traffic()
     tr = None
-    if traffic and traffic.get("pass") == dominant:
+    # the committed figure is per particle of a working set larger than L2;
+    # it scales with the particle count only while the step stays DRAM-resident
+    if traffic and traffic.get("pass") == dominant and flush is None:
         tr = traffic.get("dram_bytes_per_particle", 0) * n
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": tr,
@@ -330,18 +448,18 @@ def engine_arm(args):
                 "algorithmic_bytes_per_launch": int(alg_bytes),
                 "launch_ms": round(per_launch[dominant], 4)}
     steps_reps = reps
-    workload = WORKLOAD
-    if args.rigid_bodies == 0 or args.container_resolution != 64:
-        workload += " [variant: %d rigid bodies, %d^3 container map]" % (
-            args.rigid_bodies, args.container_resolution)
+    workload = workload_name(args)
+    bodies_desc = ", seeded rigid bodies" if scene.num_boundaries > 1 else ""
+    l2 = ("working set > 126 MB L2 (inputs larger than L2, no flush)" if flush is None else
+          "working set < L2: a 252 MB buffer is rewritten before every timed step (untimed)")
     result = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded jittered lattice, seeded rigid bodies)",
+        "data": "synthetic (seeded jittered lattice%s)" % bodies_desc,
         "config": {"workload": workload, "particles_per_gpu": n, "global_particles":
                    total_particles, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
+                   "l2": l2,
                    "mean_divergence_iterations": round(sum(r[0] for r in steps_reps) /
                                                        len(steps_reps), 3),
                    "mean_density_iterations": round(sum(r[1] for r in steps_reps) /
@@ -358,7 +476,7 @@ def engine_arm(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(scene, sp, float(sp.max_dt), args.cpu_seconds,
-                                              host_state, host_bodies)
+                                              host_state, host_bodies, args.method)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -379,22 +497,22 @@ def reference_arm(args):
     from oracle import binding as orc
     torch.cuda.set_device(local)
     engine = _capi.Engine(local)
-    scene = build_scene(engine)  # setup only: grids built on the device, untimed
+    # setup only: grids built on the device, untimed
+    scene = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
+                        container_resolution=args.container_resolution)
     hb, keep, rigid = scene.host_bodies()
     nb = scene.num_boundaries
     bodies = (type(hb[0]) * nb)(*[hb[b] for b in range(nb)])
-    st = scene.state()
-    state = {k: np.ascontiguousarray(st[k]).copy()
-             for k in ("x", "v", "kappa", "kappa_v", "density", "density_adv", "a")}
+    state = oracle_state(scene.state(), args.method)
     sp = scenes.solver_params()
     dt = float(sp.max_dt)
     # each benchmark step is one full oracle step; warm-up steps are shortened
     # to one so the run stays within minutes
     for _ in range(min(args.warmup, 1)):
-        dt, _ = orc.run("df", scene.cn, scene.cni, bodies, rigid, state, sp, dt, 1)
+        dt, _ = orc.run(args.method, scene.cn, scene.cni, bodies, rigid, state, sp, dt, 1)
     steps = max(1, min(args.steps, 5))
     t0 = time.perf_counter()
-    dt, _ = orc.run("df", scene.cn, scene.cni, bodies, rigid, state, sp, dt, steps)
+    dt, _ = orc.run(args.method, scene.cn, scene.cni, bodies, rigid, state, sp, dt, steps)
     el = time.perf_counter() - t0
     value = scene.n * steps / el
     print(json.dumps({
@@ -402,11 +520,13 @@ def reference_arm(args):
         "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1),
         "ms_per_step": round(el * 1e3 / steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded jittered lattice, seeded rigid bodies)",
-        "config": {"workload": WORKLOAD, "particles_per_gpu": scene.n},
+        "data": "synthetic (seeded jittered lattice%s)" % (
+            ", seeded rigid bodies" if scene.num_boundaries > 1 else ""),
+        "config": {"workload": workload_name(args), "particles_per_gpu": scene.n},
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": orc.num_threads(),
                          "kind": "port",
-                         "sample": "%d full steps of the 1,048,576-particle scene" % steps},
+                         "sample": "%d full steps of the %s-particle scene" % (
+                             steps, format(scene.n, ","))},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
