@@ -97,6 +97,30 @@ class SolverParams(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+WARM_NUM_FEATURES, WARM_HIDDEN, WARM_NUM_OUTPUTS, WARM_NUM_PARAMS = 12, 64, 2, 5122
+
+
+class WarmNet(ctypes.Structure):
+    """al_warm_net: device parameter pointer plus input/output scalings."""
+    _fields_ = [("params", ctypes.c_void_p),
+                ("feature_shift", ctypes.c_float * WARM_NUM_FEATURES),
+                ("feature_scale", ctypes.c_float * WARM_NUM_FEATURES),
+                ("output_scale", ctypes.c_float * WARM_NUM_OUTPUTS),
+                ("reserved", ctypes.c_uint32 * 2)]
+
+
+def make_warm_net(params, shift, scale, out_scale):
+    """WarmNet over a device tensor of WARM_NUM_PARAMS floats."""
+    w = WarmNet()
+    w.params = params.data_ptr()
+    for k in range(WARM_NUM_FEATURES):
+        w.feature_shift[k] = float(shift[k])
+        w.feature_scale[k] = float(scale[k])
+    for k in range(WARM_NUM_OUTPUTS):
+        w.output_scale[k] = float(out_scale[k])
+    return w
+
+
 class StepReport(ctypes.Structure):
     _fields_ = [("num_divergence_solve", ctypes.c_uint32),
                 ("num_density_solve", ctypes.c_uint32),
@@ -165,6 +189,7 @@ _SIGNATURES = {
     "al_engine_set_graph_mode": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_engine_graph_stats": (ctypes.c_int, [_P, _P, _P]),
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
+    "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
     "al_engine_reset_stats": (ctypes.c_int, [_P]),
     "al_engine_launch_count": (ctypes.c_int, [_P, _P]),
     "al_engine_kernel_stat": (ctypes.c_int, [_P, _U, ctypes.c_char_p, ctypes.c_size_t, _P, _P]),

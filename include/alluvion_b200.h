@@ -445,6 +445,48 @@ AL_API int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_co
                           al_rigid_f64* rigid, const al_solver_params* params, double* dt,
                           al_step_report* report, void* stream);
 
+/* ---------------------------------------------------- learned warm start
+ * No reference counterpart.  A per-particle MLP 12 -> 64 -> 64 -> 2 with
+ * GELU (tanh form), BF16 operands and FP32 accumulation on the tensor
+ * cores, predicts the converged kappa_v and kappa of a DFSPH step from
+ * features available when the step starts; the predictions replace the
+ * previous-step warm starts (runner.hpp:3230-3249, 3430-3449) under the
+ * same gates (rho_dot > 0, rho_adv > 1).  The solves' tolerances still
+ * decide convergence, so the result stays within tolerance and only the
+ * iteration counts change.
+ *
+ * Features (raw FP32, particle order), at the start of the step:
+ *   0 rho / rho0 - 1                1 rho_dot * dt (clamped >= 0; 0 if < 20 neighbors)
+ *   2 neighbors / 32                3 previous kappa_v (particle_kappa_v / dt)
+ *   4 previous kappa (particle_kappa / dt^2)
+ *   5 sum of boundary volumes / particle volume
+ *   6 |v|                            7 |v| dt / (2 r)
+ *   8 DFSPH factor (before the 1/dt scaling)
+ *   9 boundary density term sum_b (W V)_b
+ *  10 |sum_j V grad W_ij + sum_b (grad W V)_b| * 2 r     11 dt
+ * Targets: the converged kappa_v (particle_kappa_v / dt after the step) and
+ * kappa (particle_kappa / dt^2 after the step). */
+#define AL_WARM_NUM_FEATURES 12
+#define AL_WARM_HIDDEN 64
+#define AL_WARM_NUM_OUTPUTS 2
+/* flat FP32 parameters: W1[64][12], b1[64], W2[64][64], b2[64], W3[2][64], b3[2] */
+#define AL_WARM_NUM_PARAMS 5122
+
+typedef struct al_warm_net {
+  const float* params;       /* device, AL_WARM_NUM_PARAMS FP32 (rounded to BF16 for the MMAs) */
+  float feature_shift[AL_WARM_NUM_FEATURES]; /* input = (feature - shift) * scale */
+  float feature_scale[AL_WARM_NUM_FEATURES];
+  float output_scale[AL_WARM_NUM_OUTPUTS];   /* kappa_v = y0 * scale0, kappa = y1 * scale1 */
+  uint32_t reserved[2];
+} al_warm_net;
+
+/* out[p][0..1] = predicted {kappa_v, kappa} of features[p] (device [n][12]
+ * raw FP32) for p < n.  AL_ERR_TIMEOUT if a bounded tensor-core wait gave
+ * up. */
+AL_API int al_warm_net_forward_f32(al_engine* engine, const al_warm_net* net,
+                                   const float* features, uint32_t n, float* out,
+                                   void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
