@@ -190,6 +190,8 @@ _SIGNATURES = {
     "al_engine_graph_stats": (ctypes.c_int, [_P, _P, _P]),
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
+    "al_warm_net_gradient_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
+    "al_warm_net_adam_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _U, ctypes.c_float, _P]),
     "al_engine_reset_stats": (ctypes.c_int, [_P]),
     "al_engine_launch_count": (ctypes.c_int, [_P, _P]),
     "al_engine_kernel_stat": (ctypes.c_int, [_P, _U, ctypes.c_char_p, ctypes.c_size_t, _P, _P]),

@@ -487,6 +487,21 @@ AL_API int al_warm_net_forward_f32(al_engine* engine, const al_warm_net* net,
                                    const float* features, uint32_t n, float* out,
                                    void* stream);
 
+/* Loss L = 0.5 / n * sum_p |y_p - t_p|^2 of the network outputs y (before
+ * output_scale) against targets[p] / output_scale (targets: device [n][2]
+ * raw {kappa_v, kappa}), and dL/dparams into grad (device
+ * [AL_WARM_NUM_PARAMS]), with the tensor cores' own forward and backward
+ * kernels; the gradient is summed over the batch in a fixed order
+ * (deterministic).  loss: host out, may be NULL. */
+AL_API int al_warm_net_gradient_f32(al_engine* engine, const al_warm_net* net,
+                                    const float* features, const float* targets, uint32_t n,
+                                    float* grad, double* loss, void* stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8; step counts from 1) on
+ * the FP32 master parameters; m, v: device [AL_WARM_NUM_PARAMS] moments.
+ * Asynchronous on `stream`. */
+AL_API int al_warm_net_adam_f32(al_engine* engine, float* params, const float* grad, float* m,
+                                float* v, uint32_t step, float lr, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -8,9 +8,10 @@ computes its products on the tensor cores with BF16 operands and FP32
 accumulation; this restatement computes in float64 and rounds to BF16
 (round to nearest even) at exactly the points where the engine does:
 the normalised inputs, the weights, the hidden activations and, in the
-backward pass, the pre-activation gradients that feed tensor-core
-products.  `quantize=False` gives the plain float64 network, against
-which finite differences pin the analytic gradient.
+backward pass, the output and pre-activation gradients that feed
+tensor-core products (every weight and bias gradient is such a product).
+`quantize=False` gives the plain float64 network, against which finite
+differences pin the analytic gradient.
 
 Parameter layout (flat float32, as include/alluvion_b200.h states):
 W1[64][12], b1[64], W2[64][64], b2[64], W3[2][64], b3[2].
@@ -101,15 +102,18 @@ def loss_and_grad(params, xn, targets, quantize=True):
     loss = 0.5 / B * np.sum((y - t) ** 2)
     dy = (y - t) / B
     g = {}
-    g["W3"] = dy.T @ c["h2"]
-    g["b3"] = dy.sum(0)
+    # the engine forms every weight and bias gradient as a tensor-core
+    # product of BF16 operands: dy, dz2 and dz1 are rounded there
+    dyq = q(dy)
+    g["W3"] = dyq.T @ c["h2"]
+    g["b3"] = dyq.sum(0)
     dz2 = (dy @ c["W3"]) * gelu_grad(c["z2"])
-    g["b2"] = dz2.sum(0)
     dz2q = q(dz2)
+    g["b2"] = dz2q.sum(0)
     g["W2"] = dz2q.T @ c["h1"]
     dz1 = (dz2q @ c["W2"]) * gelu_grad(c["z1"])
-    g["b1"] = dz1.sum(0)
     dz1q = q(dz1)
+    g["b1"] = dz1q.sum(0)
     g["W1"] = dz1q.T @ c["x"]
     return loss, pack(g)
 
