@@ -121,6 +121,11 @@ def make_warm_net(params, shift, scale, out_scale):
     return w
 
 
+class WarmStart(ctypes.Structure):
+    """al_warm_start: optional network and optional feature output."""
+    _fields_ = [("net", ctypes.c_void_p), ("features_out", ctypes.c_void_p)]
+
+
 class StepReport(ctypes.Structure):
     _fields_ = [("num_divergence_solve", ctypes.c_uint32),
                 ("num_density_solve", ctypes.c_uint32),
@@ -190,6 +195,7 @@ _SIGNATURES = {
     "al_engine_graph_stats": (ctypes.c_int, [_P, _P, _P]),
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
+    "al_df_step_warm_f32": (ctypes.c_int, [_P] * 8 + [_P, _P, _P]),
     "al_warm_net_gradient_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
     "al_warm_net_adam_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _U, ctypes.c_float, _P]),
     "al_engine_reset_stats": (ctypes.c_int, [_P]),

@@ -8,13 +8,24 @@
 
 namespace alb {
 
+// What phase 2 of the build hands to the EX hook for particle s.
+template <class TF>
+struct BuildOut {
+  uint32_t cnt;    // neighbors in the list
+  TF div;          // sum_j V (v_i - v_j) . grad W_ij, list order
+  vec3<TF> vi;     // the particle's velocity (EX::self_v)
+  TF density;      // rho / rho0 (fluid + boundary terms)
+  TF alpha;        // DFSPH factor (0 without FACTOR)
+  TF grad_norm2;   // |sum_j V grad W_ij + sum_b (grad W V)_b|^2 (0 without FACTOR)
+};
+
 // EX hook of k_build_neighbors that adds nothing.
 template <class TF>
 struct NoExtra {
   static constexpr bool kOn = false;
   __device__ __forceinline__ vec3<TF> self_v(uint32_t) const { return vec3<TF>{0, 0, 0}; }
   __device__ __forceinline__ vec3<TF> vj(uint32_t) const { return vec3<TF>{0, 0, 0}; }
-  __device__ __forceinline__ void finish(uint32_t, uint32_t, TF, vec3<TF>) const {}
+  __device__ __forceinline__ void finish(uint32_t, const BuildOut<TF>&) const {}
 };
 
 namespace {
@@ -109,12 +120,15 @@ __global__ void __launch_bounds__(kBlock)
   density += bk.density_term(s);
   rho[s] = density * c.rho0;
   if (rho_rec) rho_rec[size_t(s) * kRecStride] = density * c.rho0;
+  TF a = 0, g2 = 0;
   if (FACTOR) {
     grad_i += bk.grad_term(s);
-    sum_grad += length_sqr(grad_i);
-    alpha[s] = sum_grad > c.eps ? TF(-1) / sum_grad : TF(0);
+    g2 = length_sqr(grad_i);
+    sum_grad += g2;
+    a = sum_grad > c.eps ? TF(-1) / sum_grad : TF(0);
+    alpha[s] = a;
   }
-  if (EX::kOn) ex.finish(s, cnt, div, vi);
+  if (EX::kOn) ex.finish(s, BuildOut<TF>{cnt, div, vi, density, a, g2});
 }
 
 }  // namespace

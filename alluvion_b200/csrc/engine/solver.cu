@@ -6,6 +6,7 @@
 #include "build_kernel.cuh"
 #include "neighbors.cuh"
 #include "solver.cuh"
+#include "warmnet.cuh"
 
 namespace alb {
 
@@ -289,28 +290,69 @@ __global__ void k_gather_state(StepState<TF> S, const TF* __restrict__ v_ref,
 // sum_j V (v_i - v_j) . grad W_ij over the list; finish() adds the boundary
 // terms (compute_density_change, runner.hpp:3192-3228) and applies the
 // warm start.  The result also becomes the payload read by k_kappa.
+//
+// With `feat` / `feat_out` set it also writes the learned warm start's 12
+// features (the list and units are those of al_warm_net in the C header) in
+// sorted / original particle order.
 template <class TF>
 struct WarmDivergence {
   static constexpr bool kOn = true;
   StepState<TF> S;
+  float* feat = nullptr;      // [n][12] sorted order
+  float* feat_out = nullptr;  // [n][12] original order
+  TF two_r = 0, vol = 0;
   __device__ __forceinline__ vec3<TF> self_v(uint32_t s) const { return xyz(RV(S, s)); }
   __device__ __forceinline__ vec3<TF> vj(uint32_t t) const { return xyz(gV(S, t)); }
-  __device__ __forceinline__ void finish(uint32_t s, uint32_t cnt, TF acc, vec3<TF> vi) const {
+  __device__ __forceinline__ void finish(uint32_t s, const BuildOut<TF>& o) const {
+    TF acc = o.div, bvol = 0, bden = 0;
     for (uint32_t m = S.mask[s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
       const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
       const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
-      acc += dot(vi - body_velocity(S.rigid[b], xyz(bn)), xyz(kg));
+      acc += dot(o.vi - body_velocity(S.rigid[b], xyz(bn)), xyz(kg));
+      bvol += bn.w;
+      bden += kg.w;
     }
     TF adv = fmax(acc, TF(0));
-    if (cnt < 20) adv = 0;
+    if (o.cnt < 20) adv = 0;
     const TF dt = S.ctrl->dt;
     const TF kv = S.kappa_v[s];
     const TF w = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
     S.kappa_v[s] = w;
     RX(S, s).w = w;
+    if (feat || feat_out) {
+      const TF speed = sqrt(length_sqr(o.vi));
+      const float f[AL_WARM_NUM_FEATURES] = {
+          float(o.density - TF(1)), float(adv * dt), float(TF(o.cnt) / TF(32)),
+          float(kv / dt), float(S.kappa[s] / (dt * dt)), float(bvol / vol),
+          float(speed), float(speed * dt / two_r), float(o.alpha), float(bden),
+          float(sqrt(o.grad_norm2) * two_r), float(dt)};
+      if (feat) {
+#pragma unroll
+        for (int k = 0; k < AL_WARM_NUM_FEATURES; ++k)
+          feat[size_t(s) * AL_WARM_NUM_FEATURES + k] = f[k];
+      }
+      if (feat_out) {
+        const uint32_t i = S.perm[s];
+#pragma unroll
+        for (int k = 0; k < AL_WARM_NUM_FEATURES; ++k)
+          feat_out[size_t(i) * AL_WARM_NUM_FEATURES + k] = f[k];
+      }
+    }
   }
 };
+
+// Learned divergence warm start: kappa_v = predicted kappa_v where the
+// reference's gate holds (rho_dot > 0, i.e. feature 1 > 0), else 0.
+template <class TF>
+__global__ void k_apply_warm_div(StepState<TF> S, const float* __restrict__ feat,
+                                 const float* __restrict__ pred) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF w = feat[size_t(s) * AL_WARM_NUM_FEATURES + 1] > 0.f ? TF(pred[2 * size_t(s)]) : TF(0);
+  S.kappa_v[s] = w;
+  RX(S, s).w = w;
+}
 
 enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 
@@ -566,14 +608,19 @@ __global__ void k_integrate_np(StepState<TF> S) {
 }
 
 // warm_start_pressure_solve0 (runner.hpp:3430-3449).
+// With `pred` (learned warm start) the predicted kappa replaces the
+// previous-step value under the same gate (rho_adv > 1).
 template <class TF>
-__global__ void __launch_bounds__(kBlock) k_p_warm0(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kBlock)
+    k_p_warm0(Cn<TF> c, StepState<TF> S, const float* __restrict__ pred) {
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
   const TF kp = S.kappa[L.s];
-  const TF w = adv > TF(1) ? TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt) : TF(0);
+  const TF warm = pred ? TF(pred[2 * size_t(L.s) + 1])
+                       : TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt);
+  const TF w = adv > TF(1) ? warm : TF(0);
   S.kappa[L.s] = w;
   RX(S, L.s).w = w;
 }
@@ -1001,6 +1048,13 @@ struct StepPlan {
   uint32_t* flags = nullptr;
   BodyDev<TF>* bodies_dev = nullptr;
   Staging<TF> io;
+  // learned warm start (float DFSPH steps): features in sorted order and
+  // the network's predictions; features_out in original order
+  bool learned = false;
+  WarmNetDev net{};
+  float* warm_feat = nullptr;
+  float* warm_feat_out = nullptr;
+  float* warm_pred = nullptr;
 };
 
 // Adds a device-driven WHILE loop at the current end of the capture on
@@ -1087,14 +1141,21 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
   TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
-  if (div && n > 0)
+  if (div && n > 0) {
+    WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol};
     ALB_LAUNCH(e, "neighbors", 1, st,
                (k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>>
                 <<<blocks_for(n, kBlock), kBlock, 0, st>>>(c, P.g, gs.cell_start, S.x, n, sbk,
                                                            S.nbr, S.ncount, S.rho, S.alpha,
-                                                           rho_rec, gs.flags,
-                                                           WarmDivergence<TF>{S})));
-  else
+                                                           rho_rec, gs.flags, wd)));
+    if (P.learned) {
+      ALB_LAUNCH(e, "warm_net", 1, st,
+                 ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, st)));
+      ALB_LAUNCH(e, "warm_apply", 1, st,
+                 (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(
+                     S, P.warm_feat, P.warm_pred)));
+    }
+  } else
     ALB_LAUNCH(e, "neighbors", 1, st,
                ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
                                                    iisph ? nullptr : S.alpha, rho_rec, st)));
@@ -1140,7 +1201,8 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     if (!iisph) {
       ALB_LAUNCH(e, "integrate_np", 1, st, k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S));
       if (den) {
-        ALB_LAUNCH(e, "press_warm0", 1, st, k_p_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+        ALB_LAUNCH(e, "press_warm0", 1, st,
+                   k_p_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S, P.warm_pred));
         ALB_LAUNCH(e, "press_warm1", 1, st,
                    k_kappa<TF, kPressWarm><<<pblocks, kBlock, 0, st>>>(c, S));
         ALB_LAUNCH(e, "press_rho_adv", 1, st,
@@ -1236,6 +1298,9 @@ std::vector<uint64_t> step_key(const al_engine* e, const StepPlan<TF>& P,
   add(cn, sizeof(*cn));
   add(cni, sizeof(*cni));
   add(P.f, sizeof(*P.f));
+  k.push_back(uint64_t(P.learned));
+  k.push_back(reinterpret_cast<uint64_t>(P.warm_feat_out));
+  if (P.learned) add(&P.net, sizeof(P.net));
   return k;
 }
 
@@ -1245,7 +1310,7 @@ template <class TF>
 int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
              const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
              typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
-             al_step_report* report, cudaStream_t st) {
+             al_step_report* report, cudaStream_t st, const al_warm_start* warm = nullptr) {
   ALB_TRY(check_step_args<TF>(f, cni, bodies, rigid, sp, dt));
   ALB_TRY(e->activate());
   StepPlan<TF> P;
@@ -1289,6 +1354,20 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   ALB_TRY(e->buf("red", S.grid, &S.red));
   ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
   S.bodies = P.bodies_dev;
+  if (warm && (warm->net || warm->features_out)) {
+    if (sizeof(TF) != 4 || iisph || !P.div) {
+      set_error("learned warm start: float32 DFSPH steps with the divergence solve only");
+      return AL_ERR_UNSUPPORTED;
+    }
+    P.warm_feat_out = warm->features_out;
+    if (warm->net) {
+      ALB_CHECK_ARG(warm->net->params != nullptr, "learned warm start: params is null");
+      P.learned = true;
+      P.net = to_warm_dev(*warm->net);
+      ALB_TRY(e->buf("warm.feat", size_t(n) * AL_WARM_NUM_FEATURES, &P.warm_feat));
+      ALB_TRY(e->buf("warm.pred", size_t(n) * AL_WARM_NUM_OUTPUTS, &P.warm_pred));
+    }
+  }
   // ---- host staging: control block, bodies, rigid state
   ALB_TRY(staging<TF>(e, &P.io));
   Ctrl<TF>* hc = P.io.hc;
@@ -1375,6 +1454,10 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   if (hf[0]) return AL_ERR_OUT_OF_GRID;
   if (hf[1]) return AL_ERR_CELL_OVERFLOW;
   if (hf[2]) return AL_ERR_NEIGHBOR_OVERFLOW;
+  if (hf[3]) {
+    set_error("learned warm start: a tensor-core wait timed out");
+    return AL_ERR_TIMEOUT;
+  }
   return AL_OK;
 }
 
@@ -1401,6 +1484,15 @@ int al_df_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* c
   ALB_CHECK_ARG(engine && cn, "al_df_step: null argument");
   return run_step<double>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
                           static_cast<cudaStream_t>(stream));
+}
+int al_df_step_warm_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                        const al_fluid_f32* fluid, const al_body_f32* bodies,
+                        al_rigid_f32* rigid, const al_solver_params* params,
+                        const al_warm_start* warm, float* dt, al_step_report* report,
+                        void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_df_step_warm_f32: null argument");
+  return run_step<float>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
+                         static_cast<cudaStream_t>(stream), warm);
 }
 int al_ii_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
                    const al_fluid_f32* fluid, const al_body_f32* bodies, al_rigid_f32* rigid,

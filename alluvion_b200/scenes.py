@@ -287,17 +287,27 @@ class DeviceScene:
             bufs["particle_boundary"], bufs["particle_boundary_kernel"] = export_boundary
         return _capi.make_fluid(self.n, **bufs)
 
-    def step(self, method, sp, dt, report=None, stream=None, allow=()):
-        """One DFSPH ('df') or IISPH ('ii') step; returns (dt_out, report)."""
+    def step(self, method, sp, dt, report=None, stream=None, allow=(), warm=None):
+        """One DFSPH ('df') or IISPH ('ii') step; returns (dt_out, report).
+        warm: an _capi.WarmStart for the float32 DFSPH step with the learned
+        warm start and/or feature output (al_df_step_warm_f32)."""
         T = self.dtype.type
         dt_c = (ctypes_real(self.dtype))(T(dt))
         rep = report if report is not None else _capi.StepReport()
         fluid = self.fluid()
+        bodies = _capi.ptr(self.bodies) if self.num_boundaries else None
+        rigid = _capi.ptr(self.rigid) if self.num_boundaries else None
+        if warm is not None:
+            assert method == "df" and self.sfx == "f32", "learned warm start: float32 DFSPH"
+            status = _capi.lib().al_df_step_warm_f32(
+                self.engine.handle, _capi.ptr(self.cn), _capi.ptr(self.cni), _capi.ptr(fluid),
+                bodies, rigid, _capi.ptr(sp), _capi.ptr(warm), _capi.ptr(dt_c), _capi.ptr(rep),
+                stream)
+            _capi.check(status, "al_df_step_warm_f32", allow=allow)
+            return float(dt_c.value), rep
         fn = getattr(_capi.lib(), "al_%s_step_%s" % (method, self.sfx))
         status = fn(self.engine.handle, _capi.ptr(self.cn), _capi.ptr(self.cni), _capi.ptr(fluid),
-                    _capi.ptr(self.bodies) if self.num_boundaries else None,
-                    _capi.ptr(self.rigid) if self.num_boundaries else None,
-                    _capi.ptr(sp), _capi.ptr(dt_c), _capi.ptr(rep), stream)
+                    bodies, rigid, _capi.ptr(sp), _capi.ptr(dt_c), _capi.ptr(rep), stream)
         _capi.check(status, "al_%s_step" % method, allow=allow)
         return float(dt_c.value), rep
 

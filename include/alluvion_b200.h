@@ -502,6 +502,23 @@ AL_API int al_warm_net_gradient_f32(al_engine* engine, const al_warm_net* net,
 AL_API int al_warm_net_adam_f32(al_engine* engine, float* params, const float* grad, float* m,
                                 float* v, uint32_t step, float lr, void* stream);
 
+/* Warm-start options of al_df_step_warm_f32. */
+typedef struct al_warm_start {
+  const al_warm_net* net; /* NULL: the reference's previous-step warm starts */
+  float* features_out;    /* NULL or device [N][12]: this step's features, particle order */
+} al_warm_start;
+
+/* al_df_step_f32 with the learned warm start (warm->net) and/or the
+ * features of the step written out for training (warm->features_out).
+ * Float32 DFSPH with the divergence solve enabled only
+ * (AL_ERR_UNSUPPORTED otherwise); AL_ERR_TIMEOUT if a bounded tensor-core
+ * wait gave up (the step's outputs are then invalid). */
+AL_API int al_df_step_warm_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                               const al_fluid_f32* fluid, const al_body_f32* bodies,
+                               al_rigid_f32* rigid, const al_solver_params* params,
+                               const al_warm_start* warm, float* dt, al_step_report* report,
+                               void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

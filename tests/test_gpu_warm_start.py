@@ -1,0 +1,88 @@
+"""The learned warm start inside the DFSPH step (al_df_step_warm_f32):
+the features the step exports, and what a network trained with the
+engine's own kernels gains over the reference's previous-step warm start.
+
+The gain is measured where the solves iterate: at max_dt = 1e-3 s (five
+times the benchmark's 2e-4 s, CFL number ~0.15) and 0.1 % tolerance the
+plain density solve needs ~4 Jacobi iterations per step.  At the
+benchmark's 2e-4 s both warm starts converge within the solver's minimum
+iteration counts, so there is nothing to gain there.
+"""
+import numpy as np
+import pytest
+import torch
+
+from alluvion_b200 import _capi, scenes, warm_start
+
+pytestmark = pytest.mark.gpu
+
+LATTICE, RADIUS, CONTAINER = (64, 64, 64), 0.005, (1.6, 0.8, 0.8)
+
+
+def _scene(engine, seed, lattice=LATTICE):
+    return scenes.dam_break(engine, np.float32, lattice, RADIUS, CONTAINER, [], seed=seed,
+                            volume_resolution=48)
+
+
+def test_step_features_match_step_inputs_and_outputs(engine):
+    sc = _scene(engine, 3, lattice=(24, 24, 24))
+    sp = scenes.solver_params()
+    dt = 2e-4
+    for _ in range(3):  # non-zero previous kappa / velocities
+        dt, _ = sc.step("df", sp, dt)
+    before = sc.state()
+    feat = torch.zeros((sc.n, 12), dtype=torch.float32, device="cuda")
+    ws = _capi.WarmStart()
+    ws.net = None
+    ws.features_out = feat.data_ptr()
+    dt_in = dt
+    dt_out, rep = sc.step("df", sp, dt, warm=ws)
+    after = sc.state()
+    f = feat.cpu().numpy().astype(np.float64)
+    rho0 = float(sc.cn.density0)
+    np.testing.assert_allclose(f[:, 0], after["density"] / rho0 - 1, atol=1e-6)
+    k = f[:, 2] * 32
+    assert np.all(k == np.round(k)) and k.min() >= 0 and k.max() <= 64
+    np.testing.assert_allclose(f[:, 3], before["kappa_v"] / dt_in, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(f[:, 4], before["kappa"] / dt_in ** 2, rtol=1e-6, atol=1e-5)
+    speed = np.linalg.norm(before["v"].astype(np.float64), axis=1)
+    np.testing.assert_allclose(f[:, 6], speed, rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(f[:, 7], speed * dt_in / (2 * RADIUS), rtol=1e-5, atol=1e-9)
+    # the exported factor was scaled by 1 / dt^2 in the density solve
+    np.testing.assert_allclose(f[:, 8], after["dfsph_factor"] * dt_out ** 2, rtol=1e-4,
+                               atol=1e-12)
+    assert np.all(f[:, 11] == np.float32(dt_in))
+    assert np.all(f[:, 1] >= 0) and np.all(f[:, 10] >= 0)
+    # boundary volumes come from cubic-Lagrange interpolation of the volume
+    # map, which may undershoot slightly below zero at the map's edge
+    assert f[:, 5].min() >= -0.02 * f[:, 5].max(), (f[:, 5].min(), f[:, 5].max())
+
+
+def _iterations(engine, seed, sp, net, steps=150):
+    sc = _scene(engine, seed)
+    ws = net.warm_start() if net is not None else None
+    dt = float(sp.max_dt)
+    its, errs = [], []
+    for _ in range(steps):
+        dt, rep = sc.step("df", sp, dt, warm=ws)
+        its.append((rep.num_divergence_solve, rep.num_density_solve))
+        if rep.num_density_solve < sp.max_density_solve:
+            errs.append(rep.mean_density_error)
+    return np.array(its, dtype=np.float64), np.array(errs)
+
+
+def test_learned_warm_start_reduces_density_iterations(engine):
+    sp = scenes.solver_params()
+    sp.max_dt = 1e-3
+    train = _scene(engine, 1)
+    x, t = warm_start.collect(train, sp, 200, 16384, seed=1)
+    net, losses = warm_start.fit(engine, x, t, steps=3000, batch=32768, seed=1)
+    assert np.mean(losses[-50:]) < 0.5 * np.mean(losses[:50])
+    plain, e_plain = _iterations(engine, 2, sp, None)
+    learned, e_learned = _iterations(engine, 2, sp, net)
+    p_den, l_den = plain[:, 1].mean(), learned[:, 1].mean()
+    assert p_den >= 2.5, "plain solve should iterate in this regime: %.2f" % p_den
+    assert l_den <= 0.8 * p_den, (p_den, l_den, plain[:, 0].mean(), learned[:, 0].mean())
+    # accuracy unchanged: every converged solve ends within the tolerance
+    assert np.all(e_learned <= sp.density_error_tolerance)
+    assert np.all(e_plain <= sp.density_error_tolerance)
