@@ -113,6 +113,11 @@ def parse_args():
                    help="launch every kernel from the host (no captured step graph)")
     p.add_argument("--workload", choices=sorted(WORKLOADS), default="dambreak-1m")
     p.add_argument("--method", choices=["df", "ii"], default="df")
+    p.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
+                   help="learned: DFSPH with the learned warm start, trained (untimed) on a "
+                        "differently seeded scene of the same workload")
+    p.add_argument("--max-dt", type=float, default=None,
+                   help="time-step cap (default 2e-4 s)")
     return p.parse_args()
 
 
@@ -223,13 +228,46 @@ def workload_bodies(wl):
 
 
 def build_scene(engine, workload="dambreak-1m", dtype=np.float32, rigid_bodies=None,
-                container_resolution=None):
+                container_resolution=None, seed=SEED):
     from alluvion_b200 import scenes
     wl = WORKLOADS[workload]
     bodies = [] if rigid_bodies == 0 else workload_bodies(wl)
     res = container_resolution or wl["container_resolution"]
     return scenes.dam_break(engine, dtype, wl["lattice"], wl["radius"], wl["container"], bodies,
-                            seed=SEED, volume_resolution=res)
+                            seed=seed, volume_resolution=res)
+
+
+TRAIN_STEPS, TRAIN_PER_STEP, FIT_STEPS = 300, 32768, 5000
+
+
+def train_warm_start(engine, args, sp):
+    """Untimed setup of --warm-start learned: plain steps of the workload at
+    seed SEED + 1 provide (features, converged kappa) pairs; the network is
+    fitted with the engine's own kernels."""
+    from alluvion_b200 import warm_start
+    sc = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
+                     container_resolution=args.container_resolution, seed=SEED + 1)
+    x, t = warm_start.collect(sc, sp, TRAIN_STEPS, TRAIN_PER_STEP, seed=SEED + 1)
+    net, losses = warm_start.fit(engine, x, t, steps=FIT_STEPS, seed=SEED + 1)
+    info = {"samples": int(x.shape[0]), "adam_steps": FIT_STEPS,
+            "loss_first_last": [round(float(np.mean(losses[:50])), 4),
+                                round(float(np.mean(losses[-50:])), 4)]}
+    del sc, x, t
+    return net, info
+
+
+def iteration_counts(engine, args, sp, steps, warm=None):
+    """Mean (divergence, density) iterations over `steps` steps of a fresh
+    copy of the benchmark scene."""
+    sc = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
+                     container_resolution=args.container_resolution)
+    dt = float(sp.max_dt)
+    its = []
+    for _ in range(steps):
+        dt, rep = sc.step(args.method, sp, dt, warm=warm)
+        its.append((rep.num_divergence_solve, rep.num_density_solve))
+    a = np.asarray(its, dtype=np.float64)
+    return [round(float(a[:, 0].mean()), 3), round(float(a[:, 1].mean()), 3)]
 
 
 def workload_name(args):
@@ -239,6 +277,10 @@ def workload_name(args):
         name += " [variant: %s rigid bodies, %d^3 container map]" % (
             "no" if args.rigid_bodies == 0 else "with",
             args.container_resolution or wl["container_resolution"])
+    if getattr(args, "warm_start", "plain") == "learned":
+        name += ", learned warm start"
+    if getattr(args, "max_dt", None):
+        name += ", max_dt %g s" % args.max_dt
     return name
 
 
@@ -267,7 +309,7 @@ L2_BYTES = 126 * 2 ** 20
 STEP_BYTES_PER_PARTICLE = 300
 
 
-def timed_steps(scene, sp, dt, steps, torch, on_step=None, method="df", flush=None):
+def timed_steps(scene, sp, dt, steps, torch, on_step=None, method="df", flush=None, warm=None):
     """Runs `steps` steps between CUDA events on the launching (default)
     stream, synchronised on both sides.  With `flush` (a device buffer
     larger than L2), every step is timed alone after the buffer is
@@ -286,7 +328,7 @@ def timed_steps(scene, sp, dt, steps, torch, on_step=None, method="df", flush=No
             start.record()
         if on_step:
             on_step("before")
-        dt, rep = scene.step(method, sp, dt)
+        dt, rep = scene.step(method, sp, dt, warm=warm)
         if on_step:
             on_step("after")
         if flush is not None:
@@ -362,15 +404,28 @@ def engine_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     engine = _capi.Engine(local)
     engine.set_graph_mode(not args.eager)
+    sp = scenes.solver_params()
+    if args.max_dt:
+        sp.max_dt = args.max_dt
+    warm, warm_info = None, None
+    if args.warm_start == "learned":
+        if args.method != "df":
+            raise SystemExit("--warm-start learned: DFSPH only")
+        net, warm_info = train_warm_start(engine, args, sp)
+        warm = net.warm_start()
+        n_cmp = args.warmup + args.steps
+        warm_info["iterations_per_step"] = {
+            "learned": iteration_counts(engine, args, sp, n_cmp, warm),
+            "plain": iteration_counts(engine, args, sp, n_cmp, None),
+            "steps": n_cmp}
     scene = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
                         container_resolution=args.container_resolution)
-    sp = scenes.solver_params()
     dt = float(sp.max_dt)
     host_state = scene.state() if rank == 0 and world == 1 else None
     host_bodies = scene.host_bodies() if host_state is not None else None
     # warm-up
     for _ in range(args.warmup):
-        dt, _ = scene.step(args.method, sp, dt)
+        dt, _ = scene.step(args.method, sp, dt, warm=warm)
     # ---- device-resident timed region (value)
     barrier(world)
     clocks = ClockSampler(local)
@@ -380,7 +435,8 @@ def engine_arm(args):
     flush = None
     if scene.n * STEP_BYTES_PER_PARTICLE < L2_BYTES:
         flush = torch.zeros(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
-    ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch, method=args.method, flush=flush)
+    ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch, method=args.method, flush=flush,
+                               warm=warm)
     launches = engine.launch_count() - launches0
     graphs1 = engine.graph_stats()
     clk = clocks.stop()
@@ -407,7 +463,7 @@ def engine_arm(args):
                 h.copy_(d, non_blocking=True)
     barrier(world)
     ms_e2e, dt, _ = timed_steps(scene, sp, dt, args.steps, torch, on_step=io,
-                                method=args.method, flush=flush)
+                                method=args.method, flush=flush, warm=warm)
     barrier(world)
     ms_e2e = max_over_ranks(ms_e2e, world, torch)
     e2e = total_particles * args.steps / (ms_e2e / 1e3)
@@ -415,7 +471,7 @@ def engine_arm(args):
     engine.reset_stats()
     engine.set_profiling(True)
     prof_steps = 3
-    _, dt, preps = timed_steps(scene, sp, dt, prof_steps, torch, method=args.method)
+    _, dt, preps = timed_steps(scene, sp, dt, prof_steps, torch, method=args.method, warm=warm)
     engine.set_profiling(False)
     stats = engine.kernel_stats()
     iters_div = sum(r[0] for r in preps) / prof_steps
@@ -466,6 +522,8 @@ def engine_arm(args):
                                                     len(steps_reps), 3),
                    "active_boundary_pairs": int(pairs),
                    "launch": "eager" if args.eager else "step graph (conditional WHILE loops)",
+                   "max_dt": float(sp.max_dt),
+                   "warm_start": args.warm_start,
                    "graph_replays_timed": graphs1[1] - graphs0[1],
                    "pass_ms_per_step": {k: round(v, 4) for k, v in pass_ms.items()}},
         "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -474,7 +532,9 @@ def engine_arm(args):
         "roofline": roofline,
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if warm_info is not None:
+        result["config"]["learned_warm_start"] = warm_info
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and warm is None:
         result["cpu_baseline"] = cpu_baseline(scene, sp, float(sp.max_dt), args.cpu_seconds,
                                               host_state, host_bodies, args.method)
     if world > 1:
