@@ -126,6 +126,14 @@ class WarmStart(ctypes.Structure):
     _fields_ = [("net", ctypes.c_void_p), ("features_out", ctypes.c_void_p)]
 
 
+class SceneF32(ctypes.Structure):
+    """al_scene_f32: one scene of a batched step."""
+    _fields_ = [("cn", ctypes.c_void_p), ("cni", ctypes.c_void_p), ("fluid", ctypes.c_void_p),
+                ("bodies", ctypes.c_void_p), ("rigid", ctypes.c_void_p),
+                ("params", ctypes.c_void_p), ("dt", ctypes.c_void_p), ("report", ctypes.c_void_p),
+                ("status", ctypes.c_int), ("reserved", ctypes.c_uint32)]
+
+
 class StepReport(ctypes.Structure):
     _fields_ = [("num_divergence_solve", ctypes.c_uint32),
                 ("num_density_solve", ctypes.c_uint32),
@@ -196,6 +204,7 @@ _SIGNATURES = {
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
     "al_df_step_warm_f32": (ctypes.c_int, [_P] * 8 + [_P, _P, _P]),
+    "al_df_batch_step_f32": (ctypes.c_int, [_P, _P, _U, _P]),
     "al_warm_net_gradient_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
     "al_warm_net_adam_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _U, ctypes.c_float, _P]),
     "al_engine_reset_stats": (ctypes.c_int, [_P]),

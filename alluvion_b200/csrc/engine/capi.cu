@@ -23,7 +23,7 @@ int al_engine::activate() const {
 }
 
 int al_engine::buffer(const char* name, size_t bytes, void** out) {
-  Scratch& s = scratch[name];
+  Scratch& s = ns.empty() ? scratch[name] : scratch[ns + name];
   if (s.bytes < bytes || s.ptr == nullptr) {
     if (s.ptr) {
       ALB_CUDA(cudaFree(s.ptr));
@@ -115,6 +115,19 @@ int al_engine::capture_streams() {
   return AL_OK;
 }
 
+int al_engine::branches(uint32_t count) {
+  if (!fork_event) ALB_CUDA(cudaEventCreateWithFlags(&fork_event, cudaEventDisableTiming));
+  while (branch_streams.size() < count) {
+    cudaStream_t s = nullptr;
+    ALB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    branch_streams.push_back(s);
+    cudaEvent_t ev = nullptr;
+    ALB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    join_events.push_back(ev);
+  }
+  return AL_OK;
+}
+
 void al_engine::drop_graphs() {
   for (Graph& g : graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -127,6 +140,9 @@ al_engine::~al_engine() {
   drop_graphs();
   if (capture_stream) cudaStreamDestroy(capture_stream);
   if (body_stream) cudaStreamDestroy(body_stream);
+  for (cudaStream_t s : branch_streams) cudaStreamDestroy(s);
+  for (cudaEvent_t ev : join_events) cudaEventDestroy(ev);
+  if (fork_event) cudaEventDestroy(fork_event);
   for (auto& kv : scratch)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (pinned) cudaFreeHost(pinned);

@@ -114,6 +114,14 @@ struct al_engine {
   cudaStream_t body_stream = nullptr;
   int capture_streams();  // creates the two capture streams on first use
   void drop_graphs();
+  // Batched steps: one capture branch (stream + join event) per scene, a
+  // fork event, and the buffer namespace of the scene being prepared or
+  // enqueued ("" outside batches).
+  std::vector<cudaStream_t> branch_streams;
+  std::vector<cudaEvent_t> join_events;
+  cudaEvent_t fork_event = nullptr;
+  int branches(uint32_t count);  // creates streams / events up to `count`
+  std::string ns;
   // pinned host staging (control readback, reports)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

@@ -1020,15 +1020,19 @@ struct Staging {
   uint32_t* hf = nullptr;  // [4]
 };
 
+// Staging of slot `slot` out of `nslots` equal slots (batched steps give
+// every scene its own slot).
 template <class TF>
-int staging(al_engine* e, Staging<TF>* out) {
+int staging(al_engine* e, Staging<TF>* out, uint32_t slot = 0, uint32_t nslots = 1) {
   auto up64 = [](size_t b) { return (b + 63) & ~size_t(63); };
   const size_t off_b = up64(sizeof(Ctrl<TF>));
   const size_t off_r = off_b + up64(sizeof(BodyDev<TF>) * AL_MAX_BOUNDARIES);
   const size_t off_f = off_r + up64(sizeof(RigidDev<TF>) * AL_MAX_BOUNDARIES);
+  const size_t slot_bytes = off_f + 128;
   void* pinned = nullptr;
-  ALB_TRY(e->host_pinned(off_f + 128, &pinned));
-  char* base = static_cast<char*>(pinned);  // cudaMallocHost: page aligned
+  ALB_TRY(e->host_pinned(slot_bytes * nslots, &pinned));
+  // cudaMallocHost: page aligned; slots are multiples of 64 bytes
+  char* base = static_cast<char*>(pinned) + slot_bytes * slot;
   out->hc = reinterpret_cast<Ctrl<TF>*>(base);
   out->hb = reinterpret_cast<BodyDev<TF>*>(base + off_b);
   out->hr = reinterpret_cast<RigidDev<TF>*>(base + off_r);
@@ -1306,21 +1310,36 @@ std::vector<uint64_t> step_key(const al_engine* e, const StepPlan<TF>& P,
 
 constexpr size_t kMaxGraphs = 8;
 
+// Host-side arguments of one scene's step (the C ABI's per-call inputs).
 template <class TF>
-int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
-             const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
-             typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
-             al_step_report* report, cudaStream_t st, const al_warm_start* warm = nullptr) {
-  ALB_TRY(check_step_args<TF>(f, cni, bodies, rigid, sp, dt));
-  ALB_TRY(e->activate());
-  StepPlan<TF> P;
+struct StepArgs {
+  bool iisph = false;
+  const typename FluidT<TF>::cn* cn = nullptr;
+  const al_consti* cni = nullptr;
+  const typename FluidT<TF>::type* f = nullptr;
+  const typename FluidT<TF>::body* bodies = nullptr;
+  typename FluidT<TF>::rigid* rigid = nullptr;
+  const al_solver_params* sp = nullptr;
+  TF* dt = nullptr;
+  al_step_report* report = nullptr;
+  const al_warm_start* warm = nullptr;
+};
+
+// Validates the arguments, sizes the scene's scratch (under the engine's
+// current buffer namespace) and fills staging slot `slot` of `nslots`.
+template <class TF>
+int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t slot,
+                 uint32_t nslots) {
+  ALB_TRY(check_step_args<TF>(A.f, A.cni, A.bodies, A.rigid, A.sp, A.dt));
+  const al_solver_params* sp = A.sp;
+  const bool iisph = A.iisph;
   P.iisph = iisph;
   P.div = !iisph && sp->enable_divergence_solve;
   P.den = iisph || sp->enable_density_solve;
-  P.c = to_cn<TF>(*cn);
-  P.g = to_dims(*cni);
-  P.f = f;
-  const uint32_t n = f->num_particles;
+  P.c = to_cn<TF>(*A.cn);
+  P.g = to_dims(*A.cni);
+  P.f = A.f;
+  const uint32_t n = A.f->num_particles;
   const uint32_t nb = P.g.nb;
   StepState<TF>& S = P.S;
   S.n = n;
@@ -1354,6 +1373,7 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   ALB_TRY(e->buf("red", S.grid, &S.red));
   ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
   S.bodies = P.bodies_dev;
+  const al_warm_start* warm = A.warm;
   if (warm && (warm->net || warm->features_out)) {
     if (sizeof(TF) != 4 || iisph || !P.div) {
       set_error("learned warm start: float32 DFSPH steps with the divergence solve only");
@@ -1369,10 +1389,10 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
     }
   }
   // ---- host staging: control block, bodies, rigid state
-  ALB_TRY(staging<TF>(e, &P.io));
+  ALB_TRY(staging<TF>(e, &P.io, slot, nslots));
   Ctrl<TF>* hc = P.io.hc;
   std::memset(hc, 0, sizeof(Ctrl<TF>));
-  hc->dt = *dt;
+  hc->dt = *A.dt;
   hc->length_scale = P.c.radius * TF(2);
   hc->cfl = TF(sp->cfl);
   hc->max_dt = TF(sp->max_dt);
@@ -1386,36 +1406,105 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   hc->integrate_rigids = sp->integrate_rigids;
   for (int k = 0; k < 3; ++k) hc->pile_gravity[k] = TF(sp->pile_gravity[k]);
   for (uint32_t b = 0; b < nb; ++b) {
-    P.io.hb[b] = to_body_dev<TF>(bodies[b]);
+    P.io.hb[b] = to_body_dev<TF>(A.bodies[b]);
     ALB_TRY(validate_body(P.io.hb[b], true, true));
-    P.io.hr[b] = to_rigid_dev<TF>(rigid[b]);
+    P.io.hr[b] = to_rigid_dev<TF>(A.rigid[b]);
   }
+  return AL_OK;
+}
+
+// Reads a completed step back: report, dt, rigid state, status.
+template <class TF>
+int finish_step(const StepArgs<TF>& A, const StepPlan<TF>& P) {
+  al_step_report rep = P.io.hc->rep;
+  const uint32_t* hf = P.io.hf;
+  for (int k = 0; k < 3; ++k) rep.grid_anomaly[k] = hf[k];
+  if (P.S.n == 0) rep.dt = double(*A.dt);
+  *A.dt = TF(rep.dt);
+  const RigidDev<TF>* hr = P.io.hr;
+  for (uint32_t b = 0; b < P.S.nb; ++b) {
+    for (int k = 0; k < 3; ++k) {
+      A.rigid[b].x[k] = (&hr[b].x.x)[k];
+      A.rigid[b].v[k] = (&hr[b].v.x)[k];
+      A.rigid[b].omega[k] = (&hr[b].omega.x)[k];
+    }
+    A.rigid[b].q[0] = hr[b].q.x;
+    A.rigid[b].q[1] = hr[b].q.y;
+    A.rigid[b].q[2] = hr[b].q.z;
+    A.rigid[b].q[3] = hr[b].q.w;
+  }
+  if (A.report) *A.report = rep;
+  if (hf[0]) return AL_ERR_OUT_OF_GRID;
+  if (hf[1]) return AL_ERR_CELL_OVERFLOW;
+  if (hf[2]) return AL_ERR_NEIGHBOR_OVERFLOW;
+  if (hf[3]) {
+    set_error("learned warm start: a tensor-core wait timed out");
+    return AL_ERR_TIMEOUT;
+  }
+  return AL_OK;
+}
+
+// Cached graph for `key`, capturing it with `capture` when the key ran
+// eagerly before.  Returns null (run eagerly) otherwise.
+template <class Capture>
+int find_or_capture(al_engine* e, const std::vector<uint64_t>& key, Capture&& capture,
+                    al_engine::Graph** out) {
+  *out = nullptr;
+  for (al_engine::Graph& gr : e->graphs)
+    if (gr.key == key) *out = &gr;
+  if (*out) return AL_OK;
+  bool seen = false;
+  for (const auto& k : e->seen_keys) seen = seen || k == key;
+  if (!seen) return AL_OK;
+  al_engine::Graph gr;
+  gr.key = key;
+  ALB_TRY(capture(&gr.exec, &gr.fixed_launches));
+  if (!gr.exec) return AL_OK;
+  if (e->graphs.size() >= kMaxGraphs) {
+    cudaGraphExecDestroy(e->graphs.front().exec);
+    e->graphs.erase(e->graphs.begin());
+  }
+  e->graphs.push_back(std::move(gr));
+  *out = &e->graphs.back();
+  ++e->graph_captures;
+  return AL_OK;
+}
+
+void remember_key(al_engine* e, std::vector<uint64_t> key) {
+  if (e->seen_keys.size() >= 2 * kMaxGraphs) e->seen_keys.erase(e->seen_keys.begin());
+  e->seen_keys.push_back(std::move(key));
+}
+
+template <class TF>
+int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
+             const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
+             typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
+             al_step_report* report, cudaStream_t st, const al_warm_start* warm = nullptr) {
+  ALB_TRY(e->activate());
+  e->ns.clear();
+  StepArgs<TF> A;
+  A.iisph = iisph;
+  A.cn = cn;
+  A.cni = cni;
+  A.f = f;
+  A.bodies = bodies;
+  A.rigid = rigid;
+  A.sp = sp;
+  A.dt = dt;
+  A.report = report;
+  A.warm = warm;
+  StepPlan<TF> P;
+  ALB_TRY(prepare_step<TF>(e, A, P, 0, 1));
   // ---- launch: a cached graph when this configuration ran before, else
   // eagerly (the first run of a configuration sizes every scratch buffer)
-  const bool use_graph = e->graph_mode && !e->profiling && n > 0;
+  const bool use_graph = e->graph_mode && !e->profiling && P.S.n > 0;
   al_engine::Graph* graph = nullptr;
-  std::vector<uint64_t> key;
-  if (use_graph) {
-    key = step_key<TF>(e, P, cn, cni);
-    for (al_engine::Graph& gr : e->graphs)
-      if (gr.key == key) graph = &gr;
-    bool seen = false;
-    for (const auto& k : e->seen_keys) seen = seen || k == key;
-    if (!graph && seen) {
-      al_engine::Graph gr;
-      gr.key = key;
-      ALB_TRY(capture_step<TF>(e, P, &gr.exec, &gr.fixed_launches));
-      if (gr.exec) {
-        if (e->graphs.size() >= kMaxGraphs) {
-          cudaGraphExecDestroy(e->graphs.front().exec);
-          e->graphs.erase(e->graphs.begin());
-        }
-        e->graphs.push_back(std::move(gr));
-        graph = &e->graphs.back();
-        ++e->graph_captures;
-      }
-    }
-  }
+  if (use_graph)
+    ALB_TRY(find_or_capture(e, step_key<TF>(e, P, cn, cni),
+                            [&](cudaGraphExec_t* x, uint32_t* fl) {
+                              return capture_step<TF>(e, P, x, fl);
+                            },
+                            &graph));
   if (graph) {
     ALB_CUDA(cudaGraphLaunch(graph->exec, st));
     ++e->graph_replays;
@@ -1424,40 +1513,126 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   }
   ALB_CUDA(cudaStreamSynchronize(st));
   e->flush_stats();
-  if (use_graph && !graph) {
-    // remember the configuration with the scratch generation it left
-    key = step_key<TF>(e, P, cn, cni);
-    if (e->seen_keys.size() >= 2 * kMaxGraphs) e->seen_keys.erase(e->seen_keys.begin());
-    e->seen_keys.push_back(std::move(key));
-  }
-  al_step_report rep = hc->rep;
+  // remember the configuration with the scratch generation it left
+  if (use_graph && !graph) remember_key(e, step_key<TF>(e, P, cn, cni));
+  const al_step_report& r = P.io.hc->rep;
   if (graph)
     e->launches += graph->fixed_launches +
-                   2ull * (uint64_t(rep.num_divergence_solve) + rep.num_density_solve);
-  const uint32_t* hf = P.io.hf;
-  for (int k = 0; k < 3; ++k) rep.grid_anomaly[k] = hf[k];
-  if (n == 0) rep.dt = double(*dt);
-  *dt = TF(rep.dt);
-  const RigidDev<TF>* hr = P.io.hr;
-  for (uint32_t b = 0; b < nb; ++b) {
-    for (int k = 0; k < 3; ++k) {
-      rigid[b].x[k] = (&hr[b].x.x)[k];
-      rigid[b].v[k] = (&hr[b].v.x)[k];
-      rigid[b].omega[k] = (&hr[b].omega.x)[k];
+                   2ull * (uint64_t(r.num_divergence_solve) + r.num_density_solve);
+  return finish_step<TF>(A, P);
+}
+
+// ------------------------------------------------------------ batched steps
+// Every scene of a batch keeps its scratch under its own namespace and its
+// own staging slot; a batch is captured as one graph whose branches (one
+// per scene, forked from and joined to the capture stream) are the scenes'
+// whole steps, each with its own conditional solver loops.  One launch and
+// one synchronisation advance every scene; the branches' kernels overlap on
+// the GPU.
+std::string batch_ns(uint32_t k) { return "batch" + std::to_string(k) + "."; }
+
+template <class TF>
+int capture_batch(al_engine* e, std::vector<StepPlan<TF>>& plans, cudaGraphExec_t* exec,
+                  uint32_t* fixed) {
+  *exec = nullptr;
+  const uint32_t K = uint32_t(plans.size());
+  ALB_TRY(e->capture_streams());
+  ALB_TRY(e->branches(K));
+  cudaStream_t cs = e->capture_stream;
+  const uint64_t launches0 = e->launches;
+  const uint64_t gen0 = e->generation;
+  ALB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int rc = AL_OK, loops = 0;
+  cudaError_t ce = cudaEventRecord(e->fork_event, cs);
+  for (uint32_t k = 0; k < K && rc == AL_OK && ce == cudaSuccess; ++k) {
+    cudaStream_t bs = e->branch_streams[k];
+    ce = cudaStreamWaitEvent(bs, e->fork_event, 0);
+    if (ce != cudaSuccess) break;
+    e->ns = batch_ns(k);
+    rc = enqueue_step<TF>(e, plans[k], bs, true, &loops);
+    if (rc != AL_OK) break;
+    ce = cudaEventRecord(e->join_events[k], bs);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cs, e->join_events[k], 0);
+  }
+  e->ns.clear();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(cs, &graph);
+  const uint64_t captured = e->launches - launches0;
+  e->launches = launches0;
+  if (rc != AL_OK || ce != cudaSuccess || end != cudaSuccess || e->generation != gen0) {
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != AL_OK) return rc;
+    ALB_CUDA(ce);
+    ALB_CUDA(end);
+    return AL_OK;
+  }
+  const cudaError_t inst = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) *exec = nullptr;
+  ALB_CUDA(inst);
+  *fixed = uint32_t(captured - 2u * uint32_t(loops));
+  return AL_OK;
+}
+
+template <class TF>
+std::vector<uint64_t> batch_key(al_engine* e, const std::vector<StepArgs<TF>>& args,
+                                const std::vector<StepPlan<TF>>& plans) {
+  std::vector<uint64_t> key{0xBA7C4ull, uint64_t(args.size())};
+  for (size_t k = 0; k < args.size(); ++k) {
+    const std::vector<uint64_t> kk = step_key<TF>(e, plans[k], args[k].cn, args[k].cni);
+    key.insert(key.end(), kk.begin(), kk.end());
+  }
+  return key;
+}
+
+template <class TF>
+int run_batch(al_engine* e, const std::vector<StepArgs<TF>>& args, std::vector<int>& status,
+              cudaStream_t st) {
+  ALB_TRY(e->activate());
+  struct NsReset {
+    al_engine* e;
+    ~NsReset() { e->ns.clear(); }
+  } reset{e};
+  const uint32_t K = uint32_t(args.size());
+  std::vector<StepPlan<TF>> plans(K);
+  bool nonempty = true;
+  for (uint32_t k = 0; k < K; ++k) {
+    e->ns = batch_ns(k);
+    ALB_TRY(prepare_step<TF>(e, args[k], plans[k], k, K));
+    nonempty = nonempty && plans[k].S.n > 0;
+  }
+  e->ns.clear();
+  const bool use_graph = e->graph_mode && !e->profiling && nonempty;
+  al_engine::Graph* graph = nullptr;
+  if (use_graph)
+    ALB_TRY(find_or_capture(e, batch_key<TF>(e, args, plans),
+                            [&](cudaGraphExec_t* x, uint32_t* fl) {
+                              return capture_batch<TF>(e, plans, x, fl);
+                            },
+                            &graph));
+  if (graph) {
+    ALB_CUDA(cudaGraphLaunch(graph->exec, st));
+    ++e->graph_replays;
+  } else {
+    for (uint32_t k = 0; k < K; ++k) {
+      e->ns = batch_ns(k);
+      ALB_TRY(enqueue_step<TF>(e, plans[k], st, false, nullptr));
     }
-    rigid[b].q[0] = hr[b].q.x;
-    rigid[b].q[1] = hr[b].q.y;
-    rigid[b].q[2] = hr[b].q.z;
-    rigid[b].q[3] = hr[b].q.w;
+    e->ns.clear();
   }
-  if (report) *report = rep;
-  if (hf[0]) return AL_ERR_OUT_OF_GRID;
-  if (hf[1]) return AL_ERR_CELL_OVERFLOW;
-  if (hf[2]) return AL_ERR_NEIGHBOR_OVERFLOW;
-  if (hf[3]) {
-    set_error("learned warm start: a tensor-core wait timed out");
-    return AL_ERR_TIMEOUT;
+  ALB_CUDA(cudaStreamSynchronize(st));
+  e->flush_stats();
+  if (use_graph && !graph) remember_key(e, batch_key<TF>(e, args, plans));
+  status.assign(K, AL_OK);
+  uint64_t iters = 0;
+  for (uint32_t k = 0; k < K; ++k) {
+    const al_step_report& r = plans[k].io.hc->rep;
+    iters += uint64_t(r.num_divergence_solve) + r.num_density_solve;
+    status[k] = finish_step<TF>(args[k], plans[k]);
   }
+  if (graph) e->launches += graph->fixed_launches + 2ull * iters;
+  for (int s : status)
+    if (s != AL_OK) return s;
   return AL_OK;
 }
 
@@ -1509,6 +1684,31 @@ int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* c
   ALB_CHECK_ARG(engine && cn, "al_ii_step: null argument");
   return run_step<double>(engine, true, cn, cni, fluid, bodies, rigid, params, dt, report,
                           static_cast<cudaStream_t>(stream));
+}
+
+int al_df_batch_step_f32(al_engine* engine, al_scene_f32* scenes, uint32_t num_scenes,
+                         void* stream) {
+  ALB_CHECK_ARG(engine && (num_scenes == 0 || scenes), "al_df_batch_step_f32: null argument");
+  ALB_CHECK_ARG(num_scenes <= AL_MAX_BATCH, "al_df_batch_step_f32: too many scenes");
+  if (num_scenes == 0) return AL_OK;
+  std::vector<StepArgs<float>> args(num_scenes);
+  for (uint32_t k = 0; k < num_scenes; ++k) {
+    const al_scene_f32& sc = scenes[k];
+    ALB_CHECK_ARG(sc.cn != nullptr, "al_df_batch_step_f32: scene constants are null");
+    args[k].cn = sc.cn;
+    args[k].cni = sc.cni;
+    args[k].f = sc.fluid;
+    args[k].bodies = sc.bodies;
+    args[k].rigid = sc.rigid;
+    args[k].sp = sc.params;
+    args[k].dt = sc.dt;
+    args[k].report = sc.report;
+  }
+  std::vector<int> status;
+  const int rc = run_batch<float>(engine, args, status, static_cast<cudaStream_t>(stream));
+  for (uint32_t k = 0; k < num_scenes; ++k)
+    scenes[k].status = k < status.size() ? status[k] : rc;
+  return rc;
 }
 
 }  // extern "C"

@@ -4,6 +4,7 @@ Constants are derived in the solver's real type with the operation order of
 Const<TF>::set_kernel_radius / set_particle_attr (constants.hpp:100-128), so
 float32 scenes see exactly the float32 values the reference would.
 """
+import ctypes
 import math
 
 import numpy as np
@@ -428,3 +429,30 @@ def solver_params(**kw):
         else:
             setattr(p, k, v)
     return p
+
+
+def batch_step(engine, scene_list, sp, dts, stream=None, allow=()):
+    """One DFSPH step of every float32 scene in one call
+    (al_df_batch_step_f32).  dts: per-scene time steps.  Returns (new dts,
+    reports, per-scene statuses)."""
+    k = len(scene_list)
+    arr = (_capi.SceneF32 * k)()
+    keep = []
+    dt_c = [ctypes.c_float(float(d)) for d in dts]
+    reps = [_capi.StepReport() for _ in range(k)]
+    for i, sc in enumerate(scene_list):
+        assert sc.sfx == "f32", "batched steps: float32 scenes"
+        fl = sc.fluid()
+        keep.append(fl)
+        a = arr[i]
+        a.cn = _capi.ptr(sc.cn).value
+        a.cni = _capi.ptr(sc.cni).value
+        a.fluid = _capi.ptr(fl).value
+        a.bodies = _capi.ptr(sc.bodies).value if sc.num_boundaries else None
+        a.rigid = _capi.ptr(sc.rigid).value if sc.num_boundaries else None
+        a.params = _capi.ptr(sp).value
+        a.dt = ctypes.addressof(dt_c[i])
+        a.report = ctypes.addressof(reps[i])
+    status = _capi.lib().al_df_batch_step_f32(engine.handle, arr, k, stream)
+    _capi.check(status, "al_df_batch_step_f32", allow=allow)
+    return [d.value for d in dt_c], reps, [arr[i].status for i in range(k)]

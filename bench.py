@@ -54,6 +54,13 @@ WORKLOADS = {
              "tank, sphere r=0.1 + box 0.16 m + torus R=0.1 r=0.04 with 128^3 cubic-Lagrange "
              "SDF + volume maps, two-way coupled"),
 }
+BATCH_WORKLOADS = {
+    "batch64": dict(
+        scenes=64, radius=0.01,
+        desc="batched dam breaks: 64 scenes, particle counts log-uniform in [8,192, 262,144] "
+             "(cubic lattices, r=0.01 m, seeded), boxes scaled with the count from 1.0x0.7x0.7 m, "
+             "0-2 seeded rigid spheres per scene, 32^3 volume maps, one graph launch per step"),
+}
 METHOD_NAME = {"df": "DFSPH", "ii": "IISPH"}
 
 # Compulsory per-particle state traffic per pass, float32 ("Model A": every
@@ -111,7 +118,8 @@ def parse_args():
                    help="volume-map resolution of the container (default: the workload's)")
     p.add_argument("--eager", action="store_true",
                    help="launch every kernel from the host (no captured step graph)")
-    p.add_argument("--workload", choices=sorted(WORKLOADS), default="dambreak-1m")
+    p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS),
+                   default="dambreak-1m")
     p.add_argument("--method", choices=["df", "ii"], default="df")
     p.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
                    help="learned: DFSPH with the learned warm start, trained (untimed) on a "
@@ -393,6 +401,183 @@ def cpu_baseline(scene, sp, dt, budget_s, host_state, host_bodies, method="df"):
                                                                       el)}
 
 
+def batch_scene_list(engine, spec, seed=SEED):
+    """The batch workload's scenes (seeded)."""
+    from alluvion_b200 import _capi, scenes
+    rng = np.random.Generator(np.random.PCG64(seed + 3000))
+    r = spec["radius"]
+    h = 4 * r
+    out = []
+    for _ in range(spec["scenes"]):
+        target = np.exp(rng.uniform(np.log(8192), np.log(262144)))
+        a = max(4, int(round(target ** (1.0 / 3.0))))
+        s = (a ** 3 / 32768.0) ** (1.0 / 3.0)
+        block = 2 * r * a
+        box = np.array([max(1.0 * s, 1.6 * block + 2 * h), max(0.7 * s, block + 3 * h),
+                        max(0.7 * s, block + 2 * h)])
+        bodies = []
+        for _ in range(int(rng.integers(0, 3))):
+            rad = 0.05 * s
+            y = block + h + rad + 0.5 * h
+            if y + rad + h > box[1]:
+                continue
+            rho = rng.uniform(500.0, 2000.0)
+            mass = rho * 4.0 / 3.0 * np.pi * rad ** 3
+            pos = (rng.uniform(0.3, 0.7) * box[0], y, rng.uniform(0.3, 0.7) * box[2])
+            bodies.append(dict(shape=_capi.SHAPE_SPHERE, params=[rad], sign=1.0, resolution=32,
+                               use_distance_grid=True, mass=mass,
+                               inertia=scenes.sphere_inertia(mass, rad), x=pos))
+        seed_k = int(rng.integers(0, 2 ** 31))
+        out.append(scenes.dam_break(engine, np.float32, (a, a, a), r, tuple(box), bodies,
+                                    seed=seed_k, volume_resolution=32))
+    return out
+
+
+def batch_arm(args):
+    """Config-3 style batch: every step advances all scenes with one
+    al_df_batch_step_f32 call (one graph launch from the second step on)."""
+    import torch
+    from alluvion_b200 import _capi, scenes
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    spec = BATCH_WORKLOADS[args.workload]
+    engine = _capi.Engine(local)
+    engine.set_graph_mode(not args.eager)
+    sl = batch_scene_list(engine, spec)
+    sp = scenes.solver_params()
+    if args.max_dt:
+        sp.max_dt = args.max_dt
+    total_n = sum(sc.n for sc in sl)
+    host_state = [sc.state() for sc in sl] if rank == 0 and world == 1 else None
+    host_bodies = [sc.host_bodies() for sc in sl] if host_state is not None else None
+    dts = [float(sp.max_dt)] * len(sl)
+    for _ in range(args.warmup):
+        dts, _, _ = scenes.batch_step(engine, sl, sp, dts)
+
+    def run(steps, on_step=None):
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        nonlocal dts
+        its = []
+        start.record()
+        for _ in range(steps):
+            if on_step:
+                on_step("before")
+            dts, reps, _ = scenes.batch_step(engine, sl, sp, dts)
+            if on_step:
+                on_step("after")
+            its.append([(r.num_divergence_solve, r.num_density_solve) for r in reps])
+        stop.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop), np.asarray(its, dtype=np.float64)
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = engine.launch_count()
+    graphs0 = engine.graph_stats()
+    ms, its = run(args.steps)
+    launches = engine.launch_count() - launches0
+    graphs1 = engine.graph_stats()
+    clk = clocks.stop()
+    barrier(world)
+    ms = max_over_ranks(ms, world, torch)
+    value = total_n * world * args.steps / (ms / 1e3)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    dev_in = [t for sc in sl for t in (sc.x, sc.v, sc.kappa, sc.kappa_v)]
+    host_in = [pin(t.cpu().numpy()) for t in dev_in]
+    dev_out = [t for sc in sl for t in (sc.x, sc.v)]
+    host_out = [pin(t.cpu().numpy()) for t in dev_out]
+    h2d = sum(t.numel() * t.element_size() for t in host_in)
+    d2h = sum(t.numel() * t.element_size() for t in host_out)
+
+    def io(phase):
+        if phase == "before":
+            for d, hh in zip(dev_in, host_in):
+                d.copy_(hh, non_blocking=True)
+        else:
+            for d, hh in zip(dev_out, host_out):
+                hh.copy_(d, non_blocking=True)
+    barrier(world)
+    ms_e2e, _ = run(args.steps, io)
+    ms_e2e = max_over_ranks(ms_e2e, world, torch)
+    e2e = total_n * world * args.steps / (ms_e2e / 1e3)
+    peak, peak_kind = measured_peaks()
+    result = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded jittered lattices, seeded rigid spheres)",
+        "config": {"workload": "DFSPH " + spec["desc"], "scenes": len(sl),
+                   "particles_per_gpu": total_n, "global_particles": total_n * world,
+                   "scene_particles_min_max": [min(sc.n for sc in sl), max(sc.n for sc in sl)],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
+                   "launch": "eager" if args.eager else "batch graph (one branch per scene)",
+                   "graph_replays_timed": graphs1[1] - graphs0[1],
+                   "mean_divergence_iterations": round(float(its[:, :, 0].mean()), 3),
+                   "mean_density_iterations": round(float(its[:, :, 1].mean()), 3)},
+        "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": None,
+        "clocks": clk,
+    }
+    # roofline of the dominant pass from the eager per-pass times (scenes in turn)
+    engine.reset_stats()
+    engine.set_profiling(True)
+    run(2)
+    engine.set_profiling(False)
+    pass_ms = {}
+    for name, (tot, cnt) in engine.kernel_stats().items():
+        pp = GROUP_PASS.get(name)
+        if pp:
+            pass_ms[pp] = pass_ms.get(pp, 0.0) + tot / 2
+    dominant = max(pass_ms, key=pass_ms.get)
+    runs = {"div_iteration": float(its[:, :, 0].mean()),
+            "press_iteration": float(its[:, :, 1].mean())}.get(dominant, 1.0)
+    bpp, bpair = MODEL_A[dominant]
+    alg = bpp * total_n
+    per_launch = pass_ms[dominant] / max(runs, 1e-9)
+    achieved = alg / (per_launch / 1e3) / 1e9
+    result["config"]["pass_ms_per_step_sequential"] = {k: round(v, 4) for k, v in pass_ms.items()}
+    result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                          "kernel": dominant, "peak_kind": peak_kind,
+                          "algorithmic_bytes_per_launch": int(alg),
+                          "launch_ms": round(per_launch, 4),
+                          "note": "per-pass times from eager steps (scenes in turn)"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import binding as orc
+        t0 = time.perf_counter()
+        done = 0
+        k = 0
+        while time.perf_counter() - t0 < args.cpu_seconds and k < len(sl):
+            sc = sl[k]
+            hb, keep, rigid = host_bodies[k]
+            nb = sc.num_boundaries
+            bodies = (type(hb[0]) * nb)(*[hb[b] for b in range(nb)])
+            state = oracle_state(host_state[k], "df")
+            orc.run("df", sc.cn, sc.cni, bodies, rigid.copy(), state, sp, float(sp.max_dt), 1)
+            done += sc.n
+            k += 1
+        el = time.perf_counter() - t0
+        result["cpu_baseline"] = {"value": round(done / el, 1), "unit": UNIT,
+                                  "cores": orc.num_threads(), "kind": "port",
+                                  "sample": "one step of each of the first %d scenes, %.1f s"
+                                            % (k, el)}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
 def engine_arm(args):
     import torch
     from alluvion_b200 import _capi, scenes
@@ -545,6 +730,44 @@ def engine_arm(args):
         print(json.dumps(result), flush=True)
 
 
+def reference_batch(args, engine):
+    """Reference arm of a batch workload: the oracle port advances every
+    scene of the batch by one step per benchmark step (scenes in turn, all
+    host cores)."""
+    from alluvion_b200 import scenes
+    from oracle import binding as orc
+    spec = BATCH_WORKLOADS[args.workload]
+    sl = batch_scene_list(engine, spec)  # setup: grids built on the device, untimed
+    sp = scenes.solver_params()
+    items = []
+    for sc in sl:
+        hb, keep, rigid = sc.host_bodies()
+        nb = sc.num_boundaries
+        bodies = (type(hb[0]) * nb)(*[hb[b] for b in range(nb)])
+        items.append([sc, bodies, keep, rigid, oracle_state(sc.state(), "df"), float(sp.max_dt)])
+    total_n = sum(sc.n for sc in sl)
+    steps = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for it in items:
+            sc, bodies, _, rigid, state, dt = it
+            it[5], _ = orc.run("df", sc.cn, sc.cni, bodies, rigid, state, sp, dt, 1)
+    el = time.perf_counter() - t0
+    value = total_n * steps / el
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
+        "n_gpus": 1, "steps": steps, "warmup": 0, "ms_per_step": round(el * 1e3 / steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded jittered lattices, seeded rigid spheres)",
+        "config": {"workload": "DFSPH " + spec["desc"], "particles_per_gpu": total_n},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": orc.num_threads(),
+                         "kind": "port",
+                         "sample": "%d step(s) of all %d scenes" % (steps, len(sl))},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def reference_arm(args):
     """The reference's CPU formulation of the path (the oracle port: the
     reference itself needs Eigen/GLFW/glm and does not build here), timed on
@@ -557,6 +780,8 @@ def reference_arm(args):
     from oracle import binding as orc
     torch.cuda.set_device(local)
     engine = _capi.Engine(local)
+    if args.workload in BATCH_WORKLOADS:
+        return reference_batch(args, engine)
     # setup only: grids built on the device, untimed
     scene = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
                         container_resolution=args.container_resolution)
@@ -596,6 +821,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload in BATCH_WORKLOADS:
+        batch_arm(args)
     else:
         engine_arm(args)
 

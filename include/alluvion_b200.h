@@ -519,6 +519,32 @@ AL_API int al_df_step_warm_f32(al_engine* engine, const al_const_f32* cn, const 
                                const al_warm_start* warm, float* dt, al_step_report* report,
                                void* stream);
 
+/* ------------------------------------------------------- batched scenes
+ * No reference counterpart (the reference advances one scene per call).
+ * Advances every scene by one DFSPH step (each with its own dt, iteration
+ * counts and report; same semantics as al_df_step_f32 per scene).  From the
+ * second call with the same configuration on, the whole batch is one
+ * captured CUDA graph whose parallel branches are the scenes' steps: one
+ * launch and one synchronisation for all scenes, whose kernels overlap on
+ * the GPU.  Each scene keeps its own scratch.  Returns AL_OK, or the first
+ * scene's failure; every scene's own status is in scenes[k].status. */
+#define AL_MAX_BATCH 256
+typedef struct al_scene_f32 {
+  const al_const_f32* cn;
+  const al_consti* cni;
+  const al_fluid_f32* fluid;
+  const al_body_f32* bodies;
+  al_rigid_f32* rigid;
+  const al_solver_params* params;
+  float* dt;               /* host in/out */
+  al_step_report* report;  /* host out, may be NULL */
+  int status;              /* out */
+  uint32_t reserved;
+} al_scene_f32;
+
+AL_API int al_df_batch_step_f32(al_engine* engine, al_scene_f32* scenes, uint32_t num_scenes,
+                                void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
