@@ -134,6 +134,29 @@ class SceneF32(ctypes.Structure):
                 ("status", ctypes.c_int), ("reserved", ctypes.c_uint32)]
 
 
+class ContactBodyF32(ctypes.Structure):
+    """al_contact_body_f32: collision vertices (device, body frame) and
+    contact coefficients of one body."""
+    _fields_ = [("vertices", ctypes.c_void_p), ("num_vertices", ctypes.c_uint32),
+                ("restitution", ctypes.c_float), ("friction", ctypes.c_float),
+                ("reserved", ctypes.c_uint32)]
+
+
+class ContactF32(ctypes.Structure):
+    """al_contact_f32 (Contact<float3, float>, contact.hpp:8-25)."""
+    _fields_ = [("i", ctypes.c_uint32), ("j", ctypes.c_uint32),
+                ("cp_i", ctypes.c_float * 3), ("cp_j", ctypes.c_float * 3),
+                ("n", ctypes.c_float * 3), ("t", ctypes.c_float * 3),
+                ("iiwi_diag", ctypes.c_float * 3), ("iiwi_off_diag", ctypes.c_float * 3),
+                ("iiwj_diag", ctypes.c_float * 3), ("iiwj_off_diag", ctypes.c_float * 3),
+                ("friction", ctypes.c_float), ("nkninv", ctypes.c_float),
+                ("pmax", ctypes.c_float), ("goalu", ctypes.c_float),
+                ("impulse_sum", ctypes.c_float)]
+
+
+CONTACT_FLOATS = ctypes.sizeof(ContactF32) // 4
+
+
 class StepReport(ctypes.Structure):
     _fields_ = [("num_divergence_solve", ctypes.c_uint32),
                 ("num_density_solve", ctypes.c_uint32),
@@ -205,6 +228,9 @@ _SIGNATURES = {
     "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
     "al_df_step_warm_f32": (ctypes.c_int, [_P] * 8 + [_P, _P, _P]),
     "al_df_batch_step_f32": (ctypes.c_int, [_P, _P, _U, _P]),
+    "al_find_contacts_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, ctypes.c_float, _U, _P, _P,
+                                            _P]),
+    "al_solve_contacts_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _P]),
     "al_warm_net_gradient_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
     "al_warm_net_adam_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _U, ctypes.c_float, _P]),
     "al_engine_reset_stats": (ctypes.c_int, [_P]),

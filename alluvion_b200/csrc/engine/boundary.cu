@@ -3,6 +3,7 @@
 #include <cmath>
 
 #include "boundary.cuh"
+#include "body_geometry.cuh"
 #include "peirce_tables.h"
 
 namespace alb {
@@ -36,180 +37,6 @@ template <>
 struct PeirceSel<double> {
   __device__ static const PeirceDevD& get() { return c_peirce_d; }
 };
-
-// ------------------------------------------------------------- geometry
-template <class TF>
-__device__ __forceinline__ vec3<TF> rotate(vec3<TF> v, vec4<TF> q) {
-  vec3<TF> r;
-  r.x = (TF(1) - TF(2) * (q.y * q.y + q.z * q.z)) * v.x + TF(2) * (q.x * q.y - q.z * q.w) * v.y +
-        TF(2) * (q.x * q.z + q.y * q.w) * v.z;
-  r.y = TF(2) * (q.x * q.y + q.z * q.w) * v.x + (TF(1) - TF(2) * (q.x * q.x + q.z * q.z)) * v.y +
-        TF(2) * (q.y * q.z - q.x * q.w) * v.z;
-  r.z = TF(2) * (q.x * q.z - q.y * q.w) * v.x + TF(2) * (q.y * q.z + q.x * q.w) * v.y +
-        (TF(1) - TF(2) * (q.x * q.x + q.y * q.y)) * v.z;
-  return r;
-}
-
-template <class TF>
-__device__ __forceinline__ TF box_sdf(vec3<TF> x, TF hx, TF hy, TF hz, TF outset) {
-  vec3<TF> d{fabs(x.x) - hx, fabs(x.y) - hy, fabs(x.z) - hz};
-  vec3<TF> cl{fmax(d.x, TF(0)), fmax(d.y, TF(0)), fmax(d.z, TF(0))};
-  return sqrt(length_sqr(cl)) + fmin(fmax(d.x, fmax(d.y, d.z)), TF(0)) - outset;
-}
-
-// Analytic signed distances (dg/box_distance.hpp:23-30,
-// dg/sphere_distance.hpp:18-20, dg/box_shell_distance.hpp:36-47) and the
-// torus |(|x_xz| - R, y)| - r.
-template <class TF>
-__device__ __forceinline__ TF shape_sdf(const BodyDev<TF>& b, vec3<TF> x) {
-  switch (b.shape) {
-    case AL_SHAPE_BOX:
-      return box_sdf(x, b.p[0], b.p[1], b.p[2], b.p[3]);
-    case AL_SHAPE_SPHERE:
-      return sqrt(length_sqr(x)) - b.p[0];
-    case AL_SHAPE_BOX_SHELL: {
-      TF inner = box_sdf(x, b.p[0], b.p[1], b.p[2], b.p[6]);
-      TF outer = box_sdf(x, b.p[3], b.p[4], b.p[5], b.p[6]);
-      return fmax(outer, -inner);
-    }
-    default: {
-      TF rho = sqrt(x.x * x.x + x.z * x.z) - b.p[0];
-      return sqrt(rho * rho + x.y * x.y) - b.p[1];
-    }
-  }
-}
-
-// Un-normalised outward direction: the position for a sphere
-// (sphere_distance.hpp:21), central differences with step h/256 otherwise
-// (box_distance.hpp:28-38).
-template <class TF>
-__device__ __forceinline__ vec3<TF> shape_gradient(const BodyDev<TF>& b, vec3<TF> x, TF h) {
-  if (b.shape == AL_SHAPE_SPHERE) return x;
-  const TF s = h * TF(0.00390625);
-  return vec3<TF>{shape_sdf(b, vec3<TF>{x.x + s, x.y, x.z}) - shape_sdf(b, vec3<TF>{x.x - s, x.y, x.z}),
-                  shape_sdf(b, vec3<TF>{x.x, x.y + s, x.z}) - shape_sdf(b, vec3<TF>{x.x, x.y - s, x.z}),
-                  shape_sdf(b, vec3<TF>{x.x, x.y, x.z + s}) - shape_sdf(b, vec3<TF>{x.x, x.y, x.z - s})};
-}
-
-// resolve (runner.hpp:1180-1195): cell of x and reference coordinates.
-template <class TF>
-__device__ __forceinline__ bool resolve(const BodyDev<TF>& b, vec3<TF> x, int ip[3],
-                                        vec3<TF>& xi) {
-  if (!(x.x >= b.dmin.x && x.y >= b.dmin.y && x.z >= b.dmin.z && b.dmax.x >= x.x &&
-        b.dmax.y >= x.y && b.dmax.z >= x.z))
-    return false;
-  const vec3<TF> inv{TF(1) / b.cs.x, TF(1) / b.cs.y, TF(1) / b.cs.z};
-  ip[0] = min(int((x.x - b.dmin.x) * inv.x), int(b.res[0]) - 1);
-  ip[1] = min(int((x.y - b.dmin.y) * inv.y), int(b.res[1]) - 1);
-  ip[2] = min(int((x.z - b.dmin.z) * inv.z), int(b.res[2]) - 1);
-  const vec3<TF> lo{b.dmin.x + b.cs.x * TF(ip[0]), b.dmin.y + b.cs.y * TF(ip[1]),
-                    b.dmin.z + b.cs.z * TF(ip[2])};
-  xi = vec3<TF>{TF(2) * (x.x - lo.x) * inv.x - TF(1), TF(2) * (x.y - lo.y) * inv.y - TF(1),
-                TF(2) * (x.z - lo.z) * inv.z - TF(1)};
-  return true;
-}
-
-// Linear index of the j-th node of cell ip (get_cells, runner.hpp:1197-1257):
-// 8 vertices, then per x-, y-, z-edge family four edges of two third-point
-// nodes.
-__device__ __forceinline__ uint32_t lagrange_node(const uint32_t r[3], uint32_t x, uint32_t y,
-                                                  uint32_t z, int j) {
-  const uint32_t nx = r[0], ny = r[1], nz = r[2];
-  if (j < 8)
-    return (nx + 1) * (ny + 1) * (z + ((j >> 2) & 1)) + (nx + 1) * (y + ((j >> 1) & 1)) + x +
-           (j & 1);
-  uint32_t base = (nx + 1) * (ny + 1) * (nz + 1);
-  if (j < 16) {
-    const int e = j - 8;
-    return base + 2 * (nx * (ny + 1) * (z + ((e >> 1) & 1)) + nx * (y + ((e >> 2) & 1)) + x) +
-           (e & 1);
-  }
-  base += 2 * nx * (ny + 1) * (nz + 1);
-  if (j < 24) {
-    const int e = j - 16;
-    return base + 2 * (ny * (nz + 1) * (x + ((e >> 1) & 1)) + ny * (z + ((e >> 2) & 1)) + y) +
-           (e & 1);
-  }
-  base += 2 * (nx + 1) * ny * (nz + 1);
-  const int e = j - 24;
-  return base + 2 * (nz * (nx + 1) * (y + ((e >> 1) & 1)) + nz * (x + ((e >> 2) & 1)) + z) +
-         (e & 1);
-}
-
-// Shape function j of the 32-node element at reference point p and,
-// if GRAD, its derivatives (the element of get_shape_function_and_gradient,
-// runner.hpp:1354-1584):
-//   corner: (1/64)(1+sx x)(1+sy y)(1+sz z)(9|p|^2 - 19)
-//   edge:   (9/64)(1-t^2)(1+3 s t)(1+s1 u)(1+s2 w)
-template <class TF, bool GRAD>
-__device__ __forceinline__ void shape_j(int j, vec3<TF> p, TF r2, TF& N, vec3<TF>& dN) {
-  const TF c64 = TF(1) / TF(64), e64 = TF(9) / TF(64);
-  if (j < 8) {
-    const TF sx = (j & 1) ? TF(1) : TF(-1), sy = (j & 2) ? TF(1) : TF(-1),
-             sz = (j & 4) ? TF(1) : TF(-1);
-    const TF ax = TF(1) + sx * p.x, ay = TF(1) + sy * p.y, az = TF(1) + sz * p.z;
-    const TF f = TF(9) * r2 - TF(19);
-    N = c64 * ax * ay * az * f;
-    if (GRAD) {
-      dN.x = c64 * ay * az * (sx * f + TF(18) * p.x * ax);
-      dN.y = c64 * ax * az * (sy * f + TF(18) * p.y * ay);
-      dN.z = c64 * ax * ay * (sz * f + TF(18) * p.z * az);
-    }
-    return;
-  }
-  // family: axis of the edge, and the axes selected by bits 1 and 2
-  int axis, a1, a2, e;
-  if (j < 16) {
-    e = j - 8;
-    axis = 0;
-    a1 = 2;
-    a2 = 1;
-  } else if (j < 24) {
-    e = j - 16;
-    axis = 1;
-    a1 = 0;
-    a2 = 2;
-  } else {
-    e = j - 24;
-    axis = 2;
-    a1 = 1;
-    a2 = 0;
-  }
-  const TF u[3] = {p.x, p.y, p.z};
-  const TF s = (e & 1) ? TF(1) : TF(-1), s1 = (e & 2) ? TF(1) : TF(-1),
-           s2 = (e & 4) ? TF(1) : TF(-1);
-  const TF t = u[axis], A = TF(1) + s1 * u[a1], B = TF(1) + s2 * u[a2];
-  const TF g = (TF(1) - t * t) * (TF(1) + TF(3) * s * t);
-  N = e64 * g * A * B;
-  if (GRAD) {
-    const TF dg = TF(3) * s * (TF(1) - t * t) - TF(2) * t * (TF(1) + TF(3) * s * t);
-    TF d[3];
-    d[axis] = e64 * dg * A * B;
-    d[a1] = e64 * g * s1 * B;
-    d[a2] = e64 * g * A * s2;
-    dN = vec3<TF>{d[0], d[1], d[2]};
-  }
-}
-
-// Interpolated value of `nodes` at x (interpolate_distance_without_
-// intermediates, runner.hpp:1596-1614): +max outside the domain.
-template <class TF>
-__device__ __forceinline__ TF interpolate_grid(const BodyDev<TF>& b, const TF* __restrict__ nodes,
-                                               vec3<TF> x) {
-  int ip[3];
-  vec3<TF> xi;
-  if (!resolve(b, x, ip, xi)) return max_value<TF>();
-  const TF r2 = xi.x * xi.x + xi.y * xi.y + xi.z * xi.z;
-  TF phi = 0;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    TF N;
-    vec3<TF> dN;
-    shape_j<TF, false>(j, xi, r2, N, dN);
-    phi += __ldg(nodes + lagrange_node(b.res, ip[0], ip[1], ip[2], j)) * N;
-  }
-  return phi;
-}
 
 // Boundary sample of one particle against one body
 // (compute_volume_and_boundary_x[_analytic], runner.hpp:1696-1771, and the

@@ -519,6 +519,48 @@ AL_API int al_df_step_warm_f32(al_engine* engine, const al_const_f32* cn, const 
                                const al_warm_start* warm, float* dt, al_step_report* report,
                                void* stream);
 
+/* ------------------------------------------------------------- contacts
+ * Rigid-rigid contacts on the device: Pile::find_contacts (pile.hpp:886-900,
+ * volume-map branch) with collision_test (runner.hpp:3833-4010; analytic
+ * distance for analytic bodies, the distance grid through
+ * collision_find_dist_normal, runner.hpp:1793-1822, for bodies with
+ * use_distance_grid) and Pile::solve_contacts (pile.hpp:906-979).  The
+ * reference appends contacts with an atomic counter, so its contact order
+ * and hence its sequential-impulse result vary from run to run; the
+ * engine lists contacts in (i, j, vertex) order, deterministically. */
+typedef struct al_contact_body_f32 {
+  const float* vertices;  /* device [num_vertices][3], body frame (collision vertices) */
+  uint32_t num_vertices;
+  float restitution;      /* pair restitution: product of the two bodies' */
+  float friction;         /* pair friction: sum of the two bodies' */
+  uint32_t reserved;
+} al_contact_body_f32;
+
+/* Contact<float3, float> (contact.hpp:8-25). */
+typedef struct al_contact_f32 {
+  uint32_t i, j;
+  float cp_i[3], cp_j[3], n[3], t[3];
+  float iiwi_diag[3], iiwi_off_diag[3], iiwj_diag[3], iiwj_off_diag[3];
+  float friction, nkninv, pmax, goalu, impulse_sum;
+} al_contact_f32;
+
+/* Tests every collision vertex of body i against body j for each ordered
+ * pair i != j (not both kinematic, mass 0) and writes the contacts
+ * (dist - contact_tolerance < 0) to `contacts` (device, up to
+ * max_contacts) in (i, j, vertex) order; *num_found (host) receives the
+ * count found, which may exceed max_contacts (the reference then clamps,
+ * pile.hpp:908-914).  bodies / rigid / contact_bodies: host arrays. */
+AL_API int al_find_contacts_f32(al_engine* engine, const al_body_f32* bodies,
+                                const al_rigid_f32* rigid,
+                                const al_contact_body_f32* contact_bodies, uint32_t num_bodies,
+                                float contact_tolerance, uint32_t max_contacts,
+                                al_contact_f32* contacts, uint32_t* num_found, void* stream);
+/* Five sequential-impulse sweeps over contacts[0, num_contacts) (device),
+ * in order, on the device; rigid (host in/out): v and omega updated. */
+AL_API int al_solve_contacts_f32(al_engine* engine, const al_body_f32* bodies,
+                                 al_rigid_f32* rigid, uint32_t num_bodies,
+                                 al_contact_f32* contacts, uint32_t num_contacts, void* stream);
+
 /* ------------------------------------------------------- batched scenes
  * No reference counterpart (the reference advances one scene per call).
  * Advances every scene by one DFSPH step (each with its own dt, iteration

@@ -25,6 +25,9 @@ def lib():
             "orc_num_grid_nodes": (_U, [_P]),
             "orc_shape_functions_f64": (None, [_P, _P, _P]),
             "orc_cell_nodes": (None, [_P, _P, _P]),
+            # bodies, rigid, contact bodies, nb, tolerance, max, out -> count
+            "orc_find_contacts_f32": (_U, [_P, _P, _P, _U, ctypes.c_float, _U, _P]),
+            "orc_solve_contacts_f32": (None, [_P, _P, _U, _P, _U]),
         }
         for s in ("f32", "f64"):
             sig["orc_grid_sort_" + s] = (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P])
@@ -184,3 +187,20 @@ def run(method, cn, cni, bodies, rigid, state, sp, dt, steps):
             _p(state["a"]), _p(sp), _p(dt_arr), steps, _p(reports))
     assert status == 0
     return float(dt_arr[0]), list(reports)
+
+
+def find_contacts(bodies, rigid, contact_bodies, tolerance, max_contacts):
+    """Pile::find_contacts restated: (count found, ContactF32 array) with HOST
+    pointers in bodies (node arrays) and contact_bodies (vertices)."""
+    from alluvion_b200 import _capi
+    out = (_capi.ContactF32 * max(max_contacts, 1))()
+    nb = len(contact_bodies)
+    cb = (_capi.ContactBodyF32 * max(nb, 1))(*contact_bodies)
+    n = lib().orc_find_contacts_f32(_p(bodies), _p(rigid), _p(cb), nb, float(tolerance),
+                                    max_contacts, _p(out))
+    return int(n), out
+
+
+def solve_contacts(bodies, rigid, contacts, num):
+    """Pile::solve_contacts restated: updates rigid (RigidF32 array) in place."""
+    lib().orc_solve_contacts_f32(_p(bodies), _p(rigid), len(rigid), _p(contacts), num)

@@ -388,3 +388,103 @@ int orc_ii_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ contacts
+namespace {
+
+template <class TF, class CB>
+void load_contact_bodies(const al_body_f32* bodies, const al_rigid_f32* rigid, const CB* cb,
+                         uint32_t nb, std::vector<Body<TF>>& B, std::vector<const TF*>& verts,
+                         std::vector<uint32_t>& nv, std::vector<TF>& rest, std::vector<TF>& fric) {
+  for (uint32_t b = 0; b < nb; ++b) {
+    B.push_back(make_body<TF>(bodies[b], reinterpret_cast<const TF*>(&rigid[b])));
+    verts.push_back(cb[b].vertices);
+    nv.push_back(cb[b].num_vertices);
+    rest.push_back(cb[b].restitution);
+    fric.push_back(cb[b].friction);
+  }
+}
+
+void to_abi(const Contact<float>& c, al_contact_f32& o) {
+  auto put = [](float* d, V3<float> v) {
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+  };
+  o.i = c.i;
+  o.j = c.j;
+  put(o.cp_i, c.cp_i);
+  put(o.cp_j, c.cp_j);
+  put(o.n, c.n);
+  put(o.t, c.t);
+  put(o.iiwi_diag, c.iiwi_diag);
+  put(o.iiwi_off_diag, c.iiwi_off);
+  put(o.iiwj_diag, c.iiwj_diag);
+  put(o.iiwj_off_diag, c.iiwj_off);
+  o.friction = c.friction;
+  o.nkninv = c.nkninv;
+  o.pmax = c.pmax;
+  o.goalu = c.goalu;
+  o.impulse_sum = c.impulse_sum;
+}
+
+Contact<float> from_abi(const al_contact_f32& o) {
+  Contact<float> c;
+  c.i = o.i;
+  c.j = o.j;
+  c.cp_i = v3<float>(o.cp_i);
+  c.cp_j = v3<float>(o.cp_j);
+  c.n = v3<float>(o.n);
+  c.t = v3<float>(o.t);
+  c.iiwi_diag = v3<float>(o.iiwi_diag);
+  c.iiwi_off = v3<float>(o.iiwi_off_diag);
+  c.iiwj_diag = v3<float>(o.iiwj_diag);
+  c.iiwj_off = v3<float>(o.iiwj_off_diag);
+  c.friction = o.friction;
+  c.nkninv = o.nkninv;
+  c.pmax = o.pmax;
+  c.goalu = o.goalu;
+  c.impulse_sum = o.impulse_sum;
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Pile::find_contacts with HOST vertex and node pointers; writes up to
+// max_contacts contacts in (i, j, vertex) order and returns the count found.
+uint32_t orc_find_contacts_f32(const al_body_f32* bodies, const al_rigid_f32* rigid,
+                               const al_contact_body_f32* cb, uint32_t nb, float tol,
+                               uint32_t max_contacts, al_contact_f32* out) {
+  std::vector<Body<float>> B;
+  std::vector<const float*> verts;
+  std::vector<uint32_t> nv;
+  std::vector<float> rest, fric;
+  load_contact_bodies<float>(bodies, rigid, cb, nb, B, verts, nv, rest, fric);
+  std::vector<Contact<float>> cs;
+  find_contacts(B, verts, nv, rest, fric, tol, cs);
+  for (size_t k = 0; k < cs.size() && k < max_contacts; ++k) to_abi(cs[k], out[k]);
+  return uint32_t(cs.size());
+}
+
+// Pile::solve_contacts: updates rigid[b].v / omega in place.
+void orc_solve_contacts_f32(const al_body_f32* bodies, al_rigid_f32* rigid, uint32_t nb,
+                            const al_contact_f32* contacts, uint32_t num_contacts) {
+  std::vector<Body<float>> B;
+  for (uint32_t b = 0; b < nb; ++b)
+    B.push_back(make_body<float>(bodies[b], reinterpret_cast<const float*>(&rigid[b])));
+  std::vector<Contact<float>> cs;
+  for (uint32_t k = 0; k < num_contacts; ++k) cs.push_back(from_abi(contacts[k]));
+  solve_contacts(B, cs);
+  for (uint32_t b = 0; b < nb; ++b) {
+    rigid[b].v[0] = B[b].v.x;
+    rigid[b].v[1] = B[b].v.y;
+    rigid[b].v[2] = B[b].v.z;
+    rigid[b].omega[0] = B[b].omega.x;
+    rigid[b].omega[1] = B[b].omega.y;
+    rigid[b].omega[2] = B[b].omega.z;
+  }
+}
+
+}  // extern "C"

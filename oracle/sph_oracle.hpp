@@ -1310,4 +1310,187 @@ StepReport ii_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& b
   return rep;
 }
 
+// ---------------------------------------------------------------- contacts
+// Rigid-rigid contacts: Contact (contact.hpp:8-25), collision_test
+// (runner.hpp:3833-4010; analytic distance for analytic bodies, the
+// distance grid through collision_find_dist_normal, runner.hpp:1793-1822,
+// for grid bodies), Pile::find_contacts (pile.hpp:886-900, volume-map
+// branch) and Pile::solve_contacts (pile.hpp:906-979).  The reference
+// appends contacts with an atomic counter, so its order (and the
+// sequential-impulse result) is not reproducible; here contacts are listed
+// in (i, j, vertex) order, the order of its loops.
+template <class TF>
+struct Contact {
+  uint32_t i, j;
+  V3<TF> cp_i, cp_j, n, t;
+  V3<TF> iiwi_diag, iiwi_off, iiwj_diag, iiwj_off;
+  TF friction, nkninv, pmax, goalu, impulse_sum;
+};
+
+// calculate_congruent_matrix (runner.hpp:178-199): R diag(v) R^T.
+template <class TF>
+void congruent_matrix(V3<TF> v, V4<TF> q, V3<TF>& diag, V3<TF>& off) {
+  TF m00 = 1 - 2 * (q.y * q.y + q.z * q.z), m01 = 2 * (q.x * q.y - q.z * q.w),
+     m02 = 2 * (q.x * q.z + q.y * q.w);
+  TF m10 = 2 * (q.x * q.y + q.z * q.w), m11 = 1 - 2 * (q.x * q.x + q.z * q.z),
+     m12 = 2 * (q.y * q.z - q.x * q.w);
+  TF m20 = 2 * (q.x * q.z - q.y * q.w), m21 = 2 * (q.y * q.z + q.x * q.w),
+     m22 = 1 - 2 * (q.x * q.x + q.y * q.y);
+  diag = {v.x * m00 * m00 + v.y * m01 * m01 + v.z * m02 * m02,
+          v.x * m10 * m10 + v.y * m11 * m11 + v.z * m12 * m12,
+          v.x * m20 * m20 + v.y * m21 * m21 + v.z * m22 * m22};
+  off = {v.x * m00 * m10 + v.y * m01 * m11 + v.z * m02 * m12,
+         v.x * m00 * m20 + v.y * m01 * m21 + v.z * m02 * m22,
+         v.x * m10 * m20 + v.y * m11 * m21 + v.z * m12 * m22};
+}
+
+// apply_congruent (runner.hpp:253-262).
+template <class TF>
+V3<TF> apply_congruent(V3<TF> v, V3<TF> d, V3<TF> o) {
+  return {v.x * d.x + v.y * o.x + v.z * o.y, v.x * o.x + v.y * d.y + v.z * o.z,
+          v.x * o.y + v.y * o.z + v.z * d.z};
+}
+
+// calculate_congruent_k (runner.hpp:264-288).
+template <class TF>
+void congruent_k(V3<TF> r, TF mass, V3<TF> d, V3<TF> o, V3<TF>& kd, V3<TF>& ko) {
+  kd = {0, 0, 0};
+  ko = {0, 0, 0};
+  if (mass == 0) return;
+  TF im = 1 / mass;
+  kd.x = r.z * r.z * d.y - r.y * r.z * o.z * 2 + r.y * r.y * d.z + im;
+  kd.y = r.z * r.z * d.x - r.x * r.z * o.y * 2 + r.x * r.x * d.z + im;
+  kd.z = r.y * r.y * d.x - r.x * r.y * o.x * 2 + r.x * r.x * d.y + im;
+  ko.x = -r.z * r.z * o.x + r.x * r.z * o.z + r.y * r.z * o.y - r.x * r.y * d.z;
+  ko.y = r.y * r.z * o.x - r.x * r.z * d.y - r.y * r.y * o.y + r.x * r.y * o.z;
+  ko.z = -(r.y * r.z * d.x) + r.x * r.z * o.x + r.x * r.y * o.y - r.x * r.x * o.z;
+}
+
+template <class TF>
+V3<TF> operator/(V3<TF> a, TF s) {
+  return {a.x / s, a.y / s, a.z / s};
+}
+
+// One vertex of body i against body j; returns true and fills `ct` on contact.
+template <class TF>
+bool contact_test(const Body<TF>& bi, const Body<TF>& bj, uint32_t i, uint32_t j, V3<TF> vertex,
+                  TF tol, TF restitution, TF friction, Contact<TF>& ct) {
+  ct.cp_i = rotate(vertex, bi.q) + bi.x;
+  const V3<TF> local = rotate(ct.cp_i - bj.x, conjugate(bj.q));
+  TF dist;
+  V3<TF> n{0, 0, 0};
+  if (bj.use_grid) {
+    dist = bj.sign;  // outside the map: only the existence of a collision is known
+    V3<TF> nt{0, 1, 0};
+    int ip[3];
+    V3<TF> xi;
+    if (resolve(bj.dmin, bj.dmax, bj.res, bj.cs, local, ip, xi)) {
+      TF N[32], d0[32], d1[32], d2[32];
+      uint32_t cells[32];
+      shape_functions<TF>(xi, N, d0, d1, d2);
+      cell_nodes(bj.res, ip, cells);
+      TF phi = 0;
+      V3<TF> g{0, 0, 0};
+      for (int k = 0; k < 32; ++k) {
+        const TF c = bj.dist_nodes[cells[k]];
+        phi += c * N[k];
+        g.x += c * d0[k];
+        g.y += c * d1[k];
+        g.z += c * d2[k];
+      }
+      g.x *= TF(2) / bj.cs.x;
+      g.y *= TF(2) / bj.cs.y;
+      g.z *= TF(2) / bj.cs.z;
+      dist = bj.sign * phi - tol;
+      nt = g * bj.sign;
+    }
+    if (dist < 0) n = normalized(nt);
+  } else {
+    dist = bj.sdf.sdf(local) * bj.sign - tol;
+    n = normalized(bj.sdf.gradient(local, TF(1e-3)) * bj.sign);
+  }
+  if (!(dist < 0)) return false;
+  const V3<TF> cp = local - dist * n;
+  ct.i = i;
+  ct.j = j;
+  ct.cp_j = rotate(cp, bj.q) + bj.x;
+  ct.n = rotate(n, bj.q);
+  ct.friction = friction;
+  const V3<TF> ri = ct.cp_i - bi.x, rj = ct.cp_j - bj.x;
+  const V3<TF> ui = bi.v + cross(bi.omega, ri), uj = bj.v + cross(bj.omega, rj);
+  const V3<TF> urel = ui - uj;
+  const TF urn = dot(ct.n, urel);
+  ct.t = urel - urn * ct.n;
+  if (length_sqr(ct.t) > TF(1e-6)) ct.t = normalized(ct.t);
+  congruent_matrix(V3<TF>{1 / bi.inertia.x, 1 / bi.inertia.y, 1 / bi.inertia.z}, bi.q,
+                   ct.iiwi_diag, ct.iiwi_off);
+  congruent_matrix(V3<TF>{1 / bj.inertia.x, 1 / bj.inertia.y, 1 / bj.inertia.z}, bj.q,
+                   ct.iiwj_diag, ct.iiwj_off);
+  V3<TF> kid, kio, kjd, kjo;
+  congruent_k(ri, bi.mass, ct.iiwi_diag, ct.iiwi_off, kid, kio);
+  congruent_k(rj, bj.mass, ct.iiwj_diag, ct.iiwj_off, kjd, kjo);
+  const V3<TF> kd = kid + kjd, ko = kio + kjo;
+  ct.nkninv = 1 / dot(ct.n, apply_congruent(ct.n, kd, ko));
+  ct.pmax = 1 / dot(ct.t, apply_congruent(ct.t, kd, ko)) * dot(urel, ct.t);
+  ct.goalu = urn < 0 ? -restitution * urn : TF(0);
+  ct.impulse_sum = 0;
+  return true;
+}
+
+// Pile::find_contacts over every ordered pair (i, j), i != j, not both
+// kinematic; restitution r_i r_j, friction f_i + f_j.
+template <class TF>
+void find_contacts(const std::vector<Body<TF>>& bodies, const std::vector<const TF*>& vertices,
+                   const std::vector<uint32_t>& num_vertices, const std::vector<TF>& restitution,
+                   const std::vector<TF>& friction, TF tol, std::vector<Contact<TF>>& out) {
+  out.clear();
+  const uint32_t nb = uint32_t(bodies.size());
+  for (uint32_t i = 0; i < nb; ++i)
+    for (uint32_t j = 0; j < nb; ++j) {
+      if (i == j || (bodies[i].mass == 0 && bodies[j].mass == 0)) continue;
+      for (uint32_t v = 0; v < num_vertices[i]; ++v) {
+        Contact<TF> ct;
+        const TF* p = vertices[i] + 3 * size_t(v);
+        if (contact_test(bodies[i], bodies[j], i, j, V3<TF>{p[0], p[1], p[2]}, tol,
+                         restitution[i] * restitution[j], friction[i] + friction[j], ct))
+          out.push_back(ct);
+      }
+    }
+}
+
+// Pile::solve_contacts: five sequential-impulse sweeps in contact order.
+template <class TF>
+void solve_contacts(std::vector<Body<TF>>& bodies, std::vector<Contact<TF>>& contacts) {
+  for (int sweep = 0; sweep < 5; ++sweep)
+    for (Contact<TF>& c : contacts) {
+      Body<TF>& bi = bodies[c.i];
+      Body<TF>& bj = bodies[c.j];
+      const TF depth = dot(c.n, c.cp_i - c.cp_j);
+      const V3<TF> ri = c.cp_i - bi.x, rj = c.cp_j - bj.x;
+      const V3<TF> ui = bi.v + cross(bi.omega, ri), uj = bj.v + cross(bj.omega, rj);
+      const V3<TF> urel = ui - uj;
+      const TF urn = dot(c.n, urel);
+      TF corr = c.nkninv * (c.goalu - urn);
+      if (corr < -c.impulse_sum) corr = -c.impulse_sum;
+      if (depth < 0) corr -= c.nkninv * depth;  // stiffness 1
+      V3<TF> p = corr * c.n;
+      c.impulse_sum += corr;
+      const TF pn = dot(p, c.n);
+      if (c.friction * pn > c.pmax)
+        p -= c.pmax * c.t;
+      else if (c.friction * pn < -c.pmax)
+        p += c.pmax * c.t;
+      else
+        p -= c.friction * pn * c.t;
+      if (bi.mass != 0) {
+        bi.v += p / bi.mass;
+        bi.omega += apply_congruent(cross(ri, p), c.iiwi_diag, c.iiwi_off);
+      }
+      if (bj.mass != 0) {
+        bj.v += -p / bj.mass;
+        bj.omega += apply_congruent(cross(rj, -p), c.iiwj_diag, c.iiwj_off);
+      }
+    }
+}
+
 }  // namespace oracle
