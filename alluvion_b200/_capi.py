@@ -24,7 +24,7 @@ AL_ERR_CELL_OVERFLOW = 4
 AL_ERR_NEIGHBOR_OVERFLOW = 5
 ANOMALY_STATUSES = (AL_ERR_OUT_OF_GRID, AL_ERR_CELL_OVERFLOW, AL_ERR_NEIGHBOR_OVERFLOW)
 
-SHAPE_BOX, SHAPE_SPHERE, SHAPE_BOX_SHELL, SHAPE_TORUS = 0, 1, 2, 3
+SHAPE_BOX, SHAPE_SPHERE, SHAPE_BOX_SHELL, SHAPE_TORUS, SHAPE_MESH = 0, 1, 2, 3, 4
 
 
 def _const_struct(name, real):
@@ -228,6 +228,8 @@ _SIGNATURES = {
     "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
     "al_df_step_warm_f32": (ctypes.c_int, [_P] * 8 + [_P, _P, _P]),
     "al_df_batch_step_f32": (ctypes.c_int, [_P, _P, _U, _P]),
+    "al_build_mesh_distance_grid_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, ctypes.c_float,
+                                                       _P, _P]),
     "al_find_contacts_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, ctypes.c_float, _U, _P, _P,
                                             _P]),
     "al_solve_contacts_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _P]),

@@ -148,42 +148,6 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-// index_to_node_position (runner.hpp:1131-1178).
-template <class TF>
-__device__ __forceinline__ vec3<TF> node_position(const BodyDev<TF>& b, uint32_t l) {
-  const uint32_t nx = b.res[0], ny = b.res[1], nz = b.res[2];
-  const uint32_t nv = (nx + 1) * (ny + 1) * (nz + 1);
-  const uint32_t nex = nx * (ny + 1) * (nz + 1);
-  const uint32_t ney = (nx + 1) * ny * (nz + 1);
-  auto at = [&](uint32_t a, uint32_t bb, uint32_t cc) {
-    return vec3<TF>{b.dmin.x + b.cs.x * TF(a), b.dmin.y + b.cs.y * TF(bb),
-                    b.dmin.z + b.cs.z * TF(cc)};
-  };
-  if (l < nv) {
-    const uint32_t t = l % ((ny + 1) * (nx + 1));
-    return at(t % (nx + 1), t / (nx + 1), l / ((ny + 1) * (nx + 1)));
-  }
-  if (l < nv + 2 * nex) {
-    l -= nv;
-    const uint32_t e = l / 2, t = e % ((ny + 1) * nx);
-    vec3<TF> p = at(t % nx, t / nx, e / ((ny + 1) * nx));
-    p.x += (TF(1) + TF(l % 2)) / TF(3) * b.cs.x;
-    return p;
-  }
-  if (l < nv + 2 * (nex + ney)) {
-    l -= nv + 2 * nex;
-    const uint32_t e = l / 2, t = e % ((nz + 1) * ny);
-    vec3<TF> p = at(e / ((nz + 1) * ny), t % ny, t / ny);
-    p.y += (TF(1) + TF(l % 2)) / TF(3) * b.cs.y;
-    return p;
-  }
-  l -= nv + 2 * (nex + ney);
-  const uint32_t e = l / 2, t = e % ((nx + 1) * nz);
-  vec3<TF> p = at(t / nz, e / ((nx + 1) * nz), t % nz);
-  p.z += (TF(1) + TF(l % 2)) / TF(3) * b.cs.z;
-  return p;
-}
-
 template <class TF>
 __global__ void k_node_positions(BodyDev<TF> b, TF* __restrict__ out) {
   const uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;

@@ -59,6 +59,8 @@ int volume_impl(al_engine* e, const C* cn, const B* body, TF* out, cudaStream_t 
 template <class TF, class B>
 int distance_impl(al_engine* e, const B* body, TF* out, cudaStream_t st) {
   ALB_CHECK_ARG(e && body && out, "al_build_distance_grid: null argument");
+  ALB_CHECK_ARG(body->shape != AL_SHAPE_MESH,
+                "al_build_distance_grid: mesh bodies use al_build_mesh_distance_grid_f32");
   ALB_TRY(e->activate());
   const BodyDev<TF> b = to_body_dev<TF>(*body);
   ALB_TRY(validate_body(b, false, false));

@@ -121,7 +121,7 @@ def shape_aabb(shape, params):
         R, rr = p[0], p[1]
         e = np.array([R + rr, rr, R + rr])
         return -e, e, R + rr
-    raise ValueError("unknown shape %r" % shape)
+    raise ValueError("unknown shape %r (mesh bodies pass aabb= to make_body)" % shape)
 
 
 def box_params(widths, outset=0.0):
@@ -136,18 +136,19 @@ def box_shell_params(inner_widths, thickness, outset=0.0):
 
 
 def make_body(dtype, cn, shape, params, resolution, sign=1.0, margin=None,
-              use_distance_grid=False, mass=0.0, inertia=(1.0, 1.0, 1.0)):
+              use_distance_grid=False, mass=0.0, inertia=(1.0, 1.0, 1.0), aabb=None):
     """al_body_{f32,f64} with the domain of Pile::calculate_domain_and_resolution
     (pile.hpp:40-65; margin defaults to h for sign < 0, 2h otherwise) and the
     grid attributes of Pile::calculate_grid_attributes (pile.hpp:66-78).
-    Node pointers are left NULL."""
+    Node pointers are left NULL.  aabb: (min, max, max_distance) of a mesh
+    body (AL_SHAPE_MESH), whose extent does not follow from params."""
     T = np.dtype(dtype).type
     _, BodyT, _, _ = _capi.real_types(dtype)
     h = T(cn.kernel_radius)
     if margin is None:
         margin = h if sign < 0 else h * T(2)
     margin = T(margin)
-    lo, hi, maxd = shape_aabb(shape, params)
+    lo, hi, maxd = shape_aabb(shape, params) if aabb is None else aabb
     b = BodyT()
     b.shape = shape
     b.use_distance_grid = int(bool(use_distance_grid))
@@ -250,13 +251,27 @@ class DeviceScene:
         self.bodies = (BodyT * max(nb, 1))()
         self.rigid = (RigidT * max(nb, 1))()
         for b, spec in enumerate(self.body_specs):
-            body = make_body(dtype, cn, spec["shape"], spec["params"], spec["resolution"],
-                             sign=spec.get("sign", 1.0), margin=spec.get("margin"),
-                             use_distance_grid=spec.get("use_distance_grid", False),
-                             mass=spec.get("mass", 0.0), inertia=spec.get("inertia", (1, 1, 1)))
+            mesh = spec.get("mesh")  # (vertices [nv][3], faces [nf][3]) for SHAPE_MESH
+            aabb = mesh_aabb(mesh[0], spec.get("offset", 0.0)) if mesh is not None else None
+            body = make_body(dtype, cn, spec["shape"], spec.get("params", []),
+                             spec["resolution"], sign=spec.get("sign", 1.0),
+                             margin=spec.get("margin"),
+                             use_distance_grid=mesh is not None or spec.get("use_distance_grid",
+                                                                            False),
+                             mass=spec.get("mass", 0.0), inertia=spec.get("inertia", (1, 1, 1)),
+                             aabb=aabb)
             dist = zeros(body.num_nodes) if body.use_distance_grid else None
             vol = zeros(body.num_nodes)
-            if dist is not None:
+            if mesh is not None:
+                assert self.sfx == "f32", "mesh bodies: float32 scenes"
+                v = np.ascontiguousarray(mesh[0], np.float32)
+                f = np.ascontiguousarray(mesh[1], np.uint32)
+                body.distance_nodes = dist.data_ptr()
+                _capi.check(_capi.lib().al_build_mesh_distance_grid_f32(
+                    engine.handle, _capi.ptr(body), v.ctypes.data, len(v), f.ctypes.data, len(f),
+                    ctypes.c_float(spec.get("offset", 0.0)), _capi.ptr(dist), None),
+                    "al_build_mesh_distance_grid_f32")
+            elif dist is not None:
                 body.distance_nodes = dist.data_ptr()
                 _capi.check(getattr(_capi.lib(), "al_build_distance_grid_" + self.sfx)(
                     engine.handle, _capi.ptr(body), _capi.ptr(dist), None),
@@ -456,3 +471,72 @@ def batch_step(engine, scene_list, sp, dts, stream=None, allow=()):
     status = _capi.lib().al_df_batch_step_f32(engine.handle, arr, k, stream)
     _capi.check(status, "al_df_batch_step_f32", allow=allow)
     return [d.value for d in dt_c], reps, [arr[i].status for i in range(k)]
+
+
+# ------------------------------------------------------------------ meshes
+def mesh_aabb(vertices, offset=0.0):
+    """(min, max, max_distance) of a mesh, as MeshDistance computes them
+    (dg/mesh_distance.hpp:105-125): the vertex box grown by the offset, and
+    the largest vertex radius plus the offset."""
+    v = np.asarray(vertices, np.float64)
+    return (v.min(0) - offset, v.max(0) + offset,
+            float(np.sqrt((v * v).sum(1).max())) + offset)
+
+
+def cube_mesh(half):
+    """Closed box mesh [-half, half]^3 (12 triangles, outward winding)."""
+    h = np.broadcast_to(np.asarray(half, np.float64), (3,))
+    v = np.array([[x, y, z] for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)]) * h
+    faces = [(0, 1, 3), (0, 3, 2), (4, 6, 7), (4, 7, 5), (0, 4, 5), (0, 5, 1),
+             (2, 3, 7), (2, 7, 6), (0, 2, 6), (0, 6, 4), (1, 5, 7), (1, 7, 3)]
+    return v.astype(np.float32), np.asarray(faces, np.uint32)
+
+
+def icosphere(radius, subdivisions=2):
+    """Closed sphere mesh: an icosahedron subdivided `subdivisions` times
+    with the new vertices projected to the sphere (outward winding)."""
+    t = (1 + 5 ** 0.5) / 2
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t),
+         (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    v = [np.asarray(p, np.float64) / np.linalg.norm(p) for p in v]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+         (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+         (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[key] = len(v) - 1
+            return cache[key]
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    return (np.asarray(v) * radius).astype(np.float32), np.asarray(f, np.uint32)
+
+
+def load_obj(path):
+    """Vertices [nv][3] and triangles [nf][3] of a Wavefront OBJ file (the
+    format Mesh reads for MeshDistance bodies); polygons are fanned into
+    triangles, `v/vt/vn` face entries and negative indices are accepted."""
+    verts, faces = [], []
+    with open(path) as fh:
+        for line in fh:
+            parts = line.split()
+            if not parts:
+                continue
+            if parts[0] == "v":
+                verts.append([float(x) for x in parts[1:4]])
+            elif parts[0] == "f":
+                idx = []
+                for p in parts[1:]:
+                    k = int(p.split("/")[0])
+                    idx.append(k - 1 if k > 0 else len(verts) + k)
+                for j in range(1, len(idx) - 1):
+                    faces.append((idx[0], idx[j], idx[j + 1]))
+    return np.asarray(verts, np.float32), np.asarray(faces, np.uint32)

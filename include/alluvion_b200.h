@@ -115,7 +115,9 @@ typedef enum al_shape {
   AL_SHAPE_BOX = 0,       /* shape_params: half widths x y z, outset */
   AL_SHAPE_SPHERE = 1,    /* shape_params: radius */
   AL_SHAPE_BOX_SHELL = 2, /* shape_params: inner half widths xyz, outer half widths xyz, outset */
-  AL_SHAPE_TORUS = 3      /* shape_params: major radius (x-z plane), minor radius */
+  AL_SHAPE_TORUS = 3,     /* shape_params: major radius (x-z plane), minor radius */
+  AL_SHAPE_MESH = 4       /* triangle mesh: distance_nodes from al_build_mesh_distance_grid_f32
+                             (MeshDistance, dg/mesh_distance.hpp); use_distance_grid must be 1 */
 } al_shape;
 
 typedef struct al_body_f32 {
@@ -377,6 +379,18 @@ AL_API int al_node_positions_f32(al_engine* engine, const al_body_f32* body, flo
                                  void* stream);
 AL_API int al_node_positions_f64(al_engine* engine, const al_body_f64* body, double* positions,
                                  void* stream);
+
+/* Distance grid of a triangle-mesh body (AL_SHAPE_MESH), on the device: the
+ * grid Pile builds on the host for MeshDistance bodies (pile.hpp:79-94,
+ * 512-521; MeshDistance::signedDistance, dg/mesh_distance.hpp:186-223):
+ * exact point-triangle distance, sign from angle-weighted pseudonormals of
+ * the nearest feature, minus `offset`.  The mesh (host arrays, body frame)
+ * must be a closed 2-manifold, as the reference requires.  body: domain,
+ * resolution and num_nodes; nodes: device [num_nodes].  Synchronous. */
+AL_API int al_build_mesh_distance_grid_f32(al_engine* engine, const al_body_f32* body,
+                                           const float* vertices, uint32_t num_vertices,
+                                           const uint32_t* faces, uint32_t num_faces,
+                                           float offset, float* nodes, void* stream);
 
 /* ------------------------------------------------------------ fluid steps
  * The caller-owned particle buffers of one solver (solver.hpp:286-305,

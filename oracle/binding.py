@@ -28,6 +28,7 @@ def lib():
             # bodies, rigid, contact bodies, nb, tolerance, max, out -> count
             "orc_find_contacts_f32": (_U, [_P, _P, _P, _U, ctypes.c_float, _U, _P]),
             "orc_solve_contacts_f32": (None, [_P, _P, _U, _P, _U]),
+            "orc_mesh_distance_grid_f32": (None, [_P, _P, _U, _P, _U, ctypes.c_float, _P]),
         }
         for s in ("f32", "f64"):
             sig["orc_grid_sort_" + s] = (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P])
@@ -204,3 +205,13 @@ def find_contacts(bodies, rigid, contact_bodies, tolerance, max_contacts):
 def solve_contacts(bodies, rigid, contacts, num):
     """Pile::solve_contacts restated: updates rigid (RigidF32 array) in place."""
     lib().orc_solve_contacts_f32(_p(bodies), _p(rigid), len(rigid), _p(contacts), num)
+
+
+def mesh_distance_grid(body, vertices, faces, offset=0.0):
+    """MeshDistance::signedDistance at the nodes of `body` (al_body_f32)."""
+    v = np.ascontiguousarray(vertices, np.float32)
+    f = np.ascontiguousarray(faces, np.uint32)
+    out = np.zeros(body.num_nodes, np.float32)
+    lib().orc_mesh_distance_grid_f32(_p(body), _p(v), len(v), _p(f), len(f), float(offset),
+                                     _p(out))
+    return out

@@ -488,3 +488,19 @@ void orc_solve_contacts_f32(const al_body_f32* bodies, al_rigid_f32* rigid, uint
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Distance grid of a mesh body: node positions of `b`, signed distances
+// to the mesh (host arrays) minus offset.
+void orc_mesh_distance_grid_f32(const al_body_f32* b, const float* verts, uint32_t nv,
+                                const uint32_t* faces, uint32_t nf, float offset, float* out) {
+  const Body<float> body = make_body<float>(*b, nullptr);
+  const TriMesh<float> m = make_mesh<float>(verts, nv, faces, nf);
+#pragma omp parallel for schedule(static)
+  for (int64_t l = 0; l < int64_t(body.num_nodes); ++l)
+    out[l] = mesh_signed_distance(m, node_position(body.dmin, body.res, body.cs, uint32_t(l)),
+                                  offset);
+}
+
+}  // extern "C"

@@ -26,6 +26,8 @@
 #include <cstring>
 #include <limits>
 #include <vector>
+#include <map>
+#include <array>
 
 #include "alluvion_b200.h"
 
@@ -1491,6 +1493,102 @@ void solve_contacts(std::vector<Body<TF>>& bodies, std::vector<Contact<TF>>& con
         bj.omega += apply_congruent(cross(rj, -p), c.iiwj_diag, c.iiwj_off);
       }
     }
+}
+
+// ------------------------------------------------------------ mesh distance
+// MeshDistance::signedDistance (dg/mesh_distance.hpp:186-223) by brute
+// force: exact point-triangle distance with the closest point's region
+// (Ericson, Real-Time Collision Detection, sec. 5.1.5), first nearest face,
+// sign from the angle-weighted pseudonormals of the nearest feature
+// (dg/mesh_distance.hpp:80-104, 228-266), minus the offset.
+template <class TF>
+struct TriMesh {
+  std::vector<V3<TF>> v;
+  std::vector<std::array<uint32_t, 3>> f;
+  std::vector<V3<TF>> fn, vn, en;  // en: [face][3] (halfedge k: vertex k -> k + 1)
+};
+
+template <class TF>
+TriMesh<TF> make_mesh(const TF* verts, uint32_t nv, const uint32_t* faces, uint32_t nf) {
+  TriMesh<TF> m;
+  for (uint32_t i = 0; i < nv; ++i) m.v.push_back({verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]});
+  for (uint32_t i = 0; i < nf; ++i) m.f.push_back({faces[3 * i], faces[3 * i + 1], faces[3 * i + 2]});
+  std::vector<V3<double>> fn(nf), vn(nv, V3<double>{0, 0, 0});
+  std::map<std::pair<uint32_t, uint32_t>, uint32_t> edge_face;
+  auto d3 = [&](uint32_t i) { return V3<double>{double(m.v[i].x), double(m.v[i].y), double(m.v[i].z)}; };
+  for (uint32_t i = 0; i < nf; ++i) {
+    const auto& t = m.f[i];
+    const V3<double> x0 = d3(t[0]), x1 = d3(t[1]), x2 = d3(t[2]);
+    fn[i] = normalized(cross(x1 - x0, x2 - x0));
+    const V3<double> e1 = normalized(x1 - x0), e2 = normalized(x2 - x1), e3 = normalized(x0 - x2);
+    auto ang = [](V3<double> a, V3<double> c) {
+      double d = -dot(a, c);
+      return std::acos(d < -1 ? -1 : (d > 1 ? 1 : d));
+    };
+    const double alpha[3] = {ang(e1, e3), ang(e2, e1), ang(e3, e2)};
+    for (int k = 0; k < 3; ++k) vn[t[k]] += alpha[k] * fn[i];
+    for (int k = 0; k < 3; ++k) edge_face[{t[k], t[(k + 1) % 3]}] = i;
+  }
+  auto cvt = [](V3<double> a) { return V3<TF>{TF(a.x), TF(a.y), TF(a.z)}; };
+  for (uint32_t i = 0; i < nf; ++i) {
+    m.fn.push_back(cvt(fn[i]));
+    for (int k = 0; k < 3; ++k) {
+      auto it = edge_face.find({m.f[i][(k + 1) % 3], m.f[i][k]});
+      m.en.push_back(cvt(it != edge_face.end() ? fn[i] + fn[it->second] : fn[i]));
+    }
+  }
+  for (uint32_t i = 0; i < nv; ++i) m.vn.push_back(cvt(vn[i]));
+  return m;
+}
+
+// Closest point of triangle (a, b, c) to p; region 0-2 vertex, 3 edge ab,
+// 4 edge bc, 5 edge ca, 6 face.
+template <class TF>
+V3<TF> closest_on_triangle(V3<TF> p, V3<TF> a, V3<TF> b, V3<TF> c, int& region) {
+  const V3<TF> ab = b - a, ac = c - a, ap = p - a;
+  const TF d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0 && d2 <= 0) { region = 0; return a; }
+  const V3<TF> bp = p - b;
+  const TF d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0 && d4 <= d3) { region = 1; return b; }
+  const TF vc = d1 * d4 - d3 * d2;
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) { region = 3; return a + (d1 / (d1 - d3)) * ab; }
+  const V3<TF> cp = p - c;
+  const TF d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0 && d5 <= d6) { region = 2; return c; }
+  const TF vb = d5 * d2 - d1 * d6;
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) { region = 5; return a + (d2 / (d2 - d6)) * ac; }
+  const TF va = d3 * d6 - d5 * d4;
+  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+    region = 4;
+    return b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b);
+  }
+  region = 6;
+  const TF denom = TF(1) / (va + vb + vc);
+  return a + (vb * denom) * ab + (vc * denom) * ac;
+}
+
+template <class TF>
+TF mesh_signed_distance(const TriMesh<TF>& m, V3<TF> p, TF offset) {
+  TF best = std::numeric_limits<TF>::max();
+  uint32_t bf = 0;
+  int br = 6;
+  V3<TF> bq{0, 0, 0};
+  for (uint32_t i = 0; i < m.f.size(); ++i) {
+    int r;
+    const V3<TF> q = closest_on_triangle(p, m.v[m.f[i][0]], m.v[m.f[i][1]], m.v[m.f[i][2]], r);
+    const TF d2 = length_sqr(p - q);
+    if (d2 < best) {
+      best = d2;
+      bf = i;
+      br = r;
+      bq = q;
+    }
+  }
+  const V3<TF> n = br < 3 ? m.vn[m.f[bf][br]] : (br < 6 ? m.en[3 * bf + (br - 3)] : m.fn[bf]);
+  TF dist = std::sqrt(best);
+  if (dot(p - bq, n) < 0) dist = -dist;
+  return dist - offset;
 }
 
 }  // namespace oracle
