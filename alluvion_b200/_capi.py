@@ -19,6 +19,7 @@ STATUS = {
     7: "AL_ERR_TIMEOUT", 8: "AL_ERR_NO_DEVICE", 9: "AL_ERR_ALLOC",
 }
 AL_OK = 0
+AL_ERR_INVALID = 2
 AL_ERR_OUT_OF_GRID = 3
 AL_ERR_CELL_OVERFLOW = 4
 AL_ERR_NEIGHBOR_OVERFLOW = 5
@@ -157,6 +158,21 @@ class ContactF32(ctypes.Structure):
 CONTACT_FLOATS = ctypes.sizeof(ContactF32) // 4
 
 
+class SampleF32(ctypes.Structure):
+    """al_sample_f32: sample points, particle inputs and the outputs wanted
+    (device pointers; None where unused)."""
+    _fields_ = [("sample_x", ctypes.c_void_p), ("num_samples", ctypes.c_uint32),
+                ("quantity_dim", ctypes.c_uint32), ("particle_density", ctypes.c_void_p),
+                ("particle_v", ctypes.c_void_p), ("particle_quantity", ctypes.c_void_p),
+                ("sample_boundary", ctypes.c_void_p),
+                ("sample_boundary_kernel", ctypes.c_void_p),
+                ("sample_density", ctypes.c_void_p),
+                ("sample_position_density", ctypes.c_void_p),
+                ("sample_quantity", ctypes.c_void_p), ("sample_v", ctypes.c_void_p),
+                ("sample_vorticity", ctypes.c_void_p), ("wrap_y", ctypes.c_uint32),
+                ("wrap_length", ctypes.c_float), ("reserved", ctypes.c_uint32 * 2)]
+
+
 class StepReport(ctypes.Structure):
     _fields_ = [("num_divergence_solve", ctypes.c_uint32),
                 ("num_density_solve", ctypes.c_uint32),
@@ -239,6 +255,14 @@ _SIGNATURES = {
     "al_engine_launch_count": (ctypes.c_int, [_P, _P]),
     "al_engine_kernel_stat": (ctypes.c_int, [_P, _U, ctypes.c_char_p, ctypes.c_size_t, _P, _P]),
     "al_grid_sort_noalloc_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P, _P]),
+    "al_sample_fluid_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
+    "al_density_mask_f32": (ctypes.c_int, [_P, _P, _U, _P, _P]),
+    "al_boundary_mask_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, ctypes.c_float, _P, _P]),
+    "al_distance_mask_multiple_f32": (ctypes.c_int, [_P, _P, _U, _P, _U, ctypes.c_float, _P,
+                                                     _P]),
+    "al_histogram256_f32": (ctypes.c_int, [_P, _P, _P, _U, ctypes.c_float, ctypes.c_float, _P,
+                                           _P]),
+    "al_kl_divergence": (ctypes.c_int, [_P, _P, _P, _U, _U, ctypes.c_double, _U, _P, _P]),
 }
 for _s in ("f32", "f64"):
     _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])

@@ -601,6 +601,100 @@ typedef struct al_scene_f32 {
 AL_API int al_df_batch_step_f32(al_engine* engine, al_scene_f32* scenes, uint32_t num_scenes,
                                 void* stream);
 
+/* ------------------------------------------------------------- sampling
+ * Fluid quantities at sample points, with the reference's sample neighbor
+ * list (make_neighbor_list over sample_x, runner.hpp:1869-1911: the 27
+ * cells around the sample, candidates j != sample index -- the reference
+ * compares the particle index with the sample's -- closer than h) and:
+ *   sample_density           sample_fluid_density (runner.hpp:4193-4209):
+ *                            rho0 sum_j V W
+ *   sample_position_density  sample_position_density (runner.hpp:2100-2121):
+ *                            rho0 (sum_j V W + sum_b (W V)_b)
+ *   sample_quantity          sample_fluid (runner.hpp:4173-4191) of a
+ *                            1- or 3-component particle quantity:
+ *                            sum_j m / rho_j W q_j
+ *   sample_v                 compute_sample_velocity (runner.hpp:4211-4240):
+ *                            sum_j m / rho_j W v_j + sum_b v_b (W V)_b
+ *   sample_vorticity         compute_sample_vorticity (runner.hpp:4289-4323):
+ *                            sum_j m / rho_j (v_j - v_s) x grad W
+ *                            + sum_b (v_b - v_s) x (grad W V)_b
+ * v_b = omega x (x_b - x) + v of body b at its boundary point x_b.  The
+ * body terms run over cni->num_boundaries bodies and read the samples'
+ * boundary arrays from al_compute_particle_boundary_f32 called with the
+ * sample positions, and `rigid` (host array, the bodies' states).  Each
+ * output is computed when its pointer is non-NULL; vorticity needs sample_v.
+ * All arrays are device pointers in the reference's layouts.  More than
+ * max_num_neighbors_per_particle neighbors return AL_ERR_NEIGHBOR_OVERFLOW
+ * (the first ones in canonical order are summed). */
+typedef struct al_sample_f32 {
+  const float* sample_x;               /* [num_samples][3] */
+  uint32_t num_samples;
+  uint32_t quantity_dim;               /* 1 or 3 when sample_quantity is set */
+  const float* particle_density;       /* [N], for quantity / velocity / vorticity */
+  const float* particle_v;             /* [N][3], for velocity / vorticity */
+  const float* particle_quantity;      /* [N][quantity_dim] */
+  const float* sample_boundary;        /* [num_boundaries][num_samples][4] {x_b, V} */
+  const float* sample_boundary_kernel; /* [num_boundaries][num_samples][4] {grad W V, W V} */
+  float* sample_density;               /* [num_samples] out or NULL */
+  float* sample_position_density;      /* [num_samples] out or NULL */
+  float* sample_quantity;              /* [num_samples][quantity_dim] out or NULL */
+  float* sample_v;                     /* [num_samples][3] out or NULL */
+  float* sample_vorticity;             /* [num_samples][3] out or NULL */
+  /* 1: periodic in y (make_neighbor_list<1>): neighbor cells wrap in y
+   * (wrap_ipos_y, runner.hpp:689-697) and displacements are wrapped into
+   * [-wrap_length/2, wrap_length/2) (wrap_y, runner.hpp:698-707) */
+  uint32_t wrap_y;
+  float wrap_length;                   /* Const::wrap_length (constants.hpp:130-136) */
+  uint32_t reserved[2];
+} al_sample_f32;
+
+AL_API int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                               const float* particle_x, uint32_t num_particles,
+                               const al_rigid_f32* rigid, const al_sample_f32* request,
+                               void* stream);
+
+/* compute_density_mask (runner.hpp:4359-4365): mask[i] = density[i] > 0.
+ * Device arrays. */
+AL_API int al_density_mask_f32(al_engine* engine, const float* sample_density,
+                               uint32_t num_samples, uint32_t* mask, void* stream);
+
+/* compute_boundary_mask (runner.hpp:4367-4396, launched by
+ * Runner::launch_compute_boundary_mask, runner.hpp:5516-5600):
+ * mask[i] *= (sign d(x_i) >= distance_threshold), d the body's signed
+ * distance at the sample in its frame -- the distance grid for a mesh
+ * body, the analytic shape otherwise.  body, rigid: host; sample_x, mask:
+ * device. */
+AL_API int al_boundary_mask_f32(al_engine* engine, const al_body_f32* body,
+                                const al_rigid_f32* rigid, const float* sample_x,
+                                uint32_t num_samples, float distance_threshold, float* mask,
+                                void* stream);
+
+/* compute_distance_mask_multiple (runner.hpp:4272-4287):
+ * mask[k][i] = |buoy_x[k] - grid_x[i]|^2 <= threshold^2.  Device arrays. */
+AL_API int al_distance_mask_multiple_f32(al_engine* engine, const float* grid_x,
+                                         uint32_t num_grid_points, const float* buoy_x,
+                                         uint32_t num_buoys, float distance_threshold,
+                                         float* mask, void* stream);
+
+/* Runner::launch_histogram256[_with_mask] (runner.hpp:5849-5889; kernels
+ * quantize, histogram256[_with_mask], merge_histogram256,
+ * runner.hpp:4399-4536): histogram[b] = number of i < n (with mask[i] == 1
+ * when mask is non-NULL) whose byte (floor((v[i] - v_min) * step_inverse)
+ * saturated to uint32, low 8 bits) is b, step_inverse =
+ * float(256 / (double(v_max) - double(v_min))).  One pass over v (and
+ * mask); histogram: device [256] out. */
+AL_API int al_histogram256_f32(al_engine* engine, const float* v, const float* mask, uint32_t n,
+                               float v_min, float v_max, uint32_t* histogram, void* stream);
+
+/* Runner::calculate_kl_divergence (runner.hpp:4803-4815, KLDivergence
+ * runner.hpp:746-762): sum over bins with p > 0 of
+ * p / n_p log(p / max(q, q_lower_bound) n_q / n_p), evaluated in double
+ * with a fixed-order reduction.  histogram_p, histogram_q: device [num_bins]; result: host. */
+AL_API int al_kl_divergence(al_engine* engine, const uint32_t* histogram_p,
+                            const uint32_t* histogram_q, uint32_t n_p, uint32_t n_q,
+                            double q_lower_bound, uint32_t num_bins, double* result,
+                            void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -29,6 +29,11 @@ def lib():
             "orc_find_contacts_f32": (_U, [_P, _P, _P, _U, ctypes.c_float, _U, _P]),
             "orc_solve_contacts_f32": (None, [_P, _P, _U, _P, _U]),
             "orc_mesh_distance_grid_f32": (None, [_P, _P, _U, _P, _U, ctypes.c_float, _P]),
+            # cn, cni, particle_x, n, rigid, request -> overflow
+            "orc_sample_fluid_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
+            "orc_boundary_mask_f32": (None, [_P, _P, _P, _U, ctypes.c_float, _P]),
+            "orc_histogram256_f32": (None, [_P, _P, _U, ctypes.c_float, ctypes.c_float, _P]),
+            "orc_kl_divergence": (ctypes.c_double, [_P, _P, _U, _U, ctypes.c_double, _U]),
         }
         for s in ("f32", "f64"):
             sig["orc_grid_sort_" + s] = (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P])
@@ -215,3 +220,64 @@ def mesh_distance_grid(body, vertices, faces, offset=0.0):
     lib().orc_mesh_distance_grid_f32(_p(body), _p(v), len(v), _p(f), len(f), float(offset),
                                      _p(out))
     return out
+
+
+def sample_fluid(cn, cni, particle_x, rigid, sample_x, particle_density=None, particle_v=None,
+                 particle_quantity=None, sample_boundary=None, sample_boundary_kernel=None,
+                 outputs=("density", "position_density", "quantity", "v", "vorticity"),
+                 wrap_length=None):
+    """sample_fluid / sample_fluid_density / sample_position_density /
+    compute_sample_velocity / compute_sample_vorticity restated on host
+    float32 arrays; wrap_length: periodic in y (make_neighbor_list<1>).
+    Returns (dict of outputs, neighbor overflow flag)."""
+    from alluvion_b200 import _capi
+    f32 = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+    px, sx = f32(particle_x), f32(sample_x)
+    rho, pv, pq = f32(particle_density), f32(particle_v), f32(particle_quantity)
+    sb, sbk = f32(sample_boundary), f32(sample_boundary_kernel)
+    s = len(sx)
+    qdim = 0 if pq is None else (1 if pq.ndim == 1 else pq.shape[1])
+    out = {}
+    shapes = {"density": (s,), "position_density": (s,), "quantity": (s, qdim) if qdim > 1
+              else (s,), "v": (s, 3), "vorticity": (s, 3)}
+    for k in outputs:
+        out[k] = np.zeros(shapes[k], np.float32)
+    req = _capi.SampleF32()
+    req.sample_x = sx.ctypes.data
+    req.num_samples = s
+    req.quantity_dim = qdim
+    if wrap_length is not None:
+        req.wrap_y = 1
+        req.wrap_length = float(wrap_length)
+    for name, arr in (("particle_density", rho), ("particle_v", pv), ("particle_quantity", pq),
+                      ("sample_boundary", sb), ("sample_boundary_kernel", sbk)):
+        setattr(req, name, None if arr is None else arr.ctypes.data)
+    for k, name in (("density", "sample_density"), ("position_density", "sample_position_density"),
+                    ("quantity", "sample_quantity"), ("v", "sample_v"),
+                    ("vorticity", "sample_vorticity")):
+        setattr(req, name, out[k].ctypes.data if k in out else None)
+    flag = lib().orc_sample_fluid_f32(_p(cn), _p(cni), _p(px), len(px), _p(rigid), _p(req))
+    return out, bool(flag)
+
+
+def boundary_mask(body, rigid, sample_x, threshold, mask):
+    """compute_boundary_mask restated: mask (float32) *= (sign d >= threshold)."""
+    sx = np.ascontiguousarray(sample_x, np.float32)
+    lib().orc_boundary_mask_f32(_p(body), _p(rigid), _p(sx), len(sx), float(threshold), _p(mask))
+    return mask
+
+
+def histogram256(v, v_min, v_max, mask=None):
+    """launch_histogram256[_with_mask] restated: 256 uint32 counts."""
+    v = np.ascontiguousarray(v, np.float32)
+    m = None if mask is None else np.ascontiguousarray(mask, np.float32)
+    h = np.zeros(256, np.uint32)
+    lib().orc_histogram256_f32(_p(v), _p(m), len(v), float(v_min), float(v_max), _p(h))
+    return h
+
+
+def kl_divergence(p, q, n_p, n_q, q_lower_bound):
+    """calculate_kl_divergence restated in double."""
+    p = np.ascontiguousarray(p, np.uint32)
+    q = np.ascontiguousarray(q, np.uint32)
+    return lib().orc_kl_divergence(_p(p), _p(q), n_p, n_q, float(q_lower_bound), len(p))

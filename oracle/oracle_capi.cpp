@@ -504,3 +504,67 @@ void orc_mesh_distance_grid_f32(const al_body_f32* b, const float* verts, uint32
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Sampling at sample points (sample_fluid and friends) with HOST arrays in
+// the layouts of al_sample_f32; `rigid` holds the bodies' states
+// (cni->num_boundaries of them).  Returns 1 when a sample had more
+// neighbors than the cap, else 0.
+int orc_sample_fluid_f32(const al_const_f32* cn, const al_consti* cni, const float* particle_x,
+                         uint32_t n, const al_rigid_f32* rigid, const al_sample_f32* req) {
+  const Cn<float> c = make_cn<float>(*cn);
+  std::vector<V3<float>> px(n);
+  for (uint32_t i = 0; i < n; ++i) px[i] = v3<float>(particle_x + 3 * size_t(i));
+  std::vector<V3<float>> sx(req->num_samples);
+  for (uint32_t i = 0; i < req->num_samples; ++i) sx[i] = v3<float>(req->sample_x + 3 * size_t(i));
+  std::vector<Body<float>> bodies;
+  for (uint32_t b = 0; b < cni->num_boundaries; ++b) {
+    Body<float> o{};
+    o.x = v3<float>(rigid[b].x);
+    o.v = v3<float>(rigid[b].v);
+    o.omega = v3<float>(rigid[b].omega);
+    o.q = V4<float>{rigid[b].q[0], rigid[b].q[1], rigid[b].q[2], rigid[b].q[3]};
+    bodies.push_back(o);
+  }
+  SampleRequest<float> r;
+  r.sx = sx.data();
+  r.num = req->num_samples;
+  r.rho = req->particle_density;
+  r.v = reinterpret_cast<const V3<float>*>(req->particle_v);
+  r.q = req->particle_quantity;
+  r.qdim = req->sample_quantity ? req->quantity_dim : 0;
+  r.bnd = reinterpret_cast<const V4<float>*>(req->sample_boundary);
+  r.bk = reinterpret_cast<const V4<float>*>(req->sample_boundary_kernel);
+  r.density = req->sample_density;
+  r.position_density = req->sample_position_density;
+  r.quantity = req->sample_quantity;
+  r.vel = reinterpret_cast<V3<float>*>(req->sample_v);
+  r.vort = reinterpret_cast<V3<float>*>(req->sample_vorticity);
+  r.wrap = req->wrap_y != 0;
+  r.wrap_length = req->wrap_length;
+  return sample_fluid(c, *cni, px.data(), n, bodies, r) ? 1 : 0;
+}
+
+// compute_boundary_mask with HOST node arrays: mask *= (sign d >= threshold).
+void orc_boundary_mask_f32(const al_body_f32* body, const al_rigid_f32* rigid,
+                           const float* sample_x, uint32_t n, float threshold, float* mask) {
+  const Body<float> b = make_body<float>(*body, reinterpret_cast<const float*>(rigid));
+  std::vector<V3<float>> sx(n);
+  for (uint32_t i = 0; i < n; ++i) sx[i] = v3<float>(sample_x + 3 * size_t(i));
+  boundary_mask(b, sx.data(), n, threshold, mask);
+}
+
+// launch_histogram256[_with_mask]: 256 counts of quantized bytes.
+void orc_histogram256_f32(const float* v, const float* mask, uint32_t n, float v_min, float v_max,
+                          uint32_t* hist) {
+  histogram256(v, mask, n, v_min, v_max, hist);
+}
+
+// calculate_kl_divergence in double, bins in order.
+double orc_kl_divergence(const uint32_t* p, const uint32_t* q, uint32_t n_p, uint32_t n_q,
+                         double q_lower_bound, uint32_t num_bins) {
+  return kl_divergence(p, q, n_p, n_q, q_lower_bound, num_bins);
+}
+
+}  // extern "C"

@@ -1591,4 +1591,184 @@ TF mesh_signed_distance(const TriMesh<TF>& m, V3<TF> p, TF offset) {
   return dist - offset;
 }
 
+// ------------------------------------------------------------- sampling
+// Fluid quantities at sample points.  The sample neighbor list is
+// make_neighbor_list<0> (runner.hpp:1869-1911) over sample_x: the 27 cells
+// around the sample's cell, candidates j != s (the kernel compares the
+// particle index with the sample index) with |x_s - x_j|^2 < h^2, the first
+// cap of them in canonical order.  Then:
+//   sample_fluid             (runner.hpp:4173-4191)  sum m / rho_j W q_j
+//   sample_fluid_density     (runner.hpp:4193-4209)  rho0 sum V W
+//   sample_position_density  (runner.hpp:2100-2121)  rho0 (sum V W + sum_b (W V)_b)
+//   compute_sample_velocity  (runner.hpp:4211-4240)  sum m / rho_j W v_j + sum_b v_b (W V)_b
+//   compute_sample_vorticity (runner.hpp:4289-4323)  sum m / rho_j (v_j - v_s) x grad W
+//                                                    + sum_b (v_b - v_s) x (grad W V)_b
+// with v_b = omega_b x (x_b - x_body) + v_body the body's velocity at the
+// boundary point.  Boundary terms run over every body of `bodies`.
+template <class TF>
+struct SampleRequest {
+  const V3<TF>* sx = nullptr;
+  uint32_t num = 0;
+  const TF* rho = nullptr;
+  const V3<TF>* v = nullptr;
+  const TF* q = nullptr;
+  uint32_t qdim = 0;
+  const V4<TF>* bnd = nullptr;  // [nb][S]
+  const V4<TF>* bk = nullptr;   // [nb][S]
+  TF* density = nullptr;
+  TF* position_density = nullptr;
+  TF* quantity = nullptr;
+  V3<TF>* vel = nullptr;
+  V3<TF>* vort = nullptr;
+  // make_neighbor_list<1>: cells wrap in y (wrap_ipos_y, runner.hpp:689-697)
+  // and displacements wrap into [-L/2, L/2) (wrap_y, runner.hpp:698-707)
+  bool wrap = false;
+  TF wrap_length = 0;
+};
+
+template <class TF>
+bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px, uint32_t n,
+                  const std::vector<Body<TF>>& bodies, const SampleRequest<TF>& r) {
+  const GridSort s = grid_sort(c, g, px, n);
+  const uint32_t cap = g.max_num_neighbors_per_particle;
+  const uint32_t nb = uint32_t(bodies.size());
+  bool overflow = false;
+#pragma omp parallel for schedule(static) reduction(|| : overflow)
+  for (int64_t ii = 0; ii < int64_t(r.num); ++ii) {
+    const uint32_t i = uint32_t(ii);
+    const V3<TF> xi = r.sx[i];
+    int p[3];
+    cell_coords(c, g, xi, p);
+    std::vector<uint32_t> nbr;
+    std::vector<V3<TF>> disp;  // x_s - x_j, wrapped
+    const TF wmin = r.wrap_length * TF(-0.5), wmax = r.wrap_length * TF(0.5);
+    uint32_t found = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          int q[3] = {p[0] + dx, p[1] + dy, p[2] + dz};
+          if (r.wrap) {
+            if (q[1] >= int(g.grid_res[1]))
+              q[1] -= int(g.grid_res[1]);
+            else if (q[1] < 0)
+              q[1] += int(g.grid_res[1]);
+          }
+          if (!in_grid(g, q)) continue;
+          const uint32_t cell = cell_linear(g, q);
+          for (uint32_t t = s.cell_start[cell]; t < s.cell_start[cell + 1]; ++t) {
+            const uint32_t j = s.sorted[t];
+            if (j == i) continue;
+            V3<TF> d = xi - px[j];
+            if (r.wrap) {
+              if (d.y >= wmax)
+                d.y -= r.wrap_length;
+              else if (d.y < wmin)
+                d.y += r.wrap_length;
+            }
+            if ((d.x * d.x + d.y * d.y) + d.z * d.z < c.h2) {
+              if (found < cap) {
+                nbr.push_back(j);
+                disp.push_back(d);
+              }
+              ++found;
+            }
+          }
+        }
+    if (found > cap) overflow = true;
+    TF dens = 0, qs[3] = {0, 0, 0};
+    V3<TF> vel{0, 0, 0};
+    for (size_t k = 0; k < nbr.size(); ++k) {
+      const uint32_t j = nbr[k];
+      const V3<TF> d = disp[k];
+      const TF w = W_r2(c, (d.x * d.x + d.y * d.y) + d.z * d.z);
+      dens += c.vol * w;
+      if (r.quantity) {
+        const TF mr = c.mass / r.rho[j];
+        for (uint32_t k = 0; k < r.qdim; ++k) qs[k] += mr * w * r.q[size_t(j) * r.qdim + k];
+      }
+      if (r.vel) vel += (c.mass / r.rho[j] * w) * r.v[j];
+    }
+    TF bw = 0;
+    for (uint32_t b = 0; r.bk && b < nb; ++b) {
+      const V4<TF> bx = r.bnd ? r.bnd[size_t(b) * r.num + i] : V4<TF>{0, 0, 0, 0};
+      const V4<TF> bk = r.bk[size_t(b) * r.num + i];
+      bw += bk.w;
+      if (r.vel) {
+        const V3<TF> vb =
+            cross(bodies[b].omega, V3<TF>{bx.x, bx.y, bx.z} - bodies[b].x) + bodies[b].v;
+        vel += bk.w * vb;
+      }
+    }
+    if (r.density) r.density[i] = dens * c.rho0;
+    if (r.position_density) r.position_density[i] = (dens + bw) * c.rho0;
+    if (r.quantity)
+      for (uint32_t k = 0; k < r.qdim; ++k) r.quantity[size_t(i) * r.qdim + k] = qs[k];
+    if (r.vel) r.vel[i] = vel;
+    if (r.vort) {
+      V3<TF> w{0, 0, 0};
+      for (size_t k = 0; k < nbr.size(); ++k)
+        w += (c.mass / r.rho[nbr[k]]) * cross(r.v[nbr[k]] - vel, gradW(c, disp[k]));
+      for (uint32_t b = 0; b < nb; ++b) {
+        const V4<TF> bx = r.bnd[size_t(b) * r.num + i];
+        const V4<TF> bk = r.bk[size_t(b) * r.num + i];
+        const V3<TF> vb =
+            cross(bodies[b].omega, V3<TF>{bx.x, bx.y, bx.z} - bodies[b].x) + bodies[b].v;
+        w += cross(vb - vel, V3<TF>{bk.x, bk.y, bk.z});
+      }
+      r.vort[i] = w;
+    }
+  }
+  return overflow;
+}
+
+// compute_boundary_mask (runner.hpp:4367-4396): mask *= (sign d >= threshold)
+// with d the distance grid's interpolation for a mesh body, the analytic
+// distance otherwise, at the sample in the body's frame.
+template <class TF>
+void boundary_mask(const Body<TF>& b, const V3<TF>* sx, uint32_t n, TF threshold, TF* mask) {
+  const LagrangeGrid<TF> grid{b.dmin, b.dmax, b.cs, {b.res[0], b.res[1], b.res[2]}, b.dist_nodes};
+  for (uint32_t i = 0; i < n; ++i) {
+    const V3<TF> local = rotate(sx[i] - b.x, conjugate(b.q));
+    const TF d = (b.shape == AL_SHAPE_MESH ? grid.value(local) : b.sdf.sdf(local)) * b.sign;
+    mask[i] *= TF(d >= threshold);
+  }
+}
+
+// quantize (runner.hpp:4516-4536) of one value: floor((v - v_min) *
+// step_inverse) saturated to [0, 2^32 - 1] (NaN -> 0) as __float2uint_rd
+// does, low byte kept.
+inline uint32_t quantize_byte(float v, float v_min, float step_inverse) {
+  const float d = v - v_min;
+  const float t = d * step_inverse;
+  if (!(t > 0.0f)) return 0;
+  if (t >= 4294967296.0f) return 0xFFu;
+  return uint32_t(std::floor(t)) & 0xFFu;
+}
+
+// launch_histogram256[_with_mask] (runner.hpp:5849-5889, kernels
+// runner.hpp:4399-4514): counts of quantized bytes over v[0, n), where
+// mask[i] == 1 when a mask is given.  step_inverse is
+// float(256 / (double(v_max) - double(v_min))).
+inline void histogram256(const float* v, const float* mask, uint32_t n, float v_min, float v_max,
+                         uint32_t hist[256]) {
+  const float step_inverse = float(256.0 / (double(v_max) - double(v_min)));
+  for (int b = 0; b < 256; ++b) hist[b] = 0;
+  for (uint32_t i = 0; i < n; ++i)
+    if (!mask || mask[i] == 1.0f) ++hist[quantize_byte(v[i], v_min, step_inverse)];
+}
+
+// calculate_kl_divergence (runner.hpp:4803-4815 with KLDivergence,
+// runner.hpp:746-762): sum over bins with p > 0 of
+// p / n_p * log(p / max(q, q_lower_bound) * n_q / n_p), in double.
+inline double kl_divergence(const uint32_t* p, const uint32_t* q, uint32_t n_p, uint32_t n_q,
+                            double q_lower_bound, uint32_t num_bins) {
+  const double inv = 1.0 / n_p, ratio = double(n_q) / n_p;
+  double sum = 0;
+  for (uint32_t b = 0; b < num_bins; ++b) {
+    if (p[b] == 0) continue;
+    sum += p[b] * inv * std::log(p[b] / std::max(double(q[b]), q_lower_bound) * ratio);
+  }
+  return sum;
+}
+
 }  // namespace oracle
