@@ -275,6 +275,7 @@ for _s in ("f32", "f64"):
     _SIGNATURES["al_node_positions_" + _s] = (ctypes.c_int, [_P, _P, _P, _P])
     _SIGNATURES["al_df_step_" + _s] = (ctypes.c_int, [_P] * 10)
     _SIGNATURES["al_ii_step_" + _s] = (ctypes.c_int, [_P] * 10)
+    _SIGNATURES["al_i_step_" + _s] = (ctypes.c_int, [_P] * 10)
 
 
 def declared_symbols():

@@ -889,6 +889,123 @@ __global__ void __launch_bounds__(kBlock)
   if (rho_adv_ref) rho_adv_ref[i] = S.rho_adv[L.s];
 }
 
+// ---------------------------------------------------- implicit SPH (SolverI)
+// advect_and_init_pressure (runner.hpp:2889-2900): v += dt a, last pressure
+// (kappa_v) = pressure / 2.
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_i_advect(StepState<TF> S) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const TF dt = S.ctrl->dt;
+  const vec4<TF> a = S.a[s];
+  const vec4<TF> v = RV(S, s);
+  RV(S, s) = vec4<TF>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, v.w};
+  S.kappa_v[s] = S.kappa[s] * TF(0.5);
+}
+
+// calculate_isph_diagonal_adv_density (runner.hpp:2901-2954): the Jacobi
+// diagonal (times rho0) into kk, the advected density into rho_adv.
+template <class TF>
+__global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
+  const Lane L = pair_lane(S.n);
+  const TF dt = S.ctrl->dt;
+  vec3<TF> xi{0, 0, 0}, vi{0, 0, 0};
+  TF rho = c.rho0;
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(RX(S, L.s));
+    vi = xyz(RV(S, L.s));
+    rho = S.rho[L.s];
+    cnt = S.ncount[L.s];
+  }
+  const TF eps = TF(0.01) * c.h2;
+  TF adv = 0, diag = 0;
+  for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const vec3<TF> d = xi - xyz(xj);  // vj = {v, rho}
+    const vec3<TF> gw = gradW(c, d);
+    const TF rj = vj.w;
+    adv += dt * c.vol * dot(vi - xyz(vj), gw);
+    diag += c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gw);
+  });
+  adv = group_sum(adv);
+  diag = group_sum(diag);
+  if (!L.lead()) return;
+  adv += rho / c.rho0;
+  for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
+    const uint32_t b = __ffs(m) - 1;
+    const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
+    const vec3<TF> gwv = xyz(S.bk[size_t(b) * S.n + L.s]);
+    const vec3<TF> xib = xi - xyz(bn);
+    adv += dt * dot(vi - body_velocity(S.rigid[b], xyz(bn)), gwv);
+    diag += (rho + c.rho0) / (rho * c.rho0) / (length_sqr(xib) + eps) * dot(xib, gwv);
+  }
+  S.kk[L.s] = diag * c.rho0;
+  S.rho_adv[L.s] = adv;
+}
+
+// isph_solve_iteration (runner.hpp:3006-3053): damped Jacobi (weight 2/3)
+// on the neighbors' last pressures, and the mean density error of
+// solver_i.hpp:272-274 (double, on the device).  The reference copies
+// pressure into last_pressure after each iteration; here the two arrays
+// swap roles by iteration parity: iteration k reads kappa_v and writes
+// kappa when k is even, the reverse when odd.
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_i_iter(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  const Lane L = pair_lane(S.n);
+  const TF dt = S.ctrl->dt;
+  const bool odd = (S.ctrl->it & 1u) != 0;
+  const TF* __restrict__ last = odd ? S.kappa : S.kappa_v;
+  TF* __restrict__ next = odd ? S.kappa_v : S.kappa;
+  vec3<TF> xi{0, 0, 0};
+  TF rho = c.rho0, lp = 0;
+  uint32_t cnt = 0;
+  if (L.act) {
+    xi = xyz(RX(S, L.s));
+    rho = S.rho[L.s];
+    lp = last[L.s];
+    cnt = S.ncount[L.s];
+  }
+  const TF eps = TF(0.01) * c.h2;
+  TF off = 0;
+  for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t t, const vec4<TF>& xj, const vec4<TF>& vj) {
+    const vec3<TF> d = xi - xyz(xj);
+    const TF rj = vj.w;
+    off -= c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
+           __ldg(last + t);
+  });
+  off = group_sum(off);
+  double val = 0;
+  if (L.lead()) {
+    off *= c.rho0;
+    const TF diag = S.kk[L.s];
+    const TF bterm = TF(1) - S.rho_adv[L.s];
+    const TF dt2 = dt * dt;
+    const TF denom = diag * dt2;
+    const TF w = TF(2) / TF(3);
+    TF p = 0;
+    if (fabs(denom) > TF(1.0e-9))
+      p = fmax((TF(1) - w) * lp + w * (bterm / denom - off / diag), TF(0));
+    const TF err = p == TF(0) ? TF(0) : (denom * p + off * dt2 - bterm);
+    S.err[L.s] = err;
+    next[L.s] = p;
+    val = double(err);
+  }
+  double total;
+  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total) && threadIdx.x == 0)
+    finish_iteration(*S.ctrl, total, S.n, 1, handle, use_handle);
+}
+
+// After an even, non-zero number of iterations the final pressure sits in
+// kappa_v: move it to kappa, where the acceleration pass reads it.
+template <class TF>
+__global__ void k_i_final(StepState<TF> S) {
+  const uint32_t it = S.ctrl->it;
+  if (it == 0 || (it & 1u)) return;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S.n; s += gridDim.x * blockDim.x)
+    S.kappa[s] = S.kappa_v[s];
+}
+
 // Per-body totals of the rigid slots (solver_df.hpp:346-353) in double and
 // Pile::integrate_kinematics (pile.hpp:794-815).  One block per body.
 template <class TF>
@@ -1045,6 +1162,7 @@ int staging(al_engine* e, Staging<TF>* out, uint32_t slot = 0, uint32_t nslots =
 template <class TF>
 struct StepPlan {
   bool iisph = false, div = false, den = false;
+  bool isph = false;  // implicit SPH (SolverI); iisph is set too (pressure state)
   Cn<TF> c;
   GridDims g;
   const typename FluidT<TF>::type* f = nullptr;
@@ -1225,6 +1343,21 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                      S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
                      f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
                      f->particle_kappa_v, f->particle_density_adv));
+    } else if (P.isph) {
+      ALB_LAUNCH(e, "i_advect", 1, st, k_i_advect<TF><<<blocks, kBlock, 0, st>>>(S));
+      ALB_LAUNCH(e, "i_diag", 1, st, k_i_diag<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+      ALB_TRY(solve(1, P.io.hc->max_den,
+                    [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+                      ALB_LAUNCH(e, "i_iter", 1, s,
+                                 k_i_iter<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                      return AL_OK;
+                    }));
+      ALB_LAUNCH(e, "i_final", 1, st,
+                 k_i_final<TF><<<blocks, kBlock, 0, st>>>(S));
+      ALB_LAUNCH(e, "finish", 1, st,
+                 k_ii_accel_finish<TF><<<pblocks, kBlock, 0, st>>>(
+                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                     f->particle_pressure, f->particle_density_adv));
     } else {
       ALB_LAUNCH(e, "ii_predict0", 1, st, k_ii_predict0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
       ALB_LAUNCH(e, "ii_predict1", 1, st, k_ii_predict1<TF><<<pblocks, kBlock, 0, st>>>(c, S));
@@ -1253,6 +1386,13 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   return AL_OK;
 }
 
+// Kernels one solver-loop iteration launches: the update and the residual
+// (DFSPH, IISPH), one fused pass (implicit SPH).
+template <class TF>
+uint32_t iteration_launches(const StepPlan<TF>& P) {
+  return P.isph ? 1u : 2u;
+}
+
 // Captures one step into an executable graph.  Sets `*exec` to null (and
 // returns AL_OK) when a scratch buffer moved during the capture.
 template <class TF>
@@ -1279,7 +1419,7 @@ int capture_step(al_engine* e, StepPlan<TF>& P, cudaGraphExec_t* exec, uint32_t*
   cudaGraphDestroy(graph);
   if (inst != cudaSuccess) *exec = nullptr;
   ALB_CUDA(inst);
-  *fixed = uint32_t(captured - 2u * uint32_t(loops));
+  *fixed = uint32_t(captured - iteration_launches(P) * uint32_t(loops));
   return AL_OK;
 }
 
@@ -1289,8 +1429,8 @@ int capture_step(al_engine* e, StepPlan<TF>& P, cudaGraphExec_t* exec, uint32_t*
 template <class TF>
 std::vector<uint64_t> step_key(const al_engine* e, const StepPlan<TF>& P,
                                const typename FluidT<TF>::cn* cn, const al_consti* cni) {
-  std::vector<uint64_t> k{sizeof(TF), uint64_t(P.iisph), uint64_t(P.div), uint64_t(P.den),
-                          e->generation};
+  std::vector<uint64_t> k{sizeof(TF),         uint64_t(P.iisph), uint64_t(P.isph),
+                          uint64_t(P.div),    uint64_t(P.den),   e->generation};
   auto add = [&k](const void* p, size_t bytes) {
     const unsigned char* b = static_cast<const unsigned char*>(p);
     for (size_t i = 0; i < bytes; i += 8) {
@@ -1310,10 +1450,14 @@ std::vector<uint64_t> step_key(const al_engine* e, const StepPlan<TF>& P,
 
 constexpr size_t kMaxGraphs = 8;
 
+// Solver methods of run_step: SolverDf, SolverIi, SolverI.
+constexpr int kMethodDf = 0, kMethodIi = 1, kMethodI = 2;
+
 // Host-side arguments of one scene's step (the C ABI's per-call inputs).
 template <class TF>
 struct StepArgs {
   bool iisph = false;
+  bool isph = false;
   const typename FluidT<TF>::cn* cn = nullptr;
   const al_consti* cni = nullptr;
   const typename FluidT<TF>::type* f = nullptr;
@@ -1332,8 +1476,9 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
                  uint32_t nslots) {
   ALB_TRY(check_step_args<TF>(A.f, A.cni, A.bodies, A.rigid, A.sp, A.dt));
   const al_solver_params* sp = A.sp;
-  const bool iisph = A.iisph;
+  const bool iisph = A.iisph || A.isph;
   P.iisph = iisph;
+  P.isph = A.isph;
   P.div = !iisph && sp->enable_divergence_solve;
   P.den = iisph || sp->enable_density_solve;
   P.c = to_cn<TF>(*A.cn);
@@ -1359,6 +1504,8 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   if (iisph) {
     ALB_TRY(e->buf("sorted.kk", n, &S.kk));
     ALB_TRY(e->buf("sorted.err", n, &S.err));
+  }
+  if (iisph && !P.isph) {
     ALB_TRY(e->buf("sorted.dii", n, &S.dii));
     ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
   }
@@ -1476,14 +1623,15 @@ void remember_key(al_engine* e, std::vector<uint64_t> key) {
 }
 
 template <class TF>
-int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const al_consti* cni,
+int run_step(al_engine* e, int method, const typename FluidT<TF>::cn* cn, const al_consti* cni,
              const typename FluidT<TF>::type* f, const typename FluidT<TF>::body* bodies,
              typename FluidT<TF>::rigid* rigid, const al_solver_params* sp, TF* dt,
              al_step_report* report, cudaStream_t st, const al_warm_start* warm = nullptr) {
   ALB_TRY(e->activate());
   e->ns.clear();
   StepArgs<TF> A;
-  A.iisph = iisph;
+  A.iisph = method == kMethodIi;
+  A.isph = method == kMethodI;
   A.cn = cn;
   A.cni = cni;
   A.f = f;
@@ -1518,7 +1666,8 @@ int run_step(al_engine* e, bool iisph, const typename FluidT<TF>::cn* cn, const 
   const al_step_report& r = P.io.hc->rep;
   if (graph)
     e->launches += graph->fixed_launches +
-                   2ull * (uint64_t(r.num_divergence_solve) + r.num_density_solve);
+                   uint64_t(iteration_launches(P)) *
+                       (uint64_t(r.num_divergence_solve) + r.num_density_solve);
   return finish_step<TF>(A, P);
 }
 
@@ -1649,7 +1798,7 @@ int al_df_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* c
                    const al_solver_params* params, float* dt, al_step_report* report,
                    void* stream) {
   ALB_CHECK_ARG(engine && cn, "al_df_step: null argument");
-  return run_step<float>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
+  return run_step<float>(engine, kMethodDf, cn, cni, fluid, bodies, rigid, params, dt, report,
                          static_cast<cudaStream_t>(stream));
 }
 int al_df_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
@@ -1657,7 +1806,7 @@ int al_df_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* c
                    const al_solver_params* params, double* dt, al_step_report* report,
                    void* stream) {
   ALB_CHECK_ARG(engine && cn, "al_df_step: null argument");
-  return run_step<double>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
+  return run_step<double>(engine, kMethodDf, cn, cni, fluid, bodies, rigid, params, dt, report,
                           static_cast<cudaStream_t>(stream));
 }
 int al_df_step_warm_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
@@ -1666,7 +1815,7 @@ int al_df_step_warm_f32(al_engine* engine, const al_const_f32* cn, const al_cons
                         const al_warm_start* warm, float* dt, al_step_report* report,
                         void* stream) {
   ALB_CHECK_ARG(engine && cn, "al_df_step_warm_f32: null argument");
-  return run_step<float>(engine, false, cn, cni, fluid, bodies, rigid, params, dt, report,
+  return run_step<float>(engine, kMethodDf, cn, cni, fluid, bodies, rigid, params, dt, report,
                          static_cast<cudaStream_t>(stream), warm);
 }
 int al_ii_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
@@ -1674,7 +1823,7 @@ int al_ii_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* c
                    const al_solver_params* params, float* dt, al_step_report* report,
                    void* stream) {
   ALB_CHECK_ARG(engine && cn, "al_ii_step: null argument");
-  return run_step<float>(engine, true, cn, cni, fluid, bodies, rigid, params, dt, report,
+  return run_step<float>(engine, kMethodIi, cn, cni, fluid, bodies, rigid, params, dt, report,
                          static_cast<cudaStream_t>(stream));
 }
 int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
@@ -1682,7 +1831,24 @@ int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* c
                    const al_solver_params* params, double* dt, al_step_report* report,
                    void* stream) {
   ALB_CHECK_ARG(engine && cn, "al_ii_step: null argument");
-  return run_step<double>(engine, true, cn, cni, fluid, bodies, rigid, params, dt, report,
+  return run_step<double>(engine, kMethodIi, cn, cni, fluid, bodies, rigid, params, dt, report,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int al_i_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                  const al_fluid_f32* fluid, const al_body_f32* bodies, al_rigid_f32* rigid,
+                  const al_solver_params* params, float* dt, al_step_report* report,
+                  void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_i_step: null argument");
+  return run_step<float>(engine, kMethodI, cn, cni, fluid, bodies, rigid, params, dt, report,
+                         static_cast<cudaStream_t>(stream));
+}
+int al_i_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                  const al_fluid_f64* fluid, const al_body_f64* bodies, al_rigid_f64* rigid,
+                  const al_solver_params* params, double* dt, al_step_report* report,
+                  void* stream) {
+  ALB_CHECK_ARG(engine && cn, "al_i_step: null argument");
+  return run_step<double>(engine, kMethodI, cn, cni, fluid, bodies, rigid, params, dt, report,
                           static_cast<cudaStream_t>(stream));
 }
 

@@ -61,10 +61,10 @@ struct StepState {
   TF* rho = nullptr;
   TF* alpha = nullptr;
   TF* rho_adv = nullptr;
-  TF* kappa = nullptr;    // DFSPH kappa, IISPH pressure
-  TF* kappa_v = nullptr;  // DFSPH kappa_v, IISPH last pressure
-  TF* kk = nullptr;       // IISPH aii
-  TF* err = nullptr;      // IISPH density error
+  TF* kappa = nullptr;    // DFSPH kappa, IISPH / implicit SPH pressure
+  TF* kappa_v = nullptr;  // DFSPH kappa_v, IISPH / implicit SPH last pressure
+  TF* kk = nullptr;       // IISPH aii, implicit SPH diagonal (times rho0)
+  TF* err = nullptr;      // IISPH / implicit SPH density error
   vec4<TF>* dii = nullptr;
   vec4<TF>* dij_pj = nullptr;
   uint32_t* nbr = nullptr;

@@ -6,10 +6,11 @@ radius 0.05 m, 2 boxes of side 0.08 m, seeded, 64^3 cubic-Lagrange distance
 grids and volume maps), at 0.1 % density / divergence tolerance.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                  [--workload dambreak-1m|dambreak-32k|dambreak-8m] [--method df|ii]
+                  [--workload dambreak-1m|dambreak-32k|dambreak-8m] [--method df|ii|i]
 
-One step = one SolverDf step (solver_df.hpp:74-359), or one SolverIi step
-(solver_ii.hpp:76-243) with --method ii, over the whole scene.  The default
+One step = one SolverDf step (solver_df.hpp:74-359), one SolverIi step
+(solver_ii.hpp:76-243) with --method ii, or one SolverI step (implicit SPH,
+solver_i.hpp:79-327) with --method i, over the whole scene.  The default
 workload is the 1M-particle scene; dambreak-32k (32^3 lattice, r = 0.01 m,
 no rigid bodies) and dambreak-8m (256 x 128 x 256 lattice, r = 0.0025 m,
 sphere + box + torus with 128^3 grids) are the small and large variants.
@@ -61,7 +62,7 @@ BATCH_WORKLOADS = {
              "(cubic lattices, r=0.01 m, seeded), boxes scaled with the count from 1.0x0.7x0.7 m, "
              "0-2 seeded rigid spheres per scene, 32^3 volume maps, one graph launch per step"),
 }
-METHOD_NAME = {"df": "DFSPH", "ii": "IISPH"}
+METHOD_NAME = {"df": "DFSPH", "ii": "IISPH", "i": "implicit SPH (SolverI)"}
 
 # Compulsory per-particle state traffic per pass, float32 ("Model A": every
 # per-particle array read/written once per pass, neighbor gathers served
@@ -86,6 +87,15 @@ MODEL_A = {
     "ii_predict": (152, 48),
     "ii_iteration": (110, 16),
     "ii_finish": (80, 32),
+    # implicit SPH (SolverI): advect_and_init_pressure reads v, a, p and
+    # writes v, p_last (56 B); the diagonal pass reads x, v, rho and writes
+    # diag, rho_adv (48 B + 32 B per pair); one Jacobi iteration reads x,
+    # rho, p_last, diag, rho_adv and writes p, err (56 B); the final copy of
+    # an even iteration count moves p (8 B)
+    "i_advect": (56, 0),
+    "i_diag": (48, 32),
+    "i_iteration": (56, 0),
+    "i_final": (8, 0),
 }
 # engine launch groups -> Model A pass
 GROUP_PASS = {
@@ -96,10 +106,14 @@ GROUP_PASS = {
     "press_warm1": "press_warm", "press_rho_adv": "press_warm", "press_iter": "press_iteration",
     "press_residual": "press_iteration", "finish": "finish",
     "ii_predict0": "ii_predict", "ii_predict1": "ii_predict", "ii_iter0": "ii_iteration",
-    "ii_iter1": "ii_iteration",
+    "ii_iter1": "ii_iteration", "i_advect": "i_advect", "i_diag": "i_diag",
+    "i_iter": "i_iteration", "i_final": "i_final",
 }
+# the write-back group of the pressure methods is their acceleration pass
+FINISH_PASS = {"df": "finish", "ii": "ii_finish", "i": "ii_finish"}
 # how many times a pass runs per step: iteration passes once per iteration
-PASS_PER_STEP = {"div_iteration": "div", "press_iteration": "den", "ii_iteration": "den"}
+PASS_PER_STEP = {"div_iteration": "div", "press_iteration": "den", "ii_iteration": "den",
+                 "i_iteration": "den"}
 
 
 def parse_args():
@@ -120,7 +134,7 @@ def parse_args():
                    help="launch every kernel from the host (no captured step graph)")
     p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS),
                    default="dambreak-1m")
-    p.add_argument("--method", choices=["df", "ii"], default="df")
+    p.add_argument("--method", choices=["df", "ii", "i"], default="df")
     p.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
                    help="learned: DFSPH with the learned warm start, trained (untimed) on a "
                         "differently seeded scene of the same workload")
@@ -368,7 +382,7 @@ def barrier(world):
 
 
 # per-particle state a step reads and writes besides x and v
-STATE = {"df": ("kappa", "kappa_v"), "ii": ("pressure",)}
+STATE = {"df": ("kappa", "kappa_v"), "ii": ("pressure",), "i": ("pressure",)}
 
 
 def oracle_state(host_state, method):
@@ -664,7 +678,7 @@ def engine_arm(args):
     pairs = sum(r[3] for r in preps) / prof_steps
     pass_ms = {}
     for name, (tot, cnt) in stats.items():
-        p = GROUP_PASS.get(name)
+        p = FINISH_PASS[args.method] if name == "finish" else GROUP_PASS.get(name)
         if p:
             pass_ms[p] = pass_ms.get(p, 0.0) + tot / prof_steps
     per_launch = {}

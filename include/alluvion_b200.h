@@ -459,6 +459,23 @@ AL_API int al_ii_step_f64(al_engine* engine, const al_const_f64* cn, const al_co
                           al_rigid_f64* rigid, const al_solver_params* params, double* dt,
                           al_step_report* report, void* stream);
 
+/* One implicit SPH step: SolverI<TF>::step<0> (solver_i.hpp:79-327) with
+ * volume-map boundaries, without contacts: advect_and_init_pressure,
+ * calculate_isph_diagonal_adv_density and damped-Jacobi
+ * isph_solve_iteration (runner.hpp:2889-3053) until the mean density error
+ * is under density_error_tolerance (min/max_density_solve), then
+ * compute_pressure_accels and kinematic_integration.  Same conventions as
+ * al_ii_step: uses particle_pressure (in/out); particle_density_adv receives
+ * the advected density. */
+AL_API int al_i_step_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                         const al_fluid_f32* fluid, const al_body_f32* bodies,
+                         al_rigid_f32* rigid, const al_solver_params* params, float* dt,
+                         al_step_report* report, void* stream);
+AL_API int al_i_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                         const al_fluid_f64* fluid, const al_body_f64* bodies,
+                         al_rigid_f64* rigid, const al_solver_params* params, double* dt,
+                         al_step_report* report, void* stream);
+
 /* ---------------------------------------------------- learned warm start
  * No reference counterpart.  A per-particle MLP 12 -> 64 -> 64 -> 2 with
  * GELU (tanh form), BF16 operands and FP32 accumulation on the tensor

@@ -47,6 +47,7 @@ def lib():
             # params, dt, steps, reports (IISPH: pressure instead of kappa, kappa_v)
             sig["orc_df_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 9 + [_U, _P])
             sig["orc_ii_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 8 + [_U, _P])
+            sig["orc_i_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 8 + [_U, _P])
         for name, (res, args) in sig.items():
             fn = getattr(handle, name)
             fn.restype = res
@@ -172,7 +173,7 @@ def boundary(cn, bodies, rigid, x):
 def run(method, cn, cni, bodies, rigid, state, sp, dt, steps):
     """Advances `state` (dict of host arrays: x, v, kappa, kappa_v | pressure,
     density, density_adv, a) by `steps` steps in place; returns (dt, reports).
-    method: 'df' or 'ii'."""
+    method: 'df' (DFSPH), 'ii' (IISPH) or 'i' (implicit SPH, SolverI)."""
     from alluvion_b200 import _capi
     x = state["x"]
     T = x.dtype
@@ -187,7 +188,7 @@ def run(method, cn, cni, bodies, rigid, state, sp, dt, steps):
             _p(state["density_adv"]), _p(state["a"]), _p(sp), _p(dt_arr), steps,
             _p(reports))
     else:
-        status = getattr(lib(), "orc_ii_run_" + _sfx(T))(
+        status = getattr(lib(), "orc_%s_run_%s" % (method, _sfx(T)))(
             _p(cn), _p(cni), _p(bodies) if nb else None, _p(rigid), n, _p(x), _p(state["v"]),
             _p(state["pressure"]), _p(state["density"]), _p(state["density_adv"]),
             _p(state["a"]), _p(sp), _p(dt_arr), steps, _p(reports))

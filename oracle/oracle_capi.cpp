@@ -178,11 +178,12 @@ void boundary_impl(const C* cn, const B* bodies, const TF* rigid, uint32_t nb, c
 // Runs `steps` solver steps on host arrays.  State arrays are in/out.
 // rigid: nb x 13 values (x, v, q, omega).  reports: `steps` entries.
 template <class TF, class C, class B>
-int run_impl(bool iisph, const C* cn, const al_consti* cni, const B* bodies, TF* rigid,
+int run_impl(int method, const C* cn, const al_consti* cni, const B* bodies, TF* rigid,
              uint32_t n, TF* x, TF* v, TF* kappa_or_pressure, TF* kappa_v, TF* density,
              TF* density_adv, TF* a, const al_solver_params* sp_in, TF* dt, uint32_t steps,
              al_step_report* reports) {
   Cn<TF> c = make_cn<TF>(*cn);
+  const bool iisph = method != 0;  // 0 DFSPH, 1 IISPH, 2 implicit SPH (SolverI)
   const uint32_t nb = cni->num_boundaries;
   std::vector<Body<TF>> bs;
   for (uint32_t b = 0; b < nb; ++b) bs.push_back(make_body<TF>(bodies[b], rigid + 13 * b));
@@ -219,8 +220,10 @@ int run_impl(bool iisph, const C* cn, const al_consti* cni, const B* bodies, TF*
   TF step_dt = *dt;
   for (uint32_t s = 0; s < steps; ++s) {
     std::vector<V3<double>> F, T;
-    StepReport r = iisph ? ii_step(c, *cni, bs, f, sp, step_dt, pg, sp_in->integrate_rigids != 0, &F, &T)
-                         : df_step(c, *cni, bs, f, sp, step_dt, pg, sp_in->integrate_rigids != 0, &F, &T);
+    const bool ib = sp_in->integrate_rigids != 0;
+    StepReport r = method == 1   ? ii_step(c, *cni, bs, f, sp, step_dt, pg, ib, &F, &T)
+                   : method == 2 ? i_step(c, *cni, bs, f, sp, step_dt, pg, ib, &F, &T)
+                                 : df_step(c, *cni, bs, f, sp, step_dt, pg, ib, &F, &T);
     if (reports) {
       al_step_report& o = reports[s];
       std::memset(&o, 0, sizeof(o));
@@ -361,7 +364,7 @@ int orc_df_run_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f
                    float* rigid, uint32_t n, float* x, float* v, float* kappa, float* kappa_v,
                    float* density, float* density_adv, float* a, const al_solver_params* sp,
                    float* dt, uint32_t steps, al_step_report* reports) {
-  return run_impl<float>(false, cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density,
+  return run_impl<float>(0, cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density,
                          density_adv, a, sp, dt, steps, reports);
 }
 int orc_df_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f64* bodies,
@@ -369,21 +372,36 @@ int orc_df_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f
                    double* kappa_v, double* density, double* density_adv, double* a,
                    const al_solver_params* sp, double* dt, uint32_t steps,
                    al_step_report* reports) {
-  return run_impl<double>(false, cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density,
+  return run_impl<double>(0, cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density,
                           density_adv, a, sp, dt, steps, reports);
 }
 int orc_ii_run_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f32* bodies,
                    float* rigid, uint32_t n, float* x, float* v, float* pressure, float* density,
                    float* density_adv, float* a, const al_solver_params* sp, float* dt,
                    uint32_t steps, al_step_report* reports) {
-  return run_impl<float>(true, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+  return run_impl<float>(1, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
                          density_adv, a, sp, dt, steps, reports);
 }
 int orc_ii_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f64* bodies,
                    double* rigid, uint32_t n, double* x, double* v, double* pressure,
                    double* density, double* density_adv, double* a, const al_solver_params* sp,
                    double* dt, uint32_t steps, al_step_report* reports) {
-  return run_impl<double>(true, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+  return run_impl<double>(1, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+                          density_adv, a, sp, dt, steps, reports);
+}
+
+int orc_i_run_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f32* bodies,
+                  float* rigid, uint32_t n, float* x, float* v, float* pressure, float* density,
+                  float* density_adv, float* a, const al_solver_params* sp, float* dt,
+                  uint32_t steps, al_step_report* reports) {
+  return run_impl<float>(2, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+                         density_adv, a, sp, dt, steps, reports);
+}
+int orc_i_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f64* bodies,
+                  double* rigid, uint32_t n, double* x, double* v, double* pressure,
+                  double* density, double* density_adv, double* a, const al_solver_params* sp,
+                  double* dt, uint32_t steps, al_step_report* reports) {
+  return run_impl<double>(2, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
                           density_adv, a, sp, dt, steps, reports);
 }
 

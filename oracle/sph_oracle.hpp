@@ -1162,6 +1162,50 @@ StepReport df_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& b
   return rep;
 }
 
+// compute_pressure_accels (runner.hpp:2774-2817), kinematic_integration<0>
+// (runner.hpp:2873-2887), the per-body totals and Pile::integrate_kinematics:
+// the common tail of SolverIi::step and SolverI::step.
+template <class TF>
+void pressure_accels_and_integrate(const Cn<TF>& c, std::vector<Body<TF>>& bodies, Fluid<TF>& f,
+                                   TF dt, std::vector<V3<double>>* F_out,
+                                   std::vector<V3<double>>* T_out, V3<TF> pile_gravity,
+                                   bool integrate_bodies) {
+  const uint32_t n = f.n;
+  const TF rho0 = c.rho0;
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    uint32_t i = uint32_t(ii);
+    TF rho = f.density[i], dpi = f.pressure[i] / (rho * rho);
+    V3<TF> ai{0, 0, 0};
+    for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      TF rj = f.density[j], dpj = f.pressure[j] / (rj * rj);
+      ai -= (c.mass * (dpi + dpj)) * gradW(c, xv(f, i, j));
+    }
+    for (uint32_t b = 0; b < f.nb; ++b) {
+      const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
+      const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
+      V3<TF> a = (rho0 * dpi) * V3<TF>{k4.x, k4.y, k4.z};
+      V3<TF> force = c.mass * a;
+      ai -= a;
+      f.force[size_t(b) * f.n + i] += force;
+      f.torque[size_t(b) * f.n + i] += cross(V3<TF>{bn.x, bn.y, bn.z} - bodies[b].x, force);
+    }
+    f.pressure_accel[i] = rho0 * ai;
+  }
+  // kinematic_integration<0> (runner.hpp:2873-2887)
+  for (uint32_t i = 0; i < n; ++i) {
+    V3<TF> v = f.v[i] + f.pressure_accel[i] * dt;
+    f.x[i] += v * dt;
+    f.v[i] = v;
+  }
+  std::vector<V3<double>> F, T;
+  rigid_totals(f, F, T);
+  if (F_out) *F_out = F;
+  if (T_out) *T_out = T;
+  if (integrate_bodies) integrate_kinematics(bodies, F, T, pile_gravity, dt);
+}
+
 // SolverIi<TF>::step<0> (solver_ii.hpp:76-243) without contacts.
 template <class TF>
 StepReport ii_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& bodies, Fluid<TF>& f,
@@ -1276,39 +1320,100 @@ StepReport ii_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& b
   }
   rep.num_density_solve = it;
   rep.mean_density_error = mean;
-  // compute_pressure_accels (runner.hpp:2774-2817)
+  pressure_accels_and_integrate(c, bodies, f, dt, F_out, T_out, pile_gravity, integrate_bodies);
+  return rep;
+}
+
+// SolverI<TF>::step<0> (solver_i.hpp:79-327), the implicit SPH solver
+// with volume-map boundaries, without contacts:
+//   advect_and_init_pressure (runner.hpp:2889-2900)
+//   calculate_isph_diagonal_adv_density (runner.hpp:2901-2954)
+//   isph_solve_iteration (runner.hpp:3006-3053): damped Jacobi, weight 2/3,
+//     on the last pressures, then last <- pressure and the mean density
+//     error (solver_i.hpp:243-276)
+//   then the tail shared with SolverIi.
+template <class TF>
+StepReport i_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& bodies, Fluid<TF>& f,
+                  const SolverParams& sp, TF& dt, V3<TF> pile_gravity, bool integrate_bodies,
+                  std::vector<V3<double>>* F_out = nullptr,
+                  std::vector<V3<double>>* T_out = nullptr) {
+  StepReport rep;
+  const uint32_t n = f.n;
+  std::fill(f.force.begin(), f.force.end(), V3<TF>{0, 0, 0});
+  std::fill(f.torque.begin(), f.torque.end(), V3<TF>{0, 0, 0});
+  compute_boundaries(c, bodies, f);
+  update_particle_neighbors(c, g, f);
+  rep.grid_anomaly[0] = f.gs.out_of_grid;
+  rep.grid_anomaly[1] = f.gs.cell_overflow;
+  rep.grid_anomaly[2] = f.nl.overflow;
+  compute_viscosity(c, bodies, f);
+  update_dt(c, bodies, f, sp, dt, rep);
+  rep.dt = dt;
+  const TF V = c.vol, rho0 = c.rho0, eps = TF(0.01) * c.h2;
+  for (uint32_t i = 0; i < n; ++i) {
+    f.v[i] += dt * f.a[i];
+    f.last_pressure[i] = f.pressure[i] * TF(0.5);
+  }
+  // diag (times rho0) into aii, density_adv
 #pragma omp parallel for schedule(static)
   for (int64_t ii = 0; ii < int64_t(n); ++ii) {
-    uint32_t i = uint32_t(ii);
-    TF rho = f.density[i], dpi = f.pressure[i] / (rho * rho);
-    V3<TF> ai{0, 0, 0};
+    const uint32_t i = uint32_t(ii);
+    const V3<TF> vi = f.v[i];
+    const TF rho = f.density[i];
+    TF adv = rho / rho0, diag = 0;
     for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
-      uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
-      TF rj = f.density[j], dpj = f.pressure[j] / (rj * rj);
-      ai -= (c.mass * (dpi + dpj)) * gradW(c, xv(f, i, j));
+      const uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+      const V3<TF> d = xv(f, i, j);
+      const TF rj = f.density[j];
+      const V3<TF> gw = gradW(c, d);
+      adv += dt * V * dot(vi - f.v[j], gw);
+      diag += V * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gw);
     }
     for (uint32_t b = 0; b < f.nb; ++b) {
       const V4<TF>& bn = f.bnd[size_t(b) * f.n + i];
       const V4<TF>& k4 = f.bk[size_t(b) * f.n + i];
-      V3<TF> a = (rho0 * dpi) * V3<TF>{k4.x, k4.y, k4.z};
-      V3<TF> force = c.mass * a;
-      ai -= a;
-      f.force[size_t(b) * f.n + i] += force;
-      f.torque[size_t(b) * f.n + i] += cross(V3<TF>{bn.x, bn.y, bn.z} - bodies[b].x, force);
+      const V3<TF> gwv{k4.x, k4.y, k4.z};
+      const V3<TF> xib = f.x[i] - V3<TF>{bn.x, bn.y, bn.z};
+      const V3<TF> vj = body_velocity(bodies[b], V3<TF>{bn.x, bn.y, bn.z});
+      adv += dt * dot(vi - vj, gwv);
+      diag += (rho + rho0) / (rho * rho0) / (length_sqr(xib) + eps) * dot(xib, gwv);
     }
-    f.pressure_accel[i] = rho0 * ai;
+    f.aii[i] = diag * rho0;
+    f.density_adv[i] = adv;
   }
-  // kinematic_integration<0> (runner.hpp:2873-2887)
-  for (uint32_t i = 0; i < n; ++i) {
-    V3<TF> v = f.v[i] + f.pressure_accel[i] * dt;
-    f.x[i] += v * dt;
-    f.v[i] = v;
+  double mean = std::numeric_limits<double>::max();
+  uint32_t it = 0;
+  while ((mean > sp.density_error_tolerance || it < sp.min_density_solve) &&
+         it < sp.max_density_solve) {
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+      const uint32_t i = uint32_t(ii);
+      const TF lp = f.last_pressure[i], rho = f.density[i], diag = f.aii[i];
+      const TF bterm = 1 - f.density_adv[i], dt2 = dt * dt, denom = diag * dt2;
+      const TF w = TF(2) / 3;
+      TF p = 0, off = 0;
+      for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
+        const uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
+        const V3<TF> d = xv(f, i, j);
+        const TF rj = f.density[j];
+        off -= V * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
+               f.last_pressure[j];
+      }
+      off *= rho0;
+      if (std::fabs(denom) > TF(1.0e-9))
+        p = std::max((1 - w) * lp + w * (bterm / denom - off / diag), TF(0));
+      f.density_err[i] = p == 0 ? TF(0) : (denom * p + off * dt2 - bterm);
+      f.pressure[i] = p;
+    }
+    for (uint32_t i = 0; i < n; ++i) f.last_pressure[i] = f.pressure[i];
+    double sum = 0;
+    for (uint32_t i = 0; i < n; ++i) sum += double(f.density_err[i]);
+    mean = sum / double(n);
+    ++it;
   }
-  std::vector<V3<double>> F, T;
-  rigid_totals(f, F, T);
-  if (F_out) *F_out = F;
-  if (T_out) *T_out = T;
-  if (integrate_bodies) integrate_kinematics(bodies, F, T, pile_gravity, dt);
+  rep.num_density_solve = it;
+  rep.mean_density_error = mean;
+  pressure_accels_and_integrate(c, bodies, f, dt, F_out, T_out, pile_gravity, integrate_bodies);
   return rep;
 }
 

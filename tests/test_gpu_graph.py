@@ -68,7 +68,7 @@ def _run(engine, method, dtype, graph, steps=6):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("method", ["df", "ii"])
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
 def test_graph_matches_eager(engine, method, dtype):
     eager = _run(engine, method, dtype, graph=False)
     graph = _run(engine, method, dtype, graph=True)

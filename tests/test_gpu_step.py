@@ -1,7 +1,8 @@
 """GPU parity of whole solver steps against the oracle, through the C ABI:
-SolverDf::step<0> (solver_df.hpp:74-359) and SolverIi::step<0>
-(solver_ii.hpp:76-243), both without contacts, on seeded dam-break scenes
-with a container and two-way coupled rigid bodies.
+SolverDf::step<0> (solver_df.hpp:74-359), SolverIi::step<0>
+(solver_ii.hpp:76-243) and SolverI::step<0> (solver_i.hpp:79-327), all
+without contacts, on seeded dam-break scenes with a container and two-way
+coupled rigid bodies.
 
 Tolerances (stated per quantity, relative to the quantity's scale; float32
 differences come from FMA contraction and summation order of the same
@@ -72,7 +73,7 @@ TOL = {
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("steps", [1, 4])
-@pytest.mark.parametrize("method", ["df", "ii"])
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
 def test_step_parity(engine, dtype, steps, method):
     scene = _scene(engine, dtype)
     sp = scenes.solver_params()
@@ -106,7 +107,7 @@ def test_step_parity(engine, dtype, steps, method):
                "rigid force %d" % b)
 
 
-@pytest.mark.parametrize("method", ["df", "ii"])
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
 def test_step_without_bodies_conserves_momentum(engine, method):
     """Free blob, g = 0, no boundaries, viscosity 0: the pressure pair terms are
     antisymmetric, so total momentum is conserved (the reference's viscosity
@@ -144,6 +145,24 @@ def test_iteration_caps_and_disabled_solves(engine):
     _, rep2 = scene2.step("df", sp2, 1e-4)
     assert rep2.num_density_solve == 0 and rep2.num_divergence_solve == 0
     _close(scene2.state()["v"], ostate2["v"], 1e-3, "v")
+
+
+@pytest.mark.parametrize("iterations", [0, 1, 2, 3])
+def test_implicit_sph_iteration_counts(engine, iterations):
+    """SolverI with exactly K Jacobi iterations: the engine alternates its two
+    pressure arrays by iteration parity, the reference copies; K = 0 keeps
+    the previous step's pressure for the accelerations."""
+    dtype = np.float32
+    scene = _scene(engine, dtype)
+    scene.pressure.copy_(torch.linspace(0.0, 50.0, scene.n, device="cuda"))
+    sp = scenes.solver_params(min_density_solve=iterations, max_density_solve=iterations)
+    ostate, _, _, oreps = _oracle_run(scene, "i", sp, 1e-4, 1)
+    _, rep = scene.step("i", sp, 1e-4)
+    assert rep.num_density_solve == iterations == oreps[0].num_density_solve
+    g = scene.state()
+    _close(g["pressure"], ostate["pressure"], 1e-2, "pressure")
+    _close(g["x"], ostate["x"], 1e-5, "x")
+    _close(g["v"], ostate["v"], 1e-3, "v")
 
 
 def test_empty_fluid_step(engine):

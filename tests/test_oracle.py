@@ -167,7 +167,7 @@ def _host_scene(dtype, lattice=(6, 6, 6), r=0.01, container=(0.2, 0.2, 0.2), res
     return cn, cni, arr, scenes.rigid_array(dtype, rig).reshape(-1, 13), state, keep
 
 
-@pytest.mark.parametrize("method", ["df", "ii"])
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
 def test_oracle_step_conserves_momentum_without_boundaries(method):
     dtype = np.float64
     # pressure terms are pairwise antisymmetric; the reference's viscosity
@@ -185,7 +185,7 @@ def test_oracle_step_conserves_momentum_without_boundaries(method):
     assert all(r.num_density_solve >= 2 for r in reps)
 
 
-@pytest.mark.parametrize("method", ["df", "ii"])
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
 def test_oracle_step_in_container(method):
     dtype = np.float32
     cn, cni, bodies, rigid, state, keep = _host_scene(dtype)
