@@ -158,6 +158,19 @@ class ContactF32(ctypes.Structure):
 CONTACT_FLOATS = ctypes.sizeof(ContactF32) // 4
 
 
+def _pellets_struct(real):
+    class Pellets(ctypes.Structure):
+        _fields_ = [("local_x", ctypes.c_void_p), ("num_pellets", ctypes.c_uint32),
+                    ("count", ctypes.c_uint32 * AL_MAX_BOUNDARIES), ("x", ctypes.c_void_p),
+                    ("pressure", ctypes.c_void_p), ("reserved", ctypes.c_uint32 * 2)]
+    Pellets.__name__ = "Pellets" + ("F32" if real is ctypes.c_float else "F64")
+    return Pellets
+
+
+PelletsF32 = _pellets_struct(ctypes.c_float)
+PelletsF64 = _pellets_struct(ctypes.c_double)
+
+
 class SampleF32(ctypes.Structure):
     """al_sample_f32: sample points, particle inputs and the outputs wanted
     (device pointers; None where unused)."""
@@ -276,6 +289,7 @@ for _s in ("f32", "f64"):
     _SIGNATURES["al_df_step_" + _s] = (ctypes.c_int, [_P] * 10)
     _SIGNATURES["al_ii_step_" + _s] = (ctypes.c_int, [_P] * 10)
     _SIGNATURES["al_i_step_" + _s] = (ctypes.c_int, [_P] * 10)
+    _SIGNATURES["al_i_step_pellets_" + _s] = (ctypes.c_int, [_P] * 11)
 
 
 def declared_symbols():

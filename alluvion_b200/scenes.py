@@ -540,3 +540,27 @@ def load_obj(path):
                 for j in range(1, len(idx) - 1):
                     faces.append((idx[0], idx[j], idx[j + 1]))
     return np.asarray(verts, np.float32), np.asarray(faces, np.uint32)
+
+
+# ------------------------------------------------------------------ pellets
+def box_shell_pellets(inner_size, spacing, layers=3):
+    """Boundary particles of a box container in its frame (centred): lattice
+    points of the given spacing in `layers` layers outside the interior box
+    of size inner_size (the fluid side), for the pellet boundary model."""
+    half = 0.5 * np.asarray(inner_size, np.float64)
+    lo = -half - (layers - 0.5) * spacing
+    counts = np.floor((2 * half + (2 * layers - 1) * spacing) / spacing).astype(int) + 1
+    axes = [lo[k] + spacing * np.arange(counts[k]) for k in range(3)]
+    g = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+    outside = np.any(np.abs(g) > half, axis=1)
+    return g[outside]
+
+
+def sphere_pellets(radius, spacing, thickness):
+    """Boundary particles of a sphere in its frame: lattice points of the
+    given spacing with radius - thickness < |x| <= radius."""
+    m = int(np.ceil(radius / spacing))
+    a = spacing * np.arange(-m, m + 1)
+    g = np.stack(np.meshgrid(a, a, a, indexing="ij"), -1).reshape(-1, 3)
+    r = np.linalg.norm(g, axis=1)
+    return g[(r <= radius) & (r > radius - thickness)]

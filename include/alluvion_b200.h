@@ -476,6 +476,55 @@ AL_API int al_i_step_f64(al_engine* engine, const al_const_f64* cn, const al_con
                          al_rigid_f64* rigid, const al_solver_params* params, double* dt,
                          al_step_report* report, void* stream);
 
+/* ------------------------------------------------- pellet boundary model
+ * Bodies represented by boundary particles ("pellets", Pile with
+ * VolumeMethod::pellets): SolverI<TF>::step<0> (solver_i.hpp:79-327) on the
+ * pellet branch, without contacts --
+ *   transform_pellets (runner.hpp:4070-4082) from each body's pose,
+ *   one grid over particles and pellets, bead / pellet neighbor lists
+ *   (make_bead_pellet_neighbor_list, runner.hpp:1912-1966: particle j < N
+ *   is a bead, j >= N a pellet; pellets get lists too),
+ *   compute_density_with_pellets (runner.hpp:2074-2098),
+ *   compute_viscosity_with_pellets (runner.hpp:2251-2299),
+ *   calculate_isph_diagonal_adv_density_with_pellets (runner.hpp:2955-3004),
+ *   per iteration extrapolate_pressure_to_pellet (runner.hpp:2543-2607,
+ *   Shepard average + linear moving-least-squares term through a 3x3
+ *   pseudo-inverse with singular values below 1e-2 dropped) and
+ *   isph_solve_iteration_with_pellets (runner.hpp:3055-3121),
+ *   compute_pressure_accels_with_pellets (runner.hpp:2819-2871),
+ *   kinematic_integration, per-body totals and Pile::integrate_kinematics.
+ * Pellets weigh as fluid particles of rest density rho0.  Bodies need
+ * mass, inertia and max_distance; their node arrays are not read.
+ * Eager: the host reads the loop flag after every iteration. */
+typedef struct al_pellets_f32 {
+  const float* local_x;  /* device [num_pellets][3]: body frame, body after body */
+  uint32_t num_pellets;
+  uint32_t count[AL_MAX_BOUNDARIES]; /* pellets of each body, in body order */
+  float* x;              /* device [num_pellets][3] out or NULL: world positions */
+  float* pressure;       /* device [num_pellets] out or NULL: extrapolated pressure */
+  uint32_t reserved[2];
+} al_pellets_f32;
+
+typedef struct al_pellets_f64 {
+  const double* local_x;
+  uint32_t num_pellets;
+  uint32_t count[AL_MAX_BOUNDARIES];
+  double* x;
+  double* pressure;
+  uint32_t reserved[2];
+} al_pellets_f64;
+
+AL_API int al_i_step_pellets_f32(al_engine* engine, const al_const_f32* cn,
+                                 const al_consti* cni, const al_fluid_f32* fluid,
+                                 const al_body_f32* bodies, al_rigid_f32* rigid,
+                                 const al_pellets_f32* pellets, const al_solver_params* params,
+                                 float* dt, al_step_report* report, void* stream);
+AL_API int al_i_step_pellets_f64(al_engine* engine, const al_const_f64* cn,
+                                 const al_consti* cni, const al_fluid_f64* fluid,
+                                 const al_body_f64* bodies, al_rigid_f64* rigid,
+                                 const al_pellets_f64* pellets, const al_solver_params* params,
+                                 double* dt, al_step_report* report, void* stream);
+
 /* ---------------------------------------------------- learned warm start
  * No reference counterpart.  A per-particle MLP 12 -> 64 -> 64 -> 2 with
  * GELU (tanh form), BF16 operands and FP32 accumulation on the tensor

@@ -48,6 +48,9 @@ def lib():
             sig["orc_df_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 9 + [_U, _P])
             sig["orc_ii_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 8 + [_U, _P])
             sig["orc_i_run_" + s] = (ctypes.c_int, [_P] * 4 + [_U] + [_P] * 8 + [_U, _P])
+            # ... a, pellet_local, counts, num_pellets, sp, dt, steps, reports, pellet_x, pellet_p
+            sig["orc_i_run_pellets_" + s] = (
+                ctypes.c_int, [_P] * 4 + [_U] + [_P] * 8 + [_U, _P, _P, _U, _P, _P, _P])
         for name, (res, args) in sig.items():
             fn = getattr(handle, name)
             fn.restype = res
@@ -282,3 +285,28 @@ def kl_divergence(p, q, n_p, n_q, q_lower_bound):
     p = np.ascontiguousarray(p, np.uint32)
     q = np.ascontiguousarray(q, np.uint32)
     return lib().orc_kl_divergence(_p(p), _p(q), n_p, n_q, float(q_lower_bound), len(p))
+
+
+def run_pellets(cn, cni, bodies, rigid, state, pellet_local, counts, sp, dt, steps):
+    """SolverI with the pellet boundary model: advances `state` (x, v,
+    pressure, density, density_adv, a) by `steps` steps in place.  Returns
+    (dt, reports, pellet world positions, pellet pressures) of the last step."""
+    from alluvion_b200 import _capi
+    x = state["x"]
+    T = x.dtype
+    n = x.shape[0]
+    local = np.ascontiguousarray(pellet_local, T).reshape(-1, 3)
+    npl = len(local)
+    cnt = np.ascontiguousarray(counts, np.uint32)
+    dt_arr = np.array([dt], dtype=T)
+    reports = (_capi.StepReport * steps)()
+    px = np.zeros((npl, 3), T)
+    pp = np.zeros(npl, T)
+    nb = len(bodies)
+    status = getattr(lib(), "orc_i_run_pellets_" + _sfx(T))(
+        _p(cn), _p(cni), _p(bodies) if nb else None, _p(rigid), n, _p(x), _p(state["v"]),
+        _p(state["pressure"]), _p(state["density"]), _p(state["density_adv"]), _p(state["a"]),
+        _p(local) if npl else None, _p(cnt), npl, _p(sp), _p(dt_arr), steps, _p(reports),
+        _p(px), _p(pp))
+    assert status == 0
+    return float(dt_arr[0]), list(reports), px, pp

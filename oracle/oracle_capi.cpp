@@ -181,9 +181,11 @@ template <class TF, class C, class B>
 int run_impl(int method, const C* cn, const al_consti* cni, const B* bodies, TF* rigid,
              uint32_t n, TF* x, TF* v, TF* kappa_or_pressure, TF* kappa_v, TF* density,
              TF* density_adv, TF* a, const al_solver_params* sp_in, TF* dt, uint32_t steps,
-             al_step_report* reports) {
+             al_step_report* reports, const PelletSet<TF>* pel = nullptr,
+             TF* pellet_x = nullptr, TF* pellet_p = nullptr) {
   Cn<TF> c = make_cn<TF>(*cn);
-  const bool iisph = method != 0;  // 0 DFSPH, 1 IISPH, 2 implicit SPH (SolverI)
+  // 0 DFSPH, 1 IISPH, 2 implicit SPH (SolverI), 3 SolverI with pellets
+  const bool iisph = method != 0;
   const uint32_t nb = cni->num_boundaries;
   std::vector<Body<TF>> bs;
   for (uint32_t b = 0; b < nb; ++b) bs.push_back(make_body<TF>(bodies[b], rigid + 13 * b));
@@ -221,9 +223,21 @@ int run_impl(int method, const C* cn, const al_consti* cni, const B* bodies, TF*
   for (uint32_t s = 0; s < steps; ++s) {
     std::vector<V3<double>> F, T;
     const bool ib = sp_in->integrate_rigids != 0;
+    std::vector<V3<TF>> px;
+    std::vector<TF> pp;
     StepReport r = method == 1   ? ii_step(c, *cni, bs, f, sp, step_dt, pg, ib, &F, &T)
                    : method == 2 ? i_step(c, *cni, bs, f, sp, step_dt, pg, ib, &F, &T)
+                   : method == 3 ? i_step_pellets(c, *cni, bs, f, *pel, sp, step_dt, pg, ib, &F,
+                                                  &T, &px, &pp)
                                  : df_step(c, *cni, bs, f, sp, step_dt, pg, ib, &F, &T);
+    for (size_t k = 0; k < px.size(); ++k) {
+      if (pellet_x) {
+        pellet_x[3 * k] = px[k].x;
+        pellet_x[3 * k + 1] = px[k].y;
+        pellet_x[3 * k + 2] = px[k].z;
+      }
+      if (pellet_p) pellet_p[k] = pp[k];
+    }
     if (reports) {
       al_step_report& o = reports[s];
       std::memset(&o, 0, sizeof(o));
@@ -281,6 +295,26 @@ int run_impl(int method, const C* cn, const al_consti* cni, const B* bodies, TF*
     std::copy(vals, vals + 13, r);
   }
   return 0;
+}
+
+// SolverI with pellets: pellet_local [P][3] body frame, body after body,
+// counts[nb]; pellet_x / pellet_p (may be NULL) receive the last step's
+// world positions and extrapolated pressures.
+template <class TF, class C, class B>
+int run_pellets(const C* cn, const al_consti* cni, const B* bodies, TF* rigid, uint32_t n, TF* x,
+                TF* v, TF* pressure, TF* density, TF* density_adv, TF* a, const TF* pellet_local,
+                const uint32_t* counts, uint32_t np, const al_solver_params* sp, TF* dt,
+                uint32_t steps, al_step_report* reports, TF* pellet_x, TF* pellet_p) {
+  PelletSet<TF> pel;
+  uint32_t b = 0, left = cni->num_boundaries ? counts[0] : 0;
+  for (uint32_t k = 0; k < np; ++k) {
+    while (left == 0 && b + 1 < cni->num_boundaries) left = counts[++b];
+    pel.local.push_back(v3<TF>(pellet_local + 3 * size_t(k)));
+    pel.body.push_back(b);
+    if (left) --left;
+  }
+  return run_impl<TF>(3, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
+                      density_adv, a, sp, dt, steps, reports, &pel, pellet_x, pellet_p);
 }
 
 }  // namespace
@@ -403,6 +437,25 @@ int orc_i_run_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f6
                   double* dt, uint32_t steps, al_step_report* reports) {
   return run_impl<double>(2, cn, cni, bodies, rigid, n, x, v, pressure, nullptr, density,
                           density_adv, a, sp, dt, steps, reports);
+}
+
+int orc_i_run_pellets_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f32* bodies,
+                          float* rigid, uint32_t n, float* x, float* v, float* pressure,
+                          float* density, float* density_adv, float* a, const float* pellet_local,
+                          const uint32_t* counts, uint32_t np, const al_solver_params* sp,
+                          float* dt, uint32_t steps, al_step_report* reports, float* pellet_x,
+                          float* pellet_p) {
+  return run_pellets<float>(cn, cni, bodies, rigid, n, x, v, pressure, density, density_adv, a,
+                            pellet_local, counts, np, sp, dt, steps, reports, pellet_x, pellet_p);
+}
+int orc_i_run_pellets_f64(const al_const_f64* cn, const al_consti* cni, const al_body_f64* bodies,
+                          double* rigid, uint32_t n, double* x, double* v, double* pressure,
+                          double* density, double* density_adv, double* a,
+                          const double* pellet_local, const uint32_t* counts, uint32_t np,
+                          const al_solver_params* sp, double* dt, uint32_t steps,
+                          al_step_report* reports, double* pellet_x, double* pellet_p) {
+  return run_pellets<double>(cn, cni, bodies, rigid, n, x, v, pressure, density, density_adv, a,
+                             pellet_local, counts, np, sp, dt, steps, reports, pellet_x, pellet_p);
 }
 
 }  // extern "C"

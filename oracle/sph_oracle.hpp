@@ -1417,6 +1417,314 @@ StepReport i_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& bo
   return rep;
 }
 
+// ------------------------------------------------- pellet boundary model
+// SolverI<TF>::step<0> (solver_i.hpp:79-327) on the pellet branch
+// (VolumeMethod::pellets), without contacts.  Pellets are boundary particles
+// given in their body's frame; points 0..n-1 are the fluid particles
+// ("beads"), n..n+P-1 the pellets.
+template <class TF>
+struct PelletSet {
+  std::vector<V3<TF>> local;   // body frame
+  std::vector<uint32_t> body;  // body of each pellet
+};
+
+// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+// (Golub and Van Loan, Matrix Computations, sec. 8.5), six sweeps: a ends
+// diagonal, the columns of q are the eigenvectors.
+template <class TF>
+void jacobi_eigen3(TF a[3][3], TF q[3][3]) {
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) q[r][k] = r == k ? TF(1) : TF(0);
+  for (int sweep = 0; sweep < 6; ++sweep) {
+    for (int pr = 0; pr < 3; ++pr) {
+      const int p = pr == 2 ? 1 : 0;
+      const int r = pr == 0 ? 1 : 2;
+      const TF apr = a[p][r];
+      if (apr == TF(0)) continue;
+      const TF theta = (a[r][r] - a[p][p]) / (TF(2) * apr);
+      const TF t = (theta >= TF(0) ? TF(1) : TF(-1)) /
+                   (std::fabs(theta) + std::sqrt(theta * theta + TF(1)));
+      const TF cs = TF(1) / std::sqrt(t * t + TF(1));
+      const TF sn = t * cs;
+      a[p][p] -= t * apr;
+      a[r][r] += t * apr;
+      a[p][r] = a[r][p] = TF(0);
+      const int k = 3 - p - r;
+      const TF akp = a[k][p], akr = a[k][r];
+      a[k][p] = a[p][k] = cs * akp - sn * akr;
+      a[k][r] = a[r][k] = sn * akp + cs * akr;
+      for (int row = 0; row < 3; ++row) {
+        const TF qp = q[row][p], qr = q[row][r];
+        q[row][p] = cs * qp - sn * qr;
+        q[row][r] = sn * qp + cs * qr;
+      }
+    }
+  }
+}
+
+// extrapolate_pressure_to_pellet (runner.hpp:2543-2607) for point i from
+// its bead list: Shepard average plus the linear MLS term through the
+// pseudo-inverse of the weighted second moment (eigenvalues of magnitude
+// <= 1e-2 dropped), clamped at 0; 0 without bead neighbors (the
+// reference's 0/0 becomes 0 through fmax).
+template <class TF>
+TF extrapolate_pellet(const Cn<TF>& c, const std::vector<V3<TF>>& X, const std::vector<TF>& pr,
+                      const uint32_t* list, uint32_t cnt, V3<TF> xi) {
+  TF wsum = 0;
+  V3<TF> center{0, 0, 0};
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const TF w = W_r2(c, dist2(xi, X[list[k]])) * c.vol;
+    wsum += w;
+    center += w * X[list[k]];
+  }
+  if (!(wsum > 0)) return 0;
+  center = (TF(1) / wsum) * center;
+  TF alpha = 0;
+  V3<TF> psum{0, 0, 0};
+  TF m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (uint32_t k = 0; k < cnt; ++k) {
+    const uint32_t j = list[k];
+    const V3<TF> xt = X[j] - center;
+    const TF w = W_r2(c, dist2(xi, X[j])) * c.vol;
+    const TF wp = w * pr[j];
+    alpha += wp;
+    psum += wp * xt;
+    m[0][0] += w * xt.x * xt.x;
+    m[1][1] += w * xt.y * xt.y;
+    m[2][2] += w * xt.z * xt.z;
+    m[0][1] += w * (xt.x * xt.y);
+    m[0][2] += w * (xt.x * xt.z);
+    m[1][2] += w * (xt.y * xt.z);
+  }
+  m[1][0] = m[0][1];
+  m[2][0] = m[0][2];
+  m[2][1] = m[1][2];
+  alpha /= wsum;
+  TF q[3][3];
+  jacobi_eigen3(m, q);
+  V3<TF> plane{0, 0, 0};
+  for (int e = 0; e < 3; ++e) {
+    const TF lam = m[e][e];
+    if (!(std::fabs(lam) > TF(1e-2))) continue;
+    const V3<TF> qe{q[0][e], q[1][e], q[2][e]};
+    plane += (dot(qe, psum) / lam) * qe;
+  }
+  return std::max(alpha + dot(plane, xi - center), TF(0));
+}
+
+template <class TF>
+StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& bodies,
+                          Fluid<TF>& f, const PelletSet<TF>& pel, const SolverParams& sp, TF& dt,
+                          V3<TF> pile_gravity, bool integrate_bodies,
+                          std::vector<V3<double>>* F_out, std::vector<V3<double>>* T_out,
+                          std::vector<V3<TF>>* pellet_x, std::vector<TF>* pellet_p) {
+  StepReport rep;
+  const uint32_t n = f.n, np = uint32_t(pel.local.size()), total = n + np;
+  const TF eps = TF(0.01) * c.h2;
+  std::fill(f.force.begin(), f.force.end(), V3<TF>{0, 0, 0});
+  std::fill(f.torque.begin(), f.torque.end(), V3<TF>{0, 0, 0});
+  // transform_pellets (runner.hpp:4070-4082)
+  std::vector<V3<TF>> X(f.x), Vv(f.v);
+  X.resize(total);
+  Vv.resize(total);
+  for (uint32_t p = 0; p < np; ++p) {
+    const Body<TF>& b = bodies[pel.body[p]];
+    const V3<TF> rl = rotate(pel.local[p], b.q);
+    X[n + p] = rl + b.x;
+    Vv[n + p] = cross(b.omega, rl) + b.v;
+  }
+  // one grid, bead / pellet lists (make_bead_pellet_neighbor_list,
+  // runner.hpp:1912-1966) for every point
+  const GridSort s = grid_sort(c, g, X.data(), total);
+  rep.grid_anomaly[0] = s.out_of_grid;
+  rep.grid_anomaly[1] = s.cell_overflow;
+  const uint32_t cap = g.max_num_neighbors_per_particle;
+  std::vector<uint32_t> bl(size_t(total) * cap), pl(size_t(total) * cap), bc(total), pc(total);
+  bool overflow = false;
+#pragma omp parallel for schedule(static) reduction(|| : overflow)
+  for (int64_t ii = 0; ii < int64_t(total); ++ii) {
+    const uint32_t i = uint32_t(ii);
+    int p[3];
+    cell_coords(c, g, X[i], p);
+    uint32_t nbd = 0, npl = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          int q[3] = {p[0] + dx, p[1] + dy, p[2] + dz};
+          if (!in_grid(g, q)) continue;
+          const uint32_t cell = cell_linear(g, q);
+          for (uint32_t t = s.cell_start[cell]; t < s.cell_start[cell + 1]; ++t) {
+            const uint32_t j = s.sorted[t];
+            if (j == i || !(dist2(X[i], X[j]) < c.h2)) continue;
+            if (j < n) {
+              if (nbd < cap) bl[size_t(i) * cap + nbd] = j;
+              ++nbd;
+            } else {
+              if (npl < cap) pl[size_t(i) * cap + npl] = j;
+              ++npl;
+            }
+          }
+        }
+    if (nbd > cap || npl > cap) overflow = true;
+    bc[i] = std::min(nbd, cap);
+    pc[i] = std::min(npl, cap);
+  }
+  rep.grid_anomaly[2] = overflow;
+  auto B = [&](uint32_t i, uint32_t k) { return bl[size_t(i) * cap + k]; };
+  auto Pn = [&](uint32_t i, uint32_t k) { return pl[size_t(i) * cap + k]; };
+  // compute_density_with_pellets (runner.hpp:2074-2098)
+  for (uint32_t i = 0; i < n; ++i) {
+    TF d = c.w0;
+    for (uint32_t k = 0; k < bc[i]; ++k) d += W_r2(c, dist2(X[i], X[B(i, k)]));
+    for (uint32_t k = 0; k < pc[i]; ++k) d += W_r2(c, dist2(X[i], X[Pn(i, k)]));
+    f.density[i] = d * c.mass;
+  }
+  // clear_acceleration + compute_viscosity_with_pellets (runner.hpp:2251-2299)
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    const uint32_t i = uint32_t(ii);
+    V3<TF> da{0, 0, 0};
+    for (uint32_t k = 0; k < bc[i]; ++k) {
+      const uint32_t j = B(i, k);
+      const V3<TF> d = X[i] - X[j];
+      da += (c.visc * c.mass / f.density[j] * dot(d, gradW(c, d)) / (length_sqr(d) + eps)) *
+            (Vv[i] - Vv[j]);
+    }
+    for (uint32_t k = 0; k < pc[i]; ++k) {
+      const uint32_t j = Pn(i, k);
+      const V3<TF> d = X[i] - X[j];
+      const V3<TF> a =
+          (c.vol * c.bvisc * dot(d, gradW(c, d)) / (length_sqr(d) + eps)) * (Vv[i] - Vv[j]);
+      da += a;
+      const uint32_t b = pel.body[j - n];
+      const V3<TF> force = (-c.mass) * a;
+      f.force[size_t(b) * n + i] += force;
+      f.torque[size_t(b) * n + i] += cross(X[j] - bodies[b].x, force);
+    }
+    f.a[i] = c.g + da;
+  }
+  update_dt(c, bodies, f, sp, dt, rep);
+  rep.dt = dt;
+  // advect_and_init_pressure
+  std::vector<TF> P(total, 0), L(total, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    f.v[i] += dt * f.a[i];
+    Vv[i] = f.v[i];
+    P[i] = f.pressure[i];
+    L[i] = f.pressure[i] * TF(0.5);
+  }
+  // calculate_isph_diagonal_adv_density_with_pellets (runner.hpp:2955-3004)
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    const uint32_t i = uint32_t(ii);
+    const TF rho = f.density[i];
+    TF adv = rho / c.rho0, diag = 0;
+    for (uint32_t k = 0; k < bc[i]; ++k) {
+      const uint32_t j = B(i, k);
+      const V3<TF> d = X[i] - X[j];
+      const TF rj = f.density[j];
+      const V3<TF> gw = gradW(c, d);
+      adv += dt * c.vol * dot(Vv[i] - Vv[j], gw);
+      diag += c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gw);
+    }
+    for (uint32_t k = 0; k < pc[i]; ++k) {
+      const uint32_t j = Pn(i, k);
+      const V3<TF> d = X[i] - X[j];
+      const V3<TF> gwv = c.vol * gradW(c, d);
+      adv += dt * dot(Vv[i] - Vv[j], gwv);
+      diag += (rho + c.rho0) / (rho * c.rho0) / (length_sqr(d) + eps) * dot(d, gwv);
+    }
+    f.aii[i] = diag * c.rho0;
+    f.density_adv[i] = adv;
+  }
+  auto extrapolate = [&](std::vector<TF>& pr) {
+#pragma omp parallel for schedule(static)
+    for (int64_t pp = 0; pp < int64_t(np); ++pp) {
+      const uint32_t i = n + uint32_t(pp);
+      pr[i] = extrapolate_pellet(c, X, pr, &bl[size_t(i) * cap], bc[i], X[i]);
+    }
+  };
+  double mean = std::numeric_limits<double>::max();
+  uint32_t it = 0;
+  while ((mean > sp.density_error_tolerance || it < sp.min_density_solve) &&
+         it < sp.max_density_solve) {
+    extrapolate(L);
+    // isph_solve_iteration_with_pellets (runner.hpp:3055-3121)
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+      const uint32_t i = uint32_t(ii);
+      const TF rho = f.density[i], diag = f.aii[i];
+      const TF bterm = 1 - f.density_adv[i], dt2 = dt * dt, denom = diag * dt2;
+      const TF w = TF(2) / 3;
+      TF off = 0, pv = 0;
+      for (uint32_t k = 0; k < bc[i]; ++k) {
+        const uint32_t j = B(i, k);
+        const V3<TF> d = X[i] - X[j];
+        const TF rj = f.density[j];
+        off -= c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
+               L[j];
+      }
+      for (uint32_t k = 0; k < pc[i]; ++k) {
+        const uint32_t j = Pn(i, k);
+        const V3<TF> d = X[i] - X[j];
+        off -= c.vol * (rho + c.rho0) / (rho * c.rho0) / (length_sqr(d) + eps) *
+               dot(d, gradW(c, d)) * L[j];
+      }
+      off *= c.rho0;
+      if (std::fabs(denom) > TF(1.0e-9))
+        pv = std::max((1 - w) * L[i] + w * (bterm / denom - off / diag), TF(0));
+      f.density_err[i] = pv == 0 ? TF(0) : (denom * pv + off * dt2 - bterm);
+      P[i] = pv;
+    }
+    for (uint32_t i = 0; i < n; ++i) L[i] = P[i];
+    double sum = 0;
+    for (uint32_t i = 0; i < n; ++i) sum += double(f.density_err[i]);
+    mean = sum / double(n);
+    ++it;
+  }
+  rep.num_density_solve = it;
+  rep.mean_density_error = mean;
+  extrapolate(P);
+  // compute_pressure_accels_with_pellets (runner.hpp:2819-2871) and
+  // kinematic_integration<0>
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+    const uint32_t i = uint32_t(ii);
+    const TF rho = f.density[i], dpi = P[i] / (rho * rho);
+    V3<TF> ai{0, 0, 0};
+    for (uint32_t k = 0; k < bc[i]; ++k) {
+      const uint32_t j = B(i, k);
+      const TF rj = f.density[j], dpj = P[j] / (rj * rj);
+      ai -= (c.mass * (dpi + dpj)) * gradW(c, X[i] - X[j]);
+    }
+    for (uint32_t k = 0; k < pc[i]; ++k) {
+      const uint32_t j = Pn(i, k);
+      const TF dpj = P[j] / (c.rho0 * c.rho0);
+      const V3<TF> a = (c.mass * (dpi + dpj)) * gradW(c, X[i] - X[j]);
+      const V3<TF> force = c.mass * a;
+      ai -= a;
+      const uint32_t b = pel.body[j - n];
+      f.force[size_t(b) * n + i] += force;
+      f.torque[size_t(b) * n + i] += cross(X[j] - bodies[b].x, force);
+    }
+    f.pressure_accel[i] = c.rho0 * ai;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    const V3<TF> v = f.v[i] + f.pressure_accel[i] * dt;
+    f.x[i] += v * dt;
+    f.v[i] = v;
+    f.pressure[i] = P[i];
+  }
+  if (pellet_x) pellet_x->assign(X.begin() + n, X.end());
+  if (pellet_p) pellet_p->assign(P.begin() + n, P.end());
+  std::vector<V3<double>> F, T;
+  rigid_totals(f, F, T);
+  if (F_out) *F_out = F;
+  if (T_out) *T_out = T;
+  if (integrate_bodies) integrate_kinematics(bodies, F, T, pile_gravity, dt);
+  return rep;
+}
+
 // ---------------------------------------------------------------- contacts
 // Rigid-rigid contacts: Contact (contact.hpp:8-25), collision_test
 // (runner.hpp:3833-4010; analytic distance for analytic bodies, the
