@@ -162,7 +162,7 @@ def _pellets_struct(real):
     class Pellets(ctypes.Structure):
         _fields_ = [("local_x", ctypes.c_void_p), ("num_pellets", ctypes.c_uint32),
                     ("count", ctypes.c_uint32 * AL_MAX_BOUNDARIES), ("x", ctypes.c_void_p),
-                    ("pressure", ctypes.c_void_p), ("reserved", ctypes.c_uint32 * 2)]
+                    ("pressure", ctypes.c_void_p), ("v", ctypes.c_void_p)]
     Pellets.__name__ = "Pellets" + ("F32" if real is ctypes.c_float else "F64")
     return Pellets
 
@@ -183,7 +183,9 @@ class SampleF32(ctypes.Structure):
                 ("sample_position_density", ctypes.c_void_p),
                 ("sample_quantity", ctypes.c_void_p), ("sample_v", ctypes.c_void_p),
                 ("sample_vorticity", ctypes.c_void_p), ("wrap_y", ctypes.c_uint32),
-                ("wrap_length", ctypes.c_float), ("reserved", ctypes.c_uint32 * 2)]
+                ("wrap_length", ctypes.c_float), ("pellet_x", ctypes.c_void_p),
+                ("pellet_v", ctypes.c_void_p), ("num_pellets", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class StepReport(ctypes.Structure):

@@ -528,10 +528,12 @@ __global__ void k_pel_force_slots(PelletState<TF> S, double* ft, uint32_t chunk)
 }
 
 template <class TF>
-__global__ void k_pel_outputs(PelletState<TF> S, TF* __restrict__ x_out, TF* __restrict__ p_out) {
+__global__ void k_pel_outputs(PelletState<TF> S, TF* __restrict__ x_out, TF* __restrict__ p_out,
+                              TF* __restrict__ v_out) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= S.np) return;
   if (x_out) stv(x_out, p, ldv(S.x, S.n + p));
+  if (v_out) stv(v_out, p, ldv(S.v, S.n + p));
   if (p_out) p_out[p] = final_pressure(S, S.ctrl->it)[S.n + p];
 }
 
@@ -707,10 +709,10 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
                  (k_pel_force_slots<TF><<<dim3(slots, nb), 256, 0, st>>>(S, ft, chunk)));
   }
   if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(SS));
-  if (np && (pel->x || pel->pressure))
+  if (np && (pel->x || pel->pressure || pel->v))
     ALB_LAUNCH(e, "pellet_outputs", 1, st,
-               (k_pel_outputs<TF><<<blocks_for(np, kBlock), kBlock, 0, st>>>(S, pel->x,
-                                                                             pel->pressure)));
+               (k_pel_outputs<TF><<<blocks_for(np, kBlock), kBlock, 0, st>>>(
+                   S, pel->x, pel->pressure, pel->v)));
   ALB_CUDA(cudaGetLastError());
   uint32_t hf[4];
   ALB_CUDA(cudaMemcpyAsync(&hc, S.ctrl, sizeof(hc), cudaMemcpyDeviceToHost, st));

@@ -60,6 +60,9 @@ struct SampleDev {
   float* vort;       // [S][3]
   uint32_t wrap;     // periodic in y
   float wrap_length, wrap_min, wrap_max;
+  uint32_t nbead;    // points j < nbead are particles, the rest pellets
+  uint32_t npel;     // pellets (0: volume-map bodies, if any)
+  const float* pv;   // [npel][3] pellet velocities
 };
 
 // wrap_y (runner.hpp:698-707) of a displacement's y component.
@@ -98,7 +101,10 @@ __global__ void __launch_bounds__(kBlock)
   float dens = 0;
   float qs[3] = {0, 0, 0};
   V3 vel{0, 0, 0}, vort{0, 0, 0};
-  uint32_t cnt = 0;
+  // pellet terms (the *_with_pellets kernels): sum W, V W v_p, V (v_p - v_s) x grad W
+  float wb = 0, wp = 0;
+  V3 velp{0, 0, 0}, vortp{0, 0, 0};
+  uint32_t cnt = 0, cntp = 0;
   if (z0 <= z1) {
     for (int dx = -1; dx <= 1; ++dx) {
       const int cx = ip[0] + dx;
@@ -122,10 +128,23 @@ __global__ void __launch_bounds__(kBlock)
           if (sd.wrap) d.y = wrap_dy(sd, d.y);
           const float d2 = add_rn(add_rn(mul_rn(d.x, d.x), mul_rn(d.y, d.y)), mul_rn(d.z, d.z));
           if (!(d2 < c.h2)) continue;
+          if (j >= sd.nbead) {  // a pellet
+            if (cntp++ >= g.cap_nbr) continue;
+            const V3 vp = ld3(sd.pv, j - sd.nbead);
+            if (!VORT) {
+              const float w = W_r2(c, d2);
+              wp += w;
+              if (sd.vel) velp += (c.vol * w) * vp;
+            } else {
+              vortp += c.vol * cross(vp - vi, gradW(c, d));
+            }
+            continue;
+          }
           if (cnt++ >= g.cap_nbr) continue;
           if (!VORT) {
             const float w = W_r2(c, d2);
             if (want_w) dens += c.vol * w;
+            if (sd.npel) wb += w;
             if (sd.quantity || sd.vel) {
               const float mrw = c.mass / __ldg(sd.rho + j) * w;
               for (uint32_t k = 0; k < sd.qdim; ++k) qs[k] += mrw * __ldg(sd.q + size_t(j) * sd.qdim + k);
@@ -138,10 +157,13 @@ __global__ void __launch_bounds__(kBlock)
       }
     }
   }
-  if (cnt > g.cap_nbr) flags[2] = 1u;
-  // body terms (runner.hpp:2116-2118, 4228-4236, 4310-4321)
+  if (cnt > g.cap_nbr || cntp > g.cap_nbr) flags[2] = 1u;
+  // pellet sums after the particles' (the reference's list order)
+  vel += velp;
+  vort += vortp;
+  // volume-map body terms (runner.hpp:2116-2118, 4228-4236, 4310-4321)
   float bw = 0;
-  for (uint32_t b = 0; b < g.nb; ++b) {
+  for (uint32_t b = 0; b < (sd.npel ? 0u : g.nb); ++b) {
     const float* bk = sd.bker + (size_t(b) * sd.num + s) * 4;
     if (!VORT) {
       bw += bk[3];
@@ -152,7 +174,8 @@ __global__ void __launch_bounds__(kBlock)
   }
   if (!VORT) {
     if (sd.density) sd.density[s] = dens * c.rho0;
-    if (sd.pdensity) sd.pdensity[s] = (dens + bw) * c.rho0;
+    if (sd.pdensity)  // sample_position_density[_with_pellets]
+      sd.pdensity[s] = sd.npel ? (wb + wp) * c.mass : (dens + bw) * c.rho0;
     if (sd.quantity)
       for (uint32_t k = 0; k < sd.qdim; ++k) sd.quantity[size_t(s) * sd.qdim + k] = qs[k];
     if (sd.vel) st3(sd.vel, s, vel);
@@ -289,10 +312,16 @@ int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_cons
   ALB_CHECK_ARG(cni->num_boundaries <= AL_MAX_BOUNDARIES, "al_sample_fluid_f32: too many bodies");
   ALB_CHECK_ARG(!req->wrap_y || req->wrap_length > 0.f,
                 "al_sample_fluid_f32: wrap_y needs a positive wrap_length");
-  const bool body_terms = req->sample_position_density || req->sample_v;
+  const uint32_t npel = req->num_pellets;
+  ALB_CHECK_ARG(npel == 0 || (req->pellet_x && (req->pellet_v || !(req->sample_v ||
+                                                                  req->sample_vorticity))),
+                "al_sample_fluid_f32: pellet_x / pellet_v are null");
+  ALB_CHECK_ARG(uint64_t(num_particles) + npel < (1ull << 31), "al_sample_fluid_f32: too many points");
+  const bool body_terms = npel == 0 && (req->sample_position_density || req->sample_v);
   ALB_CHECK_ARG(cni->num_boundaries == 0 || !body_terms || req->sample_boundary_kernel,
                 "al_sample_fluid_f32: sample_boundary_kernel is null");
-  ALB_CHECK_ARG(cni->num_boundaries == 0 || !req->sample_v || (req->sample_boundary && rigid),
+  ALB_CHECK_ARG(cni->num_boundaries == 0 || npel || !req->sample_v ||
+                    (req->sample_boundary && rigid),
                 "al_sample_fluid_f32: velocities need sample_boundary and rigid");
   ALB_TRY(engine->activate());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -323,15 +352,29 @@ int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_cons
   ALB_TRY(engine->buf("flags", 4, &flags));
   ALB_TRY(engine->buf("rigid", AL_MAX_BOUNDARIES, &dr));
   ALB_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), st));
-  if (g.nb && req->sample_v) {
+  if (g.nb && req->sample_v && npel == 0) {
     RigidDev<float> hr[AL_MAX_BOUNDARIES];
     for (uint32_t b = 0; b < g.nb; ++b) hr[b] = to_rigid_dev<float>(rigid[b]);
     ALB_CUDA(cudaMemcpyAsync(dr, hr, sizeof(RigidDev<float>) * g.nb, cudaMemcpyHostToDevice, st));
   }
+  // with pellets, one grid over particles and pellets (pellets after the
+  // particles, as the reference stores them)
+  const float* grid_x = particle_x;
+  const uint32_t npts = num_particles + npel;
+  if (npel) {
+    float* all = nullptr;
+    ALB_TRY(engine->buf("all.x", size_t(npts) * 3, &all));
+    if (num_particles)
+      ALB_CUDA(cudaMemcpyAsync(all, particle_x, sizeof(float) * 3 * num_particles,
+                               cudaMemcpyDeviceToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(all + size_t(num_particles) * 3, req->pellet_x,
+                             sizeof(float) * 3 * npel, cudaMemcpyDeviceToDevice, st));
+    ALB_TRY(engine->buf("sorted.x", npts, &xs));
+    grid_x = all;
+  }
   GridState gs;
   ALB_LAUNCH(engine, "sample_grid", 7, st,
-             ALB_TRY(grid_build<float>(engine, c, g, particle_x, num_particles, xs, flags, gs,
-                                       st)));
+             ALB_TRY(grid_build<float>(engine, c, g, grid_x, npts, xs, flags, gs, st)));
   SampleDev sd{req->sample_x,
                req->num_samples,
                req->sample_quantity ? req->quantity_dim : 0u,
@@ -348,7 +391,10 @@ int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_cons
                req->wrap_y ? 1u : 0u,
                req->wrap_length,
                req->wrap_length * -0.5f,
-               req->wrap_length * 0.5f};
+               req->wrap_length * 0.5f,
+               num_particles,
+               npel,
+               req->pellet_v};
   const uint32_t blocks = blocks_for(req->num_samples, kBlock);
   GridDims g1 = g;
   if (!body_terms) g1.nb = 0;  // the first pass reads no body arrays

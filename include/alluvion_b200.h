@@ -502,7 +502,7 @@ typedef struct al_pellets_f32 {
   uint32_t count[AL_MAX_BOUNDARIES]; /* pellets of each body, in body order */
   float* x;              /* device [num_pellets][3] out or NULL: world positions */
   float* pressure;       /* device [num_pellets] out or NULL: extrapolated pressure */
-  uint32_t reserved[2];
+  float* v;              /* device [num_pellets][3] out or NULL: pellet velocities */
 } al_pellets_f32;
 
 typedef struct al_pellets_f64 {
@@ -511,7 +511,7 @@ typedef struct al_pellets_f64 {
   uint32_t count[AL_MAX_BOUNDARIES];
   double* x;
   double* pressure;
-  uint32_t reserved[2];
+  double* v;
 } al_pellets_f64;
 
 AL_API int al_i_step_pellets_f32(al_engine* engine, const al_const_f32* cn,
@@ -711,7 +711,15 @@ typedef struct al_sample_f32 {
    * [-wrap_length/2, wrap_length/2) (wrap_y, runner.hpp:698-707) */
   uint32_t wrap_y;
   float wrap_length;                   /* Const::wrap_length (constants.hpp:130-136) */
-  uint32_t reserved[2];
+  /* pellet boundary model (the *_with_pellets sampling kernels,
+   * runner.hpp:2122-2147, 4242-4275, 4325-4357): pellets join the grid after
+   * the particles; position density becomes m (sum_particles W + sum_pellets W),
+   * velocity adds V W v_p, vorticity V (v_p - v_s) x grad W, and no
+   * volume-map body terms are added */
+  const float* pellet_x;               /* [num_pellets][3] world positions */
+  const float* pellet_v;               /* [num_pellets][3], for velocity / vorticity */
+  uint32_t num_pellets;
+  uint32_t reserved;
 } al_sample_f32;
 
 AL_API int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,

@@ -229,7 +229,7 @@ def mesh_distance_grid(body, vertices, faces, offset=0.0):
 def sample_fluid(cn, cni, particle_x, rigid, sample_x, particle_density=None, particle_v=None,
                  particle_quantity=None, sample_boundary=None, sample_boundary_kernel=None,
                  outputs=("density", "position_density", "quantity", "v", "vorticity"),
-                 wrap_length=None):
+                 wrap_length=None, pellet_x=None, pellet_v=None):
     """sample_fluid / sample_fluid_density / sample_position_density /
     compute_sample_velocity / compute_sample_vorticity restated on host
     float32 arrays; wrap_length: periodic in y (make_neighbor_list<1>).
@@ -253,6 +253,11 @@ def sample_fluid(cn, cni, particle_x, rigid, sample_x, particle_density=None, pa
     if wrap_length is not None:
         req.wrap_y = 1
         req.wrap_length = float(wrap_length)
+    pxh, pvh = f32(pellet_x), f32(pellet_v)
+    if pxh is not None and len(pxh):
+        req.pellet_x = pxh.ctypes.data
+        req.pellet_v = pvh.ctypes.data if pvh is not None else None
+        req.num_pellets = len(pxh)
     for name, arr in (("particle_density", rho), ("particle_v", pv), ("particle_quantity", pq),
                       ("sample_boundary", sb), ("sample_boundary_kernel", sbk)):
         setattr(req, name, None if arr is None else arr.ctypes.data)

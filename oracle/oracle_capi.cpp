@@ -590,7 +590,7 @@ int orc_sample_fluid_f32(const al_const_f32* cn, const al_consti* cni, const flo
   std::vector<V3<float>> sx(req->num_samples);
   for (uint32_t i = 0; i < req->num_samples; ++i) sx[i] = v3<float>(req->sample_x + 3 * size_t(i));
   std::vector<Body<float>> bodies;
-  for (uint32_t b = 0; b < cni->num_boundaries; ++b) {
+  for (uint32_t b = 0; rigid && b < cni->num_boundaries; ++b) {
     Body<float> o{};
     o.x = v3<float>(rigid[b].x);
     o.v = v3<float>(rigid[b].v);
@@ -614,6 +614,9 @@ int orc_sample_fluid_f32(const al_const_f32* cn, const al_consti* cni, const flo
   r.vort = reinterpret_cast<V3<float>*>(req->sample_vorticity);
   r.wrap = req->wrap_y != 0;
   r.wrap_length = req->wrap_length;
+  r.pel_x = reinterpret_cast<const V3<float>*>(req->pellet_x);
+  r.pel_v = reinterpret_cast<const V3<float>*>(req->pellet_v);
+  r.npel = req->num_pellets;
   return sample_fluid(c, *cni, px.data(), n, bodies, r) ? 1 : 0;
 }
 

@@ -2037,12 +2037,20 @@ struct SampleRequest {
   // and displacements wrap into [-L/2, L/2) (wrap_y, runner.hpp:698-707)
   bool wrap = false;
   TF wrap_length = 0;
+  // pellet boundary model (*_with_pellets, runner.hpp:2122-2147,
+  // 4242-4275, 4325-4357): pellets join the grid after the particles
+  const V3<TF>* pel_x = nullptr;
+  const V3<TF>* pel_v = nullptr;
+  uint32_t npel = 0;
 };
 
 template <class TF>
-bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px, uint32_t n,
+bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px_in, uint32_t n,
                   const std::vector<Body<TF>>& bodies, const SampleRequest<TF>& r) {
-  const GridSort s = grid_sort(c, g, px, n);
+  std::vector<V3<TF>> all(px_in, px_in + n);
+  for (uint32_t k = 0; k < r.npel; ++k) all.push_back(r.pel_x[k]);
+  const V3<TF>* px = all.data();
+  const GridSort s = grid_sort(c, g, px, n + r.npel);
   const uint32_t cap = g.max_num_neighbors_per_particle;
   const uint32_t nb = uint32_t(bodies.size());
   bool overflow = false;
@@ -2052,10 +2060,10 @@ bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px, uint32_
     const V3<TF> xi = r.sx[i];
     int p[3];
     cell_coords(c, g, xi, p);
-    std::vector<uint32_t> nbr;
-    std::vector<V3<TF>> disp;  // x_s - x_j, wrapped
+    std::vector<uint32_t> nbr, pnbr;
+    std::vector<V3<TF>> disp, pdisp;  // x_s - x_j, wrapped
     const TF wmin = r.wrap_length * TF(-0.5), wmax = r.wrap_length * TF(0.5);
-    uint32_t found = 0;
+    uint32_t found = 0, pfound = 0;
     for (int dx = -1; dx <= 1; ++dx)
       for (int dy = -1; dy <= 1; ++dy)
         for (int dz = -1; dz <= 1; ++dz) {
@@ -2078,31 +2086,45 @@ bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px, uint32_
               else if (d.y < wmin)
                 d.y += r.wrap_length;
             }
-            if ((d.x * d.x + d.y * d.y) + d.z * d.z < c.h2) {
-              if (found < cap) {
-                nbr.push_back(j);
-                disp.push_back(d);
+            if (!((d.x * d.x + d.y * d.y) + d.z * d.z < c.h2)) continue;
+            if (j >= n) {
+              if (pfound < cap) {
+                pnbr.push_back(j - n);
+                pdisp.push_back(d);
               }
-              ++found;
+              ++pfound;
+              continue;
             }
+            if (found < cap) {
+              nbr.push_back(j);
+              disp.push_back(d);
+            }
+            ++found;
           }
         }
-    if (found > cap) overflow = true;
-    TF dens = 0, qs[3] = {0, 0, 0};
+    if (found > cap || pfound > cap) overflow = true;
+    TF dens = 0, qs[3] = {0, 0, 0}, wb = 0, wp = 0;
     V3<TF> vel{0, 0, 0};
     for (size_t k = 0; k < nbr.size(); ++k) {
       const uint32_t j = nbr[k];
       const V3<TF> d = disp[k];
       const TF w = W_r2(c, (d.x * d.x + d.y * d.y) + d.z * d.z);
       dens += c.vol * w;
+      wb += w;
       if (r.quantity) {
         const TF mr = c.mass / r.rho[j];
         for (uint32_t k = 0; k < r.qdim; ++k) qs[k] += mr * w * r.q[size_t(j) * r.qdim + k];
       }
       if (r.vel) vel += (c.mass / r.rho[j] * w) * r.v[j];
     }
+    for (size_t k = 0; k < pnbr.size(); ++k) {
+      const V3<TF> d = pdisp[k];
+      const TF w = W_r2(c, (d.x * d.x + d.y * d.y) + d.z * d.z);
+      wp += w;
+      if (r.vel) vel += (c.vol * w) * r.pel_v[pnbr[k]];
+    }
     TF bw = 0;
-    for (uint32_t b = 0; r.bk && b < nb; ++b) {
+    for (uint32_t b = 0; r.npel == 0 && r.bk && b < nb; ++b) {
       const V4<TF> bx = r.bnd ? r.bnd[size_t(b) * r.num + i] : V4<TF>{0, 0, 0, 0};
       const V4<TF> bk = r.bk[size_t(b) * r.num + i];
       bw += bk.w;
@@ -2113,7 +2135,8 @@ bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px, uint32_
       }
     }
     if (r.density) r.density[i] = dens * c.rho0;
-    if (r.position_density) r.position_density[i] = (dens + bw) * c.rho0;
+    if (r.position_density)
+      r.position_density[i] = r.npel ? (wb + wp) * c.mass : (dens + bw) * c.rho0;
     if (r.quantity)
       for (uint32_t k = 0; k < r.qdim; ++k) r.quantity[size_t(i) * r.qdim + k] = qs[k];
     if (r.vel) r.vel[i] = vel;
@@ -2121,7 +2144,9 @@ bool sample_fluid(const Cn<TF>& c, const al_consti& g, const V3<TF>* px, uint32_
       V3<TF> w{0, 0, 0};
       for (size_t k = 0; k < nbr.size(); ++k)
         w += (c.mass / r.rho[nbr[k]]) * cross(r.v[nbr[k]] - vel, gradW(c, disp[k]));
-      for (uint32_t b = 0; b < nb; ++b) {
+      for (size_t k = 0; k < pnbr.size(); ++k)
+        w += c.vol * cross(r.pel_v[pnbr[k]] - vel, gradW(c, pdisp[k]));
+      for (uint32_t b = 0; r.npel == 0 && b < nb; ++b) {
         const V4<TF> bx = r.bnd[size_t(b) * r.num + i];
         const V4<TF> bk = r.bk[size_t(b) * r.num + i];
         const V3<TF> vb =

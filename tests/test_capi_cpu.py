@@ -52,3 +52,42 @@ def test_null_arguments_rejected():
     lib = _capi.lib()
     assert lib.al_grid_sort_f32(None, None, None, None, 0, None, None, None, None, None) == 2
     assert lib.al_engine_create(0, None) == 2
+
+
+# ctypes mirror -> C typedef of include/alluvion_b200.h
+ABI_STRUCTS = {
+    "ConstF32": "al_const_f32", "ConstF64": "al_const_f64", "ConstI": "al_consti",
+    "BodyF32": "al_body_f32", "BodyF64": "al_body_f64", "RigidF32": "al_rigid_f32",
+    "RigidF64": "al_rigid_f64", "SolverParams": "al_solver_params",
+    "StepReport": "al_step_report", "Fluid": "al_fluid_f32", "WarmNet": "al_warm_net",
+    "WarmStart": "al_warm_start", "SceneF32": "al_scene_f32",
+    "ContactBodyF32": "al_contact_body_f32", "ContactF32": "al_contact_f32",
+    "SampleF32": "al_sample_f32", "PelletsF32": "al_pellets_f32",
+    "PelletsF64": "al_pellets_f64",
+}
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Every ctypes mirror has the C struct's size and field offsets (gcc
+    compiles a probe of sizeof / offsetof from the header)."""
+    import subprocess
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "alluvion_b200.h"',
+             'int main(void) {']
+    for py, c in ABI_STRUCTS.items():
+        cls = getattr(_capi, py)
+        lines.append('  printf("%s size %%zu\\n", sizeof(%s));' % (py, c))
+        for name, _ in cls._fields_:
+            lines.append('  printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (py, name, c, name))
+    lines += ['  return 0;', '}']
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = dict(line.rsplit(" ", 1) for line in out.strip().splitlines())
+    for py in ABI_STRUCTS:
+        cls = getattr(_capi, py)
+        assert int(got["%s size" % py]) == ctypes.sizeof(cls), py
+        for name, _ in cls._fields_:
+            assert int(got["%s.%s" % (py, name)]) == getattr(cls, name).offset, (py, name)

@@ -93,6 +93,7 @@ def _device_run(engine, dtype, cn, cni, x, barr, rarr, local, counts, sp, dt, st
                              particle_pressure=P, particle_density_adv=ADV)
     L = torch.from_numpy(np.ascontiguousarray(local)).cuda()
     PX = torch.zeros(len(local), 3, dtype=td, device="cuda")
+    PV = torch.zeros(len(local), 3, dtype=td, device="cuda")
     PP = torch.zeros(len(local), dtype=td, device="cuda")
     pel = (_capi.PelletsF32 if dtype == np.float32 else _capi.PelletsF64)()
     pel.local_x = L.data_ptr()
@@ -100,6 +101,7 @@ def _device_run(engine, dtype, cn, cni, x, barr, rarr, local, counts, sp, dt, st
     for b, c in enumerate(counts):
         pel.count[b] = c
     pel.x = PX.data_ptr()
+    pel.v = PV.data_ptr()
     pel.pressure = PP.data_ptr()
     fn = getattr(_capi.lib(), "al_i_step_pellets_" + _capi.suffix(dtype))
     real = _capi.real_types(dtype)[3]
@@ -113,6 +115,7 @@ def _device_run(engine, dtype, cn, cni, x, barr, rarr, local, counts, sp, dt, st
         reps.append(rep)
     g = lambda t: t.cpu().numpy()
     return dict(x=g(X), v=g(V), density=g(RHO), pressure=g(P), a=g(A), px=g(PX), pp=g(PP),
+                pv=g(PV),
                 dt=float(dt_c.value), reps=reps,
                 rigid=scenes.rigid_array(dtype, [rarr[b] for b in range(len(rarr))]))
 
@@ -229,3 +232,50 @@ def test_pellet_step_errors(engine):
     with pytest.raises(_capi.EngineError):
         _device_run(engine, dtype, cn, cni, x, barr, rarr, local, bad, scenes.solver_params(),
                     1e-4, 1)
+
+
+def test_sampling_with_pellets(engine):
+    """sample_position_density / compute_sample_velocity / _vorticity
+    _with_pellets: samples see the pellets (world positions and velocities
+    from a pellet step) as in the reference's *_with_pellets kernels."""
+    dtype = np.float32
+    cn, cni, x, barr, rarr, local, counts = _scene(dtype)
+    got = _device_run(engine, dtype, cn, cni, x, barr, rarr, local, counts,
+                      scenes.solver_params(), 1e-4, 1)
+    r = float(cn.particle_radius)
+    g = np.linspace(-5 * r, 35 * r, 21)
+    sx = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3).astype(dtype)
+    s = len(sx)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    X, RHO, V, SX = dev(got["x"]), dev(got["density"]), dev(got["v"]), dev(sx)
+    PX, PV = dev(got["px"]), dev(got["pv"])
+    outs = {k: torch.zeros((s, 3) if k in ("v", "vorticity") else (s,), device="cuda")
+            for k in ("density", "position_density", "v", "vorticity")}
+    req = _capi.SampleF32()
+    req.sample_x = SX.data_ptr()
+    req.num_samples = s
+    req.particle_density = RHO.data_ptr()
+    req.particle_v = V.data_ptr()
+    req.sample_density = outs["density"].data_ptr()
+    req.sample_position_density = outs["position_density"].data_ptr()
+    req.sample_v = outs["v"].data_ptr()
+    req.sample_vorticity = outs["vorticity"].data_ptr()
+    req.pellet_x = PX.data_ptr()
+    req.pellet_v = PV.data_ptr()
+    req.num_pellets = len(local)
+    _capi.check(_capi.lib().al_sample_fluid_f32(engine.handle, _capi.ptr(cn), _capi.ptr(cni),
+                                                X.data_ptr(), len(x), None, _capi.ptr(req),
+                                                None), "sample with pellets")
+    ref, overflow = orc.sample_fluid(cn, cni, got["x"], None, sx, got["density"], got["v"],
+                                     outputs=("density", "position_density", "v", "vorticity"),
+                                     pellet_x=got["px"], pellet_v=got["pv"])
+    assert not overflow
+    for k in ("density", "position_density", "v"):
+        _close(outs[k].cpu().numpy(), ref[k], 1e-5, k)
+    _close(outs["vorticity"].cpu().numpy(), ref["vorticity"], 1e-4, "vorticity")
+    # the pellets count: samples in the container walls have position density
+    pd = outs["position_density"].cpu().numpy()
+    in_wall = np.any(sx < -4 * r, axis=1)  # more than h from every particle
+    assert pd[in_wall].max() > 0 and outs["density"].cpu().numpy()[in_wall].max() == 0
+    # a moving pellet sphere gives samples near it the sphere's velocity
+    assert np.abs(ref["v"]).max() > 0
