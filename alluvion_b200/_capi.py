@@ -26,6 +26,7 @@ AL_ERR_NEIGHBOR_OVERFLOW = 5
 ANOMALY_STATUSES = (AL_ERR_OUT_OF_GRID, AL_ERR_CELL_OVERFLOW, AL_ERR_NEIGHBOR_OVERFLOW)
 
 SHAPE_BOX, SHAPE_SPHERE, SHAPE_BOX_SHELL, SHAPE_TORUS, SHAPE_MESH = 0, 1, 2, 3, 4
+SHAPE_CYLINDER, SHAPE_CAPSULE, SHAPE_INFINITE_CYLINDER, SHAPE_INFINITE_TUBE = 5, 6, 7, 8
 
 
 def _const_struct(name, real):
@@ -95,7 +96,8 @@ class SolverParams(ctypes.Structure):
                 ("min_dt", ctypes.c_double),
                 ("pile_gravity", ctypes.c_double * 3),
                 ("integrate_rigids", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("wrap_y", ctypes.c_uint32),
+                ("wrap_length", ctypes.c_double)]
 
 
 WARM_NUM_FEATURES, WARM_HIDDEN, WARM_NUM_OUTPUTS, WARM_NUM_PARAMS = 12, 64, 2, 5122

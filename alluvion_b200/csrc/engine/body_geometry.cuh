@@ -11,6 +11,10 @@ namespace alb {
 namespace {
 
 // ------------------------------------------------------------- geometry
+__host__ __device__ __forceinline__ bool shape_is_y_invariant(uint32_t shape) {
+  return shape == AL_SHAPE_INFINITE_CYLINDER || shape == AL_SHAPE_INFINITE_TUBE;
+}
+
 template <class TF>
 __device__ __forceinline__ vec3<TF> rotate(vec3<TF> v, vec4<TF> q) {
   vec3<TF> r;
@@ -31,11 +35,30 @@ __device__ __forceinline__ TF box_sdf(vec3<TF> x, TF hx, TF hy, TF hz, TF outset
 }
 
 // Analytic signed distances (dg/box_distance.hpp:23-30,
-// dg/sphere_distance.hpp:18-20, dg/box_shell_distance.hpp:36-47) and the
-// torus |(|x_xz| - R, y)| - r.
+// dg/sphere_distance.hpp:18-20, dg/box_shell_distance.hpp:36-47,
+// dg/cylinder_distance.hpp:28-35, dg/capsule_distance.hpp:24-27,
+// dg/infinite_cylinder_distance.hpp:20-22, dg/infinite_tube_distance.hpp:32-36)
+// and the torus |(|x_xz| - R, y)| - r.
 template <class TF>
 __device__ __forceinline__ TF shape_sdf(const BodyDev<TF>& b, vec3<TF> x) {
   switch (b.shape) {
+    case AL_SHAPE_CYLINDER: {
+      const TF d0 = sqrt(x.x * x.x + x.z * x.z) - b.p[0];
+      const TF d1 = fabs(x.y + b.p[2]) - b.p[1] * TF(0.5);
+      const TF c0 = fmax(d0, TF(0)), c1 = fmax(d1, TF(0));
+      return fmin(fmax(d0, d1), TF(0)) + sqrt(c0 * c0 + c1 * c1);
+    }
+    case AL_SHAPE_CAPSULE: {
+      const TF hh = b.p[1] * TF(0.5);
+      const vec3<TF> m{x.x, x.y - fmax(-hh, fmin(x.y, hh)), x.z};
+      return sqrt(length_sqr(m)) - b.p[0];
+    }
+    case AL_SHAPE_INFINITE_CYLINDER:
+      return sqrt(x.x * x.x + x.z * x.z) - b.p[0];
+    case AL_SHAPE_INFINITE_TUBE: {
+      const TF rd = sqrt(x.x * x.x + x.z * x.z);
+      return fmax(b.p[0] - rd, rd - b.p[1]);
+    }
     case AL_SHAPE_BOX:
       return box_sdf(x, b.p[0], b.p[1], b.p[2], b.p[3]);
     case AL_SHAPE_SPHERE:
@@ -53,11 +76,20 @@ __device__ __forceinline__ TF shape_sdf(const BodyDev<TF>& b, vec3<TF> x) {
 }
 
 // Un-normalised outward direction: the position for a sphere
-// (sphere_distance.hpp:21), central differences with step h/256 otherwise
-// (box_distance.hpp:28-38).
+// (sphere_distance.hpp:21), the radial direction for the y-invariant shapes,
+// central differences with step h/256 otherwise (box_distance.hpp:28-38).
 template <class TF>
 __device__ __forceinline__ vec3<TF> shape_gradient(const BodyDev<TF>& b, vec3<TF> x, TF h) {
   if (b.shape == AL_SHAPE_SPHERE) return x;
+  // the y-invariant shapes return the radial direction
+  // (dg/infinite_cylinder_distance.hpp:23-25, dg/infinite_tube_distance.hpp:37-43)
+  if (b.shape == AL_SHAPE_INFINITE_CYLINDER) return vec3<TF>{x.x, TF(0), x.z};
+  if (b.shape == AL_SHAPE_INFINITE_TUBE) {
+    const TF s = (x.x * x.x + x.z * x.z) * TF(4) > (b.p[0] + b.p[1]) * (b.p[0] + b.p[1])
+                     ? TF(1)
+                     : TF(-1);
+    return vec3<TF>{s * x.x, TF(0), s * x.z};
+  }
   const TF s = h * TF(0.00390625);
   return vec3<TF>{shape_sdf(b, vec3<TF>{x.x + s, x.y, x.z}) - shape_sdf(b, vec3<TF>{x.x - s, x.y, x.z}),
                   shape_sdf(b, vec3<TF>{x.x, x.y + s, x.z}) - shape_sdf(b, vec3<TF>{x.x, x.y - s, x.z}),

@@ -46,7 +46,10 @@ __device__ __forceinline__ void sample_body(const Cn<TF>& c, const BodyDev<TF>& 
                                             const RigidDev<TF>& r, vec3<TF> x, vec4<TF>& bnd,
                                             vec4<TF>& bk) {
   const vec4<TF> qc{-r.q.x, -r.q.y, -r.q.z, r.q.w};
-  const vec3<TF> local = rotate(x - r.x, qc);
+  vec3<TF> local = rotate(x - r.x, qc);
+  // compute_volume_and_boundary_x_analytic<1> for the y-invariant shapes
+  // (runner.hpp:1744-1746)
+  if (shape_is_y_invariant(b.shape)) local.y = TF(0);
   vec3<TF> bx = x, xi_bxj{0, 0, 0};
   TF d = 0, vol = 0;
   int ip[3];

@@ -71,9 +71,12 @@ RigidDev<TF> to_rigid_dev(const R& r) {
 
 template <class TF>
 inline int validate_body(const BodyDev<TF>& b, bool need_dist, bool need_vol) {
-  ALB_CHECK_ARG(b.shape <= AL_SHAPE_MESH, "body: unknown shape");
+  ALB_CHECK_ARG(b.shape <= AL_SHAPE_INFINITE_TUBE, "body: unknown shape");
   ALB_CHECK_ARG(b.shape != AL_SHAPE_MESH || b.use_grid,
                 "body: a mesh body needs its distance grid (use_distance_grid = 1)");
+  ALB_CHECK_ARG(!(b.shape == AL_SHAPE_INFINITE_CYLINDER || b.shape == AL_SHAPE_INFINITE_TUBE) ||
+                    !b.use_grid,
+                "body: y-invariant shapes are sampled analytically (use_distance_grid = 0)");
   ALB_CHECK_ARG(b.res[0] > 0 && b.res[1] > 0 && b.res[2] > 0, "body: zero resolution");
   uint64_t nx = b.res[0], ny = b.res[1], nz = b.res[2];
   uint64_t nn = (nx + 1) * (ny + 1) * (nz + 1) +

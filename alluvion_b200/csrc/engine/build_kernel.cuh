@@ -64,12 +64,18 @@ __global__ void __launch_bounds__(kBlock)
       const int cx = ip[0] + dx;
       if (cx < 0 || cx >= int(g.res[0])) continue;
       for (int dy = -1; dy <= 1; ++dy) {
-        const int cy = ip[1] + dy;
+        int cy = ip[1] + dy;
+        if (c.wrap) {  // wrap_ipos_y (runner.hpp:689-697)
+          if (cy >= int(g.res[1]))
+            cy -= int(g.res[1]);
+          else if (cy < 0)
+            cy += int(g.res[1]);
+        }
         if (cy < 0 || cy >= int(g.res[1])) continue;
         const uint32_t b = cell_start[cell_linear(g, cx, cy, z0)];
         const uint32_t e = cell_start[cell_linear(g, cx, cy, z1) + 1];
         for (uint32_t t = b; t < e; ++t) {
-          const TF d2 = dist2_rn(xi, xyz(__ldg(xs + t)));
+          const TF d2 = pdist2(c, xi, xyz(__ldg(xs + t)));
           if (d2 < c.h2 && t != s) {
             if (cnt < g.cap_nbr) nbr[size_t(cnt) * n + s] = t;
             ++cnt;
@@ -104,9 +110,9 @@ __global__ void __launch_bounds__(kBlock)
 #pragma unroll
     for (uint32_t q = 0; q < kB; ++q) {
       if (k0 + q >= cnt) break;
-      density += c.vol * W_r2(c, dist2_rn(xi, xj[q]));
+      density += c.vol * W_r2(c, pdist2(c, xi, xj[q]));
       if (FACTOR || EX::kOn) {
-        const vec3<TF> d{sub_rn(xi.x, xj[q].x), sub_rn(xi.y, xj[q].y), sub_rn(xi.z, xj[q].z)};
+        const vec3<TF> d = pdisp(c, xi, xj[q]);
         const vec3<TF> gw = gradW(c, d);
         if (FACTOR) {
           const vec3<TF> gpj = (-c.vol) * gw;

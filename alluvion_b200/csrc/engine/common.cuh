@@ -152,7 +152,44 @@ struct Cn {
   TF h, h2, k, l, w0, radius, vol, mass, rho0, visc, bvisc, eps;
   vec3<TF> g;
   TF inv_h, inv_h2;  // 1 / h and 1 / h^2, rounded once on the host
+  // periodic in y (the solvers' step<1>): Const::wrap_length and its
+  // half-range bounds (constants.hpp:130-136); wrap = 0 otherwise
+  TF wrap_len = 0, wrap_min = 0, wrap_max = 0;
+  int wrap = 0;
 };
+
+// Sets the periodic-y fields as Const::set_wrap_length does.
+template <class TF>
+inline void set_wrap(Cn<TF>& c, TF length) {
+  c.wrap = 1;
+  c.wrap_len = length;
+  c.wrap_min = length * TF(-0.5);
+  c.wrap_max = length * TF(0.5);
+}
+
+// wrap_y (runner.hpp:698-707) of a displacement's or position's y.
+template <class TF>
+__device__ __forceinline__ TF wrap_y(const Cn<TF>& c, TF y) {
+  if (!c.wrap) return y;
+  if (y >= c.wrap_max) return sub_rn(y, c.wrap_len);
+  if (y < c.wrap_min) return add_rn(y, c.wrap_len);
+  return y;
+}
+
+// x_i - x_j with each difference rounded on its own, y wrapped when the
+// step is periodic: the displacement make_neighbor_list<wrap> stores
+// (runner.hpp:1893-1894).
+template <class TF>
+__device__ __forceinline__ vec3<TF> pdisp(const Cn<TF>& c, vec3<TF> a, vec3<TF> b) {
+  return vec3<TF>{sub_rn(a.x, b.x), wrap_y(c, sub_rn(a.y, b.y)), sub_rn(a.z, b.z)};
+}
+// |pdisp|^2 as ((dx*dx + dy*dy) + dz*dz), every operation rounded.
+template <class TF>
+__device__ __forceinline__ TF pdist2(const Cn<TF>& c, vec3<TF> a, vec3<TF> b) {
+  const vec3<TF> d = pdisp(c, a, b);
+  return add_rn(add_rn(mul_rn(d.x, d.x), mul_rn(d.y, d.y)), mul_rn(d.z, d.z));
+}
+
 
 template <class TF, class C>
 inline Cn<TF> to_cn(const C& c) {

@@ -573,6 +573,10 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
                 "al_i_step_pellets: particle_x / particle_v / particle_pressure are null");
   ALB_CHECK_ARG(np == 0 || pel->local_x, "al_i_step_pellets: pellet local_x is null");
   ALB_CHECK_ARG(np == 0 || nb > 0, "al_i_step_pellets: pellets need bodies");
+  if (sp->wrap_y) {
+    set_error("al_i_step_pellets: periodic (wrap_y) steps are not supported on the pellet branch");
+    return AL_ERR_UNSUPPORTED;
+  }
   ALB_CHECK_ARG(uint64_t(n) + np < (1ull << 31), "al_i_step_pellets: too many points");
   BodyOffsets off{};
   uint64_t acc = 0;
@@ -583,7 +587,7 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
   off.start[nb] = uint32_t(acc);
   ALB_CHECK_ARG(acc == np, "al_i_step_pellets: pellet counts do not add up to num_pellets");
   for (uint32_t b = 0; b < nb; ++b)
-    ALB_CHECK_ARG(bodies[b].shape <= AL_SHAPE_MESH, "al_i_step_pellets: unknown body shape");
+    ALB_CHECK_ARG(bodies[b].shape <= AL_SHAPE_INFINITE_TUBE, "al_i_step_pellets: unknown body shape");
   ALB_TRY(e->activate());
   e->ns.clear();
   struct NsReset {

@@ -174,7 +174,7 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
                                                   uint32_t cnt) {
   TF acc = 0;
   for_each_neighbor<2, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
-    const vec3<TF> d = xi - xyz(xj);
+    const vec3<TF> d = pdisp(c, xi, xyz(xj));
     acc += c.vol * dot(vi - xyz(vj), gradW(c, d));
   });
   acc = group_sum(acc);
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
     const TF ksum = ki + xj.w;
     if (fabs(ksum) > c.eps) {
-      const vec3<TF> gw = gradW(c, xi - xyz(xj));
+      const vec3<TF> gw = gradW(c, pdisp(c, xi, xyz(xj)));
       if (kDiv) {
         const vec3<TF> gpj = (-c.vol) * gw;
         dv -= (dt * ksum) * gpj;
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kBlock)
     cnt = S.ncount[L.s];
   }
   for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
-    const vec3<TF> d = xi - xyz(xj);  // vj = {v, rho}
+    const vec3<TF> d = pdisp(c, xi, xyz(xj));  // vj = {v, rho}
     da += (c.visc * c.mass / vj.w * dot(d, gradW(c, d)) /
            (length_sqr(d) + TF(0.01) * c.h2)) *
           (vi - xyz(vj));
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(kBlock)
 // pressure_solve_finish + integrate_velocity<0> (runner.hpp:3606-3623),
 // written straight back to the caller's buffers in original order.
 template <class TF>
-__global__ void k_df_finish(StepState<TF> S, int density_solve, TF* __restrict__ x_ref,
+__global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __restrict__ x_ref,
                             TF* __restrict__ v_ref, TF* __restrict__ a_ref,
                             TF* __restrict__ rho_ref, TF* __restrict__ alpha_ref,
                             TF* __restrict__ kappa_ref, TF* __restrict__ kappa_v_ref,
@@ -570,7 +570,9 @@ __global__ void k_df_finish(StepState<TF> S, int density_solve, TF* __restrict__
   const TF dt = S.ctrl->dt;
   const vec3<TF> v = xyz(RV(S, s));
   const vec3<TF> x = xyz(RX(S, s));
-  st3(x_ref, i, x + dt * v);
+  vec3<TF> xn = x + dt * v;
+  xn.y = wrap_y(c, xn.y);  // integrate_velocity<1> (runner.hpp:3619-3620)
+  st3(x_ref, i, xn);
   st3(v_ref, i, v);
   if (a_ref) st3(a_ref, i, xyz(S.a[s]));
   if (rho_ref) rho_ref[i] = S.rho[s];
@@ -599,7 +601,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
   }
   vec3<TF> dii{0, 0, 0};
   for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
-    dii -= (c.vol / rho2) * gradW(c, xi - xyz(xj));
+    dii -= (c.vol / rho2) * gradW(c, pdisp(c, xi, xyz(xj)));
   });
   dii = group_sum(dii);
   if (!L.lead()) return;
@@ -637,7 +639,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
   const TF rho2 = rho * rho, inv_rho2 = TF(1) / rho2, dpi = c.vol * inv_rho2;
   TF adv = 0, aii = 0;
   for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
-    const vec3<TF> gw = gradW(c, xi - xyz(xj));
+    const vec3<TF> gw = gradW(c, pdisp(c, xi, xyz(xj)));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
     adv += dt * c.vol * dot(vi - xyz(vj), gw);
     aii += c.vol * dot(dii - dji, gw);
@@ -678,7 +680,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
   vec3<TF> acc{0, 0, 0};
   for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
     const TF rj = vj.w, rj2 = rj * rj;
-    acc -= (c.vol / rj2 * xj.w) * gradW(c, xi - xyz(xj));
+    acc -= (c.vol / rj2 * xj.w) * gradW(c, pdisp(c, xi, xyz(xj)));
   });
   acc = group_sum(acc);
   if (!L.lead()) return;
@@ -707,7 +709,7 @@ __global__ void __launch_bounds__(kBlock)
   const TF rho2 = rho * rho, dpi = c.vol / rho2;
   TF sum = 0;
   for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t t, const vec4<TF>& xj, const vec4<TF>&) {
-    const vec3<TF> gw = gradW(c, xi - xyz(xj));
+    const vec3<TF> gw = gradW(c, pdisp(c, xi, xyz(xj)));
     const vec3<TF> dji = (dpi * c.rho0) * gw;
     const vec3<TF> dji_pi = dji * lp;
     sum += c.vol *
@@ -759,7 +761,7 @@ __global__ void __launch_bounds__(kBlock)
   for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t t, const vec4<TF>& xj, const vec4<TF>& vj) {
     const TF rj = vj.w;
     const TF dpj = __ldg(S.kappa + t) / (rj * rj);
-    ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - xyz(xj));
+    ai -= (c.mass * (dpi + dpj)) * gradW(c, pdisp(c, xi, xyz(xj)));
   });
   ai = group_sum(ai);
   const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
@@ -781,7 +783,9 @@ __global__ void __launch_bounds__(kBlock)
   const vec3<TF> ap = c.rho0 * ai;
   const vec3<TF> v = xyz(RV(S, L.s)) + ap * dt;
   const uint32_t i = S.perm[L.s];
-  st3(x_ref, i, xi + v * dt);
+  vec3<TF> xn = xi + v * dt;
+  xn.y = wrap_y(c, xn.y);  // kinematic_integration<1> (runner.hpp:2881-2884)
+  st3(x_ref, i, xn);
   st3(v_ref, i, v);
   if (a_ref) st3(a_ref, i, xyz(S.a[L.s]));
   if (rho_ref) rho_ref[i] = S.rho[L.s];
@@ -821,7 +825,7 @@ __global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
   const TF eps = TF(0.01) * c.h2;
   TF adv = 0, diag = 0;
   for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>& vj) {
-    const vec3<TF> d = xi - xyz(xj);  // vj = {v, rho}
+    const vec3<TF> d = pdisp(c, xi, xyz(xj));  // vj = {v, rho}
     const vec3<TF> gw = gradW(c, d);
     const TF rj = vj.w;
     adv += dt * c.vol * dot(vi - xyz(vj), gw);
@@ -869,7 +873,7 @@ __global__ void __launch_bounds__(kBlock)
   const TF eps = TF(0.01) * c.h2;
   TF off = 0;
   for_each_neighbor<4, true>(S, L, cnt, [&](uint32_t t, const vec4<TF>& xj, const vec4<TF>& vj) {
-    const vec3<TF> d = xi - xyz(xj);
+    const vec3<TF> d = pdisp(c, xi, xyz(xj));
     const TF rj = vj.w;
     off -= c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
            __ldg(last + t);
@@ -1159,7 +1163,7 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
       }
       ALB_LAUNCH(e, "finish", 1, st,
                  k_df_finish<TF><<<blocks, kBlock, 0, st>>>(
-                     S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                     c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
                      f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
                      f->particle_kappa_v, f->particle_density_adv));
     } else if (P.isph) {
@@ -1261,6 +1265,8 @@ std::vector<uint64_t> step_key(const al_engine* e, const StepPlan<TF>& P,
   add(cn, sizeof(*cn));
   add(cni, sizeof(*cni));
   add(P.f, sizeof(*P.f));
+  k.push_back(uint64_t(P.c.wrap));  // baked into the captured kernels' parameters
+  add(&P.c.wrap_len, sizeof(P.c.wrap_len));
   k.push_back(uint64_t(P.learned));
   k.push_back(reinterpret_cast<uint64_t>(P.warm_feat_out));
   if (P.learned) add(&P.net, sizeof(P.net));
@@ -1301,6 +1307,10 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   P.div = !iisph && sp->enable_divergence_solve;
   P.den = iisph || sp->enable_density_solve;
   P.c = to_cn<TF>(*A.cn);
+  if (sp->wrap_y) {  // SolverDf / SolverIi / SolverI::step<1>
+    ALB_CHECK_ARG(sp->wrap_length > 0, "step: wrap_y needs a positive wrap_length");
+    set_wrap(P.c, TF(sp->wrap_length));
+  }
   P.g = to_dims(*A.cni);
   P.f = A.f;
   const uint32_t n = A.f->num_particles;

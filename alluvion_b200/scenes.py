@@ -104,7 +104,9 @@ def fluid_block(num, box_min, particle_radius, dtype=np.float32, jitter=0.1, see
 def shape_aabb(shape, params):
     """(aabb_min, aabb_max, max_distance) of an analytic shape in its frame
     (dg/box_distance.hpp:13-17, dg/sphere_distance.hpp:11-13,
-    dg/box_shell_distance.hpp:13-21; the torus is new)."""
+    dg/box_shell_distance.hpp:13-21 and the constructors of the cylinder,
+    capsule, infinite cylinder and infinite tube distances; the torus is new).
+    The infinite tube's optional third parameter is its box half length in y."""
     p = [float(v) for v in params]
     if shape == _capi.SHAPE_BOX:
         hw = np.array(p[:3])
@@ -121,6 +123,19 @@ def shape_aabb(shape, params):
         R, rr = p[0], p[1]
         e = np.array([R + rr, rr, R + rr])
         return -e, e, R + rr
+    if shape == _capi.SHAPE_CYLINDER:  # dg/cylinder_distance.hpp:13-22
+        rr, hh, com = p[0], 0.5 * p[1], p[2]
+        return (np.array([-rr, -hh - com, -rr]), np.array([rr, hh - com, rr]),
+                float(np.sqrt(rr * rr + (hh + abs(com)) ** 2)))
+    if shape == _capi.SHAPE_CAPSULE:  # dg/capsule_distance.hpp:13-19
+        rr, hh = p[0], 0.5 * p[1]
+        return np.array([-rr, -hh - rr, -rr]), np.array([rr, hh + rr, rr]), hh + rr
+    if shape == _capi.SHAPE_INFINITE_CYLINDER:  # finite box (infinite_cylinder_distance.hpp:13-16)
+        rr = p[0]
+        return np.full(3, -rr), np.full(3, rr), rr
+    if shape == _capi.SHAPE_INFINITE_TUBE:  # infinite_tube_distance.hpp:15-28
+        ro, half = p[1], (p[2] if len(p) > 2 and p[2] else p[1])
+        return (np.array([-ro, -half, -ro]), np.array([ro, half, ro]), max(half, ro))
     raise ValueError("unknown shape %r (mesh bodies pass aabb= to make_body)" % shape)
 
 

@@ -116,9 +116,21 @@ typedef enum al_shape {
   AL_SHAPE_SPHERE = 1,    /* shape_params: radius */
   AL_SHAPE_BOX_SHELL = 2, /* shape_params: inner half widths xyz, outer half widths xyz, outset */
   AL_SHAPE_TORUS = 3,     /* shape_params: major radius (x-z plane), minor radius */
-  AL_SHAPE_MESH = 4       /* triangle mesh: distance_nodes from al_build_mesh_distance_grid_f32
+  AL_SHAPE_MESH = 4,      /* triangle mesh: distance_nodes from al_build_mesh_distance_grid_f32
                              (MeshDistance, dg/mesh_distance.hpp); use_distance_grid must be 1 */
+  AL_SHAPE_CYLINDER = 5,  /* shape_params: radius, height, com_y (CylinderDistance,
+                             dg/cylinder_distance.hpp; axis y, centre at y = -com_y) */
+  AL_SHAPE_CAPSULE = 6,   /* shape_params: radius, height of the straight part (CapsuleDistance,
+                             dg/capsule_distance.hpp; axis y) */
+  AL_SHAPE_INFINITE_CYLINDER = 7, /* shape_params: radius (InfiniteCylinderDistance,
+                             dg/infinite_cylinder_distance.hpp; invariant along y) */
+  AL_SHAPE_INFINITE_TUBE = 8 /* shape_params: inner radius, outer radius (InfiniteTubeDistance,
+                             dg/infinite_tube_distance.hpp; invariant along y) */
 } al_shape;
+/* The y-invariant shapes are sampled as the reference's
+ * compute_volume_and_boundary_x_analytic<1> does (runner.hpp:1744-1746): the
+ * body-frame y of the particle is set to 0, so the volume map is read on its
+ * y = 0 slice; they need use_distance_grid = 0. */
 
 typedef struct al_body_f32 {
   uint32_t shape;
@@ -192,7 +204,13 @@ typedef struct al_solver_params {
   double min_dt;
   double pile_gravity[3];
   uint32_t integrate_rigids; /* 1: apply Pile::integrate_kinematics after the fluid step */
-  uint32_t reserved;
+  /* 1: periodic in y, the solvers' step<1> (SolverDf / SolverIi / SolverI
+   * step_wrap1): neighbor cells wrap in y (wrap_ipos_y, runner.hpp:689-697),
+   * displacements and integrated positions wrap into
+   * [-wrap_length/2, wrap_length/2) (wrap_y, runner.hpp:698-707).  The grid's
+   * y extent must be the period (grid_res[1] cells of size h). */
+  uint32_t wrap_y;
+  double wrap_length;        /* Const::wrap_length (constants.hpp:130-136) */
 } al_solver_params;
 
 /* What one step reports (the solvers' read-only report fields,

@@ -206,6 +206,10 @@ int run_impl(int method, const C* cn, const al_consti* cni, const B* bodies, TF*
     if (kappa_v) std::copy(kappa_v, kappa_v + n, f.kappa_v.begin());
   }
   f.resize(n, nb);
+  if (sp_in->wrap_y) {  // step<1>
+    f.wrap = true;
+    f.wrap_len = TF(sp_in->wrap_length);
+  }
   SolverParams sp;
   sp.density_change_tolerance = sp_in->density_change_tolerance;
   sp.density_error_tolerance = sp_in->density_error_tolerance;

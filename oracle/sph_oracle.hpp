@@ -201,6 +201,16 @@ GridSort grid_sort(const Cn<TF>& c, const al_consti& g, const V3<TF>* x, uint32_
   return s;
 }
 
+// wrap_y (runner.hpp:698-707) with the half-range bounds of
+// Const::set_wrap_length (constants.hpp:130-136).
+template <class TF>
+inline TF wrap_coord(bool wrap, TF len, TF y) {
+  if (!wrap) return y;
+  if (y >= len * TF(0.5)) return y - len;
+  if (y < len * TF(-0.5)) return y + len;
+  return y;
+}
+
 // Squared distance with a fixed operation order ((dx*dx + dy*dy) + dz*dz),
 // the order length_sqr uses in the reference.
 template <class TF>
@@ -222,7 +232,7 @@ struct NeighborList {
 // entries are kept and `overflow` is raised.
 template <class TF>
 NeighborList neighbor_list(const Cn<TF>& c, const al_consti& g, const V3<TF>* x, uint32_t n,
-                           const GridSort& s) {
+                           const GridSort& s, bool wrap = false, TF wrap_len = 0) {
   NeighborList nl;
   nl.cap = g.max_num_neighbors_per_particle;
   nl.count.assign(n, 0);
@@ -238,12 +248,20 @@ NeighborList neighbor_list(const Cn<TF>& c, const al_consti& g, const V3<TF>* x,
       for (int dy = -1; dy <= 1; ++dy)
         for (int dz = -1; dz <= 1; ++dz) {
           int q[3] = {p[0] + dx, p[1] + dy, p[2] + dz};
+          if (wrap) {  // wrap_ipos_y (runner.hpp:689-697)
+            if (q[1] >= int(g.grid_res[1]))
+              q[1] -= int(g.grid_res[1]);
+            else if (q[1] < 0)
+              q[1] += int(g.grid_res[1]);
+          }
           if (!in_grid(g, q)) continue;
           uint32_t cell = cell_linear(g, q);
           for (uint32_t t = s.cell_start[cell]; t < s.cell_start[cell + 1]; ++t) {
             uint32_t j = s.sorted[t];
             if (j == i) continue;
-            if (dist2(x[i], x[j]) < c.h2) {
+            V3<TF> d = x[i] - x[j];
+            d.y = wrap_coord(wrap, wrap_len, d.y);
+            if ((d.x * d.x + d.y * d.y) + d.z * d.z < c.h2) {
               if (found < nl.cap) nl.index[size_t(i) * nl.cap + found] = j;
               ++found;
             }
@@ -431,8 +449,9 @@ struct LagrangeGrid {
 
 // ------------------------------------------------------- analytic distances
 // dg/box_distance.hpp:23-39, dg/sphere_distance.hpp:18-21,
-// dg/box_shell_distance.hpp:36-59.  The torus (tube radius r around a circle
-// of radius R in the x-z plane) has no reference counterpart.
+// dg/box_shell_distance.hpp:36-59, the cylinder, capsule, infinite cylinder
+// and infinite tube below.  The torus (tube radius r around a circle of
+// radius R in the x-z plane) has no reference counterpart.
 template <class TF>
 struct Shape {
   uint32_t kind;
@@ -461,6 +480,23 @@ struct Shape {
         TF rho = std::sqrt(x.x * x.x + x.z * x.z) - p[0];
         return std::sqrt(rho * rho + x.y * x.y) - p[1];
       }
+      case AL_SHAPE_CYLINDER: {  // dg/cylinder_distance.hpp:28-35
+        const TF d0 = std::sqrt(x.x * x.x + x.z * x.z) - p[0];
+        const TF d1 = std::fabs(x.y + p[2]) - p[1] * TF(0.5);
+        const TF c0 = std::max(d0, TF(0)), c1 = std::max(d1, TF(0));
+        return std::min(std::max(d0, d1), TF(0)) + std::sqrt(c0 * c0 + c1 * c1);
+      }
+      case AL_SHAPE_CAPSULE: {  // dg/capsule_distance.hpp:24-27
+        const TF hh = p[1] * TF(0.5);
+        const V3<TF> m{x.x, x.y - std::max(-hh, std::min(x.y, hh)), x.z};
+        return std::sqrt(dot(m, m)) - p[0];
+      }
+      case AL_SHAPE_INFINITE_CYLINDER:  // dg/infinite_cylinder_distance.hpp:20-22
+        return std::sqrt(x.x * x.x + x.z * x.z) - p[0];
+      case AL_SHAPE_INFINITE_TUBE: {  // dg/infinite_tube_distance.hpp:32-36
+        const TF rd = std::sqrt(x.x * x.x + x.z * x.z);
+        return std::max(p[0] - rd, rd - p[1]);
+      }
       default:
         return std::numeric_limits<TF>::max();
     }
@@ -470,6 +506,13 @@ struct Shape {
   // h * 2^-8 (box_distance.hpp:28-38).
   V3<TF> gradient(V3<TF> x, TF h) const {
     if (kind == AL_SHAPE_SPHERE) return x;
+    // radial direction of the y-invariant shapes
+    // (dg/infinite_cylinder_distance.hpp:23-25, dg/infinite_tube_distance.hpp:37-43)
+    if (kind == AL_SHAPE_INFINITE_CYLINDER) return V3<TF>{x.x, 0, x.z};
+    if (kind == AL_SHAPE_INFINITE_TUBE) {
+      const TF s = (x.x * x.x + x.z * x.z) * 4 > (p[0] + p[1]) * (p[0] + p[1]) ? TF(1) : TF(-1);
+      return V3<TF>{s * x.x, 0, s * x.z};
+    }
     const TF step = h * TF(0.00390625);
     return V3<TF>{sdf(x + V3<TF>{step, 0, 0}) - sdf(x - V3<TF>{step, 0, 0}),
                   sdf(x + V3<TF>{0, step, 0}) - sdf(x - V3<TF>{0, step, 0}),
@@ -624,6 +667,8 @@ struct Body {
 template <class TF>
 void boundary_sample(const Cn<TF>& c, const Body<TF>& b, V3<TF> x, V4<TF>& bnd, V4<TF>& bk) {
   V3<TF> local = rotate(x - b.x, conjugate(b.q));
+  // compute_volume_and_boundary_x_analytic<1> (runner.hpp:1744-1746)
+  if (b.shape == AL_SHAPE_INFINITE_CYLINDER || b.shape == AL_SHAPE_INFINITE_TUBE) local.y = 0;
   V3<TF> bx = x, xi_bxj{0, 0, 0};
   TF d = 0, vol = 0;
   int ip[3];
@@ -677,6 +722,9 @@ void boundary_sample(const Cn<TF>& c, const Body<TF>& b, V3<TF> x, V4<TF>& bnd, 
 template <class TF>
 struct Fluid {
   uint32_t n = 0, nb = 0;
+  // periodic in y (step<1>): Const::wrap_length, 0 when not periodic
+  bool wrap = false;
+  TF wrap_len = 0;
   std::vector<V3<TF>> x, v, a;
   std::vector<TF> density, factor, kappa, kappa_v, density_adv;
   std::vector<TF> pressure, last_pressure, aii, density_err;
@@ -727,7 +775,7 @@ void compute_density(const Cn<TF>& c, Fluid<TF>& f) {
     TF rho = c.vol * c.w0;
     for (uint32_t k = 0; k < f.nl.count[i]; ++k) {
       uint32_t j = f.nl.index[size_t(i) * f.nl.cap + k];
-      rho += c.vol * W_r2(c, length_sqr(f.x[i] - f.x[j]));
+      rho += c.vol * W_r2(c, length_sqr(xv(f, i, j)));
     }
     for (uint32_t b = 0; b < f.nb; ++b) rho += f.bk[size_t(b) * f.n + i].w;
     f.density[i] = rho * c.rho0;
@@ -738,13 +786,17 @@ void compute_density(const Cn<TF>& c, Fluid<TF>& f) {
 template <class TF>
 void update_particle_neighbors(const Cn<TF>& c, const al_consti& g, Fluid<TF>& f) {
   f.gs = grid_sort(c, g, f.x.data(), f.n);
-  f.nl = neighbor_list(c, g, f.x.data(), f.n, f.gs);
+  f.nl = neighbor_list(c, g, f.x.data(), f.n, f.gs, f.wrap, f.wrap_len);
   compute_density(c, f);
 }
 
+// x_i - x_j, y wrapped on a periodic step (make_neighbor_list<1>,
+// runner.hpp:1893-1894).
 template <class TF>
 inline V3<TF> xv(const Fluid<TF>& f, uint32_t i, uint32_t j) {
-  return f.x[i] - f.x[j];
+  V3<TF> d = f.x[i] - f.x[j];
+  d.y = wrap_coord(f.wrap, f.wrap_len, d.y);
+  return d;
 }
 template <class TF>
 inline V3<TF> body_velocity(const Body<TF>& b, V3<TF> at) {
@@ -1153,7 +1205,10 @@ StepReport df_step(const Cn<TF>& c, const al_consti& g, std::vector<Body<TF>>& b
     for (uint32_t i = 0; i < n; ++i) f.kappa[i] *= dt * dt;
   }
   // integrate_velocity<0> (runner.hpp:3613-3623)
-  for (uint32_t i = 0; i < n; ++i) f.x[i] += dt * f.v[i];
+  for (uint32_t i = 0; i < n; ++i) {  // integrate_velocity<wrap>
+    f.x[i] += dt * f.v[i];
+    f.x[i].y = wrap_coord(f.wrap, f.wrap_len, f.x[i].y);
+  }
   std::vector<V3<double>> F, T;
   rigid_totals(f, F, T);
   if (F_out) *F_out = F;
@@ -1193,10 +1248,11 @@ void pressure_accels_and_integrate(const Cn<TF>& c, std::vector<Body<TF>>& bodie
     }
     f.pressure_accel[i] = rho0 * ai;
   }
-  // kinematic_integration<0> (runner.hpp:2873-2887)
+  // kinematic_integration<wrap> (runner.hpp:2873-2887)
   for (uint32_t i = 0; i < n; ++i) {
     V3<TF> v = f.v[i] + f.pressure_accel[i] * dt;
     f.x[i] += v * dt;
+    f.x[i].y = wrap_coord(f.wrap, f.wrap_len, f.x[i].y);
     f.v[i] = v;
   }
   std::vector<V3<double>> F, T;

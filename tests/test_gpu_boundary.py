@@ -102,6 +102,10 @@ def test_volume_field_field_gen(engine):
     (_capi.SHAPE_SPHERE, [0.05], 1.0),
     (_capi.SHAPE_BOX_SHELL, [0.2, 0.15, 0.2, 0.22, 0.17, 0.22, 0.0], 1.0),
     (_capi.SHAPE_TORUS, [0.06, 0.02], 1.0),
+    (_capi.SHAPE_CYLINDER, [0.04, 0.1, 0.01], 1.0),
+    (_capi.SHAPE_CAPSULE, [0.03, 0.08], 1.0),
+    (_capi.SHAPE_INFINITE_CYLINDER, [0.05], -1.0),
+    (_capi.SHAPE_INFINITE_TUBE, [0.04, 0.07, 0.05], 1.0),
 ])
 def test_analytic_volume_and_distance_grid(engine, shape, params, sign):
     dtype = np.float32
@@ -156,3 +160,67 @@ def test_particle_boundary_parity(engine, dtype):
         assert np.array_equal(g_bnd[b][:, 3] != 0, o_bnd[b][:, 3] != 0)
     assert (o_bnd[0][:, 3] != 0).sum() > 100  # the walls are felt
     assert (o_bnd[1][:, 3] != 0).sum() > 10 and (o_bnd[2][:, 3] != 0).sum() > 10
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_particle_boundary_new_shapes(engine, dtype):
+    """Cylinder and capsule (grid-sampled and analytic), and the y-invariant
+    infinite cylinder (a pipe, fluid inside) and infinite tube, sampled as
+    compute_volume_and_boundary_x_analytic<1> does (body-frame y set to 0)."""
+    bodies = [
+        dict(shape=_capi.SHAPE_CYLINDER, params=[0.035, 0.08, 0.005], sign=1.0, resolution=16,
+             use_distance_grid=True, mass=1.0, x=(0.1, 0.1, 0.1), q=(0.0, 0.0, 0.38268343,
+                                                                    0.92387953)),
+        dict(shape=_capi.SHAPE_CAPSULE, params=[0.03, 0.06], sign=1.0, resolution=16,
+             use_distance_grid=False, mass=1.0, x=(0.27, 0.12, 0.2)),
+        dict(shape=_capi.SHAPE_INFINITE_CYLINDER, params=[0.14], sign=-1.0, resolution=12,
+             use_distance_grid=False, mass=0.0, x=(0.15, 0.15, 0.15)),
+        dict(shape=_capi.SHAPE_INFINITE_TUBE, params=[0.02, 0.035, 0.05], sign=1.0,
+             resolution=12, use_distance_grid=False, mass=0.0, x=(0.2, 0.2, 0.1)),
+    ]
+    scene = scenes.dam_break(engine, dtype, (14, 14, 14), 0.01, (0.3, 0.3, 0.3), bodies,
+                             seed=6, volume_resolution=12)
+    n, nb = scene.n, scene.num_boundaries
+    T = scene.tdtype
+    bnd = torch.zeros(nb, n, 4, dtype=T, device="cuda")
+    bk = torch.zeros(nb, n, 4, dtype=T, device="cuda")
+    status = _lib("al_compute_particle_boundary", dtype)(
+        engine.handle, _capi.ptr(scene.cn), nb, _capi.ptr(scene.bodies), _capi.ptr(scene.rigid),
+        _capi.ptr(scene.x), n, _capi.ptr(bnd), _capi.ptr(bk), None)
+    assert status == 0
+    hb, keep, rigid = scene.host_bodies()
+    o_bnd, o_bk = orc.boundary(scene.cn, (type(hb[0]) * nb)(*[hb[b] for b in range(nb)]),
+                               rigid, host(scene.x))
+    g_bnd, g_bk = host(bnd), host(bk)
+    tol = 1e-5 if dtype == np.float32 else 1e-11
+    for b in range(1, nb):
+        # boundary points of particles the body does not reach (V = 0) come
+        # from finite-difference normals far from the surface, noisy in
+        # float32; the active ones are compared at the full bound
+        act = o_bnd[b][:, 3] != 0
+        np.testing.assert_allclose(g_bnd[b][act], o_bnd[b][act], rtol=tol, atol=tol * 0.5,
+                                   err_msg="body %d" % b)
+        np.testing.assert_allclose(g_bnd[b][~act], o_bnd[b][~act], rtol=1e-3, atol=1e-4,
+                                   err_msg="body %d (inactive)" % b)
+        scale = np.abs(o_bk[b]).max() + 1e-30
+        np.testing.assert_allclose(g_bk[b], o_bk[b], rtol=tol * 10, atol=tol * scale,
+                                   err_msg="body %d" % b)
+        assert np.array_equal(g_bnd[b][:, 3] != 0, o_bnd[b][:, 3] != 0)
+        assert (o_bnd[b][:, 3] != 0).sum() > 10, b
+    # the pipe's boundary points lie on its cylinder (radius 0.14 about the
+    # body's y axis) for particles that feel it
+    act = o_bnd[3][:, 3] != 0
+    r = np.hypot(g_bnd[3][act, 0] - 0.15, g_bnd[3][act, 2] - 0.15)
+    np.testing.assert_allclose(r, 0.14, atol=1e-4)
+
+
+def test_y_invariant_shapes_reject_distance_grids(engine):
+    dtype = np.float32
+    cn = scenes.make_const(dtype, 0.01)
+    body = scenes.make_body(dtype, cn, _capi.SHAPE_INFINITE_CYLINDER, [0.1], 8,
+                            use_distance_grid=True)
+    out = torch.zeros(body.num_nodes, device="cuda")
+    body.volume_nodes = out.data_ptr()
+    body.distance_nodes = out.data_ptr()
+    assert _lib("al_build_volume_field", dtype)(engine.handle, _capi.ptr(cn), _capi.ptr(body),
+                                                _capi.ptr(out), None) == _capi.AL_ERR_INVALID
