@@ -43,13 +43,14 @@ namespace {
 // `EX` adds one more sum over the list to phase 2 (EX::kOn): it supplies
 // the particle's and the neighbors' velocities and receives
 // sum_j V (v_i - v_j) . grad W_ij, in list order, at the end.
-template <class TF, class BK, bool FACTOR, class EX>
+template <class TF, class BK, bool FACTOR, class EX, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_build_neighbors(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
                       const vec4<TF>* __restrict__ xs, uint32_t n, BK bk,
                       uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount,
                       TF* __restrict__ rho, TF* __restrict__ alpha, TF* __restrict__ rho_rec,
                       uint32_t* __restrict__ flags, EX ex) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const vec3<TF> xi = xyz(xs[s]);

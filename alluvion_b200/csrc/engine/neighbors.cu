@@ -48,12 +48,22 @@ int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState&
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
                             TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st) {
   if (gs.n == 0) return AL_OK;
-  if (alpha)
-    k_build_neighbors<TF, BK, true, NoExtra<TF>><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
+  const uint32_t blocks = blocks_for(gs.n, kBlock);
+  // compile-time wrap flag: the non-periodic build carries no wrap branches
+  if (alpha && c.wrap)
+    k_build_neighbors<TF, BK, true, NoExtra<TF>, true><<<blocks, kBlock, 0, st>>>(
+        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        NoExtra<TF>{});
+  else if (alpha)
+    k_build_neighbors<TF, BK, true, NoExtra<TF>, false><<<blocks, kBlock, 0, st>>>(
+        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        NoExtra<TF>{});
+  else if (c.wrap)
+    k_build_neighbors<TF, BK, false, NoExtra<TF>, true><<<blocks, kBlock, 0, st>>>(
         c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
         NoExtra<TF>{});
   else
-    k_build_neighbors<TF, BK, false, NoExtra<TF>><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
+    k_build_neighbors<TF, BK, false, NoExtra<TF>, false><<<blocks, kBlock, 0, st>>>(
         c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
         NoExtra<TF>{});
   ALB_CUDA(cudaGetLastError());

@@ -302,8 +302,9 @@ enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 // (runner.hpp:3251-3295), divergence_solve_iteration (:3316-3363),
 // warm_start_pressure_solve1 (:3451-3491), pressure_solve_iteration
 // (:3543-3588).  Boundary reaction forces go to the per-block rigid slots.
-template <class TF, int MODE>
+template <class TF, int MODE, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
@@ -355,8 +356,9 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
 
 // compute_velocity_of_density_change (runner.hpp:3297-3314); also forms
 // k = rho_adv * alpha for the first divergence iteration.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF adv = density_change(c, S, L);
   if (!L.lead()) return;
@@ -369,9 +371,10 @@ __global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<
 
 // compute_divergence_solve_density_error (runner.hpp:3396-3410) with the
 // mean of solver_df.hpp:160-161 reduced in double on the device.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_df_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF adv = density_change(c, S, L);
   double val = 0;
@@ -389,9 +392,10 @@ __global__ void __launch_bounds__(kBlock)
 // divergence_solve_finish (runner.hpp:3412-3420) when `finish_div`, and
 // calculate_cfl_v2 (runner.hpp:2533-2541) reduced to the global max; the
 // last block applies Solver::update_dt (solver.hpp:153-169).
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_viscosity(Cn<TF> c, StepState<TF> S, int finish_div) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, da{0, 0, 0};
@@ -510,9 +514,10 @@ __global__ void k_integrate_np(StepState<TF> S) {
 // warm_start_pressure_solve0 (runner.hpp:3430-3449).
 // With `pred` (learned warm start) the predicted kappa replaces the
 // previous-step value under the same gate (rho_adv > 1).
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_p_warm0(Cn<TF> c, StepState<TF> S, const float* __restrict__ pred) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
@@ -526,8 +531,9 @@ __global__ void __launch_bounds__(kBlock)
 }
 
 // compute_rho_adv (runner.hpp:3525-3541); also k for the first iteration.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
@@ -540,9 +546,10 @@ __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<T
 
 // compute_pressure_solve_density_error (runner.hpp:3590-3604); the mean is
 // sum(rho_adv - 1) / N in double (solver_df.hpp:323-325 forms sum/N - 1).
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_p_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF adv = density_adv(c, S, L, S.ctrl->dt);
   double val = 0;
@@ -558,12 +565,13 @@ __global__ void __launch_bounds__(kBlock)
 
 // pressure_solve_finish + integrate_velocity<0> (runner.hpp:3606-3623),
 // written straight back to the caller's buffers in original order.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __restrict__ x_ref,
                             TF* __restrict__ v_ref, TF* __restrict__ a_ref,
                             TF* __restrict__ rho_ref, TF* __restrict__ alpha_ref,
                             TF* __restrict__ kappa_ref, TF* __restrict__ kappa_v_ref,
                             TF* __restrict__ rho_adv_ref) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S.n) return;
   const uint32_t i = S.perm[s];
@@ -587,8 +595,9 @@ __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __
 // ------------------------------------------------------------------ IISPH
 // predict_advection0 (runner.hpp:2609-2639).  kappa holds the pressure,
 // kappa_v the last pressure.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   vec3<TF> xi{0, 0, 0};
   TF rho2 = 1;
@@ -622,8 +631,9 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
 }
 
 // predict_advection1 (runner.hpp:2640-2690).  aii goes to kk.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, dii{0, 0, 0};
@@ -665,8 +675,9 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
 // the first, also performs the reference's last_pressure <- pressure copy
 // (solver_ii.hpp:204) for the own particle; this kernel reads the
 // neighbors' pressure (equal to their last pressure after that copy).
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const bool first = S.ctrl->it == 0;
   vec3<TF> xi{0, 0, 0};
@@ -691,9 +702,10 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
 
 // pressure_solve_iteration1 (runner.hpp:2716-2772) and the mean of
 // solver_ii.hpp:205-206 (double, on the device).
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_ii_iter1(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, dij_pj{0, 0, 0};
@@ -743,11 +755,12 @@ __global__ void __launch_bounds__(kBlock)
 
 // compute_pressure_accels (runner.hpp:2774-2817) + kinematic_integration<0>
 // (runner.hpp:2873-2887), written back in original order.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_ii_accel_finish(Cn<TF> c, StepState<TF> S, TF* __restrict__ x_ref, TF* __restrict__ v_ref,
                       TF* __restrict__ a_ref, TF* __restrict__ rho_ref, TF* __restrict__ p_ref,
                       TF* __restrict__ rho_adv_ref) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   vec3<TF> ai{0, 0, 0}, xi{0, 0, 0};
   TF dpi = 0;
@@ -809,8 +822,9 @@ __global__ void __launch_bounds__(kBlock) k_i_advect(StepState<TF> S) {
 
 // calculate_isph_diagonal_adv_density (runner.hpp:2901-2954): the Jacobi
 // diagonal (times rho0) into kk, the advected density into rho_adv.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0};
@@ -853,9 +867,10 @@ __global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
 // pressure into last_pressure after each iteration; here the two arrays
 // swap roles by iteration parity: iteration k reads kappa_v and writes
 // kappa when k is even, the reverse when odd.
-template <class TF>
+template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_i_iter(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
+  if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S.n);
   const TF dt = S.ctrl->dt;
   const bool odd = (S.ctrl->it & 1u) != 0;
@@ -1048,6 +1063,7 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   const auto* f = P.f;
   const uint32_t n = S.n, nb = S.nb;
   const bool iisph = P.iisph, div = P.div, den = P.den;
+  const bool wr = c.wrap != 0;  // periodic-y instantiations of the pair passes
   ALB_CUDA(cudaMemcpyAsync(S.ctrl, P.io.hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
   if (nb) {
     ALB_CUDA(cudaMemcpyAsync(P.bodies_dev, P.io.hb, sizeof(BodyDev<TF>) * nb,
@@ -1089,10 +1105,14 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   if (div && n > 0) {
     WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol};
     ALB_LAUNCH(e, "neighbors", 1, st,
-               (k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>>
-                <<<blocks_for(n, kBlock), kBlock, 0, st>>>(c, P.g, gs.cell_start, S.x, n, sbk,
-                                                           S.nbr, S.ncount, S.rho, S.alpha,
-                                                           rho_rec, gs.flags, wd)));
+               (wr ? k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, true>
+                         <<<blocks_for(n, kBlock), kBlock, 0, st>>>(
+                             c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
+                             rho_rec, gs.flags, wd)
+                   : k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false>
+                         <<<blocks_for(n, kBlock), kBlock, 0, st>>>(
+                             c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
+                             rho_rec, gs.flags, wd)));
     if (P.learned) {
       ALB_LAUNCH(e, "warm_net", 1, st,
                  ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, st)));
@@ -1129,73 +1149,80 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   if (n > 0) {
     if (div) {
       ALB_LAUNCH(e, "div_warm1", 1, st,
-                 k_kappa<TF, kDivWarm><<<pblocks, kBlock, 0, st>>>(c, S));
+                 (wr ? k_kappa<TF, kDivWarm, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_kappa<TF, kDivWarm, false><<<pblocks, kBlock, 0, st>>>(c, S)));
       ALB_LAUNCH(e, "div_rho_adv", 1, st,
-                 k_df_rho_adv_init<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+                 (wr ? k_df_rho_adv_init<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_df_rho_adv_init<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
       ALB_TRY(solve(0, P.io.hc->max_div,
                     [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
                       ALB_LAUNCH(e, "div_iter", 1, s,
-                                 k_kappa<TF, kDivIter><<<pblocks, kBlock, 0, s>>>(c, S));
+                                 (wr ? k_kappa<TF, kDivIter, true><<<pblocks, kBlock, 0, s>>>(c, S) : k_kappa<TF, kDivIter, false><<<pblocks, kBlock, 0, s>>>(c, S)));
                       ALB_LAUNCH(e, "div_residual", 1, s,
-                                 k_df_residual<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                                 (wr ? k_df_residual<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_df_residual<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
                       return AL_OK;
                     }));
     }
     ALB_LAUNCH(e, "viscosity", 1, st,
-               k_viscosity<TF><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0));
+               (wr ? k_viscosity<TF, true><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0) : k_viscosity<TF, false><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0)));
     if (!iisph) {
       ALB_LAUNCH(e, "integrate_np", 1, st, k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S));
       if (den) {
         ALB_LAUNCH(e, "press_warm0", 1, st,
-                   k_p_warm0<TF><<<pblocks, kBlock, 0, st>>>(c, S, P.warm_pred));
+                   (wr ? k_p_warm0<TF, true><<<pblocks, kBlock, 0, st>>>(c, S, P.warm_pred) : k_p_warm0<TF, false><<<pblocks, kBlock, 0, st>>>(c, S, P.warm_pred)));
         ALB_LAUNCH(e, "press_warm1", 1, st,
-                   k_kappa<TF, kPressWarm><<<pblocks, kBlock, 0, st>>>(c, S));
+                   (wr ? k_kappa<TF, kPressWarm, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_kappa<TF, kPressWarm, false><<<pblocks, kBlock, 0, st>>>(c, S)));
         ALB_LAUNCH(e, "press_rho_adv", 1, st,
-                   k_p_rho_adv_init<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+                   (wr ? k_p_rho_adv_init<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_p_rho_adv_init<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
         ALB_TRY(solve(1, P.io.hc->max_den,
                       [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
                         ALB_LAUNCH(e, "press_iter", 1, s,
-                                   k_kappa<TF, kPressIter><<<pblocks, kBlock, 0, s>>>(c, S));
+                                   (wr ? k_kappa<TF, kPressIter, true><<<pblocks, kBlock, 0, s>>>(c, S) : k_kappa<TF, kPressIter, false><<<pblocks, kBlock, 0, s>>>(c, S)));
                         ALB_LAUNCH(e, "press_residual", 1, s,
-                                   k_p_residual<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                                   (wr ? k_p_residual<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_p_residual<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
                         return AL_OK;
                       }));
       }
       ALB_LAUNCH(e, "finish", 1, st,
-                 k_df_finish<TF><<<blocks, kBlock, 0, st>>>(
+                 (wr ? k_df_finish<TF, true><<<blocks, kBlock, 0, st>>>(
                      c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
                      f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                     f->particle_kappa_v, f->particle_density_adv));
+                     f->particle_kappa_v, f->particle_density_adv) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
+                     c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                     f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
+                     f->particle_kappa_v, f->particle_density_adv)));
     } else if (P.isph) {
       ALB_LAUNCH(e, "i_advect", 1, st, k_i_advect<TF><<<blocks, kBlock, 0, st>>>(S));
-      ALB_LAUNCH(e, "i_diag", 1, st, k_i_diag<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "i_diag", 1, st, (wr ? k_i_diag<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_i_diag<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
       ALB_TRY(solve(1, P.io.hc->max_den,
                     [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
                       ALB_LAUNCH(e, "i_iter", 1, s,
-                                 k_i_iter<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                                 (wr ? k_i_iter<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_i_iter<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
                       return AL_OK;
                     }));
       ALB_LAUNCH(e, "i_final", 1, st,
                  k_i_final<TF><<<blocks, kBlock, 0, st>>>(S));
       ALB_LAUNCH(e, "finish", 1, st,
-                 k_ii_accel_finish<TF><<<pblocks, kBlock, 0, st>>>(
+                 (wr ? k_ii_accel_finish<TF, true><<<pblocks, kBlock, 0, st>>>(
                      c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-                     f->particle_pressure, f->particle_density_adv));
+                     f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pblocks, kBlock, 0, st>>>(
+                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                     f->particle_pressure, f->particle_density_adv)));
     } else {
-      ALB_LAUNCH(e, "ii_predict0", 1, st, k_ii_predict0<TF><<<pblocks, kBlock, 0, st>>>(c, S));
-      ALB_LAUNCH(e, "ii_predict1", 1, st, k_ii_predict1<TF><<<pblocks, kBlock, 0, st>>>(c, S));
+      ALB_LAUNCH(e, "ii_predict0", 1, st, (wr ? k_ii_predict0<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_ii_predict0<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
+      ALB_LAUNCH(e, "ii_predict1", 1, st, (wr ? k_ii_predict1<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_ii_predict1<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
       ALB_TRY(solve(1, P.io.hc->max_den,
                     [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
                       ALB_LAUNCH(e, "ii_iter0", 1, s,
-                                 k_ii_iter0<TF><<<pblocks, kBlock, 0, s>>>(c, S));
+                                 (wr ? k_ii_iter0<TF, true><<<pblocks, kBlock, 0, s>>>(c, S) : k_ii_iter0<TF, false><<<pblocks, kBlock, 0, s>>>(c, S)));
                       ALB_LAUNCH(e, "ii_iter1", 1, s,
-                                 k_ii_iter1<TF><<<pblocks, kBlock, 0, s>>>(c, S, h, use));
+                                 (wr ? k_ii_iter1<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_ii_iter1<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
                       return AL_OK;
                     }));
       ALB_LAUNCH(e, "finish", 1, st,
-                 k_ii_accel_finish<TF><<<pblocks, kBlock, 0, st>>>(
+                 (wr ? k_ii_accel_finish<TF, true><<<pblocks, kBlock, 0, st>>>(
                      c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-                     f->particle_pressure, f->particle_density_adv));
+                     f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pblocks, kBlock, 0, st>>>(
+                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                     f->particle_pressure, f->particle_density_adv)));
     }
   }
   if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(S));
