@@ -91,3 +91,54 @@ def test_ctypes_structs_match_the_header_layout(tmp_path):
         assert int(got["%s size" % py]) == ctypes.sizeof(cls), py
         for name, _ in cls._fields_:
             assert int(got["%s.%s" % (py, name)]) == getattr(cls, name).offset, (py, name)
+
+
+def test_cpp_layer_compiles_and_maps_statuses(tmp_path):
+    """include/alluvion_b200.hpp: compiles with g++ against the library; a
+    failed engine creation throws alluvion_b200::error with the status; the
+    capacity anomalies stay quiet unless asked (the reference reports its
+    grid_anomaly flags without throwing)."""
+    import subprocess
+    import torch
+    src = tmp_path / "shim.cpp"
+    src.write_text(r"""
+#include <cstdio>
+#include "alluvion_b200.hpp"
+namespace ab = alluvion_b200;
+// every step template instantiates for both real types
+template al_step_report ab::step<float>(const ab::engine&, ab::method, const al_const_f32&,
+    const al_consti&, const al_fluid_f32&, const al_body_f32*, al_rigid_f32*,
+    const al_solver_params&, float&, void*);
+template al_step_report ab::step<double>(const ab::engine&, ab::method, const al_const_f64&,
+    const al_consti&, const al_fluid_f64&, const al_body_f64*, al_rigid_f64*,
+    const al_solver_params&, double&, void*);
+template al_step_report ab::step_pellets<float>(const ab::engine&, const al_const_f32&,
+    const al_consti&, const al_fluid_f32&, const al_body_f32*, al_rigid_f32*,
+    const al_pellets_f32&, const al_solver_params&, float&, void*);
+int main() {
+  int created = -1;
+  try {
+    ab::engine e(0);
+    created = 0;
+  } catch (const ab::error& err) {
+    created = err.status();
+  }
+  bool quiet = true, loud = false;
+  try { ab::check(AL_ERR_NEIGHBOR_OVERFLOW, "x"); } catch (...) { quiet = false; }
+  try { ab::check(AL_ERR_NEIGHBOR_OVERFLOW, "x", true); }
+  catch (const ab::error& e) { loud = e.status() == AL_ERR_NEIGHBOR_OVERFLOW; }
+  int invalid = 0;
+  try { ab::check(AL_ERR_INVALID, "y"); } catch (const ab::error& e) { invalid = e.status(); }
+  std::printf("%d %d %d %d\n", created, int(quiet), int(loud), invalid);
+  return 0;
+}
+""")
+    exe = tmp_path / "shim"
+    libdir = os.path.dirname(_capi.lib()._name)
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-L", libdir, "-lalluvion_b200", "-Wl,-rpath," + libdir, "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    created, quiet, loud, invalid = map(int, out)
+    assert created == (0 if torch.cuda.is_available() else 8)
+    assert quiet == 1 and loud == 1 and invalid == 2
