@@ -173,6 +173,25 @@ PelletsF32 = _pellets_struct(ctypes.c_float)
 PelletsF64 = _pellets_struct(ctypes.c_double)
 
 
+class PelletRelaxParams(ctypes.Structure):
+    """al_pellet_relax_params (SolverPellet's coefficients)."""
+    _fields_ = [("cohesion", ctypes.c_double), ("adhesion", ctypes.c_double),
+                ("cfl_factor", ctypes.c_double), ("contact_tolerance", ctypes.c_double),
+                ("wrap_y", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("wrap_length", ctypes.c_double)]
+
+
+def pellet_relax_params(cohesion=4.0, adhesion=2.0, cfl_factor=0.25, contact_tolerance=0.0,
+                        wrap_length=None):
+    """SolverPellet's defaults (solver_pellet.hpp:47-50)."""
+    p = PelletRelaxParams()
+    p.cohesion, p.adhesion, p.cfl_factor = cohesion, adhesion, cfl_factor
+    p.contact_tolerance = contact_tolerance
+    if wrap_length is not None:
+        p.wrap_y, p.wrap_length = 1, wrap_length
+    return p
+
+
 class SampleF32(ctypes.Structure):
     """al_sample_f32: sample points, particle inputs and the outputs wanted
     (device pointers; None where unused)."""
@@ -294,6 +313,7 @@ for _s in ("f32", "f64"):
     _SIGNATURES["al_ii_step_" + _s] = (ctypes.c_int, [_P] * 10)
     _SIGNATURES["al_i_step_" + _s] = (ctypes.c_int, [_P] * 10)
     _SIGNATURES["al_i_step_pellets_" + _s] = (ctypes.c_int, [_P] * 11)
+    _SIGNATURES["al_relax_pellets_" + _s] = (ctypes.c_int, [_P] * 5 + [_U, _P, _U, _P, _P, _P])
 
 
 def declared_symbols():

@@ -216,6 +216,36 @@ __device__ __forceinline__ TF interpolate_grid(const BodyDev<TF>& b, const TF* _
   return phi;
 }
 
+// Interpolated value of `nodes` at x and its gradient scaled by 2 / cell
+// size (interpolate_and_derive, runner.hpp:1773-1791); false outside the
+// domain.
+template <class TF>
+__device__ __forceinline__ bool interpolate_grid_gradient(const BodyDev<TF>& b,
+                                                          const TF* __restrict__ nodes,
+                                                          vec3<TF> x, TF& phi, vec3<TF>& grad) {
+  int ip[3];
+  vec3<TF> xi;
+  if (!resolve(b, x, ip, xi)) return false;
+  const TF r2 = xi.x * xi.x + xi.y * xi.y + xi.z * xi.z;
+  phi = 0;
+  grad = vec3<TF>{0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    TF N;
+    vec3<TF> dN;
+    shape_j<TF, true>(j, xi, r2, N, dN);
+    const TF v = __ldg(nodes + lagrange_node(b.res, ip[0], ip[1], ip[2], j));
+    phi += v * N;
+    grad.x += v * dN.x;
+    grad.y += v * dN.y;
+    grad.z += v * dN.z;
+  }
+  grad.x *= TF(2) / b.cs.x;
+  grad.y *= TF(2) / b.cs.y;
+  grad.z *= TF(2) / b.cs.z;
+  return true;
+}
+
 // index_to_node_position (runner.hpp:1131-1178).
 template <class TF>
 __device__ __forceinline__ vec3<TF> node_position(const BodyDev<TF>& b, uint32_t l) {

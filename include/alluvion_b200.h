@@ -543,6 +543,45 @@ AL_API int al_i_step_pellets_f64(al_engine* engine, const al_const_f64* cn,
                                  const al_pellets_f64* pellets, const al_solver_params* params,
                                  double* dt, al_step_report* report, void* stream);
 
+/* Pellet relaxation: SolverPellet<TF>::step<wrap> (solver_pellet.hpp:57-119),
+ * the reference's tool that spreads boundary particles ("pellets") over a
+ * body by repeated steps of
+ *   update_particle_neighbors (pellet branch: density m (W(0) + sum W)),
+ *   compute_cohesion_adhesion_displacement (runner.hpp:2453-2532):
+ *     dx = -cohesion sum_j m / rho_j (1 - 2r / |x_ij|) W x_ij
+ *          - adhesion m / rho_i W(d) d n   (d, n: the body's distance and
+ *          normal at x_i minus contact_tolerance on the analytic branch),
+ *   compute_dfsph_factor_with_pellets (runner.hpp:3156-3190),
+ *   pellet_divergence_solve_iteration (runner.hpp:3365-3395),
+ *   cfl = min(cfl_factor 0.4 (2r) / max |dx|, 1) (solver_pellet.hpp:100-103),
+ *   move_and_avoid_boundary (runner.hpp:4010-4066): x += cfl dx, pushed back
+ *     to distance r from the body.
+ * The body is evaluated in its own frame at the particle positions (the
+ * reference's pile holds this one body at the origin); a mesh body uses its
+ * distance grid, every other shape its analytic distance.  `body` is a host
+ * struct (device node arrays); particle_x (device, [n][3]) is updated in
+ * place; particle_dx ([n][3], the reference's particle_v) and
+ * particle_density ([n]) receive the last step's values when non-NULL. */
+typedef struct al_pellet_relax_params {
+  double cohesion;          /* SolverPellet::cohesion (default 4) */
+  double adhesion;          /* SolverPellet::adhesion (default 2) */
+  double cfl_factor;        /* SolverPellet::cfl_factor (default 0.25) */
+  double contact_tolerance; /* Const::contact_tolerance */
+  uint32_t wrap_y;          /* 1: step<1> (periodic in y) */
+  uint32_t reserved;
+  double wrap_length;
+} al_pellet_relax_params;
+
+AL_API int al_relax_pellets_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                                const al_body_f32* body, float* particle_x, uint32_t num_particles,
+                                const al_pellet_relax_params* params, uint32_t steps,
+                                float* particle_dx, float* particle_density, void* stream);
+AL_API int al_relax_pellets_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                                const al_body_f64* body, double* particle_x,
+                                uint32_t num_particles, const al_pellet_relax_params* params,
+                                uint32_t steps, double* particle_dx, double* particle_density,
+                                void* stream);
+
 /* ---------------------------------------------------- learned warm start
  * No reference counterpart.  A per-particle MLP 12 -> 64 -> 64 -> 2 with
  * GELU (tanh form), BF16 operands and FP32 accumulation on the tensor

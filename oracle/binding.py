@@ -34,6 +34,7 @@ def lib():
             "orc_boundary_mask_f32": (None, [_P, _P, _P, _U, ctypes.c_float, _P]),
             "orc_histogram256_f32": (None, [_P, _P, _U, ctypes.c_float, ctypes.c_float, _P]),
             "orc_kl_divergence": (ctypes.c_double, [_P, _P, _U, _U, ctypes.c_double, _U]),
+            "orc_relax_pellets_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _U, _P, _P]),
         }
         for s in ("f32", "f64"):
             sig["orc_grid_sort_" + s] = (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P])
@@ -315,3 +316,14 @@ def run_pellets(cn, cni, bodies, rigid, state, pellet_local, counts, sp, dt, ste
         _p(px), _p(pp))
     assert status == 0
     return float(dt_arr[0]), list(reports), px, pp
+
+
+def relax_pellets(cn, cni, body, x, params, steps):
+    """SolverPellet<float>::step restated: returns (x, dx, density) after
+    `steps` steps and the neighbor-overflow flag."""
+    xs = np.ascontiguousarray(x, np.float32).copy()
+    dx = np.zeros_like(xs)
+    rho = np.zeros(len(xs), np.float32)
+    over = lib().orc_relax_pellets_f32(_p(cn), _p(cni), _p(body), _p(xs), len(xs), _p(params),
+                                       steps, _p(dx), _p(rho))
+    return xs, dx, rho, bool(over)

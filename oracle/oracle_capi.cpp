@@ -646,3 +646,41 @@ double orc_kl_divergence(const uint32_t* p, const uint32_t* q, uint32_t n_p, uin
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// SolverPellet<float>::step repeated `steps` times on host arrays:
+// x [n][3] in/out, dx [n][3] / rho [n] (may be NULL) of the last step.
+// Returns 1 on a neighbor overflow.
+int orc_relax_pellets_f32(const al_const_f32* cn, const al_consti* cni, const al_body_f32* body,
+                          float* x, uint32_t n, const al_pellet_relax_params* p, uint32_t steps,
+                          float* dx, float* rho) {
+  const Cn<float> c = make_cn<float>(*cn);
+  const Body<float> b = make_body<float>(*body, nullptr);
+  std::vector<V3<float>> xs(n);
+  for (uint32_t i = 0; i < n; ++i) xs[i] = v3<float>(x + 3 * size_t(i));
+  RelaxParams rp;
+  rp.cohesion = p->cohesion;
+  rp.adhesion = p->adhesion;
+  rp.cfl_factor = p->cfl_factor;
+  rp.tolerance = p->contact_tolerance;
+  rp.wrap = p->wrap_y != 0;
+  rp.wrap_length = p->wrap_length;
+  std::vector<V3<float>> d;
+  std::vector<float> r;
+  const bool over = relax_pellets(c, *cni, b, xs, rp, steps, &d, &r);
+  for (uint32_t i = 0; i < n; ++i) {
+    x[3 * size_t(i)] = xs[i].x;
+    x[3 * size_t(i) + 1] = xs[i].y;
+    x[3 * size_t(i) + 2] = xs[i].z;
+    if (dx && !d.empty()) {
+      dx[3 * size_t(i)] = d[i].x;
+      dx[3 * size_t(i) + 1] = d[i].y;
+      dx[3 * size_t(i) + 2] = d[i].z;
+    }
+    if (rho && !r.empty()) rho[i] = r[i];
+  }
+  return over ? 1 : 0;
+}
+
+}  // extern "C"

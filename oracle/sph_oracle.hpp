@@ -1781,6 +1781,151 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
   return rep;
 }
 
+// ----------------------------------------------------- pellet relaxation
+// SolverPellet<TF>::step<wrap> (solver_pellet.hpp:57-119): the body is
+// evaluated in its own frame at the particle positions.
+struct RelaxParams {
+  double cohesion = 4, adhesion = 2, cfl_factor = 0.25, tolerance = 0;
+  bool wrap = false;
+  double wrap_length = 0;
+};
+
+// interpolate_and_derive (runner.hpp:1773-1791): value and gradient scaled
+// by 2 / cell size; false outside the domain.
+template <class TF>
+bool grid_value_gradient(const Body<TF>& b, V3<TF> x, TF& phi, V3<TF>& grad) {
+  int ip[3];
+  V3<TF> xi;
+  if (!resolve(b.dmin, b.dmax, b.res, b.cs, x, ip, xi)) return false;
+  TF N[32], d0[32], d1[32], d2[32];
+  uint32_t cells[32];
+  shape_functions<TF>(xi, N, d0, d1, d2);
+  cell_nodes(b.res, ip, cells);
+  phi = 0;
+  grad = {0, 0, 0};
+  for (int j = 0; j < 32; ++j) {
+    const TF v = b.dist_nodes[cells[j]];
+    phi += v * N[j];
+    grad.x += v * d0[j];
+    grad.y += v * d1[j];
+    grad.z += v * d2[j];
+  }
+  grad.x *= TF(2) / b.cs.x;
+  grad.y *= TF(2) / b.cs.y;
+  grad.z *= TF(2) / b.cs.z;
+  return true;
+}
+
+// The body's distance (times sign) and normal as the relaxation kernels read
+// them: the grid for a mesh body (normal scaled by sign / |n|), else the
+// analytic distance minus the tolerance with the step-1e-3 normal.
+template <class TF>
+bool relax_body_distance(const Body<TF>& b, TF tolerance, V3<TF> x, TF& dist, V3<TF>& n) {
+  if (b.shape == AL_SHAPE_MESH) {
+    TF phi;
+    V3<TF> g;
+    if (!grid_value_gradient(b, x, phi, g)) return false;
+    dist = phi * b.sign;
+    const TF nl2 = length_sqr(g);
+    n = (b.sign * (nl2 > 0 ? inv_sqrt(nl2) : TF(0))) * g;
+    return true;
+  }
+  dist = b.sdf.sdf(x) * b.sign - tolerance;
+  n = b.sdf.gradient(x, TF(1e-3)) * b.sign;
+  return true;
+}
+
+template <class TF>
+bool relax_pellets(const Cn<TF>& c, const al_consti& g, const Body<TF>& b,
+                   std::vector<V3<TF>>& x, const RelaxParams& p, uint32_t steps,
+                   std::vector<V3<TF>>* dx_out, std::vector<TF>* rho_out) {
+  const uint32_t n = uint32_t(x.size());
+  const TF len = TF(p.wrap_length), tol = TF(p.tolerance);
+  const TF coh = TF(p.cohesion), adh = TF(p.adhesion);
+  bool overflow = false;
+  std::vector<TF> rho(n), factor(n);
+  std::vector<V3<TF>> dx(n);
+  for (uint32_t step = 0; step < steps; ++step) {
+    const GridSort s = grid_sort(c, g, x.data(), n);
+    const NeighborList nl = neighbor_list(c, g, x.data(), n, s, p.wrap, len);
+    overflow = overflow || nl.overflow;
+    auto disp = [&](uint32_t i, uint32_t j) {
+      V3<TF> d = x[i] - x[j];
+      d.y = wrap_coord(p.wrap, len, d.y);
+      return d;
+    };
+    // compute_density_with_pellets without pellets
+    for (uint32_t i = 0; i < n; ++i) {
+      TF d = c.w0;
+      for (uint32_t k = 0; k < nl.count[i]; ++k)
+        d += W_r2(c, length_sqr(disp(i, nl.index[size_t(i) * nl.cap + k])));
+      rho[i] = d * c.mass;
+    }
+    // compute_cohesion_adhesion_displacement (runner.hpp:2453-2532)
+    for (uint32_t i = 0; i < n; ++i) {
+      V3<TF> v{0, 0, 0};
+      for (uint32_t k = 0; k < nl.count[i]; ++k) {
+        const uint32_t j = nl.index[size_t(i) * nl.cap + k];
+        const V3<TF> d = disp(i, j);
+        const TF w = W_r2(c, length_sqr(d));
+        v -= (coh * c.mass / rho[j] * (TF(1) - c.radius * TF(2) * inv_sqrt(length_sqr(d))) * w) *
+             d;
+      }
+      TF dist;
+      V3<TF> nrm;
+      if (relax_body_distance(b, tol, x[i], dist, nrm)) {
+        const TF nn = length_sqr(nrm);
+        if (b.shape == AL_SHAPE_MESH || nn >= TF(1e-7))
+          v -= (adh * c.mass / rho[i] * W_dist(c, dist)) * (dist * (inv_sqrt(nn) * nrm));
+      }
+      dx[i] = v;
+    }
+    // compute_dfsph_factor_with_pellets (runner.hpp:3156-3190)
+    for (uint32_t i = 0; i < n; ++i) {
+      TF sum = 0;
+      V3<TF> gi{0, 0, 0};
+      for (uint32_t k = 0; k < nl.count[i]; ++k) {
+        const V3<TF> gp = (-c.vol) * gradW(c, disp(i, nl.index[size_t(i) * nl.cap + k]));
+        sum += length_sqr(gp);
+        gi -= gp;
+      }
+      sum += length_sqr(gi);
+      factor[i] = sum > c.eps ? TF(-1) / sum : TF(0);
+    }
+    // pellet_divergence_solve_iteration (runner.hpp:3365-3395) and the CFL
+    TF vmax = 0;
+    std::vector<V3<TF>> dn(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      const TF ki = (rho[i] / c.rho0 - TF(1)) * factor[i];
+      V3<TF> v = dx[i];
+      for (uint32_t k = 0; k < nl.count[i]; ++k) {
+        const uint32_t j = nl.index[size_t(i) * nl.cap + k];
+        const TF ks = ki + (rho[j] / c.rho0 - TF(1)) * factor[j];
+        if (std::fabs(ks) > c.eps) v -= ks * ((-c.vol) * gradW(c, disp(i, j)));
+      }
+      dn[i] = v;
+      vmax = std::max(vmax, length_sqr(v));
+    }
+    const TF cfl = std::min(TF(p.cfl_factor) * TF(0.4) * c.radius * TF(2) * (TF(1) / std::sqrt(vmax)),
+                            TF(1));
+    // move_and_avoid_boundary<wrap> (runner.hpp:4010-4066)
+    for (uint32_t i = 0; i < n; ++i) {
+      V3<TF> xi = x[i] + dn[i] * cfl;
+      TF dist;
+      V3<TF> nrm;
+      if (relax_body_distance(b, tol, xi, dist, nrm) && dist < c.radius)
+        xi += (c.radius - dist) * (inv_sqrt(length_sqr(nrm)) * nrm);
+      xi.y = wrap_coord(p.wrap, len, xi.y);
+      x[i] = xi;
+    }
+    if (step + 1 == steps) {
+      if (dx_out) *dx_out = dn;
+      if (rho_out) *rho_out = rho;
+    }
+  }
+  return overflow;
+}
+
 // ---------------------------------------------------------------- contacts
 // Rigid-rigid contacts: Contact (contact.hpp:8-25), collision_test
 // (runner.hpp:3833-4010; analytic distance for analytic bodies, the
