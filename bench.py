@@ -62,6 +62,18 @@ BATCH_WORKLOADS = {
              "(cubic lattices, r=0.01 m, seeded), boxes scaled with the count from 1.0x0.7x0.7 m, "
              "0-2 seeded rigid spheres per scene, 32^3 volume maps, one graph launch per step"),
 }
+# Post-processing variants (the reference's statistics kernels): their own
+# metric, not the headline.
+POSTPROC_WORKLOADS = {
+    "histogram-256m": dict(
+        n=1 << 28, metric="values/s (histogram256 with mask)", unit="values/s",
+        desc="histogram256 with mask of 268,435,456 seeded uniform float32 values (1 GiB, and "
+             "a 1 GiB mask, both larger than L2) in 256 bins"),
+    "sampling-1m": dict(
+        n=1 << 20, metric="samples/s (density, velocity, vorticity)", unit="samples/s",
+        desc="density, velocity and vorticity at 1,048,576 seeded samples in a jittered "
+             "1,000,000-particle lattice (r = 0.01 m, 100^3), no bodies"),
+}
 METHOD_NAME = {"df": "DFSPH", "ii": "IISPH", "i": "implicit SPH (SolverI)"}
 
 # Compulsory per-particle state traffic per pass, float32 ("Model A": every
@@ -132,8 +144,8 @@ def parse_args():
                    help="volume-map resolution of the container (default: the workload's)")
     p.add_argument("--eager", action="store_true",
                    help="launch every kernel from the host (no captured step graph)")
-    p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS),
-                   default="dambreak-1m")
+    p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) +
+                   sorted(POSTPROC_WORKLOADS), default="dambreak-1m")
     p.add_argument("--method", choices=["df", "ii", "i"], default="df")
     p.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
                    help="learned: DFSPH with the learned warm start, trained (untimed) on a "
@@ -831,8 +843,198 @@ def reference_arm(args):
     }), flush=True)
 
 
+def postproc_inputs(spec, name, torch, device):
+    """Seeded inputs of a post-processing workload (on `device`)."""
+    g = torch.Generator(device=device)
+    g.manual_seed(SEED)
+    if name == "histogram-256m":
+        v = torch.rand(spec["n"], device=device, generator=g)
+        m = (torch.rand(spec["n"], device=device, generator=g) < 0.5).float()
+        return dict(v=v, mask=m)
+    side = 100
+    idx = torch.arange(side ** 3, device=device)
+    lat = torch.stack([idx // (side * side), (idx // side) % side, idx % side], 1).float()
+    x = (lat + 0.5) * 0.02 + (torch.rand(lat.shape, device=device, generator=g) - 0.5) * 0.002
+    rho = 1000.0 + 10.0 * torch.rand(side ** 3, device=device, generator=g)
+    v = torch.randn(side ** 3, 3, device=device, generator=g)
+    sx = torch.rand(spec["n"], 3, device=device, generator=g) * 1.96 + 0.02
+    return dict(x=x.contiguous(), rho=rho, v=v.contiguous(), sx=sx.contiguous())
+
+
+def postproc_arm(args):
+    """Post-processing variants: histogram256 with mask, and sampling."""
+    import ctypes
+    import torch
+    from alluvion_b200 import _capi, scenes
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    engine = _capi.Engine(local)
+    spec = POSTPROC_WORKLOADS[args.workload]
+    lib = _capi.lib()
+    inp = postproc_inputs(spec, args.workload, torch, "cuda")
+    hist = torch.zeros(256, dtype=torch.int32, device="cuda")
+    if args.workload == "histogram-256m":
+        n = spec["n"]
+        def run(v, m):
+            _capi.check(lib.al_histogram256_f32(engine.handle, v.data_ptr(), m.data_ptr(), n,
+                                                ctypes.c_float(0.0), ctypes.c_float(1.0),
+                                                hist.data_ptr(), None), "histogram")
+        call = lambda: run(inp["v"], inp["mask"])
+        units = n
+        alg_bytes = 8 * n  # values and mask, read once
+    else:
+        cn = scenes.make_const(np.float32, 0.01)
+        cni = scenes.make_consti((0.0, 0.0, 0.0), (2.0, 2.0, 2.0), float(cn.kernel_radius))
+        s = spec["n"]
+        outs = [torch.zeros(s, device="cuda"), torch.zeros(s, 3, device="cuda"),
+                torch.zeros(s, 3, device="cuda")]
+        req = _capi.SampleF32()
+        req.sample_x, req.num_samples = inp["sx"].data_ptr(), s
+        req.particle_density, req.particle_v = inp["rho"].data_ptr(), inp["v"].data_ptr()
+        req.sample_density, req.sample_v = outs[0].data_ptr(), outs[1].data_ptr()
+        req.sample_vorticity = outs[2].data_ptr()
+        npart = inp["x"].shape[0]
+        def call():
+            _capi.check(lib.al_sample_fluid_f32(engine.handle, _capi.ptr(cn), _capi.ptr(cni),
+                                                inp["x"].data_ptr(), npart, None, _capi.ptr(req),
+                                                None), "sample")
+        units = s
+        # particle x, rho, v read once; samples read, three outputs written
+        alg_bytes = npart * (12 + 4 + 12) + s * (12 + 4 + 12 + 12)
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        call()
+    b.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b)
+    value = units * args.steps / (ms / 1e3)
+    # per-launch device time of the dominant launch group
+    engine.reset_stats()
+    engine.set_profiling(True)
+    call()
+    engine.synchronize()
+    engine.set_profiling(False)
+    stats = engine.kernel_stats()
+    dom = max(stats, key=lambda k: stats[k][0])
+    launch_ms = stats[dom][0] / max(stats[dom][1], 1)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms / args.steps / 1e3) / 1e9
+    # end to end: inputs from pinned host memory, results back, every step
+    if args.workload == "histogram-256m":
+        hv = inp["v"].cpu().pin_memory()
+        hm = inp["mask"].cpu().pin_memory()
+        hh = torch.zeros(256, dtype=torch.int32).pin_memory()
+        def e2e_step():
+            inp["v"].copy_(hv, non_blocking=True)
+            inp["mask"].copy_(hm, non_blocking=True)
+            call()
+            hh.copy_(hist, non_blocking=True)
+        h2d, d2h = 8 * spec["n"], 1024
+    else:
+        hs = inp["sx"].cpu().pin_memory()
+        hx = inp["x"].cpu().pin_memory()
+        ho = [o.cpu().pin_memory() for o in outs]
+        def e2e_step():
+            inp["sx"].copy_(hs, non_blocking=True)
+            inp["x"].copy_(hx, non_blocking=True)
+            call()
+            for h, o in zip(ho, outs):
+                h.copy_(o, non_blocking=True)
+        h2d = hs.numel() * 4 + hx.numel() * 4
+        d2h = sum(o.numel() * 4 for o in outs)
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_steps = max(3, min(args.steps, 10))
+    for _ in range(e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e = units * e_steps / (time.perf_counter() - t0)
+    result = {
+        "metric": spec["metric"], "value": round(value, 1), "unit": spec["unit"], "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": spec["desc"], "l2": "inputs larger than L2 (no flush)",
+                   "launch_groups_ms": {k: round(v[0], 4) for k, v in stats.items()}},
+        "e2e": {"value": round(e2e, 1), "unit": spec["unit"], "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(engine.launch_count()),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "kernel": dom, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": int(alg_bytes),
+                     "launch_ms": round(launch_ms, 4)},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        result["cpu_baseline"] = postproc_cpu(args, spec, inp)
+    print(json.dumps(result), flush=True)
+
+
+def postproc_cpu(args, spec, inp):
+    """The oracle on a bounded sample of the same workload, host threads."""
+    from oracle import binding as orc
+    if args.workload == "histogram-256m":
+        m = 1 << 24
+        v = inp["v"][:m].cpu().numpy()
+        mk = inp["mask"][:m].cpu().numpy()
+        t0 = time.perf_counter()
+        orc.histogram256(v, 0.0, 1.0, mk)
+        dt = time.perf_counter() - t0
+        return {"value": round(m / dt, 1), "unit": spec["unit"], "cores": 1, "kind": "port",
+                "sample": "the oracle's histogram of the first %d values and mask" % m}
+    from alluvion_b200 import scenes
+    cn = scenes.make_const(np.float32, 0.01)
+    cni = scenes.make_consti((0.0, 0.0, 0.0), (2.0, 2.0, 2.0), float(cn.kernel_radius))
+    m = 1 << 16
+    t0 = time.perf_counter()
+    orc.sample_fluid(cn, cni, inp["x"].cpu().numpy(), None, inp["sx"][:m].cpu().numpy(),
+                     inp["rho"].cpu().numpy(), inp["v"].cpu().numpy(),
+                     outputs=("density", "v", "vorticity"))
+    dt = time.perf_counter() - t0
+    return {"value": round(m / dt, 1), "unit": spec["unit"], "cores": orc.lib().orc_num_threads(),
+            "kind": "port",
+            "sample": "the oracle's sampling of the first %d samples (grid sort of all "
+                      "particles included)" % m}
+
+
+def postproc_reference(args):
+    """Reference arm of the post-processing variants: the oracle port."""
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    import torch
+    spec = POSTPROC_WORKLOADS[args.workload]
+    inp = postproc_inputs(spec, args.workload, torch, "cpu")
+    for _ in range(max(args.warmup, 1)):
+        base = postproc_cpu(args, spec, inp)
+    vals = [postproc_cpu(args, spec, inp)["value"] for _ in range(max(1, min(args.steps, 3)))]
+    v = float(np.median(vals))
+    print(json.dumps({"impl": "reference", "metric": spec["metric"], "value": round(v, 1),
+                      "unit": spec["unit"], "n_gpus": world, "steps": len(vals),
+                      "warmup": args.warmup, "higher_is_better": True,
+                      "config": {"workload": spec["desc"]},
+                      "cpu_baseline": dict(base, value=round(v, 1)),
+                      "e2e": {"value": round(v, 1), "unit": spec["unit"],
+                              "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload in POSTPROC_WORKLOADS:
+        if args.impl == "reference":
+            postproc_reference(args)
+        else:
+            postproc_arm(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
     elif args.workload in BATCH_WORKLOADS:
