@@ -11,7 +11,11 @@
 // order.  Pressures live in two [N + P] arrays whose roles swap with the
 // iteration parity (the reference copies pressure into last_pressure after
 // every iteration); the pellet part of the array an iteration reads is
-// filled just before it by the extrapolation.
+// filled just before it by the extrapolation.  With wrap_y (step<1>) the
+// lists' cells and displacements wrap in y, rigid torque arms use the
+// pellet image x_i - x_ij, and integrated positions wrap; the
+// extrapolation's weighted centre uses absolute positions, as the
+// reference's does.
 #include <cfloat>
 #include <cstring>
 #include <vector>
@@ -144,14 +148,20 @@ __global__ void __launch_bounds__(kBlock)
       const int cx = ip[0] + dx;
       if (cx < 0 || cx >= int(g.res[0])) continue;
       for (int dy = -1; dy <= 1; ++dy) {
-        const int cy = ip[1] + dy;
+        int cy = ip[1] + dy;
+        if (c.wrap) {  // make_bead_pellet_neighbor_list<1>
+          if (cy >= int(g.res[1]))
+            cy -= int(g.res[1]);
+          else if (cy < 0)
+            cy += int(g.res[1]);
+        }
         if (cy < 0 || cy >= int(g.res[1])) continue;
         const uint32_t b = cell_start[cell_linear(g, cx, cy, z0)];
         const uint32_t e = cell_start[cell_linear(g, cx, cy, z1) + 1];
         for (uint32_t t = b; t < e; ++t) {
           const uint32_t j = S.perm[t];
           if (j == i) continue;
-          const TF d2 = dist2_rn(xi, xyz(xs[t]));
+          const TF d2 = pdist2(c, xi, xyz(xs[t]));
           if (!(d2 < c.h2)) continue;
           if (j < S.n) {
             if (nbead < S.cap) S.blist[size_t(nbead) * total + i] = j;
@@ -190,21 +200,21 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t nbd = S.bcnt[i];
     for (uint32_t k = 0; k < nbd; ++k) {
       const uint32_t j = S.blist[size_t(k) * total + i];
-      const vec3<TF> d = xi - ldv(S.x, j);
+      const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
       da += (c.visc * c.mass / S.rho[j] * dot(d, gradW(c, d)) / (length_sqr(d) + eps)) *
             (vi - ldv(S.v, j));
     }
     const uint32_t npl = S.pcnt[i];
     for (uint32_t k = 0; k < npl; ++k) {
       const uint32_t j = S.plist[size_t(k) * total + i];
-      const vec3<TF> xj = ldv(S.x, j);
-      const vec3<TF> d = xi - xj;
+      const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
       const vec3<TF> a =
           (c.vol * c.bvisc * dot(d, gradW(c, d)) / (length_sqr(d) + eps)) * (vi - ldv(S.v, j));
       da += a;
       const uint32_t b = S.pbody[j - S.n];
       const vec3<TF> f = (-c.mass) * a;
-      add_force(S, b, i, f, cross(xj - S.rigid[b].x, f));
+      // pellet_x = x_i - x_ij (runner.hpp:2289): the pellet's image next to x_i
+      add_force(S, b, i, f, cross((xi - d) - S.rigid[b].x, f));
     }
     const vec3<TF> acc = c.g + da;
     stv(S.a, i, acc);
@@ -274,7 +284,7 @@ __global__ void __launch_bounds__(kBlock) k_pel_diag(Cn<TF> c, PelletState<TF> S
   const uint32_t nbd = S.bcnt[i];
   for (uint32_t k = 0; k < nbd; ++k) {
     const uint32_t j = S.blist[size_t(k) * total + i];
-    const vec3<TF> d = xi - ldv(S.x, j);
+    const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
     const TF rj = S.rho[j];
     const vec3<TF> gw = gradW(c, d);
     adv += dt * c.vol * dot(vi - ldv(S.v, j), gw);
@@ -283,7 +293,7 @@ __global__ void __launch_bounds__(kBlock) k_pel_diag(Cn<TF> c, PelletState<TF> S
   const uint32_t npl = S.pcnt[i];
   for (uint32_t k = 0; k < npl; ++k) {
     const uint32_t j = S.plist[size_t(k) * total + i];
-    const vec3<TF> d = xi - ldv(S.x, j);
+    const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
     const vec3<TF> gwv = c.vol * gradW(c, d);
     adv += dt * dot(vi - ldv(S.v, j), gwv);
     diag += (rho + c.rho0) / (rho * c.rho0) / (length_sqr(d) + eps) * dot(d, gwv);
@@ -356,7 +366,7 @@ __global__ void k_pel_extrapolate(Cn<TF> c, PelletState<TF> S, int final_pass) {
   for (uint32_t k = 0; k < cnt; ++k) {
     const uint32_t j = S.blist[size_t(k) * total + i];
     const vec3<TF> xj = ldv(S.x, j);
-    const TF w = W_r2(c, dist2_rn(xi, xj)) * c.vol;
+    const TF w = W_r2(c, pdist2(c, xi, xj)) * c.vol;  // the list's (wrapped) x_ij
     wsum += w;
     center += w * xj;
   }
@@ -372,7 +382,7 @@ __global__ void k_pel_extrapolate(Cn<TF> c, PelletState<TF> S, int final_pass) {
     const uint32_t j = S.blist[size_t(k) * total + i];
     const vec3<TF> xj = ldv(S.x, j);
     const vec3<TF> xt = xj - center;
-    const TF w = W_r2(c, dist2_rn(xi, xj)) * c.vol;
+    const TF w = W_r2(c, pdist2(c, xi, xj)) * c.vol;
     const TF wp = w * pr[j];
     alpha += wp;
     psum += wp * xt;
@@ -422,7 +432,7 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t nbd = S.bcnt[i];
     for (uint32_t k = 0; k < nbd; ++k) {
       const uint32_t j = S.blist[size_t(k) * total + i];
-      const vec3<TF> d = xi - ldv(S.x, j);
+      const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
       const TF rj = S.rho[j];
       off -= c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
              last[j];
@@ -430,7 +440,7 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t npl = S.pcnt[i];
     for (uint32_t k = 0; k < npl; ++k) {
       const uint32_t j = S.plist[size_t(k) * total + i];
-      const vec3<TF> d = xi - ldv(S.x, j);
+      const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
       off -= c.vol * (rho + c.rho0) / (rho * c.rho0) / (length_sqr(d) + eps) *
              dot(d, gradW(c, d)) * last[j];
     }
@@ -477,23 +487,25 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t j = S.blist[size_t(k) * total + i];
     const TF rj = S.rho[j];
     const TF dpj = pr[j] / (rj * rj);
-    ai -= (c.mass * (dpi + dpj)) * gradW(c, xi - ldv(S.x, j));
+    ai -= (c.mass * (dpi + dpj)) * gradW(c, pdisp(c, xi, ldv(S.x, j)));
   }
   const uint32_t npl = S.pcnt[i];
   const TF r02 = c.rho0 * c.rho0;
   for (uint32_t k = 0; k < npl; ++k) {
     const uint32_t j = S.plist[size_t(k) * total + i];
-    const vec3<TF> xj = ldv(S.x, j);
+    const vec3<TF> d = pdisp(c, xi, ldv(S.x, j));
     const TF dpj = pr[j] / r02;
-    const vec3<TF> a = (c.mass * (dpi + dpj)) * gradW(c, xi - xj);
+    const vec3<TF> a = (c.mass * (dpi + dpj)) * gradW(c, d);
     const vec3<TF> f = c.mass * a;
     ai -= a;
     const uint32_t b = S.pbody[j - S.n];
-    add_force(S, b, i, f, cross(xj - S.rigid[b].x, f));
+    add_force(S, b, i, f, cross((xi - d) - S.rigid[b].x, f));  // x_j = x_i - x_ij
   }
   const TF dt = S.ctrl->dt;
   const vec3<TF> v = ldv(S.v, i) + (c.rho0 * ai) * dt;
-  stv(x_ref, i, xi + v * dt);
+  vec3<TF> xn = xi + v * dt;
+  xn.y = wrap_y(c, xn.y);  // kinematic_integration<wrap>
+  stv(x_ref, i, xn);
   stv(v_ref, i, v);
   if (a_ref) stv(a_ref, i, ldv(S.a, i));
   if (rho_ref) rho_ref[i] = rho;
@@ -573,10 +585,7 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
                 "al_i_step_pellets: particle_x / particle_v / particle_pressure are null");
   ALB_CHECK_ARG(np == 0 || pel->local_x, "al_i_step_pellets: pellet local_x is null");
   ALB_CHECK_ARG(np == 0 || nb > 0, "al_i_step_pellets: pellets need bodies");
-  if (sp->wrap_y) {
-    set_error("al_i_step_pellets: periodic (wrap_y) steps are not supported on the pellet branch");
-    return AL_ERR_UNSUPPORTED;
-  }
+  ALB_CHECK_ARG(!sp->wrap_y || sp->wrap_length > 0, "al_i_step_pellets: wrap_y needs a length");
   ALB_CHECK_ARG(uint64_t(n) + np < (1ull << 31), "al_i_step_pellets: too many points");
   BodyOffsets off{};
   uint64_t acc = 0;
@@ -595,7 +604,8 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
     ~NsReset() { e->ns.clear(); }
   } reset{e};
   e->ns = "pellet.";
-  const Cn<TF> c = to_cn<TF>(*cn);
+  Cn<TF> c = to_cn<TF>(*cn);
+  if (sp->wrap_y) set_wrap(c, TF(sp->wrap_length));  // SolverI::step<1>
   const GridDims g = to_dims(*cni);
   const uint32_t total = n + np;
   PelletState<TF> S;

@@ -513,6 +513,7 @@ AL_API int al_i_step_f64(al_engine* engine, const al_const_f64* cn, const al_con
  *   kinematic_integration, per-body totals and Pile::integrate_kinematics.
  * Pellets weigh as fluid particles of rest density rho0.  Bodies need
  * mass, inertia and max_distance; their node arrays are not read.
+ * params->wrap_y selects step<1> (periodic in y, as for al_i_step_f32).
  * Eager: the host reads the loop flag after every iteration. */
 typedef struct al_pellets_f32 {
   const float* local_x;  /* device [num_pellets][3]: body frame, body after body */

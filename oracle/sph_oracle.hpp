@@ -1525,11 +1525,19 @@ void jacobi_eigen3(TF a[3][3], TF q[3][3]) {
 // reference's 0/0 becomes 0 through fmax).
 template <class TF>
 TF extrapolate_pellet(const Cn<TF>& c, const std::vector<V3<TF>>& X, const std::vector<TF>& pr,
-                      const uint32_t* list, uint32_t cnt, V3<TF> xi) {
+                      const uint32_t* list, uint32_t cnt, V3<TF> xi, bool wrap = false,
+                      TF wrap_len = 0) {
+  // W of the list's (wrapped) x_ij; the centre from absolute positions, as
+  // the reference computes it
+  auto w2 = [&](uint32_t j) {
+    V3<TF> d = xi - X[j];
+    d.y = wrap_coord(wrap, wrap_len, d.y);
+    return length_sqr(d);
+  };
   TF wsum = 0;
   V3<TF> center{0, 0, 0};
   for (uint32_t k = 0; k < cnt; ++k) {
-    const TF w = W_r2(c, dist2(xi, X[list[k]])) * c.vol;
+    const TF w = W_r2(c, w2(list[k])) * c.vol;
     wsum += w;
     center += w * X[list[k]];
   }
@@ -1541,7 +1549,7 @@ TF extrapolate_pellet(const Cn<TF>& c, const std::vector<V3<TF>>& X, const std::
   for (uint32_t k = 0; k < cnt; ++k) {
     const uint32_t j = list[k];
     const V3<TF> xt = X[j] - center;
-    const TF w = W_r2(c, dist2(xi, X[j])) * c.vol;
+    const TF w = W_r2(c, w2(j)) * c.vol;
     const TF wp = w * pr[j];
     alpha += wp;
     psum += wp * xt;
@@ -1594,6 +1602,12 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
   const GridSort s = grid_sort(c, g, X.data(), total);
   rep.grid_anomaly[0] = s.out_of_grid;
   rep.grid_anomaly[1] = s.cell_overflow;
+  // x_i - x_j of the lists, y wrapped on a periodic step
+  auto D = [&](uint32_t i, uint32_t j) {
+    V3<TF> d = X[i] - X[j];
+    d.y = wrap_coord(f.wrap, f.wrap_len, d.y);
+    return d;
+  };
   const uint32_t cap = g.max_num_neighbors_per_particle;
   std::vector<uint32_t> bl(size_t(total) * cap), pl(size_t(total) * cap), bc(total), pc(total);
   bool overflow = false;
@@ -1607,11 +1621,17 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
       for (int dy = -1; dy <= 1; ++dy)
         for (int dz = -1; dz <= 1; ++dz) {
           int q[3] = {p[0] + dx, p[1] + dy, p[2] + dz};
+          if (f.wrap) {  // make_bead_pellet_neighbor_list<1>
+            if (q[1] >= int(g.grid_res[1]))
+              q[1] -= int(g.grid_res[1]);
+            else if (q[1] < 0)
+              q[1] += int(g.grid_res[1]);
+          }
           if (!in_grid(g, q)) continue;
           const uint32_t cell = cell_linear(g, q);
           for (uint32_t t = s.cell_start[cell]; t < s.cell_start[cell + 1]; ++t) {
             const uint32_t j = s.sorted[t];
-            if (j == i || !(dist2(X[i], X[j]) < c.h2)) continue;
+            if (j == i || !(length_sqr(D(i, j)) < c.h2)) continue;
             if (j < n) {
               if (nbd < cap) bl[size_t(i) * cap + nbd] = j;
               ++nbd;
@@ -1631,8 +1651,8 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
   // compute_density_with_pellets (runner.hpp:2074-2098)
   for (uint32_t i = 0; i < n; ++i) {
     TF d = c.w0;
-    for (uint32_t k = 0; k < bc[i]; ++k) d += W_r2(c, dist2(X[i], X[B(i, k)]));
-    for (uint32_t k = 0; k < pc[i]; ++k) d += W_r2(c, dist2(X[i], X[Pn(i, k)]));
+    for (uint32_t k = 0; k < bc[i]; ++k) d += W_r2(c, length_sqr(D(i, B(i, k))));
+    for (uint32_t k = 0; k < pc[i]; ++k) d += W_r2(c, length_sqr(D(i, Pn(i, k))));
     f.density[i] = d * c.mass;
   }
   // clear_acceleration + compute_viscosity_with_pellets (runner.hpp:2251-2299)
@@ -1642,20 +1662,20 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
     V3<TF> da{0, 0, 0};
     for (uint32_t k = 0; k < bc[i]; ++k) {
       const uint32_t j = B(i, k);
-      const V3<TF> d = X[i] - X[j];
+      const V3<TF> d = D(i, j);
       da += (c.visc * c.mass / f.density[j] * dot(d, gradW(c, d)) / (length_sqr(d) + eps)) *
             (Vv[i] - Vv[j]);
     }
     for (uint32_t k = 0; k < pc[i]; ++k) {
       const uint32_t j = Pn(i, k);
-      const V3<TF> d = X[i] - X[j];
+      const V3<TF> d = D(i, j);
       const V3<TF> a =
           (c.vol * c.bvisc * dot(d, gradW(c, d)) / (length_sqr(d) + eps)) * (Vv[i] - Vv[j]);
       da += a;
       const uint32_t b = pel.body[j - n];
       const V3<TF> force = (-c.mass) * a;
       f.force[size_t(b) * n + i] += force;
-      f.torque[size_t(b) * n + i] += cross(X[j] - bodies[b].x, force);
+      f.torque[size_t(b) * n + i] += cross((X[i] - d) - bodies[b].x, force);  // pellet_x
     }
     f.a[i] = c.g + da;
   }
@@ -1677,7 +1697,7 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
     TF adv = rho / c.rho0, diag = 0;
     for (uint32_t k = 0; k < bc[i]; ++k) {
       const uint32_t j = B(i, k);
-      const V3<TF> d = X[i] - X[j];
+      const V3<TF> d = D(i, j);
       const TF rj = f.density[j];
       const V3<TF> gw = gradW(c, d);
       adv += dt * c.vol * dot(Vv[i] - Vv[j], gw);
@@ -1685,7 +1705,7 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
     }
     for (uint32_t k = 0; k < pc[i]; ++k) {
       const uint32_t j = Pn(i, k);
-      const V3<TF> d = X[i] - X[j];
+      const V3<TF> d = D(i, j);
       const V3<TF> gwv = c.vol * gradW(c, d);
       adv += dt * dot(Vv[i] - Vv[j], gwv);
       diag += (rho + c.rho0) / (rho * c.rho0) / (length_sqr(d) + eps) * dot(d, gwv);
@@ -1697,7 +1717,7 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
 #pragma omp parallel for schedule(static)
     for (int64_t pp = 0; pp < int64_t(np); ++pp) {
       const uint32_t i = n + uint32_t(pp);
-      pr[i] = extrapolate_pellet(c, X, pr, &bl[size_t(i) * cap], bc[i], X[i]);
+      pr[i] = extrapolate_pellet(c, X, pr, &bl[size_t(i) * cap], bc[i], X[i], f.wrap, f.wrap_len);
     }
   };
   double mean = std::numeric_limits<double>::max();
@@ -1715,14 +1735,14 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
       TF off = 0, pv = 0;
       for (uint32_t k = 0; k < bc[i]; ++k) {
         const uint32_t j = B(i, k);
-        const V3<TF> d = X[i] - X[j];
+        const V3<TF> d = D(i, j);
         const TF rj = f.density[j];
         off -= c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
                L[j];
       }
       for (uint32_t k = 0; k < pc[i]; ++k) {
         const uint32_t j = Pn(i, k);
-        const V3<TF> d = X[i] - X[j];
+        const V3<TF> d = D(i, j);
         off -= c.vol * (rho + c.rho0) / (rho * c.rho0) / (length_sqr(d) + eps) *
                dot(d, gradW(c, d)) * L[j];
       }
@@ -1751,23 +1771,25 @@ StepReport i_step_pellets(const Cn<TF>& c, const al_consti& g, std::vector<Body<
     for (uint32_t k = 0; k < bc[i]; ++k) {
       const uint32_t j = B(i, k);
       const TF rj = f.density[j], dpj = P[j] / (rj * rj);
-      ai -= (c.mass * (dpi + dpj)) * gradW(c, X[i] - X[j]);
+      ai -= (c.mass * (dpi + dpj)) * gradW(c, D(i, j));
     }
     for (uint32_t k = 0; k < pc[i]; ++k) {
       const uint32_t j = Pn(i, k);
       const TF dpj = P[j] / (c.rho0 * c.rho0);
-      const V3<TF> a = (c.mass * (dpi + dpj)) * gradW(c, X[i] - X[j]);
+      const V3<TF> d = D(i, j);
+      const V3<TF> a = (c.mass * (dpi + dpj)) * gradW(c, d);
       const V3<TF> force = c.mass * a;
       ai -= a;
       const uint32_t b = pel.body[j - n];
       f.force[size_t(b) * n + i] += force;
-      f.torque[size_t(b) * n + i] += cross(X[j] - bodies[b].x, force);
+      f.torque[size_t(b) * n + i] += cross((X[i] - d) - bodies[b].x, force);
     }
     f.pressure_accel[i] = c.rho0 * ai;
   }
   for (uint32_t i = 0; i < n; ++i) {
     const V3<TF> v = f.v[i] + f.pressure_accel[i] * dt;
     f.x[i] += v * dt;
+    f.x[i].y = wrap_coord(f.wrap, f.wrap_len, f.x[i].y);
     f.v[i] = v;
     f.pressure[i] = P[i];
   }

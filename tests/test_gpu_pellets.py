@@ -279,3 +279,54 @@ def test_sampling_with_pellets(engine):
     assert pd[in_wall].max() > 0 and outs["density"].cpu().numpy()[in_wall].max() == 0
     # a moving pellet sphere gives samples near it the sphere's velocity
     assert np.abs(ref["v"]).max() > 0
+
+
+def test_periodic_pellet_pipe_matches_oracle(engine):
+    """SolverI::step<1> on the pellet branch: a pipe of pellet rings, periodic
+    in y over 8 cells, fluid falling through the seam."""
+    dtype = np.float32
+    r = 0.01
+    cn = scenes.make_const(dtype, r)
+    h = float(cn.kernel_radius)
+    L = 8 * h
+    R, centre = 0.1, 0.15
+    ys = -L / 2 + r + 2 * r * np.arange(int(round(L / (2 * r))))
+    rings = []
+    for k in range(3):
+        rho = R + r + 2 * r * k
+        m = int(round(2 * np.pi * rho / (2 * r)))
+        th = 2 * np.pi * np.arange(m) / m
+        ring = np.stack([rho * np.cos(th), np.zeros(m), rho * np.sin(th)], 1)
+        for y in ys:
+            rings.append(ring + np.array([0.0, y, 0.0]))
+    local = np.concatenate(rings).astype(dtype)
+    a = np.arange(centre - R + 1.5 * r, centre + R - r, 2 * r)
+    fy = -L / 2 + 1e-4 + 2 * r * np.arange(int(round(L / (2 * r))))
+    X, Y, Z = np.meshgrid(a, fy, a, indexing="ij")
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    x = x[np.hypot(x[:, 0] - centre, x[:, 2] - centre) < R - r].astype(dtype)
+    v = np.zeros_like(x)
+    v[:, 1] = -2.0
+    cni = scenes.make_consti((0.0, -L / 2, 0.0), (0.3, L / 2, 0.3), h, 1)
+    cni.grid_offset[1] = -4
+    cni.grid_res[1] = 8
+    body = _body(dtype, 0.0, (1, 1, 1), 0.0)
+    barr = (type(body) * 1)(body)
+    rarr = (type(scenes.rigid_state(dtype)) * 1)(scenes.rigid_state(dtype, x=(centre, 0.0, centre)))
+    rarr_o = (type(rarr[0]) * 1)(rarr[0])
+    sp = scenes.solver_params(wrap_y=1, wrap_length=L)
+    steps = 3
+    ref = _oracle_run(dtype, cn, cni, x, barr, rarr_o, local, [len(local)], sp, 1e-4, steps, v=v)
+    got = _device_run(engine, dtype, cn, cni, x, barr, rarr, local, [len(local)], sp, 1e-4, steps,
+                      v=v)
+    for rr, o in zip(got["reps"], ref["reps"]):
+        assert rr.num_density_solve == o.num_density_solve
+        assert list(rr.grid_anomaly) == [0, 0, 0]
+    crossed = (x[:, 1] < -L / 2 + 1e-3) & (got["x"][:, 1] > L / 2 - 3e-3)
+    assert crossed.sum() > 10
+    dx = got["x"].astype(np.float64) - ref["x"]
+    dx[:, 1] -= L * np.round(dx[:, 1] / L)
+    assert np.abs(dx).max() <= 5e-5 * 0.3
+    _close(got["v"], ref["v"], 1e-2, "v")
+    _close(got["density"], ref["density"], 5e-3, "density")
+    _close(got["pressure"], ref["pressure"], 5e-2, "pressure")
