@@ -304,6 +304,8 @@ for _s in ("f32", "f64"):
     _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])
     _SIGNATURES["al_update_particle_neighbors_" + _s] = (
         ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P, _P])
+    _SIGNATURES["al_update_particle_neighbors_periodic_" + _s] = (
+        ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P, ctypes.c_double, _P])
     _SIGNATURES["al_compute_particle_boundary_" + _s] = (
         ctypes.c_int, [_P, _P, _U, _P, _P, _P, _U, _P, _P, _P])
     _SIGNATURES["al_build_volume_field_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _P])

@@ -326,7 +326,8 @@ int grid_sort_impl(al_engine* e, const C* cn, const al_consti* cni, const TF* x,
 template <class TF, class C>
 int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const TF* x,
                           uint32_t n, const TF* boundary_kernel, TF* density, uint32_t* num_nbr,
-                          TF* neighbors, uint32_t* grid_anomaly, void* stream) {
+                          TF* neighbors, uint32_t* grid_anomaly, void* stream,
+                          double wrap_length = 0) {
   ALB_CHECK_ARG(e && cn && ((x && num_nbr) || n == 0),
                 "al_update_particle_neighbors: null argument");
   ALB_TRY(check_consti(cni));
@@ -335,6 +336,7 @@ int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const
   ALB_TRY(e->activate());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   Cn<TF> c = to_cn<TF>(*cn);
+  if (wrap_length > 0) set_wrap(c, TF(wrap_length));  // update_particle_neighbors<1>
   GridDims g = to_dims(*cni);
   vec4<TF>* xs = nullptr;
   uint32_t *flags = nullptr, *nbr = nullptr, *ncount = nullptr;
@@ -349,7 +351,7 @@ int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const
   ALB_TRY(grid_build<TF>(e, c, g, x, n, xs, flags, gs, st));
   RefBoundaryKernel<TF> bk{boundary_kernel, gs.perm, n, g.nb};
   ALB_TRY(build_neighbors_density<TF>(c, g, gs, xs, bk, nbr, ncount, rho, nullptr, nullptr, st));
-  ALB_TRY(export_neighbors<TF>(g, gs, xs, nbr, ncount, rho, neighbors, num_nbr, density, st));
+  ALB_TRY(export_neighbors<TF>(c, g, gs, xs, nbr, ncount, rho, neighbors, num_nbr, density, st));
   if (grid_anomaly)
     ALB_CUDA(cudaMemcpyAsync(grid_anomaly, flags, 3 * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                              st));
@@ -398,6 +400,35 @@ int al_update_particle_neighbors_f64(al_engine* engine, const al_const_f64* cn,
                                        particle_boundary_kernel, particle_density,
                                        particle_num_neighbors, particle_neighbors, grid_anomaly,
                                        stream);
+}
+
+int al_update_particle_neighbors_periodic_f32(al_engine* engine, const al_const_f32* cn,
+                                              const al_consti* cni, const float* particle_x,
+                                              uint32_t num_particles,
+                                              const float* particle_boundary_kernel,
+                                              float* particle_density,
+                                              uint32_t* particle_num_neighbors,
+                                              float* particle_neighbors, uint32_t* grid_anomaly,
+                                              double wrap_length, void* stream) {
+  ALB_CHECK_ARG(wrap_length > 0, "al_update_particle_neighbors_periodic: wrap_length <= 0");
+  return update_neighbors_impl<float>(engine, cn, cni, particle_x, num_particles,
+                                      particle_boundary_kernel, particle_density,
+                                      particle_num_neighbors, particle_neighbors, grid_anomaly,
+                                      stream, wrap_length);
+}
+int al_update_particle_neighbors_periodic_f64(al_engine* engine, const al_const_f64* cn,
+                                              const al_consti* cni, const double* particle_x,
+                                              uint32_t num_particles,
+                                              const double* particle_boundary_kernel,
+                                              double* particle_density,
+                                              uint32_t* particle_num_neighbors,
+                                              double* particle_neighbors, uint32_t* grid_anomaly,
+                                              double wrap_length, void* stream) {
+  ALB_CHECK_ARG(wrap_length > 0, "al_update_particle_neighbors_periodic: wrap_length <= 0");
+  return update_neighbors_impl<double>(engine, cn, cni, particle_x, num_particles,
+                                       particle_boundary_kernel, particle_density,
+                                       particle_num_neighbors, particle_neighbors, grid_anomaly,
+                                       stream, wrap_length);
 }
 
 }  // extern "C"

@@ -10,7 +10,8 @@ namespace {
 inline uint32_t blocks_for(uint32_t n, int block) { return (n + block - 1) / block; }
 
 template <class TF>
-__global__ void k_export_neighbors(uint32_t cap, uint32_t n, const uint32_t* __restrict__ perm,
+__global__ void k_export_neighbors(Cn<TF> c, uint32_t cap, uint32_t n,
+                                   const uint32_t* __restrict__ perm,
                                    const uint32_t* __restrict__ inv,
                                    const vec4<TF>* __restrict__ xs,
                                    const uint32_t* __restrict__ nbr,
@@ -30,9 +31,10 @@ __global__ void k_export_neighbors(uint32_t cap, uint32_t n, const uint32_t* __r
     const uint32_t j = perm[t];
     const vec3<TF> xj = xyz(xs[t]);
     TF* e = out_nbr + (size_t(i) * cap + k) * 4;
-    e[0] = sub_rn(xi.x, xj.x);
-    e[1] = sub_rn(xi.y, xj.y);
-    e[2] = sub_rn(xi.z, xj.z);
+    const vec3<TF> d = pdisp(c, xi, xj);  // wrapped in y on a periodic update
+    e[0] = d.x;
+    e[1] = d.y;
+    e[2] = d.z;
     if constexpr (sizeof(TF) == 4) {
       e[3] = __uint_as_float(j);
     } else {
@@ -71,13 +73,14 @@ int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState&
 }
 
 template <class TF>
-int export_neighbors(const GridDims& g, const GridState& gs, const vec4<TF>* xs,
+int export_neighbors(const Cn<TF>& c, const GridDims& g, const GridState& gs,
+                     const vec4<TF>* xs,
                      const uint32_t* nbr, const uint32_t* ncount, const TF* rho_sorted,
                      TF* particle_neighbors, uint32_t* particle_num_neighbors,
                      TF* particle_density, cudaStream_t st) {
   if (gs.n == 0) return AL_OK;
   k_export_neighbors<TF><<<blocks_for(gs.n, kBlock), kBlock, 0, st>>>(
-      g.cap_nbr, gs.n, gs.perm, gs.inv, xs, nbr, ncount, rho_sorted, particle_neighbors,
+      c, g.cap_nbr, gs.n, gs.perm, gs.inv, xs, nbr, ncount, rho_sorted, particle_neighbors,
       particle_num_neighbors, particle_density);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
@@ -92,10 +95,12 @@ ALB_INST(double, RefBoundaryKernel)
 ALB_INST(float, SortedBoundaryKernel)
 ALB_INST(double, SortedBoundaryKernel)
 #undef ALB_INST
-template int export_neighbors<float>(const GridDims&, const GridState&, const vec4<float>*,
+template int export_neighbors<float>(const Cn<float>&, const GridDims&, const GridState&,
+                                     const vec4<float>*,
                                      const uint32_t*, const uint32_t*, const float*, float*,
                                      uint32_t*, float*, cudaStream_t);
-template int export_neighbors<double>(const GridDims&, const GridState&, const vec4<double>*,
+template int export_neighbors<double>(const Cn<double>&, const GridDims&, const GridState&,
+                                      const vec4<double>*,
                                       const uint32_t*, const uint32_t*, const double*, double*,
                                       uint32_t*, double*, cudaStream_t);
 

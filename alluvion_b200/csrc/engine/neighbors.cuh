@@ -86,7 +86,8 @@ int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState&
 // particle_neighbors [N][cap][4] {x_i - x_j, bits(j)} (if non-null),
 // particle_num_neighbors [N], particle_density [N] (if non-null).
 template <class TF>
-int export_neighbors(const GridDims& g, const GridState& gs, const vec4<TF>* xs,
+int export_neighbors(const Cn<TF>& c, const GridDims& g, const GridState& gs,
+                     const vec4<TF>* xs,
                      const uint32_t* nbr, const uint32_t* ncount, const TF* rho_sorted,
                      TF* particle_neighbors, uint32_t* particle_num_neighbors,
                      TF* particle_density, cudaStream_t st);

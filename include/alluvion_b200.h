@@ -352,6 +352,22 @@ AL_API int al_update_particle_neighbors_f64(
     const double* particle_boundary_kernel, double* particle_density,
     uint32_t* particle_num_neighbors, double* particle_neighbors,
     uint32_t* grid_anomaly, void* stream);
+/* update_particle_neighbors<1> (launch_make_neighbor_list_wrap1): the same,
+ * periodic in y -- neighbor cells wrap (wrap_ipos_y, runner.hpp:689-697) and
+ * the entries' x_i - x_j are wrapped into [-wrap_length/2, wrap_length/2)
+ * (wrap_y, runner.hpp:698-707).  The grid's y extent must be the period. */
+AL_API int al_update_particle_neighbors_periodic_f32(
+    al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+    const float* particle_x, uint32_t num_particles,
+    const float* particle_boundary_kernel, float* particle_density,
+    uint32_t* particle_num_neighbors, float* particle_neighbors,
+    uint32_t* grid_anomaly, double wrap_length, void* stream);
+AL_API int al_update_particle_neighbors_periodic_f64(
+    al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+    const double* particle_x, uint32_t num_particles,
+    const double* particle_boundary_kernel, double* particle_density,
+    uint32_t* particle_num_neighbors, double* particle_neighbors,
+    uint32_t* grid_anomaly, double wrap_length, void* stream);
 
 /* ------------------------------------------------------ boundary sampling
  * compute_all_boundaries (solver.hpp:170-185): for every body b and

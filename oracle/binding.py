@@ -40,6 +40,8 @@ def lib():
             sig["orc_grid_sort_" + s] = (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P])
             sig["orc_update_particle_neighbors_" + s] = (
                 ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P, _P, _P])
+            sig["orc_update_particle_neighbors_periodic_" + s] = (
+                ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P, _P, _P, ctypes.c_double])
             sig["orc_node_positions_" + s] = (None, [_P, _P, _P, _P])
             sig["orc_distance_grid_" + s] = (None, [_P, _P])
             sig["orc_volume_field_" + s] = (None, [_P, _P, _P])
@@ -129,9 +131,10 @@ def grid_sort(cn, cni, x):
     return cell, perm, start, flags[:2]
 
 
-def update_particle_neighbors(cn, cni, x, boundary_kernel=None):
+def update_particle_neighbors(cn, cni, x, boundary_kernel=None, wrap_length=None):
     """Returns density [n], count [n], index [n, cap] (original indices,
-    canonical order, 0xffffffff padding), neighbors [n, cap, 4], flags[3]."""
+    canonical order, 0xffffffff padding), neighbors [n, cap, 4], flags[3].
+    wrap_length: periodic in y (update_particle_neighbors<1>)."""
     x = np.ascontiguousarray(x)
     n = x.shape[0]
     cap = cni.max_num_neighbors_per_particle
@@ -141,9 +144,13 @@ def update_particle_neighbors(cn, cni, x, boundary_kernel=None):
     nbrs = np.zeros((n, cap, 4), x.dtype)
     flags = np.zeros(4, np.uint32)
     bk = None if boundary_kernel is None else np.ascontiguousarray(boundary_kernel, x.dtype)
-    getattr(lib(), "orc_update_particle_neighbors_" + _sfx(x.dtype))(
-        _p(cn), _p(cni), _p(x), n, _p(bk), _p(density), _p(count), _p(index), _p(nbrs),
-        _p(flags))
+    args = (_p(cn), _p(cni), _p(x), n, _p(bk), _p(density), _p(count), _p(index), _p(nbrs),
+            _p(flags))
+    if wrap_length is None:
+        getattr(lib(), "orc_update_particle_neighbors_" + _sfx(x.dtype))(*args)
+    else:
+        getattr(lib(), "orc_update_particle_neighbors_periodic_" + _sfx(x.dtype))(
+            *args, float(wrap_length))
     return density, count, index, nbrs, flags[:3]
 
 

@@ -82,10 +82,14 @@ int grid_sort_impl(const C* cn, const al_consti* cni, const TF* x, uint32_t n, u
 template <class TF, class C>
 int neighbors_impl(const C* cn, const al_consti* cni, const TF* x, uint32_t n,
                    const TF* boundary_kernel, TF* density, uint32_t* count, uint32_t* index,
-                   TF* neighbors, uint32_t* flags) {
+                   TF* neighbors, uint32_t* flags, double wrap_length = 0) {
   Cn<TF> c = make_cn<TF>(*cn);
   Fluid<TF> f;
   load_fluid<TF>(f, n, cni->num_boundaries, x, nullptr);
+  if (wrap_length > 0) {  // update_particle_neighbors<1>
+    f.wrap = true;
+    f.wrap_len = TF(wrap_length);
+  }
   if (boundary_kernel)
     for (size_t k = 0; k < size_t(f.nb) * n; ++k)
       f.bk[k] = V4<TF>{boundary_kernel[4 * k], boundary_kernel[4 * k + 1],
@@ -100,7 +104,7 @@ int neighbors_impl(const C* cn, const al_consti* cni, const TF* x, uint32_t n,
       if (index) index[size_t(i) * cap + k] = k < f.nl.count[i] ? j : 0xffffffffu;
       if (neighbors && k < f.nl.count[i]) {
         TF* e = neighbors + (size_t(i) * cap + k) * 4;
-        V3<TF> d = f.x[i] - f.x[j];
+        V3<TF> d = xv(f, i, j);
         e[0] = d.x;
         e[1] = d.y;
         e[2] = d.z;
@@ -359,6 +363,22 @@ int orc_update_particle_neighbors_f64(const al_const_f64* cn, const al_consti* c
                                       double* neighbors, uint32_t* flags) {
   return neighbors_impl<double>(cn, cni, x, n, boundary_kernel, density, count, index, neighbors,
                                 flags);
+}
+int orc_update_particle_neighbors_periodic_f32(const al_const_f32* cn, const al_consti* cni,
+                                               const float* x, uint32_t n, const float* bk,
+                                               float* density, uint32_t* count, uint32_t* index,
+                                               float* neighbors, uint32_t* flags,
+                                               double wrap_length) {
+  return neighbors_impl<float>(cn, cni, x, n, bk, density, count, index, neighbors, flags,
+                               wrap_length);
+}
+int orc_update_particle_neighbors_periodic_f64(const al_const_f64* cn, const al_consti* cni,
+                                               const double* x, uint32_t n, const double* bk,
+                                               double* density, uint32_t* count, uint32_t* index,
+                                               double* neighbors, uint32_t* flags,
+                                               double wrap_length) {
+  return neighbors_impl<double>(cn, cni, x, n, bk, density, count, index, neighbors, flags,
+                                wrap_length);
 }
 
 uint32_t orc_num_grid_nodes(const uint32_t* res) { return num_grid_nodes(res); }

@@ -182,3 +182,46 @@ def test_large_block_properties(engine):
     assert np.all(perm[1:][same] > perm[:-1][same])  # stable within a cell
     o_cell, o_perm, o_start, _ = orc.grid_sort(cn, cni, x)
     assert np.array_equal(perm, o_perm)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_periodic_neighbors_bit_exact(engine, dtype):
+    """update_particle_neighbors<1>: a slab filling a period of 8 cells in y;
+    lists (order, wrapped displacement bits) bit-exact against the oracle,
+    and particles on both sides of the seam see each other."""
+    r = 0.01
+    cn = scenes.make_const(dtype, r)
+    h = float(cn.kernel_radius)
+    L = 8 * h
+    x = scenes.fluid_block((6, 16, 6), (0.0, -L / 2 - 2 * r + 0.5 * r, 0.0), r, dtype, seed=9)
+    cni = scenes.make_consti((0.0, -L / 2, 0.0), (0.15, L / 2, 0.15), h)
+    cni.grid_offset[1] = -4
+    cni.grid_res[1] = 8
+    n, cap = len(x), cni.max_num_neighbors_per_particle
+    xd = dev(x)
+    rho = torch.zeros(n, dtype=xd.dtype, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nbr = torch.zeros((n, cap, 4), dtype=xd.dtype, device="cuda")
+    fn = getattr(_capi.lib(), "al_update_particle_neighbors_periodic_" + _capi.suffix(dtype))
+    st = fn(engine.handle, ctypes.byref(cn), ctypes.byref(cni), _capi.ptr(xd), n, None,
+            _capi.ptr(rho), _capi.ptr(cnt), _capi.ptr(nbr), None, ctypes.c_double(L), None)
+    assert st == _capi.AL_OK
+    o_rho, o_cnt, o_idx, o_nbrs, o_flags = orc.update_particle_neighbors(cn, cni, x,
+                                                                        wrap_length=L)
+    g_cnt = host(cnt).view(np.uint32)
+    g_nbr = host(nbr)
+    assert np.array_equal(g_cnt, o_cnt)
+    idx = _index_bits(g_nbr, dtype)
+    for i in range(n):
+        c = g_cnt[i]
+        assert np.array_equal(idx[i, :c], o_idx[i, :c]), i
+        assert np.array_equal(g_nbr[i, :c, :3], o_nbrs[i, :c, :3]), i
+    np.testing.assert_allclose(host(rho), o_rho, rtol=RTOL[dtype])
+    # across the seam: the bottom layer's neighbours include top-layer particles,
+    # at wrapped (small) displacements
+    bottom = x[:, 1] < -L / 2 + 0.01
+    top_ids = set(np.nonzero(x[:, 1] > L / 2 - 0.02)[0].tolist())
+    i = int(np.nonzero(bottom)[0][len(np.nonzero(bottom)[0]) // 2])
+    ids = set(idx[i, :g_cnt[i]].tolist())
+    assert ids & top_ids
+    assert np.abs(g_nbr[i, :g_cnt[i], 1]).max() < h
