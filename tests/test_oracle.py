@@ -229,3 +229,47 @@ def test_neighbor_list_matches_brute_force():
         expect = set(np.nonzero((d2[i] < h2) & (np.arange(len(x)) != i))[0].tolist())
         got = set(index[i, :count[i]].tolist())
         assert got == expect
+
+
+@pytest.mark.parametrize("method", ["ii", "i", "df"])
+def test_oracle_hydrostatic_column(method):
+    """The oracle's steps on the resting water column of
+    test_gpu_hydrostatic.py (unjittered 10 x 20 x 10 lattice, outer layers
+    2.9 r from the box walls, 1500 steps at dt 2e-4): the column stays near
+    rest, its interior at rho0, and for the pressure solvers the stored
+    pressure (physical pressure over rho0) grows with depth at about g."""
+    dtype = np.float32
+    r = 0.01
+    lattice = (10, 20, 10)
+    gap = 2.9 * r
+    cn = scenes.make_const(dtype, r)
+    h = float(cn.kernel_radius)
+    x = scenes.fluid_block(lattice, (gap - 2 * r,) * 3, r, dtype, jitter=0.0)
+    size = 2 * r * (np.asarray(lattice) - 1) + 2 * gap
+    size[1] += 0.2
+    body = scenes.make_body(dtype, cn, _capi.SHAPE_BOX, scenes.box_params(size), 32, sign=-1.0)
+    vol = orc.volume_field(cn, body, dtype)
+    body.volume_nodes = vol.ctypes.data
+    bodies = (type(body) * 1)(body)
+    rigid = scenes.rigid_array(dtype, [scenes.rigid_state(dtype, x=tuple(size / 2))])
+    cni = scenes.make_consti(-0.5 * h * np.ones(3), size + 0.5 * h, h, 1)
+    n = len(x)
+    z = lambda *s: np.zeros(s, dtype)
+    st = dict(x=x.copy(), v=z(n, 3), a=z(n, 3), kappa=z(n), kappa_v=z(n), density=z(n),
+              density_adv=z(n), pressure=z(n))
+    dt, reps = orc.run(method, cn, cni, bodies, rigid.reshape(-1, 13), st,
+                       scenes.solver_params(), 2e-4, 1500)
+    speed = np.linalg.norm(st["v"], axis=1)
+    assert np.percentile(speed, 95) < 0.1
+    rho = st["density"]
+    dense = rho > 990.0
+    assert dense.mean() > 0.9 and abs(rho[dense].mean() / 1000.0 - 1) < 2e-3
+    if method == "df":
+        return
+    xx, p = st["x"], st["pressure"]
+    depth = xx[:, 1].max() - xx[:, 1]
+    inner = (np.abs(xx[:, 0] - xx[:, 0].mean()) < 0.05) & \
+            (np.abs(xx[:, 2] - xx[:, 2].mean()) < 0.05) & (depth > 0.08) & \
+            (xx[:, 1] > xx[:, 1].min() + 0.05)
+    slope = np.polyfit(depth[inner], p[inner], 1)[0]
+    assert slope == pytest.approx(9.81, rel=0.15)
