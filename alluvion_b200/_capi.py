@@ -274,6 +274,10 @@ _SIGNATURES = {
     "al_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "al_last_error": (ctypes.c_char_p, []),
     "al_engine_synchronize": (ctypes.c_int, [_P, _P]),
+    "al_allocate": (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
+    "al_free": (ctypes.c_int, [_P, _P]),
+    "al_copy": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t]),
+    "al_set": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_size_t]),
     "al_engine_set_graph_mode": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_engine_graph_stats": (ctypes.c_int, [_P, _P, _P]),
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),

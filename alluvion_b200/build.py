@@ -2,6 +2,9 @@
 
   alluvion_b200/liballuvion_b200.so   CUDA kernels + the C ABI of
                                       include/alluvion_b200.h (nvcc)
+  alluvion_b200/_alluvion_b200*.so    pybind11 module: the reference's Python
+                                      object model (Store, Pile, SolverDf, ...)
+                                      over include/alluvion_b200_solver.hpp (g++)
 
 Usage: python -m alluvion_b200.build [--force] [--verbose]
 """
@@ -69,8 +72,37 @@ def build_engine(force=False, verbose=False, ptxas_info=False):
     return ENGINE_LIB
 
 
+PY_SRC = os.path.join(PKG, "csrc", "py", "pyalluvion_b200.cpp")
+
+
+def pymodule_path():
+    import sysconfig
+    return os.path.join(PKG, "_alluvion_b200" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_pymodule(force=False, verbose=False):
+    """Compiles the pybind11 module against liballuvion_b200.so (host code
+    only: the C++ layer calls the C ABI); returns its path."""
+    import sysconfig
+    import pybind11
+    out = pymodule_path()
+    deps = [PY_SRC, ENGINE_LIB, os.path.join(INCLUDE, "alluvion_b200.h"),
+            os.path.join(INCLUDE, "alluvion_b200.hpp"),
+            os.path.join(INCLUDE, "alluvion_b200_solver.hpp")]
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= _newest(deps):
+        return out
+    tmp = out + ".tmp"
+    _run([os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-shared", "-fPIC",
+          "-fvisibility=hidden", "-I", INCLUDE, "-I", pybind11.get_include(),
+          "-I", sysconfig.get_paths()["include"], PY_SRC, "-o", tmp,
+          "-L", PKG, "-lalluvion_b200", "-Wl,-rpath,$ORIGIN"], verbose)
+    os.replace(tmp, out)
+    return out
+
+
 def build_all(force=False, verbose=False):
-    return [build_engine(force=force, verbose=verbose)]
+    return [build_engine(force=force, verbose=verbose),
+            build_pymodule(force=force, verbose=verbose)]
 
 
 if __name__ == "__main__":

@@ -211,6 +211,47 @@ int al_engine_synchronize(al_engine* engine, void* stream) {
   return engine->flush_stats();
 }
 
+int al_allocate(al_engine* engine, void** ptr, size_t bytes) {
+  ALB_CHECK_ARG(engine && ptr, "al_allocate: null argument");
+  *ptr = nullptr;
+  if (bytes == 0) return AL_OK;
+  ALB_TRY(engine->activate());
+  if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    set_error("al_allocate: cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    return AL_ERR_ALLOC;
+  }
+  return AL_OK;
+}
+
+int al_free(al_engine* engine, void* ptr) {
+  ALB_CHECK_ARG(engine != nullptr, "al_free: engine is null");
+  if (!ptr) return AL_OK;
+  ALB_TRY(engine->activate());
+  ALB_CUDA(cudaFree(ptr));
+  return AL_OK;
+}
+
+int al_copy(al_engine* engine, void* dst, const void* src, size_t bytes) {
+  ALB_CHECK_ARG(engine != nullptr, "al_copy: engine is null");
+  if (bytes == 0) return AL_OK;
+  ALB_CHECK_ARG(dst && src, "al_copy: null pointer");
+  ALB_TRY(engine->activate());
+  ALB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+  return AL_OK;
+}
+
+int al_set(al_engine* engine, void* dst, int value, size_t bytes) {
+  ALB_CHECK_ARG(engine != nullptr, "al_set: engine is null");
+  if (bytes == 0) return AL_OK;
+  ALB_CHECK_ARG(dst != nullptr, "al_set: null pointer");
+  ALB_TRY(engine->activate());
+  ALB_CUDA(cudaMemset(dst, value, bytes));
+  ALB_CUDA(cudaDeviceSynchronize());
+  return AL_OK;
+}
+
 int al_engine_set_graph_mode(al_engine* engine, int enable) {
   ALB_CHECK_ARG(engine != nullptr, "al_engine_set_graph_mode: engine is null");
   engine->graph_mode = enable != 0;

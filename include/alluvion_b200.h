@@ -247,6 +247,17 @@ AL_API const char* al_last_error(void);
 /* Blocks until all work the engine queued on `stream` has finished. */
 AL_API int al_engine_synchronize(al_engine* engine, void* stream);
 
+/* Device memory on the engine's device, the counterpart of the reference's
+ * Allocator (allocator.hpp:13-24, 45-74: allocate, free, copy, set), for
+ * hosts without a CUDA runtime of their own (the C++ Store of
+ * alluvion_b200_solver.hpp).  al_allocate of 0 bytes gives NULL; al_copy
+ * copies between any host or device addresses (unified addressing) and,
+ * like al_set, returns after the copy has completed. */
+AL_API int al_allocate(al_engine* engine, void** ptr, size_t bytes);
+AL_API int al_free(al_engine* engine, void* ptr);
+AL_API int al_copy(al_engine* engine, void* dst, const void* src, size_t bytes);
+AL_API int al_set(al_engine* engine, void* dst, int value, size_t bytes);
+
 /* Step graphs.  With graph mode on (the default), the second and later
  * al_*_step calls with the same constants, grid descriptor, fluid buffer
  * table, body count and enabled solves replay one captured CUDA graph: the

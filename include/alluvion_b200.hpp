@@ -89,6 +89,8 @@ struct real<float> {
   static constexpr auto i_step = al_i_step_f32;
   static constexpr auto i_step_pellets = al_i_step_pellets_f32;
   static constexpr auto update_particle_neighbors = al_update_particle_neighbors_f32;
+  static constexpr auto update_particle_neighbors_periodic =
+      al_update_particle_neighbors_periodic_f32;
   static constexpr auto compute_particle_boundary = al_compute_particle_boundary_f32;
   static constexpr auto build_volume_field = al_build_volume_field_f32;
   static constexpr auto build_distance_grid = al_build_distance_grid_f32;
@@ -105,6 +107,8 @@ struct real<double> {
   static constexpr auto i_step = al_i_step_f64;
   static constexpr auto i_step_pellets = al_i_step_pellets_f64;
   static constexpr auto update_particle_neighbors = al_update_particle_neighbors_f64;
+  static constexpr auto update_particle_neighbors_periodic =
+      al_update_particle_neighbors_periodic_f64;
   static constexpr auto compute_particle_boundary = al_compute_particle_boundary_f64;
   static constexpr auto build_volume_field = al_build_volume_field_f64;
   static constexpr auto build_distance_grid = al_build_distance_grid_f64;

@@ -1,0 +1,174 @@
+"""The reference's Python object model (Depot / Store / Pile / SolverDf /
+SolverIi / SolverI, alluvion/depot.py and lib/pyalluvion.cu) over the
+engine, through the pybind11 module.  A scene built the reference's way
+(Depot, Pile.add with analytic distances, solver fields) must step exactly
+as the same scene driven through the C ABI: same constants, grids, bodies
+and parameters reach the same entry points, so positions, velocities, dt
+and rigid kinematics agree bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+from alluvion_b200 import _capi, scenes
+from alluvion_b200.depot import Depot
+
+pytestmark = pytest.mark.gpu
+
+R = 0.01
+LATTICE = (8, 12, 8)
+SIZE = (0.3, 0.4, 0.3)
+SPHERE = dict(x=(0.15, 0.33, 0.15), r=0.04, rho=700.0)
+
+
+def _abi_scene(engine, dtype):
+    x = scenes.fluid_block(LATTICE, (0.02, 0.02, 0.02), R, dtype, seed=5)
+    cn = scenes.make_const(dtype, R)
+    h = float(cn.kernel_radius)
+    mass = SPHERE["rho"] * 4 / 3 * np.pi * SPHERE["r"] ** 3
+    bodies = [dict(shape=_capi.SHAPE_BOX, params=scenes.box_params(SIZE), sign=-1.0,
+                   resolution=24, use_distance_grid=False, mass=0.0,
+                   x=tuple(np.asarray(SIZE) / 2)),
+              dict(shape=_capi.SHAPE_SPHERE, params=[SPHERE["r"]], sign=1.0, resolution=16,
+                   use_distance_grid=False, mass=mass,
+                   inertia=scenes.sphere_inertia(mass, SPHERE["r"]), x=SPHERE["x"])]
+    cni = scenes.make_consti(-0.5 * h * np.ones(3), np.asarray(SIZE) + 0.5 * h, h, len(bodies))
+    return scenes.DeviceScene(engine, dtype, cn, cni, x, bodies), x, mass
+
+
+def _depot_scene(dtype, x, abi, mass, method="df"):
+    dp = Depot(dtype)
+    cn, cni = dp.cn, dp.cni
+    h = 4 * R
+    cn.set_kernel_radius(h)
+    cn.set_particle_attr(R, 1000.0 * (2 * R) ** 3, 1000.0)
+    cn.viscosity = 0.01
+    cn.boundary_viscosity = 0.01
+    cn.dfsph_factor_epsilon = 1e-6
+    cn.gravity = (0.0, -9.81, 0.0)
+    cni.grid_res = list(abi.cni.grid_res)
+    cni.grid_offset = list(abi.cni.grid_offset)
+    cni.max_num_particles_per_cell = abi.cni.max_num_particles_per_cell
+    cni.max_num_neighbors_per_particle = abi.cni.max_num_neighbors_per_particle
+    dp.copy_cn()
+    runner = dp.Runner()
+    pile = dp.Pile(dp, runner, 0)
+    pile.add(dp.BoxDistance.create(SIZE), [24, 24, 24], sign=-1, x=list(np.asarray(SIZE) / 2))
+    pile.add(dp.SphereDistance.create(SPHERE["r"]), [16, 16, 16], mass=mass,
+             inertia_tensor=list(scenes.sphere_inertia(mass, SPHERE["r"])), x=list(SPHERE["x"]))
+    pile.set_gravity((0.0, -9.81, 0.0))
+    cls = {"df": dp.SolverDf, "ii": dp.SolverIi, "i": dp.SolverI}[method]
+    solver = cls(runner, pile, dp, max_num_particles=len(x) + 100)
+    solver.num_particles = len(x)
+    solver.particle_x.set(x)
+    solver.particle_v.set_zero()
+    solver.reset_solving_var()
+    solver.initial_dt = 2e-4
+    solver.reset_t()
+    solver.max_dt = 2e-4
+    solver.cfl = 0.4
+    return dp, pile, solver
+
+
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_depot_steps_match_the_c_abi(engine, method, dtype):
+    abi, x, mass = _abi_scene(engine, dtype)
+    dp, pile, solver = _depot_scene(dtype, x, abi, mass, method)
+    sp = scenes.solver_params()
+    dt = 2e-4
+    T = np.dtype(dtype).type
+    t = T(0)
+    for k in range(4):
+        dt, rep = abi.step(method, sp, dt)
+        solver.step()
+        assert solver.dt == dt
+        t = T(t + T(dt))
+    st = abi.state()
+    n = len(x)
+    gx = solver.particle_x.get()[:n]
+    gv = solver.particle_v.get()[:n]
+    np.testing.assert_array_equal(gx, st["x"])
+    np.testing.assert_array_equal(gv, st["v"])
+    np.testing.assert_array_equal(solver.particle_density.get()[:n], st["density"])
+    if method == "df":
+        np.testing.assert_array_equal(solver.particle_kappa.get()[:n], st["kappa"])
+        assert solver.num_density_solve == rep.num_density_solve
+        assert solver.num_divergence_solve == rep.num_divergence_solve
+    else:
+        np.testing.assert_array_equal(solver.particle_pressure.get()[:n], st["pressure"])
+        assert solver.num_density_solve == rep.num_density_solve
+    # the sphere's kinematics: same device integration, written back to the pile
+    rig = abi.rigid[1]
+    np.testing.assert_array_equal(np.asarray(pile.x[1], dtype), np.asarray(rig.x[:], dtype))
+    np.testing.assert_array_equal(np.asarray(pile.v[1], dtype), np.asarray(rig.v[:], dtype))
+    np.testing.assert_array_equal(np.asarray(pile.q[1], dtype), np.asarray(rig.q[:], dtype))
+    assert pile.x[1][1] < SPHERE["x"][1]  # it falls
+    assert solver.t == t
+    assert solver.max_v2 > 0 and solver.utilized_cfl > 0
+
+
+def test_variables_and_neighbors(engine):
+    dtype = np.float32
+    abi, x, mass = _abi_scene(engine, dtype)
+    dp, pile, solver = _depot_scene(dtype, x, abi, mass)
+    n = len(x)
+    # Coated get / set, byte offsets, zero-copy torch views
+    v = dp.create([n], 3)
+    assert v.get_shape() == [n] and v.get_num_primitives_per_element() == 3
+    a = np.arange(3 * n, dtype=np.float32).reshape(n, 3)
+    v.set(a)
+    np.testing.assert_array_equal(v.get(), a)
+    t = torch.as_tensor(v, device="cuda")
+    assert t.shape == (n, 3) and t.dtype == torch.float32
+    t.mul_(2)
+    np.testing.assert_array_equal(v.get(), 2 * a)
+    v.set(np.ones((1, 3), np.float32), offset=12)
+    g = v.get()
+    assert (g[1] == 1).all()
+    np.testing.assert_array_equal(g[0], 2 * a[0])
+    np.testing.assert_array_equal(g[2:], 2 * a[2:])
+    with pytest.raises(RuntimeError):
+        v.set(np.ones((n + 1, 3), np.float32))
+    u = dp.create(4, 1, np.uint32)
+    u.set(np.array([1, 2, 3, 4], np.uint32))
+    assert u.get().tolist() == [1, 2, 3, 4]
+    dp.remove(u)
+    assert u.get_linear_shape() == 0
+    # the standalone neighbor update in the reference layout (density with
+    # the boundary terms of compute_all_boundaries)
+    solver.compute_all_boundaries()
+    solver.update_particle_neighbors()
+    assert solver.grid_anomaly.get().tolist() == [0, 0, 0]
+    nbr = solver.particle_neighbors.get()
+    cnt = solver.particle_num_neighbors.get()[:n]
+    from oracle import binding as orc
+    odens, ocount, oindex, _, flags = orc.update_particle_neighbors(abi.cn, abi.cni, x)
+    np.testing.assert_array_equal(cnt, ocount)
+    j = nbr[:n, :, 3].view(np.uint32)
+    for i in range(0, n, 97):
+        assert j[i, :cnt[i]].tolist() == oindex[i, :cnt[i]].tolist()
+
+
+def test_unsupported_options_raise(engine):
+    dp = Depot(np.float32)
+    dp.cn.set_kernel_radius(0.04)
+    dp.cn.set_particle_attr(0.01, 0.008, 1000.0)
+    dp.cni.grid_res = [8, 8, 8]
+    dp.cni.max_num_neighbors_per_particle = 64
+    dp.cni.max_num_particles_per_cell = 64
+    runner = dp.Runner()
+    pile = dp.Pile(dp, runner, 0)
+    with pytest.raises(RuntimeError):
+        dp.SolverDf(runner, pile, dp, 100, enable_vorticity=True)
+    with pytest.raises(RuntimeError):
+        dp.Pile(dp, runner, 0, volume_method=dp_volume_pellets())
+    s = dp.SolverDf(runner, pile, dp, 100)
+    s.num_particles = 101
+    s.dt = 1e-4
+    with pytest.raises(RuntimeError):
+        s.step()
+
+
+def dp_volume_pellets():
+    from alluvion_b200.depot import VolumeMethod
+    return VolumeMethod.pellets
