@@ -209,6 +209,26 @@ class SampleF32(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class SampleF64(ctypes.Structure):
+    """al_sample_f64: the double-precision request (wrap_length double)."""
+    _fields_ = [("sample_x", ctypes.c_void_p), ("num_samples", ctypes.c_uint32),
+                ("quantity_dim", ctypes.c_uint32), ("particle_density", ctypes.c_void_p),
+                ("particle_v", ctypes.c_void_p), ("particle_quantity", ctypes.c_void_p),
+                ("sample_boundary", ctypes.c_void_p),
+                ("sample_boundary_kernel", ctypes.c_void_p),
+                ("sample_density", ctypes.c_void_p),
+                ("sample_position_density", ctypes.c_void_p),
+                ("sample_quantity", ctypes.c_void_p), ("sample_v", ctypes.c_void_p),
+                ("sample_vorticity", ctypes.c_void_p), ("wrap_y", ctypes.c_uint32),
+                ("reserved0", ctypes.c_uint32), ("wrap_length", ctypes.c_double),
+                ("pellet_x", ctypes.c_void_p), ("pellet_v", ctypes.c_void_p),
+                ("num_pellets", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def sample_struct(dtype):
+    return SampleF64 if np.dtype(dtype) == np.float64 else SampleF32
+
+
 class StepReport(ctypes.Structure):
     _fields_ = [("num_divergence_solve", ctypes.c_uint32),
                 ("num_density_solve", ctypes.c_uint32),
@@ -296,8 +316,15 @@ _SIGNATURES = {
     "al_engine_kernel_stat": (ctypes.c_int, [_P, _U, ctypes.c_char_p, ctypes.c_size_t, _P, _P]),
     "al_grid_sort_noalloc_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P, _P]),
     "al_sample_fluid_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
+    "al_sample_fluid_f64": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P]),
     "al_density_mask_f32": (ctypes.c_int, [_P, _P, _U, _P, _P]),
+    "al_density_mask_f64": (ctypes.c_int, [_P, _P, _U, _P, _P]),
     "al_boundary_mask_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, ctypes.c_float, _P, _P]),
+    "al_boundary_mask_f64": (ctypes.c_int, [_P, _P, _P, _P, _U, ctypes.c_double, _P, _P]),
+    "al_distance_mask_multiple_f64": (ctypes.c_int, [_P, _P, _U, _P, _U, ctypes.c_double, _P,
+                                                     _P]),
+    "al_histogram256_f64": (ctypes.c_int, [_P, _P, _P, _U, ctypes.c_double, ctypes.c_double,
+                                           _P, _P]),
     "al_distance_mask_multiple_f32": (ctypes.c_int, [_P, _P, _U, _P, _U, ctypes.c_float, _P,
                                                      _P]),
     "al_histogram256_f32": (ctypes.c_int, [_P, _P, _P, _U, ctypes.c_float, ctypes.c_float, _P,

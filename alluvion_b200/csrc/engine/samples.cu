@@ -1,5 +1,6 @@
 // samples.cu -- fluid statistics at sample points and the reference's
-// post-processing reductions:
+// post-processing reductions, in float and double (Runner<float> and
+// Runner<double>; the _f64 entries take the same arguments in double):
 //   al_sample_fluid_f32      make_neighbor_list over sample_x
 //                            (runner.hpp:1869-1911) followed by sample_fluid,
 //                            sample_fluid_density, sample_position_density,
@@ -42,51 +43,54 @@ namespace {
 
 inline uint32_t blocks_for(uint32_t n, int block) { return (n + block - 1) / block; }
 
-using V3 = vec3<float>;
-
+template <class TF>
 struct SampleDev {
-  const float* x;    // [S][3]
+  const TF* x;    // [S][3]
   uint32_t num;
   uint32_t qdim;
-  const float* rho;  // [N] particle density (original order)
-  const float* v;    // [N][3]
-  const float* q;    // [N][qdim]
-  const float* bnd;  // [nb][S][4] {x_b, V}
-  const float* bker; // [nb][S][4] {grad W V, W V}
-  float* density;    // [S]
-  float* pdensity;   // [S]
-  float* quantity;   // [S][qdim]
-  float* vel;        // [S][3]
-  float* vort;       // [S][3]
-  uint32_t wrap;     // periodic in y
-  float wrap_length, wrap_min, wrap_max;
-  uint32_t nbead;    // points j < nbead are particles, the rest pellets
-  uint32_t npel;     // pellets (0: volume-map bodies, if any)
-  const float* pv;   // [npel][3] pellet velocities
+  const TF* rho;  // [N] particle density (original order)
+  const TF* v;    // [N][3]
+  const TF* q;    // [N][qdim]
+  const TF* bnd;  // [nb][S][4] {x_b, V}
+  const TF* bker; // [nb][S][4] {grad W V, W V}
+  TF* density;    // [S]
+  TF* pdensity;   // [S]
+  TF* quantity;   // [S][qdim]
+  TF* vel;        // [S][3]
+  TF* vort;       // [S][3]
+  uint32_t wrap;  // periodic in y
+  TF wrap_length, wrap_min, wrap_max;
+  uint32_t nbead; // points j < nbead are particles, the rest pellets
+  uint32_t npel;  // pellets (0: volume-map bodies, if any)
+  const TF* pv;   // [npel][3] pellet velocities
 };
 
 // wrap_y (runner.hpp:698-707) of a displacement's y component.
-__device__ __forceinline__ float wrap_dy(const SampleDev& sd, float dy) {
+template <class TF>
+__device__ __forceinline__ TF wrap_dy(const SampleDev<TF>& sd, TF dy) {
   if (dy >= sd.wrap_max) return sub_rn(dy, sd.wrap_length);
   if (dy < sd.wrap_min) return add_rn(dy, sd.wrap_length);
   return dy;
 }
 
 // Velocity of body b at the boundary point of sample s.
-__device__ __forceinline__ V3 body_velocity(const SampleDev& sd, const RigidDev<float>& r,
-                                            uint32_t b, uint32_t s) {
-  const float* bx = sd.bnd + (size_t(b) * sd.num + s) * 4;
-  return cross(r.omega, V3{bx[0], bx[1], bx[2]} - r.x) + r.v;
+template <class TF>
+__device__ __forceinline__ vec3<TF> body_velocity(const SampleDev<TF>& sd,
+                                                  const RigidDev<TF>& r, uint32_t b,
+                                                  uint32_t s) {
+  const TF* bx = sd.bnd + (size_t(b) * sd.num + s) * 4;
+  return cross(r.omega, vec3<TF>{bx[0], bx[1], bx[2]} - r.x) + r.v;
 }
 
 // VORT = false: densities, quantity, velocity; VORT = true: vorticity
 // (reads the samples' velocities written by the first pass).
-template <bool VORT>
+template <class TF, bool VORT>
 __global__ void __launch_bounds__(kBlock)
-    k_sample(Cn<float> c, GridDims g, const uint32_t* __restrict__ cell_start,
-             const vec4<float>* __restrict__ xs, const uint32_t* __restrict__ perm,
-             const vec4<float>* __restrict__ sample_xs, const uint32_t* __restrict__ sample_perm,
-             SampleDev sd, const RigidDev<float>* __restrict__ rigid, uint32_t* flags) {
+    k_sample(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
+             const vec4<TF>* __restrict__ xs, const uint32_t* __restrict__ perm,
+             const vec4<TF>* __restrict__ sample_xs, const uint32_t* __restrict__ sample_perm,
+             SampleDev<TF> sd, const RigidDev<TF>* __restrict__ rigid, uint32_t* flags) {
+  using V3 = vec3<TF>;
   const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (t0 >= sd.num) return;
   // samples in cell order: a warp's samples share cells
@@ -98,11 +102,11 @@ __global__ void __launch_bounds__(kBlock)
   const int z0 = max(ip[2] - 1, 0);
   const int z1 = min(ip[2] + 1, int(g.res[2]) - 1);
   const bool want_w = !VORT && (sd.density || sd.pdensity);
-  float dens = 0;
-  float qs[3] = {0, 0, 0};
+  TF dens = 0;
+  TF qs[3] = {0, 0, 0};
   V3 vel{0, 0, 0}, vort{0, 0, 0};
   // pellet terms (the *_with_pellets kernels): sum W, V W v_p, V (v_p - v_s) x grad W
-  float wb = 0, wp = 0;
+  TF wb = 0, wp = 0;
   V3 velp{0, 0, 0}, vortp{0, 0, 0};
   uint32_t cnt = 0, cntp = 0;
   if (z0 <= z1) {
@@ -126,13 +130,13 @@ __global__ void __launch_bounds__(kBlock)
           const V3 xj = xyz(__ldg(xs + t));
           V3 d{sub_rn(xi.x, xj.x), sub_rn(xi.y, xj.y), sub_rn(xi.z, xj.z)};
           if (sd.wrap) d.y = wrap_dy(sd, d.y);
-          const float d2 = add_rn(add_rn(mul_rn(d.x, d.x), mul_rn(d.y, d.y)), mul_rn(d.z, d.z));
+          const TF d2 = add_rn(add_rn(mul_rn(d.x, d.x), mul_rn(d.y, d.y)), mul_rn(d.z, d.z));
           if (!(d2 < c.h2)) continue;
           if (j >= sd.nbead) {  // a pellet
             if (cntp++ >= g.cap_nbr) continue;
             const V3 vp = ld3(sd.pv, j - sd.nbead);
             if (!VORT) {
-              const float w = W_r2(c, d2);
+              const TF w = W_r2(c, d2);
               wp += w;
               if (sd.vel) velp += (c.vol * w) * vp;
             } else {
@@ -142,11 +146,11 @@ __global__ void __launch_bounds__(kBlock)
           }
           if (cnt++ >= g.cap_nbr) continue;
           if (!VORT) {
-            const float w = W_r2(c, d2);
+            const TF w = W_r2(c, d2);
             if (want_w) dens += c.vol * w;
             if (sd.npel) wb += w;
             if (sd.quantity || sd.vel) {
-              const float mrw = c.mass / __ldg(sd.rho + j) * w;
+              const TF mrw = c.mass / __ldg(sd.rho + j) * w;
               for (uint32_t k = 0; k < sd.qdim; ++k) qs[k] += mrw * __ldg(sd.q + size_t(j) * sd.qdim + k);
               if (sd.vel) vel += mrw * ld3(sd.v, j);
             }
@@ -162,9 +166,9 @@ __global__ void __launch_bounds__(kBlock)
   vel += velp;
   vort += vortp;
   // volume-map body terms (runner.hpp:2116-2118, 4228-4236, 4310-4321)
-  float bw = 0;
+  TF bw = 0;
   for (uint32_t b = 0; b < (sd.npel ? 0u : g.nb); ++b) {
-    const float* bk = sd.bker + (size_t(b) * sd.num + s) * 4;
+    const TF* bk = sd.bker + (size_t(b) * sd.num + s) * 4;
     if (!VORT) {
       bw += bk[3];
       if (sd.vel) vel += bk[3] * body_velocity(sd, rigid[b], b, s);
@@ -184,75 +188,101 @@ __global__ void __launch_bounds__(kBlock)
   }
 }
 
-__global__ void k_density_mask(const float* __restrict__ density, uint32_t n, uint32_t* mask) {
+template <class TF>
+__global__ void k_density_mask(const TF* __restrict__ density, uint32_t n, uint32_t* mask) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) mask[i] = density[i] > 0.f;
+  if (i < n) mask[i] = density[i] > TF(0);
 }
 
 // Mesh bodies use the distance grid, analytic shapes their distance
 // function (the dispatch of launch_compute_boundary_mask).
-__global__ void k_boundary_mask(BodyDev<float> b, RigidDev<float> r, const float* __restrict__ sx,
-                                uint32_t n, float threshold, float* mask) {
+template <class TF>
+__global__ void k_boundary_mask(BodyDev<TF> b, RigidDev<TF> r, const TF* __restrict__ sx,
+                                uint32_t n, TF threshold, TF* mask) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const vec4<float> qc{-r.q.x, -r.q.y, -r.q.z, r.q.w};
-  const V3 local = rotate(ld3(sx, i) - r.x, qc);
-  const float d =
+  const vec4<TF> qc{-r.q.x, -r.q.y, -r.q.z, r.q.w};
+  const vec3<TF> local = rotate(ld3(sx, i) - r.x, qc);
+  const TF d =
       (b.shape == AL_SHAPE_MESH ? interpolate_grid(b, b.dist, local) : shape_sdf(b, local)) *
       b.sign;
-  mask[i] *= float(d >= threshold);
+  mask[i] *= TF(d >= threshold);
 }
 
-__global__ void k_distance_mask_multiple(const float* __restrict__ gx, uint32_t n,
-                                         const float* __restrict__ buoy, uint32_t nbuoy,
-                                         float thr2, float* mask) {
+template <class TF>
+__global__ void k_distance_mask_multiple(const TF* __restrict__ gx, uint32_t n,
+                                         const TF* __restrict__ buoy, uint32_t nbuoy, TF thr2,
+                                         TF* mask) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const V3 x = ld3(gx, i);
+  const vec3<TF> x = ld3(gx, i);
   for (uint32_t k = 0; k < nbuoy; ++k)
-    mask[size_t(k) * n + i] = float(length_sqr(ld3(buoy, k) - x) <= thr2);
+    mask[size_t(k) * n + i] = TF(length_sqr(ld3(buoy, k) - x) <= thr2);
 }
 
 constexpr int kHistBlock = 256;
 constexpr int kHistWarps = kHistBlock / 32;
 
 // quantize (runner.hpp:4516-4536): low byte of floor((v - v_min) * step_inverse)
-// saturated to uint32.
+// saturated to uint32.  In double the product reaches __float2uint_rd through
+// the implicit conversion to float, as in quantize<double>.
 __device__ __forceinline__ uint32_t quantize_byte(float v, float v_min, float step_inverse) {
   return __float2uint_rd(__fmul_rn(__fsub_rn(v, v_min), step_inverse)) & 0xFFu;
 }
+__device__ __forceinline__ uint32_t quantize_byte(double v, double v_min, double step_inverse) {
+  return __float2uint_rd(__double2float_rn(__dmul_rn(__dsub_rn(v, v_min), step_inverse))) &
+         0xFFu;
+}
 
-// VEC: v (and mask) are 16-byte aligned; vector k covers values 4k..4k+3.
-template <bool MASK, bool VEC>
+// 16-byte vectors of values: 4 floats or 2 doubles.
+template <class TF>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using T = float4;
+  static constexpr int kN = 4;
+  __device__ static float at(const float4& a, int i) {
+    return i == 0 ? a.x : i == 1 ? a.y : i == 2 ? a.z : a.w;
+  }
+};
+template <>
+struct Vec16<double> {
+  using T = double2;
+  static constexpr int kN = 2;
+  __device__ static double at(const double2& a, int i) { return i == 0 ? a.x : a.y; }
+};
+
+// VEC: v (and mask) are 16-byte aligned; vector k covers values
+// kN k .. kN k + kN - 1.
+template <class TF, bool MASK, bool VEC>
 __global__ void __launch_bounds__(kHistBlock)
-    k_histogram256(const float* __restrict__ v, const float* __restrict__ mask, uint32_t n,
-                   float v_min, float step_inverse, uint32_t* hist) {
+    k_histogram256(const TF* __restrict__ v, const TF* __restrict__ mask, uint32_t n, TF v_min,
+                   TF step_inverse, uint32_t* hist) {
+  using VT = Vec16<TF>;
   __shared__ uint32_t bins[kHistWarps][256];
   for (int k = threadIdx.x; k < kHistWarps * 256; k += kHistBlock) (&bins[0][0])[k] = 0;
   __syncthreads();
   uint32_t* wb = bins[threadIdx.x >> 5];
   const size_t stride = size_t(gridDim.x) * kHistBlock;
   const size_t tid = size_t(blockIdx.x) * kHistBlock + threadIdx.x;
-  auto add = [&](float x, float m) {
-    if (!MASK || m == 1.0f) atomicAdd(wb + quantize_byte(x, v_min, step_inverse), 1u);
+  auto add = [&](TF x, TF m) {
+    if (!MASK || m == TF(1)) atomicAdd(wb + quantize_byte(x, v_min, step_inverse), 1u);
   };
   size_t head = 0;
   if (VEC) {
-    const size_t nv = n >> 2;
-    const float4* v4 = reinterpret_cast<const float4*>(v);
-    const float4* m4 = reinterpret_cast<const float4*>(mask);
+    const size_t nv = n / VT::kN;
+    const typename VT::T* vv = reinterpret_cast<const typename VT::T*>(v);
+    const typename VT::T* mv = reinterpret_cast<const typename VT::T*>(mask);
     for (size_t k = tid; k < nv; k += stride) {
-      const float4 a = __ldcs(v4 + k);
-      float4 m{1.f, 1.f, 1.f, 1.f};
-      if (MASK) m = __ldcs(m4 + k);
-      add(a.x, m.x);
-      add(a.y, m.y);
-      add(a.z, m.z);
-      add(a.w, m.w);
+      const typename VT::T a = __ldcs(vv + k);
+      typename VT::T m{};
+      if (MASK) m = __ldcs(mv + k);
+#pragma unroll
+      for (int e = 0; e < VT::kN; ++e) add(VT::at(a, e), MASK ? VT::at(m, e) : TF(1));
     }
-    head = nv << 2;
+    head = nv * VT::kN;
   }
-  for (size_t i = head + tid; i < n; i += stride) add(v[i], MASK ? mask[i] : 1.f);
+  for (size_t i = head + tid; i < n; i += stride) add(v[i], MASK ? mask[i] : TF(1));
   __syncthreads();
   for (int b = threadIdx.x; b < 256; b += kHistBlock) {
     uint32_t sum = 0;
@@ -289,40 +319,58 @@ __global__ void __launch_bounds__(kKlBlock)
 
 }  // namespace alb
 
-using namespace alb;
+namespace alb {
+namespace {
 
-extern "C" {
+template <class TF>
+struct SampleTypes;
+template <>
+struct SampleTypes<float> {
+  using cn = al_const_f32;
+  using rigid = al_rigid_f32;
+  using req = al_sample_f32;
+  using body = al_body_f32;
+};
+template <>
+struct SampleTypes<double> {
+  using cn = al_const_f64;
+  using rigid = al_rigid_f64;
+  using req = al_sample_f64;
+  using body = al_body_f64;
+};
 
-int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
-                        const float* particle_x, uint32_t num_particles,
-                        const al_rigid_f32* rigid, const al_sample_f32* req, void* stream) {
-  ALB_CHECK_ARG(engine && cn && cni && req, "al_sample_fluid_f32: null argument");
-  ALB_CHECK_ARG(num_particles == 0 || particle_x, "al_sample_fluid_f32: particle_x is null");
-  ALB_CHECK_ARG(req->num_samples == 0 || req->sample_x, "al_sample_fluid_f32: sample_x is null");
+template <class TF>
+int sample_fluid(al_engine* engine, const typename SampleTypes<TF>::cn* cn, const al_consti* cni,
+                 const TF* particle_x, uint32_t num_particles,
+                 const typename SampleTypes<TF>::rigid* rigid,
+                 const typename SampleTypes<TF>::req* req, void* stream) {
+  ALB_CHECK_ARG(engine && cn && cni && req, "al_sample_fluid: null argument");
+  ALB_CHECK_ARG(num_particles == 0 || particle_x, "al_sample_fluid: particle_x is null");
+  ALB_CHECK_ARG(req->num_samples == 0 || req->sample_x, "al_sample_fluid: sample_x is null");
   ALB_CHECK_ARG(!req->sample_quantity ||
                     ((req->quantity_dim == 1 || req->quantity_dim == 3) && req->particle_quantity),
-                "al_sample_fluid_f32: quantity_dim must be 1 or 3 with particle_quantity set");
+                "al_sample_fluid: quantity_dim must be 1 or 3 with particle_quantity set");
   const bool need_rho = req->sample_quantity || req->sample_v || req->sample_vorticity;
   ALB_CHECK_ARG(num_particles == 0 || !need_rho || req->particle_density,
-                "al_sample_fluid_f32: particle_density is null");
+                "al_sample_fluid: particle_density is null");
   ALB_CHECK_ARG(!(req->sample_v || req->sample_vorticity) || req->particle_v,
-                "al_sample_fluid_f32: velocities need particle_v");
+                "al_sample_fluid: velocities need particle_v");
   ALB_CHECK_ARG(!req->sample_vorticity || req->sample_v,
-                "al_sample_fluid_f32: vorticity needs sample_v");
-  ALB_CHECK_ARG(cni->num_boundaries <= AL_MAX_BOUNDARIES, "al_sample_fluid_f32: too many bodies");
-  ALB_CHECK_ARG(!req->wrap_y || req->wrap_length > 0.f,
-                "al_sample_fluid_f32: wrap_y needs a positive wrap_length");
+                "al_sample_fluid: vorticity needs sample_v");
+  ALB_CHECK_ARG(cni->num_boundaries <= AL_MAX_BOUNDARIES, "al_sample_fluid: too many bodies");
+  ALB_CHECK_ARG(!req->wrap_y || req->wrap_length > TF(0),
+                "al_sample_fluid: wrap_y needs a positive wrap_length");
   const uint32_t npel = req->num_pellets;
   ALB_CHECK_ARG(npel == 0 || (req->pellet_x && (req->pellet_v || !(req->sample_v ||
                                                                   req->sample_vorticity))),
-                "al_sample_fluid_f32: pellet_x / pellet_v are null");
-  ALB_CHECK_ARG(uint64_t(num_particles) + npel < (1ull << 31), "al_sample_fluid_f32: too many points");
+                "al_sample_fluid: pellet_x / pellet_v are null");
+  ALB_CHECK_ARG(uint64_t(num_particles) + npel < (1ull << 31), "al_sample_fluid: too many points");
   const bool body_terms = npel == 0 && (req->sample_position_density || req->sample_v);
   ALB_CHECK_ARG(cni->num_boundaries == 0 || !body_terms || req->sample_boundary_kernel,
-                "al_sample_fluid_f32: sample_boundary_kernel is null");
+                "al_sample_fluid: sample_boundary_kernel is null");
   ALB_CHECK_ARG(cni->num_boundaries == 0 || npel || !req->sample_v ||
                     (req->sample_boundary && rigid),
-                "al_sample_fluid_f32: velocities need sample_boundary and rigid");
+                "al_sample_fluid: velocities need sample_boundary and rigid");
   ALB_TRY(engine->activate());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (req->num_samples == 0) return AL_OK;
@@ -330,81 +378,81 @@ int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_cons
     al_engine* e;
     ~NsReset() { e->ns.clear(); }
   } reset{engine};
-  const Cn<float> c = to_cn<float>(*cn);
+  const Cn<TF> c = to_cn<TF>(*cn);
   GridDims g = to_dims(*cni);
   // the samples' own cell order (their out-of-grid / crowded-cell flags are
   // not anomalies: the reference bins no samples)
   engine->ns = "sample.points.";
-  vec4<float>* sxs = nullptr;
+  vec4<TF>* sxs = nullptr;
   uint32_t* sflags = nullptr;
   ALB_TRY(engine->buf("sorted.x", req->num_samples, &sxs));
   ALB_TRY(engine->buf("flags", 4, &sflags));
   ALB_CUDA(cudaMemsetAsync(sflags, 0, 4 * sizeof(uint32_t), st));
   GridState ss;
   ALB_LAUNCH(engine, "sample_sort", 7, st,
-             ALB_TRY(grid_build<float>(engine, c, g, req->sample_x, req->num_samples, sxs, sflags,
-                                       ss, st)));
+             ALB_TRY(grid_build<TF>(engine, c, g, req->sample_x, req->num_samples, sxs, sflags,
+                                    ss, st)));
   engine->ns = "sample.";
-  vec4<float>* xs = nullptr;
+  vec4<TF>* xs = nullptr;
   uint32_t* flags = nullptr;
-  RigidDev<float>* dr = nullptr;
+  RigidDev<TF>* dr = nullptr;
   ALB_TRY(engine->buf("sorted.x", num_particles ? num_particles : 1, &xs));
   ALB_TRY(engine->buf("flags", 4, &flags));
   ALB_TRY(engine->buf("rigid", AL_MAX_BOUNDARIES, &dr));
   ALB_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(uint32_t), st));
   if (g.nb && req->sample_v && npel == 0) {
-    RigidDev<float> hr[AL_MAX_BOUNDARIES];
-    for (uint32_t b = 0; b < g.nb; ++b) hr[b] = to_rigid_dev<float>(rigid[b]);
-    ALB_CUDA(cudaMemcpyAsync(dr, hr, sizeof(RigidDev<float>) * g.nb, cudaMemcpyHostToDevice, st));
+    RigidDev<TF> hr[AL_MAX_BOUNDARIES];
+    for (uint32_t b = 0; b < g.nb; ++b) hr[b] = to_rigid_dev<TF>(rigid[b]);
+    ALB_CUDA(cudaMemcpyAsync(dr, hr, sizeof(RigidDev<TF>) * g.nb, cudaMemcpyHostToDevice, st));
   }
   // with pellets, one grid over particles and pellets (pellets after the
   // particles, as the reference stores them)
-  const float* grid_x = particle_x;
+  const TF* grid_x = particle_x;
   const uint32_t npts = num_particles + npel;
   if (npel) {
-    float* all = nullptr;
+    TF* all = nullptr;
     ALB_TRY(engine->buf("all.x", size_t(npts) * 3, &all));
     if (num_particles)
-      ALB_CUDA(cudaMemcpyAsync(all, particle_x, sizeof(float) * 3 * num_particles,
+      ALB_CUDA(cudaMemcpyAsync(all, particle_x, sizeof(TF) * 3 * num_particles,
                                cudaMemcpyDeviceToDevice, st));
     ALB_CUDA(cudaMemcpyAsync(all + size_t(num_particles) * 3, req->pellet_x,
-                             sizeof(float) * 3 * npel, cudaMemcpyDeviceToDevice, st));
+                             sizeof(TF) * 3 * npel, cudaMemcpyDeviceToDevice, st));
     ALB_TRY(engine->buf("sorted.x", npts, &xs));
     grid_x = all;
   }
   GridState gs;
   ALB_LAUNCH(engine, "sample_grid", 7, st,
-             ALB_TRY(grid_build<float>(engine, c, g, grid_x, npts, xs, flags, gs, st)));
-  SampleDev sd{req->sample_x,
-               req->num_samples,
-               req->sample_quantity ? req->quantity_dim : 0u,
-               req->particle_density,
-               req->particle_v,
-               req->particle_quantity,
-               req->sample_boundary,
-               req->sample_boundary_kernel,
-               req->sample_density,
-               req->sample_position_density,
-               req->sample_quantity,
-               req->sample_v,
-               req->sample_vorticity,
-               req->wrap_y ? 1u : 0u,
-               req->wrap_length,
-               req->wrap_length * -0.5f,
-               req->wrap_length * 0.5f,
-               num_particles,
-               npel,
-               req->pellet_v};
+             ALB_TRY(grid_build<TF>(engine, c, g, grid_x, npts, xs, flags, gs, st)));
+  SampleDev<TF> sd{req->sample_x,
+                   req->num_samples,
+                   req->sample_quantity ? req->quantity_dim : 0u,
+                   req->particle_density,
+                   req->particle_v,
+                   req->particle_quantity,
+                   req->sample_boundary,
+                   req->sample_boundary_kernel,
+                   req->sample_density,
+                   req->sample_position_density,
+                   req->sample_quantity,
+                   req->sample_v,
+                   req->sample_vorticity,
+                   req->wrap_y ? 1u : 0u,
+                   TF(req->wrap_length),
+                   TF(req->wrap_length) * TF(-0.5),
+                   TF(req->wrap_length) * TF(0.5),
+                   num_particles,
+                   npel,
+                   req->pellet_v};
   const uint32_t blocks = blocks_for(req->num_samples, kBlock);
   GridDims g1 = g;
   if (!body_terms) g1.nb = 0;  // the first pass reads no body arrays
   ALB_LAUNCH(engine, "sample", 1, st,
-             (k_sample<false><<<blocks, kBlock, 0, st>>>(c, g1, gs.cell_start, xs, gs.perm, sxs,
-                                                         ss.perm, sd, dr, flags)));
+             (k_sample<TF, false><<<blocks, kBlock, 0, st>>>(c, g1, gs.cell_start, xs, gs.perm,
+                                                             sxs, ss.perm, sd, dr, flags)));
   if (req->sample_vorticity)
     ALB_LAUNCH(engine, "sample_vorticity", 1, st,
-               (k_sample<true><<<blocks, kBlock, 0, st>>>(c, g, gs.cell_start, xs, gs.perm, sxs,
-                                                          ss.perm, sd, dr, flags)));
+               (k_sample<TF, true><<<blocks, kBlock, 0, st>>>(c, g, gs.cell_start, xs, gs.perm,
+                                                              sxs, ss.perm, sd, dr, flags)));
   ALB_CUDA(cudaGetLastError());
   uint32_t hf[4];
   ALB_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
@@ -416,64 +464,67 @@ int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_cons
   return AL_OK;
 }
 
-int al_density_mask_f32(al_engine* engine, const float* sample_density, uint32_t num_samples,
-                        uint32_t* mask, void* stream) {
+template <class TF>
+int density_mask(al_engine* engine, const TF* sample_density, uint32_t num_samples,
+                 uint32_t* mask, void* stream) {
   ALB_CHECK_ARG(engine && (num_samples == 0 || (sample_density && mask)),
-                "al_density_mask_f32: null argument");
+                "al_density_mask: null argument");
   ALB_TRY(engine->activate());
   if (num_samples == 0) return AL_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ALB_LAUNCH(engine, "density_mask", 1, st,
-             (k_density_mask<<<blocks_for(num_samples, kBlock), kBlock, 0, st>>>(
+             (k_density_mask<TF><<<blocks_for(num_samples, kBlock), kBlock, 0, st>>>(
                  sample_density, num_samples, mask)));
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }
 
-int al_boundary_mask_f32(al_engine* engine, const al_body_f32* body, const al_rigid_f32* rigid,
-                         const float* sample_x, uint32_t num_samples, float distance_threshold,
-                         float* mask, void* stream) {
+template <class TF>
+int boundary_mask(al_engine* engine, const typename SampleTypes<TF>::body* body,
+                  const typename SampleTypes<TF>::rigid* rigid, const TF* sample_x,
+                  uint32_t num_samples, TF distance_threshold, TF* mask, void* stream) {
   ALB_CHECK_ARG(engine && body && rigid && (num_samples == 0 || (sample_x && mask)),
-                "al_boundary_mask_f32: null argument");
-  const BodyDev<float> b = to_body_dev<float>(*body);
+                "al_boundary_mask: null argument");
+  const BodyDev<TF> b = to_body_dev<TF>(*body);
   ALB_TRY(validate_body(b, b.shape == AL_SHAPE_MESH, false));
   ALB_TRY(engine->activate());
   if (num_samples == 0) return AL_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ALB_LAUNCH(engine, "boundary_mask", 1, st,
-             (k_boundary_mask<<<blocks_for(num_samples, kBlock), kBlock, 0, st>>>(
-                 b, to_rigid_dev<float>(*rigid), sample_x, num_samples, distance_threshold,
-                 mask)));
+             (k_boundary_mask<TF><<<blocks_for(num_samples, kBlock), kBlock, 0, st>>>(
+                 b, to_rigid_dev<TF>(*rigid), sample_x, num_samples, distance_threshold, mask)));
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }
 
-int al_distance_mask_multiple_f32(al_engine* engine, const float* grid_x,
-                                  uint32_t num_grid_points, const float* buoy_x,
-                                  uint32_t num_buoys, float distance_threshold, float* mask,
-                                  void* stream) {
+template <class TF>
+int distance_mask_multiple(al_engine* engine, const TF* grid_x, uint32_t num_grid_points,
+                           const TF* buoy_x, uint32_t num_buoys, TF distance_threshold, TF* mask,
+                           void* stream) {
   ALB_CHECK_ARG(engine && (num_grid_points == 0 || num_buoys == 0 || (grid_x && buoy_x && mask)),
-                "al_distance_mask_multiple_f32: null argument");
+                "al_distance_mask_multiple: null argument");
   ALB_TRY(engine->activate());
   if (num_grid_points == 0 || num_buoys == 0) return AL_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ALB_LAUNCH(engine, "distance_mask_multiple", 1, st,
-             (k_distance_mask_multiple<<<blocks_for(num_grid_points, kBlock), kBlock, 0, st>>>(
+             (k_distance_mask_multiple<TF><<<blocks_for(num_grid_points, kBlock), kBlock, 0, st>>>(
                  grid_x, num_grid_points, buoy_x, num_buoys,
                  distance_threshold * distance_threshold, mask)));
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }
 
-int al_histogram256_f32(al_engine* engine, const float* v, const float* mask, uint32_t n,
-                        float v_min, float v_max, uint32_t* histogram, void* stream) {
-  ALB_CHECK_ARG(engine && histogram && (n == 0 || v), "al_histogram256_f32: null argument");
+template <class TF>
+int histogram256(al_engine* engine, const TF* v, const TF* mask, uint32_t n, TF v_min, TF v_max,
+                 uint32_t* histogram, void* stream) {
+  ALB_CHECK_ARG(engine && histogram && (n == 0 || v), "al_histogram256: null argument");
   ALB_TRY(engine->activate());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ALB_CUDA(cudaMemsetAsync(histogram, 0, 256 * sizeof(uint32_t), st));
   if (n == 0) return AL_OK;
-  const float step_inverse =
-      static_cast<float>(256.0 / (static_cast<double>(v_max) - static_cast<double>(v_min)));
+  // launch_histogram256 (runner.hpp:5852-5853): the step in double, cast to TF
+  const TF step_inverse =
+      static_cast<TF>(256.0 / (static_cast<double>(v_max) - static_cast<double>(v_min)));
   const bool vec = (reinterpret_cast<uintptr_t>(v) & 15) == 0 &&
                    (!mask || (reinterpret_cast<uintptr_t>(mask) & 15) == 0);
   // enough resident blocks to cover the SMs, each thread about 16 values
@@ -483,22 +534,86 @@ int al_histogram256_f32(al_engine* engine, const float* v, const float* mask, ui
   ALB_LAUNCH(engine, "histogram256", 1, st, {
     if (mask) {
       if (vec)
-        k_histogram256<true, true><<<grid, kHistBlock, 0, st>>>(v, mask, n, v_min, step_inverse,
-                                                                histogram);
+        k_histogram256<TF, true, true><<<grid, kHistBlock, 0, st>>>(v, mask, n, v_min,
+                                                                    step_inverse, histogram);
       else
-        k_histogram256<true, false><<<grid, kHistBlock, 0, st>>>(v, mask, n, v_min,
-                                                                 step_inverse, histogram);
+        k_histogram256<TF, true, false><<<grid, kHistBlock, 0, st>>>(v, mask, n, v_min,
+                                                                     step_inverse, histogram);
     } else {
       if (vec)
-        k_histogram256<false, true><<<grid, kHistBlock, 0, st>>>(v, nullptr, n, v_min,
-                                                                 step_inverse, histogram);
+        k_histogram256<TF, false, true><<<grid, kHistBlock, 0, st>>>(v, nullptr, n, v_min,
+                                                                     step_inverse, histogram);
       else
-        k_histogram256<false, false><<<grid, kHistBlock, 0, st>>>(v, nullptr, n, v_min,
-                                                                  step_inverse, histogram);
+        k_histogram256<TF, false, false><<<grid, kHistBlock, 0, st>>>(v, nullptr, n, v_min,
+                                                                      step_inverse, histogram);
     }
   });
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
+}
+
+}  // namespace
+}  // namespace alb
+
+using namespace alb;
+
+extern "C" {
+
+int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const al_consti* cni,
+                        const float* particle_x, uint32_t num_particles,
+                        const al_rigid_f32* rigid, const al_sample_f32* req, void* stream) {
+  return sample_fluid<float>(engine, cn, cni, particle_x, num_particles, rigid, req, stream);
+}
+int al_sample_fluid_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                        const double* particle_x, uint32_t num_particles,
+                        const al_rigid_f64* rigid, const al_sample_f64* req, void* stream) {
+  return sample_fluid<double>(engine, cn, cni, particle_x, num_particles, rigid, req, stream);
+}
+
+int al_density_mask_f32(al_engine* engine, const float* sample_density, uint32_t num_samples,
+                        uint32_t* mask, void* stream) {
+  return density_mask<float>(engine, sample_density, num_samples, mask, stream);
+}
+int al_density_mask_f64(al_engine* engine, const double* sample_density, uint32_t num_samples,
+                        uint32_t* mask, void* stream) {
+  return density_mask<double>(engine, sample_density, num_samples, mask, stream);
+}
+
+int al_boundary_mask_f32(al_engine* engine, const al_body_f32* body, const al_rigid_f32* rigid,
+                         const float* sample_x, uint32_t num_samples, float distance_threshold,
+                         float* mask, void* stream) {
+  return boundary_mask<float>(engine, body, rigid, sample_x, num_samples, distance_threshold,
+                              mask, stream);
+}
+int al_boundary_mask_f64(al_engine* engine, const al_body_f64* body, const al_rigid_f64* rigid,
+                         const double* sample_x, uint32_t num_samples, double distance_threshold,
+                         double* mask, void* stream) {
+  return boundary_mask<double>(engine, body, rigid, sample_x, num_samples, distance_threshold,
+                               mask, stream);
+}
+
+int al_distance_mask_multiple_f32(al_engine* engine, const float* grid_x,
+                                  uint32_t num_grid_points, const float* buoy_x,
+                                  uint32_t num_buoys, float distance_threshold, float* mask,
+                                  void* stream) {
+  return distance_mask_multiple<float>(engine, grid_x, num_grid_points, buoy_x, num_buoys,
+                                       distance_threshold, mask, stream);
+}
+int al_distance_mask_multiple_f64(al_engine* engine, const double* grid_x,
+                                  uint32_t num_grid_points, const double* buoy_x,
+                                  uint32_t num_buoys, double distance_threshold, double* mask,
+                                  void* stream) {
+  return distance_mask_multiple<double>(engine, grid_x, num_grid_points, buoy_x, num_buoys,
+                                        distance_threshold, mask, stream);
+}
+
+int al_histogram256_f32(al_engine* engine, const float* v, const float* mask, uint32_t n,
+                        float v_min, float v_max, uint32_t* histogram, void* stream) {
+  return histogram256<float>(engine, v, mask, n, v_min, v_max, histogram, stream);
+}
+int al_histogram256_f64(al_engine* engine, const double* v, const double* mask, uint32_t n,
+                        double v_min, double v_max, uint32_t* histogram, void* stream) {
+  return histogram256<double>(engine, v, mask, n, v_min, v_max, histogram, stream);
 }
 
 int al_kl_divergence(al_engine* engine, const uint32_t* histogram_p, const uint32_t* histogram_q,

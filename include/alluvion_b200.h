@@ -811,10 +811,40 @@ AL_API int al_sample_fluid_f32(al_engine* engine, const al_const_f32* cn, const 
                                const float* particle_x, uint32_t num_particles,
                                const al_rigid_f32* rigid, const al_sample_f32* request,
                                void* stream);
+/* The same in double (Runner<double>): every array and wrap_length double. */
+typedef struct al_sample_f64 {
+  const double* sample_x;
+  uint32_t num_samples;
+  uint32_t quantity_dim;
+  const double* particle_density;
+  const double* particle_v;
+  const double* particle_quantity;
+  const double* sample_boundary;
+  const double* sample_boundary_kernel;
+  double* sample_density;
+  double* sample_position_density;
+  double* sample_quantity;
+  double* sample_v;
+  double* sample_vorticity;
+  uint32_t wrap_y;
+  uint32_t reserved0;
+  double wrap_length;
+  const double* pellet_x;
+  const double* pellet_v;
+  uint32_t num_pellets;
+  uint32_t reserved;
+} al_sample_f64;
+
+AL_API int al_sample_fluid_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cni,
+                               const double* particle_x, uint32_t num_particles,
+                               const al_rigid_f64* rigid, const al_sample_f64* request,
+                               void* stream);
 
 /* compute_density_mask (runner.hpp:4359-4365): mask[i] = density[i] > 0.
  * Device arrays. */
 AL_API int al_density_mask_f32(al_engine* engine, const float* sample_density,
+                               uint32_t num_samples, uint32_t* mask, void* stream);
+AL_API int al_density_mask_f64(al_engine* engine, const double* sample_density,
                                uint32_t num_samples, uint32_t* mask, void* stream);
 
 /* compute_boundary_mask (runner.hpp:4367-4396, launched by
@@ -827,6 +857,10 @@ AL_API int al_boundary_mask_f32(al_engine* engine, const al_body_f32* body,
                                 const al_rigid_f32* rigid, const float* sample_x,
                                 uint32_t num_samples, float distance_threshold, float* mask,
                                 void* stream);
+AL_API int al_boundary_mask_f64(al_engine* engine, const al_body_f64* body,
+                                const al_rigid_f64* rigid, const double* sample_x,
+                                uint32_t num_samples, double distance_threshold, double* mask,
+                                void* stream);
 
 /* compute_distance_mask_multiple (runner.hpp:4272-4287):
  * mask[k][i] = |buoy_x[k] - grid_x[i]|^2 <= threshold^2.  Device arrays. */
@@ -834,6 +868,10 @@ AL_API int al_distance_mask_multiple_f32(al_engine* engine, const float* grid_x,
                                          uint32_t num_grid_points, const float* buoy_x,
                                          uint32_t num_buoys, float distance_threshold,
                                          float* mask, void* stream);
+AL_API int al_distance_mask_multiple_f64(al_engine* engine, const double* grid_x,
+                                         uint32_t num_grid_points, const double* buoy_x,
+                                         uint32_t num_buoys, double distance_threshold,
+                                         double* mask, void* stream);
 
 /* Runner::launch_histogram256[_with_mask] (runner.hpp:5849-5889; kernels
  * quantize, histogram256[_with_mask], merge_histogram256,
@@ -844,6 +882,14 @@ AL_API int al_distance_mask_multiple_f32(al_engine* engine, const float* grid_x,
  * mask); histogram: device [256] out. */
 AL_API int al_histogram256_f32(al_engine* engine, const float* v, const float* mask, uint32_t n,
                                float v_min, float v_max, uint32_t* histogram, void* stream);
+/* Runner<double>: step_inverse = 256 / (v_max - v_min) in double, and the
+ * quantize kernel's (v - v_min) * step_inverse, formed in double, reaches
+ * __float2uint_rd through the implicit conversion to float (round to
+ * nearest): byte = floor(float((v - v_min) * step_inverse)) saturated,
+ * low 8 bits. */
+AL_API int al_histogram256_f64(al_engine* engine, const double* v, const double* mask,
+                               uint32_t n, double v_min, double v_max, uint32_t* histogram,
+                               void* stream);
 
 /* Runner::calculate_kl_divergence (runner.hpp:4803-4815, KLDivergence
  * runner.hpp:746-762): sum over bins with p > 0 of

@@ -31,8 +31,11 @@ def lib():
             "orc_mesh_distance_grid_f32": (None, [_P, _P, _U, _P, _U, ctypes.c_float, _P]),
             # cn, cni, particle_x, n, rigid, request -> overflow
             "orc_sample_fluid_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
+            "orc_sample_fluid_f64": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
             "orc_boundary_mask_f32": (None, [_P, _P, _P, _U, ctypes.c_float, _P]),
+            "orc_boundary_mask_f64": (None, [_P, _P, _P, _U, ctypes.c_double, _P]),
             "orc_histogram256_f32": (None, [_P, _P, _U, ctypes.c_float, ctypes.c_float, _P]),
+            "orc_histogram256_f64": (None, [_P, _P, _U, ctypes.c_double, ctypes.c_double, _P]),
             "orc_kl_divergence": (ctypes.c_double, [_P, _P, _U, _U, ctypes.c_double, _U]),
             "orc_relax_pellets_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _U, _P, _P]),
         }
@@ -240,10 +243,13 @@ def sample_fluid(cn, cni, particle_x, rigid, sample_x, particle_density=None, pa
                  wrap_length=None, pellet_x=None, pellet_v=None):
     """sample_fluid / sample_fluid_density / sample_position_density /
     compute_sample_velocity / compute_sample_vorticity restated on host
-    float32 arrays; wrap_length: periodic in y (make_neighbor_list<1>).
-    Returns (dict of outputs, neighbor overflow flag)."""
+    arrays of particle_x's real type (float32 or float64; cn, rigid and the
+    other arrays follow it); wrap_length: periodic in y
+    (make_neighbor_list<1>).  Returns (dict of outputs, neighbor overflow
+    flag)."""
     from alluvion_b200 import _capi
-    f32 = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+    T = np.float64 if np.asarray(particle_x).dtype == np.float64 else np.float32
+    f32 = lambda a: None if a is None else np.ascontiguousarray(a, T)
     px, sx = f32(particle_x), f32(sample_x)
     rho, pv, pq = f32(particle_density), f32(particle_v), f32(particle_quantity)
     sb, sbk = f32(sample_boundary), f32(sample_boundary_kernel)
@@ -253,8 +259,8 @@ def sample_fluid(cn, cni, particle_x, rigid, sample_x, particle_density=None, pa
     shapes = {"density": (s,), "position_density": (s,), "quantity": (s, qdim) if qdim > 1
               else (s,), "v": (s, 3), "vorticity": (s, 3)}
     for k in outputs:
-        out[k] = np.zeros(shapes[k], np.float32)
-    req = _capi.SampleF32()
+        out[k] = np.zeros(shapes[k], T)
+    req = _capi.sample_struct(T)()
     req.sample_x = sx.ctypes.data
     req.num_samples = s
     req.quantity_dim = qdim
@@ -273,23 +279,30 @@ def sample_fluid(cn, cni, particle_x, rigid, sample_x, particle_density=None, pa
                     ("quantity", "sample_quantity"), ("v", "sample_v"),
                     ("vorticity", "sample_vorticity")):
         setattr(req, name, out[k].ctypes.data if k in out else None)
-    flag = lib().orc_sample_fluid_f32(_p(cn), _p(cni), _p(px), len(px), _p(rigid), _p(req))
+    flag = getattr(lib(), "orc_sample_fluid_" + _sfx(T))(_p(cn), _p(cni), _p(px), len(px),
+                                                        _p(rigid), _p(req))
     return out, bool(flag)
 
 
 def boundary_mask(body, rigid, sample_x, threshold, mask):
-    """compute_boundary_mask restated: mask (float32) *= (sign d >= threshold)."""
-    sx = np.ascontiguousarray(sample_x, np.float32)
-    lib().orc_boundary_mask_f32(_p(body), _p(rigid), _p(sx), len(sx), float(threshold), _p(mask))
+    """compute_boundary_mask restated: mask *= (sign d >= threshold), in the
+    real type of mask (float32 or float64)."""
+    T = mask.dtype.type
+    sx = np.ascontiguousarray(sample_x, T)
+    getattr(lib(), "orc_boundary_mask_" + _sfx(T))(_p(body), _p(rigid), _p(sx), len(sx),
+                                                   float(threshold), _p(mask))
     return mask
 
 
 def histogram256(v, v_min, v_max, mask=None):
-    """launch_histogram256[_with_mask] restated: 256 uint32 counts."""
-    v = np.ascontiguousarray(v, np.float32)
-    m = None if mask is None else np.ascontiguousarray(mask, np.float32)
+    """launch_histogram256[_with_mask] restated: 256 uint32 counts, in v's
+    real type (float32 or float64)."""
+    T = np.float64 if np.asarray(v).dtype == np.float64 else np.float32
+    v = np.ascontiguousarray(v, T)
+    m = None if mask is None else np.ascontiguousarray(mask, T)
     h = np.zeros(256, np.uint32)
-    lib().orc_histogram256_f32(_p(v), _p(m), len(v), float(v_min), float(v_max), _p(h))
+    getattr(lib(), "orc_histogram256_" + _sfx(T))(_p(v), _p(m), len(v), float(v_min),
+                                                  float(v_max), _p(h))
     return h
 
 

@@ -602,60 +602,92 @@ void orc_mesh_distance_grid_f32(const al_body_f32* b, const float* verts, uint32
 
 extern "C" {
 
-// Sampling at sample points (sample_fluid and friends) with HOST arrays in
-// the layouts of al_sample_f32; `rigid` holds the bodies' states
-// (cni->num_boundaries of them).  Returns 1 when a sample had more
-// neighbors than the cap, else 0.
-int orc_sample_fluid_f32(const al_const_f32* cn, const al_consti* cni, const float* particle_x,
-                         uint32_t n, const al_rigid_f32* rigid, const al_sample_f32* req) {
-  const Cn<float> c = make_cn<float>(*cn);
-  std::vector<V3<float>> px(n);
-  for (uint32_t i = 0; i < n; ++i) px[i] = v3<float>(particle_x + 3 * size_t(i));
-  std::vector<V3<float>> sx(req->num_samples);
-  for (uint32_t i = 0; i < req->num_samples; ++i) sx[i] = v3<float>(req->sample_x + 3 * size_t(i));
-  std::vector<Body<float>> bodies;
+}  // extern "C"
+
+namespace {
+
+template <class TF, class Req, class ConstT, class RigidT>
+int sample_impl(const ConstT* cn, const al_consti* cni, const TF* particle_x, uint32_t n,
+                const RigidT* rigid, const Req* req) {
+  const Cn<TF> c = make_cn<TF>(*cn);
+  std::vector<V3<TF>> px(n);
+  for (uint32_t i = 0; i < n; ++i) px[i] = v3<TF>(particle_x + 3 * size_t(i));
+  std::vector<V3<TF>> sx(req->num_samples);
+  for (uint32_t i = 0; i < req->num_samples; ++i) sx[i] = v3<TF>(req->sample_x + 3 * size_t(i));
+  std::vector<Body<TF>> bodies;
   for (uint32_t b = 0; rigid && b < cni->num_boundaries; ++b) {
-    Body<float> o{};
-    o.x = v3<float>(rigid[b].x);
-    o.v = v3<float>(rigid[b].v);
-    o.omega = v3<float>(rigid[b].omega);
-    o.q = V4<float>{rigid[b].q[0], rigid[b].q[1], rigid[b].q[2], rigid[b].q[3]};
+    Body<TF> o{};
+    o.x = v3<TF>(rigid[b].x);
+    o.v = v3<TF>(rigid[b].v);
+    o.omega = v3<TF>(rigid[b].omega);
+    o.q = V4<TF>{rigid[b].q[0], rigid[b].q[1], rigid[b].q[2], rigid[b].q[3]};
     bodies.push_back(o);
   }
-  SampleRequest<float> r;
+  SampleRequest<TF> r;
   r.sx = sx.data();
   r.num = req->num_samples;
   r.rho = req->particle_density;
-  r.v = reinterpret_cast<const V3<float>*>(req->particle_v);
+  r.v = reinterpret_cast<const V3<TF>*>(req->particle_v);
   r.q = req->particle_quantity;
   r.qdim = req->sample_quantity ? req->quantity_dim : 0;
-  r.bnd = reinterpret_cast<const V4<float>*>(req->sample_boundary);
-  r.bk = reinterpret_cast<const V4<float>*>(req->sample_boundary_kernel);
+  r.bnd = reinterpret_cast<const V4<TF>*>(req->sample_boundary);
+  r.bk = reinterpret_cast<const V4<TF>*>(req->sample_boundary_kernel);
   r.density = req->sample_density;
   r.position_density = req->sample_position_density;
   r.quantity = req->sample_quantity;
-  r.vel = reinterpret_cast<V3<float>*>(req->sample_v);
-  r.vort = reinterpret_cast<V3<float>*>(req->sample_vorticity);
+  r.vel = reinterpret_cast<V3<TF>*>(req->sample_v);
+  r.vort = reinterpret_cast<V3<TF>*>(req->sample_vorticity);
   r.wrap = req->wrap_y != 0;
-  r.wrap_length = req->wrap_length;
-  r.pel_x = reinterpret_cast<const V3<float>*>(req->pellet_x);
-  r.pel_v = reinterpret_cast<const V3<float>*>(req->pellet_v);
+  r.wrap_length = TF(req->wrap_length);
+  r.pel_x = reinterpret_cast<const V3<TF>*>(req->pellet_x);
+  r.pel_v = reinterpret_cast<const V3<TF>*>(req->pellet_v);
   r.npel = req->num_pellets;
   return sample_fluid(c, *cni, px.data(), n, bodies, r) ? 1 : 0;
+}
+
+template <class TF, class BodyT, class RigidT>
+void boundary_mask_impl(const BodyT* body, const RigidT* rigid, const TF* sample_x, uint32_t n,
+                        TF threshold, TF* mask) {
+  const Body<TF> b = make_body<TF>(*body, reinterpret_cast<const TF*>(rigid));
+  std::vector<V3<TF>> sx(n);
+  for (uint32_t i = 0; i < n; ++i) sx[i] = v3<TF>(sample_x + 3 * size_t(i));
+  boundary_mask(b, sx.data(), n, threshold, mask);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Sampling at sample points (sample_fluid and friends) with HOST arrays in
+// the layouts of al_sample_f32 / al_sample_f64; `rigid` holds the bodies'
+// states (cni->num_boundaries of them).  Returns 1 when a sample had more
+// neighbors than the cap, else 0.
+int orc_sample_fluid_f32(const al_const_f32* cn, const al_consti* cni, const float* particle_x,
+                         uint32_t n, const al_rigid_f32* rigid, const al_sample_f32* req) {
+  return sample_impl<float>(cn, cni, particle_x, n, rigid, req);
+}
+int orc_sample_fluid_f64(const al_const_f64* cn, const al_consti* cni, const double* particle_x,
+                         uint32_t n, const al_rigid_f64* rigid, const al_sample_f64* req) {
+  return sample_impl<double>(cn, cni, particle_x, n, rigid, req);
 }
 
 // compute_boundary_mask with HOST node arrays: mask *= (sign d >= threshold).
 void orc_boundary_mask_f32(const al_body_f32* body, const al_rigid_f32* rigid,
                            const float* sample_x, uint32_t n, float threshold, float* mask) {
-  const Body<float> b = make_body<float>(*body, reinterpret_cast<const float*>(rigid));
-  std::vector<V3<float>> sx(n);
-  for (uint32_t i = 0; i < n; ++i) sx[i] = v3<float>(sample_x + 3 * size_t(i));
-  boundary_mask(b, sx.data(), n, threshold, mask);
+  boundary_mask_impl<float>(body, rigid, sample_x, n, threshold, mask);
+}
+void orc_boundary_mask_f64(const al_body_f64* body, const al_rigid_f64* rigid,
+                           const double* sample_x, uint32_t n, double threshold, double* mask) {
+  boundary_mask_impl<double>(body, rigid, sample_x, n, threshold, mask);
 }
 
 // launch_histogram256[_with_mask]: 256 counts of quantized bytes.
 void orc_histogram256_f32(const float* v, const float* mask, uint32_t n, float v_min, float v_max,
                           uint32_t* hist) {
+  histogram256(v, mask, n, v_min, v_max, hist);
+}
+void orc_histogram256_f64(const double* v, const double* mask, uint32_t n, double v_min,
+                          double v_max, uint32_t* hist) {
   histogram256(v, mask, n, v_min, v_max, hist);
 }
 

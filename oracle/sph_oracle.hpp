@@ -2406,16 +2406,28 @@ inline uint32_t quantize_byte(float v, float v_min, float step_inverse) {
   return uint32_t(std::floor(t)) & 0xFFu;
 }
 
+// quantize<double>: (v - v_min) * step_inverse is formed in double and
+// reaches __float2uint_rd through the implicit conversion to float (round to
+// nearest), then the same saturation.
+inline uint32_t quantize_byte(double v, double v_min, double step_inverse) {
+  const double d = v - v_min;
+  const float t = float(d * step_inverse);
+  if (!(t > 0.0f)) return 0;
+  if (t >= 4294967296.0f) return 0xFFu;
+  return uint32_t(std::floor(t)) & 0xFFu;
+}
+
 // launch_histogram256[_with_mask] (runner.hpp:5849-5889, kernels
 // runner.hpp:4399-4514): counts of quantized bytes over v[0, n), where
 // mask[i] == 1 when a mask is given.  step_inverse is
-// float(256 / (double(v_max) - double(v_min))).
-inline void histogram256(const float* v, const float* mask, uint32_t n, float v_min, float v_max,
-                         uint32_t hist[256]) {
-  const float step_inverse = float(256.0 / (double(v_max) - double(v_min)));
+// TF(256 / (double(v_max) - double(v_min))).
+template <class TF>
+void histogram256(const TF* v, const TF* mask, uint32_t n, TF v_min, TF v_max,
+                  uint32_t hist[256]) {
+  const TF step_inverse = TF(256.0 / (double(v_max) - double(v_min)));
   for (int b = 0; b < 256; ++b) hist[b] = 0;
   for (uint32_t i = 0; i < n; ++i)
-    if (!mask || mask[i] == 1.0f) ++hist[quantize_byte(v[i], v_min, step_inverse)];
+    if (!mask || mask[i] == TF(1)) ++hist[quantize_byte(v[i], v_min, step_inverse)];
 }
 
 // calculate_kl_divergence (runner.hpp:4803-4815 with KLDivergence,

@@ -62,7 +62,7 @@ ABI_STRUCTS = {
     "StepReport": "al_step_report", "Fluid": "al_fluid_f32", "WarmNet": "al_warm_net",
     "WarmStart": "al_warm_start", "SceneF32": "al_scene_f32",
     "ContactBodyF32": "al_contact_body_f32", "ContactF32": "al_contact_f32",
-    "SampleF32": "al_sample_f32", "PelletsF32": "al_pellets_f32",
+    "SampleF32": "al_sample_f32", "SampleF64": "al_sample_f64", "PelletsF32": "al_pellets_f32",
     "PelletsF64": "al_pellets_f64", "PelletRelaxParams": "al_pellet_relax_params",
 }
 
