@@ -173,3 +173,37 @@ def test_empty_fluid_step(engine):
     scene = scenes.DeviceScene(engine, dtype, cn, cni, x, [])
     dt, rep = scene.step("df", scenes.solver_params(), 1e-4)
     assert dt == pytest.approx(1e-4)
+
+
+@pytest.mark.parametrize("method", ["df", "ii", "i"])
+def test_step_parity_with_truncated_neighbor_lists(engine, method):
+    """max_num_neighbors_per_particle below the lattice's ~30 neighbors: the
+    reference keeps the first `cap` candidates in its scan order and flags
+    grid_anomaly[2] (runner.hpp:1896-1909); every pass of the step then
+    sums over the truncated (asymmetric) lists.  The engine keeps the same
+    entries, reports AL_ERR_NEIGHBOR_OVERFLOW after writing its outputs, and
+    the step matches the oracle's truncated step within the float32
+    four-step bounds."""
+    dtype = np.float32
+    extra = [dict(shape=_capi.SHAPE_SPHERE, params=[0.035], sign=1.0, resolution=16,
+                  use_distance_grid=True, mass=0.12, inertia=scenes.sphere_inertia(0.12, 0.035),
+                  x=(0.14, 0.32, 0.13), v=(0.0, -0.3, 0.0))]
+    scene = scenes.dam_break(engine, dtype, (12, 10, 10), 0.01, (0.45, 0.4, 0.35), extra,
+                             seed=9, volume_resolution=16, max_num_neighbors_per_particle=20)
+    sp = scenes.solver_params()
+    steps = 2
+    ostate, origid, odt, oreps = _oracle_run(scene, method, sp, 1e-4, steps)
+    dt = 1e-4
+    reps = []
+    for _ in range(steps):
+        dt, rep = scene.step(method, sp, dt, allow=(_capi.AL_ERR_NEIGHBOR_OVERFLOW,))
+        reps.append(rep)
+    for r, o in zip(reps, oreps):
+        assert list(r.grid_anomaly) == [0, 0, 1] and list(o.grid_anomaly) == [0, 0, 1]
+        assert r.num_density_solve == o.num_density_solve
+        assert r.num_divergence_solve == o.num_divergence_solve
+    tol = TOL[(dtype, 4)]
+    g = scene.state()
+    _close(g["x"], ostate["x"], tol["x"], "x")
+    _close(g["v"], ostate["v"], tol["v"], "v")
+    _close(g["density"], ostate["density"], tol["density"], "density")
