@@ -203,8 +203,9 @@ def test_oracle_step_in_container(method):
 
 
 def test_oracle_float32_tracks_float64():
-    """The error of the float32 path against the float64 plain method after a
-    few steps (stated in DESIGN.md)."""
+    """The error of the float32 path against the float64 plain method after
+    three steps of the 216-particle container scene: positions within 1e-6 m,
+    velocities within 1e-3 of their scale."""
     out = {}
     for dtype in (np.float32, np.float64):
         cn, cni, bodies, rigid, state, keep = _host_scene(dtype)
