@@ -1,6 +1,6 @@
 // pyalluvion_b200.cpp -- pybind11 module with the reference's Python class
 // names (lib/pyalluvion.cu: Store, Const<suffix>, ConstiN, Runner, Pile,
-// Solver, SolverDf, SolverIi, SolverI and the dg distances, suffixed
+// Solver, SolverDf, SolverIi, SolverI, SolverPellet and the dg distances, suffixed
 // "float" / "double") over the C++ layer of alluvion_b200_solver.hpp.
 // Variables expose the numpy get / set of the reference's Coated variables
 // (alluvion/variable.py:22-44) and __cuda_array_interface__ for zero-copy
@@ -222,10 +222,30 @@ void declare_real(py::module& m, py::module& dg_m, const char* sfx) {
       .def(
           "add",
           [](P& p, std::shared_ptr<dg::Distance<TF>> d, py::object resolution, TF cell_width,
-             TF margin, TF sign, py::object collision_mesh, TF mass, TF restitution, TF friction,
-             py::object inertia, py::object x, py::object q, py::object) {
+             TF margin, TF sign, py::object collision_mesh, py::object pellets, TF mass,
+             TF restitution, TF friction, py::object inertia, py::object x, py::object q,
+             py::object) {
             auto r = resolution.cast<std::vector<uint32_t>>();
             if (r.size() != 3) throw error(AL_ERR_INVALID, "resolution: 3 components");
+            if (!pellets.is_none()) {  // the pellet overload: numpy [n][3] or a Variable
+              std::vector<std::array<TF, 3>> pl;
+              if (py::isinstance<Variable>(pellets)) {
+                const Variable& v = pellets.cast<const Variable&>();
+                if (v.get_num_primitives_per_element() != 3 ||
+                    v.get_type() != numeric_type_of<TF>())
+                  throw error(AL_ERR_INVALID, "pellets: a [n] x 3 variable of the pile's type");
+                pl.resize(v.get_linear_shape());
+                if (!pl.empty()) v.get_bytes(pl.data(), pl.size() * sizeof(pl[0]));
+              } else {
+                py::array_t<TF, py::array::c_style | py::array::forcecast> a(pellets);
+                if (a.ndim() != 2 || a.shape(1) != 3)
+                  throw error(AL_ERR_INVALID, "pellets: [n][3]");
+                pl.resize(a.shape(0));
+                if (!pl.empty()) std::memcpy(pl.data(), a.data(), a.nbytes());
+              }
+              return p.add(std::move(d), {r[0], r[1], r[2]}, cell_width, margin, sign, pl, mass,
+                           restitution, friction, t3<TF>(inertia), t3<TF>(x), t4<TF>(q));
+            }
             Mesh<TF> cm;
             if (!collision_mesh.is_none()) cm = collision_mesh.cast<Mesh<TF>>();
             return p.add(std::move(d), {r[0], r[1], r[2]}, cell_width, margin, sign, cm, mass,
@@ -233,11 +253,14 @@ void declare_real(py::module& m, py::module& dg_m, const char* sfx) {
           },
           py::arg("distance"), py::arg("resolution") = std::vector<uint32_t>{0, 0, 0},
           py::arg("cell_width") = TF(0), py::arg("margin") = std::numeric_limits<TF>::infinity(),
-          py::arg("sign") = TF(1), py::arg("collision_mesh") = py::none(), py::arg("mass") = TF(0),
+          py::arg("sign") = TF(1), py::arg("collision_mesh") = py::none(),
+          py::arg("pellets") = py::none(), py::arg("mass") = TF(0),
           py::arg("restitution") = TF(1), py::arg("friction") = TF(0),
           py::arg("inertia_tensor") = std::vector<TF>{1, 1, 1},
           py::arg("x") = std::vector<TF>{0, 0, 0}, py::arg("q") = std::vector<TF>{0, 0, 0, 1},
           py::arg("display_mesh") = py::none())
+      .def_property_readonly("num_pellets", &P::num_pellets)
+      .def_readonly("max_num_pellets", &P::max_num_pellets_)
       .def("get_size", &P::get_size)
       .def("set_gravity", [](P& p, py::object g) { p.set_gravity(t3<TF>(g)); })
       .def("copy_kinematics_to_device", &P::copy_kinematics_to_device)
@@ -353,6 +376,21 @@ void declare_real(py::module& m, py::module& dg_m, const char* sfx) {
         .def("step", &Sp::template step<0>)
         .def("step_wrap1", &Sp::template step<1>);
   };
+  using Pel = SolverPellet<TF>;
+  py::class_<Pel, S>(m, ("SolverPellet" + s).c_str())
+      .def(py::init<Runner<TF>&, P&, Store&, uint32_t, const Const<TF>*, const ConstiN*, bool>(),
+           py::arg("runner"), py::arg("pile"), py::arg("store"), py::arg("max_num_particles"),
+           py::arg("cn") = nullptr, py::arg("cni") = nullptr, py::arg("graphical") = false,
+           py::keep_alive<1, 2>(), py::keep_alive<1, 3>(), py::keep_alive<1, 4>())
+      .def_readwrite("cfl_factor", &Pel::cfl_factor)
+      .def_readwrite("cohesion", &Pel::cohesion)
+      .def_readwrite("adhesion", &Pel::adhesion)
+      .def_property_readonly("particle_dfsph_factor",
+                             [](const Pel& x) { return x.particle_dfsph_factor; }, ref)
+      .def("set_pellets", &Pel::set_pellets)
+      .def("step", &Pel::template step<0>)
+      .def("step_wrap1", &Pel::template step<1>);
+
   struct IiTag {
     using type = SolverIi<TF>;
   };

@@ -25,7 +25,8 @@ import numpy as np
 from . import _alluvion_b200 as _al
 from ._alluvion_b200 import NumericType, Store, VolumeMethod  # noqa: F401
 
-_FLOAT_TYPED = ["Runner", "Pile", "SolverDf", "SolverIi", "SolverI", "Solver", "Mesh", "Const"]
+_FLOAT_TYPED = ["Runner", "Pile", "SolverDf", "SolverIi", "SolverI", "SolverPellet", "Solver",
+                "Mesh", "Const"]
 _FLOAT_TYPED_DG = ["BoxDistance", "BoxShellDistance", "CapsuleDistance", "CylinderDistance",
                    "Distance", "InfiniteCylinderDistance", "InfiniteTubeDistance",
                    "SphereDistance", "MeshDistance", "TriangleMesh"]

@@ -88,6 +88,7 @@ struct real<float> {
   static constexpr auto ii_step = al_ii_step_f32;
   static constexpr auto i_step = al_i_step_f32;
   static constexpr auto i_step_pellets = al_i_step_pellets_f32;
+  static constexpr auto relax_pellets = al_relax_pellets_f32;
   static constexpr auto update_particle_neighbors = al_update_particle_neighbors_f32;
   static constexpr auto update_particle_neighbors_periodic =
       al_update_particle_neighbors_periodic_f32;
@@ -106,6 +107,7 @@ struct real<double> {
   static constexpr auto ii_step = al_ii_step_f64;
   static constexpr auto i_step = al_i_step_f64;
   static constexpr auto i_step_pellets = al_i_step_pellets_f64;
+  static constexpr auto relax_pellets = al_relax_pellets_f64;
   static constexpr auto update_particle_neighbors = al_update_particle_neighbors_f64;
   static constexpr auto update_particle_neighbors_periodic =
       al_update_particle_neighbors_periodic_f64;

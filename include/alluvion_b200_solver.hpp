@@ -4,8 +4,9 @@
  * Variable (store.hpp, variable.hpp), Const / ConstiN (constants.hpp),
  * the analytic and mesh distances (the dg distance headers), Pile (pile.hpp),
  * Runner (a tag: launches are the engine's), and Solver / SolverDf /
- * SolverIi / SolverI (solver.hpp, solver_df.hpp, solver_ii.hpp,
- * solver_i.hpp) with the reference's field names, defaults and step<wrap>.
+ * SolverIi / SolverI / SolverPellet (solver.hpp, solver_df.hpp,
+ * solver_ii.hpp, solver_i.hpp, solver_pellet.hpp) with the reference's
+ * field names, defaults and step<wrap>.
  * Header-only; the pybind11 module alluvion_b200/_alluvion_b200 exposes it
  * with the reference's Python class names.
  *
@@ -20,8 +21,9 @@
  *    sums, narrowed), and no per-particle particle_force / particle_torque
  *    buffers exist.
  *  - Options outside the engine's scope (ushers, surface tension,
- *    vorticity, graphical buffers, the pellet volume method of Pile)
- *    throw error(AL_ERR_UNSUPPORTED).
+ *    vorticity, graphical buffers) throw error(AL_ERR_UNSUPPORTED); a
+ *    pile with VolumeMethod::pellets steps with SolverI (its pellet branch)
+ *    and relaxes with SolverPellet, as in the reference.
  */
 #ifndef ALLUVION_B200_SOLVER_HPP
 #define ALLUVION_B200_SOLVER_HPP
@@ -382,18 +384,13 @@ class Pile {
   Pile(Store& store, Runner<TF>& runner, uint32_t max_num_contacts,
        VolumeMethod volume_method = VolumeMethod::volume_map, uint32_t max_num_pellets = 10000,
        const Const<TF>* cn = nullptr, const ConstiN* cni = nullptr)
-      : store_(store),
+      : max_num_contacts_(max_num_contacts),
+        max_num_pellets_(volume_method == VolumeMethod::pellets ? max_num_pellets : 0),
+        volume_method_(volume_method),
+        store_(store),
         runner_(runner),
-        max_num_contacts_(max_num_contacts),
-        max_num_pellets_(0),
         cn_(cn ? cn : &store.get_cn<TF>()),
-        cni_(cni ? cni : &store.get_cni()) {
-    (void)max_num_pellets;
-    if (volume_method != VolumeMethod::volume_map)
-      throw error(AL_ERR_UNSUPPORTED,
-                  "Pile: the pellet volume method is not a volume-map pile (use the pellet "
-                  "step entry points)");
-  }
+        cni_(cni ? cni : &store.get_cni()) {}
   Pile(const Pile&) = delete;
   Pile& operator=(const Pile&) = delete;
   ~Pile() {
@@ -401,6 +398,7 @@ class Pile {
       if (v) store_.remove(*v);
     for (Variable* v : volume_grids_)
       if (v) store_.remove(*v);
+    if (pellet_x_) store_.remove(*pellet_x_);
   }
 
   // Pile::add (pile.hpp:217-284, 285-349): grid domain and resolution by
@@ -412,6 +410,32 @@ class Pile {
                const Mesh<TF>& collision_mesh = Mesh<TF>(), TF mass = 0, TF restitution = 1,
                TF friction = 0, T3 inertia_tensor = {1, 1, 1}, T3 x = {0, 0, 0},
                TQ q = {0, 0, 0, 1}) {
+    return add_impl(std::move(distance), resolution, cell_width, margin, sign,
+                    collision_mesh.vertices, {}, mass, restitution, friction, inertia_tensor, x,
+                    q);
+  }
+  // The pellet overload (pile.hpp:217-284): with VolumeMethod::pellets the
+  // body-frame pellets are the body's boundary particles and its collision
+  // vertices; the pile's pellet count may not pass max_num_pellets.
+  uint32_t add(std::shared_ptr<dg::Distance<TF>> distance, std::array<uint32_t, 3> resolution,
+               TF cell_width, TF margin, TF sign, const std::vector<T3>& pellets, TF mass = 0,
+               TF restitution = 1, TF friction = 0, T3 inertia_tensor = {1, 1, 1},
+               T3 x = {0, 0, 0}, TQ q = {0, 0, 0, 1}) {
+    if (volume_method_ != VolumeMethod::pellets && !pellets.empty())
+      throw error(AL_ERR_INVALID, "Pile::add: pellets need VolumeMethod::pellets");
+    if (num_pellets_ + pellets.size() > max_num_pellets_)
+      throw error(AL_ERR_INVALID, "Pile::add: the pellet count " +
+                                      std::to_string(num_pellets_ + pellets.size()) +
+                                      " exceeds the limit " + std::to_string(max_num_pellets_));
+    return add_impl(std::move(distance), resolution, cell_width, margin, sign, pellets, pellets,
+                    mass, restitution, friction, inertia_tensor, x, q);
+  }
+
+ private:
+  uint32_t add_impl(std::shared_ptr<dg::Distance<TF>> distance,
+                    std::array<uint32_t, 3> resolution, TF cell_width, TF margin, TF sign,
+                    const std::vector<T3>& collision_vertices, const std::vector<T3>& pellets,
+                    TF mass, TF restitution, TF friction, T3 inertia_tensor, T3 x, TQ q) {
     if (!distance) throw error(AL_ERR_INVALID, "Pile::add: distance is null");
     if (get_size() >= AL_MAX_BOUNDARIES)
       throw error(AL_ERR_UNSUPPORTED, "Pile::add: at most AL_MAX_BOUNDARIES bodies");
@@ -428,7 +452,10 @@ class Pile {
     force_.push_back({0, 0, 0});
     torque_.push_back({0, 0, 0});
     sign_list_.push_back(sign);
-    collision_vertex_list_.push_back(collision_mesh.vertices);
+    collision_vertex_list_.push_back(collision_vertices);
+    pellet_list_.push_back(pellets);
+    num_pellets_ += static_cast<uint32_t>(pellets.size());
+    pellets_dirty_ = true;
     // calculate_domain_and_resolution
     if (std::isinf(margin)) margin = sign < 0 ? cn_->kernel_radius : cn_->kernel_radius * 2;
     T3 dmin, dmax;
@@ -451,6 +478,8 @@ class Pile {
     build_grid(i);
     return i;
   }
+
+ public:
   // The reference's add(Distance*): the pile takes ownership.
   template <class... A>
   uint32_t add(dg::Distance<TF>* distance, A&&... rest) {
@@ -512,6 +541,25 @@ class Pile {
       for (int k = 0; k < 4; ++k) q_[i][k] = r[i].q[k];
     }
   }
+  // Body-frame pellets of every body, body after body, on the device (the
+  // reference's concatenated pellet buffer), and each body's count.
+  const Variable* local_pellets() {
+    if (pellets_dirty_) {
+      if (pellet_x_) store_.remove(*pellet_x_);
+      pellet_x_ = nullptr;
+      if (num_pellets_) {
+        std::vector<T3> all;
+        all.reserve(num_pellets_);
+        for (const auto& p : pellet_list_) all.insert(all.end(), p.begin(), p.end());
+        pellet_x_ = store_.create<TF>({num_pellets_}, 3);
+        pellet_x_->set_bytes(all.data(), all.size() * sizeof(T3));
+      }
+      pellets_dirty_ = false;
+    }
+    return pellet_x_;
+  }
+  uint32_t num_pellets() const { return num_pellets_; }
+  bool pellet_mode() const { return volume_method_ == VolumeMethod::pellets; }
   bool has_collision_vertices() const {
     for (const auto& c : collision_vertex_list_)
       if (!c.empty()) return true;
@@ -526,8 +574,10 @@ class Pile {
   std::vector<std::array<uint32_t, 3>> resolution_list_;
   std::vector<uint32_t> grid_size_list_;
   std::vector<std::vector<std::array<TF, 3>>> collision_vertex_list_;
+  std::vector<std::vector<std::array<TF, 3>>> pellet_list_;
   uint32_t max_num_contacts_;
   uint32_t max_num_pellets_;
+  VolumeMethod volume_method_;
 
  private:
   // Pile::build_grid (pile.hpp:497-622) with calculate_grid_attributes
@@ -559,6 +609,7 @@ class Pile {
               "Pile::add (mesh distance grid)");
       }
     }
+    if (volume_method_ != VolumeMethod::volume_map) return;  // pellets need no volume map
     volume_grids_[i] = store_.create<TF>({grid_size_list_[i]});
     const Body b = bodies()[i];
     check(real<TF>::build_volume_field(store_.eng(), cn_->c(), &b,
@@ -573,6 +624,9 @@ class Pile {
   std::vector<std::shared_ptr<dg::Distance<TF>>> distance_list_;
   std::vector<Variable*> distance_grids_, volume_grids_;
   T3 gravity_{0, 0, 0};
+  uint32_t num_pellets_ = 0;
+  bool pellets_dirty_ = false;
+  Variable* pellet_x_ = nullptr;
 };
 
 // Solver<TF> (solver.hpp): particle buffers, time stepping fields, the
@@ -598,8 +652,10 @@ class Solver {
                   "the engine's scope");
     particle_radius = cn_->particle_radius;
     const uint32_t n = max_num_particles, nb = std::max<uint32_t>(pile.get_size(), 1);
-    particle_x = store.create<TF>({n}, 3);
-    particle_v = store.create<TF>({n}, 3);
+    // the pellets' world positions and velocities follow the particles
+    // (solver.hpp:30-36)
+    particle_x = store.create<TF>({n + pile.max_num_pellets_}, 3);
+    particle_v = store.create<TF>({n + pile.max_num_pellets_}, 3);
     particle_a = store.create<TF>({n}, 3);
     particle_density = store.create<TF>({n});
     particle_boundary = store.create<TF>({nb, n}, 4);
@@ -816,6 +872,8 @@ class SolverDf : public Solver<TF> {
   // SolverDf::step<wrap> (solver_df.hpp:74-359).
   template <uint32_t wrap>
   void step() {
+    if (this->pile.pellet_mode())
+      throw error(AL_ERR_UNSUPPORTED, "SolverDf::step: pellet piles step with SolverI");
     al_solver_params p = this->base_params(wrap);
     p.density_change_tolerance = density_change_tolerance;
     p.density_error_tolerance = density_error_tolerance;
@@ -864,7 +922,7 @@ class SolverPressure : public Solver<TF> {
                  const ConstiN* cni = nullptr, bool graphical = false)
       : Base(runner, pile, store, max_num_particles, num_ushers, enable_surface_tension,
              enable_vorticity, cn, cni, graphical) {
-    particle_pressure = store.create<TF>({max_num_particles});
+    particle_pressure = store.create<TF>({max_num_particles + pile.max_num_pellets_});
     particle_adv_density = store.create<TF>({max_num_particles});
   }
   ~SolverPressure() override {
@@ -880,15 +938,41 @@ class SolverPressure : public Solver<TF> {
     p.min_density_solve = min_density_solve;
     p.max_density_solve = max_density_solve;
     p.enable_density_solve = 1;
-    const auto f = this->fluid_table(nullptr, nullptr, nullptr,
-                                     particle_adv_density->template data<TF>(),
-                                     particle_pressure->template data<TF>());
-    const al_step_report rep = this->run_step(
-        [&](al_engine* e, auto* cn, auto* ci, auto* b, auto* r, auto* pp, TF* d, auto* rp) {
-          return Implicit ? real<TF>::i_step(e, cn, ci, &f, b, r, pp, d, rp, nullptr)
-                          : real<TF>::ii_step(e, cn, ci, &f, b, r, pp, d, rp, nullptr);
-        },
-        p, Implicit ? "SolverI::step" : "SolverIi::step");
+    auto f = this->fluid_table(nullptr, nullptr, nullptr,
+                               particle_adv_density->template data<TF>(),
+                               particle_pressure->template data<TF>());
+    al_step_report rep;
+    if (this->pile.pellet_mode()) {
+      if (!Implicit)
+        throw error(AL_ERR_UNSUPPORTED, "SolverIi::step: pellet piles step with SolverI");
+      // the pellet branch of SolverI::step (solver_i.hpp:79-327): pellet
+      // world positions, velocities and pressures land after the particles
+      f.particle_boundary = nullptr;
+      f.particle_boundary_kernel = nullptr;
+      typename real<TF>::pellets pel;
+      std::memset(&pel, 0, sizeof(pel));
+      const Variable* lp = this->pile.local_pellets();
+      const uint32_t n = this->num_particles;
+      pel.local_x = lp ? lp->template data<TF>() : nullptr;
+      pel.num_pellets = this->pile.num_pellets();
+      for (uint32_t b = 0; b < this->pile.get_size(); ++b)
+        pel.count[b] = uint32_t(this->pile.pellet_list_[b].size());
+      pel.x = this->particle_x->template data<TF>() + size_t(n) * 3;
+      pel.v = this->particle_v->template data<TF>() + size_t(n) * 3;
+      pel.pressure = particle_pressure->template data<TF>() + n;
+      rep = this->run_step(
+          [&](al_engine* e, auto* cn, auto* ci, auto* b, auto* r, auto* pp, TF* d, auto* rp) {
+            return real<TF>::i_step_pellets(e, cn, ci, &f, b, r, &pel, pp, d, rp, nullptr);
+          },
+          p, "SolverI::step (pellets)");
+    } else {
+      rep = this->run_step(
+          [&](al_engine* e, auto* cn, auto* ci, auto* b, auto* r, auto* pp, TF* d, auto* rp) {
+            return Implicit ? real<TF>::i_step(e, cn, ci, &f, b, r, pp, d, rp, nullptr)
+                            : real<TF>::ii_step(e, cn, ci, &f, b, r, pp, d, rp, nullptr);
+          },
+          p, Implicit ? "SolverI::step" : "SolverIi::step");
+    }
     num_density_solve = rep.num_density_solve;
     mean_density_error = TF(rep.mean_density_error);
   }
@@ -904,6 +988,59 @@ template <class TF>
 using SolverIi = SolverPressure<TF, false>;
 template <class TF>
 using SolverI = SolverPressure<TF, true>;
+
+// SolverPellet<TF> (solver_pellet.hpp): spreads pellets inside or around
+// the pile's one body by relaxation steps (cohesion / adhesion
+// displacement, the pellet DFSPH divergence iteration, a CFL-limited move
+// that keeps them off the boundary).  particle_v receives each step's
+// displacement and particle_density the pellets' density, as in the
+// reference.
+template <class TF>
+class SolverPellet : public Solver<TF> {
+ public:
+  using Base = Solver<TF>;
+  SolverPellet(Runner<TF>& runner, Pile<TF>& pile, Store& store, uint32_t max_num_particles,
+               const Const<TF>* cn = nullptr, const ConstiN* cni = nullptr,
+               bool graphical = false)
+      : Base(runner, pile, store, max_num_particles, 0, false, false, cn, cni, graphical) {
+    particle_dfsph_factor = store.create<TF>({max_num_particles});
+  }
+  ~SolverPellet() override { this->store.remove(*particle_dfsph_factor); }
+  // SolverPellet::set_pellets (solver_pellet.hpp:53-56).
+  void set_pellets(const Variable& x) {
+    const uint32_t n = x.get_linear_shape();
+    if (n > this->max_num_particles)
+      throw error(AL_ERR_INVALID, "SolverPellet::set_pellets: more pellets than max_num_particles");
+    this->num_particles = n;
+    this->particle_x->set_from(x);
+  }
+  // SolverPellet::step<wrap> (solver_pellet.hpp:57-119).
+  template <uint32_t wrap>
+  void step() {
+    this->check_counts();
+    if (this->pile.get_size() != 1)
+      throw error(AL_ERR_INVALID, "SolverPellet::step: the pile must hold one body");
+    const auto bodies = this->pile.bodies();
+    al_pellet_relax_params p;
+    std::memset(&p, 0, sizeof(p));
+    p.cohesion = cohesion;
+    p.adhesion = adhesion;
+    p.cfl_factor = cfl_factor;
+    p.contact_tolerance = this->cn_->contact_tolerance;
+    p.wrap_y = wrap;
+    p.wrap_length = double(this->cn_->wrap_length);
+    ConstiN ci = *this->cni_;
+    ci.num_boundaries = 0;
+    check(real<TF>::relax_pellets(this->store.eng(), this->cn_->c(), &ci, bodies.data(),
+                                  this->particle_x->template data<TF>(), this->num_particles, &p,
+                                  1u, this->particle_v->template data<TF>(),
+                                  this->particle_density->template data<TF>(), nullptr),
+          "SolverPellet::step");
+  }
+
+  TF cohesion = 4, adhesion = 2, cfl_factor = TF(0.25);
+  Variable* particle_dfsph_factor;
+};
 
 }  // namespace alluvion_b200
 

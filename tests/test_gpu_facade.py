@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from alluvion_b200 import _capi, scenes
-from alluvion_b200.depot import Depot
+from alluvion_b200.depot import Depot, VolumeMethod
 
 pytestmark = pytest.mark.gpu
 
@@ -160,8 +160,12 @@ def test_unsupported_options_raise(engine):
     pile = dp.Pile(dp, runner, 0)
     with pytest.raises(RuntimeError):
         dp.SolverDf(runner, pile, dp, 100, enable_vorticity=True)
+    # pellets belong to VolumeMethod.pellets piles, within max_num_pellets
     with pytest.raises(RuntimeError):
-        dp.Pile(dp, runner, 0, volume_method=dp_volume_pellets())
+        pile.add(dp.SphereDistance.create(0.05), [4, 4, 4], pellets=np.zeros((3, 3), np.float32))
+    ppile = dp.Pile(dp, runner, 0, volume_method=VolumeMethod.pellets, max_num_pellets=4)
+    with pytest.raises(RuntimeError):
+        ppile.add(dp.SphereDistance.create(0.05), [4, 4, 4], pellets=np.zeros((5, 3), np.float32))
     s = dp.SolverDf(runner, pile, dp, 100)
     s.num_particles = 101
     s.dt = 1e-4
@@ -169,6 +173,111 @@ def test_unsupported_options_raise(engine):
         s.step()
 
 
-def dp_volume_pellets():
-    from alluvion_b200.depot import VolumeMethod
-    return VolumeMethod.pellets
+
+def _depot_consts(dp, cni_src, r=R):
+    cn, cni = dp.cn, dp.cni
+    cn.set_kernel_radius(4 * r)
+    cn.set_particle_attr(r, 1000.0 * (2 * r) ** 3, 1000.0)
+    cn.viscosity = 0.01
+    cn.boundary_viscosity = 0.01
+    cn.dfsph_factor_epsilon = 1e-6
+    cn.gravity = (0.0, -9.81, 0.0)
+    cni.grid_res = list(cni_src.grid_res)
+    cni.grid_offset = list(cni_src.grid_offset)
+    cni.max_num_particles_per_cell = cni_src.max_num_particles_per_cell
+    cni.max_num_neighbors_per_particle = cni_src.max_num_neighbors_per_particle
+    return cn, cni
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_depot_pellet_step_matches_the_c_abi(engine, dtype):
+    """SolverI on a pile with VolumeMethod.pellets (a box of pellets and a
+    moving, spinning sphere of pellets) steps as al_i_step_pellets does;
+    the pellets' world positions and pressures land after the particles in
+    particle_x / particle_pressure, as in the reference."""
+    from test_gpu_pellets import _scene as pellet_scene, _device_run
+    r = 0.01
+    cn_abi, cni_abi, x, barr, rarr, local, counts = pellet_scene(dtype)
+    sp = scenes.solver_params()
+    ref = _device_run(engine, dtype, cn_abi, cni_abi, x, barr, rarr, local, counts, sp, 1e-4, 2)
+    dp = Depot(dtype)
+    _depot_consts(dp, cni_abi, r)
+    runner = dp.Runner()
+    pile = dp.Pile(dp, runner, 0, volume_method=VolumeMethod.pellets,
+                   max_num_pellets=len(local))
+    size = 30 * r
+    c0 = counts[0]
+    pile.add(dp.BoxShellDistance.create([size] * 3, 2 * r), [1, 1, 1], pellets=local[:c0],
+             x=[size / 2] * 3)
+    rad = 4 * r
+    m = 0.2
+    pile.add(dp.SphereDistance.create(rad), [1, 1, 1], pellets=local[c0:], mass=m,
+             inertia_tensor=list(scenes.sphere_inertia(m, rad)),
+             x=list(r * np.asarray((23.5, 8.0, 15.0))))
+    v, om = pile.v, pile.omega
+    v[1], om[1] = [-0.2, 0.0, 0.0], [0.0, 0.0, 1.0]
+    pile.v, pile.omega = v, om
+    pile.set_gravity((0.0, -9.81, 0.0))
+    assert pile.num_pellets == len(local)
+    solver = dp.SolverI(runner, pile, dp, max_num_particles=len(x))
+    n = len(x)
+    solver.num_particles = n
+    solver.particle_x.set(x)
+    solver.initial_dt = 1e-4
+    solver.reset_t()
+    solver.max_dt, solver.cfl = 2e-4, 0.4
+    for _ in range(2):
+        solver.step()
+    gx = solver.particle_x.get()
+    np.testing.assert_array_equal(gx[:n], ref["x"])
+    np.testing.assert_array_equal(solver.particle_v.get()[:n], ref["v"])
+    np.testing.assert_array_equal(solver.particle_pressure.get()[:n], ref["pressure"])
+    np.testing.assert_array_equal(gx[n:n + len(local)], ref["px"])
+    np.testing.assert_array_equal(solver.particle_pressure.get()[n:n + len(local)], ref["pp"])
+    assert solver.dt == ref["dt"]
+    np.testing.assert_array_equal(np.asarray(pile.x[1], dtype), ref["rigid"][1, :3])
+    # the other solvers do not step pellet piles
+    with pytest.raises(RuntimeError):
+        dp.SolverDf(runner, pile, dp, max_num_particles=n).step()
+
+
+def test_solver_pellet_matches_the_c_abi(engine):
+    """SolverPellet (set_pellets, step) relaxes pellets inside a sphere as
+    al_relax_pellets_f32 does: positions, displacements (particle_v) and
+    densities bit for bit."""
+    dtype = np.float32
+    cn = scenes.make_const(dtype, 0.01)
+    Rs = 0.2
+    body = scenes.make_body(dtype, cn, _capi.SHAPE_SPHERE, [Rs], 8, sign=-1.0)
+    cni = scenes.make_consti((-Rs - 0.05,) * 3, (Rs + 0.05,) * 3, float(cn.kernel_radius))
+    m = int(np.ceil(Rs / 0.02))
+    a = 0.02 * (np.arange(-m, m + 1) + 0.25)
+    g = np.stack(np.meshgrid(a, a, a, indexing="ij"), -1).reshape(-1, 3)
+    g = g[np.linalg.norm(g, axis=1) < Rs - 0.03]
+    rng = np.random.Generator(np.random.PCG64(2))
+    x = (g + rng.uniform(-0.004, 0.004, g.shape)).astype(np.float32)
+    X = torch.from_numpy(x.copy()).cuda()
+    DX = torch.zeros_like(X)
+    RHO = torch.zeros(len(x), device="cuda")
+    p = _capi.pellet_relax_params()
+    for _ in range(2):
+        _capi.check(_capi.lib().al_relax_pellets_f32(
+            engine.handle, _capi.ptr(cn), _capi.ptr(cni), _capi.ptr(body), X.data_ptr(), len(x),
+            _capi.ptr(p), 1, DX.data_ptr(), RHO.data_ptr(), None), "relax")
+    dp = Depot(dtype)
+    _depot_consts(dp, cni, 0.01)
+    runner = dp.Runner()
+    pile = dp.Pile(dp, runner, 0, volume_method=VolumeMethod.pellets, max_num_pellets=0)
+    pile.add(dp.SphereDistance.create(Rs), [8, 8, 8], sign=-1)
+    solver = dp.SolverPellet(runner, pile, dp, max_num_particles=len(x))
+    assert (solver.cohesion, solver.adhesion, solver.cfl_factor) == (4.0, 2.0, 0.25)
+    pel = dp.create(len(x), 3)
+    pel.set(x)
+    solver.set_pellets(pel)
+    assert solver.num_particles == len(x)
+    for _ in range(2):
+        solver.step()
+    n = len(x)
+    np.testing.assert_array_equal(solver.particle_x.get()[:n], X.cpu().numpy())
+    np.testing.assert_array_equal(solver.particle_v.get()[:n], DX.cpu().numpy())
+    np.testing.assert_array_equal(solver.particle_density.get()[:n], RHO.cpu().numpy())
