@@ -264,6 +264,11 @@ void declare_real(py::module& m, py::module& dg_m, const char* sfx) {
       .def("get_size", &P::get_size)
       .def("set_gravity", [](P& p, py::object g) { p.set_gravity(t3<TF>(g)); })
       .def("copy_kinematics_to_device", &P::copy_kinematics_to_device)
+      .def("write_file", &P::write_file, py::arg("filename"), py::arg("x_scale") = TF(1),
+           py::arg("v_scale") = TF(1), py::arg("omega_scale") = TF(1))
+      .def("read_file", &P::read_file, py::arg("filename"), py::arg("num_rigids") = -1,
+           py::arg("dst_offset") = 0, py::arg("src_offset") = 0)
+      .def_static("get_size_from_file", &P::get_size_from_file, py::arg("filename"))
       .def_readwrite("mass", &P::mass_)
       .def_readwrite("x", &P::x_)
       .def_readwrite("v", &P::v_)
@@ -435,6 +440,9 @@ PYBIND11_MODULE(_alluvion_b200, m) {
              v.set_bytes(a.data(), size_t(a.nbytes()), offset);
            },
            py::arg("src"), py::arg("offset") = 0)
+      .def("write_file", &Variable::write_file, py::arg("filename"),
+           py::arg("shape_outermost") = 0, py::arg("offset") = 0)
+      .def("read_file", &Variable::read_file, py::arg("filename"))
       .def("set_zero", &Variable::set_zero)
       .def("set_from", &Variable::set_from)
       .def("get", &variable_get)

@@ -32,6 +32,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <fstream>
 #include <limits>
 #include <memory>
 #include <string>
@@ -99,9 +100,99 @@ class Variable {
     const size_t b = std::min(src.get_num_bytes(), get_num_bytes());
     check(al_copy(engine_, ptr_, src.ptr_, b), "Variable::set_from");
   }
+  // Variable::write_file (variable.hpp:132-167): the shape (outermost entry
+  // shape_outermost, 0 = all), a 0 terminator, the primitives per element,
+  // the type label, then the elements from element `offset` on.  (With
+  // shape_outermost 0 the reference writes the header of the whole variable
+  // but no elements; here the elements follow, as the header says.)
+  void write_file(const std::string& filename, uint32_t shape_outermost = 0,
+                  uint32_t offset = 0) const {
+    if (shape_.empty()) throw error(AL_ERR_INVALID, "write_file: empty variable");
+    if (shape_outermost > shape_[0])
+      throw error(AL_ERR_INVALID, "Writing more than the outermost shape (" +
+                                      std::to_string(shape_outermost) + ">" +
+                                      std::to_string(shape_[0]) + ").");
+    if (shape_outermost == 0) shape_outermost = shape_[0];
+    const size_t esize = numeric_size(type_) * n_;
+    const size_t per_outer = size_t(get_linear_shape()) / shape_[0];
+    const size_t bytes = per_outer * shape_outermost * esize, boff = size_t(offset) * esize;
+    if (bytes + boff > get_num_bytes())
+      throw error(AL_ERR_INVALID, "Writing more than allocated: " + std::to_string(bytes + boff) +
+                                      " " + std::to_string(get_num_bytes()));
+    std::ofstream f(filename, std::ios::binary | std::ios::trunc);
+    if (!f) throw error(AL_ERR_INVALID, "Failed to open alu file: " + filename);
+    for (size_t i = 0; i < shape_.size(); ++i) {
+      const uint32_t v = i == 0 ? shape_outermost : shape_[i];
+      f.write(reinterpret_cast<const char*>(&v), 4);
+    }
+    const uint32_t end = 0;
+    f.write(reinterpret_cast<const char*>(&end), 4);
+    f.write(reinterpret_cast<const char*>(&n_), 4);
+    const char label = type_label(type_);
+    f.write(&label, 1);
+    std::vector<char> host(bytes);
+    if (bytes) get_bytes(host.data(), bytes, boff);
+    f.write(host.data(), std::streamsize(bytes));
+  }
+  // Variable::read_file (variable.hpp:169-262): checks the dimensions, the
+  // inner shape and the primitives per element, converts float <-> double,
+  // and returns the outermost shape read.
+  uint32_t read_file(const std::string& filename) {
+    std::ifstream f(filename, std::ios::binary);
+    if (!f.is_open()) throw error(AL_ERR_INVALID, "Failed to open alu file: " + filename);
+    uint32_t outer = 0;
+    for (size_t i = 0; i < shape_.size(); ++i) {
+      uint32_t v = 0;
+      f.read(reinterpret_cast<char*>(&v), 4);
+      if (v == 0) throw error(AL_ERR_INVALID, "Shape mismatch when reading " + filename);
+      if (i == 0) {
+        outer = v;
+        if (outer > shape_[0])
+          throw error(AL_ERR_INVALID, "Reading more than the outermost shape: " + filename);
+      } else if (v != shape_[i]) {
+        throw error(AL_ERR_INVALID, "Shape mismatch for shape item " + std::to_string(i) +
+                                        ": " + filename);
+      }
+    }
+    uint32_t end = 1, p = 0;
+    f.read(reinterpret_cast<char*>(&end), 4);
+    if (end != 0) throw error(AL_ERR_INVALID, "Dimension mismatch when reading " + filename);
+    f.read(reinterpret_cast<char*>(&p), 4);
+    if (p != n_)
+      throw error(AL_ERR_INVALID, "Num primitives per unit mismatch when reading " + filename);
+    char label = 0;
+    f.read(&label, 1);
+    const size_t prims = size_t(get_linear_shape()) / shape_[0] * outer * n_;
+    const char mine = type_label(type_);
+    std::vector<char> host(prims * numeric_size(type_));
+    if (label == mine) {
+      f.read(host.data(), std::streamsize(host.size()));
+    } else if (label == 'f' && mine == 'd') {
+      std::vector<float> src(prims);
+      f.read(reinterpret_cast<char*>(src.data()), std::streamsize(prims * 4));
+      for (size_t i = 0; i < prims; ++i) reinterpret_cast<double*>(host.data())[i] = src[i];
+    } else if (label == 'd' && mine == 'f') {
+      std::vector<double> src(prims);
+      f.read(reinterpret_cast<char*>(src.data()), std::streamsize(prims * 8));
+      for (size_t i = 0; i < prims; ++i)
+        reinterpret_cast<float*>(host.data())[i] = static_cast<float>(src[i]);
+    } else {
+      throw error(AL_ERR_INVALID, "Data type mismatch when reading " + filename);
+    }
+    if (!host.empty()) set_bytes(host.data(), host.size());
+    return outer;
+  }
 
  private:
   friend class Store;
+  static char type_label(NumericType t) {
+    switch (t) {
+      case NumericType::f32: return 'f';
+      case NumericType::f64: return 'd';
+      case NumericType::i32: return 'i';
+      default: return 'u';
+    }
+  }
   void bounds(size_t num_bytes, size_t offset, const char* where) const {
     if (offset > get_num_bytes() || num_bytes > get_num_bytes() - offset)
       throw error(AL_ERR_INVALID, std::string(where) + ": range past the end of the variable");
@@ -490,6 +581,48 @@ class Pile {
   const T3& gravity() const { return gravity_; }
   // Kinematics travel by value with each step.
   void copy_kinematics_to_device() {}
+  // Pile::write_file / read_file / get_size_from_file (pile.hpp:757-793):
+  // per body x, v, q, omega of the real type; x, v and omega scaled on
+  // writing.
+  void write_file(const std::string& filename, TF x_scale = 1, TF v_scale = 1,
+                  TF omega_scale = 1) const {
+    std::ofstream f(filename, std::ios::binary | std::ios::trunc);
+    if (!f) throw error(AL_ERR_INVALID, "Pile::write_file: cannot open " + filename);
+    for (uint32_t i = 0; i < get_size(); ++i) {
+      TF rec[13];
+      for (int k = 0; k < 3; ++k) {
+        rec[k] = x_[i][k] * x_scale;
+        rec[3 + k] = v_[i][k] * v_scale;
+        rec[10 + k] = omega_[i][k] * omega_scale;
+      }
+      for (int k = 0; k < 4; ++k) rec[6 + k] = q_[i][k];
+      f.write(reinterpret_cast<const char*>(rec), sizeof(rec));
+    }
+  }
+  void read_file(const std::string& filename, int num_rigids = -1, uint32_t dst_offset = 0,
+                 uint32_t src_offset = 0) {
+    std::ifstream f(filename, std::ios::binary);
+    uint32_t n = get_size();
+    if (num_rigids >= 0) n = std::min(n, uint32_t(num_rigids));
+    f.seekg(std::streamoff(13 * sizeof(TF)) * src_offset, std::ios_base::cur);
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t d = dst_offset + i;
+      if (d >= get_size()) throw error(AL_ERR_INVALID, "Pile::read_file: past the last body");
+      TF rec[13];
+      f.read(reinterpret_cast<char*>(rec), sizeof(rec));
+      for (int k = 0; k < 3; ++k) {
+        x_[d][k] = rec[k];
+        v_[d][k] = rec[3 + k];
+        omega_[d][k] = rec[10 + k];
+      }
+      for (int k = 0; k < 4; ++k) q_[d][k] = rec[6 + k];
+      if (f.peek() == std::ifstream::traits_type::eof()) break;
+    }
+  }
+  static uint32_t get_size_from_file(const std::string& filename) {
+    std::ifstream f(filename, std::ifstream::ate | std::ifstream::binary);
+    return f ? uint32_t(f.tellg() / std::streamoff(13 * sizeof(TF))) : 0u;
+  }
   const std::vector<Variable*>& get_distance_grids() const { return distance_grids_; }
   const std::vector<Variable*>& get_volume_grids() const { return volume_grids_; }
 

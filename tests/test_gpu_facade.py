@@ -281,3 +281,57 @@ def test_solver_pellet_matches_the_c_abi(engine):
     np.testing.assert_array_equal(solver.particle_x.get()[:n], X.cpu().numpy())
     np.testing.assert_array_equal(solver.particle_v.get()[:n], DX.cpu().numpy())
     np.testing.assert_array_equal(solver.particle_density.get()[:n], RHO.cpu().numpy())
+
+
+def test_variable_and_pile_files_match_the_reference_layouts(engine, tmp_path):
+    """Variable.write_file / read_file and Pile.write_file / read_file /
+    get_size_from_file produce the reference's byte layouts (the ones
+    alluvion_b200.alu restates) and read them back; float files load into
+    double variables."""
+    from alluvion_b200 import alu
+    dp = Depot(np.float32)
+    rng = np.random.Generator(np.random.PCG64(8))
+    a = rng.normal(size=(10, 3)).astype(np.float32)
+    v = dp.create(10, 3)
+    v.set(a)
+    p_all, p_part = tmp_path / "all.alu", tmp_path / "part.alu"
+    v.write_file(str(p_all))
+    v.write_file(str(p_part), 4, 2)  # elements 2..5
+    ref_all, ref_part = tmp_path / "ref_all.alu", tmp_path / "ref_part.alu"
+    alu.write_alu(ref_all, a, 3)
+    alu.write_alu(ref_part, a[2:6], 3)
+    assert p_all.read_bytes() == ref_all.read_bytes()
+    assert p_part.read_bytes() == ref_part.read_bytes()
+    w = dp.create(10, 3)
+    assert w.read_file(str(p_part)) == 4
+    np.testing.assert_array_equal(w.get()[:4], a[2:6])
+    d = dp.create(10, 3, np.float64)
+    assert d.read_file(str(p_all)) == 10
+    np.testing.assert_array_equal(d.get(), a.astype(np.float64))
+    with pytest.raises(RuntimeError):
+        dp.create(10, 1).read_file(str(p_all))  # primitives per element differ
+    with pytest.raises(RuntimeError):
+        v.write_file(str(p_all), 11)
+    # pile state files
+    runner = dp.Runner()
+    dp.cn.set_kernel_radius(0.04)
+    dp.cn.set_particle_attr(0.01, 0.008, 1000.0)
+    pile = dp.Pile(dp, runner, 0)
+    for k in range(3):
+        pile.add(dp.SphereDistance.create(0.05), [4, 4, 4], mass=1.0,
+                 x=[0.1 * k, 0.2, 0.3], q=[0.0, 0.0, 0.0, 1.0])
+    vv = pile.v
+    vv[1] = [1.0, 2.0, 3.0]
+    pile.v = vv
+    pf = tmp_path / "pile.bin"
+    pile.write_file(str(pf), 2.0, 1.0, 1.0)
+    rig = scenes.rigid_array(np.float32, [
+        scenes.rigid_state(np.float32, x=(0.1 * k, 0.2, 0.3), v=(1.0, 2.0, 3.0) if k == 1
+                           else (0, 0, 0)) for k in range(3)]).reshape(-1, 13)
+    rf = tmp_path / "ref_pile.bin"
+    alu.write_pile(rf, rig, x_scale=2.0)
+    assert pf.read_bytes() == rf.read_bytes()
+    assert dp.Pile.get_size_from_file(str(pf)) == 3
+    pile.read_file(str(rf), 1, 2, 1)  # body 1 of the file into body 2
+    assert pile.v[2] == [1.0, 2.0, 3.0]
+    assert pile.x[2] == pytest.approx([0.2, 0.4, 0.6])
