@@ -330,6 +330,14 @@ _SIGNATURES = {
     "al_histogram256_f32": (ctypes.c_int, [_P, _P, _P, _U, ctypes.c_float, ctypes.c_float, _P,
                                            _P]),
     "al_kl_divergence": (ctypes.c_int, [_P, _P, _P, _U, _U, ctypes.c_double, _U, _P, _P]),
+    "al_calculate_se_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _U, _P]),
+    "al_calculate_se_f64": (ctypes.c_int, [_P, _P, _P, _P, _U, _U, _P]),
+    "al_calculate_se_weighted_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _U, _P, _P]),
+    "al_calculate_se_weighted_f64": (ctypes.c_int, [_P, _P, _P, _P, _U, _U, _P, _P]),
+    "al_calculate_se_yz_masked_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P]),
+    "al_calculate_se_yz_masked_f64": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P]),
+    "al_sum_products_f32": (ctypes.c_int, [_P, _P, _P, _U, _U, _P, _P]),
+    "al_sum_products_f64": (ctypes.c_int, [_P, _P, _P, _U, _U, _P, _P]),
 }
 for _s in ("f32", "f64"):
     _SIGNATURES["al_grid_sort_" + _s] = (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _P, _P, _P, _P])

@@ -113,7 +113,26 @@ void declare_real(py::module& m, py::module& dg_m, const char* sfx) {
             for (int k = 0; k < 3; ++k) c.gravity[k] = v[k];
           });
 
-  py::class_<Runner<TF>>(m, ("Runner" + s).c_str()).def(py::init<>());
+  using R = Runner<TF>;
+  py::class_<R>(m, ("Runner" + s).c_str())
+      .def(py::init<>())
+      .def_static("calculate_se", &R::calculate_se, py::arg("v0"), py::arg("v1"),
+                  py::arg("se"), py::arg("n"), py::arg("offset") = 0)
+      .def_static("calculate_se_weighted", &R::calculate_se_weighted, py::arg("v0"),
+                  py::arg("v1"), py::arg("weight0"), py::arg("n"), py::arg("offset") = 0)
+      .def_static("calculate_se_yz_masked", &R::calculate_se_yz_masked, py::arg("v0"),
+                  py::arg("v1"), py::arg("mask"), py::arg("n"), py::arg("offset") = 0)
+      .def_static(
+          "sum_products",
+          [](const Variable& v0, const Variable& v1, uint32_t n, uint32_t offset) -> py::object {
+            auto r = R::sum_products(v0, v1, n, offset);
+            if (r.size() == 1) return py::float_(r[0]);
+            return py::cast(r);
+          },
+          py::arg("v0"), py::arg("v1"), py::arg("n"), py::arg("offset") = 0)
+      .def_static("calculate_kl_divergence", &R::calculate_kl_divergence,
+                  py::arg("histogram_p"), py::arg("histogram_q"), py::arg("n_p"), py::arg("n_q"),
+                  py::arg("q_lower_bound") = TF(1e-6), py::arg("num_bins") = 256);
 
   py::class_<dg::Distance<TF>, std::shared_ptr<dg::Distance<TF>>>(dg_m, ("Distance" + s).c_str())
       .def_readonly("aabb_min", &dg::Distance<TF>::aabb_min)

@@ -900,6 +900,39 @@ AL_API int al_kl_divergence(al_engine* engine, const uint32_t* histogram_p,
                             double q_lower_bound, uint32_t num_bins, double* result,
                             void* stream);
 
+/* ------------------------------------------------------------- metrics
+ * The Runner reductions that score sampled fields against targets
+ * (runner.hpp:715-744, 4710-4800).  v0, v1: device [n][dims] (dims 1..4,
+ * the reference's scalar or vector element); per-element terms in the
+ * arrays' real type (correctly rounded, no contraction), sums in double in
+ * a fixed order (the reference sums in the real type with
+ * thrust::transform_reduce).  result: host.
+ *   al_calculate_se_*           se[i] = |v0[i] - v1[i]|^2 (device [n] out)
+ *   al_calculate_se_weighted_*  *result = sum_i weight[i] |v0[i] - v1[i]|^2
+ *   al_calculate_se_yz_masked_* *result = sum over mask[i] == 1 of
+ *                               (v0 - v1).y^2 + (v0 - v1).z^2  (dims 3)
+ *   al_sum_products_*           result[k] = sum_i v0[i][k] v1[i][k], k < dims */
+AL_API int al_calculate_se_f32(al_engine* engine, const float* v0, const float* v1, float* se,
+                               uint32_t n, uint32_t dims, void* stream);
+AL_API int al_calculate_se_f64(al_engine* engine, const double* v0, const double* v1,
+                               double* se, uint32_t n, uint32_t dims, void* stream);
+AL_API int al_calculate_se_weighted_f32(al_engine* engine, const float* v0, const float* v1,
+                                        const float* weight, uint32_t n, uint32_t dims,
+                                        double* result, void* stream);
+AL_API int al_calculate_se_weighted_f64(al_engine* engine, const double* v0, const double* v1,
+                                        const double* weight, uint32_t n, uint32_t dims,
+                                        double* result, void* stream);
+AL_API int al_calculate_se_yz_masked_f32(al_engine* engine, const float* v0, const float* v1,
+                                         const float* mask, uint32_t n, double* result,
+                                         void* stream);
+AL_API int al_calculate_se_yz_masked_f64(al_engine* engine, const double* v0, const double* v1,
+                                         const double* mask, uint32_t n, double* result,
+                                         void* stream);
+AL_API int al_sum_products_f32(al_engine* engine, const float* v0, const float* v1, uint32_t n,
+                               uint32_t dims, double* result, void* stream);
+AL_API int al_sum_products_f64(al_engine* engine, const double* v0, const double* v1, uint32_t n,
+                               uint32_t dims, double* result, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

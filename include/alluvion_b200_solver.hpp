@@ -70,6 +70,7 @@ class Variable {
            NumericType type)
       : engine_(e), ptr_(p), shape_(std::move(shape)), n_(num_primitives), type_(type) {}
   void* ptr() const { return ptr_; }
+  al_engine* engine_handle() const { return engine_; }
   template <class T>
   T* data() const { return static_cast<T*>(ptr_); }
   const std::vector<uint32_t>& get_shape() const { return shape_; }
@@ -456,10 +457,113 @@ struct Mesh {
   std::vector<std::array<uint32_t, 3>> faces;
 };
 
-// Runner<TF>: the reference's launcher (launch statistics, reductions).
-// Every launch is the engine's here, so it carries no state.
+// Runner<TF>: the reference's launcher.  Every launch is the engine's here,
+// so it carries no state; its static reductions over variables
+// (runner.hpp:4710-4815) run on the device through the metric entries,
+// summing in double, and return the real type as the reference does.
 template <class TF>
-class Runner {};
+class Runner {
+ public:
+  // calculate_se: se[offset + i] = |v0 - v1|^2 of element offset + i.
+  static void calculate_se(const Variable& v0, const Variable& v1, Variable& se, uint32_t n,
+                           uint32_t offset = 0) {
+    const uint32_t d = dims_of(v0, v1, n, offset, "Runner::calculate_se");
+    if (se.get_type() != numeric_type_of<TF>() || se.get_num_primitives_per_element() != 1 ||
+        size_t(offset) + n > se.get_linear_shape())
+      throw error(AL_ERR_INVALID, "Runner::calculate_se: se must be a scalar variable of n");
+    check(real_se(v0.engine_handle(), at(v0, offset), at(v1, offset), at(se, offset), n, d),
+          "Runner::calculate_se");
+  }
+  static TF calculate_se_weighted(const Variable& v0, const Variable& v1, const Variable& weight,
+                                  uint32_t n, uint32_t offset = 0) {
+    const uint32_t d = dims_of(v0, v1, n, offset, "Runner::calculate_se_weighted");
+    scalar_of(weight, n, offset, "Runner::calculate_se_weighted");
+    double r = 0;
+    check(real_se_weighted(v0.engine_handle(), at(v0, offset), at(v1, offset),
+                           at(weight, offset), n, d, &r),
+          "Runner::calculate_se_weighted");
+    return TF(r);
+  }
+  static TF calculate_se_yz_masked(const Variable& v0, const Variable& v1, const Variable& mask,
+                                   uint32_t n, uint32_t offset = 0) {
+    if (dims_of(v0, v1, n, offset, "Runner::calculate_se_yz_masked") != 3)
+      throw error(AL_ERR_INVALID, "Runner::calculate_se_yz_masked: 3-vectors");
+    scalar_of(mask, n, offset, "Runner::calculate_se_yz_masked");
+    double r = 0;
+    check(real_se_yz(v0.engine_handle(), at(v0, offset), at(v1, offset), at(mask, offset), n,
+                     &r),
+          "Runner::calculate_se_yz_masked");
+    return TF(r);
+  }
+  // sum_products: the component-wise sum of v0 v1 (one value per primitive).
+  static std::vector<TF> sum_products(const Variable& v0, const Variable& v1, uint32_t n,
+                                      uint32_t offset = 0) {
+    const uint32_t d = dims_of(v0, v1, n, offset, "Runner::sum_products");
+    double r[4] = {0, 0, 0, 0};
+    check(real_sum_products(v0.engine_handle(), at(v0, offset), at(v1, offset), n, d, r),
+          "Runner::sum_products");
+    return std::vector<TF>(r, r + d);
+  }
+  // calculate_kl_divergence (runner.hpp:4803-4815) of two uint32 histograms.
+  static TF calculate_kl_divergence(const Variable& p, const Variable& q, uint32_t n_p,
+                                    uint32_t n_q, TF q_lower_bound = TF(1e-6),
+                                    uint32_t num_bins = 256) {
+    if (p.get_type() != NumericType::u32 || q.get_type() != NumericType::u32 ||
+        p.get_linear_shape() < num_bins || q.get_linear_shape() < num_bins)
+      throw error(AL_ERR_INVALID, "Runner::calculate_kl_divergence: uint32 histograms");
+    double r = 0;
+    check(al_kl_divergence(p.engine_handle(), p.template data<uint32_t>(),
+                           q.template data<uint32_t>(), n_p, n_q, double(q_lower_bound),
+                           num_bins, &r, nullptr),
+          "Runner::calculate_kl_divergence");
+    return TF(r);
+  }
+
+ private:
+  static const TF* at(const Variable& v, uint32_t offset) {
+    return v.template data<TF>() + size_t(offset) * v.get_num_primitives_per_element();
+  }
+  static TF* at(Variable& v, uint32_t offset) {
+    return v.template data<TF>() + size_t(offset) * v.get_num_primitives_per_element();
+  }
+  static uint32_t dims_of(const Variable& a, const Variable& b, uint32_t n, uint32_t offset,
+                          const char* where) {
+    const uint32_t d = a.get_num_primitives_per_element();
+    if (a.get_type() != numeric_type_of<TF>() || b.get_type() != numeric_type_of<TF>() ||
+        b.get_num_primitives_per_element() != d || d < 1 || d > 4 ||
+        size_t(offset) + n > a.get_linear_shape() || size_t(offset) + n > b.get_linear_shape())
+      throw error(AL_ERR_INVALID, std::string(where) + ": mismatched variables");
+    return d;
+  }
+  static void scalar_of(const Variable& v, uint32_t n, uint32_t offset, const char* where) {
+    if (v.get_type() != numeric_type_of<TF>() || v.get_num_primitives_per_element() != 1 ||
+        size_t(offset) + n > v.get_linear_shape())
+      throw error(AL_ERR_INVALID, std::string(where) + ": a scalar variable of n");
+  }
+  static int real_se(al_engine* e, const TF* a, const TF* b, TF* se, uint32_t n, uint32_t d) {
+    if constexpr (std::is_same_v<TF, float>) return al_calculate_se_f32(e, a, b, se, n, d, nullptr);
+    else return al_calculate_se_f64(e, a, b, se, n, d, nullptr);
+  }
+  static int real_se_weighted(al_engine* e, const TF* a, const TF* b, const TF* w, uint32_t n,
+                              uint32_t d, double* r) {
+    if constexpr (std::is_same_v<TF, float>)
+      return al_calculate_se_weighted_f32(e, a, b, w, n, d, r, nullptr);
+    else
+      return al_calculate_se_weighted_f64(e, a, b, w, n, d, r, nullptr);
+  }
+  static int real_se_yz(al_engine* e, const TF* a, const TF* b, const TF* m, uint32_t n,
+                        double* r) {
+    if constexpr (std::is_same_v<TF, float>)
+      return al_calculate_se_yz_masked_f32(e, a, b, m, n, r, nullptr);
+    else
+      return al_calculate_se_yz_masked_f64(e, a, b, m, n, r, nullptr);
+  }
+  static int real_sum_products(al_engine* e, const TF* a, const TF* b, uint32_t n, uint32_t d,
+                               double* r) {
+    if constexpr (std::is_same_v<TF, float>) return al_sum_products_f32(e, a, b, n, d, r, nullptr);
+    else return al_sum_products_f64(e, a, b, n, d, r, nullptr);
+  }
+};
 
 enum class VolumeMethod { volume_map = 0, pellets = 1 };
 
