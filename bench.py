@@ -379,12 +379,22 @@ def timed_steps(scene, sp, dt, steps, torch, on_step=None, method="df", flush=No
 
 
 def max_over_ranks(value, world, torch):
+    """The largest of the ranks' values (device times: the job ends with its
+    slowest rank).  The tensor lives where the process group's backend
+    reduces: on the GPU for nccl, on the host for gloo."""
     if world == 1:
         return value
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(units_per_rank, world, steps, ms_max):
+    """Whole-job units per second: every rank advances its own replica of
+    units_per_rank for `steps` steps; the job takes the slowest rank's time."""
+    return units_per_rank * world * steps / (ms_max / 1e3)
 
 
 def barrier(world):
@@ -512,7 +522,7 @@ def batch_arm(args):
     clk = clocks.stop()
     barrier(world)
     ms = max_over_ranks(ms, world, torch)
-    value = total_n * world * args.steps / (ms / 1e3)
+    value = job_throughput(total_n, world, args.steps, ms)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     dev_in = [t for sc in sl for t in (sc.x, sc.v, sc.kappa, sc.kappa_v)]
     host_in = [pin(t.cpu().numpy()) for t in dev_in]
@@ -531,7 +541,7 @@ def batch_arm(args):
     barrier(world)
     ms_e2e, _ = run(args.steps, io)
     ms_e2e = max_over_ranks(ms_e2e, world, torch)
-    e2e = total_n * world * args.steps / (ms_e2e / 1e3)
+    e2e = job_throughput(total_n, world, args.steps, ms_e2e)
     peak, peak_kind = measured_peaks()
     result = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
@@ -654,7 +664,7 @@ def engine_arm(args):
     barrier(world)
     ms = max_over_ranks(ms, world, torch)
     total_particles = scene.n * world
-    value = total_particles * args.steps / (ms / 1e3)
+    value = job_throughput(scene.n, world, args.steps, ms)
     # ---- end to end: host buffers in pinned memory, H2D + step + D2H per step
     n = scene.n
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
@@ -677,7 +687,7 @@ def engine_arm(args):
                                 method=args.method, flush=flush, warm=warm)
     barrier(world)
     ms_e2e = max_over_ranks(ms_e2e, world, torch)
-    e2e = total_particles * args.steps / (ms_e2e / 1e3)
+    e2e = job_throughput(scene.n, world, args.steps, ms_e2e)
     # ---- per-pass device times (profiling pass after the timed region)
     engine.reset_stats()
     engine.set_profiling(True)
