@@ -14,7 +14,7 @@
 namespace alb {
 
 constexpr uint32_t kNoCell = 0xffffffffu;
-constexpr int kBlock = 256;  // threads per block of the particle passes
+constexpr int kBlock = 128;  // threads per block of the particle passes (64..512 measured: 128 best)
 
 // ------------------------------------------------------------- vectors
 template <class TF>
