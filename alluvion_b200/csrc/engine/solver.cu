@@ -87,43 +87,57 @@ __device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b,
   __syncthreads();
 }
 
-// Pair passes run kTPP threads per particle: lane `sub` of a particle's
-// group walks neighbors sub, sub + kTPP, ...; the group combines its partial
-// sums with warp shuffles (fixed order, deterministic) and lane 0 applies
-// the boundary terms and writes the results.  With batched gathers
-// (for_each_neighbor) and 128-thread blocks one thread per particle keeps
-// enough gathers in flight: measured on the 1 M-particle dam break, 1.93 ms
-// per step at 1 thread, 1.98 at 2, 2.33 at 4.
-constexpr int kTPP = 1;
+// Pair passes run `tpp` threads per particle (1, 2, 4 or 8, chosen per
+// step from the particle count): lane `sub` of a particle's group walks
+// neighbors sub, sub + tpp, ...; the group combines its partial sums with
+// warp shuffles (fixed order, deterministic) and lane 0 applies the boundary
+// terms and writes the results.  With batched gathers (for_each_neighbor)
+// and 128-thread blocks one thread per particle keeps enough gathers in
+// flight once the particles alone fill the GPU (measured on the 1 M-particle
+// dam break: 1.93 ms per step at 1 thread, 1.98 at 2, 2.33 at 4); smaller
+// scenes split each particle's neighbors over more lanes until about
+// kPairThreads threads run (the 32,768-particle dam break: 0.29 / 0.255 /
+// 0.268 ms per step at 8 / 4 / 2 threads per particle).
+constexpr uint64_t kPairThreads = uint64_t(1) << 17;
+
+inline uint32_t pair_tpp(uint32_t n) {
+  uint32_t tpp = 1;
+  while (tpp < 8 && uint64_t(n) * tpp < kPairThreads) tpp <<= 1;
+  return tpp;
+}
 
 struct Lane {
-  uint32_t s, sub;
+  uint32_t s, sub, tpp;
   bool act;
   __device__ __forceinline__ bool lead() const { return act && sub == 0; }
 };
 
-__device__ __forceinline__ Lane pair_lane(uint32_t n) {
+template <class TF>
+__device__ __forceinline__ Lane pair_lane(const StepState<TF>& S) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t shift = __ffs(S.tpp) - 1;
   Lane l;
-  l.s = g / kTPP;
-  l.sub = g % kTPP;
-  l.act = l.s < n;
+  l.tpp = S.tpp;
+  l.s = g >> shift;
+  l.sub = g & (S.tpp - 1);
+  l.act = l.s < S.n;
   return l;
 }
 
-inline uint32_t pair_blocks(uint32_t n) {
-  return uint32_t((uint64_t(n) * kTPP + kBlock - 1) / kBlock);
+inline uint32_t pair_blocks(uint32_t n, uint32_t tpp) {
+  return uint32_t((uint64_t(n) * tpp + kBlock - 1) / kBlock);
 }
 
+// Sum over the particle's lane group (every lane of the warp calls it; the
+// group's lanes are consecutive and tpp divides 32).
 template <class T>
-__device__ __forceinline__ T group_sum(T v) {
-#pragma unroll
-  for (int o = kTPP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+__device__ __forceinline__ T group_sum(T v, const Lane& L) {
+  for (uint32_t o = L.tpp >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 template <class TF>
-__device__ __forceinline__ vec3<TF> group_sum(vec3<TF> v) {
-  return vec3<TF>{group_sum(v.x), group_sum(v.y), group_sum(v.z)};
+__device__ __forceinline__ vec3<TF> group_sum(vec3<TF> v, const Lane& L) {
+  return vec3<TF>{group_sum(v.x, L), group_sum(v.y, L), group_sum(v.z, L)};
 }
 
 template <class TF>
@@ -131,7 +145,7 @@ __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, u
   return __ldcs(S.nbr + size_t(k) * S.n + s);
 }
 
-// Visits the lane's neighbors k = sub, sub + kTPP, ... < cnt in batches of
+// Visits the lane's neighbors k = sub, sub + tpp, ... < cnt in batches of
 // B: the batch's list entries are loaded first, then all their records,
 // then `f(t, x_j, v_j)` runs for each in list order (the order of a plain
 // loop, so sums are bit-identical to one).  Batching keeps B dependent
@@ -143,11 +157,11 @@ __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, u
 template <int B, bool V, class TF, class F>
 __device__ __forceinline__ void for_each_neighbor(const StepState<TF>& S, const Lane& L,
                                                   uint32_t cnt, F&& f) {
-  for (uint32_t k0 = L.sub; k0 < cnt; k0 += B * kTPP) {
+  for (uint32_t k0 = L.sub; k0 < cnt; k0 += B * L.tpp) {
     uint32_t t[B];
 #pragma unroll
     for (int b = 0; b < B; ++b) {
-      const uint32_t k = k0 + b * kTPP;
+      const uint32_t k = k0 + b * L.tpp;
       t[b] = k < cnt ? nbr_at(S, k, L.s) : L.s;  // own slot: a valid address
     }
     vec4<TF> xj[B], vj[B];
@@ -162,7 +176,7 @@ __device__ __forceinline__ void for_each_neighbor(const StepState<TF>& S, const 
     }
 #pragma unroll
     for (int b = 0; b < B; ++b)
-      if (k0 + b * kTPP < cnt) f(t[b], xj[b], vj[b]);
+      if (k0 + b * L.tpp < cnt) f(t[b], xj[b], vj[b]);
   }
 }
 
@@ -179,7 +193,7 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
     const vec3<TF> d = pdisp(c, xi, xyz(xj));
     acc += c.vol * dot(vi - xyz(vj), gradW(c, d));
   });
-  acc = group_sum(acc);
+  acc = group_sum(acc, L);
   if (L.act) {
     for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
@@ -308,7 +322,7 @@ template <class TF, int MODE, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   TF ki = 0;
   vec3<TF> dv{0, 0, 0};
@@ -332,7 +346,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
       }
     }
   });
-  dv = group_sum(dv);
+  dv = group_sum(dv, L);
   const uint32_t m = (L.lead() && fabs(ki) > c.eps) ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
@@ -361,7 +375,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
 template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF adv = density_change(c, S, L);
   if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
@@ -377,7 +391,7 @@ template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_df_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF adv = density_change(c, S, L);
   double val = 0;
   if (L.lead()) {
@@ -398,7 +412,7 @@ template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_viscosity(Cn<TF> c, StepState<TF> S, int finish_div) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, da{0, 0, 0};
   uint32_t cnt = 0;
@@ -413,7 +427,7 @@ __global__ void __launch_bounds__(kBlock)
            (length_sqr(d) + TF(0.01) * c.h2)) *
           (vi - xyz(vj));
   });
-  da = group_sum(da);
+  da = group_sum(da, L);
   const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
@@ -520,7 +534,7 @@ template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_p_warm0(Cn<TF> c, StepState<TF> S, const float* __restrict__ pred) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
@@ -536,7 +550,7 @@ __global__ void __launch_bounds__(kBlock)
 template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
@@ -552,7 +566,7 @@ template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_p_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF adv = density_adv(c, S, L, S.ctrl->dt);
   double val = 0;
   if (L.lead()) {
@@ -600,7 +614,7 @@ __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __
 template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   vec3<TF> xi{0, 0, 0};
   TF rho2 = 1;
   uint32_t cnt = 0;
@@ -614,7 +628,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
   for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
     dii -= (c.vol / rho2) * gradW(c, pdisp(c, xi, xyz(xj)));
   });
-  dii = group_sum(dii);
+  dii = group_sum(dii, L);
   if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
   const vec4<TF> a = S.a[L.s];
@@ -636,7 +650,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
 template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, dii{0, 0, 0};
   TF rho = c.rho0;
@@ -656,8 +670,8 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
     adv += dt * c.vol * dot(vi - xyz(vj), gw);
     aii += c.vol * dot(dii - dji, gw);
   });
-  adv = group_sum(adv);
-  aii = group_sum(aii);
+  adv = group_sum(adv, L);
+  aii = group_sum(aii, L);
   if (!L.lead()) return;
   adv += rho / c.rho0;
   for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
@@ -680,7 +694,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
 template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const bool first = S.ctrl->it == 0;
   vec3<TF> xi{0, 0, 0};
   uint32_t cnt = 0;
@@ -695,7 +709,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
     const TF rj = vj.w, rj2 = rj * rj;
     acc -= (c.vol / rj2 * xj.w) * gradW(c, pdisp(c, xi, xyz(xj)));
   });
-  acc = group_sum(acc);
+  acc = group_sum(acc, L);
   if (!L.lead()) return;
   if (!first) S.kappa_v[L.s] = S.kappa[L.s];
   acc = acc * c.rho0;
@@ -708,7 +722,7 @@ template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_ii_iter1(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, dij_pj{0, 0, 0};
   TF lp = 0, rho = c.rho0;
@@ -729,7 +743,7 @@ __global__ void __launch_bounds__(kBlock)
     sum += c.vol *
            dot(dij_pj - ldx(S.dii, t) * __ldg(S.kappa_v + t) - (ldx(S.dij_pj, t) - dji_pi), gw);
   });
-  sum = group_sum(sum);
+  sum = group_sum(sum, L);
   double val = 0;
   if (L.lead()) {
     for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
@@ -763,7 +777,7 @@ __global__ void __launch_bounds__(kBlock)
                       TF* __restrict__ a_ref, TF* __restrict__ rho_ref, TF* __restrict__ p_ref,
                       TF* __restrict__ rho_adv_ref) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   vec3<TF> ai{0, 0, 0}, xi{0, 0, 0};
   TF dpi = 0;
   uint32_t cnt = 0;
@@ -778,7 +792,7 @@ __global__ void __launch_bounds__(kBlock)
     const TF dpj = __ldg(S.kappa + t) / (rj * rj);
     ai -= (c.mass * (dpi + dpj)) * gradW(c, pdisp(c, xi, xyz(xj)));
   });
-  ai = group_sum(ai);
+  ai = group_sum(ai, L);
   const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
@@ -827,7 +841,7 @@ __global__ void __launch_bounds__(kBlock) k_i_advect(StepState<TF> S) {
 template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0};
   TF rho = c.rho0;
@@ -847,8 +861,8 @@ __global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
     adv += dt * c.vol * dot(vi - xyz(vj), gw);
     diag += c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gw);
   });
-  adv = group_sum(adv);
-  diag = group_sum(diag);
+  adv = group_sum(adv, L);
+  diag = group_sum(diag, L);
   if (!L.lead()) return;
   adv += rho / c.rho0;
   for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
@@ -873,7 +887,7 @@ template <class TF, bool WR = false>
 __global__ void __launch_bounds__(kBlock)
     k_i_iter(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S.n);
+  const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   const bool odd = (S.ctrl->it & 1u) != 0;
   const TF* __restrict__ last = odd ? S.kappa : S.kappa_v;
@@ -895,7 +909,7 @@ __global__ void __launch_bounds__(kBlock)
     off -= c.vol * (rho + rj) / (rho * rj) / (length_sqr(d) + eps) * dot(d, gradW(c, d)) *
            __ldg(last + t);
   });
-  off = group_sum(off);
+  off = group_sum(off, L);
   double val = 0;
   if (L.lead()) {
     off *= c.rho0;
@@ -1082,7 +1096,7 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
              ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
   S.perm = gs.perm;
   const uint32_t blocks = blocks_for(n, kBlock);
-  const uint32_t pblocks = pair_blocks(n);
+  const uint32_t pblocks = pair_blocks(n, S.tpp);
   if (n > 0) {
     const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
     if (iisph)
@@ -1348,7 +1362,8 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   S.n = n;
   S.nb = nb;
   S.cap = P.g.cap_nbr;
-  S.grid = pair_blocks(n) > 0 ? pair_blocks(n) : 1;  // grid of the pair passes
+  S.tpp = pair_tpp(n);
+  S.grid = pair_blocks(n, S.tpp) > 0 ? pair_blocks(n, S.tpp) : 1;  // grid of the pair passes
   // ---- buffers
   ALB_TRY(e->buf("flags", 4, &P.flags));
   ALB_TRY(e->buf("sorted.x", n, &S.x));

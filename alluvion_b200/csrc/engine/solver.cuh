@@ -48,6 +48,7 @@ struct Ctrl {
 template <class TF>
 struct StepState {
   uint32_t n = 0, nb = 0, cap = 0, grid = 0;
+  uint32_t tpp = 1;  // threads per particle of the pair passes (pair_tpp)
   vec4<TF>* x = nullptr;    // sorted positions (grid sort, boundaries, build)
   // Interleaved particle records of the pair passes: rec[2s] = {x, payload},
   // rec[2s + 1] = {v, rho}.  One 32-byte sector (float) holds all a
