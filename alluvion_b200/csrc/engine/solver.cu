@@ -1335,6 +1335,9 @@ struct StepArgs {
   TF* dt = nullptr;
   al_step_report* report = nullptr;
   const al_warm_start* warm = nullptr;
+  // particles that share the GPU with this scene's passes (a batch's total;
+  // 0: the scene's own); it sets the pair passes' threads per particle
+  uint64_t pair_total = 0;
 };
 
 // Validates the arguments, sizes the scene's scratch (under the engine's
@@ -1362,7 +1365,7 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   S.n = n;
   S.nb = nb;
   S.cap = P.g.cap_nbr;
-  S.tpp = pair_tpp(n);
+  S.tpp = pair_tpp(A.pair_total ? uint32_t(std::min<uint64_t>(A.pair_total, 0xffffffffu)) : n);
   S.grid = pair_blocks(n, S.tpp) > 0 ? pair_blocks(n, S.tpp) : 1;  // grid of the pair passes
   // ---- buffers
   ALB_TRY(e->buf("flags", 4, &P.flags));
@@ -1743,6 +1746,10 @@ int al_df_batch_step_f32(al_engine* engine, al_scene_f32* scenes, uint32_t num_s
     args[k].dt = sc.dt;
     args[k].report = sc.report;
   }
+  // the scenes' passes run side by side: threads per particle from the total
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < num_scenes; ++k) total += args[k].f ? args[k].f->num_particles : 0u;
+  for (uint32_t k = 0; k < num_scenes; ++k) args[k].pair_total = total;
   std::vector<int> status;
   const int rc = run_batch<float>(engine, args, status, static_cast<cudaStream_t>(stream));
   for (uint32_t k = 0; k < num_scenes; ++k)
