@@ -150,10 +150,11 @@ __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, u
 // then `f(t, x_j, v_j)` runs for each in list order (the order of a plain
 // loop, so sums are bit-identical to one).  Batching keeps B dependent
 // index -> record chains in flight per lane; it pays in the passes with
-// much arithmetic per neighbor (measured on the 1M-particle dam break:
-// B = 4 for k_kappa and viscosity, B = 2 for the velocity-divergence
-// passes, which have little arithmetic per neighbor).  `v_j` is loaded
-// only when V.
+// much arithmetic per neighbor (measured on the 1M-particle dam break at
+// one thread per particle: B = 8 for k_kappa (1.922 vs 1.928 ms per step at
+// 4, 1.946 at 2), 4 for viscosity, 2 for the velocity-divergence passes,
+// which have little arithmetic per neighbor).  `v_j` is loaded only when
+// V.
 template <int B, bool V, class TF, class F>
 __device__ __forceinline__ void for_each_neighbor(const StepState<TF>& S, const Lane& L,
                                                   uint32_t cnt, F&& f) {
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
     xi = xyz(r);
     cnt = S.ncount[L.s];
   }
-  for_each_neighbor<4, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
+  for_each_neighbor<8, false>(S, L, cnt, [&](uint32_t, const vec4<TF>& xj, const vec4<TF>&) {
     const TF ksum = ki + xj.w;
     if (fabs(ksum) > c.eps) {
       const vec3<TF> gw = gradW(c, pdisp(c, xi, xyz(xj)));
