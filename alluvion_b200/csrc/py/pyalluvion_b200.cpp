@@ -344,6 +344,9 @@ void declare_real(py::module& m, py::module& dg_m, const char* sfx) {
       .def("reset_solving_var", &S::reset_solving_var)
       .def("reset_t", &S::reset_t)
       .def("compute_all_boundaries", &S::compute_all_boundaries)
+      .def("sample_all_boundaries", &S::sample_all_boundaries, py::arg("sample_x"),
+           py::arg("sample_boundary"), py::arg("sample_boundary_kernel"),
+           py::arg("num_samples"))
       .def("update_particle_neighbors", &S::template update_particle_neighbors<0>)
       .def("update_particle_neighbors_wrap1", &S::template update_particle_neighbors<1>);
 

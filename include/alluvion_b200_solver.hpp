@@ -927,6 +927,25 @@ class Solver {
               particle_boundary_kernel->template data<TF>(), nullptr),
           "Solver::compute_all_boundaries");
   }
+  // Solver::sample_all_boundaries (solver.hpp:186-203): the bodies' volume
+  // and kernel terms at sample points, in the particle_boundary layout
+  // ([num_bodies][num_samples] x 4).
+  void sample_all_boundaries(const Variable& sample_x, Variable& sample_boundary,
+                             Variable& sample_boundary_kernel, uint32_t num_samples) {
+    const size_t need = size_t(pile.get_size()) * num_samples * 4;
+    if (sample_x.get_linear_shape() < num_samples ||
+        sample_boundary.get_num_primitives() < need ||
+        sample_boundary_kernel.get_num_primitives() < need)
+      throw error(AL_ERR_INVALID, "Solver::sample_all_boundaries: variables too small");
+    const auto bodies = pile.bodies();
+    const auto rig = pile.rigid();
+    check(real<TF>::compute_particle_boundary(
+              store.eng(), cn_->c(), pile.get_size(), bodies.data(), rig.data(),
+              sample_x.template data<TF>(), num_samples,
+              sample_boundary.template data<TF>(), sample_boundary_kernel.template data<TF>(),
+              nullptr),
+          "Solver::sample_all_boundaries");
+  }
   // Solver::update_particle_neighbors<wrap> (solver.hpp:225-260): grid,
   // neighbor list in the reference layout and the density with the
   // boundary terms of the last compute_all_boundaries.

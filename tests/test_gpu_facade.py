@@ -335,3 +335,29 @@ def test_variable_and_pile_files_match_the_reference_layouts(engine, tmp_path):
     pile.read_file(str(rf), 1, 2, 1)  # body 1 of the file into body 2
     assert pile.v[2] == [1.0, 2.0, 3.0]
     assert pile.x[2] == pytest.approx([0.2, 0.4, 0.6])
+
+
+def test_sample_all_boundaries_matches_the_c_abi(engine):
+    """Solver.sample_all_boundaries (solver.hpp:186-203) writes the same
+    boundary terms at sample points as al_compute_particle_boundary_f32
+    called with the sample positions."""
+    dtype = np.float32
+    abi, x, mass = _abi_scene(engine, dtype)
+    dp, pile, solver = _depot_scene(dtype, x, abi, mass)
+    rng = np.random.Generator(np.random.PCG64(4))
+    s = 3000
+    sx = rng.uniform(0.0, 0.3, size=(s, 3)).astype(np.float32)
+    vx = dp.create(s, 3)
+    vx.set(sx)
+    nb = pile.get_size()
+    vb, vk = dp.create([nb, s], 4), dp.create([nb, s], 4)
+    solver.sample_all_boundaries(vx, vb, vk, s)
+    sx_d = torch.from_numpy(sx).cuda()
+    sb = torch.zeros(nb, s, 4, device="cuda")
+    sbk = torch.zeros(nb, s, 4, device="cuda")
+    _capi.check(_capi.lib().al_compute_particle_boundary_f32(
+        engine.handle, _capi.ptr(abi.cn), nb, _capi.ptr(abi.bodies), _capi.ptr(abi.rigid),
+        sx_d.data_ptr(), s, sb.data_ptr(), sbk.data_ptr(), None), "boundary")
+    np.testing.assert_array_equal(vb.get(), sb.cpu().numpy())
+    np.testing.assert_array_equal(vk.get(), sbk.cpu().numpy())
+    assert np.abs(vk.get()[:, :, 3]).max() > 0
