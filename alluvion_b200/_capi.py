@@ -299,6 +299,9 @@ _SIGNATURES = {
     "al_copy": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t]),
     "al_set": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_size_t]),
     "al_engine_set_graph_mode": (ctypes.c_int, [_P, ctypes.c_int]),
+    "al_engine_set_launch_shape": (ctypes.c_int, [_P, ctypes.c_char_p, _U, _U, _U, _U]),
+    "al_engine_get_launch_shape": (ctypes.c_int, [_P, ctypes.c_char_p, _U, _U, _P, _P]),
+    "al_tunable_group": (ctypes.c_int, [_U, ctypes.POINTER(ctypes.c_char_p), _P]),
     "al_engine_graph_stats": (ctypes.c_int, [_P, _P, _P]),
     "al_engine_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_warm_net_forward_f32": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
@@ -438,6 +441,21 @@ class Engine:
         check(lib().al_engine_launch_count(self.handle, ctypes.byref(c)), "launch_count")
         return c.value
 
+    def set_launch_shape(self, group, bucket, batch, block, tpp):
+        """Launch shape of a tunable pass group for scenes of 2^bucket..2^(bucket+1)
+        particles in single (batch=0) or batched (batch=1) steps; 0 keeps a default."""
+        check(lib().al_engine_set_launch_shape(self.handle, group.encode(), int(bucket),
+                                               int(batch), int(block), int(tpp)),
+              "al_engine_set_launch_shape")
+
+    def launch_shape(self, group, num_particles, batch=0):
+        """(block, threads per particle) a step of num_particles would use."""
+        b, t = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().al_engine_get_launch_shape(self.handle, group.encode(), int(num_particles),
+                                               int(batch), ctypes.byref(b), ctypes.byref(t)),
+              "al_engine_get_launch_shape")
+        return b.value, t.value
+
     def kernel_stats(self):
         """{launch group name: (total_ms, count)} recorded while profiling."""
         out = {}
@@ -450,6 +468,17 @@ class Engine:
             out[buf.value.decode()] = (ms.value, cnt.value)
             i += 1
         return out
+
+
+def tunable_groups():
+    """[(name, is_pair_pass)] of the step's pass groups with a settable shape."""
+    out = []
+    name, pair = ctypes.c_char_p(), ctypes.c_uint32()
+    k = 0
+    while lib().al_tunable_group(k, ctypes.byref(name), ctypes.byref(pair)) == AL_OK:
+        out.append((name.value.decode(), bool(pair.value)))
+        k += 1
+    return out
 
 
 def ptr(t):

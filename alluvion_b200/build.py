@@ -57,14 +57,20 @@ def build_engine(force=False, verbose=False, ptxas_info=False):
     build_dir = os.path.join(PKG, "_build")
     os.makedirs(build_dir, exist_ok=True)
     objs = []
+    jobs = []
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     for src in engine_sources():
         obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < _newest(
                 [src] + engine_deps()[len(engine_sources()):]):
-            _run([NVCC, *NVCC_FLAGS, *extra, "-I", INCLUDE, "-I", ENGINE_DIR,
-                  "-c", src, "-o", obj], verbose)
+            jobs.append([NVCC, *NVCC_FLAGS, *extra, "-I", INCLUDE, "-I", ENGINE_DIR,
+                         "-c", src, "-o", obj])
         objs.append(obj)
+    # translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     tmp = ENGINE_LIB + ".tmp"
     _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs,
           "-o", tmp, "-lcuda"], verbose)

@@ -44,7 +44,7 @@ namespace {
 // the particle's and the neighbors' velocities and receives
 // sum_j V (v_i - v_j) . grad W_ij, in list order, at the end.
 template <class TF, class BK, bool FACTOR, class EX, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_build_neighbors(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
                       const vec4<TF>* __restrict__ xs, uint32_t n, BK bk,
                       uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount,

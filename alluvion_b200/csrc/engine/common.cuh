@@ -15,6 +15,9 @@ namespace alb {
 
 constexpr uint32_t kNoCell = 0xffffffffu;
 constexpr int kBlock = 128;  // threads per block of the particle passes (64..512 measured: 128 best)
+// Largest block of the passes whose shape the launch-shape table can set
+// (their __launch_bounds__ and block-sized shared arrays).
+constexpr int kMaxBlock = 256;
 
 // ------------------------------------------------------------- vectors
 template <class TF>

@@ -6,7 +6,9 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
+#include <tuple>
 #include <unordered_map>
 #include <utility>
 #include <vector>
@@ -126,11 +128,25 @@ struct al_engine {
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
 
+  // Launch shapes of the tunable pass groups (al_engine_set_launch_shape):
+  // (group, particle-count bucket floor(log2 n), context 0 single / 1 batch)
+  // -> (threads per block, threads per particle).  Entries override the
+  // defaults; setting one invalidates the captured graphs.
+  std::map<std::tuple<std::string, uint32_t, uint32_t>, std::pair<uint32_t, uint32_t>> shapes;
+
   // Returns a device buffer of at least `bytes` under `name`.
   int buffer(const char* name, size_t bytes, void** out);
   template <class T>
   int buf(const char* name, size_t count, T** out) {
     return buffer(name, count * sizeof(T), reinterpret_cast<void**>(out));
+  }
+  // As buf(); *fresh tells whether the buffer was (re)allocated by this call.
+  template <class T>
+  int buf(const char* name, size_t count, T** out, bool* fresh) {
+    const uint64_t g0 = generation;  // buffer() counts every allocation it makes
+    const int rc = buffer(name, count * sizeof(T), reinterpret_cast<void**>(out));
+    *fresh = rc == AL_OK && generation != g0;
+    return rc;
   }
   int host_pinned(size_t bytes, void** out);
   int activate() const;

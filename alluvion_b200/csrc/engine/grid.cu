@@ -136,40 +136,105 @@ __global__ void k_scatter(const uint32_t* __restrict__ cell, const uint32_t* __r
   perm[start[c] + rank[i]] = i;
 }
 
-// Sorts every bucket's members by original index (insertion sort; buckets
-// hold ~8 particles at rest density).  The tail bucket of out-of-grid
-// particles is left in arrival order.
+// Sorts every bucket's members by original index: one thread per cell,
+// insertion sort in a local array (buckets hold ~8 particles at rest
+// density and at most max_num_particles_per_cell = 64 without a
+// cell-overflow report).  Larger cells are left to k_order_crowded.  The
+// tail bucket of out-of-grid particles is left in arrival order.
+constexpr uint32_t kOrderLocal = 64;
+
 __global__ void k_order_cells(const uint32_t* __restrict__ start, uint32_t ncells,
                               uint32_t* __restrict__ perm) {
   uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
   const uint32_t b = start[c], e = start[c + 1];
-  if (e - b < 2) return;
-  constexpr uint32_t kLocal = 32;
-  if (e - b <= kLocal) {
-    uint32_t a[kLocal];
-    uint32_t m = e - b;
-    for (uint32_t k = 0; k < m; ++k) {
-      uint32_t v = perm[b + k];
-      uint32_t j = k;
-      while (j > 0 && a[j - 1] > v) {
-        a[j] = a[j - 1];
-        --j;
-      }
-      a[j] = v;
+  if (e - b < 2 || e - b > kOrderLocal) return;
+  uint32_t a[kOrderLocal];
+  const uint32_t m = e - b;
+  for (uint32_t k = 0; k < m; ++k) {
+    uint32_t v = perm[b + k];
+    uint32_t j = k;
+    while (j > 0 && a[j - 1] > v) {
+      a[j] = a[j - 1];
+      --j;
     }
-    for (uint32_t k = 0; k < m; ++k) perm[b + k] = a[k];
-  } else {
-    for (uint32_t k = b + 1; k < e; ++k) {
-      uint32_t v = perm[k];
-      uint32_t j = k;
-      while (j > b && perm[j - 1] > v) {
-        perm[j] = perm[j - 1];
-        --j;
+    a[j] = v;
+  }
+  for (uint32_t k = 0; k < m; ++k) perm[b + k] = a[k];
+}
+
+// Cells above kOrderLocal members (an overflow the sort reports, but whose
+// outputs are still written in canonical order): each block walks the cells
+// in chunks of its width, and sorts each crowded cell it finds with all its
+// threads, by a bitonic sort in shared memory for up to kCrowdedSmem
+// members (indices are distinct, so the order is total).  Beyond that one
+// thread sorts in place (a degenerate pile of thousands of particles in one
+// cell).
+constexpr uint32_t kCrowdedThreads = 256;
+constexpr uint32_t kCrowdedSmem = 4096;
+constexpr uint32_t kCrowdedBlocks = 256;
+
+__global__ void __launch_bounds__(kCrowdedThreads)
+    k_order_crowded(const uint32_t* __restrict__ start, uint32_t ncells,
+                    uint32_t* __restrict__ perm) {
+  __shared__ uint32_t v[kCrowdedSmem];
+  __shared__ uint32_t crowded[kCrowdedThreads];
+  __shared__ uint32_t ncrowded;
+  for (uint32_t base = blockIdx.x * kCrowdedThreads; base < ncells;
+       base += gridDim.x * kCrowdedThreads) {
+    if (threadIdx.x == 0) ncrowded = 0;
+    __syncthreads();
+    const uint32_t c = base + threadIdx.x;
+    if (c < ncells && start[c + 1] - start[c] > kOrderLocal)
+      crowded[atomicAdd(&ncrowded, 1u)] = c;
+    __syncthreads();
+    const uint32_t nc = ncrowded;
+    for (uint32_t q = 0; q < nc; ++q) {
+      const uint32_t cc = crowded[q];
+      const uint32_t b = start[cc], m = start[cc + 1] - b;
+      if (m <= kCrowdedSmem) {
+        uint32_t len = 1;
+        while (len < m) len <<= 1;
+        for (uint32_t k = threadIdx.x; k < len; k += kCrowdedThreads)
+          v[k] = k < m ? perm[b + k] : 0xffffffffu;
+        __syncthreads();
+        for (uint32_t size = 2; size <= len; size <<= 1) {
+          for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t k = threadIdx.x; k < len; k += kCrowdedThreads) {
+              const uint32_t partner = k ^ stride;
+              if (partner > k) {
+                const bool up = (k & size) == 0;
+                const uint32_t x = v[k], y = v[partner];
+                if ((x > y) == up) {
+                  v[k] = y;
+                  v[partner] = x;
+                }
+              }
+            }
+            __syncthreads();
+          }
+        }
+        for (uint32_t k = threadIdx.x; k < m; k += kCrowdedThreads) perm[b + k] = v[k];
+        __syncthreads();
+      } else if (threadIdx.x == 0) {
+        for (uint32_t k = b + 1; k < b + m; ++k) {
+          const uint32_t x = perm[k];
+          uint32_t j = k;
+          while (j > b && perm[j - 1] > x) {
+            perm[j] = perm[j - 1];
+            --j;
+          }
+          perm[j] = x;
+        }
       }
-      perm[j] = v;
+      __syncthreads();
     }
   }
+}
+
+inline uint32_t crowded_blocks(uint32_t ncells) {
+  const uint32_t chunks = (ncells + kCrowdedThreads - 1) / kCrowdedThreads;
+  return chunks < kCrowdedBlocks ? (chunks ? chunks : 1u) : kCrowdedBlocks;
 }
 
 template <class TF>
@@ -227,6 +292,8 @@ int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* parti
                                                       gs.perm);
   k_order_cells<<<blocks_for(g.ncells, kBlock), kBlock, 0, st>>>(gs.cell_start, g.ncells,
                                                                  gs.perm);
+  k_order_crowded<<<crowded_blocks(g.ncells), kCrowdedThreads, 0, st>>>(gs.cell_start, g.ncells,
+                                                                        gs.perm);
   k_gather_x<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(particle_x, gs.perm, n, xs, gs.inv);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
@@ -254,6 +321,7 @@ int grid_sort_into(const Cn<TF>& c, const GridDims& g, const TF* particle_x, uin
   k_scatter<<<blocks_for(n, kBlock), kBlock, 0, st>>>(cell, sc.rank, sc.start, n, g.ncells,
                                                       perm);
   k_order_cells<<<blocks_for(g.ncells, kBlock), kBlock, 0, st>>>(sc.start, g.ncells, perm);
+  k_order_crowded<<<crowded_blocks(g.ncells), kCrowdedThreads, 0, st>>>(sc.start, g.ncells, perm);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }

@@ -27,6 +27,10 @@ struct GridState {
   uint32_t* flags = nullptr;       // [4] grid_anomaly[0..2] + spare (device)
 };
 
+// Kernels one grid_build launches (hash, three scan passes, scatter, the two
+// per-cell orderings, gather).
+constexpr int kGridBuildKernels = 8;
+
 // Hashes, sorts and gathers positions into `xs` (sorted order, w = 0).
 // particle_x is the caller's [n][3] array.  `flags` must be zeroed by the
 // caller (it is also used by later passes).

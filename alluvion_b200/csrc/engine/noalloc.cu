@@ -1,22 +1,23 @@
 // noalloc.cu -- a grid sort that allocates nothing.
 //
-// Some callers cannot let a library call cudaMalloc: a host that captures
-// its whole frame into a CUDA graph (allocation is not allowed while a
-// stream is being captured), a renderer or game engine that owns the device
-// memory budget and forbids plugins from allocating behind its back, or a
-// real-time loop that cannot afford the implicit device synchronisation a
-// cudaMalloc / cudaFree pair can cause.  For them this file provides
-// al_grid_sort_noalloc_f32: the same cell hash and stable counting sort as
-// al_grid_sort_f32, with all of its scratch in one file-scope device array
-// that is sized at compile time.  The caller still passes the inputs and
-// the output buffers.
+// Some callers cannot let a library call cudaMalloc: a renderer or game
+// engine that owns the device memory budget and forbids plugins from
+// allocating behind its back, or a real-time loop that cannot afford the
+// implicit device synchronisation a cudaMalloc / cudaFree pair can cause.
+// For them this file provides al_grid_sort_noalloc_f32: the same cell hash
+// and stable counting sort as al_grid_sort_f32, with all of its scratch in
+// one file-scope device array that is sized at compile time.  The caller
+// still passes the inputs and the output buffers.
 //
-// The array is part of the library's device image: every GPU that loads the
-// library holds its 12.6 MiB until the process exits.  Every call shares
-// it, so two calls that overlap on the GPU (different streams, or different
-// host threads with no ordering between them) race and corrupt each other;
-// callers must order them.  The array keeps the previous call's contents;
-// the call clears what must start at zero (cell counts, anomaly flags).
+// The array is part of the library's device image.  Once the image is
+// loaded on a GPU (with CUDA's lazy module loading, at this entry point's
+// first call on that GPU) the GPU holds its 12.6 MiB until the process
+// exits.  Every call shares it, so two calls that overlap on the GPU
+// (different streams, or different host threads with no ordering between
+// them) race and corrupt each other; callers must order them.  The array
+// keeps the previous call's contents; the call clears what must start at
+// zero (cell counts, anomaly flags).  Each call ends by reading the anomaly
+// flags back to the host, which synchronises the caller's stream.
 #include <mutex>
 #include <string>
 

@@ -312,7 +312,7 @@ int relax(al_engine* e, const typename RelaxTypes<TF>::cn* cn, const al_consti* 
   for (uint32_t it = 0; it < steps; ++it) {
     const bool last = it + 1 == steps;
     GridState gs;
-    ALB_LAUNCH(e, "relax_grid", 7, st,
+    ALB_LAUNCH(e, "relax_grid", kGridBuildKernels, st,
                ALB_TRY(grid_build<TF>(e, c, g, x, n, xs, flags, gs, st)));
     S.perm = gs.perm;
     ALB_LAUNCH(e, "relax_lists", 1, st,

@@ -688,7 +688,7 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
                (k_pel_place<TF><<<tb, kBlock, 0, st>>>(S, f->particle_x, f->particle_v,
                                                        f->particle_pressure, pel->local_x, off)));
     GridState gs;
-    ALB_LAUNCH(e, "pellet_grid", 7, st,
+    ALB_LAUNCH(e, "pellet_grid", kGridBuildKernels, st,
                ALB_TRY(grid_build<TF>(e, c, g, S.x, total, xs, flags, gs, st)));
     S.perm = gs.perm;
     ALB_LAUNCH(e, "pellet_lists", 1, st,

@@ -393,7 +393,7 @@ int sample_fluid(al_engine* engine, const typename SampleTypes<TF>::cn* cn, cons
   ALB_TRY(engine->buf("flags", 4, &sflags));
   ALB_CUDA(cudaMemsetAsync(sflags, 0, 4 * sizeof(uint32_t), st));
   GridState ss;
-  ALB_LAUNCH(engine, "sample_sort", 7, st,
+  ALB_LAUNCH(engine, "sample_sort", kGridBuildKernels, st,
              ALB_TRY(grid_build<TF>(engine, c, g, req->sample_x, req->num_samples, sxs, sflags,
                                     ss, st)));
   engine->ns = "sample.";
@@ -425,7 +425,7 @@ int sample_fluid(al_engine* engine, const typename SampleTypes<TF>::cn* cn, cons
     grid_x = all;
   }
   GridState gs;
-  ALB_LAUNCH(engine, "sample_grid", 7, st,
+  ALB_LAUNCH(engine, "sample_grid", kGridBuildKernels, st,
              ALB_TRY(grid_build<TF>(engine, c, g, grid_x, npts, xs, flags, gs, st)));
   SampleDev<TF> sd{req->sample_x,
                    req->num_samples,

@@ -69,7 +69,7 @@ __device__ __forceinline__ void gXV(const StepState<double>& S, uint32_t t, vec4
 template <class TF>
 __device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b, vec3<TF> f,
                                              vec3<TF> t) {
-  __shared__ double part[6][kBlock / 32];
+  __shared__ double part[6][kMaxBlock / 32];
   double v[6] = {double(f.x), double(f.y), double(f.z), double(t.x), double(t.y), double(t.z)};
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -81,7 +81,7 @@ __device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b,
   __syncthreads();
   if (threadIdx.x < 6) {
     double s = 0;
-    for (int w = 0; w < kBlock / 32; ++w) s += part[threadIdx.x][w];
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) s += part[threadIdx.x][w];
     S.ft[(size_t(blockIdx.x) * S.nb + b) * 6 + threadIdx.x] += s;
   }
   __syncthreads();
@@ -106,6 +106,26 @@ inline uint32_t pair_tpp(uint32_t n) {
   return tpp;
 }
 
+// Threads per block and per particle of one pass launch.
+struct LaunchShape {
+  uint32_t block, tpp;
+};
+
+// The pass groups whose launch shape the table sets: `pair` groups walk
+// neighbor lists and take threads per particle too.
+struct TunableGroup {
+  const char* name;
+  bool pair;
+};
+constexpr TunableGroup kTunable[] = {
+    {"neighbors", false},    {"div_warm1", true},     {"div_rho_adv", true},
+    {"div_iter", true},      {"div_residual", true},  {"viscosity", true},
+    {"press_warm0", true},   {"press_warm1", true},   {"press_rho_adv", true},
+    {"press_iter", true},    {"press_residual", true}, {"ii_predict0", true},
+    {"ii_predict1", true},   {"ii_iter0", true},      {"ii_iter1", true},
+    {"i_diag", true},        {"i_iter", true},        {"finish", true}};
+constexpr uint32_t kNumTunable = sizeof(kTunable) / sizeof(kTunable[0]);
+
 struct Lane {
   uint32_t s, sub, tpp;
   bool act;
@@ -124,8 +144,8 @@ __device__ __forceinline__ Lane pair_lane(const StepState<TF>& S) {
   return l;
 }
 
-inline uint32_t pair_blocks(uint32_t n, uint32_t tpp) {
-  return uint32_t((uint64_t(n) * tpp + kBlock - 1) / kBlock);
+inline uint32_t pair_blocks(uint32_t n, uint32_t tpp, uint32_t block = kBlock) {
+  return uint32_t((uint64_t(n) * tpp + block - 1) / block);
 }
 
 // Sum over the particle's lane group (every lane of the warp calls it; the
@@ -147,8 +167,11 @@ __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, u
 
 // Visits the lane's neighbors k = sub, sub + tpp, ... < cnt in batches of
 // B: the batch's list entries are loaded first, then all their records,
-// then `f(t, x_j, v_j)` runs for each in list order (the order of a plain
-// loop, so sums are bit-identical to one).  Batching keeps B dependent
+// then `f(t, x_j, v_j)` runs for each in list order.  At one thread per
+// particle that is the order of a plain loop over the list, so sums are
+// bit-identical to one; with tpp > 1 each lane sums every tpp-th neighbor
+// and group_sum combines the partial sums, a different (fixed) order whose
+// float results differ in the last bits.  Batching keeps B dependent
 // index -> record chains in flight per lane; it pays in the passes with
 // much arithmetic per neighbor (measured on the 1M-particle dam break at
 // one thread per particle: B = 8 for k_kappa (1.922 vs 1.928 ms per step at
@@ -260,6 +283,9 @@ struct WarmDivergence {
   float* feat = nullptr;      // [n][12] sorted order
   float* feat_out = nullptr;  // [n][12] original order
   TF two_r = 0, vol = 0;
+  // learned warm start gate: nonzero when the previous step of this scene ran
+  // both solves at their minimum iteration counts (the prediction is not used)
+  const uint32_t* floor = nullptr;
   __device__ __forceinline__ vec3<TF> self_v(uint32_t s) const { return xyz(RV(S, s)); }
   __device__ __forceinline__ vec3<TF> vj(uint32_t t) const { return xyz(gV(S, t)); }
   __device__ __forceinline__ void finish(uint32_t s, const BuildOut<TF>& o) const {
@@ -279,14 +305,15 @@ struct WarmDivergence {
     const TF w = adv > TF(0) ? TF(0.5) * fmax(kv, TF(-0.5)) / dt : TF(0);
     S.kappa_v[s] = w;
     RX(S, s).w = w;
-    if (feat || feat_out) {
+    const bool learned = feat && !(floor && *floor);
+    if (learned || feat_out) {
       const TF speed = sqrt(length_sqr(o.vi));
       const float f[AL_WARM_NUM_FEATURES] = {
           float(o.density - TF(1)), float(adv * dt), float(TF(o.cnt) / TF(32)),
           float(kv / dt), float(S.kappa[s] / (dt * dt)), float(bvol / vol),
           float(speed), float(speed * dt / two_r), float(o.alpha), float(bden),
           float(sqrt(o.grad_norm2) * two_r), float(dt)};
-      if (feat) {
+      if (learned) {
 #pragma unroll
         for (int k = 0; k < AL_WARM_NUM_FEATURES; ++k)
           feat[size_t(s) * AL_WARM_NUM_FEATURES + k] = f[k];
@@ -302,12 +329,14 @@ struct WarmDivergence {
 };
 
 // Learned divergence warm start: kappa_v = predicted kappa_v where the
-// reference's gate holds (rho_dot > 0, i.e. feature 1 > 0), else 0.
+// reference's gate holds (rho_dot > 0, i.e. feature 1 > 0), else 0.  When
+// the floor gate is set the build's plain warm start stays.
 template <class TF>
 __global__ void k_apply_warm_div(StepState<TF> S, const float* __restrict__ feat,
-                                 const float* __restrict__ pred) {
+                                 const float* __restrict__ pred,
+                                 const uint32_t* __restrict__ floor) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
+  if (s >= S.n || *floor) return;
   const TF w = feat[size_t(s) * AL_WARM_NUM_FEATURES + 1] > 0.f ? TF(pred[2 * size_t(s)]) : TF(0);
   S.kappa_v[s] = w;
   RX(S, s).w = w;
@@ -320,7 +349,7 @@ enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 // warm_start_pressure_solve1 (:3451-3491), pressure_solve_iteration
 // (:3543-3588).  Boundary reaction forces go to the per-block rigid slots.
 template <class TF, int MODE, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
   const Lane L = pair_lane(S);
@@ -374,7 +403,7 @@ __global__ void __launch_bounds__(kBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
 // compute_velocity_of_density_change (runner.hpp:3297-3314); also forms
 // k = rho_adv * alpha for the first divergence iteration.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   const TF adv = density_change(c, S, L);
@@ -389,7 +418,7 @@ __global__ void __launch_bounds__(kBlock) k_df_rho_adv_init(Cn<TF> c, StepState<
 // compute_divergence_solve_density_error (runner.hpp:3396-3410) with the
 // mean of solver_df.hpp:160-161 reduced in double on the device.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_df_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
@@ -410,7 +439,7 @@ __global__ void __launch_bounds__(kBlock)
 // calculate_cfl_v2 (runner.hpp:2533-2541) reduced to the global max; the
 // last block applies Solver::update_dt (solver.hpp:153-169).
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_viscosity(Cn<TF> c, StepState<TF> S, int finish_div) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
@@ -484,7 +513,7 @@ __global__ void __launch_bounds__(kBlock)
     v2 = length_sqr(vi + a * dt);
   }
   // block max, then one ordered-bits atomicMax per block
-  __shared__ TF wmax[kBlock / 32];
+  __shared__ TF wmax[kMaxBlock / 32];
   __shared__ bool last;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
@@ -492,7 +521,7 @@ __global__ void __launch_bounds__(kBlock)
   __syncthreads();
   if (threadIdx.x == 0) {
     TF bm = wmax[0];
-    for (int w = 1; w < kBlock / 32; ++w) bm = fmax(bm, wmax[w]);
+    for (int w = 1; w < int(blockDim.x >> 5); ++w) bm = fmax(bm, wmax[w]);
     unsigned long long bits;
     if constexpr (sizeof(TF) == 4)
       bits = __float_as_uint(bm);
@@ -530,17 +559,20 @@ __global__ void k_integrate_np(StepState<TF> S) {
 
 // warm_start_pressure_solve0 (runner.hpp:3430-3449).
 // With `pred` (learned warm start) the predicted kappa replaces the
-// previous-step value under the same gate (rho_adv > 1).
+// previous-step value under the same gate (rho_adv > 1), unless the floor
+// gate is set.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
-    k_p_warm0(Cn<TF> c, StepState<TF> S, const float* __restrict__ pred) {
+__global__ void __launch_bounds__(kMaxBlock)
+    k_p_warm0(Cn<TF> c, StepState<TF> S, const float* __restrict__ pred,
+              const uint32_t* __restrict__ floor) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
   const TF kp = S.kappa[L.s];
-  const TF warm = pred ? TF(pred[2 * size_t(L.s) + 1])
+  const bool learned = pred && !(floor && *floor);
+  const TF warm = learned ? TF(pred[2 * size_t(L.s) + 1])
                        : TF(0.5) * fmax(kp, TF(-0.00025)) / (dt * dt);
   const TF w = adv > TF(1) ? warm : TF(0);
   S.kappa[L.s] = w;
@@ -549,7 +581,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // compute_rho_adv (runner.hpp:3525-3541); also k for the first iteration.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
@@ -564,7 +596,7 @@ __global__ void __launch_bounds__(kBlock) k_p_rho_adv_init(Cn<TF> c, StepState<T
 // compute_pressure_solve_density_error (runner.hpp:3590-3604); the mean is
 // sum(rho_adv - 1) / N in double (solver_df.hpp:323-325 forms sum/N - 1).
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_p_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
@@ -587,9 +619,16 @@ __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __
                             TF* __restrict__ v_ref, TF* __restrict__ a_ref,
                             TF* __restrict__ rho_ref, TF* __restrict__ alpha_ref,
                             TF* __restrict__ kappa_ref, TF* __restrict__ kappa_v_ref,
-                            TF* __restrict__ rho_adv_ref) {
+                            TF* __restrict__ rho_adv_ref, uint32_t* __restrict__ warm_floor) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (warm_floor && s == 0) {
+    // learned warm start gate of the next step: both solves of this one ran
+    // at their minimum counts, where no warm start can save an iteration
+    const Ctrl<TF>& C = *S.ctrl;
+    *warm_floor = (C.rep.num_divergence_solve <= C.min_div &&
+                   C.rep.num_density_solve <= C.min_den) ? 1u : 0u;
+  }
   if (s >= S.n) return;
   const uint32_t i = S.perm[s];
   const TF dt = S.ctrl->dt;
@@ -613,7 +652,7 @@ __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __
 // predict_advection0 (runner.hpp:2609-2639).  kappa holds the pressure,
 // kappa_v the last pressure.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_ii_predict0(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   vec3<TF> xi{0, 0, 0};
@@ -649,7 +688,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict0(Cn<TF> c, StepState<TF> 
 
 // predict_advection1 (runner.hpp:2640-2690).  aii goes to kk.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_ii_predict1(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
@@ -693,7 +732,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_predict1(Cn<TF> c, StepState<TF> 
 // (solver_ii.hpp:204) for the own particle; this kernel reads the
 // neighbors' pressure (equal to their last pressure after that copy).
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   const bool first = S.ctrl->it == 0;
@@ -720,7 +759,7 @@ __global__ void __launch_bounds__(kBlock) k_ii_iter0(Cn<TF> c, StepState<TF> S) 
 // pressure_solve_iteration1 (runner.hpp:2716-2772) and the mean of
 // solver_ii.hpp:205-206 (double, on the device).
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_ii_iter1(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
@@ -773,7 +812,7 @@ __global__ void __launch_bounds__(kBlock)
 // compute_pressure_accels (runner.hpp:2774-2817) + kinematic_integration<0>
 // (runner.hpp:2873-2887), written back in original order.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_ii_accel_finish(Cn<TF> c, StepState<TF> S, TF* __restrict__ x_ref, TF* __restrict__ v_ref,
                       TF* __restrict__ a_ref, TF* __restrict__ rho_ref, TF* __restrict__ p_ref,
                       TF* __restrict__ rho_adv_ref) {
@@ -827,7 +866,7 @@ __global__ void __launch_bounds__(kBlock)
 // advect_and_init_pressure (runner.hpp:2889-2900): v += dt a, last pressure
 // (kappa_v) = pressure / 2.
 template <class TF>
-__global__ void __launch_bounds__(kBlock) k_i_advect(StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_i_advect(StepState<TF> S) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S.n) return;
   const TF dt = S.ctrl->dt;
@@ -840,7 +879,7 @@ __global__ void __launch_bounds__(kBlock) k_i_advect(StepState<TF> S) {
 // calculate_isph_diagonal_adv_density (runner.hpp:2901-2954): the Jacobi
 // diagonal (times rho0) into kk, the advected density into rho_adv.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
+__global__ void __launch_bounds__(kMaxBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
   const TF dt = S.ctrl->dt;
@@ -885,7 +924,7 @@ __global__ void __launch_bounds__(kBlock) k_i_diag(Cn<TF> c, StepState<TF> S) {
 // swap roles by iteration parity: iteration k reads kappa_v and writes
 // kappa when k is even, the reverse when odd.
 template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kMaxBlock)
     k_i_iter(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const Lane L = pair_lane(S);
@@ -1032,6 +1071,22 @@ struct StepPlan {
   float* warm_feat = nullptr;
   float* warm_feat_out = nullptr;
   float* warm_pred = nullptr;
+  // [0]: 1 when the scene's previous step ran both solves at their minimum
+  // iteration counts; the network is then skipped (fresh scenes start at 0)
+  uint32_t* warm_floor = nullptr;
+  // launch shapes: particle-count bucket and context of the shape table
+  uint32_t bucket = 0, ctx = 0;
+  // Shape of pass group `group` (defaults: 128-thread blocks; pair passes
+  // pair_tpp(n) threads per particle, other passes one).
+  LaunchShape shape(const al_engine* e, const char* group, bool pair) const {
+    LaunchShape sh{uint32_t(kBlock), pair ? pair_tpp(S.n) : 1u};
+    auto it = e->shapes.find(std::make_tuple(std::string(group), bucket, ctx));
+    if (it != e->shapes.end()) {
+      if (it->second.first) sh.block = it->second.first;
+      if (pair && it->second.second) sh.tpp = it->second.second;
+    }
+    return sh;
+  }
 };
 
 // Adds a device-driven WHILE loop at the current end of the capture on
@@ -1093,11 +1148,19 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
   // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
   GridState gs;
-  ALB_LAUNCH(e, "grid_sort", 7, st,
+  ALB_LAUNCH(e, "grid_sort", kGridBuildKernels, st,
              ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
   S.perm = gs.perm;
   const uint32_t blocks = blocks_for(n, kBlock);
-  const uint32_t pblocks = pair_blocks(n, S.tpp);
+  // grid, block and lane state of pair pass group `g` (launch-shape table)
+  auto pair_shape = [&](const char* g, uint32_t& grid, uint32_t& block) {
+    const LaunchShape sh = P.shape(e, g, true);
+    StepState<TF> Sg = S;
+    Sg.tpp = sh.tpp;
+    grid = pair_blocks(n, sh.tpp, sh.block);
+    block = sh.block;
+    return Sg;
+  };
   if (n > 0) {
     const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
     if (iisph)
@@ -1120,22 +1183,25 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
   TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
   if (div && n > 0) {
-    WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol};
+    WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol,
+                          P.warm_floor};
+    const uint32_t nbb = P.shape(e, "neighbors", false).block;
     ALB_LAUNCH(e, "neighbors", 1, st,
                (wr ? k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, true>
-                         <<<blocks_for(n, kBlock), kBlock, 0, st>>>(
+                         <<<blocks_for(n, nbb), nbb, 0, st>>>(
                              c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
                              rho_rec, gs.flags, wd)
                    : k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false>
-                         <<<blocks_for(n, kBlock), kBlock, 0, st>>>(
+                         <<<blocks_for(n, nbb), nbb, 0, st>>>(
                              c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
                              rho_rec, gs.flags, wd)));
     if (P.learned) {
       ALB_LAUNCH(e, "warm_net", 1, st,
-                 ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, st)));
+                 ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, st,
+                                      P.warm_floor)));
       ALB_LAUNCH(e, "warm_apply", 1, st,
                  (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(
-                     S, P.warm_feat, P.warm_pred)));
+                     S, P.warm_feat, P.warm_pred, P.warm_floor)));
     }
   } else
     ALB_LAUNCH(e, "neighbors", 1, st,
@@ -1165,36 +1231,76 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
   };
   if (n > 0) {
     if (div) {
-      ALB_LAUNCH(e, "div_warm1", 1, st,
-                 (wr ? k_kappa<TF, kDivWarm, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_kappa<TF, kDivWarm, false><<<pblocks, kBlock, 0, st>>>(c, S)));
-      ALB_LAUNCH(e, "div_rho_adv", 1, st,
-                 (wr ? k_df_rho_adv_init<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_df_rho_adv_init<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("div_warm1", pg_, pb_);
+        ALB_LAUNCH(e, "div_warm1", 1, st,
+                   (wr ? k_kappa<TF, kDivWarm, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_kappa<TF, kDivWarm, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+      }
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("div_rho_adv", pg_, pb_);
+        ALB_LAUNCH(e, "div_rho_adv", 1, st,
+                   (wr ? k_df_rho_adv_init<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_df_rho_adv_init<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+      }
       ALB_TRY(solve(0, P.io.hc->max_div,
                     [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
-                      ALB_LAUNCH(e, "div_iter", 1, s,
-                                 (wr ? k_kappa<TF, kDivIter, true><<<pblocks, kBlock, 0, s>>>(c, S) : k_kappa<TF, kDivIter, false><<<pblocks, kBlock, 0, s>>>(c, S)));
-                      ALB_LAUNCH(e, "div_residual", 1, s,
-                                 (wr ? k_df_residual<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_df_residual<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
+                      {
+                        uint32_t pg_, pb_;
+                        const StepState<TF> Sg_ = pair_shape("div_iter", pg_, pb_);
+                        ALB_LAUNCH(e, "div_iter", 1, s,
+                                   (wr ? k_kappa<TF, kDivIter, true><<<pg_, pb_, 0, s>>>(c, Sg_) : k_kappa<TF, kDivIter, false><<<pg_, pb_, 0, s>>>(c, Sg_)));
+                      }
+                      {
+                        uint32_t pg_, pb_;
+                        const StepState<TF> Sg_ = pair_shape("div_residual", pg_, pb_);
+                        ALB_LAUNCH(e, "div_residual", 1, s,
+                                   (wr ? k_df_residual<TF, true><<<pg_, pb_, 0, s>>>(c, Sg_, h, use) : k_df_residual<TF, false><<<pg_, pb_, 0, s>>>(c, Sg_, h, use)));
+                      }
                       return AL_OK;
                     }));
     }
-    ALB_LAUNCH(e, "viscosity", 1, st,
-               (wr ? k_viscosity<TF, true><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0) : k_viscosity<TF, false><<<pblocks, kBlock, 0, st>>>(c, S, div ? 1 : 0)));
+    {
+      uint32_t pg_, pb_;
+      const StepState<TF> Sg_ = pair_shape("viscosity", pg_, pb_);
+      ALB_LAUNCH(e, "viscosity", 1, st,
+                 (wr ? k_viscosity<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_, div ? 1 : 0) : k_viscosity<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_, div ? 1 : 0)));
+    }
     if (!iisph) {
       ALB_LAUNCH(e, "integrate_np", 1, st, k_integrate_np<TF><<<blocks, kBlock, 0, st>>>(S));
       if (den) {
-        ALB_LAUNCH(e, "press_warm0", 1, st,
-                   (wr ? k_p_warm0<TF, true><<<pblocks, kBlock, 0, st>>>(c, S, P.warm_pred) : k_p_warm0<TF, false><<<pblocks, kBlock, 0, st>>>(c, S, P.warm_pred)));
-        ALB_LAUNCH(e, "press_warm1", 1, st,
-                   (wr ? k_kappa<TF, kPressWarm, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_kappa<TF, kPressWarm, false><<<pblocks, kBlock, 0, st>>>(c, S)));
-        ALB_LAUNCH(e, "press_rho_adv", 1, st,
-                   (wr ? k_p_rho_adv_init<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_p_rho_adv_init<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
+        {
+          uint32_t pg_, pb_;
+          const StepState<TF> Sg_ = pair_shape("press_warm0", pg_, pb_);
+          ALB_LAUNCH(e, "press_warm0", 1, st,
+                     (wr ? k_p_warm0<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_, P.warm_pred, P.warm_floor) : k_p_warm0<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_, P.warm_pred, P.warm_floor)));
+        }
+        {
+          uint32_t pg_, pb_;
+          const StepState<TF> Sg_ = pair_shape("press_warm1", pg_, pb_);
+          ALB_LAUNCH(e, "press_warm1", 1, st,
+                     (wr ? k_kappa<TF, kPressWarm, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_kappa<TF, kPressWarm, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+        }
+        {
+          uint32_t pg_, pb_;
+          const StepState<TF> Sg_ = pair_shape("press_rho_adv", pg_, pb_);
+          ALB_LAUNCH(e, "press_rho_adv", 1, st,
+                     (wr ? k_p_rho_adv_init<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_p_rho_adv_init<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+        }
         ALB_TRY(solve(1, P.io.hc->max_den,
                       [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
-                        ALB_LAUNCH(e, "press_iter", 1, s,
-                                   (wr ? k_kappa<TF, kPressIter, true><<<pblocks, kBlock, 0, s>>>(c, S) : k_kappa<TF, kPressIter, false><<<pblocks, kBlock, 0, s>>>(c, S)));
-                        ALB_LAUNCH(e, "press_residual", 1, s,
-                                   (wr ? k_p_residual<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_p_residual<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
+                        {
+                          uint32_t pg_, pb_;
+                          const StepState<TF> Sg_ = pair_shape("press_iter", pg_, pb_);
+                          ALB_LAUNCH(e, "press_iter", 1, s,
+                                     (wr ? k_kappa<TF, kPressIter, true><<<pg_, pb_, 0, s>>>(c, Sg_) : k_kappa<TF, kPressIter, false><<<pg_, pb_, 0, s>>>(c, Sg_)));
+                        }
+                        {
+                          uint32_t pg_, pb_;
+                          const StepState<TF> Sg_ = pair_shape("press_residual", pg_, pb_);
+                          ALB_LAUNCH(e, "press_residual", 1, s,
+                                     (wr ? k_p_residual<TF, true><<<pg_, pb_, 0, s>>>(c, Sg_, h, use) : k_p_residual<TF, false><<<pg_, pb_, 0, s>>>(c, Sg_, h, use)));
+                        }
                         return AL_OK;
                       }));
       }
@@ -1202,44 +1308,76 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                  (wr ? k_df_finish<TF, true><<<blocks, kBlock, 0, st>>>(
                      c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
                      f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                     f->particle_kappa_v, f->particle_density_adv) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
+                     f->particle_kappa_v, f->particle_density_adv, P.warm_floor) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
                      c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
                      f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                     f->particle_kappa_v, f->particle_density_adv)));
+                     f->particle_kappa_v, f->particle_density_adv, P.warm_floor)));
     } else if (P.isph) {
       ALB_LAUNCH(e, "i_advect", 1, st, k_i_advect<TF><<<blocks, kBlock, 0, st>>>(S));
-      ALB_LAUNCH(e, "i_diag", 1, st, (wr ? k_i_diag<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_i_diag<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("i_diag", pg_, pb_);
+        ALB_LAUNCH(e, "i_diag", 1, st, (wr ? k_i_diag<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_i_diag<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+      }
       ALB_TRY(solve(1, P.io.hc->max_den,
                     [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
-                      ALB_LAUNCH(e, "i_iter", 1, s,
-                                 (wr ? k_i_iter<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_i_iter<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
+                      {
+                        uint32_t pg_, pb_;
+                        const StepState<TF> Sg_ = pair_shape("i_iter", pg_, pb_);
+                        ALB_LAUNCH(e, "i_iter", 1, s,
+                                   (wr ? k_i_iter<TF, true><<<pg_, pb_, 0, s>>>(c, Sg_, h, use) : k_i_iter<TF, false><<<pg_, pb_, 0, s>>>(c, Sg_, h, use)));
+                      }
                       return AL_OK;
                     }));
       ALB_LAUNCH(e, "i_final", 1, st,
                  k_i_final<TF><<<blocks, kBlock, 0, st>>>(S));
-      ALB_LAUNCH(e, "finish", 1, st,
-                 (wr ? k_ii_accel_finish<TF, true><<<pblocks, kBlock, 0, st>>>(
-                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-                     f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pblocks, kBlock, 0, st>>>(
-                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-                     f->particle_pressure, f->particle_density_adv)));
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("finish", pg_, pb_);
+        ALB_LAUNCH(e, "finish", 1, st,
+                   (wr ? k_ii_accel_finish<TF, true><<<pg_, pb_, 0, st>>>(
+                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pg_, pb_, 0, st>>>(
+                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       f->particle_pressure, f->particle_density_adv)));
+      }
     } else {
-      ALB_LAUNCH(e, "ii_predict0", 1, st, (wr ? k_ii_predict0<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_ii_predict0<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
-      ALB_LAUNCH(e, "ii_predict1", 1, st, (wr ? k_ii_predict1<TF, true><<<pblocks, kBlock, 0, st>>>(c, S) : k_ii_predict1<TF, false><<<pblocks, kBlock, 0, st>>>(c, S)));
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("ii_predict0", pg_, pb_);
+        ALB_LAUNCH(e, "ii_predict0", 1, st, (wr ? k_ii_predict0<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_ii_predict0<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+      }
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("ii_predict1", pg_, pb_);
+        ALB_LAUNCH(e, "ii_predict1", 1, st, (wr ? k_ii_predict1<TF, true><<<pg_, pb_, 0, st>>>(c, Sg_) : k_ii_predict1<TF, false><<<pg_, pb_, 0, st>>>(c, Sg_)));
+      }
       ALB_TRY(solve(1, P.io.hc->max_den,
                     [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
-                      ALB_LAUNCH(e, "ii_iter0", 1, s,
-                                 (wr ? k_ii_iter0<TF, true><<<pblocks, kBlock, 0, s>>>(c, S) : k_ii_iter0<TF, false><<<pblocks, kBlock, 0, s>>>(c, S)));
-                      ALB_LAUNCH(e, "ii_iter1", 1, s,
-                                 (wr ? k_ii_iter1<TF, true><<<pblocks, kBlock, 0, s>>>(c, S, h, use) : k_ii_iter1<TF, false><<<pblocks, kBlock, 0, s>>>(c, S, h, use)));
+                      {
+                        uint32_t pg_, pb_;
+                        const StepState<TF> Sg_ = pair_shape("ii_iter0", pg_, pb_);
+                        ALB_LAUNCH(e, "ii_iter0", 1, s,
+                                   (wr ? k_ii_iter0<TF, true><<<pg_, pb_, 0, s>>>(c, Sg_) : k_ii_iter0<TF, false><<<pg_, pb_, 0, s>>>(c, Sg_)));
+                      }
+                      {
+                        uint32_t pg_, pb_;
+                        const StepState<TF> Sg_ = pair_shape("ii_iter1", pg_, pb_);
+                        ALB_LAUNCH(e, "ii_iter1", 1, s,
+                                   (wr ? k_ii_iter1<TF, true><<<pg_, pb_, 0, s>>>(c, Sg_, h, use) : k_ii_iter1<TF, false><<<pg_, pb_, 0, s>>>(c, Sg_, h, use)));
+                      }
                       return AL_OK;
                     }));
-      ALB_LAUNCH(e, "finish", 1, st,
-                 (wr ? k_ii_accel_finish<TF, true><<<pblocks, kBlock, 0, st>>>(
-                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-                     f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pblocks, kBlock, 0, st>>>(
-                     c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
-                     f->particle_pressure, f->particle_density_adv)));
+      {
+        uint32_t pg_, pb_;
+        const StepState<TF> Sg_ = pair_shape("finish", pg_, pb_);
+        ALB_LAUNCH(e, "finish", 1, st,
+                   (wr ? k_ii_accel_finish<TF, true><<<pg_, pb_, 0, st>>>(
+                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pg_, pb_, 0, st>>>(
+                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       f->particle_pressure, f->particle_density_adv)));
+      }
     }
   }
   if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(S));
@@ -1336,9 +1474,8 @@ struct StepArgs {
   TF* dt = nullptr;
   al_step_report* report = nullptr;
   const al_warm_start* warm = nullptr;
-  // particles that share the GPU with this scene's passes (a batch's total;
-  // 0: the scene's own); it sets the pair passes' threads per particle
-  uint64_t pair_total = 0;
+  // launch-shape context: 0 single step, 1 a scene of a batched step
+  uint32_t batch = 0;
 };
 
 // Validates the arguments, sizes the scene's scratch (under the engine's
@@ -1366,8 +1503,18 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   S.n = n;
   S.nb = nb;
   S.cap = P.g.cap_nbr;
-  S.tpp = pair_tpp(A.pair_total ? uint32_t(std::min<uint64_t>(A.pair_total, 0xffffffffu)) : n);
-  S.grid = pair_blocks(n, S.tpp) > 0 ? pair_blocks(n, S.tpp) : 1;  // grid of the pair passes
+  P.bucket = n ? uint32_t(31 - __builtin_clz(n)) : 0u;
+  P.ctx = A.batch;
+  S.tpp = pair_tpp(n);
+  // per-block buffers (rigid partials, reduction partials) hold the largest
+  // grid any pair pass of this scene launches
+  S.grid = pair_blocks(n, S.tpp);
+  for (uint32_t k = 0; k < kNumTunable; ++k) {
+    if (!kTunable[k].pair) continue;
+    const LaunchShape sh = P.shape(e, kTunable[k].name, true);
+    S.grid = std::max(S.grid, pair_blocks(n, sh.tpp, sh.block));
+  }
+  if (S.grid == 0) S.grid = 1;
   // ---- buffers
   ALB_TRY(e->buf("flags", 4, &P.flags));
   ALB_TRY(e->buf("sorted.x", n, &S.x));
@@ -1410,6 +1557,9 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
       P.net = to_warm_dev(*warm->net);
       ALB_TRY(e->buf("warm.feat", size_t(n) * AL_WARM_NUM_FEATURES, &P.warm_feat));
       ALB_TRY(e->buf("warm.pred", size_t(n) * AL_WARM_NUM_OUTPUTS, &P.warm_pred));
+      bool fresh = false;
+      ALB_TRY(e->buf("warm.floor", 4, &P.warm_floor, &fresh));
+      if (fresh) ALB_CUDA(cudaMemset(P.warm_floor, 0, 4 * sizeof(uint32_t)));
     }
   }
   // ---- host staging: control block, bodies, rigid state
@@ -1729,6 +1879,64 @@ int al_i_step_f64(al_engine* engine, const al_const_f64* cn, const al_consti* cn
                           static_cast<cudaStream_t>(stream));
 }
 
+int al_engine_set_launch_shape(al_engine* engine, const char* group, uint32_t bucket,
+                               uint32_t batch, uint32_t block, uint32_t tpp) {
+  ALB_CHECK_ARG(engine && group, "al_engine_set_launch_shape: null argument");
+  const TunableGroup* tg = nullptr;
+  for (uint32_t k = 0; k < kNumTunable; ++k)
+    if (std::string(kTunable[k].name) == group) tg = &kTunable[k];
+  if (!tg) {
+    set_error(std::string("al_engine_set_launch_shape: no tunable pass group '") + group + "'");
+    return AL_ERR_INVALID;
+  }
+  ALB_CHECK_ARG(bucket < 32 && batch < 2, "al_engine_set_launch_shape: bucket < 32, batch 0 or 1");
+  ALB_CHECK_ARG(block == 0 || block == 64 || block == 128 || block == 256,
+                "al_engine_set_launch_shape: block must be 64, 128 or 256 (0: default)");
+  ALB_CHECK_ARG(tpp == 0 || tpp == 1 || ((tpp == 2 || tpp == 4 || tpp == 8) && tg->pair),
+                "al_engine_set_launch_shape: threads per particle 1, 2, 4 or 8 (pair passes "
+                "only; 0: default)");
+  const auto key = std::make_tuple(std::string(group), bucket, batch);
+  if (block == 0 && tpp == 0)
+    engine->shapes.erase(key);
+  else
+    engine->shapes[key] = std::make_pair(block, tpp);
+  ALB_CUDA(cudaSetDevice(engine->device));
+  engine->drop_graphs();  // captured steps hold the old shapes
+  ++engine->generation;
+  return AL_OK;
+}
+
+int al_engine_get_launch_shape(al_engine* engine, const char* group, uint32_t num_particles,
+                               uint32_t batch, uint32_t* block, uint32_t* tpp) {
+  ALB_CHECK_ARG(engine && group && block && tpp, "al_engine_get_launch_shape: null argument");
+  const TunableGroup* tg = nullptr;
+  for (uint32_t k = 0; k < kNumTunable; ++k)
+    if (std::string(kTunable[k].name) == group) tg = &kTunable[k];
+  if (!tg) {
+    set_error(std::string("al_engine_get_launch_shape: no tunable pass group '") + group + "'");
+    return AL_ERR_INVALID;
+  }
+  StepPlan<float> P;
+  P.S.n = num_particles;
+  P.bucket = num_particles ? uint32_t(31 - __builtin_clz(num_particles)) : 0u;
+  P.ctx = batch ? 1u : 0u;
+  const LaunchShape sh = P.shape(engine, group, tg->pair);
+  *block = sh.block;
+  *tpp = sh.tpp;
+  return AL_OK;
+}
+
+int al_tunable_group(uint32_t index, const char** name, uint32_t* pair) {
+  ALB_CHECK_ARG(name && pair, "al_tunable_group: null argument");
+  if (index >= kNumTunable) {
+    set_error("al_tunable_group: index past the last group");
+    return AL_ERR_INVALID;
+  }
+  *name = kTunable[index].name;
+  *pair = kTunable[index].pair ? 1u : 0u;
+  return AL_OK;
+}
+
 int al_df_batch_step_f32(al_engine* engine, al_scene_f32* scenes, uint32_t num_scenes,
                          void* stream) {
   ALB_CHECK_ARG(engine && (num_scenes == 0 || scenes), "al_df_batch_step_f32: null argument");
@@ -1747,10 +1955,8 @@ int al_df_batch_step_f32(al_engine* engine, al_scene_f32* scenes, uint32_t num_s
     args[k].dt = sc.dt;
     args[k].report = sc.report;
   }
-  // the scenes' passes run side by side: threads per particle from the total
-  uint64_t total = 0;
-  for (uint32_t k = 0; k < num_scenes; ++k) total += args[k].f ? args[k].f->num_particles : 0u;
-  for (uint32_t k = 0; k < num_scenes; ++k) args[k].pair_total = total;
+  // launch shapes from the batch context of the shape table
+  for (uint32_t k = 0; k < num_scenes; ++k) args[k].batch = 1;
   std::vector<int> status;
   const int rc = run_batch<float>(engine, args, status, static_cast<cudaStream_t>(stream));
   for (uint32_t k = 0; k < num_scenes; ++k)

@@ -104,7 +104,11 @@ __device__ __forceinline__ bool run_layer(uint32_t d_tmem, const uint8_t* a, con
 
 __global__ void __launch_bounds__(kTile)
     k_warm_forward(WarmNetDev net, const float* __restrict__ features, uint32_t n,
-                   float* __restrict__ out, uint32_t* __restrict__ err) {
+                   float* __restrict__ out, uint32_t* __restrict__ err,
+                   const uint32_t* __restrict__ skip) {
+  // the whole grid leaves before any shared-memory or TMEM work when the
+  // step's gate says the prediction is not used
+  if (skip && *skip) return;
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t* A1 = sm + kSmA1;
   uint8_t* A2 = sm + kSmA2;
@@ -496,7 +500,7 @@ __global__ void k_warm_adam(float* __restrict__ p, const float* __restrict__ g,
 }  // namespace
 
 int warm_forward(al_engine* e, const WarmNetDev& net, const float* features, uint32_t n,
-                 float* out, uint32_t* err, cudaStream_t st) {
+                 float* out, uint32_t* err, cudaStream_t st, const uint32_t* skip) {
   if (n == 0) return AL_OK;
   static bool attr_set[64] = {};
   if (e->device >= 0 && e->device < 64 && !attr_set[e->device]) {
@@ -506,7 +510,7 @@ int warm_forward(al_engine* e, const WarmNetDev& net, const float* features, uin
   }
   const uint32_t tiles = blocks_for(n, kTile);
   const uint32_t grid = tiles < uint32_t(2 * e->num_sms) ? tiles : uint32_t(2 * e->num_sms);
-  k_warm_forward<<<grid, kTile, kInferSmem, st>>>(net, features, n, out, err);
+  k_warm_forward<<<grid, kTile, kInferSmem, st>>>(net, features, n, out, err, skip);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }

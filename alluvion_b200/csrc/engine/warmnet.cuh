@@ -77,8 +77,9 @@ __device__ __forceinline__ void warm_normalize(const WarmNetDev& net, const floa
 }
 
 // out[p][0..1] = net(features[p]) * out_scale for p < n (features: raw
-// [n][12] FP32).  Raises err[0] if a tensor-core wait timed out.
+// [n][12] FP32).  Raises err[0] if a tensor-core wait timed out.  With
+// `skip` (device word) nonzero when the kernel runs, it returns at once.
 int warm_forward(al_engine* e, const WarmNetDev& net, const float* features, uint32_t n,
-                 float* out, uint32_t* err, cudaStream_t st);
+                 float* out, uint32_t* err, cudaStream_t st, const uint32_t* skip = nullptr);
 
 }  // namespace alb

@@ -226,6 +226,61 @@ def box_inertia(mass, widths):
             mass * (wx * wx + wy * wy) / 12)
 
 
+def body_from_spec(dtype, cn, spec):
+    """al_body_{f32,f64} (node pointers NULL) of a body spec dict: keys shape,
+    params, sign, resolution, use_distance_grid, mass, inertia, optional
+    margin, and mesh = (vertices, faces) with offset for AL_SHAPE_MESH."""
+    mesh = spec.get("mesh")
+    aabb = mesh_aabb(mesh[0], spec.get("offset", 0.0)) if mesh is not None else None
+    return make_body(dtype, cn, spec["shape"], spec.get("params", []), spec["resolution"],
+                     sign=spec.get("sign", 1.0), margin=spec.get("margin"),
+                     use_distance_grid=mesh is not None or spec.get("use_distance_grid", False),
+                     mass=spec.get("mass", 0.0), inertia=spec.get("inertia", (1, 1, 1)),
+                     aabb=aabb)
+
+
+def rigid_from_spec(dtype, spec):
+    return rigid_state(dtype, x=spec.get("x", (0, 0, 0)), v=spec.get("v", (0, 0, 0)),
+                       q=spec.get("q", (0, 0, 0, 1)), omega=spec.get("omega", (0, 0, 0)))
+
+
+class SceneSpec:
+    """Host description of a seeded scene: constants (cn, cni), particle
+    positions x [n][3] and body spec dicts (see body_from_spec), with no
+    device memory and no call into the engine library."""
+
+    def __init__(self, dtype, cn, cni, x, bodies):
+        self.dtype = np.dtype(dtype)
+        self.cn = cn
+        self.cni = cni
+        self.x = x
+        self.body_specs = list(bodies)
+        self.cni.num_boundaries = len(self.body_specs)
+
+    @property
+    def n(self):
+        return int(self.x.shape[0])
+
+    @property
+    def num_boundaries(self):
+        return len(self.body_specs)
+
+    def bodies(self):
+        """ctypes array of al_body (node pointers NULL) and rigid (nb, 13)."""
+        _, BodyT, _, _ = _capi.real_types(self.dtype)
+        nb = self.num_boundaries
+        arr = (BodyT * max(nb, 1))()
+        for b, spec in enumerate(self.body_specs):
+            arr[b] = body_from_spec(self.dtype, self.cn, spec)
+        rigid = rigid_array(self.dtype, [rigid_from_spec(self.dtype, s) for s in self.body_specs])
+        return arr, rigid
+
+    def device(self, engine, device="cuda"):
+        """The scene on a CUDA device (grids built by the engine)."""
+        return DeviceScene(engine, self.dtype, self.cn, self.cni, self.x, self.body_specs,
+                           device=device)
+
+
 class DeviceScene:
     """A seeded scene held on one CUDA device: constants, grid dimensions,
     bodies with device-built distance grids and volume maps, and the
@@ -267,14 +322,7 @@ class DeviceScene:
         self.rigid = (RigidT * max(nb, 1))()
         for b, spec in enumerate(self.body_specs):
             mesh = spec.get("mesh")  # (vertices [nv][3], faces [nf][3]) for SHAPE_MESH
-            aabb = mesh_aabb(mesh[0], spec.get("offset", 0.0)) if mesh is not None else None
-            body = make_body(dtype, cn, spec["shape"], spec.get("params", []),
-                             spec["resolution"], sign=spec.get("sign", 1.0),
-                             margin=spec.get("margin"),
-                             use_distance_grid=mesh is not None or spec.get("use_distance_grid",
-                                                                            False),
-                             mass=spec.get("mass", 0.0), inertia=spec.get("inertia", (1, 1, 1)),
-                             aabb=aabb)
+            body = body_from_spec(dtype, cn, spec)
             dist = zeros(body.num_nodes) if body.use_distance_grid else None
             vol = zeros(body.num_nodes)
             if mesh is not None:
@@ -298,10 +346,7 @@ class DeviceScene:
             self.bodies[b] = body
             self.distance_nodes.append(dist)
             self.volume_nodes.append(vol)
-            self.rigid[b] = rigid_state(dtype, x=spec.get("x", (0, 0, 0)),
-                                        v=spec.get("v", (0, 0, 0)),
-                                        q=spec.get("q", (0, 0, 0, 1)),
-                                        omega=spec.get("omega", (0, 0, 0)))
+            self.rigid[b] = rigid_from_spec(dtype, spec)
         self.cni.num_boundaries = nb
         torch.cuda.synchronize()
 
@@ -362,6 +407,27 @@ class DeviceScene:
         rigid = rigid_array(self.dtype, [self.rigid[b] for b in range(nb)])
         return hb, keep, rigid
 
+    STATE_KEYS = ("x", "v", "a", "density", "dfsph_factor", "kappa", "kappa_v", "density_adv",
+                  "pressure")
+
+    def snapshot(self):
+        """Device copies of the mutable state (particles and rigid bodies)."""
+        dev = {k: getattr(self, k).clone() for k in self.STATE_KEYS}
+        rig = []
+        for b in range(self.num_boundaries):
+            r = type(self.rigid[b])()
+            ctypes.memmove(ctypes.addressof(r), ctypes.addressof(self.rigid[b]), ctypes.sizeof(r))
+            rig.append(r)
+        return dev, rig
+
+    def restore(self, snap):
+        """Puts back a snapshot() (same scene, same buffers)."""
+        dev, rig = snap
+        for k, t in dev.items():
+            getattr(self, k).copy_(t)
+        for b, r in enumerate(rig):
+            ctypes.memmove(ctypes.addressof(self.rigid[b]), ctypes.addressof(r), ctypes.sizeof(r))
+
     def state(self):
         """Host copies of the particle state."""
         g = lambda t: t.cpu().numpy()
@@ -394,6 +460,17 @@ def dam_break(engine, dtype, lattice, particle_radius, container, bodies=(), see
     the volume-map boundary term, runner.hpp:1982-2072, a particle at h/2
     from a wall sees rho ~ 2 rho0, so that layout starts far from
     equilibrium.  At h the wall term is exactly zero.)"""
+    return dam_break_spec(dtype, lattice, particle_radius, container, bodies, seed=seed,
+                          volume_resolution=volume_resolution, jitter=jitter,
+                          max_num_particles_per_cell=max_num_particles_per_cell,
+                          max_num_neighbors_per_particle=max_num_neighbors_per_particle,
+                          **const_kw).device(engine)
+
+
+def dam_break_spec(dtype, lattice, particle_radius, container, bodies=(), seed=0,
+                   volume_resolution=64, jitter=0.1, max_num_particles_per_cell=64,
+                   max_num_neighbors_per_particle=64, **const_kw):
+    """The host description (SceneSpec) of dam_break's scene."""
     cn = make_const(dtype, particle_radius, **const_kw)
     h = float(cn.kernel_radius)
     gap = h - 2 * float(particle_radius)
@@ -405,7 +482,7 @@ def dam_break(engine, dtype, lattice, particle_radius, container, bodies=(), see
     all_bodies = [cont] + list(bodies)
     cni = make_consti(-0.5 * h * np.ones(3), size + 0.5 * h, h, len(all_bodies),
                       max_num_particles_per_cell, max_num_neighbors_per_particle)
-    return DeviceScene(engine, dtype, cn, cni, x, all_bodies)
+    return SceneSpec(dtype, cn, cni, x, all_bodies)
 
 
 def seeded_rigid_bodies(seed, container, particle_radius, spheres=2, boxes=2,

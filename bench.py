@@ -75,6 +75,8 @@ POSTPROC_WORKLOADS = {
              "1,000,000-particle lattice (r = 0.01 m, 100^3), no bodies"),
 }
 METHOD_NAME = {"df": "DFSPH", "ii": "IISPH", "i": "implicit SPH (SolverI)"}
+# the large coupled scene: 8,388,608 particles, three bodies on 128^3 grids
+DEFAULT_WORKLOAD = "dambreak-8m"
 
 # Compulsory per-particle state traffic per pass, float32 ("Model A": every
 # per-particle array read/written once per pass, neighbor gathers served
@@ -145,14 +147,27 @@ def parse_args():
     p.add_argument("--eager", action="store_true",
                    help="launch every kernel from the host (no captured step graph)")
     p.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) +
-                   sorted(POSTPROC_WORKLOADS), default="dambreak-1m")
+                   sorted(POSTPROC_WORKLOADS), default=DEFAULT_WORKLOAD)
     p.add_argument("--method", choices=["df", "ii", "i"], default="df")
-    p.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
-                   help="learned: DFSPH with the learned warm start, trained (untimed) on a "
-                        "differently seeded scene of the same workload")
+    p.add_argument("--warm-start", choices=["auto", "plain", "learned", "both"], default="auto",
+                   help="learned: DFSPH with the learned warm start; both: plain and learned "
+                        "arms from the same initial state, the learned one reported as the "
+                        "value; auto: both on the default workload's DFSPH, else plain")
+    p.add_argument("--warm-net", default=None,
+                   help="network file (default: the committed alluvion_b200/data/"
+                        "warm_start_dambreak.npz); 'train': fit one now (untimed)")
+    p.add_argument("--fp64-steps", type=int, default=None,
+                   help="steps of the float32-vs-float64 error statement (default 20 on the "
+                        "default workload, else 0)")
+    p.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
+                   help="sweep the pass groups' launch shapes before timing (untimed; "
+                        "alluvion_b200.autotune); auto: on for batched workloads")
     p.add_argument("--max-dt", type=float, default=None,
                    help="time-step cap (default 2e-4 s)")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.fp64_steps is None:
+        a.fp64_steps = 20 if a.workload == DEFAULT_WORKLOAD and a.impl == "engine" else 0
+    return a
 
 
 def dist_env():
@@ -261,14 +276,58 @@ def workload_bodies(wl):
     return []
 
 
-def build_scene(engine, workload="dambreak-1m", dtype=np.float32, rigid_bodies=None,
-                container_resolution=None, seed=SEED):
+def build_scene_spec(workload="dambreak-1m", dtype=np.float32, rigid_bodies=None,
+                     container_resolution=None, seed=SEED):
+    """Host description of a workload's seeded scene (no engine involved)."""
     from alluvion_b200 import scenes
     wl = WORKLOADS[workload]
     bodies = [] if rigid_bodies == 0 else workload_bodies(wl)
     res = container_resolution or wl["container_resolution"]
-    return scenes.dam_break(engine, dtype, wl["lattice"], wl["radius"], wl["container"], bodies,
-                            seed=seed, volume_resolution=res)
+    return scenes.dam_break_spec(dtype, wl["lattice"], wl["radius"], wl["container"], bodies,
+                                 seed=seed, volume_resolution=res)
+
+
+def build_scene(engine, workload="dambreak-1m", dtype=np.float32, rigid_bodies=None,
+                container_resolution=None, seed=SEED):
+    return build_scene_spec(workload, dtype, rigid_bodies, container_resolution,
+                            seed).device(engine)
+
+
+def oracle_scene(spec, dilate=2):
+    """The scene's grids built by the oracle on the host cores, for the CPU
+    arms that must not load the engine: distance nodes sampled from the
+    analytic shapes, volume maps filled lazily (same node values as the
+    eager build), with every node the particles can reach within `dilate`
+    cells computed up front.  Returns (bodies, keep-alive arrays, rigid,
+    seconds)."""
+    from oracle import binding as orc
+    t0 = time.perf_counter()
+    bodies, rigid = spec.bodies()
+    keep = []
+    for b in range(spec.num_boundaries):
+        body = bodies[b]
+        assert "mesh" not in spec.body_specs[b], "oracle_scene: analytic shapes only"
+        if body.use_distance_grid:
+            dist = orc.distance_grid(body, spec.dtype)
+            keep.append(dist)
+            body.distance_nodes = dist.ctypes.data
+        vol = orc.lazy_volume_field(spec.cn, body, spec.dtype)
+        keep.append(vol)
+        body.volume_nodes = vol.ctypes.data
+        orc.lazy_volume_touch(body, rigid[b], spec.x, dilate)
+    return bodies, keep, rigid, time.perf_counter() - t0
+
+
+def lazy_nodes_computed(keep):
+    """Volume-map nodes computed so far by the oracle's lazy maps."""
+    from oracle import binding as orc
+    return sum(sum(orc.lazy_volume_counts(a)) for a in keep)
+
+
+def release_oracle_scene(spec, keep):
+    from oracle import binding as orc
+    for a in keep:
+        orc.lazy_volume_release(a)
 
 
 TRAIN_STEPS, TRAIN_PER_STEP, FIT_STEPS = 300, 32768, 5000
@@ -290,29 +349,17 @@ def train_warm_start(engine, args, sp):
     return net, info
 
 
-def iteration_counts(engine, args, sp, steps, warm=None):
-    """Mean (divergence, density) iterations over `steps` steps of a fresh
-    copy of the benchmark scene."""
-    sc = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
-                     container_resolution=args.container_resolution)
-    dt = float(sp.max_dt)
-    its = []
-    for _ in range(steps):
-        dt, rep = sc.step(args.method, sp, dt, warm=warm)
-        its.append((rep.num_divergence_solve, rep.num_density_solve))
-    a = np.asarray(its, dtype=np.float64)
-    return [round(float(a[:, 0].mean()), 3), round(float(a[:, 1].mean()), 3)]
-
-
-def workload_name(args):
+def workload_name(args, warm_mode="plain"):
     wl = WORKLOADS[args.workload]
     name = METHOD_NAME[args.method] + " " + wl["desc"]
     if args.rigid_bodies == 0 or args.container_resolution:
         name += " [variant: %s rigid bodies, %d^3 container map]" % (
             "no" if args.rigid_bodies == 0 else "with",
             args.container_resolution or wl["container_resolution"])
-    if getattr(args, "warm_start", "plain") == "learned":
+    if warm_mode == "learned":
         name += ", learned warm start"
+    elif warm_mode == "both":
+        name += ", learned warm start (plain DFSPH beside it)"
     if getattr(args, "max_dt", None):
         name += ", max_dt %g s" % args.max_dt
     return name
@@ -370,12 +417,31 @@ def timed_steps(scene, sp, dt, steps, torch, on_step=None, method="df", flush=No
             torch.cuda.synchronize()
             total += start.elapsed_time(stop)
         reps.append((rep.num_divergence_solve, rep.num_density_solve,
-                     rep.mean_density_error, rep.num_active_boundary_pairs))
+                     rep.mean_density_error, rep.num_active_boundary_pairs,
+                     rep.mean_density_change))
     if flush is None:
         stop.record()
         torch.cuda.synchronize()
         total = start.elapsed_time(stop)
     return total, dt, reps
+
+
+def accuracy_summary(reps):
+    """Iteration counts and achieved errors of a run's steps.  reps: tuples
+    (divergence iterations, density iterations, mean density error, active
+    boundary pairs, mean density change) per step.  The density error is
+    the density solve's final mean (rho_adv - rho0) / rho0, held below the
+    0.1 % tolerance; the density change is the divergence solve's final
+    mean drho/dt / rho0 in 1/s, held below 0.1 % / dt."""
+    a = np.asarray([r[:5] for r in reps], dtype=np.float64)
+    return {"mean_divergence_iterations": round(float(a[:, 0].mean()), 3),
+            "mean_density_iterations": round(float(a[:, 1].mean()), 3),
+            "max_density_iterations": int(a[:, 1].max()),
+            "density_error_mean": float("%.4g" % a[:, 2].mean()),
+            "density_error_max": float("%.4g" % a[:, 2].max()),
+            "density_change_mean_per_s": float("%.4g" % a[:, 4].mean()),
+            "density_change_max_per_s": float("%.4g" % a[:, 4].max()),
+            "density_error_tolerance": 1e-3}
 
 
 def max_over_ranks(value, world, torch):
@@ -438,7 +504,12 @@ def cpu_baseline(scene, sp, dt, budget_s, host_state, host_bodies, method="df"):
 
 
 def batch_scene_list(engine, spec, seed=SEED):
-    """The batch workload's scenes (seeded)."""
+    """The batch workload's scenes (seeded), on the device."""
+    return [sp.device(engine) for sp in batch_scene_specs(spec, seed)]
+
+
+def batch_scene_specs(spec, seed=SEED):
+    """Host descriptions of the batch workload's scenes (seeded)."""
     from alluvion_b200 import _capi, scenes
     rng = np.random.Generator(np.random.PCG64(seed + 3000))
     r = spec["radius"]
@@ -464,8 +535,8 @@ def batch_scene_list(engine, spec, seed=SEED):
                                use_distance_grid=True, mass=mass,
                                inertia=scenes.sphere_inertia(mass, rad), x=pos))
         seed_k = int(rng.integers(0, 2 ** 31))
-        out.append(scenes.dam_break(engine, np.float32, (a, a, a), r, tuple(box), bodies,
-                                    seed=seed_k, volume_resolution=32))
+        out.append(scenes.dam_break_spec(np.float32, (a, a, a), r, tuple(box), bodies,
+                                         seed=seed_k, volume_resolution=32))
     return out
 
 
@@ -488,6 +559,12 @@ def batch_arm(args):
     if args.max_dt:
         sp.max_dt = args.max_dt
     total_n = sum(sc.n for sc in sl)
+    tuning = None
+    if args.autotune != "off":
+        from alluvion_b200 import autotune
+        t0 = time.perf_counter()
+        tuning = autotune.tune_batch(engine, sl, sp)
+        tuning["seconds"] = round(time.perf_counter() - t0, 1)
     host_state = [sc.state() for sc in sl] if rank == 0 and world == 1 else None
     host_bodies = [sc.host_bodies() for sc in sl] if host_state is not None else None
     dts = [float(sp.max_dt)] * len(sl)
@@ -554,6 +631,9 @@ def batch_arm(args):
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
                    "launch": "eager" if args.eager else "batch graph (one branch per scene)",
+                   "autotune": None if tuning is None else {
+                       k: tuning[k] for k in ("batch_ms_default", "batch_ms_tuned", "buckets",
+                                              "seconds")},
                    "graph_replays_timed": graphs1[1] - graphs0[1],
                    "mean_divergence_iterations": round(float(its[:, :, 0].mean()), 3),
                    "mean_density_iterations": round(float(its[:, :, 1].mean()), 3)},
@@ -614,6 +694,140 @@ def batch_arm(args):
         print(json.dumps(result), flush=True)
 
 
+def load_warm_net(engine, args, sp):
+    """The committed network (alluvion_b200/data/warm_start_dambreak.npz,
+    trained by alluvion_b200.train_warm_start on 200 seeded 1M-particle dam
+    breaks), or one trained now on a differently seeded scene of the
+    workload when --warm-net train."""
+    from alluvion_b200 import warm_start
+    if args.warm_net == "train":
+        return train_warm_start(engine, args, sp)
+    path = args.warm_net or os.path.join(ROOT, "alluvion_b200", "data",
+                                         "warm_start_dambreak.npz")
+    net = warm_start.WarmStartNet.load(path)
+    info = {"network": os.path.relpath(path, ROOT)}
+    ev = os.path.splitext(path)[0] + "_eval.json"
+    if os.path.exists(ev):
+        with open(ev) as f:
+            info["trained"] = json.load(f).get("training")
+    return net, info
+
+
+def time_arm(engine, scene, sp, args, warm, world, local, torch, want_e2e, clocks_on):
+    """Warm-up, the device-resident timed region, optionally the end-to-end
+    region, and a profiling pass of one arm; returns a dict."""
+    dt = float(sp.max_dt)
+    for _ in range(args.warmup):
+        dt, _ = scene.step(args.method, sp, dt, warm=warm)
+    barrier(world)
+    clocks = ClockSampler(local) if clocks_on else None
+    if clocks:
+        clocks.start()
+    launches0 = engine.launch_count()
+    graphs0 = engine.graph_stats()
+    flush = None
+    if scene.n * STEP_BYTES_PER_PARTICLE < L2_BYTES:
+        flush = torch.zeros(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch, method=args.method, flush=flush,
+                               warm=warm)
+    out = {"launches": engine.launch_count() - launches0,
+           "graph_replays": engine.graph_stats()[1] - graphs0[1],
+           "clocks": clocks.stop() if clocks else None, "flush": flush is not None}
+    barrier(world)
+    out["ms"] = max_over_ranks(ms, world, torch)
+    out["value"] = job_throughput(scene.n, world, args.steps, out["ms"])
+    out["reps"] = reps
+    if want_e2e:
+        # host copies of the step's inputs (x, v and the warm-start state) in
+        # pinned memory: uploaded before and x, v read back after every step
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        dev_in = [scene.x, scene.v] + [getattr(scene, k) for k in STATE[args.method]]
+        host_in = [pin(t.cpu().numpy()) for t in dev_in]
+        out["h2d"] = sum(t.numel() * t.element_size() for t in host_in)
+        out["d2h"] = sum(t.numel() * t.element_size() for t in host_in[:2])
+
+        def io(phase):
+            if phase == "before":
+                for d, h in zip(dev_in, host_in):
+                    d.copy_(h, non_blocking=True)
+            else:
+                for d, h in zip(dev_in[:2], host_in[:2]):
+                    h.copy_(d, non_blocking=True)
+        barrier(world)
+        ms_e2e, dt, _ = timed_steps(scene, sp, dt, args.steps, torch, on_step=io,
+                                    method=args.method, flush=flush, warm=warm)
+        barrier(world)
+        out["ms_e2e"] = max_over_ranks(ms_e2e, world, torch)
+        out["e2e"] = job_throughput(scene.n, world, args.steps, out["ms_e2e"])
+    # per-pass device times (profiling pass after the timed regions)
+    engine.reset_stats()
+    engine.set_profiling(True)
+    prof_steps = 3
+    _, dt, preps = timed_steps(scene, sp, dt, prof_steps, torch, method=args.method, warm=warm)
+    engine.set_profiling(False)
+    pass_ms = {}
+    for name, (tot, cnt) in engine.kernel_stats().items():
+        p = FINISH_PASS[args.method] if name == "finish" else GROUP_PASS.get(
+            name, "warm_start" if name.startswith("warm") else None)
+        if p:
+            pass_ms[p] = pass_ms.get(p, 0.0) + tot / prof_steps
+    out["pass_ms"] = pass_ms
+    out["iters"] = (sum(r[0] for r in preps) / prof_steps, sum(r[1] for r in preps) / prof_steps)
+    out["pairs"] = sum(r[3] for r in preps) / prof_steps
+    return out
+
+
+def fp64_error(engine, args, sp, steps):
+    """Per-quantity error of the float32 plain method against a float64 run
+    of the plain method from the same initial positions, after `steps`
+    steps: L2-relative and max-relative (of each quantity's scale)."""
+    f32 = build_scene(engine, args.workload, np.float32, args.rigid_bodies,
+                      args.container_resolution)
+    f64 = build_scene(engine, args.workload, np.float64, args.rigid_bodies,
+                      args.container_resolution)
+    f64.x.copy_(f32.x.double())
+    d32 = d64 = float(sp.max_dt)
+    for _ in range(steps):
+        d32, _ = f32.step(args.method, sp, d32)
+        d64, _ = f64.step(args.method, sp, d64)
+    a, b = f32.state(), f64.state()
+    out = {"steps": steps}
+    for k in ("x", "v", "density") + STATE[args.method]:
+        x = np.asarray(a[k], np.float64)
+        y = np.asarray(b[k], np.float64)
+        out[k] = {"l2_rel": float("%.3g" % (np.sqrt(((x - y) ** 2).sum() /
+                                                     max((y ** 2).sum(), 1e-300)))),
+                  "max_rel": float("%.3g" % (np.abs(x - y).max() /
+                                             max(np.abs(y).max(), 1e-300)))}
+    del f32, f64
+    return out
+
+
+def roofline_of(out, n, flush):
+    """Roofline of the arm's dominant pass: Model-A bytes of one launch over
+    its CUDA-event time per launch."""
+    per_launch = {}
+    for p, t in out["pass_ms"].items():
+        runs = {"div": out["iters"][0], "den": out["iters"][1]}.get(PASS_PER_STEP.get(p), 1.0)
+        if runs > 0 and p in MODEL_A:
+            per_launch[p] = t / runs
+    dominant = max((p for p in out["pass_ms"] if p in MODEL_A), key=out["pass_ms"].get)
+    peak, peak_kind = measured_peaks()
+    bpp, bpair = MODEL_A[dominant]
+    alg_bytes = bpp * n + bpair * out["pairs"]
+    achieved = alg_bytes / (per_launch[dominant] / 1e3) / 1e9
+    traffic = committed_traffic()
+    tr = None
+    # the committed figure is per particle of a working set larger than L2;
+    # it scales with the particle count only while the step stays DRAM-resident
+    if traffic and traffic.get("pass") == dominant and not flush:
+        tr = traffic.get("dram_bytes_per_particle", 0) * n
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": tr, "kernel": dominant,
+            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": int(alg_bytes),
+            "launch_ms": round(per_launch[dominant], 4)}
+
+
 def engine_arm(args):
     import torch
     from alluvion_b200 import _capi, scenes
@@ -628,134 +842,80 @@ def engine_arm(args):
     sp = scenes.solver_params()
     if args.max_dt:
         sp.max_dt = args.max_dt
-    warm, warm_info = None, None
-    if args.warm_start == "learned":
-        if args.method != "df":
-            raise SystemExit("--warm-start learned: DFSPH only")
-        net, warm_info = train_warm_start(engine, args, sp)
-        warm = net.warm_start()
-        n_cmp = args.warmup + args.steps
-        warm_info["iterations_per_step"] = {
-            "learned": iteration_counts(engine, args, sp, n_cmp, warm),
-            "plain": iteration_counts(engine, args, sp, n_cmp, None),
-            "steps": n_cmp}
+    warm_mode = args.warm_start
+    if warm_mode == "auto":
+        warm_mode = "both" if args.method == "df" and args.workload == DEFAULT_WORKLOAD \
+            else "plain"
+    if warm_mode != "plain" and args.method != "df":
+        raise SystemExit("--warm-start learned: DFSPH only")
+    net, warm_info = (None, None)
+    if warm_mode != "plain":
+        net, warm_info = load_warm_net(engine, args, sp)
     scene = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
                         container_resolution=args.container_resolution)
-    dt = float(sp.max_dt)
+    n = scene.n
     host_state = scene.state() if rank == 0 and world == 1 else None
     host_bodies = scene.host_bodies() if host_state is not None else None
-    # warm-up
-    for _ in range(args.warmup):
-        dt, _ = scene.step(args.method, sp, dt, warm=warm)
-    # ---- device-resident timed region (value)
-    barrier(world)
-    clocks = ClockSampler(local)
-    clocks.start()
-    launches0 = engine.launch_count()
-    graphs0 = engine.graph_stats()
-    flush = None
-    if scene.n * STEP_BYTES_PER_PARTICLE < L2_BYTES:
-        flush = torch.zeros(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
-    ms, dt, reps = timed_steps(scene, sp, dt, args.steps, torch, method=args.method, flush=flush,
-                               warm=warm)
-    launches = engine.launch_count() - launches0
-    graphs1 = engine.graph_stats()
-    clk = clocks.stop()
-    barrier(world)
-    ms = max_over_ranks(ms, world, torch)
-    total_particles = scene.n * world
-    value = job_throughput(scene.n, world, args.steps, ms)
-    # ---- end to end: host buffers in pinned memory, H2D + step + D2H per step
-    n = scene.n
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    # host copies of the step's inputs (x, v and the warm-start state) in
-    # pinned memory: uploaded before and x, v read back after every step
-    dev_in = [scene.x, scene.v] + [getattr(scene, k) for k in STATE[args.method]]
-    host_in = [pin(t.cpu().numpy()) for t in dev_in]
-    h2d = sum(t.numel() * t.element_size() for t in host_in)
-    d2h = sum(t.numel() * t.element_size() for t in host_in[:2])
-
-    def io(phase):
-        if phase == "before":
-            for d, h in zip(dev_in, host_in):
-                d.copy_(h, non_blocking=True)
-        else:
-            for d, h in zip(dev_in[:2], host_in[:2]):
-                h.copy_(d, non_blocking=True)
-    barrier(world)
-    ms_e2e, dt, _ = timed_steps(scene, sp, dt, args.steps, torch, on_step=io,
-                                method=args.method, flush=flush, warm=warm)
-    barrier(world)
-    ms_e2e = max_over_ranks(ms_e2e, world, torch)
-    e2e = job_throughput(scene.n, world, args.steps, ms_e2e)
-    # ---- per-pass device times (profiling pass after the timed region)
-    engine.reset_stats()
-    engine.set_profiling(True)
-    prof_steps = 3
-    _, dt, preps = timed_steps(scene, sp, dt, prof_steps, torch, method=args.method, warm=warm)
-    engine.set_profiling(False)
-    stats = engine.kernel_stats()
-    iters_div = sum(r[0] for r in preps) / prof_steps
-    iters_den = sum(r[1] for r in preps) / prof_steps
-    pairs = sum(r[3] for r in preps) / prof_steps
-    pass_ms = {}
-    for name, (tot, cnt) in stats.items():
-        p = FINISH_PASS[args.method] if name == "finish" else GROUP_PASS.get(name)
-        if p:
-            pass_ms[p] = pass_ms.get(p, 0.0) + tot / prof_steps
-    per_launch = {}
-    for p, t in pass_ms.items():
-        runs = {"div": iters_div, "den": iters_den}.get(PASS_PER_STEP.get(p), 1.0)
-        if runs > 0:
-            per_launch[p] = t / runs
-    dominant = max(pass_ms, key=pass_ms.get)
-    peak, peak_kind = measured_peaks()
-    bpp, bpair = MODEL_A[dominant]
-    alg_bytes = bpp * n + bpair * pairs
-    achieved = alg_bytes / (per_launch[dominant] / 1e3) / 1e9
-    traffic = committed_traffic()
-    tr = None
-    # the committed figure is per particle of a working set larger than L2;
-    # it scales with the particle count only while the step stays DRAM-resident
-    if traffic and traffic.get("pass") == dominant and flush is None:
-        tr = traffic.get("dram_bytes_per_particle", 0) * n
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": tr,
-                "kernel": dominant, "peak_kind": peak_kind,
-                "algorithmic_bytes_per_launch": int(alg_bytes),
-                "launch_ms": round(per_launch[dominant], 4)}
-    steps_reps = reps
-    workload = workload_name(args)
+    tuning = None
+    if args.autotune == "on":
+        from alluvion_b200 import autotune
+        t0 = time.perf_counter()
+        tuning = autotune.tune_scene(engine, scene, sp, method=args.method)
+        tuning["seconds"] = round(time.perf_counter() - t0, 1)
+    snap = scene.snapshot()
+    arms = ([("plain", None)] if warm_mode in ("plain", "both") else []) + \
+           ([("learned", net.warm_start())] if warm_mode in ("learned", "both") else [])
+    primary = arms[-1][0]
+    res = {}
+    for name, warm in arms:
+        scene.restore(snap)
+        res[name] = time_arm(engine, scene, sp, args, warm, world, local, torch,
+                             want_e2e=name == primary, clocks_on=name == primary)
+    main_ = res[primary]
+    roofline = roofline_of(main_, n, main_["flush"])
     bodies_desc = ", seeded rigid bodies" if scene.num_boundaries > 1 else ""
-    l2 = ("working set > 126 MB L2 (inputs larger than L2, no flush)" if flush is None else
+    l2 = ("working set > 126 MB L2 (inputs larger than L2, no flush)" if not main_["flush"] else
           "working set < L2: a 252 MB buffer is rewritten before every timed step (untimed)")
+    config = {"workload": workload_name(args, warm_mode), "particles_per_gpu": n,
+              "global_particles": n * world,
+              "parallelism": "replicas" if world > 1 else "single", "l2": l2,
+              **accuracy_summary(main_["reps"]),
+              "active_boundary_pairs": int(main_["pairs"]),
+              "launch": "eager" if args.eager else "step graph (conditional WHILE loops)",
+              "max_dt": float(sp.max_dt), "warm_start": primary,
+              "graph_replays_timed": main_["graph_replays"],
+              "pass_ms_per_step": {k: round(v, 4) for k, v in main_["pass_ms"].items()}}
+    if warm_info is not None:
+        arm_rows = {}
+        for name, r in res.items():
+            arm_rows[name] = dict({"value": round(r["value"], 1),
+                                   "ms_per_step": round(r["ms"] / args.steps, 4)},
+                                  **accuracy_summary(r["reps"]))
+        warm_info["arms"] = arm_rows
+        warm_info["gate"] = ("the network runs on a scene's first step and after every step "
+                             "whose solves went beyond their minimum iteration counts; after "
+                             "a step at the minimum counts no warm start can save an iteration, "
+                             "so it is skipped (plain warm start)")
+        config["learned_warm_start"] = warm_info
+    if tuning is not None:
+        config["autotune"] = {"seconds": tuning["seconds"], "shapes": {
+            e["group"]: [e["block"], e["tpp"]] for e in tuning["entries"]}}
+    if args.fp64_steps and rank == 0:
+        config["error_vs_fp64_plain"] = fp64_error(engine, args, sp, args.fp64_steps)
     result = {
-        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "metric": METRIC, "value": round(main_["value"], 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(main_["ms"] / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded jittered lattice%s)" % bodies_desc,
-        "config": {"workload": workload, "particles_per_gpu": n, "global_particles":
-                   total_particles, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": l2,
-                   "mean_divergence_iterations": round(sum(r[0] for r in steps_reps) /
-                                                       len(steps_reps), 3),
-                   "mean_density_iterations": round(sum(r[1] for r in steps_reps) /
-                                                    len(steps_reps), 3),
-                   "active_boundary_pairs": int(pairs),
-                   "launch": "eager" if args.eager else "step graph (conditional WHILE loops)",
-                   "max_dt": float(sp.max_dt),
-                   "warm_start": args.warm_start,
-                   "graph_replays_timed": graphs1[1] - graphs0[1],
-                   "pass_ms_per_step": {k: round(v, 4) for k, v in pass_ms.items()}},
-        "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(launches),
+        "config": config,
+        "e2e": {"value": round(main_["e2e"], 1), "unit": UNIT,
+                "h2d_bytes_per_step": main_["h2d"], "d2h_bytes_per_step": main_["d2h"]},
+        "gpu_launches": int(main_["launches"]),
         "roofline": roofline,
-        "clocks": clk,
+        "clocks": main_["clocks"],
     }
-    if warm_info is not None:
-        result["config"]["learned_warm_start"] = warm_info
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and warm is None:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(scene, sp, float(sp.max_dt), args.cpu_seconds,
                                               host_state, host_bodies, args.method)
     if world > 1:
@@ -766,91 +926,137 @@ def engine_arm(args):
         print(json.dumps(result), flush=True)
 
 
-def reference_batch(args, engine):
+def reference_batch(args):
     """Reference arm of a batch workload: the oracle port advances every
     scene of the batch by one step per benchmark step (scenes in turn, all
-    host cores)."""
+    host cores), on grids the oracle builds."""
     from alluvion_b200 import scenes
     from oracle import binding as orc
     spec = BATCH_WORKLOADS[args.workload]
-    sl = batch_scene_list(engine, spec)  # setup: grids built on the device, untimed
+    specs = batch_scene_specs(spec)
     sp = scenes.solver_params()
     items = []
-    for sc in sl:
-        hb, keep, rigid = sc.host_bodies()
-        nb = sc.num_boundaries
-        bodies = (type(hb[0]) * nb)(*[hb[b] for b in range(nb)])
-        items.append([sc, bodies, keep, rigid, oracle_state(sc.state(), "df"), float(sp.max_dt)])
-    total_n = sum(sc.n for sc in sl)
-    steps = max(1, min(args.steps, 2))
-    t0 = time.perf_counter()
-    for _ in range(steps):
+    setup_s = 0.0
+    for sc in specs:
+        bodies, keep, rigid, t = oracle_scene(sc)
+        setup_s += t
+        items.append([sc, bodies, keep, rigid, zero_state(sc, "df"), float(sp.max_dt)])
+    total_n = sum(sc.n for sc in specs)
+    reps = []
+    el = 0.0
+    steps = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
         for it in items:
             sc, bodies, _, rigid, state, dt = it
-            it[5], _ = orc.run("df", sc.cn, sc.cni, bodies, rigid, state, sp, dt, 1)
-    el = time.perf_counter() - t0
+            it[5], r = orc.run("df", sc.cn, sc.cni, bodies, rigid, state, sp, dt, 1)
+            reps += r
+        el += time.perf_counter() - t0
+        steps += 1
+        if el * (steps + 1) / steps > REFERENCE_SECONDS:
+            break
+    for it in items:
+        release_oracle_scene(it[0], it[2])
     value = total_n * steps / el
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
         "n_gpus": 1, "steps": steps, "warmup": 0, "ms_per_step": round(el * 1e3 / steps, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded jittered lattices, seeded rigid spheres)",
-        "config": {"workload": "DFSPH " + spec["desc"], "particles_per_gpu": total_n},
+        "config": dict({"workload": "DFSPH " + spec["desc"], "particles_per_gpu": total_n,
+                        "grids": "built by the oracle on the host cores (untimed, %.1f s)"
+                                 % setup_s},
+                       **accuracy_summary([(r.num_divergence_solve, r.num_density_solve,
+                                            r.mean_density_error, r.num_active_boundary_pairs,
+                                            r.mean_density_change) for r in reps])),
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": orc.num_threads(),
                          "kind": "port",
-                         "sample": "%d step(s) of all %d scenes" % (steps, len(sl))},
+                         "sample": "%d step(s) of all %d scenes" % (steps, len(specs))},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+REFERENCE_SECONDS = 150.0
+
+
+def zero_state(spec, method):
+    n, T = spec.n, spec.dtype
+    st = {"x": np.ascontiguousarray(spec.x).copy(), "v": np.zeros((n, 3), T),
+          "density": np.zeros(n, T), "density_adv": np.zeros(n, T), "a": np.zeros((n, 3), T)}
+    for k in STATE[method]:
+        st[k] = np.zeros(n, T)
+    return st
 
 
 def reference_arm(args):
     """The reference's CPU formulation of the path (the oracle port: the
     reference itself needs Eigen/GLFW/glm and does not build here), timed on
-    all host cores.  Rank 0 only."""
+    all host cores.  Nothing here loads the engine: grids are built by the
+    oracle.  Rank 0 only."""
     world, rank, local = dist_env()
     if rank != 0:
         return
-    import torch
-    from alluvion_b200 import _capi, scenes
+    from alluvion_b200 import scenes
     from oracle import binding as orc
-    torch.cuda.set_device(local)
-    engine = _capi.Engine(local)
     if args.workload in BATCH_WORKLOADS:
-        return reference_batch(args, engine)
-    # setup only: grids built on the device, untimed
-    scene = build_scene(engine, args.workload, rigid_bodies=args.rigid_bodies,
-                        container_resolution=args.container_resolution)
-    hb, keep, rigid = scene.host_bodies()
-    nb = scene.num_boundaries
-    bodies = (type(hb[0]) * nb)(*[hb[b] for b in range(nb)])
-    state = oracle_state(scene.state(), args.method)
+        return reference_batch(args)
+    spec = build_scene_spec(args.workload, rigid_bodies=args.rigid_bodies,
+                            container_resolution=args.container_resolution)
+    bodies, keep, rigid, setup_s = oracle_scene(spec)
+    nodes_setup = lazy_nodes_computed(keep)
+    state = zero_state(spec, args.method)
     sp = scenes.solver_params()
+    if args.max_dt:
+        sp.max_dt = args.max_dt
     dt = float(sp.max_dt)
-    # each benchmark step is one full oracle step; warm-up steps are shortened
-    # to one so the run stays within minutes
-    for _ in range(min(args.warmup, 1)):
-        dt, _ = orc.run(args.method, scene.cn, scene.cni, bodies, rigid, state, sp, dt, 1)
-    steps = max(1, min(args.steps, 5))
-    t0 = time.perf_counter()
-    dt, _ = orc.run(args.method, scene.cn, scene.cni, bodies, rigid, state, sp, dt, steps)
-    el = time.perf_counter() - t0
-    value = scene.n * steps / el
+    t_w = time.perf_counter()
+    warm = 0
+    for _ in range(args.warmup):
+        dt, _ = orc.run(args.method, spec.cn, spec.cni, bodies, rigid, state, sp, dt, 1)
+        warm += 1
+        if time.perf_counter() - t_w > 0.25 * REFERENCE_SECONDS:
+            break
+    nodes_before = lazy_nodes_computed(keep)
+    reps = []
+    el = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        dt, r = orc.run(args.method, spec.cn, spec.cni, bodies, rigid, state, sp, dt, 1)
+        el += time.perf_counter() - t0
+        reps += r
+        if el * (len(reps) + 1) / len(reps) > REFERENCE_SECONDS:
+            break
+    steps = len(reps)
+    nodes_timed = lazy_nodes_computed(keep) - nodes_before
+    release_oracle_scene(spec, keep)
+    value = spec.n * steps / el
+    sample = "%d full steps of the %s-particle scene after %d warm-up step(s)" % (
+        steps, format(spec.n, ","), warm)
+    if steps < args.steps:
+        sample += " (%d requested; stopped at the %.0f s budget)" % (args.steps,
+                                                                    REFERENCE_SECONDS)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
-        "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1),
+        "n_gpus": world, "steps": steps, "warmup": warm,
         "ms_per_step": round(el * 1e3 / steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded jittered lattice%s)" % (
-            ", seeded rigid bodies" if scene.num_boundaries > 1 else ""),
-        "config": {"workload": workload_name(args), "particles_per_gpu": scene.n},
+            ", seeded rigid bodies" if spec.num_boundaries > 1 else ""),
+        "config": dict({"workload": workload_name(args), "particles_per_gpu": spec.n,
+                        "grids": "built by the oracle on the host cores (untimed, %.1f s): "
+                                 "analytic distance nodes, lazily filled volume maps; %d volume "
+                                 "nodes computed before the timed steps, %d during them"
+                                 % (setup_s, nodes_before, nodes_timed)},
+                       **accuracy_summary([(r.num_divergence_solve, r.num_density_solve,
+                                            r.mean_density_error, r.num_active_boundary_pairs,
+                                            r.mean_density_change) for r in reps])),
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": orc.num_threads(),
-                         "kind": "port",
-                         "sample": "%d full steps of the %s-particle scene" % (
-                             steps, format(scene.n, ","))},
+                         "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
+    del nodes_setup
 
 
 def postproc_inputs(spec, name, torch, device):

@@ -274,6 +274,31 @@ AL_API int al_engine_set_graph_mode(al_engine* engine, int enable);
 /* Number of step graphs captured and of steps run by replaying one. */
 AL_API int al_engine_graph_stats(al_engine* engine, uint64_t* captures, uint64_t* replays);
 
+/* Launch shapes of the step's tunable pass groups, the counterpart of the
+ * reference's per-kernel block sizes (Runner::optimal_block_size_dict loaded
+ * from .alcache, runner.hpp:4922-4937, found by bin/block_scan:15-36).  A
+ * shape applies to scenes of 2^bucket <= N < 2^(bucket+1) particles, in
+ * single steps (batch = 0) or as a scene of al_df_batch_step_f32 (batch =
+ * 1): `block` threads per block (64, 128 or 256) and, for the pair passes
+ * that walk neighbor lists, `tpp` threads per particle (1, 2, 4 or 8; the
+ * group's lanes split the list and combine partial sums in a fixed order,
+ * so float results depend on tpp in the last bits).  0 keeps a field's
+ * default (128-thread blocks; tpp 1 from 2^17 particles up, else the
+ * smallest of 2, 4, 8 that gives 2^17 threads); 0 / 0 removes the entry.
+ * Setting a shape drops the engine's captured step graphs.  Group names are
+ * enumerated by al_tunable_group ("finish" is the acceleration and
+ * integration pass of IISPH and implicit SPH).  No reference counterpart
+ * for tpp. */
+AL_API int al_engine_set_launch_shape(al_engine* engine, const char* group, uint32_t bucket,
+                                      uint32_t batch, uint32_t block, uint32_t tpp);
+/* The shape a step of `num_particles` particles would use for `group`. */
+AL_API int al_engine_get_launch_shape(al_engine* engine, const char* group,
+                                      uint32_t num_particles, uint32_t batch, uint32_t* block,
+                                      uint32_t* tpp);
+/* Name of tunable group `index` (static storage) and whether it is a pair
+ * pass; AL_ERR_INVALID past the last group. */
+AL_API int al_tunable_group(uint32_t index, const char** name, uint32_t* pair);
+
 /* Launch statistics, the counterpart of Runner's per-kernel event timing
  * (launch_stat_dict_, runner.hpp:4835-4859, 6306-6308).  While profiling
  * is on, every launch group is bracketed with CUDA events on its stream and
@@ -318,18 +343,18 @@ AL_API int al_grid_sort_f64(al_engine* engine, const al_const_f64* cn,
                      uint32_t* pid_length, void* stream);
 
 /* The grid sort of al_grid_sort_f32 for callers that must not let the
- * library allocate device memory (a host capturing its frame into a CUDA
- * graph, a renderer or game engine that owns the memory budget, a real-time
- * loop avoiding allocation stalls).  No counterpart in the reference.
- * Allocates nothing: all scratch is one static device array of 12.6 MiB
- * that every GPU loading the library keeps until exit.  Limits: at most
- * 1,048,576 particles and 1,048,576 grid cells; larger problems return
- * AL_ERR_INVALID.  Uses the current device.  Its first call on a device
- * looks up the array's device address, so make that first call before any
- * stream capture.  Calls share the array: calls that overlap on the GPU
- * race, so order them.  Synchronises `stream` before returning (it reads
- * the anomaly flags); returns AL_ERR_OUT_OF_GRID / AL_ERR_CELL_OVERFLOW
- * like al_grid_sort_f32. */
+ * library allocate device memory (a renderer or game engine that owns the
+ * memory budget, a real-time loop avoiding the stalls of cudaMalloc /
+ * cudaFree).  No counterpart in the reference.  Allocates nothing: all
+ * scratch is one static device array of 12.6 MiB, resident on a device
+ * from the first call there (CUDA loads the library's device image lazily)
+ * until the process exits.  Limits: at most 1,048,576 particles and
+ * 1,048,576 grid cells; larger problems return AL_ERR_INVALID.  Uses the
+ * current device.  Its first call on a device looks up the array's device
+ * address, so make that first call before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race, so order them.
+ * Synchronises `stream` before returning (it reads the anomaly flags);
+ * returns AL_ERR_OUT_OF_GRID / AL_ERR_CELL_OVERFLOW like al_grid_sort_f32. */
 AL_API int al_grid_sort_noalloc_f32(const al_const_f32* cn, const al_consti* cni,
                                     const float* particle_x, uint32_t num_particles,
                                     uint32_t* particle_cell, uint32_t* sorted_to_original,

@@ -915,7 +915,12 @@ class Solver {
     t = 0;
     dt = initial_dt;
   }
-  // Solver::compute_all_boundaries (solver.hpp:170-185).
+  // Solver::compute_all_boundaries (solver.hpp:170-185).  Rows of
+  // particle_boundary / particle_boundary_kernel are num_particles long:
+  // body b's entries start at b * num_particles (the reference indexes them
+  // with the variable's max_num_particles stride; the two agree while
+  // num_particles == max_num_particles, and update_particle_neighbors and
+  // the steps read the rows with the same num_particles stride).
   void compute_all_boundaries() {
     check_counts();
     const auto bodies = pile.bodies();
@@ -937,6 +942,16 @@ class Solver {
         sample_boundary.get_num_primitives() < need ||
         sample_boundary_kernel.get_num_primitives() < need)
       throw error(AL_ERR_INVALID, "Solver::sample_all_boundaries: variables too small");
+    // the rows are written num_samples apart; a [num_bodies][capacity]
+    // variable with capacity != num_samples would be indexed with another
+    // stride by the reference's Variable<2> (variable.hpp:281-290)
+    for (const Variable* v : {&sample_boundary, &sample_boundary_kernel}) {
+      const auto& sh = v->get_shape();
+      if (sh.size() == 2 && sh[1] != num_samples)
+        throw error(AL_ERR_INVALID,
+                    "Solver::sample_all_boundaries: sample_boundary variables must have shape "
+                    "[num_bodies][num_samples]");
+    }
     const auto bodies = pile.bodies();
     const auto rig = pile.rigid();
     check(real<TF>::compute_particle_boundary(

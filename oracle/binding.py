@@ -38,6 +38,7 @@ def lib():
             "orc_histogram256_f64": (None, [_P, _P, _U, ctypes.c_double, ctypes.c_double, _P]),
             "orc_kl_divergence": (ctypes.c_double, [_P, _P, _U, _U, ctypes.c_double, _U]),
             "orc_relax_pellets_f32": (ctypes.c_int, [_P, _P, _P, _P, _U, _P, _U, _P, _P]),
+            "orc_lazy_volume_release": (None, [_P]),
         }
         for s in ("f32", "f64"):
             sig["orc_grid_sort_" + s] = (ctypes.c_int, [_P, _P, _P, _U, _P, _P, _P, _P])
@@ -48,6 +49,9 @@ def lib():
             sig["orc_node_positions_" + s] = (None, [_P, _P, _P, _P])
             sig["orc_distance_grid_" + s] = (None, [_P, _P])
             sig["orc_volume_field_" + s] = (None, [_P, _P, _P])
+            sig["orc_lazy_volume_register_" + s] = (None, [_P, _P, _P])
+            sig["orc_lazy_volume_counts_" + s] = (None, [_P, _P])
+            sig["orc_lazy_volume_touch_" + s] = (None, [_P, _P, _P, _U, _U])
             sig["orc_boundary_" + s] = (None, [_P, _P, _P, _U, _P, _U, _P, _P])
             # cn, cni, bodies, rigid, n, x, v, kappa, kappa_v, density, density_adv, a,
             # params, dt, steps, reports (IISPH: pressure instead of kappa, kappa_v)
@@ -169,6 +173,36 @@ def volume_field(cn, body, dtype):
     out = np.zeros(body.num_nodes, dtype)
     getattr(lib(), "orc_volume_field_" + _sfx(dtype))(_p(cn), _p(body), _p(out))
     return out
+
+
+def lazy_volume_field(cn, body, dtype):
+    """A volume map whose nodes the oracle computes on first use (same values
+    as volume_field at every node it reads).  Point body.volume_nodes at the
+    returned array; body.distance_nodes (HOST) must outlive it.  Release
+    with lazy_volume_release."""
+    out = np.zeros(body.num_nodes, dtype)
+    getattr(lib(), "orc_lazy_volume_register_" + _sfx(dtype))(_p(cn), _p(body), _p(out))
+    return out
+
+
+def lazy_volume_counts(out):
+    """(nodes computed by sampling, nodes set by the analytic shortcuts)."""
+    c = np.zeros(2, np.uint64)
+    getattr(lib(), "orc_lazy_volume_counts_" + _sfx(out.dtype))(_p(out), _p(c))
+    return int(c[0]), int(c[1])
+
+
+def lazy_volume_touch(body, rigid_row, x, dilate=1):
+    """Computes now the lazy map's nodes that particles x (n, 3), within
+    `dilate` cells, will read; body.volume_nodes must be a lazy map."""
+    x = np.ascontiguousarray(x)
+    r = np.ascontiguousarray(rigid_row, x.dtype)
+    getattr(lib(), "orc_lazy_volume_touch_" + _sfx(x.dtype))(_p(body), _p(r), _p(x), x.shape[0],
+                                                             int(dilate))
+
+
+def lazy_volume_release(out):
+    lib().orc_lazy_volume_release(_p(out))
 
 
 def boundary(cn, bodies, rigid, x):

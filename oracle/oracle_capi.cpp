@@ -7,6 +7,9 @@
 #include <omp.h>
 
 #include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "sph_oracle.hpp"
@@ -18,6 +21,22 @@ namespace {
 template <class TF>
 V3<TF> v3(const TF* p) {
   return V3<TF>{p[0], p[1], p[2]};
+}
+
+// Lazily filled volume maps, keyed by their node array (see LazyVolume).
+template <class TF>
+std::map<const void*, std::unique_ptr<LazyVolume<TF>>>& lazy_registry() {
+  static std::map<const void*, std::unique_ptr<LazyVolume<TF>>> reg;
+  return reg;
+}
+std::mutex g_lazy_mutex;
+
+template <class TF>
+LazyVolume<TF>* find_lazy(const void* nodes) {
+  std::lock_guard<std::mutex> lock(g_lazy_mutex);
+  auto& reg = lazy_registry<TF>();
+  auto it = reg.find(nodes);
+  return it == reg.end() ? nullptr : it->second.get();
 }
 
 template <class TF, class B>
@@ -33,6 +52,7 @@ Body<TF> make_body(const B& b, const TF* rigid) {
   o.num_nodes = b.num_nodes;
   o.dist_nodes = b.distance_nodes;
   o.vol_nodes = b.volume_nodes;
+  o.lazy_vol = find_lazy<TF>(b.volume_nodes);
   o.sdf.kind = b.shape;
   for (int k = 0; k < 8; ++k) o.sdf.p[k] = b.shape_params[k];
   o.max_distance = b.max_distance;
@@ -139,6 +159,62 @@ void distance_grid_impl(const B* b, TF* out) {
 #pragma omp parallel for schedule(static)
   for (int64_t l = 0; l < int64_t(body.num_nodes); ++l)
     out[l] = body.sdf.sdf(node_position(body.dmin, body.res, body.cs, uint32_t(l)));
+}
+
+template <class TF, class C, class B>
+void lazy_register_impl(const C* cn, const B* b, TF* out) {
+  Cn<TF> c = make_cn<TF>(*cn);
+  B geo = *b;
+  geo.volume_nodes = nullptr;  // not a lazy map itself
+  Body<TF> body = make_body<TF>(geo, nullptr);
+  auto lv = std::make_unique<LazyVolume<TF>>(c, body.dmin, body.dmax, body.cs, body.res,
+                                             body.use_grid, body.sign, body.sdf,
+                                             body.dist_nodes, out);
+  std::lock_guard<std::mutex> lock(g_lazy_mutex);
+  lazy_registry<TF>()[out] = std::move(lv);
+}
+
+// Computes every node of the Lagrange cells within `dilate` cells of each
+// particle's cell in the body's frame (the nodes the next steps' boundary
+// samples read), so that a timed run afterwards finds them ready.
+template <class TF, class B>
+void lazy_touch_impl(const B* b, const TF* rigid, const TF* x, uint32_t n, uint32_t dilate) {
+  LazyVolume<TF>* lv = find_lazy<TF>(b->volume_nodes);
+  if (!lv) return;
+  const Body<TF> body = make_body<TF>(*b, rigid);
+  const int d = int(dilate);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t i = 0; i < int64_t(n); ++i) {
+    V3<TF> local = rotate(v3<TF>(x + 3 * i) - body.x, conjugate(body.q));
+    if (body.shape == AL_SHAPE_INFINITE_CYLINDER || body.shape == AL_SHAPE_INFINITE_TUBE)
+      local.y = 0;
+    // cell of the particle in the body's grid, possibly outside it: particles
+    // up to `dilate` cells outside the domain may move in
+    const V3<TF> rel = local - body.dmin;
+    const TF fx = std::floor(rel.x / body.cs.x), fy = std::floor(rel.y / body.cs.y),
+             fz = std::floor(rel.z / body.cs.z);
+    const TF lim = TF(1 << 20);
+    if (!(std::fabs(fx) < lim && std::fabs(fy) < lim && std::fabs(fz) < lim)) continue;
+    const int ip[3] = {int(fx), int(fy), int(fz)};
+    for (int a = -d; a <= d; ++a)
+      for (int bb = -d; bb <= d; ++bb)
+        for (int cc = -d; cc <= d; ++cc) {
+          int q[3] = {ip[0] + a, ip[1] + bb, ip[2] + cc};
+          if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= int(body.res[0]) ||
+              q[1] >= int(body.res[1]) || q[2] >= int(body.res[2]))
+            continue;
+          uint32_t cells[32];
+          cell_nodes(body.res, q, cells);
+          for (int j = 0; j < 32; ++j) lv->get(cells[j]);
+        }
+  }
+}
+
+template <class TF>
+void lazy_counts_impl(const TF* out, uint64_t counts[2]) {
+  LazyVolume<TF>* lv = find_lazy<TF>(out);
+  counts[0] = lv ? lv->sampled.load() : 0;
+  counts[1] = lv ? lv->skipped.load() : 0;
 }
 
 template <class TF, class C, class B>
@@ -407,6 +483,35 @@ void orc_volume_field_f32(const al_const_f32* cn, const al_body_f32* b, float* o
 }
 void orc_volume_field_f64(const al_const_f64* cn, const al_body_f64* b, double* out) {
   volume_field_impl<double>(cn, b, out);
+}
+// Registers `out` (the body's num_nodes volume values) as a lazily filled
+// volume map: steps that get a body whose volume_nodes == out compute each
+// node on first use.  distance_nodes must stay valid while registered.
+void orc_lazy_volume_register_f32(const al_const_f32* cn, const al_body_f32* b, float* out) {
+  lazy_register_impl<float>(cn, b, out);
+}
+void orc_lazy_volume_register_f64(const al_const_f64* cn, const al_body_f64* b, double* out) {
+  lazy_register_impl<double>(cn, b, out);
+}
+// Nodes computed so far: [0] by sampling, [1] by the analytic shortcuts.
+void orc_lazy_volume_counts_f32(const float* out, uint64_t counts[2]) {
+  lazy_counts_impl<float>(out, counts);
+}
+void orc_lazy_volume_counts_f64(const double* out, uint64_t counts[2]) {
+  lazy_counts_impl<double>(out, counts);
+}
+void orc_lazy_volume_touch_f32(const al_body_f32* b, const float* rigid, const float* x,
+                               uint32_t n, uint32_t dilate) {
+  lazy_touch_impl<float>(b, rigid, x, n, dilate);
+}
+void orc_lazy_volume_touch_f64(const al_body_f64* b, const double* rigid, const double* x,
+                               uint32_t n, uint32_t dilate) {
+  lazy_touch_impl<double>(b, rigid, x, n, dilate);
+}
+void orc_lazy_volume_release(const void* out) {
+  std::lock_guard<std::mutex> lock(g_lazy_mutex);
+  lazy_registry<float>().erase(out);
+  lazy_registry<double>().erase(out);
 }
 
 void orc_boundary_f32(const al_const_f32* cn, const al_body_f32* bodies, const float* rigid,

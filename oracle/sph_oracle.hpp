@@ -21,6 +21,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -642,6 +643,72 @@ TF volume_at(const Cn<TF>& c, const PeirceTables& pt, V3<TF> x, TF sign, Phi phi
   return TF(sum * double(c.h2) * double(c.h));
 }
 
+// A volume map whose node values are computed on first use, each by the
+// same volume_at() as the eager build (so every value read is the one the
+// eager build writes, bit for bit).  A step reads the map only at the 32
+// nodes of the Lagrange cells that hold particles; building the whole map
+// on the host (1.9 M nodes x 27,000 samples at 64^3) would take far longer
+// than the steps it serves.  For analytic distances (exact, 1-Lipschitz
+// SDFs) two node classes need no sampling: a node at least 2h (plus
+// rounding slack) outside the body has every sample point at d > h, where
+// W = 0, so its value is exactly 0; a node at least h inside has every
+// sample at d <= 0, so its value is the all-ones sum, computed once with
+// the same loop.  Concurrent first uses of one node compute the same bits.
+template <class TF>
+struct LazyVolume {
+  Cn<TF> c;
+  PeirceTables pt;
+  V3<TF> dmin, dmax, cs;
+  uint32_t res[3];
+  uint32_t num_nodes;
+  uint32_t use_grid;
+  TF sign;
+  Shape<TF> sdf;
+  const TF* dist_nodes;
+  TF* values;
+  std::vector<std::atomic<uint8_t>> done;
+  std::atomic<uint64_t> sampled{0}, skipped{0};
+  TF full = 0;
+
+  LazyVolume(const Cn<TF>& c_, V3<TF> dmin_, V3<TF> dmax_, V3<TF> cs_, const uint32_t r[3],
+             uint32_t use_grid_, TF sign_, const Shape<TF>& sdf_, const TF* dist, TF* out)
+      : c(c_), pt(peirce_tables()), dmin(dmin_), dmax(dmax_), cs(cs_),
+        num_nodes(num_grid_nodes(r)), use_grid(use_grid_), sign(sign_), sdf(sdf_),
+        dist_nodes(dist), values(out), done(num_grid_nodes(r)) {
+    for (int k = 0; k < 3; ++k) res[k] = r[k];
+    for (auto& d : done) d.store(0, std::memory_order_relaxed);
+    const TF big = std::numeric_limits<TF>::max() / TF(4);
+    full = volume_at(c, pt, V3<TF>{0, 0, 0}, sign, [&](V3<TF>) { return -sign * big; });
+  }
+  // Value of node l; `skip` tells whether a shortcut gave it.
+  TF compute(uint32_t l, bool& skip) {
+    const V3<TF> x = node_position(dmin, res, cs, l);
+    skip = false;
+    if (use_grid) {
+      const LagrangeGrid<TF> grid{dmin, dmax, cs, {res[0], res[1], res[2]}, dist_nodes};
+      return volume_at(c, pt, x, sign, [&](V3<TF> p) { return grid.value(p); });
+    }
+    const TF d0 = sdf.sdf(x) * sign;
+    const TF mag = std::max(std::fabs(x.x), std::max(std::fabs(x.y), std::fabs(x.z))) + c.h;
+    const TF slack = TF(1e-3) * c.h + TF(64) * std::numeric_limits<TF>::epsilon() * mag;
+    skip = true;
+    if (d0 >= TF(2) * c.h + slack) return TF(0);
+    if (d0 <= -(c.h + slack)) return full;
+    skip = false;
+    return volume_at(c, pt, x, sign, [&](V3<TF> p) { return sdf.sdf(p); });
+  }
+  TF get(uint32_t l) {
+    if (done[l].load(std::memory_order_acquire)) return values[l];
+    bool skip;
+    const TF v = compute(l, skip);
+    __atomic_store(&values[l], &v, __ATOMIC_RELAXED);
+    uint8_t expected = 0;
+    if (done[l].compare_exchange_strong(expected, 1, std::memory_order_acq_rel))
+      (skip ? skipped : sampled).fetch_add(1, std::memory_order_relaxed);
+    return v;
+  }
+};
+
 // ------------------------------------------------------------------ bodies
 template <class TF>
 struct Body {
@@ -652,12 +719,14 @@ struct Body {
   uint32_t num_nodes;
   const TF* dist_nodes;
   const TF* vol_nodes;
+  LazyVolume<TF>* lazy_vol = nullptr;  // when set, vol_nodes fill on first use
   Shape<TF> sdf;
   TF max_distance, mass;
   V3<TF> inertia;
   // kinematics (pile.hpp:103-110)
   V3<TF> x, v, omega;
   V4<TF> q;
+  TF vol(uint32_t l) const { return lazy_vol ? lazy_vol->get(l) : vol_nodes[l]; }
 };
 
 // Boundary sample of one particle against one body:
@@ -698,7 +767,7 @@ void boundary_sample(const Cn<TF>& c, const Body<TF>& b, V3<TF> x, V4<TF>& bnd, 
       nrm = (nl2 > 0 ? inv_sqrt(nl2) : TF(0)) * nrm;
       xi_bxj = d * nrm;
       bx = x - xi_bxj;
-      for (int j = 0; j < 32; ++j) vol += b.vol_nodes[cells[j]] * N[j];
+      for (int j = 0; j < 32; ++j) vol += b.vol(cells[j]) * N[j];
     }
   } else {
     d = b.sdf.sdf(local) * b.sign;
@@ -710,7 +779,7 @@ void boundary_sample(const Cn<TF>& c, const Body<TF>& b, V3<TF> x, V4<TF>& bnd, 
     if (inside) {
       shape_functions<TF>(xi, N, nullptr, nullptr, nullptr);
       cell_nodes(b.res, ip, cells);
-      for (int j = 0; j < 32; ++j) vol += b.vol_nodes[cells[j]] * N[j];
+      for (int j = 0; j < 32; ++j) vol += b.vol(cells[j]) * N[j];
     }
   }
   V3<TF> kg = gradW(c, xi_bxj);

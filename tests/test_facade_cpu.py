@@ -131,3 +131,34 @@ int main() {
     assert int(out[0]) == (0 if torch.cuda.is_available() else 8)
     assert float(out[1]) == pytest.approx(0.31)
     assert float(out[2]) == pytest.approx(1e-6)
+
+
+def test_launch_shape_table_round_trip(tmp_path):
+    """alluvion_b200.autotune tables: JSON round trip, validation of names
+    and ranges, and load() applying every entry (a stand-in engine records
+    the calls; no device is needed)."""
+    from alluvion_b200 import autotune
+
+    class Recorder:
+        def __init__(self):
+            self.calls = []
+
+        def set_launch_shape(self, *args):
+            self.calls.append(args)
+
+    table = {"device": "test", "entries": [
+        {"group": "press_iter", "bucket": 20, "batch": 0, "block": 256, "tpp": 1, "ms": 0.1},
+        {"group": "neighbors", "bucket": 20, "batch": 1, "block": 64, "tpp": 1, "ms": 0.3}]}
+    path = str(tmp_path / "t.json")
+    autotune.save(table, path)
+    rec = Recorder()
+    loaded = autotune.load(rec, path)
+    assert loaded["entries"] == table["entries"]
+    assert rec.calls == [("press_iter", 20, 0, 256, 1), ("neighbors", 20, 1, 64, 1)]
+    assert autotune.bucket_of(1 << 20) == 20 and autotune.bucket_of((1 << 20) - 1) == 19
+    bad = {"entries": [dict(table["entries"][0], block=96)]}
+    with pytest.raises(ValueError):
+        autotune.validate(bad)
+    dup = {"entries": [table["entries"][0], dict(table["entries"][0])]}
+    with pytest.raises(ValueError):
+        autotune.validate(dup)

@@ -1,7 +1,12 @@
 """Batched scenes (al_df_batch_step_f32) against the same scenes stepped
 one at a time with al_df_step_f32.  Each batch branch runs the scene's own
-kernels with the same launch shapes, so the results are bit-identical,
-whether the batch runs eagerly (first call) or as one replayed graph."""
+kernels; with the default launch-shape tables (the same shapes in the
+single and the batch context: threads per particle from the scene's own
+particle count) the launch shapes are the same too, so the results are
+bit-identical, whether the batch runs eagerly (first call) or as one
+replayed graph.  Tuned tables that give a scene another shape in a batch
+change its float results in the last bits (tests/test_gpu_launch_shapes.py
+covers that case against the oracle)."""
 import numpy as np
 import pytest
 

@@ -1,0 +1,272 @@
+"""Parity at the benchmark configurations' own sizes, through the C ABI.
+
+Scenes are the bench's seeded workloads: the 32,768-particle dam break in a
+1.0 x 0.7 x 0.7 m box with a 64^3 volume map (config 1) and the
+1,048,576-particle dam break in a 2 x 1 x 2 m box with four rigid bodies on
+64^3 grids (config 2).  The engine steps them with SolverDf::step
+(solver_df.hpp:74-359) and SolverIi::step (solver_ii.hpp:76-243) semantics;
+the oracle restates the same routines on the host.
+
+Bars (measured on B200 in the comments; bounds leave a margin):
+* float64, engine against oracle: the same formulas in the same precision,
+  so relative errors stay at rounding level (1e-16 .. 1e-11 over 20 steps)
+  and the iteration counts are equal at every step.
+* float32, engine against oracle: equal iteration counts at every step;
+  after the first step relative errors of x 1e-6, v 1e-4, density 1e-5,
+  kappa 1e-3.  Later, the jittered start's pressure kicks amplify the last
+  bits (FMA contraction, summation order) chaotically: the engine's float32
+  trajectory then differs from the oracle's by as much as it differs from
+  its own float64 trajectory.  The bound is stated that way: the
+  L2-relative difference from the oracle is at most 3x the L2-relative
+  difference between the engine's float32 and float64 runs (plus 1e-6).
+* neighbor lists at 1,048,576 particles: cell ids, permutation, counts,
+  indices and displacement bits identical.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import bench
+from alluvion_b200 import _capi, scenes
+from oracle import binding as orc
+
+pytestmark = pytest.mark.gpu
+
+QUANT = {"df": ("x", "v", "density", "kappa", "kappa_v"), "ii": ("x", "v", "density", "pressure")}
+
+
+def _maxrel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _l2rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+class OracleRun:
+    """The oracle's copy of a device scene (same grids, same initial state)."""
+
+    def __init__(self, scene, method):
+        self.scene = scene
+        self.method = method
+        self.hb, self.keep, self.rigid = scene.host_bodies()
+        nb = scene.num_boundaries
+        self.bodies = (type(self.hb[0]) * nb)(*[self.hb[b] for b in range(nb)])
+        st = scene.state()
+        self.state = {k: np.ascontiguousarray(st[k]).copy() for k in
+                      ("x", "v", "kappa", "kappa_v", "density", "density_adv", "a", "pressure")}
+        self.dt = float(scenes.solver_params().max_dt)
+
+    def step(self, sp):
+        self.dt, reps = orc.run(self.method, self.scene.cn, self.scene.cni, self.bodies,
+                                self.rigid, self.state, sp, self.dt, 1)
+        return reps[0]
+
+
+def _spec(workload, dtype, bodies=None):
+    wl = bench.WORKLOADS[workload]
+    b = bench.workload_bodies(wl) if bodies is None else bodies
+    return scenes.dam_break_spec(dtype, wl["lattice"], wl["radius"], wl["container"], b,
+                                 seed=bench.SEED, volume_resolution=wl["container_resolution"])
+
+
+def _twin(engine, workload, bodies=None, keep=None):
+    """The workload's scene twice: float32, and float64 started from the
+    same (float32) positions.  keep: mask of the particles to keep."""
+    spec32 = _spec(workload, np.float32, bodies)
+    spec64 = _spec(workload, np.float64, bodies)
+    x = spec32.x if keep is None else spec32.x[keep]
+    spec32.x = np.ascontiguousarray(x)
+    spec64.x = np.ascontiguousarray(x.astype(np.float64))
+    return spec32.device(engine), spec64.device(engine)
+
+
+def _iters(rep):
+    return rep.num_divergence_solve, rep.num_density_solve
+
+
+@pytest.mark.parametrize("method", ["df", "ii"])
+def test_config1_float64_matches_oracle_over_20_steps(engine, method):
+    """Config 1 in float64: engine and oracle agree to rounding level for 20
+    steps (measured: max relative error <= 8e-12, kappa at step 10)."""
+    sc = _spec("dambreak-32k", np.float64).device(engine)
+    orun = OracleRun(sc, method)
+    sp = scenes.solver_params()
+    dt = float(sp.max_dt)
+    tol = {"x": 1e-13, "v": 1e-11, "density": 1e-12, "kappa": 1e-10, "kappa_v": 1e-10,
+           "pressure": 1e-10}
+    for s in range(20):
+        dt, rep = sc.step(method, sp, dt)
+        o = orun.step(sp)
+        assert _iters(rep) == _iters(o), "step %d" % s
+        assert rep.dt == o.dt
+    g = sc.state()
+    for k in QUANT[method]:
+        assert _maxrel(g[k], orun.state[k]) <= tol[k], k
+
+
+@pytest.mark.parametrize("method", ["df", "ii"])
+def test_config1_float32_matches_oracle_over_50_steps(engine, method):
+    """Config 1 in float32 for 50 steps: equal iteration counts every step,
+    tight errors after step 1, and afterwards differences from the oracle
+    no larger than the float32 rounding sensitivity of the trajectory
+    (3x the engine's own float32-vs-float64 difference)."""
+    s32, s64 = _twin(engine, "dambreak-32k")
+    orun = OracleRun(s32, method)
+    sp = scenes.solver_params()
+    d32 = d64 = float(sp.max_dt)
+    for s in range(1, 51):
+        d32, rep = s32.step(method, sp, d32)
+        d64, _ = s64.step(method, sp, d64)
+        o = orun.step(sp)
+        assert _iters(rep) == _iters(o), "step %d" % s
+        if s == 1:
+            g = s32.state()
+            first = {"x": 1e-6, "v": 1e-4, "density": 1e-5, "kappa": 1e-3, "kappa_v": 1e-3,
+                     "pressure": 1e-3}
+            for k in QUANT[method]:
+                if np.abs(orun.state[k]).max() > 0:
+                    assert _maxrel(g[k], orun.state[k]) <= first[k], (k, s)
+    g, g64 = s32.state(), s64.state()
+    for k in QUANT[method]:
+        e_orc = _l2rel(g[k], orun.state[k])
+        e_f64 = _l2rel(g[k], g64[k])
+        assert e_orc <= 3 * e_f64 + 1e-6, (k, e_orc, e_f64)
+
+
+@pytest.mark.parametrize("method", ["df", "ii"])
+def test_config2_matches_oracle(engine, method):
+    """Config 2 (1,048,576 particles, four rigid bodies, 64^3 grids), two
+    float32 steps against the oracle and two float64 steps: iteration counts
+    equal; float64 errors <= 1e-11 (measured <= 3.2e-13); float32 after the
+    first step x 1e-6, v 1e-4, density 1e-5, kappa 1e-3 (measured 9e-8,
+    7e-6, 6e-7, 1.4e-5); after the second, within the float32 rounding
+    sensitivity (3x the float32-vs-float64 difference)."""
+    s32, s64 = _twin(engine, "dambreak-1m")
+    o32 = OracleRun(s32, method)
+    o64 = OracleRun(s64, method)
+    sp = scenes.solver_params()
+    d32 = d64 = float(sp.max_dt)
+    first = {"x": 1e-6, "v": 1e-4, "density": 1e-5, "kappa": 1e-3, "kappa_v": 1e-3,
+             "pressure": 1e-3}
+    for s in range(1, 3):
+        d32, r32 = s32.step(method, sp, d32)
+        d64, r64 = s64.step(method, sp, d64)
+        a32, a64 = o32.step(sp), o64.step(sp)
+        assert _iters(r32) == _iters(a32) and _iters(r64) == _iters(a64), s
+        g32, g64 = s32.state(), s64.state()
+        for k in QUANT[method]:
+            assert _maxrel(g64[k], o64.state[k]) <= 1e-11, (k, s)
+            if s == 1 and np.abs(o32.state[k]).max() > 0:
+                assert _maxrel(g32[k], o32.state[k]) <= first[k], (k, s)
+            if s == 2:
+                assert _l2rel(g32[k], o32.state[k]) <= 3 * _l2rel(g32[k], g64[k]) + 1e-6, (k, s)
+
+
+def _submerged(engine):
+    """Config 2 with the four bodies placed inside the fluid block (seeded),
+    fluid particles within 2r of a body removed, so the two-way coupling
+    acts from the first step; float32 and float64 twins."""
+    wl = bench.WORKLOADS["dambreak-1m"]
+    bodies = bench.workload_bodies(wl)
+    rng = np.random.default_rng(5)
+    for b in bodies:
+        b["x"] = (rng.uniform(0.3, 1.0), rng.uniform(0.2, 0.45), rng.uniform(0.3, 1.0))
+    x = _spec("dambreak-1m", np.float32, bodies).x.astype(np.float64)
+    r = wl["radius"]
+    keep = np.ones(len(x), bool)
+    for b in bodies:
+        d = x - np.asarray(b["x"])
+        if b["shape"] == _capi.SHAPE_SPHERE:
+            sdf = np.sqrt((d * d).sum(1)) - b["params"][0]
+        else:
+            q = np.abs(d) - np.asarray(b["params"][:3])
+            sdf = np.sqrt((np.maximum(q, 0) ** 2).sum(1)) + np.minimum(q.max(1), 0)
+        keep &= sdf > 2 * r
+    return _twin(engine, "dambreak-1m", bodies, keep)
+
+
+@pytest.mark.parametrize("method", ["df", "ii"])
+def test_config2_coupled_bodies_match_oracle(engine, method):
+    """Config 2 with the bodies in the fluid: rigid forces and torques (FP64
+    sums) and rigid motion against the oracle after two steps, float64
+    within 1e-10, float32 forces within 1e-3 of their scale after the first
+    step; iteration counts equal."""
+    s32, s64 = _submerged(engine)
+    o32 = OracleRun(s32, method)
+    o64 = OracleRun(s64, method)
+    sp = scenes.solver_params()
+    d32 = d64 = float(sp.max_dt)
+    nb = s32.num_boundaries
+    for s in range(1, 3):
+        d32, r32 = s32.step(method, sp, d32)
+        d64, r64 = s64.step(method, sp, d64)
+        a32, a64 = o32.step(sp), o64.step(sp)
+        assert _iters(r32) == _iters(a32) and _iters(r64) == _iters(a64), s
+        f64 = np.array([r64.force[b] for b in range(1, nb)])
+        fo64 = np.array([a64.force[b] for b in range(1, nb)])
+        t64 = np.array([r64.torque[b] for b in range(1, nb)])
+        to64 = np.array([a64.torque[b] for b in range(1, nb)])
+        assert np.abs(fo64).max() > 0  # the bodies are coupled from the start
+        assert _maxrel(f64, fo64) <= 1e-10 and _maxrel(t64, to64) <= 1e-9, s
+        if s == 1:
+            f32 = np.array([r32.force[b] for b in range(1, nb)])
+            fo32 = np.array([a32.force[b] for b in range(1, nb)])
+            assert _maxrel(f32, fo32) <= 1e-3
+    g64 = scenes.rigid_array(np.float64, [s64.rigid[b] for b in range(nb)])
+    assert _maxrel(g64[1:, :6], o64.rigid[1:, :6]) <= 1e-10
+    assert _maxrel(s64.state()["v"], o64.state["v"]) <= 1e-10
+
+
+def test_config2_neighbor_lists_bit_exact(engine):
+    """Config 2's 1,048,576 initial positions: cell ids, sorted permutation,
+    cell starts, neighbor counts, neighbor indices (canonical order) and the
+    stored displacement bits equal the oracle's."""
+    spec = _spec("dambreak-1m", np.float32)
+    cn, x = spec.cn, spec.x
+    cni = _capi.ConstI.from_buffer_copy(spec.cni)
+    cni.num_boundaries = 0  # lists and fluid density only (no boundary terms passed)
+    n = x.shape[0]
+    ncells = cni.grid_res[0] * cni.grid_res[1] * cni.grid_res[2]
+    xd = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    cell = torch.zeros(n, dtype=torch.int32, device="cuda")
+    perm = torch.zeros(n, dtype=torch.int32, device="cuda")
+    start = torch.zeros(ncells + 1, dtype=torch.int32, device="cuda")
+    st = _capi.lib().al_grid_sort_f32(engine.handle, ctypes.byref(cn), ctypes.byref(cni),
+                                      _capi.ptr(xd), n, _capi.ptr(cell), _capi.ptr(perm),
+                                      _capi.ptr(start), None, None)
+    assert st == _capi.AL_OK
+    o_cell, o_perm, o_start, o_flags = orc.grid_sort(cn, cni, x)
+    u = lambda t: t.cpu().numpy().view(np.uint32)
+    assert np.array_equal(u(cell), o_cell)
+    assert np.array_equal(u(perm), o_perm)
+    assert np.array_equal(u(start), o_start)
+    del cell, perm, start
+    cap = cni.max_num_neighbors_per_particle
+    rho = torch.zeros(n, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nbr = torch.zeros((n, cap, 4), device="cuda")
+    anomaly = torch.zeros(3, dtype=torch.int32, device="cuda")
+    st = _capi.lib().al_update_particle_neighbors_f32(
+        engine.handle, ctypes.byref(cn), ctypes.byref(cni), _capi.ptr(xd), n, None,
+        _capi.ptr(rho), _capi.ptr(cnt), _capi.ptr(nbr), _capi.ptr(anomaly), None)
+    assert st == _capi.AL_OK
+    o_rho, o_cnt, o_idx, o_nbrs, o_fl = orc.update_particle_neighbors(cn, cni, x)
+    g_cnt = u(cnt)
+    assert np.array_equal(g_cnt, o_cnt)
+    assert 20 < g_cnt.mean() < 40
+    g = nbr.cpu().numpy()
+    del nbr
+    live = np.arange(cap)[None, :] < g_cnt[:, None]
+    idx = np.ascontiguousarray(g[..., 3]).view(np.uint32)
+    assert np.array_equal(idx[live], o_idx[live])
+    bits = np.ascontiguousarray(g[..., :3]).view(np.uint32)
+    obits = np.ascontiguousarray(o_nbrs[..., :3]).view(np.uint32)
+    assert np.array_equal(bits[live], obits[live])
+    np.testing.assert_allclose(rho.cpu().numpy(), o_rho, rtol=1e-6)

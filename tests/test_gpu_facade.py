@@ -361,3 +361,8 @@ def test_sample_all_boundaries_matches_the_c_abi(engine):
     np.testing.assert_array_equal(vb.get(), sb.cpu().numpy())
     np.testing.assert_array_equal(vk.get(), sbk.cpu().numpy())
     assert np.abs(vk.get()[:, :, 3]).max() > 0
+    # rows of a [nb][capacity] variable with capacity != num_samples would
+    # sit at another stride than the reference's Variable<2> indexing: refused
+    wb, wk = dp.create([nb, s + 10], 4), dp.create([nb, s + 10], 4)
+    with pytest.raises(Exception, match="num_samples"):
+        solver.sample_all_boundaries(vx, wb, wk, s)

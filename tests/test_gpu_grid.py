@@ -225,3 +225,30 @@ def test_periodic_neighbors_bit_exact(engine, dtype):
     ids = set(idx[i, :g_cnt[i]].tolist())
     assert ids & top_ids
     assert np.abs(g_nbr[i, :g_cnt[i], 1]).max() < h
+
+
+@pytest.mark.parametrize("crowd", [40, 300, 5000])
+def test_crowded_cells_sorted_canonically(engine, crowd):
+    """A cell holding many particles: 40 extra members (within the 64-member
+    capacity of the per-thread ordering), 300 (the block-cooperative bitonic
+    path) and 5000 (above its shared-memory size, one thread in place).  The
+    permutation equals the oracle's canonical (cell, index) order; beyond
+    the cell capacity the overflow is reported, as the reference's
+    grid_anomaly[1]."""
+    cn, cni, x = _block(np.float32, dims=(8, 8, 8), seed=5)
+    h = float(cn.kernel_radius)
+    corner = (np.floor(x[100] / h)) * h
+    rng = np.random.default_rng(crowd)
+    pile = (corner + rng.uniform(0.1 * h, 0.9 * h, size=(crowd, 3))).astype(np.float32)
+    xs = np.concatenate([x, pile])
+    xs = xs[rng.permutation(len(xs))]
+    status, cell, perm, start, plen = _grid_sort(engine, cn, cni, xs)
+    o_cell, o_perm, o_start, o_flags = orc.grid_sort(cn, cni, xs)
+    assert np.array_equal(cell, o_cell)
+    assert np.array_equal(start, o_start)
+    assert np.array_equal(perm, o_perm)
+    assert plen.max() >= crowd
+    if plen.max() > cni.max_num_particles_per_cell:
+        assert status == _capi.AL_ERR_CELL_OVERFLOW and o_flags[1] == 1
+    else:
+        assert status == _capi.AL_OK

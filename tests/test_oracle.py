@@ -274,3 +274,65 @@ def test_oracle_hydrostatic_column(method):
             (xx[:, 1] > xx[:, 1].min() + 0.05)
     slope = np.polyfit(depth[inner], p[inner], 1)[0]
     assert slope == pytest.approx(9.81, rel=0.15)
+
+
+@pytest.mark.parametrize("case", ["container_box", "sphere_analytic", "box_grid"])
+def test_lazy_volume_map_equals_eager_build(case):
+    """The lazily filled volume map (nodes computed on first use; analytic
+    bodies skip nodes 2h outside / h inside the shape) returns the eager
+    build's values bit for bit: boundary samples over particles in every
+    Lagrange cell are identical, and so is every node they touched."""
+    dtype = np.float32
+    cn = scenes.make_const(dtype, 0.01)
+    h = float(cn.kernel_radius)
+    if case == "container_box":
+        size = np.array([0.3, 0.2, 0.25])
+        body = scenes.make_body(dtype, cn, _capi.SHAPE_BOX, scenes.box_params(size), 10,
+                                sign=-1.0)
+        rigid_x = size / 2
+    elif case == "sphere_analytic":
+        body = scenes.make_body(dtype, cn, _capi.SHAPE_SPHERE, [0.05], 8, sign=1.0)
+        rigid_x = np.zeros(3)
+    else:
+        body = scenes.make_body(dtype, cn, _capi.SHAPE_BOX, scenes.box_params((0.06, 0.05, 0.08)),
+                                8, sign=1.0, use_distance_grid=True)
+        rigid_x = np.zeros(3)
+    keep = []
+    if body.use_distance_grid:
+        dist = orc.distance_grid(body, dtype)
+        keep.append(dist)
+        body.distance_nodes = dist.ctypes.data
+    eager = orc.volume_field(cn, body, dtype)
+    lazy = orc.lazy_volume_field(cn, body, dtype)
+    try:
+        res = np.array(list(body.resolution))
+        dmin = np.array(list(body.domain_min), np.float64)
+        cs = np.array(list(body.cell_size), np.float64)
+        # one particle per cell (cell centre + a small seeded offset), in world coordinates
+        idx = np.stack(np.meshgrid(*[np.arange(r) for r in res], indexing="ij"), -1).reshape(-1, 3)
+        rng = np.random.default_rng(3)
+        local = dmin + (idx + 0.5 + rng.uniform(-0.3, 0.3, idx.shape)) * cs
+        x = (local + rigid_x).astype(dtype)
+        rigid = np.zeros((1, 13), dtype)
+        rigid[0, :3] = rigid_x
+        rigid[0, 9] = 1.0
+        Body = type(body)
+        b_eager = (Body * 1)(body)
+        b_eager[0].volume_nodes = eager.ctypes.data
+        b_lazy = (Body * 1)(body)
+        b_lazy[0].volume_nodes = lazy.ctypes.data
+        bnd_e, bk_e = orc.boundary(cn, b_eager, rigid, x)
+        bnd_l, bk_l = orc.boundary(cn, b_lazy, rigid, x)
+        assert np.array_equal(bnd_e.view(np.uint32), bnd_l.view(np.uint32))
+        assert np.array_equal(bk_e.view(np.uint32), bk_l.view(np.uint32))
+        # every node belongs to some cell, so every node was computed
+        assert np.array_equal(eager.view(np.uint32), lazy.view(np.uint32))
+        sampled, skipped = orc.lazy_volume_counts(lazy)
+        assert sampled + skipped == body.num_nodes
+        if case == "container_box":
+            assert skipped > 0  # interior nodes far from the walls need no sampling
+        if case == "box_grid":
+            assert skipped == 0  # grid distances are always sampled
+        assert np.abs(eager).max() > 0.5 * h ** 3
+    finally:
+        orc.lazy_volume_release(lazy)

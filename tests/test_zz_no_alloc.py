@@ -1,13 +1,16 @@
 """The allocation-free grid sort (al_grid_sort_noalloc_f32).
 
-Callers such as a host that captures its frame into a CUDA graph, or a
-renderer that owns the device memory budget, cannot let the library call
-cudaMalloc; this entry point keeps its scratch in one static device array.
-The test calls it through the C ABI twice in a row, on two different
-particle sets, and checks each result against the allocating
+Callers such as a renderer that owns the device memory budget, or a
+real-time loop that cannot take the stalls of cudaMalloc / cudaFree, cannot
+let the library allocate; this entry point keeps its scratch in one static
+device array.  The test calls it through the C ABI twice in a row, on two
+different particle sets, and checks each result against the allocating
 al_grid_sort_f32 (integer outputs: bit-exact, the bar of the grid tests).
 The second call must see no stale counts from the first, and must not
-change the device's free memory.  Collected last on purpose.
+change the device's free memory (the first call may: CUDA loads the
+library's device image, and with it the static array, lazily).  The
+anomaly statuses (a particle outside the grid, a cell above its capacity)
+must equal the allocating sort's.  Collected last on purpose.
 """
 import ctypes
 
@@ -79,3 +82,39 @@ def test_noalloc_rejects_sizes_beyond_the_static_limit():
     status = _capi.lib().al_grid_sort_noalloc_f32(ctypes.byref(cn), ctypes.byref(cni), None,
                                                   (1 << 20) + 1, None, None, None, None, None)
     assert status == 2
+
+
+@pytest.mark.parametrize("case", ["out_of_grid", "cell_overflow"])
+def test_noalloc_reports_the_same_anomalies(case):
+    """A particle far outside the grid (AL_ERR_OUT_OF_GRID) and a cell
+    capacity below the lattice's ~8 particles per cell
+    (AL_ERR_CELL_OVERFLOW): both entry points return the same status and
+    the same outputs."""
+    lib = _capi.lib()
+    engine = _capi.Engine(0)
+    try:
+        cn, cni, x = _inputs(23, (8, 8, 8))
+        x = x.copy()
+        if case == "out_of_grid":
+            x[5] = (50.0, 50.0, 50.0)
+            expect = _capi.AL_ERR_OUT_OF_GRID
+        else:
+            cni.max_num_particles_per_cell = 4
+            expect = _capi.AL_ERR_CELL_OVERFLOW
+        s_ref, ref, _ = _run(lib.al_grid_sort_f32, (engine.handle,), cn, cni, x)
+        s_na, got, _ = _run(lib.al_grid_sort_noalloc_f32, (), cn, cni, x)
+        assert s_ref == expect and s_na == expect
+        inside = int(ref[2][-1])
+        for name, a, b in zip(("cell", "perm", "cell_start", "pid_length"), got, ref):
+            if name == "perm":
+                # out-of-grid particles sit after the in-grid ones, in any order
+                assert np.array_equal(a[:inside], b[:inside]), name
+                assert set(a[inside:]) == set(b[inside:]), name
+            else:
+                assert np.array_equal(a, b), name
+        # a clean call afterwards starts from cleared flags
+        cn2, cni2, x2 = _inputs(24, (6, 6, 6))
+        s2, _, _ = _run(lib.al_grid_sort_noalloc_f32, (), cn2, cni2, x2)
+        assert s2 == _capi.AL_OK
+    finally:
+        engine.close()
