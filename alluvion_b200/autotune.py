@@ -13,9 +13,10 @@ on how many threads the pass has to fill the GPU with.
                                   launch with the engine's CUDA-event
                                   statistics (each candidate from the same
                                   state); single-step context
-  tune_batch(engine, scenes, sp)  per bucket, the shape that minimises the
-                                  whole batched step (graph replays, scenes
-                                  side by side); batch context
+  tune_batch(engine, scenes, sp)  whole batched steps timed (graph replays,
+                                  scenes side by side): the best shape for
+                                  all buckets alike, then coordinate descent
+                                  over the buckets; batch context
   save(table, path), load(engine, path), apply(engine, table)
 
 A table is a dict {"device": ..., "entries": [{"group", "bucket", "batch",
@@ -134,13 +135,13 @@ def tune_scene(engine, scene, sp, method="df", steps=3, warm=None):
     return table
 
 
-def tune_batch(engine, scene_list, sp, steps=4, candidates=None, step_fn=None):
-    """Coordinate descent over the batch's particle-count buckets: for each
-    bucket in turn, every candidate shape is applied to all pass groups of
-    that bucket (batch context) and whole batched steps are timed (graph
-    replays, scenes from the same state each trial); the fastest is kept.
-    Returns and applies the table; `step_fn(dts)` steps the batch (default
-    scenes.batch_step)."""
+def tune_batch(engine, scene_list, sp, steps=8, candidates=None, step_fn=None):
+    """Shapes for a batch, timed on whole batched steps (graph replays,
+    every trial from the same restored state), in two stages: the best
+    shape applied to every particle-count bucket alike, then coordinate
+    descent over the buckets from there, keeping a change only when it
+    saves more than 1 % of the batch step.  Returns and applies the table;
+    `step_fn(dts)` steps the batch (default scenes.batch_step)."""
     import torch
     from . import scenes as _scenes
     cands = candidates or PAIR_CANDIDATES
@@ -150,9 +151,9 @@ def tune_batch(engine, scene_list, sp, steps=4, candidates=None, step_fn=None):
         step_fn = lambda dts: _scenes.batch_step(engine, scene_list, sp, dts)[0]
     buckets = sorted({bucket_of(sc.n) for sc in scene_list})
 
-    def set_bucket(b, blk, tpp):
+    def set_bucket(b, shape):
         for name, pair in groups:
-            engine.set_launch_shape(name, b, 1, blk, tpp if pair else 1)
+            engine.set_launch_shape(name, b, 1, shape[0], shape[1] if pair else 1)
 
     def trial():
         for sc, sn in zip(scene_list, snaps):
@@ -170,27 +171,36 @@ def tune_batch(engine, scene_list, sp, steps=4, candidates=None, step_fn=None):
         torch.cuda.synchronize()
         return t0.elapsed_time(t1) / steps
 
-    chosen = {}
     base_ms = trial()
-    best_total = base_ms
+    uniform = None
+    for shape in cands:
+        for b in buckets:
+            set_bucket(b, shape)
+        ms = trial()
+        if uniform is None or ms < uniform[0]:
+            uniform = (ms, shape)
+    current = {b: uniform[1] for b in buckets}
     for b in buckets:
-        best = None
-        for blk, tpp in cands:
-            set_bucket(b, blk, tpp)
+        set_bucket(b, uniform[1])
+    best = trial()
+    for b in buckets:
+        for shape in cands:
+            if shape == current[b]:
+                continue
+            set_bucket(b, shape)
             ms = trial()
-            if best is None or ms < best[0]:
-                best = (ms, blk, tpp)
-        chosen[b] = best
-        set_bucket(b, best[1], best[2])
-        best_total = best[0]
+            if ms < 0.99 * best:
+                best, current[b] = ms, shape
+        set_bucket(b, current[b])
     for sc, sn in zip(scene_list, snaps):
         sc.restore(sn)
-    entries = [{"group": name, "bucket": b, "batch": 1, "block": chosen[b][1],
-                "tpp": chosen[b][2] if pair else 1, "ms": round(chosen[b][0], 5)}
+    entries = [{"group": name, "bucket": b, "batch": 1, "block": current[b][0],
+                "tpp": current[b][1] if pair else 1, "ms": round(best, 5)}
                for b in buckets for name, pair in groups]
     table = {"device": torch.cuda.get_device_name(), "entries": entries,
-             "batch_ms_default": round(base_ms, 4), "batch_ms_tuned": round(best_total, 4),
-             "buckets": {str(b): {"block": chosen[b][1], "tpp": chosen[b][2],
+             "batch_ms_default": round(base_ms, 4), "batch_ms_uniform": round(uniform[0], 4),
+             "uniform_shape": list(uniform[1]), "batch_ms_tuned": round(best, 4),
+             "buckets": {str(b): {"block": current[b][0], "tpp": current[b][1],
                                   "scenes": int(np.sum([bucket_of(sc.n) == b
                                                         for sc in scene_list]))}
                          for b in buckets}}

@@ -283,8 +283,8 @@ struct WarmDivergence {
   float* feat = nullptr;      // [n][12] sorted order
   float* feat_out = nullptr;  // [n][12] original order
   TF two_r = 0, vol = 0;
-  // learned warm start gate: nonzero when the previous step of this scene ran
-  // both solves at their minimum iteration counts (the prediction is not used)
+  // learned warm start gate (warm_gate_update): nonzero when this step skips
+  // the network
   const uint32_t* floor = nullptr;
   __device__ __forceinline__ vec3<TF> self_v(uint32_t s) const { return xyz(RV(S, s)); }
   __device__ __forceinline__ vec3<TF> vj(uint32_t t) const { return xyz(gV(S, t)); }
@@ -328,6 +328,32 @@ struct WarmDivergence {
   }
 };
 
+// The learned warm start's per-scene gate, kept in four device words:
+//   [0] 1 when the next step skips the network (plain warm starts)
+//   [1] steps since the network last ran
+//   [2] solver iterations (divergence + density) of the last step that ran it
+//   [3] solver iterations of the last step that did not
+// A fresh scene starts at zero (the first step runs the network).  After
+// each step (k_df_finish): the network runs next only if this step's solves
+// went beyond their minimum iteration counts (at the minimum no warm start
+// can save an iteration) and its last outcome was no worse than the plain
+// start's last outcome, or it has not run for 64 steps (a new try).  So a
+// network that predicts poorly for a scene costs at most one step in 64.
+template <class TF>
+__device__ __forceinline__ void warm_gate_update(const Ctrl<TF>& C, uint32_t* w) {
+  const bool used = w[0] == 0u;
+  const uint32_t tot = C.rep.num_divergence_solve + C.rep.num_density_solve;
+  if (used)
+    w[2] = tot;
+  else
+    w[3] = tot;
+  w[1] = used ? 0u : w[1] + 1u;
+  const bool at_floor =
+      C.rep.num_divergence_solve <= C.min_div && C.rep.num_density_solve <= C.min_den;
+  const bool net_ok = w[2] <= w[3] || w[1] >= 64u;
+  w[0] = (!at_floor && net_ok) ? 0u : 1u;
+}
+
 // Learned divergence warm start: kappa_v = predicted kappa_v where the
 // reference's gate holds (rho_dot > 0, i.e. feature 1 > 0), else 0.  When
 // the floor gate is set the build's plain warm start stays.
@@ -348,8 +374,11 @@ enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 // (runner.hpp:3251-3295), divergence_solve_iteration (:3316-3363),
 // warm_start_pressure_solve1 (:3451-3491), pressure_solve_iteration
 // (:3543-3588).  Boundary reaction forces go to the per-block rigid slots.
+// The float kernel is held at 56 registers (9 resident 128-thread blocks
+// per SM; with 256-thread launch bounds the compiler took 58, and the
+// 256-register allocation granule then allows only 8); double needs more.
 template <class TF, int MODE, bool WR = false>
-__global__ void __launch_bounds__(kMaxBlock) k_kappa(Cn<TF> c, StepState<TF> S) {
+__global__ void __maxnreg__(sizeof(TF) == 4 ? 56 : 128) k_kappa(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
   const Lane L = pair_lane(S);
@@ -622,13 +651,7 @@ __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __
                             TF* __restrict__ rho_adv_ref, uint32_t* __restrict__ warm_floor) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (warm_floor && s == 0) {
-    // learned warm start gate of the next step: both solves of this one ran
-    // at their minimum counts, where no warm start can save an iteration
-    const Ctrl<TF>& C = *S.ctrl;
-    *warm_floor = (C.rep.num_divergence_solve <= C.min_div &&
-                   C.rep.num_density_solve <= C.min_den) ? 1u : 0u;
-  }
+  if (warm_floor && s == 0) warm_gate_update(*S.ctrl, warm_floor);
   if (s >= S.n) return;
   const uint32_t i = S.perm[s];
   const TF dt = S.ctrl->dt;
@@ -1071,8 +1094,8 @@ struct StepPlan {
   float* warm_feat = nullptr;
   float* warm_feat_out = nullptr;
   float* warm_pred = nullptr;
-  // [0]: 1 when the scene's previous step ran both solves at their minimum
-  // iteration counts; the network is then skipped (fresh scenes start at 0)
+  // the learned warm start's gate words (warm_gate_update); zero for a fresh
+  // scene
   uint32_t* warm_floor = nullptr;
   // launch shapes: particle-count bucket and context of the shape table
   uint32_t bucket = 0, ctx = 0;
@@ -1336,9 +1359,9 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
         const StepState<TF> Sg_ = pair_shape("finish", pg_, pb_);
         ALB_LAUNCH(e, "finish", 1, st,
                    (wr ? k_ii_accel_finish<TF, true><<<pg_, pb_, 0, st>>>(
-                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       c, Sg_, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
                        f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pg_, pb_, 0, st>>>(
-                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       c, Sg_, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
                        f->particle_pressure, f->particle_density_adv)));
       }
     } else {
@@ -1373,9 +1396,9 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
         const StepState<TF> Sg_ = pair_shape("finish", pg_, pb_);
         ALB_LAUNCH(e, "finish", 1, st,
                    (wr ? k_ii_accel_finish<TF, true><<<pg_, pb_, 0, st>>>(
-                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       c, Sg_, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
                        f->particle_pressure, f->particle_density_adv) : k_ii_accel_finish<TF, false><<<pg_, pb_, 0, st>>>(
-                       c, S, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
+                       c, Sg_, f->particle_x, f->particle_v, f->particle_a, f->particle_density,
                        f->particle_pressure, f->particle_density_adv)));
       }
     }

@@ -66,11 +66,17 @@ def run_iterations(engine, spec, sp, steps, warm=None):
 
 
 def net_used(its, sp):
-    """Steps on which the learned start is applied: the first, and every step
-    after one whose solves went beyond their minimum iteration counts."""
-    used = [True]
-    for d, r in its[:-1]:
-        used.append(bool(d > sp.min_divergence_solve or r > sp.min_density_solve))
+    """Steps on which the engine's gate runs the network (the rule of
+    warm_gate_update in the engine, replayed on the iteration record)."""
+    w = [0, 0, 0, 0]
+    used = []
+    for d, r in its:
+        u = w[0] == 0
+        used.append(u)
+        w[2 if u else 3] = d + r
+        w[1] = 0 if u else w[1] + 1
+        at_floor = d <= sp.min_divergence_solve and r <= sp.min_density_solve
+        w[0] = 0 if (not at_floor and (w[2] <= w[3] or w[1] >= 64)) else 1
     return np.asarray(used)
 
 
@@ -87,11 +93,20 @@ def main():
     ap.add_argument("--eval-steps", type=int, default=200)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--eval-out", default=EVALUATION)
+    ap.add_argument("--eval-only", action="store_true",
+                    help="evaluate the network in --out again (its training record is kept)")
     args = ap.parse_args()
     import torch
     torch.cuda.set_device(0)
     engine = _capi.Engine(0)
     sp = scenes.solver_params()
+    if args.eval_only:
+        net = warm_start.WarmStartNet.load(args.out)
+        with open(args.eval_out) as f:
+            training = json.load(f)["training"]
+        evaluate(engine, net, sp, args, training)
+        engine.close()
+        return
     t_start = time.perf_counter()
     xs, ts = [], []
     for k in range(args.scenes):
@@ -111,6 +126,20 @@ def main():
     t_fit = time.perf_counter() - t0
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     net.save(args.out)
+    training = {"scenes": args.scenes, "steps_per_scene": args.steps,
+                "samples": int(feats.shape[0]), "adam_steps": args.fit_steps,
+                "batch": args.batch, "lr": args.lr,
+                "loss_first_last": [round(float(np.mean(losses[:100])), 5),
+                                    round(float(np.mean(losses[-100:])), 5)],
+                "collect_s": round(t_collect, 1), "fit_s": round(t_fit, 1)}
+    del feats, targs
+    evaluate(engine, net, sp, args, training)
+    engine.close()
+
+
+def evaluate(engine, net, sp, args, training):
+    """Plain against learned warm start on the held-out seeds; writes the
+    evaluation JSON (with the training record) and prints its summary."""
     rows = []
     for k in range(args.eval_scenes):
         spec = scene_spec(EVAL_SEED0 + k)
@@ -134,12 +163,7 @@ def main():
     lm = np.array([r["learned_ms_per_step"] for r in rows])
     n = scene_spec(EVAL_SEED0).n
     summary = {
-        "training": {"scenes": args.scenes, "steps_per_scene": args.steps,
-                     "samples": int(feats.shape[0]), "adam_steps": args.fit_steps,
-                     "batch": args.batch, "lr": args.lr,
-                     "loss_first_last": [round(float(np.mean(losses[:100])), 5),
-                                         round(float(np.mean(losses[-100:])), 5)],
-                     "collect_s": round(t_collect, 1), "fit_s": round(t_fit, 1)},
+        "training": training,
         "evaluation": {"scenes": args.eval_scenes, "steps": args.eval_steps,
                        "particles": n, "max_dt": float(sp.max_dt),
                        "min_iterations": [int(sp.min_divergence_solve),
@@ -147,13 +171,14 @@ def main():
                        "plain_iterations_per_step": [round(float(v), 4) for v in pi.mean(0)],
                        "learned_iterations_per_step": [round(float(v), 4) for v in li.mean(0)],
                        "plain_particle_steps_per_s": round(n / (pm.mean() / 1e3), 1),
-                       "learned_particle_steps_per_s": round(n / (lm.mean() / 1e3), 1)},
+                       "learned_particle_steps_per_s": round(n / (lm.mean() / 1e3), 1),
+                       "learned_steps_using_net": int(sum(r["learned_steps_using_net"]
+                                                          for r in rows))},
         "per_scene": rows,
     }
     with open(args.eval_out, "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps({k: summary[k] for k in ("training", "evaluation")}, indent=1))
-    engine.close()
 
 
 if __name__ == "__main__":

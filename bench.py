@@ -632,7 +632,8 @@ def batch_arm(args):
                    "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
                    "launch": "eager" if args.eager else "batch graph (one branch per scene)",
                    "autotune": None if tuning is None else {
-                       k: tuning[k] for k in ("batch_ms_default", "batch_ms_tuned", "buckets",
+                       k: tuning[k] for k in ("batch_ms_default", "batch_ms_uniform",
+                                              "uniform_shape", "batch_ms_tuned", "buckets",
                                               "seconds")},
                    "graph_replays_timed": graphs1[1] - graphs0[1],
                    "mean_divergence_iterations": round(float(its[:, :, 0].mean()), 3),
@@ -892,10 +893,11 @@ def engine_arm(args):
                                    "ms_per_step": round(r["ms"] / args.steps, 4)},
                                   **accuracy_summary(r["reps"]))
         warm_info["arms"] = arm_rows
-        warm_info["gate"] = ("the network runs on a scene's first step and after every step "
-                             "whose solves went beyond their minimum iteration counts; after "
-                             "a step at the minimum counts no warm start can save an iteration, "
-                             "so it is skipped (plain warm start)")
+        warm_info["gate"] = ("the network runs on a scene's first step, then after a step "
+                             "whose solves went beyond their minimum iteration counts if its "
+                             "last outcome was no worse than the plain start's (or it has not "
+                             "run for 64 steps); at the minimum counts no warm start can save "
+                             "an iteration")
         config["learned_warm_start"] = warm_info
     if tuning is not None:
         config["autotune"] = {"seconds": tuning["seconds"], "shapes": {

@@ -700,6 +700,12 @@ typedef struct al_warm_start {
 
 /* al_df_step_f32 with the learned warm start (warm->net) and/or the
  * features of the step written out for training (warm->features_out).
+ * The engine keeps a per-scene gate on the device: the network runs on the
+ * scene's first step, then only after a step whose solves went beyond their
+ * minimum iteration counts and while its last outcome (iterations of the
+ * last step that ran it) is no worse than the plain start's last outcome,
+ * or when it has not run for 64 steps; other steps use the reference's
+ * previous-step warm starts.
  * Float32 DFSPH with the divergence solve enabled only
  * (AL_ERR_UNSUPPORTED otherwise); AL_ERR_TIMEOUT if a bounded tensor-core
  * wait gave up (the step's outputs are then invalid). */

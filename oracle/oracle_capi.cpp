@@ -227,10 +227,14 @@ void volume_field_impl(const C* cn, const B* b, TF* out) {
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t l = 0; l < int64_t(body.num_nodes); ++l) {
     V3<TF> x = node_position(body.dmin, body.res, body.cs, uint32_t(l));
-    if (body.use_grid)
-      out[l] = volume_at(c, pt, x, body.sign, [&](V3<TF> p) { return grid.value(p); });
-    else
+    if (body.use_grid) {
+      LagrangeGrid<TF> g = grid;
+      typename LagrangeGrid<TF>::Cache cache;
+      g.cache = &cache;
+      out[l] = volume_at(c, pt, x, body.sign, [&](V3<TF> p) { return g.value(p); });
+    } else {
       out[l] = volume_at(c, pt, x, body.sign, [&](V3<TF> p) { return body.sdf.sdf(p); });
+    }
   }
 }
 

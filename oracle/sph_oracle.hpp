@@ -425,6 +425,41 @@ void shape_functions(V3<TF> p, TF N[32], TF* dN0, TF* dN1, TF* dN2) {
   edge_family(24, 2, 1, 0);  // z-edges: bit1 -> y, bit2 -> x
 }
 
+// The values N of shape_functions() without derivatives, bit for bit (the
+// same rounded operations in the same order; sign factors +-1 multiply
+// exactly), with the per-axis factors formed once.  Used by the volume-map
+// integration, which evaluates 27,000 samples per node.
+template <class TF>
+inline void shape_values(V3<TF> p, TF N[32]) {
+  const TF u[3] = {p.x, p.y, p.z};
+  const TF r2 = p.x * p.x + p.y * p.y + p.z * p.z;
+  const TF c64 = TF(1) / TF(64), e64 = TF(9) / TF(64);
+  const TF f = 9 * r2 - 19;
+  TF m[3], q[3], g[3][2];
+  for (int k = 0; k < 3; ++k) {
+    m[k] = 1 - u[k];  // 1 + (-1) u
+    q[k] = 1 + u[k];
+    const TF tt = 1 - u[k] * u[k];
+    const TF t3 = 3 * u[k];
+    g[k][0] = tt * (1 - t3);  // s = -1: 1 + (-3) t
+    g[k][1] = tt * (1 + t3);
+  }
+  for (int j = 0; j < 8; ++j) {
+    const TF ax = (j & 1) ? q[0] : m[0], ay = (j & 2) ? q[1] : m[1], az = (j & 4) ? q[2] : m[2];
+    N[j] = c64 * ax * ay * az * f;
+  }
+  const int fam[3][3] = {{0, 2, 1}, {1, 0, 2}, {2, 1, 0}};  // axis, bit1 axis, bit2 axis
+  for (int fi = 0; fi < 3; ++fi) {
+    const int axis = fam[fi][0], b1 = fam[fi][1], b2 = fam[fi][2];
+    for (int e = 0; e < 8; ++e) {
+      const TF gg = g[axis][e & 1];
+      const TF a = (e & 2) ? q[b1] : m[b1];
+      const TF b = (e & 4) ? q[b2] : m[b2];
+      N[8 + 8 * fi + e] = e64 * gg * a * b;
+    }
+  }
+}
+
 // Interpolated value (interpolate, runner.hpp:1586-1594) and, optionally,
 // gradient scaled by 2 / cell size (interpolate_and_derive,
 // runner.hpp:1773-1791).  Returns FLT/DBL max outside the domain
@@ -435,17 +470,43 @@ struct LagrangeGrid {
   uint32_t res[3];
   const TF* nodes;
   TF value(V3<TF> x) const {
+    // resolve() with the reciprocal cell sizes formed once (same bits)
+    const V3<TF> inv{TF(1) / cs.x, TF(1) / cs.y, TF(1) / cs.z};
+    if (!(x.x >= dmin.x && x.y >= dmin.y && x.z >= dmin.z && dmax.x >= x.x && dmax.y >= x.y &&
+          dmax.z >= x.z))
+      return std::numeric_limits<TF>::max();
     int ip[3];
-    V3<TF> xi;
-    if (!resolve(dmin, dmax, res, cs, x, ip, xi)) return std::numeric_limits<TF>::max();
+    ip[0] = std::min(int((x.x - dmin.x) * inv.x), int(res[0]) - 1);
+    ip[1] = std::min(int((x.y - dmin.y) * inv.y), int(res[1]) - 1);
+    ip[2] = std::min(int((x.z - dmin.z) * inv.z), int(res[2]) - 1);
+    const V3<TF> lo{dmin.x + cs.x * TF(ip[0]), dmin.y + cs.y * TF(ip[1]),
+                    dmin.z + cs.z * TF(ip[2])};
+    const V3<TF> xi{2 * (x.x - lo.x) * inv.x - 1, 2 * (x.y - lo.y) * inv.y - 1,
+                    2 * (x.z - lo.z) * inv.z - 1};
     TF N[32];
-    uint32_t cells[32];
-    shape_functions<TF>(xi, N, nullptr, nullptr, nullptr);
-    cell_nodes(res, ip, cells);
+    shape_values(xi, N);
+    if (!cache || ip[0] != cache->ip[0] || ip[1] != cache->ip[1] || ip[2] != cache->ip[2]) {
+      uint32_t cells[32];
+      cell_nodes(res, ip, cells);
+      Cache local;
+      Cache& c = cache ? *cache : local;
+      for (int j = 0; j < 32; ++j) c.v[j] = nodes[cells[j]];
+      for (int k = 0; k < 3; ++k) c.ip[k] = ip[k];
+      TF phi = 0;
+      for (int j = 0; j < 32; ++j) phi += c.v[j] * N[j];
+      return phi;
+    }
     TF phi = 0;
-    for (int j = 0; j < 32; ++j) phi += nodes[cells[j]] * N[j];
+    for (int j = 0; j < 32; ++j) phi += cache->v[j] * N[j];
     return phi;
   }
+  // The node values of the last cell value() visited (consecutive samples of
+  // one volume-map node mostly fall into the same cell).
+  struct Cache {
+    int ip[3] = {-1, -1, -1};
+    TF v[32];
+  };
+  mutable Cache* cache = nullptr;
 };
 
 // ------------------------------------------------------- analytic distances
@@ -685,7 +746,9 @@ struct LazyVolume {
     const V3<TF> x = node_position(dmin, res, cs, l);
     skip = false;
     if (use_grid) {
-      const LagrangeGrid<TF> grid{dmin, dmax, cs, {res[0], res[1], res[2]}, dist_nodes};
+      LagrangeGrid<TF> grid{dmin, dmax, cs, {res[0], res[1], res[2]}, dist_nodes};
+      typename LagrangeGrid<TF>::Cache cache;
+      grid.cache = &cache;
       return volume_at(c, pt, x, sign, [&](V3<TF> p) { return grid.value(p); });
     }
     const TF d0 = sdf.sdf(x) * sign;
