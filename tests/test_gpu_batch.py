@@ -63,3 +63,44 @@ def test_batch_rejects_too_many_scenes(engine):
     arr = (_capi.SceneF32 * 1)()
     st = _capi.lib().al_df_batch_step_f32(engine.handle, arr, 257, None)
     assert st == 2  # AL_ERR_INVALID
+
+
+@pytest.mark.parametrize("shape", [None, (256, 1)])
+def test_batch_of_benchmark_scenes_matches_oracle(engine, shape):
+    """The four smallest scenes of the 64-scene benchmark batch (seeded, with
+    their rigid spheres), stepped as one batch, each against the oracle's
+    step of the same scene: equal iteration counts and the float32 one-step
+    tolerances of the single-step parity tests (the jittered start's
+    pressure kick amplifies rounding from the second step on).  With shape
+    set, the batch context runs a tuned table (other threads per particle
+    than a single step would use)."""
+    import bench
+    from alluvion_b200 import autotune
+    from test_gpu_step import TOL, _close, _oracle_run
+    specs = bench.batch_scene_specs(bench.BATCH_WORKLOADS["batch64"])
+    chosen = sorted(specs, key=lambda s: s.n)[:4]
+    batch = [s.device(engine) for s in chosen]
+    groups = _capi.tunable_groups()
+    buckets = sorted({autotune.bucket_of(sc.n) for sc in batch})
+    try:
+        if shape:
+            for b in buckets:
+                for name, pair in groups:
+                    engine.set_launch_shape(name, b, 1, shape[0], shape[1] if pair else 1)
+        sp = scenes.solver_params()
+        oracle = [_oracle_run(sc, "df", sp, 2e-4, 1) for sc in batch]
+        dts, reps, status = scenes.batch_step(engine, batch, sp, [2e-4] * len(batch))
+        assert status == [0] * len(batch)
+        tol = TOL[(np.float32, 1)]
+        for k, sc in enumerate(batch):
+            ostate, origid, odt, oreps = oracle[k]
+            assert reps[k].num_density_solve == oreps[0].num_density_solve
+            assert reps[k].num_divergence_solve == oreps[0].num_divergence_solve
+            g = sc.state()
+            _close(g["x"], ostate["x"], tol["x"], "x")
+            _close(g["v"], ostate["v"], tol["v"], "v")
+            _close(g["density"], ostate["density"], tol["density"], "density")
+    finally:
+        for b in buckets:
+            for name, _ in groups:
+                engine.set_launch_shape(name, b, 1, 0, 0)
