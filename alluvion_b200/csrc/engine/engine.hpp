@@ -133,6 +133,10 @@ struct al_engine {
   // -> (threads per block, threads per particle).  Entries override the
   // defaults; setting one invalidates the captured graphs.
   std::map<std::tuple<std::string, uint32_t, uint32_t>, std::pair<uint32_t, uint32_t>> shapes;
+  // The caller's particle_x of the last learned-warm-start step per buffer
+  // namespace: a step with other buffers is a new scene and starts its gate
+  // afresh.
+  std::unordered_map<std::string, const void*> warm_owner;
 
   // Returns a device buffer of at least `bytes` under `name`.
   int buffer(const char* name, size_t bytes, void** out);

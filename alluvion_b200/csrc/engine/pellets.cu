@@ -722,7 +722,9 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
       ALB_LAUNCH(e, "pellet_force_slots", 1, st,
                  (k_pel_force_slots<TF><<<dim3(slots, nb), 256, 0, st>>>(S, ft, chunk)));
   }
-  if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(SS));
+  if (nb)
+    ALB_LAUNCH(e, "rigid_finish", 1, st,
+               k_rigid_finish<TF><<<nb, 256, 0, st>>>(SS, SS.ft, SS.grid));
   if (np && (pel->x || pel->pressure || pel->v))
     ALB_LAUNCH(e, "pellet_outputs", 1, st,
                (k_pel_outputs<TF><<<blocks_for(np, kBlock), kBlock, 0, st>>>(

@@ -1099,6 +1099,8 @@ struct StepPlan {
   uint32_t* warm_floor = nullptr;
   // launch shapes: particle-count bucket and context of the shape table
   uint32_t bucket = 0, ctx = 0;
+  // first-stage partials of the rigid totals ([kRigidChunks][nb][6])
+  double* ftp = nullptr;
   // Shape of pass group `group` (defaults: 128-thread blocks; pair passes
   // pair_tpp(n) threads per particle, other passes one).
   LaunchShape shape(const al_engine* e, const char* group, bool pair) const {
@@ -1146,6 +1148,54 @@ int capture_while(al_engine* e, cudaStream_t st, Begin&& begin, Body&& body) {
   ALB_CUDA(end);
   return AL_OK;
 }
+
+// Adds a device-decided IF node at the current end of the capture on `st`:
+// `begin(h)` launches the kernel that sets the condition, `body(stream)`
+// launches the conditional work, captured on the engine's second stream into
+// the node's own graph.  When the condition is 0 nothing in the body runs.
+template <class Begin, class Body>
+int capture_if(al_engine* e, cudaStream_t st, Begin&& begin, Body&& body) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  ALB_CUDA(cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps));
+  cudaGraphConditionalHandle h;
+  ALB_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault));
+  ALB_TRY(begin(h));
+  ALB_CUDA(cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  ALB_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &np));
+  ALB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaStream_t bs = e->body_stream;
+  ALB_CUDA(cudaStreamBeginCaptureToGraph(bs, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  const int rc = body(bs);
+  cudaGraph_t captured = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(bs, &captured);
+  ALB_TRY(rc);
+  ALB_CUDA(end);
+  return AL_OK;
+}
+
+// Condition of the learned warm start's IF node: run the network unless the
+// gate (warm_gate_update) says this step skips it.  Also recorded in the
+// control block (the host counts the node's launches from it).
+template <class TF>
+__global__ void k_warm_if(cudaGraphConditionalHandle h, const uint32_t* __restrict__ gate,
+                          Ctrl<TF>* C) {
+  const uint32_t run = gate[0] == 0u ? 1u : 0u;
+  C->warm_ran = run;
+  cudaGraphSetConditional(h, run);
+}
+
+// Kernels inside the learned warm start's IF node (inference, application).
+constexpr uint32_t kWarmIfLaunches = 2;
 
 // Enqueues one whole step on `st`: staging uploads, grid, boundaries,
 // neighbors, the solves, write-back and the report readback.  With
@@ -1219,12 +1269,28 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                              c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
                              rho_rec, gs.flags, wd)));
     if (P.learned) {
-      ALB_LAUNCH(e, "warm_net", 1, st,
-                 ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, st,
-                                      P.warm_floor)));
-      ALB_LAUNCH(e, "warm_apply", 1, st,
-                 (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(
-                     S, P.warm_feat, P.warm_pred, P.warm_floor)));
+      // inference and its application; in a captured step they sit in an IF
+      // node, so a step whose gate is closed launches neither
+      auto infer = [&](cudaStream_t s) -> int {
+        ALB_LAUNCH(e, "warm_net", 1, s,
+                   ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, s,
+                                        P.warm_floor)));
+        ALB_LAUNCH(e, "warm_apply", 1, s,
+                   (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, s>>>(
+                       S, P.warm_feat, P.warm_pred, P.warm_floor)));
+        return AL_OK;
+      };
+      if (capture)
+        ALB_TRY(capture_if(
+            e, st,
+            [&](cudaGraphConditionalHandle h) -> int {
+              ALB_LAUNCH(e, "warm_gate", 1, st,
+                         (k_warm_if<TF><<<1, 1, 0, st>>>(h, P.warm_floor, S.ctrl)));
+              return AL_OK;
+            },
+            infer));
+      else
+        ALB_TRY(infer(st));
     }
   } else
     ALB_LAUNCH(e, "neighbors", 1, st,
@@ -1403,7 +1469,15 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
       }
     }
   }
-  if (nb) ALB_LAUNCH(e, "rigid_finish", 1, st, k_rigid_finish<TF><<<nb, 256, 0, st>>>(S));
+  if (nb) {
+    if (S.grid > kRigidChunks)
+      ALB_LAUNCH(e, "rigid_finish", 2, st,
+                 (k_rigid_partial<<<dim3(kRigidChunks, nb), 256, 0, st>>>(S.ft, S.grid, nb, P.ftp),
+                  k_rigid_finish<TF><<<nb, 256, 0, st>>>(S, P.ftp, kRigidChunks)));
+    else
+      ALB_LAUNCH(e, "rigid_finish", 1, st,
+                 k_rigid_finish<TF><<<nb, 256, 0, st>>>(S, S.ft, S.grid));
+  }
   ALB_CUDA(cudaGetLastError());
   // ---- read back: report, rigid state, anomaly flags
   ALB_CUDA(cudaMemcpyAsync(P.io.hc, S.ctrl, sizeof(Ctrl<TF>), cudaMemcpyDeviceToHost, st));
@@ -1447,7 +1521,8 @@ int capture_step(al_engine* e, StepPlan<TF>& P, cudaGraphExec_t* exec, uint32_t*
   cudaGraphDestroy(graph);
   if (inst != cudaSuccess) *exec = nullptr;
   ALB_CUDA(inst);
-  *fixed = uint32_t(captured - iteration_launches(P) * uint32_t(loops));
+  *fixed = uint32_t(captured - iteration_launches(P) * uint32_t(loops) -
+                    (P.learned ? kWarmIfLaunches : 0u));
   return AL_OK;
 }
 
@@ -1564,6 +1639,7 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   ALB_TRY(e->buf("bodies", nb ? nb : 1, &P.bodies_dev));
   ALB_TRY(e->buf("rigid", nb ? nb : 1, &S.rigid));
   ALB_TRY(e->buf("ft", size_t(S.grid) * (nb ? nb : 1) * 6, &S.ft));
+  ALB_TRY(e->buf("ftp", size_t(kRigidChunks) * (nb ? nb : 1) * 6, &P.ftp));
   ALB_TRY(e->buf("red", S.grid, &S.red));
   ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
   S.bodies = P.bodies_dev;
@@ -1582,7 +1658,13 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
       ALB_TRY(e->buf("warm.pred", size_t(n) * AL_WARM_NUM_OUTPUTS, &P.warm_pred));
       bool fresh = false;
       ALB_TRY(e->buf("warm.floor", 4, &P.warm_floor, &fresh));
-      if (fresh) ALB_CUDA(cudaMemset(P.warm_floor, 0, 4 * sizeof(uint32_t)));
+      // the gate belongs to a scene: other caller buffers than last time
+      // (or a new gate buffer) start it afresh
+      const void*& owner = e->warm_owner[e->ns];
+      if (fresh || owner != static_cast<const void*>(A.f->particle_x)) {
+        ALB_CUDA(cudaMemset(P.warm_floor, 0, 4 * sizeof(uint32_t)));
+        owner = A.f->particle_x;
+      }
     }
   }
   // ---- host staging: control block, bodies, rigid state
@@ -1717,7 +1799,8 @@ int run_step(al_engine* e, int method, const typename FluidT<TF>::cn* cn, const 
   if (graph)
     e->launches += graph->fixed_launches +
                    uint64_t(iteration_launches(P)) *
-                       (uint64_t(r.num_divergence_solve) + r.num_density_solve);
+                       (uint64_t(r.num_divergence_solve) + r.num_density_solve) +
+                   (P.learned && P.io.hc->warm_ran ? kWarmIfLaunches : 0u);
   return finish_step<TF>(A, P);
 }
 

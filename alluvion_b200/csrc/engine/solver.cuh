@@ -38,6 +38,7 @@ struct Ctrl {
   uint32_t keep_going;  // 1 while the running solve must iterate again
   uint32_t ticket;      // last-block ticket of grid reductions
   uint32_t integrate_rigids;
+  uint32_t warm_ran;    // 1 when the learned warm start's network ran this step
   double mean;          // latest mean of the running solve
   unsigned long long vmax_bits;  // max |v + a dt|^2 as ordered bits
   TF pile_gravity[3];

@@ -49,6 +49,7 @@ __global__ void k_step_init(StepState<TF> S) {
   if (threadIdx.x == 0) {
     C.ticket = 0;
     C.vmax_bits = 0;
+    C.warm_ran = 0;
     C.it = 0;
     C.keep_going = 0;
     C.mean = 0;
@@ -123,14 +124,42 @@ __device__ __forceinline__ void apply_update_dt(Ctrl<TF>& C, TF pmax) {
   C.dt = ndt;
 }
 
+// First stage of the per-body rigid totals for large grids: block (c, b)
+// sums body b's slots of the c-th contiguous chunk of the [grid][nb][6]
+// slots, in a fixed order, into slot c of `part` (same layout, gridDim.x
+// slots).  Deterministic: the chunking depends on `grid` only.
+constexpr uint32_t kRigidChunks = 128;
+
+__global__ void k_rigid_partial(const double* __restrict__ ft, uint32_t grid, uint32_t nb,
+                                double* __restrict__ part) {
+  const uint32_t b = blockIdx.y, c = blockIdx.x;
+  const uint32_t len = (grid + gridDim.x - 1) / gridDim.x;
+  const uint32_t lo = c * len, hi = min(lo + len, grid);
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t g = lo + threadIdx.x; g < hi; g += blockDim.x) {
+    const double* slot = ft + (size_t(g) * nb + b) * 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] += slot[k];
+  }
+  double tot[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) tot[k] = block_sum_double(acc[k]);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) part[(size_t(c) * nb + b) * 6 + k] = tot[k];
+  }
+}
+
 // Per-body totals of the rigid slots (solver_df.hpp:346-353) in double and
-// Pile::integrate_kinematics (pile.hpp:794-815).  One block per body.
+// Pile::integrate_kinematics (pile.hpp:794-815).  One block per body, over
+// `nslots` slots of `slots` ([nslots][nb][6]).
 template <class TF>
-__global__ void k_rigid_finish(StepState<TF> S) {
+__global__ void k_rigid_finish(StepState<TF> S, const double* __restrict__ slots,
+                               uint32_t nslots) {
   const uint32_t b = blockIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t g = threadIdx.x; g < S.grid; g += blockDim.x) {
-    const double* slot = S.ft + (size_t(g) * S.nb + b) * 6;
+  for (uint32_t g = threadIdx.x; g < nslots; g += blockDim.x) {
+    const double* slot = slots + (size_t(g) * S.nb + b) * 6;
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc[k] += slot[k];
   }

@@ -374,14 +374,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes per particle of the dominant pass from the committed ncu
-    summary (profiles/traffic.json), or None."""
+def committed_traffic(workload, pass_name):
+    """DRAM bytes per launch of `pass_name` on `workload` from the committed
+    ncu captures (profiles/traffic.json), or None when that workload and
+    pass were not captured."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            return json.load(f)
-    return None
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        entry = json.load(f).get("workloads", {}).get(workload, {}).get(pass_name)
+    return None if entry is None else float(entry["dram_bytes_per_launch"])
 
 
 L2_BYTES = 126 * 2 ** 20
@@ -804,7 +806,7 @@ def fp64_error(engine, args, sp, steps):
     return out
 
 
-def roofline_of(out, n, flush):
+def roofline_of(out, n, flush, workload):
     """Roofline of the arm's dominant pass: Model-A bytes of one launch over
     its CUDA-event time per launch."""
     per_launch = {}
@@ -817,12 +819,8 @@ def roofline_of(out, n, flush):
     bpp, bpair = MODEL_A[dominant]
     alg_bytes = bpp * n + bpair * out["pairs"]
     achieved = alg_bytes / (per_launch[dominant] / 1e3) / 1e9
-    traffic = committed_traffic()
-    tr = None
-    # the committed figure is per particle of a working set larger than L2;
-    # it scales with the particle count only while the step stays DRAM-resident
-    if traffic and traffic.get("pass") == dominant and not flush:
-        tr = traffic.get("dram_bytes_per_particle", 0) * n
+    # the capture of this workload's own dominant pass (no L2 flush variant)
+    tr = None if flush else committed_traffic(workload, dominant)
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": tr, "kernel": dominant,
             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": int(alg_bytes),
@@ -873,7 +871,9 @@ def engine_arm(args):
         res[name] = time_arm(engine, scene, sp, args, warm, world, local, torch,
                              want_e2e=name == primary, clocks_on=name == primary)
     main_ = res[primary]
-    roofline = roofline_of(main_, n, main_["flush"])
+    roofline = roofline_of(main_, n, main_["flush"], args.workload)
+    if args.rigid_bodies == 0 or args.container_resolution or args.method != "df":
+        roofline["traffic"] = None  # the captures are of the default DFSPH scenes
     bodies_desc = ", seeded rigid bodies" if scene.num_boundaries > 1 else ""
     l2 = ("working set > 126 MB L2 (inputs larger than L2, no flush)" if not main_["flush"] else
           "working set < L2: a 252 MB buffer is rewritten before every timed step (untimed)")

@@ -102,3 +102,39 @@ def test_graph_respects_profiling(engine):
         engine.reset_stats()
     assert (c1 - c0, r1 - r0) == (0, 0)
     assert stats["neighbors"][1] == 3
+
+
+def test_learned_warm_start_graph_matches_eager(engine):
+    """The learned warm start's inference sits in a conditional IF node of
+    the captured step (launched only when the per-scene gate is open); the
+    eager path launches the kernels, which return at once when it is closed.
+    Both take the same gate decisions, so every output is bit-identical, and
+    a captured step launches at most one kernel more than an eager one (the
+    node's condition) and two fewer when the gate is closed."""
+    import os
+    from alluvion_b200 import warm_start
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "alluvion_b200", "data", "warm_start_dambreak.npz")
+    net = warm_start.WarmStartNet.load(path)
+    out = {}
+    for graph in (False, True):
+        engine.set_graph_mode(graph)
+        scene = _scene(engine, np.float32, seed=13)
+        n0 = engine.launch_count()
+        c0, r0 = engine.graph_stats()
+        dt = 1e-4
+        reps = []
+        for k in range(8):
+            sp = scenes.solver_params(max_dt=4e-4 if k < 4 else 2e-4)
+            dt, rep = scene.step("df", sp, dt, warm=net.warm_start())
+            reps.append((dt, rep.num_divergence_solve, rep.num_density_solve,
+                         rep.mean_density_change, rep.mean_density_error))
+        torch.cuda.synchronize()
+        out[graph] = dict(state=scene.state(), reps=reps, launches=engine.launch_count() - n0,
+                          replays=engine.graph_stats()[1] - r0)
+    engine.set_graph_mode(True)
+    assert out[True]["replays"] >= 4
+    assert out[False]["reps"] == out[True]["reps"]
+    for k in out[False]["state"]:
+        np.testing.assert_array_equal(out[True]["state"][k], out[False]["state"][k], err_msg=k)
+    assert out[True]["launches"] <= out[False]["launches"] + 8
