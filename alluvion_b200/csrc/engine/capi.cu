@@ -382,7 +382,7 @@ int update_neighbors_impl(al_engine* e, const C* cn, const al_consti* cni, const
   vec4<TF>* xs = nullptr;
   uint32_t *flags = nullptr, *nbr = nullptr, *ncount = nullptr;
   TF* rho = nullptr;
-  ALB_TRY(e->buf("sorted.x", n, &xs));
+  ALB_TRY(e->buf("sorted.x", size_t(n) + kSortedPad, &xs));
   ALB_TRY(e->buf("flags", 4, &flags));
   ALB_TRY(e->buf("nbr.list", size_t(n) * g.cap_nbr, &nbr));
   ALB_TRY(e->buf("nbr.count", n, &ncount));

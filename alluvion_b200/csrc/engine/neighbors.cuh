@@ -18,6 +18,12 @@
 
 namespace alb {
 
+// Spare entries after the n sorted positions that the build reads: its scan
+// loads candidates in rounds of up to 8 and may read past a row's last
+// candidate (the extra bits are masked off), so every sorted-position
+// buffer passed to the build holds n + kSortedPad entries.
+constexpr uint32_t kSortedPad = 8;
+
 // Boundary kernel terms {grad W * V, W * V} in the reference's
 // [nb][N][4] layout (original particle order); used by the standalone
 // update_particle_neighbors entry point.

@@ -1615,7 +1615,7 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   if (S.grid == 0) S.grid = 1;
   // ---- buffers
   ALB_TRY(e->buf("flags", 4, &P.flags));
-  ALB_TRY(e->buf("sorted.x", n, &S.x));
+  ALB_TRY(e->buf("sorted.x", size_t(n) + kSortedPad, &S.x));
   ALB_TRY(e->buf("sorted.rec", size_t(n) * 2, &S.rec));
   ALB_TRY(e->buf("sorted.a", n, &S.a));
   ALB_TRY(e->buf("sorted.rho", n, &S.rho));
