@@ -299,6 +299,7 @@ _SIGNATURES = {
     "al_copy": (ctypes.c_int, [_P, _P, _P, ctypes.c_size_t]),
     "al_set": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_size_t]),
     "al_engine_set_graph_mode": (ctypes.c_int, [_P, ctypes.c_int]),
+    "al_engine_set_batch_fused": (ctypes.c_int, [_P, ctypes.c_int]),
     "al_engine_set_launch_shape": (ctypes.c_int, [_P, ctypes.c_char_p, _U, _U, _U, _U]),
     "al_engine_get_launch_shape": (ctypes.c_int, [_P, ctypes.c_char_p, _U, _U, _P, _P]),
     "al_tunable_group": (ctypes.c_int, [_U, ctypes.POINTER(ctypes.c_char_p), _P]),
@@ -447,6 +448,13 @@ class Engine:
         check(lib().al_engine_set_launch_shape(self.handle, group.encode(), int(bucket),
                                                int(batch), int(block), int(tpp)),
               "al_engine_set_launch_shape")
+
+    def set_batch_fused(self, enable):
+        """Batched steps run fused (one launch per solver pass over all scenes,
+        where the scenes allow it) or as one graph branch per scene (the
+        default)."""
+        check(lib().al_engine_set_batch_fused(self.handle, 1 if enable else 0),
+              "al_engine_set_batch_fused")
 
     def launch_shape(self, group, num_particles, batch=0):
         """(block, threads per particle) a step of num_particles would use."""

@@ -111,9 +111,10 @@ __global__ void __launch_bounds__(kBlock)
     k_sample_boundaries(Cn<TF> c, const BodyDev<TF>* __restrict__ bodies,
                         const RigidDev<TF>* __restrict__ rigid, uint32_t nb,
                         const vec4<TF>* __restrict__ xs, const uint32_t* __restrict__ perm,
-                        uint32_t n, uint32_t* __restrict__ mask, vec4<TF>* __restrict__ bx,
-                        vec4<TF>* __restrict__ bk, TF* __restrict__ ref_b,
-                        TF* __restrict__ ref_k, uint32_t* __restrict__ active) {
+                        uint32_t n, uint32_t stride, uint32_t* __restrict__ mask,
+                        vec4<TF>* __restrict__ bx, vec4<TF>* __restrict__ bk,
+                        TF* __restrict__ ref_b, TF* __restrict__ ref_k,
+                        uint32_t* __restrict__ active) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const vec3<TF> x = xyz(xs[s]);
@@ -125,8 +126,8 @@ __global__ void __launch_bounds__(kBlock)
     if (bnd.w != TF(0)) {
       m |= 1u << b;
       if (bx) {
-        bx[size_t(b) * n + s] = bnd;
-        bk[size_t(b) * n + s] = kk;
+        bx[size_t(b) * stride + s] = bnd;
+        bk[size_t(b) * stride + s] = kk;
       }
     }
     if (ref_b) {
@@ -237,8 +238,8 @@ int sample_boundaries(const Cn<TF>& c, const BodyDev<TF>* bodies_dev, const Rigi
                       cudaStream_t st) {
   if (n == 0) return AL_OK;
   k_sample_boundaries<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(
-      c, bodies_dev, rigid_dev, nb, xs, perm, n, bs.mask, bs.bx, bs.bk, ref_boundary, ref_kernel,
-      bs.active);
+      c, bodies_dev, rigid_dev, nb, xs, perm, n, bs.stride ? bs.stride : n, bs.mask, bs.bx, bs.bk,
+      ref_boundary, ref_kernel, bs.active);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }

@@ -96,6 +96,7 @@ struct BoundaryState {
   vec4<TF>* bx = nullptr;    // [nb][n] {x_b, V}
   vec4<TF>* bk = nullptr;    // [nb][n] {grad W * V, W * V}
   uint32_t* active = nullptr;  // optional counter += number of set mask bits
+  uint32_t stride = 0;         // row stride of bx / bk (0: n)
 };
 
 // Samples every body for every sorted particle (positions xs).  When

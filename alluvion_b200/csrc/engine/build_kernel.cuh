@@ -51,11 +51,16 @@ static_assert(32 % kScan == 0 && kScan <= kSortedPad,
 // `EX` adds one more sum over the list to phase 2 (EX::kOn): it supplies
 // the particle's and the neighbors' velocities and receives
 // sum_j V (v_i - v_j) . grad W_ij, in list order, at the end.
+//
+// The list is slot-major with row stride `stride` (n for one scene) and
+// holds sorted slots plus `base` (0 for one scene; a fused batch's scene
+// stores its slots in the shared arena, offset by its first slot).
 template <class TF, class BK, bool FACTOR, class EX, bool WR = false>
 __global__ void __launch_bounds__(kMaxBlock)
     k_build_neighbors(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
-                      const vec4<TF>* __restrict__ xs, uint32_t n, BK bk,
-                      uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount,
+                      const vec4<TF>* __restrict__ xs, uint32_t n, uint32_t stride,
+                      uint32_t base, BK bk, uint32_t* __restrict__ nbr,
+                      uint32_t* __restrict__ ncount,
                       TF* __restrict__ rho, TF* __restrict__ alpha, TF* __restrict__ rho_rec,
                       uint32_t* __restrict__ flags, EX ex) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
@@ -106,7 +111,8 @@ __global__ void __launch_bounds__(kMaxBlock)
           if (m < 32) acc &= (1u << m) - 1u;
           if (s - t0 < m) acc &= ~(1u << (s - t0));  // the particle itself
           for (; acc; acc &= acc - 1) {
-            if (cnt < g.cap_nbr) nbr[size_t(cnt) * n + s] = t0 + uint32_t(__ffs(acc) - 1);
+            if (cnt < g.cap_nbr)
+              nbr[size_t(cnt) * stride + s] = base + t0 + uint32_t(__ffs(acc) - 1);
             ++cnt;
           }
         }
@@ -129,7 +135,7 @@ __global__ void __launch_bounds__(kMaxBlock)
     uint32_t t[kB];
 #pragma unroll
     for (uint32_t q = 0; q < kB; ++q)  // this thread's own stores: plain loads
-      t[q] = k0 + q < cnt ? nbr[size_t(k0 + q) * n + s] : s;
+      t[q] = k0 + q < cnt ? nbr[size_t(k0 + q) * stride + s] - base : s;
     vec3<TF> xj[kB], vj[kB];
 #pragma unroll
     for (uint32_t q = 0; q < kB; ++q) {

@@ -124,6 +124,12 @@ struct al_engine {
   cudaEvent_t fork_event = nullptr;
   int branches(uint32_t count);  // creates streams / events up to `count`
   std::string ns;
+  // Batched steps run fused (one launch per solver pass over all scenes)
+  // when enabled (al_engine_set_batch_fused) and their scenes allow it; the
+  // block -> scene tables last uploaded for a fused batch, with their
+  // buffers.
+  bool batch_fused = false;
+  std::vector<unsigned char> fused_tables;
   // pinned host staging (control readback, reports)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

@@ -48,25 +48,27 @@ __global__ void k_export_neighbors(Cn<TF> c, uint32_t cap, uint32_t n,
 template <class TF, class BK>
 int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState& gs,
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
-                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st) {
+                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st, uint32_t stride,
+                            uint32_t base) {
   if (gs.n == 0) return AL_OK;
   const uint32_t blocks = blocks_for(gs.n, kBlock);
+  if (stride == 0) stride = gs.n;
   // compile-time wrap flag: the non-periodic build carries no wrap branches
   if (alpha && c.wrap)
     k_build_neighbors<TF, BK, true, NoExtra<TF>, true><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
         NoExtra<TF>{});
   else if (alpha)
     k_build_neighbors<TF, BK, true, NoExtra<TF>, false><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
         NoExtra<TF>{});
   else if (c.wrap)
     k_build_neighbors<TF, BK, false, NoExtra<TF>, true><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
         NoExtra<TF>{});
   else
     k_build_neighbors<TF, BK, false, NoExtra<TF>, false><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
         NoExtra<TF>{});
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
@@ -89,7 +91,7 @@ int export_neighbors(const Cn<TF>& c, const GridDims& g, const GridState& gs,
 #define ALB_INST(TF, BK)                                                                  \
   template int build_neighbors_density<TF, BK<TF>>(                                       \
       const Cn<TF>&, const GridDims&, const GridState&, const vec4<TF>*, const BK<TF>&,    \
-      uint32_t*, uint32_t*, TF*, TF*, TF*, cudaStream_t);
+      uint32_t*, uint32_t*, TF*, TF*, TF*, cudaStream_t, uint32_t, uint32_t);
 ALB_INST(float, RefBoundaryKernel)
 ALB_INST(double, RefBoundaryKernel)
 ALB_INST(float, SortedBoundaryKernel)

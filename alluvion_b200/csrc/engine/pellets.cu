@@ -674,6 +674,7 @@ int pellet_step(al_engine* e, const typename PelletTypes<TF>::cn* cn, const al_c
   // the shared kernels' view of the step
   StepState<TF> SS;
   SS.n = n;
+  SS.ls = n;
   SS.nb = nb;
   SS.grid = slots;
   SS.ft = ft;

@@ -67,8 +67,8 @@ __device__ __forceinline__ void gXV(const StepState<double>& S, uint32_t t, vec4
 // force/torque slot: warp trees, then warp partials in warp order.  All
 // threads of the block call it.  Deterministic.
 template <class TF>
-__device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b, vec3<TF> f,
-                                             vec3<TF> t) {
+__device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t bid, uint32_t b,
+                                             vec3<TF> f, vec3<TF> t) {
   __shared__ double part[6][kMaxBlock / 32];
   double v[6] = {double(f.x), double(f.y), double(f.z), double(t.x), double(t.y), double(t.z)};
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -82,9 +82,14 @@ __device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b,
   if (threadIdx.x < 6) {
     double s = 0;
     for (int w = 0; w < int(blockDim.x >> 5); ++w) s += part[threadIdx.x][w];
-    S.ft[(size_t(blockIdx.x) * S.nb + b) * 6 + threadIdx.x] += s;
+    S.ft[(size_t(bid) * S.nb + b) * 6 + threadIdx.x] += s;
   }
   __syncthreads();
+}
+template <class TF>
+__device__ __forceinline__ void block_add_ft(const StepState<TF>& S, uint32_t b, vec3<TF> f,
+                                             vec3<TF> t) {
+  block_add_ft(S, blockIdx.x, b, f, t);
 }
 
 // Pair passes run `tpp` threads per particle (1, 2, 4 or 8, chosen per
@@ -132,16 +137,58 @@ struct Lane {
   __device__ __forceinline__ bool lead() const { return act && sub == 0; }
 };
 
+// A pass block's place in its scene: the scene, the block's index among
+// the scene's blocks, their count, the end of the scene's particle range and
+// its particle count.  A one-scene launch is all one scene.
+struct BlockSpan {
+  uint32_t k, bid, nblk, end, n;
+};
+
+// With BT (a pass launched over every scene of a fused batch) narrows S to
+// the block's scene: its control block and reduction partials.  False for
+// a block past every scene.
+template <bool BT, class TF>
+__device__ __forceinline__ bool block_scene(StepState<TF>& S, BlockSpan& B) {
+  if constexpr (BT) {
+    const uint32_t k = __ldg(S.blk_scene + blockIdx.x);
+    if (k >= S.nscenes) return false;
+    const FusedScene<TF>& f = S.fused[k];
+    S.ctrl = f.ctrl;
+    S.red = f.red;
+    B = BlockSpan{k, blockIdx.x - f.blk0, f.nblk, f.s0 + f.n, f.n};
+  } else {
+    B = BlockSpan{0, blockIdx.x, gridDim.x, S.n, S.n};
+  }
+  return true;
+}
+
+// The rest of the narrowing of block_scene: the scene's bodies, rigid state
+// and rigid slots (loaded where a pass reaches its boundary terms).
+template <bool BT, class TF>
+__device__ __forceinline__ void scene_bodies(StepState<TF>& S, const BlockSpan& B) {
+  if constexpr (BT) {
+    const FusedScene<TF>& f = S.fused[B.k];
+    S.bodies = f.bodies;
+    S.rigid = f.rigid;
+    S.ft = f.ft;
+    S.nb = f.nb;
+  }
+}
+
 template <class TF>
-__device__ __forceinline__ Lane pair_lane(const StepState<TF>& S) {
+__device__ __forceinline__ Lane pair_lane(const StepState<TF>& S, const BlockSpan& B) {
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t shift = __ffs(S.tpp) - 1;
   Lane l;
   l.tpp = S.tpp;
   l.s = g >> shift;
   l.sub = g & (S.tpp - 1);
-  l.act = l.s < S.n;
+  l.act = l.s < B.end;
   return l;
+}
+template <class TF>
+__device__ __forceinline__ Lane pair_lane(const StepState<TF>& S) {
+  return pair_lane(S, BlockSpan{0, blockIdx.x, gridDim.x, S.n, S.n});
 }
 
 inline uint32_t pair_blocks(uint32_t n, uint32_t tpp, uint32_t block = kBlock) {
@@ -162,7 +209,7 @@ __device__ __forceinline__ vec3<TF> group_sum(vec3<TF> v, const Lane& L) {
 
 template <class TF>
 __device__ __forceinline__ uint32_t nbr_at(const StepState<TF>& S, uint32_t k, uint32_t s) {
-  return __ldcs(S.nbr + size_t(k) * S.n + s);
+  return __ldcs(S.nbr + size_t(k) * S.ls + s);
 }
 
 // Visits the lane's neighbors k = sub, sub + tpp, ... < cnt in batches of
@@ -221,8 +268,8 @@ __device__ __forceinline__ TF velocity_divergence(const Cn<TF>& c, const StepSta
   if (L.act) {
     for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
-      const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
+      const vec4<TF> bn = S.bx[size_t(b) * S.ls + L.s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.ls + L.s];
       const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
       acc += dot(vi - vj, xyz(kg));
     }
@@ -292,8 +339,8 @@ struct WarmDivergence {
     TF acc = o.div, bvol = 0, bden = 0;
     for (uint32_t m = S.mask[s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + s];
-      const vec4<TF> kg = S.bk[size_t(b) * S.n + s];
+      const vec4<TF> bn = S.bx[size_t(b) * S.ls + s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.ls + s];
       acc += dot(o.vi - body_velocity(S.rigid[b], xyz(bn)), xyz(kg));
       bvol += bn.w;
       bden += kg.w;
@@ -377,11 +424,16 @@ enum KappaMode { kDivWarm = 0, kDivIter = 1, kPressWarm = 2, kPressIter = 3 };
 // The float kernel is held at 56 registers (9 resident 128-thread blocks
 // per SM; with 256-thread launch bounds the compiler took 58, and the
 // 256-register allocation granule then allows only 8); double needs more.
-template <class TF, int MODE, bool WR = false>
+template <class TF, int MODE, bool WR = false, bool BT = false>
 __global__ void __maxnreg__(sizeof(TF) == 4 ? 56 : 128) k_kappa(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   constexpr bool kDiv = MODE == kDivWarm || MODE == kDivIter;
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  // a scene of a fused batch whose solve has converged sits out the
+  // remaining iterations of the others
+  if (BT && (MODE == kDivIter || MODE == kPressIter) && !S.ctrl->keep_going) return;
+  const Lane L = pair_lane(S, B);
   const TF dt = S.ctrl->dt;
   TF ki = 0;
   vec3<TF> dv{0, 0, 0};
@@ -406,20 +458,21 @@ __global__ void __maxnreg__(sizeof(TF) == 4 ? 56 : 128) k_kappa(Cn<TF> c, StepSt
     }
   });
   dv = group_sum(dv, L);
+  scene_bodies<BT>(S, B);
   const uint32_t m = (L.lead() && fabs(ki) > c.eps) ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
     if (!__syncthreads_or(mine)) continue;
     vec3<TF> f{0, 0, 0}, tq{0, 0, 0};
     if (mine) {
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
-      const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
+      const vec4<TF> bn = S.bx[size_t(b) * S.ls + L.s];
+      const vec4<TF> kg = S.bk[size_t(b) * S.ls + L.s];
       const vec3<TF> a = ki * (-xyz(kg));
       f = c.mass * a;
       dv -= dt * a;
       tq = cross(xyz(bn) - S.rigid[b].x, f);
     }
-    block_add_ft(S, b, f, tq);
+    block_add_ft(S, B.bid, b, f, tq);
   }
   if (L.lead()) {
     if (MODE == kDivIter) S.kappa_v[L.s] += ki;
@@ -431,10 +484,13 @@ __global__ void __maxnreg__(sizeof(TF) == 4 ? 56 : 128) k_kappa(Cn<TF> c, StepSt
 
 // compute_velocity_of_density_change (runner.hpp:3297-3314); also forms
 // k = rho_adv * alpha for the first divergence iteration.
-template <class TF, bool WR = false>
+template <class TF, bool WR = false, bool BT = false>
 __global__ void __launch_bounds__(kMaxBlock) k_df_rho_adv_init(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  scene_bodies<BT>(S, B);
+  const Lane L = pair_lane(S, B);
   const TF adv = density_change(c, S, L);
   if (!L.lead()) return;
   const TF dt = S.ctrl->dt;
@@ -446,11 +502,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_df_rho_adv_init(Cn<TF> c, StepSta
 
 // compute_divergence_solve_density_error (runner.hpp:3396-3410) with the
 // mean of solver_df.hpp:160-161 reduced in double on the device.
-template <class TF, bool WR = false>
+template <class TF, bool WR = false, bool BT = false>
 __global__ void __launch_bounds__(kMaxBlock)
     k_df_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  if (BT && !S.ctrl->keep_going) return;
+  scene_bodies<BT>(S, B);
+  const Lane L = pair_lane(S, B);
   const TF adv = density_change(c, S, L);
   double val = 0;
   if (L.lead()) {
@@ -459,19 +519,24 @@ __global__ void __launch_bounds__(kMaxBlock)
     val = double(adv);
   }
   double total;
-  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total) && threadIdx.x == 0)
-    finish_iteration(*S.ctrl, total, S.n, 0, handle, use_handle);
+  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total, B.bid, B.nblk) && threadIdx.x == 0)
+    finish_iteration(*S.ctrl, total, B.n, 0, handle, use_handle);
 }
 
 // clear_acceleration + compute_viscosity (runner.hpp:1974-1980, 2150-2249),
 // divergence_solve_finish (runner.hpp:3412-3420) when `finish_div`, and
 // calculate_cfl_v2 (runner.hpp:2533-2541) reduced to the global max; the
 // last block applies Solver::update_dt (solver.hpp:153-169).
-template <class TF, bool WR = false>
-__global__ void __launch_bounds__(kMaxBlock)
+//
+// The float kernel is held at 64 registers (8 resident 128-thread blocks per
+// SM): a fused batch's scene lookups would otherwise take it to 76.
+template <class TF, bool WR = false, bool BT = false>
+__global__ void __launch_bounds__(kMaxBlock, sizeof(TF) == 4 ? 4 : 1)
     k_viscosity(Cn<TF> c, StepState<TF> S, int finish_div) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  const Lane L = pair_lane(S, B);
   const TF dt = S.ctrl->dt;
   vec3<TF> xi{0, 0, 0}, vi{0, 0, 0}, da{0, 0, 0};
   uint32_t cnt = 0;
@@ -487,13 +552,14 @@ __global__ void __launch_bounds__(kMaxBlock)
           (vi - xyz(vj));
   });
   da = group_sum(da, L);
+  scene_bodies<BT>(S, B);
   const uint32_t m = L.lead() ? S.mask[L.s] : 0u;
   for (uint32_t b = 0; b < S.nb; ++b) {
     const bool mine = (m >> b) & 1u;
     if (!__syncthreads_or(mine)) continue;
     vec3<TF> fsum{0, 0, 0}, tsum{0, 0, 0};
     if (mine) {
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
+      const vec4<TF> bn = S.bx[size_t(b) * S.ls + L.s];
       const vec3<TF> bxj = xyz(bn);
       const RigidDev<TF> rg = S.rigid[b];
       vec3<TF> nrm = bxj - xi;
@@ -529,7 +595,7 @@ __global__ void __launch_bounds__(kMaxBlock)
         }
       }
     }
-    block_add_ft(S, b, fsum, tsum);
+    block_add_ft(S, B.bid, b, fsum, tsum);
   }
   TF v2 = 0;
   if (L.lead()) {
@@ -558,7 +624,7 @@ __global__ void __launch_bounds__(kMaxBlock)
       bits = (unsigned long long)__double_as_longlong(bm);
     atomicMax(&S.ctrl->vmax_bits, bits);
     __threadfence();
-    last = atomicAdd(&S.ctrl->ticket, 1u) == gridDim.x - 1;
+    last = atomicAdd(&S.ctrl->ticket, 1u) == B.nblk - 1;
   }
   __syncthreads();
   if (last && threadIdx.x == 0) {
@@ -576,10 +642,11 @@ __global__ void __launch_bounds__(kMaxBlock)
 }
 
 // integrate_non_pressure_acceleration (runner.hpp:3422-3428).
-template <class TF>
+template <class TF, bool BT = false>
 __global__ void k_integrate_np(StepState<TF> S) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
+  BlockSpan B;
+  if (!block_scene<BT>(S, B) || s >= B.end) return;
   const TF dt = S.ctrl->dt;
   const vec4<TF> a = S.a[s];
   const vec4<TF> v = RV(S, s);
@@ -590,12 +657,15 @@ __global__ void k_integrate_np(StepState<TF> S) {
 // With `pred` (learned warm start) the predicted kappa replaces the
 // previous-step value under the same gate (rho_adv > 1), unless the floor
 // gate is set.
-template <class TF, bool WR = false>
+template <class TF, bool WR = false, bool BT = false>
 __global__ void __launch_bounds__(kMaxBlock)
     k_p_warm0(Cn<TF> c, StepState<TF> S, const float* __restrict__ pred,
               const uint32_t* __restrict__ floor) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  scene_bodies<BT>(S, B);
+  const Lane L = pair_lane(S, B);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
@@ -609,10 +679,13 @@ __global__ void __launch_bounds__(kMaxBlock)
 }
 
 // compute_rho_adv (runner.hpp:3525-3541); also k for the first iteration.
-template <class TF, bool WR = false>
+template <class TF, bool WR = false, bool BT = false>
 __global__ void __launch_bounds__(kMaxBlock) k_p_rho_adv_init(Cn<TF> c, StepState<TF> S) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  scene_bodies<BT>(S, B);
+  const Lane L = pair_lane(S, B);
   const TF dt = S.ctrl->dt;
   const TF adv = density_adv(c, S, L, dt);
   if (!L.lead()) return;
@@ -624,11 +697,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_p_rho_adv_init(Cn<TF> c, StepStat
 
 // compute_pressure_solve_density_error (runner.hpp:3590-3604); the mean is
 // sum(rho_adv - 1) / N in double (solver_df.hpp:323-325 forms sum/N - 1).
-template <class TF, bool WR = false>
+template <class TF, bool WR = false, bool BT = false>
 __global__ void __launch_bounds__(kMaxBlock)
     k_p_residual(Cn<TF> c, StepState<TF> S, cudaGraphConditionalHandle handle, int use_handle) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const Lane L = pair_lane(S);
+  BlockSpan B;
+  if (!block_scene<BT>(S, B)) return;
+  if (BT && !S.ctrl->keep_going) return;
+  scene_bodies<BT>(S, B);
+  const Lane L = pair_lane(S, B);
   const TF adv = density_adv(c, S, L, S.ctrl->dt);
   double val = 0;
   if (L.lead()) {
@@ -637,8 +714,8 @@ __global__ void __launch_bounds__(kMaxBlock)
     val = double(adv) - 1.0;
   }
   double total;
-  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total) && threadIdx.x == 0)
-    finish_iteration(*S.ctrl, total, S.n, 1, handle, use_handle);
+  if (grid_sum_last(val, S.red, &S.ctrl->ticket, &total, B.bid, B.nblk) && threadIdx.x == 0)
+    finish_iteration(*S.ctrl, total, B.n, 1, handle, use_handle);
 }
 
 // pressure_solve_finish + integrate_velocity<0> (runner.hpp:3606-3623),
@@ -702,7 +779,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_ii_predict0(Cn<TF> c, StepState<T
   RX(S, L.s).w = lp;  // pressure read by the first iteration
   for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
-    const vec4<TF> kg = S.bk[size_t(b) * S.n + L.s];
+    const vec4<TF> kg = S.bk[size_t(b) * S.ls + L.s];
     dii -= vec3<TF>{kg.x / rho2, kg.y / rho2, kg.z / rho2};
   }
   dii = dii * c.rho0;
@@ -739,8 +816,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_ii_predict1(Cn<TF> c, StepState<T
   adv += rho / c.rho0;
   for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
-    const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
-    const vec3<TF> gw = xyz(S.bk[size_t(b) * S.n + L.s]);
+    const vec4<TF> bn = S.bx[size_t(b) * S.ls + L.s];
+    const vec3<TF> gw = xyz(S.bk[size_t(b) * S.ls + L.s]);
     const vec3<TF> vj = body_velocity(S.rigid[b], xyz(bn));
     const vec3<TF> dji = (inv_rho2 * c.rho0) * gw;
     adv += dt * dot(vi - vj, gw);
@@ -811,7 +888,7 @@ __global__ void __launch_bounds__(kMaxBlock)
   if (L.lead()) {
     for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
       const uint32_t b = __ffs(m) - 1;
-      sum += dot(dij_pj, xyz(S.bk[size_t(b) * S.n + L.s]));
+      sum += dot(dij_pj, xyz(S.bk[size_t(b) * S.ls + L.s]));
     }
     sum *= c.rho0;
     const TF bterm = TF(1) - S.rho_adv[L.s];
@@ -862,8 +939,8 @@ __global__ void __launch_bounds__(kMaxBlock)
     if (!__syncthreads_or(mine)) continue;
     vec3<TF> f{0, 0, 0}, tq{0, 0, 0};
     if (mine) {
-      const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
-      const vec3<TF> a = (c.rho0 * dpi) * xyz(S.bk[size_t(b) * S.n + L.s]);
+      const vec4<TF> bn = S.bx[size_t(b) * S.ls + L.s];
+      const vec3<TF> a = (c.rho0 * dpi) * xyz(S.bk[size_t(b) * S.ls + L.s]);
       f = c.mass * a;
       ai -= a;
       tq = cross(xyz(bn) - S.rigid[b].x, f);
@@ -930,8 +1007,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_i_diag(Cn<TF> c, StepState<TF> S)
   adv += rho / c.rho0;
   for (uint32_t m = S.mask[L.s]; m; m &= m - 1) {
     const uint32_t b = __ffs(m) - 1;
-    const vec4<TF> bn = S.bx[size_t(b) * S.n + L.s];
-    const vec3<TF> gwv = xyz(S.bk[size_t(b) * S.n + L.s]);
+    const vec4<TF> bn = S.bx[size_t(b) * S.ls + L.s];
+    const vec3<TF> gwv = xyz(S.bk[size_t(b) * S.ls + L.s]);
     const vec3<TF> xib = xi - xyz(bn);
     adv += dt * dot(vi - body_velocity(S.rigid[b], xyz(bn)), gwv);
     diag += (rho + c.rho0) / (rho * c.rho0) / (length_sqr(xib) + eps) * dot(xib, gwv);
@@ -1099,6 +1176,9 @@ struct StepPlan {
   uint32_t* warm_floor = nullptr;
   // launch shapes: particle-count bucket and context of the shape table
   uint32_t bucket = 0, ctx = 0;
+  // a scene of a fused batch: its first slot in the shared particle arena
+  // (the neighbor list stores arena slots); 0 for a step of its own
+  uint32_t base = 0;
   // first-stage partials of the rigid totals ([kRigidChunks][nb][6])
   double* ftp = nullptr;
   // Shape of pass group `group` (defaults: 128-thread blocks; pair passes
@@ -1197,33 +1277,26 @@ __global__ void k_warm_if(cudaGraphConditionalHandle h, const uint32_t* __restri
 // Kernels inside the learned warm start's IF node (inference, application).
 constexpr uint32_t kWarmIfLaunches = 2;
 
-// Enqueues one whole step on `st`: staging uploads, grid, boundaries,
-// neighbors, the solves, write-back and the report readback.  With
-// `capture` the solver loops become conditional WHILE nodes (and `loops`
-// counts them); otherwise the host reads the loop flag every iteration.
+// Parts of a step: all of it, or (a scene of a fused batch, whose solves
+// run as passes over every scene) the head up to the neighbor build and the
+// tail from the write-back on.
+enum StepPhase { kStepAll, kStepHead, kStepTail };
+
+// Enqueues one whole step (or its `phase`) on `st`: staging uploads, grid,
+// boundaries, neighbors, the solves, write-back and the report readback.
+// With `capture` the solver loops become conditional WHILE nodes (and
+// `loops` counts them); otherwise the host reads the loop flag every
+// iteration.
 template <class TF>
-int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, int* loops) {
+int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, int* loops,
+                 StepPhase phase = kStepAll) {
   StepState<TF>& S = P.S;
   const Cn<TF>& c = P.c;
   const auto* f = P.f;
   const uint32_t n = S.n, nb = S.nb;
   const bool iisph = P.iisph, div = P.div, den = P.den;
   const bool wr = c.wrap != 0;  // periodic-y instantiations of the pair passes
-  ALB_CUDA(cudaMemcpyAsync(S.ctrl, P.io.hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
-  if (nb) {
-    ALB_CUDA(cudaMemcpyAsync(P.bodies_dev, P.io.hb, sizeof(BodyDev<TF>) * nb,
-                             cudaMemcpyHostToDevice, st));
-    ALB_CUDA(cudaMemcpyAsync(S.rigid, P.io.hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice,
-                             st));
-  }
-  ALB_CUDA(cudaMemsetAsync(P.flags, 0, 4 * sizeof(uint32_t), st));
-  ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
-  ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
-  // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
-  GridState gs;
-  ALB_LAUNCH(e, "grid_sort", kGridBuildKernels, st,
-             ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
-  S.perm = gs.perm;
+  const bool head = phase != kStepTail, solves = phase == kStepAll, tail = phase != kStepHead;
   const uint32_t blocks = blocks_for(n, kBlock);
   // grid, block and lane state of pair pass group `g` (launch-shape table)
   auto pair_shape = [&](const char* g, uint32_t& grid, uint32_t& block) {
@@ -1234,68 +1307,86 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     block = sh.block;
     return Sg;
   };
-  if (n > 0) {
-    const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
-    if (iisph)
-      ALB_LAUNCH(e, "gather_state", 1, st,
-                 k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
-                                                                      nullptr));
-    else
-      ALB_LAUNCH(e, "gather_state", 1, st,
-                 k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
-                                                                     f->particle_kappa_v));
-  }
-  BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk, &S.ctrl->rep.num_active_boundary_pairs};
-  if (nb)
-    ALB_LAUNCH(e, "boundary", 1, st,
-               ALB_TRY(sample_boundaries<TF>(c, P.bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
-                                             f->particle_boundary, f->particle_boundary_kernel,
-                                             st)));
-  else if (n)
-    ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
-  SortedBoundaryKernel<TF> sbk{S.mask, S.bk, n};
-  TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
-  if (div && n > 0) {
-    WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol,
-                          P.warm_floor};
-    const uint32_t nbb = P.shape(e, "neighbors", false).block;
-    ALB_LAUNCH(e, "neighbors", 1, st,
-               (wr ? k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, true>
-                         <<<blocks_for(n, nbb), nbb, 0, st>>>(
-                             c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
-                             rho_rec, gs.flags, wd)
-                   : k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false>
-                         <<<blocks_for(n, nbb), nbb, 0, st>>>(
-                             c, P.g, gs.cell_start, S.x, n, sbk, S.nbr, S.ncount, S.rho, S.alpha,
-                             rho_rec, gs.flags, wd)));
-    if (P.learned) {
-      // inference and its application; in a captured step they sit in an IF
-      // node, so a step whose gate is closed launches neither
-      auto infer = [&](cudaStream_t s) -> int {
-        ALB_LAUNCH(e, "warm_net", 1, s,
-                   ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, s,
-                                        P.warm_floor)));
-        ALB_LAUNCH(e, "warm_apply", 1, s,
-                   (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, s>>>(
-                       S, P.warm_feat, P.warm_pred, P.warm_floor)));
-        return AL_OK;
-      };
-      if (capture)
-        ALB_TRY(capture_if(
-            e, st,
-            [&](cudaGraphConditionalHandle h) -> int {
-              ALB_LAUNCH(e, "warm_gate", 1, st,
-                         (k_warm_if<TF><<<1, 1, 0, st>>>(h, P.warm_floor, S.ctrl)));
-              return AL_OK;
-            },
-            infer));
-      else
-        ALB_TRY(infer(st));
+  if (head) {
+    ALB_CUDA(cudaMemcpyAsync(S.ctrl, P.io.hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
+    if (nb) {
+      ALB_CUDA(cudaMemcpyAsync(P.bodies_dev, P.io.hb, sizeof(BodyDev<TF>) * nb,
+                               cudaMemcpyHostToDevice, st));
+      ALB_CUDA(cudaMemcpyAsync(S.rigid, P.io.hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice,
+                               st));
     }
-  } else
-    ALB_LAUNCH(e, "neighbors", 1, st,
-               ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
-                                                   iisph ? nullptr : S.alpha, rho_rec, st)));
+    ALB_CUDA(cudaMemsetAsync(P.flags, 0, 4 * sizeof(uint32_t), st));
+    ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
+    ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
+    // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
+    GridState gs;
+    ALB_LAUNCH(e, "grid_sort", kGridBuildKernels, st,
+               ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
+    S.perm = gs.perm;
+    if (n > 0) {
+      const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
+      if (iisph)
+        ALB_LAUNCH(e, "gather_state", 1, st,
+                   k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                                        nullptr));
+      else
+        ALB_LAUNCH(e, "gather_state", 1, st,
+                   k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                                       f->particle_kappa_v));
+    }
+    BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk, &S.ctrl->rep.num_active_boundary_pairs, S.ls};
+    if (nb)
+      ALB_LAUNCH(e, "boundary", 1, st,
+                 ALB_TRY(sample_boundaries<TF>(c, P.bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
+                                               f->particle_boundary, f->particle_boundary_kernel,
+                                               st)));
+    else if (n)
+      ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
+    SortedBoundaryKernel<TF> sbk{S.mask, S.bk, S.ls};
+    TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
+    if (div && n > 0) {
+      WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol,
+                            P.warm_floor};
+      const uint32_t nbb = P.shape(e, "neighbors", false).block;
+      ALB_LAUNCH(e, "neighbors", 1, st,
+                 (wr ? k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, true>
+                           <<<blocks_for(n, nbb), nbb, 0, st>>>(
+                               c, P.g, gs.cell_start, S.x, n, S.ls, P.base, sbk, S.nbr, S.ncount,
+                               S.rho, S.alpha, rho_rec, gs.flags, wd)
+                     : k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false>
+                           <<<blocks_for(n, nbb), nbb, 0, st>>>(
+                               c, P.g, gs.cell_start, S.x, n, S.ls, P.base, sbk, S.nbr, S.ncount,
+                               S.rho, S.alpha, rho_rec, gs.flags, wd)));
+      if (P.learned) {
+        // inference and its application; in a captured step they sit in an IF
+        // node, so a step whose gate is closed launches neither
+        auto infer = [&](cudaStream_t s) -> int {
+          ALB_LAUNCH(e, "warm_net", 1, s,
+                     ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, s,
+                                          P.warm_floor)));
+          ALB_LAUNCH(e, "warm_apply", 1, s,
+                     (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, s>>>(
+                         S, P.warm_feat, P.warm_pred, P.warm_floor)));
+          return AL_OK;
+        };
+        if (capture)
+          ALB_TRY(capture_if(
+              e, st,
+              [&](cudaGraphConditionalHandle h) -> int {
+                ALB_LAUNCH(e, "warm_gate", 1, st,
+                           (k_warm_if<TF><<<1, 1, 0, st>>>(h, P.warm_floor, S.ctrl)));
+                return AL_OK;
+              },
+              infer));
+        else
+          ALB_TRY(infer(st));
+      }
+    } else
+      ALB_LAUNCH(e, "neighbors", 1, st,
+                 ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+                                                     iisph ? nullptr : S.alpha, rho_rec, st,
+                                                     S.ls, P.base)));
+  }  // head
   // One solver loop: kernel `k_loop_begin` sets the first condition, `body`
   // launches one iteration on the given stream.
   auto solve = [&](int density_solve, uint32_t max_iter, auto&& body) -> int {
@@ -1318,7 +1409,7 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     }
     return AL_OK;
   };
-  if (n > 0) {
+  if (n > 0 && solves) {
     if (div) {
       {
         uint32_t pg_, pb_;
@@ -1393,14 +1484,6 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                         return AL_OK;
                       }));
       }
-      ALB_LAUNCH(e, "finish", 1, st,
-                 (wr ? k_df_finish<TF, true><<<blocks, kBlock, 0, st>>>(
-                     c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
-                     f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                     f->particle_kappa_v, f->particle_density_adv, P.warm_floor) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
-                     c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
-                     f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                     f->particle_kappa_v, f->particle_density_adv, P.warm_floor)));
     } else if (P.isph) {
       ALB_LAUNCH(e, "i_advect", 1, st, k_i_advect<TF><<<blocks, kBlock, 0, st>>>(S));
       {
@@ -1468,6 +1551,19 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                        f->particle_pressure, f->particle_density_adv)));
       }
     }
+  }
+  if (n > 0 && tail && !iisph)
+    ALB_LAUNCH(e, "finish", 1, st,
+               (wr ? k_df_finish<TF, true><<<blocks, kBlock, 0, st>>>(
+                   c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                   f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
+                   f->particle_kappa_v, f->particle_density_adv, P.warm_floor) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
+                   c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                   f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
+                   f->particle_kappa_v, f->particle_density_adv, P.warm_floor)));
+  if (!tail) {
+    ALB_CUDA(cudaGetLastError());
+    return AL_OK;
   }
   if (nb) {
     if (S.grid > kRigidChunks)
@@ -1577,10 +1673,12 @@ struct StepArgs {
 };
 
 // Validates the arguments, sizes the scene's scratch (under the engine's
-// current buffer namespace) and fills staging slot `slot` of `nslots`.
+// current buffer namespace; with `alloc` false only its anomaly flags: a
+// fused batch places the particle state in its shared arena) and fills
+// staging slot `slot` of `nslots`.
 template <class TF>
 int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t slot,
-                 uint32_t nslots) {
+                 uint32_t nslots, bool alloc = true) {
   ALB_TRY(check_step_args<TF>(A.f, A.cni, A.bodies, A.rigid, A.sp, A.dt));
   const al_solver_params* sp = A.sp;
   const bool iisph = A.iisph || A.isph;
@@ -1599,6 +1697,7 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   const uint32_t nb = P.g.nb;
   StepState<TF>& S = P.S;
   S.n = n;
+  S.ls = n;
   S.nb = nb;
   S.cap = P.g.cap_nbr;
   P.bucket = n ? uint32_t(31 - __builtin_clz(n)) : 0u;
@@ -1615,33 +1714,35 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   if (S.grid == 0) S.grid = 1;
   // ---- buffers
   ALB_TRY(e->buf("flags", 4, &P.flags));
-  ALB_TRY(e->buf("sorted.x", size_t(n) + kSortedPad, &S.x));
-  ALB_TRY(e->buf("sorted.rec", size_t(n) * 2, &S.rec));
-  ALB_TRY(e->buf("sorted.a", n, &S.a));
-  ALB_TRY(e->buf("sorted.rho", n, &S.rho));
-  ALB_TRY(e->buf("sorted.alpha", n, &S.alpha));
-  ALB_TRY(e->buf("sorted.rho_adv", n, &S.rho_adv));
-  ALB_TRY(e->buf("sorted.kappa", n, &S.kappa));
-  ALB_TRY(e->buf("sorted.kappa_v", n, &S.kappa_v));
-  if (iisph) {
-    ALB_TRY(e->buf("sorted.kk", n, &S.kk));
-    ALB_TRY(e->buf("sorted.err", n, &S.err));
+  if (alloc) {
+    ALB_TRY(e->buf("sorted.x", size_t(n) + kSortedPad, &S.x));
+    ALB_TRY(e->buf("sorted.rec", size_t(n) * 2, &S.rec));
+    ALB_TRY(e->buf("sorted.a", n, &S.a));
+    ALB_TRY(e->buf("sorted.rho", n, &S.rho));
+    ALB_TRY(e->buf("sorted.alpha", n, &S.alpha));
+    ALB_TRY(e->buf("sorted.rho_adv", n, &S.rho_adv));
+    ALB_TRY(e->buf("sorted.kappa", n, &S.kappa));
+    ALB_TRY(e->buf("sorted.kappa_v", n, &S.kappa_v));
+    if (iisph) {
+      ALB_TRY(e->buf("sorted.kk", n, &S.kk));
+      ALB_TRY(e->buf("sorted.err", n, &S.err));
+    }
+    if (iisph && !P.isph) {
+      ALB_TRY(e->buf("sorted.dii", n, &S.dii));
+      ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
+    }
+    ALB_TRY(e->buf("nbr.list", size_t(n) * P.g.cap_nbr, &S.nbr));
+    ALB_TRY(e->buf("nbr.count", n, &S.ncount));
+    ALB_TRY(e->buf("bnd.mask", n, &S.mask));
+    ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
+    ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
+    ALB_TRY(e->buf("bodies", nb ? nb : 1, &P.bodies_dev));
+    ALB_TRY(e->buf("rigid", nb ? nb : 1, &S.rigid));
+    ALB_TRY(e->buf("ft", size_t(S.grid) * (nb ? nb : 1) * 6, &S.ft));
+    ALB_TRY(e->buf("ftp", size_t(kRigidChunks) * (nb ? nb : 1) * 6, &P.ftp));
+    ALB_TRY(e->buf("red", S.grid, &S.red));
+    ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
   }
-  if (iisph && !P.isph) {
-    ALB_TRY(e->buf("sorted.dii", n, &S.dii));
-    ALB_TRY(e->buf("sorted.dij_pj", n, &S.dij_pj));
-  }
-  ALB_TRY(e->buf("nbr.list", size_t(n) * P.g.cap_nbr, &S.nbr));
-  ALB_TRY(e->buf("nbr.count", n, &S.ncount));
-  ALB_TRY(e->buf("bnd.mask", n, &S.mask));
-  ALB_TRY(e->buf("bnd.x", size_t(nb ? nb : 1) * n, &S.bx));
-  ALB_TRY(e->buf("bnd.k", size_t(nb ? nb : 1) * n, &S.bk));
-  ALB_TRY(e->buf("bodies", nb ? nb : 1, &P.bodies_dev));
-  ALB_TRY(e->buf("rigid", nb ? nb : 1, &S.rigid));
-  ALB_TRY(e->buf("ft", size_t(S.grid) * (nb ? nb : 1) * 6, &S.ft));
-  ALB_TRY(e->buf("ftp", size_t(kRigidChunks) * (nb ? nb : 1) * 6, &P.ftp));
-  ALB_TRY(e->buf("red", S.grid, &S.red));
-  ALB_TRY(e->buf("ctrl", 1, &S.ctrl));
   S.bodies = P.bodies_dev;
   const al_warm_start* warm = A.warm;
   if (warm && (warm->net || warm->features_out)) {
@@ -1867,6 +1968,339 @@ std::vector<uint64_t> batch_key(al_engine* e, const std::vector<StepArgs<TF>>& a
   return key;
 }
 
+// ------------------------------------------------------------ fused batches
+// A fused batch runs each solver pass of all its scenes as one launch.  The
+// scenes' cell-sorted particles share one arena (scene k at slots
+// [s0_k, s0_k + n_k), s0_k a multiple of kFusedAlign), the neighbor lists
+// and boundary terms are slot-major over the whole arena (the lists hold
+// arena slots), and each block of a pass finds its scene in a block -> scene
+// table (block_scene) for the scene's dt, control block, bodies and
+// reductions.  Grid sort, boundary sampling and the neighbor build (the
+// scenes' grids differ) and the write-back stay per scene, in concurrent
+// graph branches.  The solver loops are one WHILE loop over all scenes: a
+// scene whose solve has converged sits out the remaining iterations and
+// the loop ends when no scene iterates again, so each scene runs exactly
+// its own iterations.  Pair passes run one thread per particle in
+// kFusedBlock-thread blocks; every reduction of a scene covers its own
+// blocks in the order a single step's 128-thread launch would, so with
+// those shapes in the shape table's batch context the branch and the
+// fused batch give bit-identical results.
+constexpr uint32_t kFusedBlock = 128;
+constexpr uint32_t kFusedAlign = 256;
+
+template <class TF>
+struct FusedPlan {
+  uint32_t K = 0, N = 0, nblocks = 0;
+  StepState<TF> S;           // the arena, as the fused passes see it
+  uint32_t* go = nullptr;    // device: 1 while some scene iterates again
+  uint32_t* hgo = nullptr;   // pinned readback of `go` (eager loops)
+};
+
+// Starts the solver loop of every scene (k_loop_begin) and sets the loop
+// condition: some scene iterates.
+template <class TF>
+__global__ void k_fused_loop_begin(const FusedScene<TF>* __restrict__ sc, uint32_t K,
+                                   int density_solve, uint32_t* go,
+                                   cudaGraphConditionalHandle handle, int use_handle) {
+  uint32_t any = 0;
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+    Ctrl<TF>& C = *sc[k].ctrl;
+    C.it = 0;
+    C.ticket = 0;
+    C.keep_going = (density_solve ? C.max_den : C.max_div) > 0 ? 1u : 0u;
+    any |= C.keep_going;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    *go = any;
+    if (use_handle) cudaGraphSetConditional(handle, any);
+  }
+}
+
+// Condition of the next iteration of a fused solver loop.
+template <class TF>
+__global__ void k_fused_loop_cond(const FusedScene<TF>* __restrict__ sc, uint32_t K,
+                                  uint32_t* go, cudaGraphConditionalHandle handle,
+                                  int use_handle) {
+  uint32_t any = 0;
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) any |= sc[k].ctrl->keep_going;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    *go = any;
+    if (use_handle) cudaGraphSetConditional(handle, any);
+  }
+}
+
+// Whether a batch can run fused: DFSPH scenes with particles, one set of
+// constants, the same solves enabled, no periodic wrap.
+template <class TF>
+bool fusable(const std::vector<StepArgs<TF>>& args) {
+  for (const StepArgs<TF>& a : args) {
+    if (a.iisph || a.isph || a.warm || !a.f || !a.sp || !a.cn || !a.cni) return false;
+    if (a.f->num_particles == 0 || a.sp->wrap_y) return false;
+    if (std::memcmp(a.cn, args[0].cn, sizeof(*a.cn)) != 0) return false;
+    if (a.sp->enable_divergence_solve != args[0].sp->enable_divergence_solve ||
+        a.sp->enable_density_solve != args[0].sp->enable_density_solve)
+      return false;
+  }
+  return !args.empty();
+}
+
+// Places the scenes (prepared without their own particle scratch) in the
+// arena, fills the block -> scene table and uploads it when it changed.
+template <class TF>
+int fused_prepare(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>& F,
+                  cudaStream_t st) {
+  const uint32_t K = uint32_t(plans.size());
+  std::vector<uint32_t> s0(K);
+  uint64_t N = 0;
+  uint32_t nbmax = 1, cap = 1;
+  size_t ft_words = 0, ftp_words = 0;
+  for (uint32_t k = 0; k < K; ++k) {
+    const StepState<TF>& Sk = plans[k].S;
+    s0[k] = uint32_t(N);
+    N = (N + Sk.n + kFusedAlign - 1) / kFusedAlign * kFusedAlign;
+    ALB_CHECK_ARG(N < (uint64_t(1) << 31), "al_df_batch_step_f32: too many particles in all");
+    nbmax = std::max(nbmax, Sk.nb);
+    cap = std::max(cap, Sk.cap);
+    const size_t nbk = Sk.nb ? Sk.nb : 1;
+    ft_words += size_t(blocks_for(Sk.n, kFusedBlock)) * nbk * 6;
+    ftp_words += size_t(kRigidChunks) * nbk * 6;
+  }
+  F.K = K;
+  F.N = uint32_t(N);
+  F.nblocks = F.N / kFusedBlock;
+  StepState<TF> A = plans[0].S;
+  FusedScene<TF>* table = nullptr;
+  uint32_t* blk = nullptr;
+  BodyDev<TF>* bodies = nullptr;
+  double* ftp = nullptr;
+  e->ns = "fused.";
+  ALB_TRY(e->buf("sorted.x", size_t(N) + kSortedPad, &A.x));
+  ALB_TRY(e->buf("sorted.rec", size_t(N) * 2, &A.rec));
+  ALB_TRY(e->buf("sorted.a", N, &A.a));
+  ALB_TRY(e->buf("sorted.rho", N, &A.rho));
+  ALB_TRY(e->buf("sorted.alpha", N, &A.alpha));
+  ALB_TRY(e->buf("sorted.rho_adv", N, &A.rho_adv));
+  ALB_TRY(e->buf("sorted.kappa", N, &A.kappa));
+  ALB_TRY(e->buf("sorted.kappa_v", N, &A.kappa_v));
+  ALB_TRY(e->buf("nbr.list", size_t(N) * cap, &A.nbr));
+  ALB_TRY(e->buf("nbr.count", N, &A.ncount));
+  ALB_TRY(e->buf("bnd.mask", N, &A.mask));
+  ALB_TRY(e->buf("bnd.x", size_t(nbmax) * N, &A.bx));
+  ALB_TRY(e->buf("bnd.k", size_t(nbmax) * N, &A.bk));
+  ALB_TRY(e->buf("ctrl", K, &A.ctrl));
+  ALB_TRY(e->buf("bodies", size_t(K) * nbmax, &bodies));
+  ALB_TRY(e->buf("rigid", size_t(K) * nbmax, &A.rigid));
+  ALB_TRY(e->buf("ft", ft_words, &A.ft));
+  ALB_TRY(e->buf("ftp", ftp_words, &ftp));
+  ALB_TRY(e->buf("red", F.nblocks, &A.red));
+  ALB_TRY(e->buf("table", K, &table));
+  ALB_TRY(e->buf("blk_scene", F.nblocks, &blk));
+  ALB_TRY(e->buf("go", 1, &F.go));
+  e->ns.clear();
+  std::vector<FusedScene<TF>> tab(K);
+  std::vector<uint32_t> hblk(F.nblocks, K);
+  size_t ft_off = 0, ftp_off = 0;
+  for (uint32_t k = 0; k < K; ++k) {
+    StepPlan<TF>& P = plans[k];
+    StepState<TF>& Sk = P.S;
+    const uint32_t o = s0[k], n = Sk.n, nb = Sk.nb, nbk = nb ? nb : 1;
+    const uint32_t nblk = blocks_for(n, kFusedBlock), blk0 = o / kFusedBlock;
+    Sk.ls = F.N;
+    Sk.x = A.x + o;
+    Sk.rec = A.rec + 2 * size_t(o);
+    Sk.a = A.a + o;
+    Sk.rho = A.rho + o;
+    Sk.alpha = A.alpha + o;
+    Sk.rho_adv = A.rho_adv + o;
+    Sk.kappa = A.kappa + o;
+    Sk.kappa_v = A.kappa_v + o;
+    Sk.nbr = A.nbr + o;
+    Sk.ncount = A.ncount + o;
+    Sk.mask = A.mask + o;
+    Sk.bx = A.bx + o;
+    Sk.bk = A.bk + o;
+    Sk.ctrl = A.ctrl + k;
+    P.bodies_dev = bodies + size_t(k) * nbmax;
+    Sk.bodies = P.bodies_dev;
+    Sk.rigid = A.rigid + size_t(k) * nbmax;
+    Sk.ft = A.ft + ft_off;
+    Sk.grid = nblk;
+    Sk.red = A.red + blk0;
+    P.ftp = ftp + ftp_off;
+    P.base = o;
+    ft_off += size_t(nblk) * nbk * 6;
+    ftp_off += size_t(kRigidChunks) * nbk * 6;
+    tab[k] = FusedScene<TF>{o, n, blk0, nblk, nb, 0u, Sk.ctrl, Sk.bodies, Sk.rigid, Sk.ft, Sk.red};
+    for (uint32_t b = blk0; b < blk0 + nblk; ++b) hblk[b] = k;
+  }
+  A.n = F.N;
+  A.ls = F.N;
+  A.tpp = 1;
+  A.grid = F.nblocks;
+  A.perm = nullptr;
+  A.blk_scene = blk;
+  A.fused = table;
+  A.nscenes = K;
+  F.S = A;
+  F.hgo = plans[0].io.hflag;
+  // upload the tables when they (or their buffers) changed
+  std::vector<unsigned char> bytes(sizeof(FusedScene<TF>) * K + sizeof(uint32_t) * F.nblocks +
+                                   2 * sizeof(void*));
+  std::memcpy(bytes.data(), tab.data(), sizeof(FusedScene<TF>) * K);
+  std::memcpy(bytes.data() + sizeof(FusedScene<TF>) * K, hblk.data(),
+              sizeof(uint32_t) * F.nblocks);
+  const void* where[2] = {table, blk};
+  std::memcpy(bytes.data() + bytes.size() - sizeof(where), where, sizeof(where));
+  if (bytes != e->fused_tables) {
+    ALB_CUDA(cudaMemcpyAsync(table, tab.data(), sizeof(FusedScene<TF>) * K,
+                             cudaMemcpyHostToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(blk, hblk.data(), sizeof(uint32_t) * F.nblocks,
+                             cudaMemcpyHostToDevice, st));
+    ALB_CUDA(cudaStreamSynchronize(st));
+    e->fused_tables.swap(bytes);
+  }
+  return AL_OK;
+}
+
+// The fused solves of a batch: every pass one launch over the arena.
+template <class TF>
+int enqueue_fused_solve(al_engine* e, const StepPlan<TF>& P0, FusedPlan<TF>& F, cudaStream_t st,
+                        bool capture, int* loops) {
+  const Cn<TF>& c = P0.c;
+  const StepState<TF>& S = F.S;
+  const uint32_t G = F.nblocks, B = kFusedBlock;
+  auto solve = [&](int density_solve, auto&& body) -> int {
+    if (capture) {
+      ++*loops;
+      return capture_while(
+          e, st,
+          [&](cudaGraphConditionalHandle h) -> int {
+            ALB_LAUNCH(e, "loop_begin", 1, st,
+                       (k_fused_loop_begin<TF><<<1, 256, 0, st>>>(S.fused, F.K, density_solve,
+                                                                   F.go, h, 1)));
+            return AL_OK;
+          },
+          body);
+    }
+    ALB_LAUNCH(e, "loop_begin", 1, st,
+               (k_fused_loop_begin<TF><<<1, 256, 0, st>>>(S.fused, F.K, density_solve, F.go,
+                                                           cudaGraphConditionalHandle(0), 0)));
+    for (;;) {
+      ALB_CUDA(cudaMemcpyAsync(F.hgo, F.go, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      ALB_CUDA(cudaStreamSynchronize(st));
+      if (!*F.hgo) break;
+      ALB_TRY(body(st, cudaGraphConditionalHandle(0), 0));
+    }
+    return AL_OK;
+  };
+  auto cond = [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+    ALB_LAUNCH(e, "loop_cond", 1, s,
+               (k_fused_loop_cond<TF><<<1, 256, 0, s>>>(S.fused, F.K, F.go, h, use)));
+    return AL_OK;
+  };
+  const cudaGraphConditionalHandle none(0);
+  if (P0.div) {
+    ALB_LAUNCH(e, "div_warm1", 1, st, (k_kappa<TF, kDivWarm, false, true><<<G, B, 0, st>>>(c, S)));
+    ALB_LAUNCH(e, "div_rho_adv", 1, st,
+               (k_df_rho_adv_init<TF, false, true><<<G, B, 0, st>>>(c, S)));
+    ALB_TRY(solve(0, [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+      ALB_LAUNCH(e, "div_iter", 1, s, (k_kappa<TF, kDivIter, false, true><<<G, B, 0, s>>>(c, S)));
+      ALB_LAUNCH(e, "div_residual", 1, s,
+                 (k_df_residual<TF, false, true><<<G, B, 0, s>>>(c, S, none, 0)));
+      return cond(s, h, use);
+    }));
+  }
+  ALB_LAUNCH(e, "viscosity", 1, st,
+             (k_viscosity<TF, false, true><<<G, B, 0, st>>>(c, S, P0.div ? 1 : 0)));
+  ALB_LAUNCH(e, "integrate_np", 1, st, (k_integrate_np<TF, true><<<G, B, 0, st>>>(S)));
+  if (P0.den) {
+    ALB_LAUNCH(e, "press_warm0", 1, st,
+               (k_p_warm0<TF, false, true><<<G, B, 0, st>>>(c, S, nullptr, nullptr)));
+    ALB_LAUNCH(e, "press_warm1", 1, st,
+               (k_kappa<TF, kPressWarm, false, true><<<G, B, 0, st>>>(c, S)));
+    ALB_LAUNCH(e, "press_rho_adv", 1, st,
+               (k_p_rho_adv_init<TF, false, true><<<G, B, 0, st>>>(c, S)));
+    ALB_TRY(solve(1, [&](cudaStream_t s, cudaGraphConditionalHandle h, int use) -> int {
+      ALB_LAUNCH(e, "press_iter", 1, s,
+                 (k_kappa<TF, kPressIter, false, true><<<G, B, 0, s>>>(c, S)));
+      ALB_LAUNCH(e, "press_residual", 1, s,
+                 (k_p_residual<TF, false, true><<<G, B, 0, s>>>(c, S, none, 0)));
+      return cond(s, h, use);
+    }));
+  }
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+// Kernels of one iteration of a fused solver loop (update, residual, loop
+// condition).
+constexpr uint32_t kFusedIterationLaunches = 3;
+
+// Enqueues a fused batch on `st`; with `capture` (st capturing) the scenes'
+// heads and tails run in parallel branches.
+template <class TF>
+int enqueue_fused_batch(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>& F,
+                        cudaStream_t st, bool capture, int* loops) {
+  const uint32_t K = uint32_t(plans.size());
+  auto phase = [&](StepPhase ph) -> int {
+    if (!capture) {
+      for (uint32_t k = 0; k < K; ++k) {
+        e->ns = batch_ns(k);
+        ALB_TRY(enqueue_step<TF>(e, plans[k], st, false, nullptr, ph));
+      }
+      e->ns.clear();
+      return AL_OK;
+    }
+    ALB_CUDA(cudaEventRecord(e->fork_event, st));
+    for (uint32_t k = 0; k < K; ++k) {
+      cudaStream_t bs = e->branch_streams[k];
+      ALB_CUDA(cudaStreamWaitEvent(bs, e->fork_event, 0));
+      e->ns = batch_ns(k);
+      ALB_TRY(enqueue_step<TF>(e, plans[k], bs, true, loops, ph));
+      ALB_CUDA(cudaEventRecord(e->join_events[k], bs));
+      ALB_CUDA(cudaStreamWaitEvent(st, e->join_events[k], 0));
+    }
+    e->ns.clear();
+    return AL_OK;
+  };
+  ALB_TRY(phase(kStepHead));
+  ALB_TRY(enqueue_fused_solve<TF>(e, plans[0], F, st, capture, loops));
+  return phase(kStepTail);
+}
+
+template <class TF>
+int capture_batch_fused(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>& F,
+                        cudaGraphExec_t* exec, uint32_t* fixed) {
+  *exec = nullptr;
+  ALB_TRY(e->capture_streams());
+  ALB_TRY(e->branches(uint32_t(plans.size())));
+  cudaStream_t cs = e->capture_stream;
+  const uint64_t launches0 = e->launches;
+  const uint64_t gen0 = e->generation;
+  ALB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int loops = 0;
+  const int rc = enqueue_fused_batch<TF>(e, plans, F, cs, true, &loops);
+  e->ns.clear();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(cs, &graph);
+  const uint64_t captured = e->launches - launches0;
+  e->launches = launches0;
+  if (rc != AL_OK || end != cudaSuccess || e->generation != gen0) {
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != AL_OK) return rc;
+    ALB_CUDA(end);
+    return AL_OK;
+  }
+  const cudaError_t inst = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (inst != cudaSuccess) *exec = nullptr;
+  ALB_CUDA(inst);
+  *fixed = uint32_t(captured - kFusedIterationLaunches * uint32_t(loops));
+  return AL_OK;
+}
+
 template <class TF>
 int run_batch(al_engine* e, const std::vector<StepArgs<TF>>& args, std::vector<int>& status,
               cudaStream_t st) {
@@ -1876,25 +2310,36 @@ int run_batch(al_engine* e, const std::vector<StepArgs<TF>>& args, std::vector<i
     ~NsReset() { e->ns.clear(); }
   } reset{e};
   const uint32_t K = uint32_t(args.size());
+  const bool fused = e->batch_fused && fusable<TF>(args);
   std::vector<StepPlan<TF>> plans(K);
   bool nonempty = true;
   for (uint32_t k = 0; k < K; ++k) {
     e->ns = batch_ns(k);
-    ALB_TRY(prepare_step<TF>(e, args[k], plans[k], k, K));
+    ALB_TRY(prepare_step<TF>(e, args[k], plans[k], k, K, !fused));
     nonempty = nonempty && plans[k].S.n > 0;
   }
   e->ns.clear();
+  FusedPlan<TF> F;
+  if (fused) ALB_TRY(fused_prepare<TF>(e, plans, F, st));
+  auto key = [&]() {
+    std::vector<uint64_t> k = batch_key<TF>(e, args, plans);
+    if (fused) k.insert(k.end(), {0xF05EDull, uint64_t(F.N)});
+    return k;
+  };
   const bool use_graph = e->graph_mode && !e->profiling && nonempty;
   al_engine::Graph* graph = nullptr;
   if (use_graph)
-    ALB_TRY(find_or_capture(e, batch_key<TF>(e, args, plans),
+    ALB_TRY(find_or_capture(e, key(),
                             [&](cudaGraphExec_t* x, uint32_t* fl) {
-                              return capture_batch<TF>(e, plans, x, fl);
+                              return fused ? capture_batch_fused<TF>(e, plans, F, x, fl)
+                                           : capture_batch<TF>(e, plans, x, fl);
                             },
                             &graph));
   if (graph) {
     ALB_CUDA(cudaGraphLaunch(graph->exec, st));
     ++e->graph_replays;
+  } else if (fused) {
+    ALB_TRY(enqueue_fused_batch<TF>(e, plans, F, st, false, nullptr));
   } else {
     for (uint32_t k = 0; k < K; ++k) {
       e->ns = batch_ns(k);
@@ -1904,15 +2349,20 @@ int run_batch(al_engine* e, const std::vector<StepArgs<TF>>& args, std::vector<i
   }
   ALB_CUDA(cudaStreamSynchronize(st));
   e->flush_stats();
-  if (use_graph && !graph) remember_key(e, batch_key<TF>(e, args, plans));
+  if (use_graph && !graph) remember_key(e, key());
   status.assign(K, AL_OK);
   uint64_t iters = 0;
+  uint32_t max_div = 0, max_den = 0;
   for (uint32_t k = 0; k < K; ++k) {
     const al_step_report& r = plans[k].io.hc->rep;
     iters += uint64_t(r.num_divergence_solve) + r.num_density_solve;
+    max_div = std::max(max_div, r.num_divergence_solve);
+    max_den = std::max(max_den, r.num_density_solve);
     status[k] = finish_step<TF>(args[k], plans[k]);
   }
-  if (graph) e->launches += graph->fixed_launches + 2ull * iters;
+  if (graph)
+    e->launches += graph->fixed_launches +
+                   (fused ? uint64_t(kFusedIterationLaunches) * (max_div + max_den) : 2ull * iters);
   for (int s : status)
     if (s != AL_OK) return s;
   return AL_OK;
@@ -2040,6 +2490,12 @@ int al_tunable_group(uint32_t index, const char** name, uint32_t* pair) {
   }
   *name = kTunable[index].name;
   *pair = kTunable[index].pair ? 1u : 0u;
+  return AL_OK;
+}
+
+int al_engine_set_batch_fused(al_engine* engine, int enable) {
+  ALB_CHECK_ARG(engine, "al_engine_set_batch_fused: null engine");
+  engine->batch_fused = enable != 0;
   return AL_OK;
 }
 

@@ -47,9 +47,15 @@ struct Ctrl {
 };
 
 template <class TF>
+struct FusedScene;
+
+template <class TF>
 struct StepState {
   uint32_t n = 0, nb = 0, cap = 0, grid = 0;
   uint32_t tpp = 1;  // threads per particle of the pair passes (pair_tpp)
+  // Stride of the slot-major arrays (nbr [cap][ls], bx / bk [nb][ls]): n for
+  // one scene; the arena's particle count for the scenes of a fused batch.
+  uint32_t ls = 0;
   vec4<TF>* x = nullptr;    // sorted positions (grid sort, boundaries, build)
   // Interleaved particle records of the pair passes: rec[2s] = {x, payload},
   // rec[2s + 1] = {v, rho}.  One 32-byte sector (float) holds all a
@@ -80,6 +86,25 @@ struct StepState {
   double* red = nullptr;  // [grid] reduction partials
   Ctrl<TF>* ctrl = nullptr;
   const uint32_t* perm = nullptr;
+  // A pass launched over every scene of a fused batch: the scene of each
+  // block (nscenes for a block past every scene) and the scenes' ranges.
+  const uint32_t* blk_scene = nullptr;
+  const FusedScene<TF>* fused = nullptr;
+  uint32_t nscenes = 0;
+};
+
+// One scene of a fused batch: its particles [s0, s0 + n) of the shared
+// arena, its blocks [blk0, blk0 + nblk) of a pass launch (128 threads, one
+// per particle), and its control block, bodies, rigid state, rigid slots
+// ([nblk][nb][6]) and reduction partials ([nblk]).
+template <class TF>
+struct FusedScene {
+  uint32_t s0, n, blk0, nblk, nb, pad;
+  Ctrl<TF>* ctrl;
+  const BodyDev<TF>* bodies;
+  RigidDev<TF>* rigid;
+  double* ft;
+  double* red;
 };
 
 }  // namespace alb

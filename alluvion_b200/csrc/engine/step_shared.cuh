@@ -18,29 +18,35 @@ __device__ __forceinline__ vec3<TF> body_velocity(const RigidDev<TF>& r, vec3<TF
   return cross(r.omega, at - r.x) + r.v;
 }
 
-// Deterministic grid-wide double sum: every block writes its block sum to
-// red[blockIdx]; the last block to finish (ticket) sums the partials in
-// block order.  Returns true in the last block, with the total in thread 0.
+// Deterministic double sum over `nblk` blocks (block `blk` of them): every
+// block writes its block sum to red[blk]; the last block to finish (ticket)
+// sums the partials in block order.  Returns true in the last block, with
+// the total in thread 0.
 __device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_t* ticket,
-                                              double* total) {
+                                              double* total, uint32_t blk, uint32_t nblk) {
   __shared__ bool last;
   const double bsum = block_sum_double(value);
   if (threadIdx.x == 0) {
-    red[blockIdx.x] = bsum;
+    red[blk] = bsum;
     __threadfence();
-    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    last = atomicAdd(ticket, 1u) == nblk - 1;
   }
   __syncthreads();
   if (!last) return false;
   __threadfence();
   double s = 0;
-  for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) s += __ldcg(red + k);
+  for (uint32_t k = threadIdx.x; k < nblk; k += blockDim.x) s += __ldcg(red + k);
   s = block_sum_double(s);
   if (threadIdx.x == 0) {
     *total = s;
     *ticket = 0;
   }
   return true;
+}
+// The same over the whole grid.
+__device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_t* ticket,
+                                              double* total) {
+  return grid_sum_last(value, red, ticket, total, blockIdx.x, gridDim.x);
 }
 
 template <class TF>

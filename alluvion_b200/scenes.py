@@ -540,9 +540,11 @@ def solver_params(**kw):
 
 def batch_step(engine, scene_list, sp, dts, stream=None, allow=()):
     """One DFSPH step of every float32 scene in one call
-    (al_df_batch_step_f32).  dts: per-scene time steps.  Returns (new dts,
+    (al_df_batch_step_f32).  sp: solver parameters for all scenes, or a list
+    with one per scene; dts: per-scene time steps.  Returns (new dts,
     reports, per-scene statuses)."""
     k = len(scene_list)
+    sps = list(sp) if isinstance(sp, (list, tuple)) else [sp] * k
     arr = (_capi.SceneF32 * k)()
     keep = []
     dt_c = [ctypes.c_float(float(d)) for d in dts]
@@ -557,7 +559,7 @@ def batch_step(engine, scene_list, sp, dts, stream=None, allow=()):
         a.fluid = _capi.ptr(fl).value
         a.bodies = _capi.ptr(sc.bodies).value if sc.num_boundaries else None
         a.rigid = _capi.ptr(sc.rigid).value if sc.num_boundaries else None
-        a.params = _capi.ptr(sp).value
+        a.params = _capi.ptr(sps[i]).value
         a.dt = ctypes.addressof(dt_c[i])
         a.report = ctypes.addressof(reps[i])
     status = _capi.lib().al_df_batch_step_f32(engine.handle, arr, k, stream)

@@ -161,7 +161,12 @@ def parse_args():
                         "default workload, else 0)")
     p.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
                    help="sweep the pass groups' launch shapes before timing (untimed; "
-                        "alluvion_b200.autotune); auto: on for batched workloads")
+                        "alluvion_b200.autotune); auto: on for batched workloads run as "
+                        "branches")
+    p.add_argument("--batch-form", choices=["fused", "branches"], default="branches",
+                   help="batched workloads: fused (one launch per solver pass over all "
+                        "scenes) or one graph branch per scene; the line also times the "
+                        "other form for comparison")
     p.add_argument("--max-dt", type=float, default=None,
                    help="time-step cap (default 2e-4 s)")
     a = p.parse_args()
@@ -544,7 +549,9 @@ def batch_scene_specs(spec, seed=SEED):
 
 def batch_arm(args):
     """Config-3 style batch: every step advances all scenes with one
-    al_df_batch_step_f32 call (one graph launch from the second step on)."""
+    al_df_batch_step_f32 call (one graph launch from the second step on),
+    fused (one launch per solver pass over all scenes) or as one graph
+    branch per scene (--batch-form)."""
     import torch
     from alluvion_b200 import _capi, scenes
     world, rank, local = dist_env()
@@ -561,12 +568,20 @@ def batch_arm(args):
     if args.max_dt:
         sp.max_dt = args.max_dt
     total_n = sum(sc.n for sc in sl)
-    tuning = None
-    if args.autotune != "off":
+
+    def tune():
+        if args.autotune == "off":
+            return None
         from alluvion_b200 import autotune
         t0 = time.perf_counter()
-        tuning = autotune.tune_batch(engine, sl, sp)
-        tuning["seconds"] = round(time.perf_counter() - t0, 1)
+        tb = autotune.tune_batch(engine, sl, sp)
+        tb["seconds"] = round(time.perf_counter() - t0, 1)
+        return {k: tb[k] for k in ("batch_ms_default", "batch_ms_uniform", "uniform_shape",
+                                   "batch_ms_tuned", "buckets", "seconds")}
+    fused = args.batch_form == "fused"
+    engine.set_batch_fused(fused)
+    # the fused form's pair passes have one launch shape; the branches are tuned
+    tuning = None if fused else tune()
     host_state = [sc.state() for sc in sl] if rank == 0 and world == 1 else None
     host_bodies = [sc.host_bodies() for sc in sl] if host_state is not None else None
     dts = [float(sp.max_dt)] * len(sl)
@@ -632,11 +647,12 @@ def batch_arm(args):
                    "scene_particles_min_max": [min(sc.n for sc in sl), max(sc.n for sc in sl)],
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
-                   "launch": "eager" if args.eager else "batch graph (one branch per scene)",
-                   "autotune": None if tuning is None else {
-                       k: tuning[k] for k in ("batch_ms_default", "batch_ms_uniform",
-                                              "uniform_shape", "batch_ms_tuned", "buckets",
-                                              "seconds")},
+                   "launch": ("eager" if args.eager else "batch graph") + (
+                       ": fused, one launch per solver pass over all scenes (pair passes "
+                       "one thread per particle, 128-thread blocks), per-scene grid sort, "
+                       "boundary sampling, neighbor build and write-back in concurrent "
+                       "branches" if fused else ": one branch per scene"),
+                   "autotune": tuning,
                    "graph_replays_timed": graphs1[1] - graphs0[1],
                    "mean_divergence_iterations": round(float(its[:, :, 0].mean()), 3),
                    "mean_density_iterations": round(float(its[:, :, 1].mean()), 3)},
@@ -646,7 +662,8 @@ def batch_arm(args):
         "roofline": None,
         "clocks": clk,
     }
-    # roofline of the dominant pass from the eager per-pass times (scenes in turn)
+    # roofline of the dominant pass from the eager per-pass times (fused: each
+    # pass one launch over all scenes; branches: the scenes in turn)
     engine.reset_stats()
     engine.set_profiling(True)
     run(2)
@@ -664,12 +681,29 @@ def batch_arm(args):
     per_launch = pass_ms[dominant] / max(runs, 1e-9)
     achieved = alg / (per_launch / 1e3) / 1e9
     result["config"]["pass_ms_per_step_sequential"] = {k: round(v, 4) for k, v in pass_ms.items()}
+    # the other form on the same scenes, for comparison (untimed tuning first)
+    other = "branches" if fused else "fused"
+    engine.set_batch_fused(not fused)
+    other_tuning = tune() if fused else None
+    for _ in range(args.warmup):
+        dts, _, _ = scenes.batch_step(engine, sl, sp, dts)
+    barrier(world)
+    ms_o, its_o = run(args.steps)
+    ms_o = max_over_ranks(ms_o, world, torch)
+    result["config"]["other_form"] = {
+        "form": other, "ms_per_step": round(ms_o / args.steps, 4),
+        "value": round(job_throughput(total_n, world, args.steps, ms_o), 1),
+        "mean_density_iterations": round(float(its_o[:, :, 1].mean()), 3),
+        "autotune": other_tuning}
+    engine.set_batch_fused(fused)
     result["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                           "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
                           "kernel": dominant, "peak_kind": peak_kind,
                           "algorithmic_bytes_per_launch": int(alg),
                           "launch_ms": round(per_launch, 4),
-                          "note": "per-pass times from eager steps (scenes in turn)"}
+                          "note": "per-pass times from eager steps (%s)" % (
+                              "each pass one launch over all scenes" if fused
+                              else "scenes in turn")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import binding as orc
         t0 = time.perf_counter()

@@ -762,10 +762,26 @@ AL_API int al_solve_contacts_f32(al_engine* engine, const al_body_f32* bodies,
  * Advances every scene by one DFSPH step (each with its own dt, iteration
  * counts and report; same semantics as al_df_step_f32 per scene).  From the
  * second call with the same configuration on, the whole batch is one
- * captured CUDA graph whose parallel branches are the scenes' steps: one
- * launch and one synchronisation for all scenes, whose kernels overlap on
- * the GPU.  Each scene keeps its own scratch.  Returns AL_OK, or the first
- * scene's failure; every scene's own status is in scenes[k].status. */
+ * captured CUDA graph: one launch and one synchronisation for all scenes.
+ *
+ * Fused (after al_engine_set_batch_fused(engine, 1), when every scene has
+ * particles, the same constants `cn`, the same solves enabled and no
+ * periodic wrap): the scenes' particles
+ * share one device arena and every solver pass is ONE kernel launch over
+ * all scenes, each block finding its scene in a block -> scene table; the
+ * solver loops are one device-driven loop in which a scene whose solve has
+ * converged sits out the remaining iterations, so each scene runs exactly
+ * its own iterations.  Pair passes run one thread per particle in
+ * 128-thread blocks.  The scenes' grid sorts, boundary sampling, neighbor
+ * builds and write-backs run as concurrent graph branches.
+ * Otherwise (the default): the graph's parallel branches are the scenes'
+ * whole steps, each with its own scratch and launch shapes (the shape
+ * table's batch context).
+ * With 128-thread blocks and one thread per particle for every pair pass in
+ * the batch context, both forms give bit-identical results.
+ * Returns AL_OK, or the first scene's failure; every scene's own status is
+ * in scenes[k].status. */
+AL_API int al_engine_set_batch_fused(al_engine* engine, int enable);
 #define AL_MAX_BATCH 256
 typedef struct al_scene_f32 {
   const al_const_f32* cn;

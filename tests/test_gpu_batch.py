@@ -1,16 +1,23 @@
-"""Batched scenes (al_df_batch_step_f32) against the same scenes stepped
-one at a time with al_df_step_f32.  Each batch branch runs the scene's own
-kernels; with the default launch-shape tables (the same shapes in the
-single and the batch context: threads per particle from the scene's own
-particle count) the launch shapes are the same too, so the results are
-bit-identical, whether the batch runs eagerly (first call) or as one
-replayed graph.  Tuned tables that give a scene another shape in a batch
-change its float results in the last bits (tests/test_gpu_launch_shapes.py
-covers that case against the oracle)."""
+"""Batched scenes (al_df_batch_step_f32).
+
+Branch form (one graph branch per scene): each branch runs the scene's own
+kernels; with the default launch-shape tables (the same shapes in the single
+and the batch context: threads per particle from the scene's own particle
+count) the results equal the same scenes stepped one at a time with
+al_df_step_f32 bit for bit, whether the batch runs eagerly (first call) or
+as one replayed graph.  Tuned tables that give a scene another shape in a
+batch change its float results in the last bits
+(tests/test_gpu_launch_shapes.py covers that case against the oracle).
+
+Fused form (one launch per solver pass over all scenes): pair
+passes run one thread per particle in 128-thread blocks, so with those
+shapes in the batch context the two forms agree bit for bit, including
+scenes whose solves take different iteration counts; against the oracle
+both meet the single-step tolerances."""
 import numpy as np
 import pytest
 
-from alluvion_b200 import _capi, scenes
+from alluvion_b200 import _capi, autotune, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +36,14 @@ def _scenes(engine):
         out.append(scenes.dam_break(engine, np.float32, lat, 0.01, (0.5, 0.4, 0.4), bodies,
                                     seed=k, volume_resolution=16))
     return out
+
+
+def _uniform_batch_shapes(engine, scene_list, block, tpp):
+    """Sets (block, tpp) for every pass group in the batch context of the
+    scenes' buckets (0, 0: back to the defaults)."""
+    for b in sorted({autotune.bucket_of(sc.n) for sc in scene_list}):
+        for name, pair in _capi.tunable_groups():
+            engine.set_launch_shape(name, b, 1, block, tpp if pair or not tpp else 1)
 
 
 def test_batch_matches_single_steps(engine):
@@ -59,21 +74,94 @@ def test_batch_matches_single_steps(engine):
             assert list(b.rigid[i].q) == list(s.rigid[i].q)
 
 
+def _states_equal(a, b):
+    sa, sb = a.state(), b.state()
+    for key in ("x", "v", "kappa", "kappa_v", "density", "a"):
+        np.testing.assert_array_equal(sa[key], sb[key], err_msg=key)
+    for i in range(a.num_boundaries):
+        for f in ("x", "v", "omega", "q"):
+            assert list(getattr(a.rigid[i], f)) == list(getattr(b.rigid[i], f)), (i, f)
+
+
+def test_fused_batch_matches_branch_batch(engine):
+    """Fused against branch form with 128-thread blocks and one thread per
+    particle in the batch context: equal dts, iteration counts, reports and
+    states bit for bit over four steps (the first eager, then captured).
+    The second scene is held to at least five density iterations, so the
+    others sit out iterations of the fused loop."""
+    fused, branch = _scenes(engine), _scenes(engine)
+    sps = [scenes.solver_params() for _ in fused]
+    sps[1] = scenes.solver_params(min_density_solve=5)
+    _uniform_batch_shapes(engine, fused, 128, 1)
+    try:
+        c0, r0 = engine.graph_stats()
+        dts_f = [2e-4] * len(fused)
+        dts_b = [2e-4] * len(branch)
+        for step in range(4):
+            engine.set_batch_fused(True)
+            dts_f, reps_f, st_f = scenes.batch_step(engine, fused, sps, dts_f)
+            engine.set_batch_fused(False)
+            dts_b, reps_b, st_b = scenes.batch_step(engine, branch, sps, dts_b)
+            assert st_f == st_b == [0] * len(fused)
+            assert dts_f == dts_b
+            for rf, rb in zip(reps_f, reps_b):
+                assert rf.num_divergence_solve == rb.num_divergence_solve
+                assert rf.num_density_solve == rb.num_density_solve
+                assert rf.mean_density_error == rb.mean_density_error
+                assert rf.mean_density_change == rb.mean_density_change
+                assert rf.num_active_boundary_pairs == rb.num_active_boundary_pairs
+                for b in range(len(rf.force)):
+                    assert list(rf.force[b]) == list(rb.force[b])
+                    assert list(rf.torque[b]) == list(rb.torque[b])
+            assert reps_f[1].num_density_solve >= 5
+            assert min(r.num_density_solve for r in reps_f) < reps_f[1].num_density_solve
+        c1, r1 = engine.graph_stats()
+        assert r1 - r0 >= 4  # both forms replayed from the second step on
+        for f, b in zip(fused, branch):
+            _states_equal(f, b)
+    finally:
+        engine.set_batch_fused(False)
+        _uniform_batch_shapes(engine, fused, 0, 0)
+
+
+def test_fused_batch_falls_back_for_mixed_constants(engine):
+    """A batch whose scenes have different constants (particle radii) runs as
+    branches: equal to the same scenes stepped alone, bit for bit."""
+    mk = lambda: [scenes.dam_break(engine, np.float32, (10, 8, 10), 0.01, (0.5, 0.4, 0.4), [],
+                                   seed=1, volume_resolution=16),
+                  scenes.dam_break(engine, np.float32, (12, 10, 12), 0.008, (0.5, 0.4, 0.4), [],
+                                   seed=2, volume_resolution=16)]
+    batch, single = mk(), mk()
+    sp = scenes.solver_params()
+    engine.set_batch_fused(True)
+    try:
+        dts_b, reps_b, status = scenes.batch_step(engine, batch, sp, [2e-4, 2e-4])
+    finally:
+        engine.set_batch_fused(False)
+    assert status == [0, 0]
+    for k, sc in enumerate(single):
+        dt, rep = sc.step("df", sp, 2e-4)
+        assert dt == dts_b[k]
+        assert rep.num_density_solve == reps_b[k].num_density_solve
+    for b, s in zip(batch, single):
+        _states_equal(b, s)
+
+
 def test_batch_rejects_too_many_scenes(engine):
     arr = (_capi.SceneF32 * 1)()
     st = _capi.lib().al_df_batch_step_f32(engine.handle, arr, 257, None)
     assert st == 2  # AL_ERR_INVALID
 
 
-@pytest.mark.parametrize("shape", [None, (256, 1)])
-def test_batch_of_benchmark_scenes_matches_oracle(engine, shape):
+@pytest.mark.parametrize("fused,shape", [(True, None), (False, None), (False, (256, 1))])
+def test_batch_of_benchmark_scenes_matches_oracle(engine, fused, shape):
     """The four smallest scenes of the 64-scene benchmark batch (seeded, with
-    their rigid spheres), stepped as one batch, each against the oracle's
-    step of the same scene: equal iteration counts and the float32 one-step
-    tolerances of the single-step parity tests (the jittered start's
-    pressure kick amplifies rounding from the second step on).  With shape
-    set, the batch context runs a tuned table (other threads per particle
-    than a single step would use)."""
+    their rigid spheres), stepped as one batch (fused, or as branches), each
+    against the oracle's step of the same scene: equal iteration counts and
+    the float32 one-step tolerances of the single-step parity tests (the
+    jittered start's pressure kick amplifies rounding from the second step
+    on).  With shape set, the batch context runs a tuned table (other threads
+    per particle than a single step would use)."""
     import bench
     from alluvion_b200 import autotune
     from test_gpu_step import TOL, _close, _oracle_run
@@ -82,6 +170,7 @@ def test_batch_of_benchmark_scenes_matches_oracle(engine, shape):
     batch = [s.device(engine) for s in chosen]
     groups = _capi.tunable_groups()
     buckets = sorted({autotune.bucket_of(sc.n) for sc in batch})
+    engine.set_batch_fused(fused)
     try:
         if shape:
             for b in buckets:
@@ -101,6 +190,7 @@ def test_batch_of_benchmark_scenes_matches_oracle(engine, shape):
             _close(g["v"], ostate["v"], tol["v"], "v")
             _close(g["density"], ostate["density"], tol["density"], "density")
     finally:
+        engine.set_batch_fused(False)
         for b in buckets:
             for name, _ in groups:
                 engine.set_launch_shape(name, b, 1, 0, 0)

@@ -89,16 +89,22 @@ def _batch_scenes(engine):
     return out
 
 
-def test_batch_equals_single_steps_with_the_same_shapes(engine):
+@pytest.mark.parametrize("fused,shape", [(False, (256, 2)), (True, (128, 1))])
+def test_batch_equals_single_steps_with_the_same_shapes(engine, fused, shape):
+    """A batch equals its scenes' single steps bit for bit when both run the
+    same launch shapes: as branches with any shape set in both contexts; fused
+    (whose pair passes always run one thread per particle in 128-thread
+    blocks) when the single steps run that shape too."""
     groups = _capi.tunable_groups()
     batch = _batch_scenes(engine)
     single = _batch_scenes(engine)
     buckets = sorted({autotune.bucket_of(sc.n) for sc in batch})
+    engine.set_batch_fused(fused)
     try:
         for b in buckets:
             for name, pair in groups:
                 for ctx in (0, 1):
-                    engine.set_launch_shape(name, b, ctx, 256, 2 if pair else 1)
+                    engine.set_launch_shape(name, b, ctx, shape[0], shape[1] if pair else 1)
         sp = scenes.solver_params()
         dts_b = [2e-4] * 3
         dts_s = [2e-4] * 3
@@ -113,6 +119,7 @@ def test_batch_equals_single_steps_with_the_same_shapes(engine):
             for key in ("x", "v", "kappa", "kappa_v", "density"):
                 np.testing.assert_array_equal(sa[key], ss[key], err_msg=key)
     finally:
+        engine.set_batch_fused(False)
         for b in buckets:
             for name, _ in groups:
                 for ctx in (0, 1):
