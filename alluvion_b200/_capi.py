@@ -451,8 +451,8 @@ class Engine:
 
     def set_batch_fused(self, enable):
         """Batched steps run fused (one launch per solver pass over all scenes,
-        where the scenes allow it) or as one graph branch per scene (the
-        default)."""
+        the default where the scenes allow it) or as one graph branch per
+        scene."""
         check(lib().al_engine_set_batch_fused(self.handle, 1 if enable else 0),
               "al_engine_set_batch_fused")
 

@@ -106,19 +106,17 @@ __device__ __forceinline__ void sample_body(const Cn<TF>& c, const BodyDev<TF>& 
   bk = vec4<TF>{vol * kg.x, vol * kg.y, vol * kg.z, vol * W_dist(c, d)};
 }
 
+// Samples every body for the particle at slot s (position xs[s]; mask,
+// bx, bk at s, rows `stride` apart) and, when ref_b / ref_k are set, writes
+// the dense reference layout at its original index i (rows of n_ref).
 template <class TF>
-__global__ void __launch_bounds__(kBlock)
-    k_sample_boundaries(Cn<TF> c, const BodyDev<TF>* __restrict__ bodies,
-                        const RigidDev<TF>* __restrict__ rigid, uint32_t nb,
-                        const vec4<TF>* __restrict__ xs, const uint32_t* __restrict__ perm,
-                        uint32_t n, uint32_t stride, uint32_t* __restrict__ mask,
-                        vec4<TF>* __restrict__ bx, vec4<TF>* __restrict__ bk,
-                        TF* __restrict__ ref_b, TF* __restrict__ ref_k,
-                        uint32_t* __restrict__ active) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
+__device__ __forceinline__ void sample_particle(
+    const Cn<TF>& c, const BodyDev<TF>* __restrict__ bodies, const RigidDev<TF>* __restrict__ rigid,
+    uint32_t nb, const vec4<TF>* __restrict__ xs, uint32_t s, uint32_t i, uint32_t n_ref,
+    uint32_t stride, uint32_t* __restrict__ mask, vec4<TF>* __restrict__ bx,
+    vec4<TF>* __restrict__ bk, TF* __restrict__ ref_b, TF* __restrict__ ref_k,
+    uint32_t* __restrict__ active) {
   const vec3<TF> x = xyz(xs[s]);
-  const uint32_t i = perm ? perm[s] : s;
   uint32_t m = 0;
   for (uint32_t b = 0; b < nb; ++b) {
     vec4<TF> bnd, kk;
@@ -131,12 +129,12 @@ __global__ void __launch_bounds__(kBlock)
       }
     }
     if (ref_b) {
-      TF* o = ref_b + (size_t(b) * n + i) * 4;
+      TF* o = ref_b + (size_t(b) * n_ref + i) * 4;
       o[0] = bnd.x;
       o[1] = bnd.y;
       o[2] = bnd.z;
       o[3] = bnd.w;
-      TF* k = ref_k + (size_t(b) * n + i) * 4;
+      TF* k = ref_k + (size_t(b) * n_ref + i) * 4;
       k[0] = kk.x;
       k[1] = kk.y;
       k[2] = kk.z;
@@ -150,6 +148,40 @@ __global__ void __launch_bounds__(kBlock)
     const unsigned tot = __reduce_add_sync(live, unsigned(__popc(m)));
     if ((threadIdx.x & 31) == unsigned(__ffs(live) - 1) && tot) atomicAdd(active, tot);
   }
+}
+
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_sample_boundaries(Cn<TF> c, const BodyDev<TF>* __restrict__ bodies,
+                        const RigidDev<TF>* __restrict__ rigid, uint32_t nb,
+                        const vec4<TF>* __restrict__ xs, const uint32_t* __restrict__ perm,
+                        uint32_t n, uint32_t stride, uint32_t* __restrict__ mask,
+                        vec4<TF>* __restrict__ bx, vec4<TF>* __restrict__ bk,
+                        TF* __restrict__ ref_b, TF* __restrict__ ref_k,
+                        uint32_t* __restrict__ active) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  sample_particle(c, bodies, rigid, nb, xs, s, perm ? perm[s] : s, n, stride, mask, bx, bk,
+                  ref_b, ref_k, active);
+}
+
+// Every scene of a fused batch in one launch: block -> scene, the scene's
+// particle at arena slot s0 + s.
+template <class TF>
+__global__ void __launch_bounds__(kBlock)
+    k_sample_boundaries_fused(Cn<TF> c, const vec4<TF>* __restrict__ xs, uint32_t stride,
+                              const uint32_t* __restrict__ blk_scene,
+                              const BoundaryScene<TF>* __restrict__ scenes, uint32_t nscenes,
+                              uint32_t* __restrict__ mask, vec4<TF>* __restrict__ bx,
+                              vec4<TF>* __restrict__ bk) {
+  const uint32_t k = __ldg(blk_scene + blockIdx.x);
+  if (k >= nscenes) return;
+  const BoundaryScene<TF>& sc = scenes[k];
+  const uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x - sc.s0;
+  if (sl >= sc.n) return;
+  const uint32_t s = sc.s0 + sl;
+  sample_particle(c, sc.bodies, sc.rigid, sc.nb, xs, s, sc.perm ? sc.perm[s] - sc.s0 : sl, sc.n,
+                  stride, mask, bx, bk, sc.ref_b, sc.ref_k, sc.active);
 }
 
 template <class TF>
@@ -245,6 +277,18 @@ int sample_boundaries(const Cn<TF>& c, const BodyDev<TF>* bodies_dev, const Rigi
 }
 
 template <class TF>
+int sample_boundaries_fused(const Cn<TF>& c, const vec4<TF>* xs, uint32_t stride,
+                            const uint32_t* blk_scene, const BoundaryScene<TF>* scenes,
+                            uint32_t nscenes, uint32_t nblocks, uint32_t* mask, vec4<TF>* bx,
+                            vec4<TF>* bk, cudaStream_t st) {
+  if (nblocks == 0) return AL_OK;
+  k_sample_boundaries_fused<TF><<<nblocks, kBlock, 0, st>>>(c, xs, stride, blk_scene, scenes,
+                                                            nscenes, mask, bx, bk);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+template <class TF>
 int build_volume_field(const Cn<TF>& c, const BodyDev<TF>& b, TF* out, cudaStream_t st) {
   const uint64_t threads = uint64_t(b.num_nodes) * 32;
   k_volume_field<TF><<<uint32_t((threads + 255) / 256), 256, 0, st>>>(c, b, out);
@@ -270,6 +314,10 @@ int node_positions(const BodyDev<TF>& b, TF* out, cudaStream_t st) {
   template int sample_boundaries<TF>(const Cn<TF>&, const BodyDev<TF>*, const RigidDev<TF>*,  \
                                      uint32_t, const vec4<TF>*, const uint32_t*, uint32_t,     \
                                      const BoundaryState<TF>&, TF*, TF*, cudaStream_t);        \
+  template int sample_boundaries_fused<TF>(const Cn<TF>&, const vec4<TF>*, uint32_t,            \
+                                           const uint32_t*, const BoundaryScene<TF>*, uint32_t, \
+                                           uint32_t, uint32_t*, vec4<TF>*, vec4<TF>*,           \
+                                           cudaStream_t);                                       \
   template int build_volume_field<TF>(const Cn<TF>&, const BodyDev<TF>&, TF*, cudaStream_t); \
   template int build_distance_grid<TF>(const BodyDev<TF>&, TF*, cudaStream_t);               \
   template int node_positions<TF>(const BodyDev<TF>&, TF*, cudaStream_t);

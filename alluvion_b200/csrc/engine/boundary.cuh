@@ -108,6 +108,31 @@ int sample_boundaries(const Cn<TF>& c, const BodyDev<TF>* bodies_dev, const Rigi
                       const BoundaryState<TF>& bs, TF* ref_boundary, TF* ref_kernel,
                       cudaStream_t st);
 
+// One scene of a fused batch for sample_boundaries_fused: its bodies, rigid
+// state, the batch's permutation (sorted arena slot -> arena slot s0 + i of
+// the scene's particle i), optional reference-layout outputs ([nb][n][4],
+// original order), active-pair counter and arena range [s0, s0 + n).
+template <class TF>
+struct BoundaryScene {
+  const BodyDev<TF>* bodies;
+  const RigidDev<TF>* rigid;
+  const uint32_t* perm;
+  TF* ref_b;
+  TF* ref_k;
+  uint32_t* active;
+  uint32_t nb, s0, n, pad;
+};
+
+// sample_boundaries for every scene of a fused batch in one launch over the
+// arena (kBlock-thread blocks; blk_scene[block] = the block's scene, or
+// nscenes past every scene): mask / bx / bk over the arena, rows `stride`
+// apart.
+template <class TF>
+int sample_boundaries_fused(const Cn<TF>& c, const vec4<TF>* xs, uint32_t stride,
+                            const uint32_t* blk_scene, const BoundaryScene<TF>* scenes,
+                            uint32_t nscenes, uint32_t nblocks, uint32_t* mask, vec4<TF>* bx,
+                            vec4<TF>* bk, cudaStream_t st);
+
 // Volume-map nodes of one body (update_volume_field).  Distance from the
 // body's grid when use_grid, else from its analytic SDF.
 template <class TF>

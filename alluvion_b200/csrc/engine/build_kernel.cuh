@@ -19,10 +19,26 @@ struct BuildOut {
   TF grad_norm2;   // |sum_j V grad W_ij + sum_b (grad W V)_b|^2 (0 without FACTOR)
 };
 
+// A build launched over every scene of a fused batch: each scene's grid,
+// cell starts, anomaly flags and range [s0, s0 + n) of the shared arena, and
+// the scene of each block (nscenes for a block past every scene).
+struct BuildScene {
+  GridDims g;
+  const uint32_t* cell_start;
+  uint32_t* flags;
+  uint32_t s0, n;
+};
+struct FusedBuild {
+  const uint32_t* blk_scene = nullptr;
+  const BuildScene* scenes = nullptr;
+  uint32_t nscenes = 0;
+};
+
 // EX hook of k_build_neighbors that adds nothing.
 template <class TF>
 struct NoExtra {
   static constexpr bool kOn = false;
+  __device__ __forceinline__ void narrow(uint32_t) {}
   __device__ __forceinline__ vec3<TF> self_v(uint32_t) const { return vec3<TF>{0, 0, 0}; }
   __device__ __forceinline__ vec3<TF> vj(uint32_t) const { return vec3<TF>{0, 0, 0}; }
   __device__ __forceinline__ void finish(uint32_t, const BuildOut<TF>&) const {}
@@ -52,20 +68,34 @@ static_assert(32 % kScan == 0 && kScan <= kSortedPad,
 // the particle's and the neighbors' velocities and receives
 // sum_j V (v_i - v_j) . grad W_ij, in list order, at the end.
 //
-// The list is slot-major with row stride `stride` (n for one scene) and
-// holds sorted slots plus `base` (0 for one scene; a fused batch's scene
-// stores its slots in the shared arena, offset by its first slot).
-template <class TF, class BK, bool FACTOR, class EX, bool WR = false>
+// The list is slot-major with row stride `stride` (n for one scene).  With
+// BT the launch covers every scene of a fused batch (fb): xs, the outputs
+// and the cell starts are in arena slots, each block takes its scene's grid,
+// cell starts and flags, and the scene's particle s0 + i looks only at the
+// scene's own cells.
+template <class TF, class BK, bool FACTOR, class EX, bool WR = false, bool BT = false>
 __global__ void __launch_bounds__(kMaxBlock)
     k_build_neighbors(Cn<TF> c, GridDims g, const uint32_t* __restrict__ cell_start,
-                      const vec4<TF>* __restrict__ xs, uint32_t n, uint32_t stride,
-                      uint32_t base, BK bk, uint32_t* __restrict__ nbr,
-                      uint32_t* __restrict__ ncount,
+                      const vec4<TF>* __restrict__ xs, uint32_t n, uint32_t stride, BK bk,
+                      uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncount,
                       TF* __restrict__ rho, TF* __restrict__ alpha, TF* __restrict__ rho_rec,
-                      uint32_t* __restrict__ flags, EX ex) {
+                      uint32_t* __restrict__ flags, EX ex, FusedBuild fb) {
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
+  uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x, s0 = 0;
+  if constexpr (BT) {
+    const uint32_t k = __ldg(fb.blk_scene + blockIdx.x);
+    if (k >= fb.nscenes) return;
+    const BuildScene& sc = fb.scenes[k];
+    g = sc.g;
+    cell_start = sc.cell_start;
+    flags = sc.flags;
+    s0 = sc.s0;
+    n = sc.n;
+    sl -= s0;
+    ex.narrow(k);
+  }
+  if (sl >= n) return;
+  const uint32_t s = s0 + sl;  // the particle's slot in xs and the outputs
   const vec3<TF> xi = xyz(xs[s]);
   int ip[3];
   cell_coords(c.h, g, xi, ip);
@@ -112,7 +142,7 @@ __global__ void __launch_bounds__(kMaxBlock)
           if (s - t0 < m) acc &= ~(1u << (s - t0));  // the particle itself
           for (; acc; acc &= acc - 1) {
             if (cnt < g.cap_nbr)
-              nbr[size_t(cnt) * stride + s] = base + t0 + uint32_t(__ffs(acc) - 1);
+              nbr[size_t(cnt) * stride + s] = t0 + uint32_t(__ffs(acc) - 1);
             ++cnt;
           }
         }
@@ -135,7 +165,7 @@ __global__ void __launch_bounds__(kMaxBlock)
     uint32_t t[kB];
 #pragma unroll
     for (uint32_t q = 0; q < kB; ++q)  // this thread's own stores: plain loads
-      t[q] = k0 + q < cnt ? nbr[size_t(k0 + q) * stride + s] - base : s;
+      t[q] = k0 + q < cnt ? nbr[size_t(k0 + q) * stride + s] : s;
     vec3<TF> xj[kB], vj[kB];
 #pragma unroll
     for (uint32_t q = 0; q < kB; ++q) {

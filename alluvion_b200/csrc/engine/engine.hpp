@@ -125,11 +125,13 @@ struct al_engine {
   int branches(uint32_t count);  // creates streams / events up to `count`
   std::string ns;
   // Batched steps run fused (one launch per solver pass over all scenes)
-  // when enabled (al_engine_set_batch_fused) and their scenes allow it; the
+  // unless disabled (al_engine_set_batch_fused) or their scenes rule it out;
+  // the
   // block -> scene tables last uploaded for a fused batch, with their
-  // buffers.
-  bool batch_fused = false;
+  // buffers, and that batch's graph key.
+  bool batch_fused = true;
   std::vector<unsigned char> fused_tables;
+  std::vector<uint64_t> fused_key;
   // pinned host staging (control readback, reports)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;

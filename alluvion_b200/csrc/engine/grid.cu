@@ -250,6 +250,57 @@ __global__ void k_gather_x(const TF* __restrict__ x, const uint32_t* __restrict_
 
 inline uint32_t blocks_for(uint32_t n, int block) { return (n + block - 1) / block; }
 
+// k_hash over the arena of a fused batch: slot g of a 128-slot block holds
+// particle g - s0 of the block's scene, or padding (no cell).
+template <class TF>
+__global__ void k_hash_fused(TF h, const uint32_t* __restrict__ blk_scene,
+                             const SortScene<TF>* __restrict__ scenes, uint32_t nscenes,
+                             uint32_t* __restrict__ cell, uint32_t* __restrict__ rank,
+                             uint32_t* __restrict__ count) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t k = blk_scene[blockIdx.x];
+  const SortScene<TF>* sc = k < nscenes ? scenes + k : nullptr;
+  const uint32_t i = sc ? g - sc->s0 : 0u;
+  if (!sc || i >= sc->n) {
+    cell[g] = kNoCell;
+    return;
+  }
+  const GridDims& gd = sc->g;
+  const vec3<TF> p = ld3(sc->x, i);
+  int ip[3];
+  cell_coords(h, gd, p, ip);
+  uint32_t lc;
+  if (in_grid(gd, ip)) {
+    lc = cell_linear(gd, ip[0], ip[1], ip[2]);
+  } else {
+    lc = gd.ncells;  // the scene's tail bucket
+    sc->flags[0] = 1u;
+  }
+  const uint32_t c = sc->cell0 + lc;
+  cell[g] = c;
+  const uint32_t r = atomicAdd(&count[c], 1u);
+  rank[g] = r;
+  if (lc < gd.ncells && r >= gd.cap_cell) sc->flags[1] = 1u;  // count > cap
+}
+
+// The padding buckets' counts (after the counts are cleared).
+template <class TF>
+__global__ void k_pad_counts(const SortScene<TF>* __restrict__ scenes, uint32_t nscenes,
+                             uint32_t* __restrict__ count) {
+  for (uint32_t k = threadIdx.x; k < nscenes; k += blockDim.x)
+    count[scenes[k].cell0 + scenes[k].g.ncells + 1] = scenes[k].pad;
+}
+
+__global__ void k_scatter_fused(const uint32_t* __restrict__ cell,
+                                const uint32_t* __restrict__ rank,
+                                const uint32_t* __restrict__ start, uint32_t n,
+                                uint32_t* __restrict__ perm) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const uint32_t c = cell[g];
+  if (c != kNoCell) perm[start[c] + rank[g]] = g;
+}
+
 }  // namespace
 
 namespace {
@@ -269,16 +320,10 @@ int scan_with_flags(al_engine* e, const uint32_t* count, uint32_t* start, uint32
 template <class TF>
 int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* particle_x,
                uint32_t n, vec4<TF>* xs, uint32_t* flags, GridState& gs, cudaStream_t st) {
-  gs.n = n;
-  gs.ncells = g.ncells;
   gs.flags = flags;
+  ALB_TRY(grid_buffers(e, g, n, gs));
   uint32_t* rank = nullptr;
-  ALB_TRY(e->buf("grid.cell", n, &gs.cell));
   ALB_TRY(e->buf("grid.rank", n, &rank));
-  ALB_TRY(e->buf("grid.perm", n, &gs.perm));
-  ALB_TRY(e->buf("grid.inv", n, &gs.inv));
-  ALB_TRY(e->buf("grid.count", size_t(g.ncells) + 1, &gs.count));
-  ALB_TRY(e->buf("grid.start", size_t(g.ncells) + 2, &gs.cell_start));
   ALB_CUDA(cudaMemsetAsync(gs.count, 0, (size_t(g.ncells) + 1) * sizeof(uint32_t), st));
   if (n == 0) {
     ALB_CUDA(cudaMemsetAsync(gs.cell_start, 0, (size_t(g.ncells) + 2) * sizeof(uint32_t), st));
@@ -297,6 +342,49 @@ int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* parti
   k_gather_x<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(particle_x, gs.perm, n, xs, gs.inv);
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
+}
+
+int grid_buffers(al_engine* e, const GridDims& g, uint32_t n, GridState& gs) {
+  gs.n = n;
+  gs.ncells = g.ncells;
+  ALB_TRY(e->buf("grid.cell", n, &gs.cell));
+  ALB_TRY(e->buf("grid.perm", n, &gs.perm));
+  ALB_TRY(e->buf("grid.inv", n, &gs.inv));
+  ALB_TRY(e->buf("grid.count", size_t(g.ncells) + 1, &gs.count));
+  ALB_TRY(e->buf("grid.start", size_t(g.ncells) + 2, &gs.cell_start));
+  return AL_OK;
+}
+
+template <class TF>
+int grid_build_fused(al_engine* e, TF h, const uint32_t* blk_scene, const SortScene<TF>* scenes,
+                     uint32_t nscenes, uint32_t narena, uint32_t ncells, GridState& gs,
+                     cudaStream_t st) {
+  gs.n = narena;
+  gs.ncells = ncells;
+  uint32_t* rank = nullptr;
+  ALB_TRY(e->buf("grid.cell", narena, &gs.cell));
+  ALB_TRY(e->buf("grid.rank", narena, &rank));
+  ALB_TRY(e->buf("grid.perm", narena, &gs.perm));
+  ALB_TRY(e->buf("grid.count", size_t(ncells) + 1, &gs.count));
+  ALB_TRY(e->buf("grid.start", size_t(ncells) + 2, &gs.cell_start));
+  ALB_CUDA(cudaMemsetAsync(gs.count, 0, (size_t(ncells) + 1) * sizeof(uint32_t), st));
+  if (narena == 0) return AL_OK;
+  k_pad_counts<TF><<<1, 256, 0, st>>>(scenes, nscenes, gs.count);
+  k_hash_fused<TF><<<narena / kBlock, kBlock, 0, st>>>(h, blk_scene, scenes, nscenes, gs.cell,
+                                                      rank, gs.count);
+  // cell caps were checked by the hash: no cells to check in the scan
+  ALB_TRY(scan_with_flags(e, gs.count, gs.cell_start, ncells + 1, 0u, 0u, nullptr, st));
+  k_scatter_fused<<<blocks_for(narena, kBlock), kBlock, 0, st>>>(gs.cell, rank, gs.cell_start,
+                                                                narena, gs.perm);
+  k_order_cells<<<blocks_for(ncells, kBlock), kBlock, 0, st>>>(gs.cell_start, ncells, gs.perm);
+  k_order_crowded<<<crowded_blocks(ncells), kCrowdedThreads, 0, st>>>(gs.cell_start, ncells,
+                                                                      gs.perm);
+  ALB_CUDA(cudaGetLastError());
+  return AL_OK;
+}
+
+uint32_t grid_fused_kernels(uint32_t ncells) {
+  return 7u + (grid_scan_tiles(ncells + 1) > 1 ? 1u : 0u);
 }
 
 uint32_t grid_scan_tiles(uint32_t len) { return (len + kScanTile - 1) / kScanTile; }
@@ -331,6 +419,9 @@ template int grid_sort_into<float>(const Cn<float>&, const GridDims&, const floa
 template int grid_sort_into<double>(const Cn<double>&, const GridDims&, const double*, uint32_t,
                                     uint32_t*, uint32_t*, const GridSortScratch&, cudaStream_t);
 
+template int grid_build_fused<float>(al_engine*, float, const uint32_t*,
+                                     const SortScene<float>*, uint32_t, uint32_t, uint32_t,
+                                     GridState&, cudaStream_t);
 template int grid_build<float>(al_engine*, const Cn<float>&, const GridDims&, const float*,
                                uint32_t, vec4<float>*, uint32_t*, GridState&, cudaStream_t);
 template int grid_build<double>(al_engine*, const Cn<double>&, const GridDims&, const double*,

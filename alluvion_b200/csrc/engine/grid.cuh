@@ -31,12 +31,44 @@ struct GridState {
 // per-cell orderings, gather).
 constexpr int kGridBuildKernels = 8;
 
+// The scratch grid_build uses for a sort of n particles on grid g, under the
+// engine's current buffer namespace (cell, perm, inv, count, cell_start of
+// gs): a later grid_build with the same sizes uses the same buffers.
+int grid_buffers(al_engine* e, const GridDims& g, uint32_t n, GridState& gs);
+
 // Hashes, sorts and gathers positions into `xs` (sorted order, w = 0).
 // particle_x is the caller's [n][3] array.  `flags` must be zeroed by the
 // caller (it is also used by later passes).
 template <class TF>
 int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* particle_x,
                uint32_t n, vec4<TF>* xs, uint32_t* flags, GridState& gs, cudaStream_t st);
+
+// One scene of a fused batch's sort: its positions (the caller's [n][3]),
+// grid, first cell in the batch's concatenated cells (its ncells cells, then
+// its out-of-grid tail bucket, then a padding bucket that holds the `pad`
+// slots up to the next scene's start), its slots [s0, s0 + n) of the
+// batch's arena and its anomaly flags.
+template <class TF>
+struct SortScene {
+  const TF* x;
+  GridDims g;
+  uint32_t cell0, s0, n, pad;
+  uint32_t* flags;
+};
+
+// Every scene of a fused batch in one counting sort over the concatenated
+// cells (ncells in all, tails and padding included): the scene of each
+// 128-slot block in blk_scene (nscenes past every scene), the arena of
+// `narena` slots.  gs.perm maps a sorted arena slot to the arena slot
+// s0 + i of the scene's particle i, gs.cell_start holds arena slots; the
+// cells' members, the out-of-grid tails included, are ordered by index.
+// Anomalies go to each scene's flags.
+template <class TF>
+int grid_build_fused(al_engine* e, TF h, const uint32_t* blk_scene, const SortScene<TF>* scenes,
+                     uint32_t nscenes, uint32_t narena, uint32_t ncells, GridState& gs,
+                     cudaStream_t st);
+// Kernels one grid_build_fused launches.
+uint32_t grid_fused_kernels(uint32_t ncells);
 
 // Scratch for grid_sort_into, all supplied by the caller.
 struct GridSortScratch {

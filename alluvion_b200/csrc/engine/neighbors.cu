@@ -48,28 +48,26 @@ __global__ void k_export_neighbors(Cn<TF> c, uint32_t cap, uint32_t n,
 template <class TF, class BK>
 int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState& gs,
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
-                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st, uint32_t stride,
-                            uint32_t base) {
+                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st) {
   if (gs.n == 0) return AL_OK;
   const uint32_t blocks = blocks_for(gs.n, kBlock);
-  if (stride == 0) stride = gs.n;
   // compile-time wrap flag: the non-periodic build carries no wrap branches
   if (alpha && c.wrap)
     k_build_neighbors<TF, BK, true, NoExtra<TF>, true><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
-        NoExtra<TF>{});
+        c, g, gs.cell_start, xs, gs.n, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        NoExtra<TF>{}, FusedBuild{});
   else if (alpha)
     k_build_neighbors<TF, BK, true, NoExtra<TF>, false><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
-        NoExtra<TF>{});
+        c, g, gs.cell_start, xs, gs.n, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        NoExtra<TF>{}, FusedBuild{});
   else if (c.wrap)
     k_build_neighbors<TF, BK, false, NoExtra<TF>, true><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
-        NoExtra<TF>{});
+        c, g, gs.cell_start, xs, gs.n, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        NoExtra<TF>{}, FusedBuild{});
   else
     k_build_neighbors<TF, BK, false, NoExtra<TF>, false><<<blocks, kBlock, 0, st>>>(
-        c, g, gs.cell_start, xs, gs.n, stride, base, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
-        NoExtra<TF>{});
+        c, g, gs.cell_start, xs, gs.n, gs.n, bk, nbr, ncount, rho, alpha, rho_rec, gs.flags,
+        NoExtra<TF>{}, FusedBuild{});
   ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }
@@ -91,7 +89,7 @@ int export_neighbors(const Cn<TF>& c, const GridDims& g, const GridState& gs,
 #define ALB_INST(TF, BK)                                                                  \
   template int build_neighbors_density<TF, BK<TF>>(                                       \
       const Cn<TF>&, const GridDims&, const GridState&, const vec4<TF>*, const BK<TF>&,    \
-      uint32_t*, uint32_t*, TF*, TF*, TF*, cudaStream_t, uint32_t, uint32_t);
+      uint32_t*, uint32_t*, TF*, TF*, TF*, cudaStream_t);
 ALB_INST(float, RefBoundaryKernel)
 ALB_INST(double, RefBoundaryKernel)
 ALB_INST(float, SortedBoundaryKernel)

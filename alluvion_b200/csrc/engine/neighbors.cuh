@@ -83,13 +83,10 @@ constexpr size_t kRecStride = 8;
 // non-null also the DFSPH factor of compute_dfsph_factor
 // (runner.hpp:3123-3154); when `rho_rec` is non-null also writes the
 // density to rho_rec[s * kRecStride].  Raises flags[2] on neighbor overflow.
-// The list's row stride is `stride` (0: n) and its entries are sorted slots
-// plus `base`.
 template <class TF, class BK>
 int build_neighbors_density(const Cn<TF>& c, const GridDims& g, const GridState& gs,
                             const vec4<TF>* xs, const BK& bk, uint32_t* nbr, uint32_t* ncount,
-                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st,
-                            uint32_t stride = 0, uint32_t base = 0);
+                            TF* rho, TF* alpha, TF* rho_rec, cudaStream_t st);
 
 // Writes reference-layout outputs in original particle order:
 // particle_neighbors [N][cap][4] {x_i - x_j, bits(j)} (if non-null),

@@ -301,12 +301,27 @@ __device__ __forceinline__ TF density_adv(const Cn<TF>& c, const StepState<TF>& 
 }
 
 // ------------------------------------------------------------- kernels
-template <class TF, bool DF>
+// With BT every scene of a fused batch in one launch: the block's scene's
+// buffers (S.io; S.perm holds arena slots s0 + i), the sorted positions
+// gathered here too.
+template <class TF, bool DF, bool BT = false>
 __global__ void k_gather_state(StepState<TF> S, const TF* __restrict__ v_ref,
                                const TF* __restrict__ k_ref, const TF* __restrict__ kv_ref) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  const uint32_t i = S.perm[s];
+  BlockSpan B;
+  if (!block_scene<BT>(S, B) || s >= B.end) return;
+  uint32_t i;
+  if constexpr (BT) {
+    const FusedIo<TF>& io = S.io[B.k];
+    i = S.perm[s] - (B.end - B.n);
+    v_ref = io.v_in;
+    k_ref = io.kappa_in;
+    kv_ref = io.kappa_v_in;
+    const vec3<TF> p = ld3(io.x_in, i);
+    S.x[s] = vec4<TF>{p.x, p.y, p.z, TF(0)};
+  } else {
+    i = S.perm[s];
+  }
   const vec3<TF> v = ld3(v_ref, i);
   RX(S, s) = vec4<TF>{S.x[s].x, S.x[s].y, S.x[s].z, TF(0)};
   RV(S, s) = vec4<TF>{v.x, v.y, v.z, TF(0)};  // rho follows from the build
@@ -333,6 +348,11 @@ struct WarmDivergence {
   // learned warm start gate (warm_gate_update): nonzero when this step skips
   // the network
   const uint32_t* floor = nullptr;
+  // a build over every scene of a fused batch: scene k's dt and rigid state
+  __device__ __forceinline__ void narrow(uint32_t k) {
+    S.ctrl = S.fused[k].ctrl;
+    S.rigid = S.fused[k].rigid;
+  }
   __device__ __forceinline__ vec3<TF> self_v(uint32_t s) const { return xyz(RV(S, s)); }
   __device__ __forceinline__ vec3<TF> vj(uint32_t t) const { return xyz(gV(S, t)); }
   __device__ __forceinline__ void finish(uint32_t s, const BuildOut<TF>& o) const {
@@ -720,7 +740,9 @@ __global__ void __launch_bounds__(kMaxBlock)
 
 // pressure_solve_finish + integrate_velocity<0> (runner.hpp:3606-3623),
 // written straight back to the caller's buffers in original order.
-template <class TF, bool WR = false>
+// With BT every scene of a fused batch in one launch, into each scene's own
+// buffers (S.io; S.perm holds arena slots s0 + i).
+template <class TF, bool WR = false, bool BT = false>
 __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __restrict__ x_ref,
                             TF* __restrict__ v_ref, TF* __restrict__ a_ref,
                             TF* __restrict__ rho_ref, TF* __restrict__ alpha_ref,
@@ -729,8 +751,23 @@ __global__ void k_df_finish(Cn<TF> c, StepState<TF> S, int density_solve, TF* __
   if constexpr (!WR) c.wrap = 0;  // non-periodic: the wrap branches fold away
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (warm_floor && s == 0) warm_gate_update(*S.ctrl, warm_floor);
-  if (s >= S.n) return;
-  const uint32_t i = S.perm[s];
+  BlockSpan B;
+  if (!block_scene<BT>(S, B) || s >= B.end) return;
+  uint32_t i;
+  if constexpr (BT) {
+    const FusedIo<TF>& io = S.io[B.k];
+    i = S.perm[s] - (B.end - B.n);
+    x_ref = io.x_out;
+    v_ref = io.v_out;
+    a_ref = io.a_out;
+    rho_ref = io.rho_out;
+    alpha_ref = io.alpha_out;
+    kappa_ref = io.kappa_out;
+    kappa_v_ref = io.kappa_v_out;
+    rho_adv_ref = io.rho_adv_out;
+  } else {
+    i = S.perm[s];
+  }
   const TF dt = S.ctrl->dt;
   const vec3<TF> v = xyz(RV(S, s));
   const vec3<TF> x = xyz(RX(S, s));
@@ -1131,15 +1168,24 @@ struct Staging {
   uint32_t* hf = nullptr;  // [4]
 };
 
+// Layout of one staging slot: control block at 0, bodies at `bodies`, rigid
+// state at `rigid`, the eager loop flag at `flag`, the anomaly flags at
+// flag + 64; `bytes` in all.
+template <class TF>
+struct StagingLayout {
+  static constexpr size_t up64(size_t b) { return (b + 63) & ~size_t(63); }
+  static constexpr size_t bodies = up64(sizeof(Ctrl<TF>));
+  static constexpr size_t rigid = bodies + up64(sizeof(BodyDev<TF>) * AL_MAX_BOUNDARIES);
+  static constexpr size_t flag = rigid + up64(sizeof(RigidDev<TF>) * AL_MAX_BOUNDARIES);
+  static constexpr size_t bytes = flag + 128;
+};
+
 // Staging of slot `slot` out of `nslots` equal slots (batched steps give
 // every scene its own slot).
 template <class TF>
 int staging(al_engine* e, Staging<TF>* out, uint32_t slot = 0, uint32_t nslots = 1) {
-  auto up64 = [](size_t b) { return (b + 63) & ~size_t(63); };
-  const size_t off_b = up64(sizeof(Ctrl<TF>));
-  const size_t off_r = off_b + up64(sizeof(BodyDev<TF>) * AL_MAX_BOUNDARIES);
-  const size_t off_f = off_r + up64(sizeof(RigidDev<TF>) * AL_MAX_BOUNDARIES);
-  const size_t slot_bytes = off_f + 128;
+  using L = StagingLayout<TF>;
+  const size_t off_b = L::bodies, off_r = L::rigid, off_f = L::flag, slot_bytes = L::bytes;
   void* pinned = nullptr;
   ALB_TRY(e->host_pinned(slot_bytes * nslots, &pinned));
   // cudaMallocHost: page aligned; slots are multiples of 64 bytes
@@ -1176,9 +1222,6 @@ struct StepPlan {
   uint32_t* warm_floor = nullptr;
   // launch shapes: particle-count bucket and context of the shape table
   uint32_t bucket = 0, ctx = 0;
-  // a scene of a fused batch: its first slot in the shared particle arena
-  // (the neighbor list stores arena slots); 0 for a step of its own
-  uint32_t base = 0;
   // first-stage partials of the rigid totals ([kRigidChunks][nb][6])
   double* ftp = nullptr;
   // Shape of pass group `group` (defaults: 128-thread blocks; pair passes
@@ -1277,26 +1320,33 @@ __global__ void k_warm_if(cudaGraphConditionalHandle h, const uint32_t* __restri
 // Kernels inside the learned warm start's IF node (inference, application).
 constexpr uint32_t kWarmIfLaunches = 2;
 
-// Parts of a step: all of it, or (a scene of a fused batch, whose solves
-// run as passes over every scene) the head up to the neighbor build and the
-// tail from the write-back on.
-enum StepPhase { kStepAll, kStepHead, kStepTail };
-
-// Enqueues one whole step (or its `phase`) on `st`: staging uploads, grid,
-// boundaries, neighbors, the solves, write-back and the report readback.
-// With `capture` the solver loops become conditional WHILE nodes (and
-// `loops` counts them); otherwise the host reads the loop flag every
-// iteration.
+// Enqueues one whole step on `st`: staging uploads, grid, boundaries,
+// neighbors, the solves, write-back and the report readback.  With
+// `capture` the solver loops become conditional WHILE nodes (and `loops`
+// counts them); otherwise the host reads the loop flag every iteration.
 template <class TF>
-int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, int* loops,
-                 StepPhase phase = kStepAll) {
+int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, int* loops) {
   StepState<TF>& S = P.S;
   const Cn<TF>& c = P.c;
   const auto* f = P.f;
   const uint32_t n = S.n, nb = S.nb;
   const bool iisph = P.iisph, div = P.div, den = P.den;
   const bool wr = c.wrap != 0;  // periodic-y instantiations of the pair passes
-  const bool head = phase != kStepTail, solves = phase == kStepAll, tail = phase != kStepHead;
+  ALB_CUDA(cudaMemcpyAsync(S.ctrl, P.io.hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
+  if (nb) {
+    ALB_CUDA(cudaMemcpyAsync(P.bodies_dev, P.io.hb, sizeof(BodyDev<TF>) * nb,
+                             cudaMemcpyHostToDevice, st));
+    ALB_CUDA(cudaMemcpyAsync(S.rigid, P.io.hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice,
+                             st));
+  }
+  ALB_CUDA(cudaMemsetAsync(P.flags, 0, 4 * sizeof(uint32_t), st));
+  ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
+  ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
+  // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
+  GridState gs;
+  ALB_LAUNCH(e, "grid_sort", kGridBuildKernels, st,
+             ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
+  S.perm = gs.perm;
   const uint32_t blocks = blocks_for(n, kBlock);
   // grid, block and lane state of pair pass group `g` (launch-shape table)
   auto pair_shape = [&](const char* g, uint32_t& grid, uint32_t& block) {
@@ -1307,86 +1357,68 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     block = sh.block;
     return Sg;
   };
-  if (head) {
-    ALB_CUDA(cudaMemcpyAsync(S.ctrl, P.io.hc, sizeof(Ctrl<TF>), cudaMemcpyHostToDevice, st));
-    if (nb) {
-      ALB_CUDA(cudaMemcpyAsync(P.bodies_dev, P.io.hb, sizeof(BodyDev<TF>) * nb,
-                               cudaMemcpyHostToDevice, st));
-      ALB_CUDA(cudaMemcpyAsync(S.rigid, P.io.hr, sizeof(RigidDev<TF>) * nb, cudaMemcpyHostToDevice,
-                               st));
-    }
-    ALB_CUDA(cudaMemsetAsync(P.flags, 0, 4 * sizeof(uint32_t), st));
-    ALB_CUDA(cudaMemsetAsync(S.ft, 0, size_t(S.grid) * (nb ? nb : 1) * 6 * sizeof(double), st));
-    ALB_LAUNCH(e, "step_init", 1, st, k_step_init<TF><<<1, 32, 0, st>>>(S));
-    // ---- grid, boundaries, neighbors, density (+ DFSPH factor)
-    GridState gs;
-    ALB_LAUNCH(e, "grid_sort", kGridBuildKernels, st,
-               ALB_TRY(grid_build<TF>(e, c, P.g, f->particle_x, n, S.x, P.flags, gs, st)));
-    S.perm = gs.perm;
-    if (n > 0) {
-      const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
-      if (iisph)
-        ALB_LAUNCH(e, "gather_state", 1, st,
-                   k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
-                                                                        nullptr));
+  if (n > 0) {
+    const TF* kref = iisph ? f->particle_pressure : f->particle_kappa;
+    if (iisph)
+      ALB_LAUNCH(e, "gather_state", 1, st,
+                 k_gather_state<TF, false><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                                      nullptr));
+    else
+      ALB_LAUNCH(e, "gather_state", 1, st,
+                 k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
+                                                                     f->particle_kappa_v));
+  }
+  BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk, &S.ctrl->rep.num_active_boundary_pairs, S.ls};
+  if (nb)
+    ALB_LAUNCH(e, "boundary", 1, st,
+               ALB_TRY(sample_boundaries<TF>(c, P.bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
+                                             f->particle_boundary, f->particle_boundary_kernel,
+                                             st)));
+  else if (n)
+    ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
+  SortedBoundaryKernel<TF> sbk{S.mask, S.bk, S.ls};
+  TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
+  if (div && n > 0) {
+    WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol,
+                          P.warm_floor};
+    const uint32_t nbb = P.shape(e, "neighbors", false).block;
+    ALB_LAUNCH(e, "neighbors", 1, st,
+               (wr ? k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, true>
+                         <<<blocks_for(n, nbb), nbb, 0, st>>>(
+                             c, P.g, gs.cell_start, S.x, n, S.ls, sbk, S.nbr, S.ncount, S.rho,
+                             S.alpha, rho_rec, gs.flags, wd, FusedBuild{})
+                   : k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false>
+                         <<<blocks_for(n, nbb), nbb, 0, st>>>(
+                             c, P.g, gs.cell_start, S.x, n, S.ls, sbk, S.nbr, S.ncount, S.rho,
+                             S.alpha, rho_rec, gs.flags, wd, FusedBuild{})));
+    if (P.learned) {
+      // inference and its application; in a captured step they sit in an IF
+      // node, so a step whose gate is closed launches neither
+      auto infer = [&](cudaStream_t s) -> int {
+        ALB_LAUNCH(e, "warm_net", 1, s,
+                   ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, s,
+                                        P.warm_floor)));
+        ALB_LAUNCH(e, "warm_apply", 1, s,
+                   (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, s>>>(
+                       S, P.warm_feat, P.warm_pred, P.warm_floor)));
+        return AL_OK;
+      };
+      if (capture)
+        ALB_TRY(capture_if(
+            e, st,
+            [&](cudaGraphConditionalHandle h) -> int {
+              ALB_LAUNCH(e, "warm_gate", 1, st,
+                         (k_warm_if<TF><<<1, 1, 0, st>>>(h, P.warm_floor, S.ctrl)));
+              return AL_OK;
+            },
+            infer));
       else
-        ALB_LAUNCH(e, "gather_state", 1, st,
-                   k_gather_state<TF, true><<<blocks, kBlock, 0, st>>>(S, f->particle_v, kref,
-                                                                       f->particle_kappa_v));
+        ALB_TRY(infer(st));
     }
-    BoundaryState<TF> bs{nb, S.mask, S.bx, S.bk, &S.ctrl->rep.num_active_boundary_pairs, S.ls};
-    if (nb)
-      ALB_LAUNCH(e, "boundary", 1, st,
-                 ALB_TRY(sample_boundaries<TF>(c, P.bodies_dev, S.rigid, nb, S.x, gs.perm, n, bs,
-                                               f->particle_boundary, f->particle_boundary_kernel,
-                                               st)));
-    else if (n)
-      ALB_CUDA(cudaMemsetAsync(S.mask, 0, size_t(n) * sizeof(uint32_t), st));
-    SortedBoundaryKernel<TF> sbk{S.mask, S.bk, S.ls};
-    TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
-    if (div && n > 0) {
-      WarmDivergence<TF> wd{S, P.warm_feat, P.warm_feat_out, c.radius * TF(2), c.vol,
-                            P.warm_floor};
-      const uint32_t nbb = P.shape(e, "neighbors", false).block;
-      ALB_LAUNCH(e, "neighbors", 1, st,
-                 (wr ? k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, true>
-                           <<<blocks_for(n, nbb), nbb, 0, st>>>(
-                               c, P.g, gs.cell_start, S.x, n, S.ls, P.base, sbk, S.nbr, S.ncount,
-                               S.rho, S.alpha, rho_rec, gs.flags, wd)
-                     : k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false>
-                           <<<blocks_for(n, nbb), nbb, 0, st>>>(
-                               c, P.g, gs.cell_start, S.x, n, S.ls, P.base, sbk, S.nbr, S.ncount,
-                               S.rho, S.alpha, rho_rec, gs.flags, wd)));
-      if (P.learned) {
-        // inference and its application; in a captured step they sit in an IF
-        // node, so a step whose gate is closed launches neither
-        auto infer = [&](cudaStream_t s) -> int {
-          ALB_LAUNCH(e, "warm_net", 1, s,
-                     ALB_TRY(warm_forward(e, P.net, P.warm_feat, n, P.warm_pred, P.flags + 3, s,
-                                          P.warm_floor)));
-          ALB_LAUNCH(e, "warm_apply", 1, s,
-                     (k_apply_warm_div<TF><<<blocks_for(n, kBlock), kBlock, 0, s>>>(
-                         S, P.warm_feat, P.warm_pred, P.warm_floor)));
-          return AL_OK;
-        };
-        if (capture)
-          ALB_TRY(capture_if(
-              e, st,
-              [&](cudaGraphConditionalHandle h) -> int {
-                ALB_LAUNCH(e, "warm_gate", 1, st,
-                           (k_warm_if<TF><<<1, 1, 0, st>>>(h, P.warm_floor, S.ctrl)));
-                return AL_OK;
-              },
-              infer));
-        else
-          ALB_TRY(infer(st));
-      }
-    } else
-      ALB_LAUNCH(e, "neighbors", 1, st,
-                 ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
-                                                     iisph ? nullptr : S.alpha, rho_rec, st,
-                                                     S.ls, P.base)));
-  }  // head
+  } else
+    ALB_LAUNCH(e, "neighbors", 1, st,
+               ALB_TRY(build_neighbors_density<TF>(c, P.g, gs, S.x, sbk, S.nbr, S.ncount, S.rho,
+                                                   iisph ? nullptr : S.alpha, rho_rec, st)));
   // One solver loop: kernel `k_loop_begin` sets the first condition, `body`
   // launches one iteration on the given stream.
   auto solve = [&](int density_solve, uint32_t max_iter, auto&& body) -> int {
@@ -1409,7 +1441,7 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
     }
     return AL_OK;
   };
-  if (n > 0 && solves) {
+  if (n > 0) {
     if (div) {
       {
         uint32_t pg_, pb_;
@@ -1484,6 +1516,14 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                         return AL_OK;
                       }));
       }
+      ALB_LAUNCH(e, "finish", 1, st,
+                 (wr ? k_df_finish<TF, true><<<blocks, kBlock, 0, st>>>(
+                     c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                     f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
+                     f->particle_kappa_v, f->particle_density_adv, P.warm_floor) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
+                     c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
+                     f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
+                     f->particle_kappa_v, f->particle_density_adv, P.warm_floor)));
     } else if (P.isph) {
       ALB_LAUNCH(e, "i_advect", 1, st, k_i_advect<TF><<<blocks, kBlock, 0, st>>>(S));
       {
@@ -1551,19 +1591,6 @@ int enqueue_step(al_engine* e, StepPlan<TF>& P, cudaStream_t st, bool capture, i
                        f->particle_pressure, f->particle_density_adv)));
       }
     }
-  }
-  if (n > 0 && tail && !iisph)
-    ALB_LAUNCH(e, "finish", 1, st,
-               (wr ? k_df_finish<TF, true><<<blocks, kBlock, 0, st>>>(
-                   c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
-                   f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                   f->particle_kappa_v, f->particle_density_adv, P.warm_floor) : k_df_finish<TF, false><<<blocks, kBlock, 0, st>>>(
-                   c, S, den ? 1 : 0, f->particle_x, f->particle_v, f->particle_a,
-                   f->particle_density, f->particle_dfsph_factor, f->particle_kappa,
-                   f->particle_kappa_v, f->particle_density_adv, P.warm_floor)));
-  if (!tail) {
-    ALB_CUDA(cudaGetLastError());
-    return AL_OK;
   }
   if (nb) {
     if (S.grid > kRigidChunks)
@@ -1706,7 +1733,7 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   // per-block buffers (rigid partials, reduction partials) hold the largest
   // grid any pair pass of this scene launches
   S.grid = pair_blocks(n, S.tpp);
-  for (uint32_t k = 0; k < kNumTunable; ++k) {
+  for (uint32_t k = 0; alloc && k < kNumTunable; ++k) {
     if (!kTunable[k].pair) continue;
     const LaunchShape sh = P.shape(e, kTunable[k].name, true);
     S.grid = std::max(S.grid, pair_blocks(n, sh.tpp, sh.block));
@@ -1988,12 +2015,23 @@ std::vector<uint64_t> batch_key(al_engine* e, const std::vector<StepArgs<TF>>& a
 constexpr uint32_t kFusedBlock = 128;
 constexpr uint32_t kFusedAlign = 256;
 
+static_assert(kFusedBlock == uint32_t(kBlock), "fused passes share the arena's block map");
+
 template <class TF>
 struct FusedPlan {
-  uint32_t K = 0, N = 0, nblocks = 0;
+  uint32_t K = 0, N = 0, nblocks = 0, nbmax = 1;
   StepState<TF> S;           // the arena, as the fused passes see it
+  const BuildScene* build = nullptr;         // device [K]
+  const BoundaryScene<TF>* bnd = nullptr;    // device [K]
+  const SortScene<TF>* sort = nullptr;       // device [K]
+  uint32_t ncells = 0;       // the scenes' concatenated cells (tails, padding)
   uint32_t* go = nullptr;    // device: 1 while some scene iterates again
   uint32_t* hgo = nullptr;   // pinned readback of `go` (eager loops)
+  // the scenes' staging slots (pinned, contiguous) and their device copy
+  void* stage_host = nullptr;
+  void* stage_dev = nullptr;
+  size_t stage_bytes = 0;
+  size_t ft_words = 0;       // rigid slots of all scenes (S.ft)
 };
 
 // Starts the solver loop of every scene (k_loop_begin) and sets the loop
@@ -2031,6 +2069,48 @@ __global__ void k_fused_loop_cond(const FusedScene<TF>* __restrict__ sc, uint32_
   }
 }
 
+// The scene view of the per-scene kernels below.
+template <class TF>
+__device__ __forceinline__ StepState<TF> scene_view(const FusedScene<TF>& f) {
+  StepState<TF> V;
+  V.n = f.n;
+  V.nb = f.nb;
+  V.ctrl = f.ctrl;
+  V.bodies = f.bodies;
+  V.rigid = f.rigid;
+  V.ft = f.ft;
+  return V;
+}
+
+// Block k: scene k's step initialisation (k_step_init) and cleared anomaly
+// flags.
+template <class TF>
+__global__ void k_fused_step_init(const FusedScene<TF>* __restrict__ sc) {
+  const FusedScene<TF>& f = sc[blockIdx.x];
+  if (threadIdx.x < 4) f.flags[threadIdx.x] = 0u;
+  step_init(scene_view(f));
+}
+
+// Rigid totals of every scene (the two stages of a single step's rigid
+// finish, in the same chunking): block (c, b, k) sums chunk c of body b of
+// scene k when the scene has more slots than kRigidChunks.
+template <class TF>
+__global__ void k_fused_rigid_partial(const FusedScene<TF>* __restrict__ sc) {
+  const FusedScene<TF>& f = sc[blockIdx.z];
+  if (blockIdx.y >= f.nb || f.nblk <= kRigidChunks) return;
+  rigid_partial(f.ft, f.nblk, f.nb, f.ftp, blockIdx.y, blockIdx.x);
+}
+
+// Block (b, k): body b of scene k's totals and integration.
+template <class TF>
+__global__ void k_fused_rigid_finish(const FusedScene<TF>* __restrict__ sc) {
+  const FusedScene<TF>& f = sc[blockIdx.y];
+  if (blockIdx.x >= f.nb) return;
+  const bool chunked = f.nblk > kRigidChunks;
+  rigid_finish(scene_view(f), chunked ? f.ftp : f.ft, chunked ? kRigidChunks : f.nblk,
+               blockIdx.x);
+}
+
 // Whether a batch can run fused: DFSPH scenes with particles, one set of
 // constants, the same solves enabled, no periodic wrap.
 template <class TF>
@@ -2054,10 +2134,15 @@ int fused_prepare(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>&
   const uint32_t K = uint32_t(plans.size());
   std::vector<uint32_t> s0(K);
   uint64_t N = 0;
+  std::vector<uint32_t> cell0(K);
+  uint64_t C = 0;
   uint32_t nbmax = 1, cap = 1;
   size_t ft_words = 0, ftp_words = 0;
   for (uint32_t k = 0; k < K; ++k) {
     const StepState<TF>& Sk = plans[k].S;
+    cell0[k] = uint32_t(C);
+    C += uint64_t(plans[k].g.ncells) + 2;  // cells, out-of-grid tail, padding
+    ALB_CHECK_ARG(C < (uint64_t(1) << 31), "al_df_batch_step_f32: too many grid cells in all");
     s0[k] = uint32_t(N);
     N = (N + Sk.n + kFusedAlign - 1) / kFusedAlign * kFusedAlign;
     ALB_CHECK_ARG(N < (uint64_t(1) << 31), "al_df_batch_step_f32: too many particles in all");
@@ -2073,7 +2158,6 @@ int fused_prepare(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>&
   StepState<TF> A = plans[0].S;
   FusedScene<TF>* table = nullptr;
   uint32_t* blk = nullptr;
-  BodyDev<TF>* bodies = nullptr;
   double* ftp = nullptr;
   e->ns = "fused.";
   ALB_TRY(e->buf("sorted.x", size_t(N) + kSortedPad, &A.x));
@@ -2089,17 +2173,33 @@ int fused_prepare(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>&
   ALB_TRY(e->buf("bnd.mask", N, &A.mask));
   ALB_TRY(e->buf("bnd.x", size_t(nbmax) * N, &A.bx));
   ALB_TRY(e->buf("bnd.k", size_t(nbmax) * N, &A.bk));
-  ALB_TRY(e->buf("ctrl", K, &A.ctrl));
-  ALB_TRY(e->buf("bodies", size_t(K) * nbmax, &bodies));
-  ALB_TRY(e->buf("rigid", size_t(K) * nbmax, &A.rigid));
+  using L = StagingLayout<TF>;
+  char* stage = nullptr;
+  ALB_TRY(e->buf("stage", L::bytes * K, &stage));
   ALB_TRY(e->buf("ft", ft_words, &A.ft));
   ALB_TRY(e->buf("ftp", ftp_words, &ftp));
   ALB_TRY(e->buf("red", F.nblocks, &A.red));
   ALB_TRY(e->buf("table", K, &table));
   ALB_TRY(e->buf("blk_scene", F.nblocks, &blk));
   ALB_TRY(e->buf("go", 1, &F.go));
+  FusedIo<TF>* io = nullptr;
+  BuildScene* build = nullptr;
+  BoundaryScene<TF>* bnd = nullptr;
+  SortScene<TF>* sort = nullptr;
+  ALB_TRY(e->buf("io", K, &io));
+  ALB_TRY(e->buf("build", K, &build));
+  ALB_TRY(e->buf("bnd", K, &bnd));
+  ALB_TRY(e->buf("sort", K, &sort));
+  // the buffers grid_build_fused will use for the permutation and cell starts
+  uint32_t *perm = nullptr, *cell_start = nullptr;
+  ALB_TRY(e->buf("grid.perm", N, &perm));
+  ALB_TRY(e->buf("grid.start", size_t(C) + 2, &cell_start));
   e->ns.clear();
   std::vector<FusedScene<TF>> tab(K);
+  std::vector<FusedIo<TF>> hio(K);
+  std::vector<BuildScene> hbuild(K);
+  std::vector<BoundaryScene<TF>> hbnd(K);
+  std::vector<SortScene<TF>> hsort(K);
   std::vector<uint32_t> hblk(F.nblocks, K);
   size_t ft_off = 0, ftp_off = 0;
   for (uint32_t k = 0; k < K; ++k) {
@@ -2121,46 +2221,113 @@ int fused_prepare(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>&
     Sk.mask = A.mask + o;
     Sk.bx = A.bx + o;
     Sk.bk = A.bk + o;
-    Sk.ctrl = A.ctrl + k;
-    P.bodies_dev = bodies + size_t(k) * nbmax;
+    // control block, bodies, rigid state and flags in the device copy of
+    // the scene's staging slot
+    char* slot = stage + L::bytes * k;
+    Sk.ctrl = reinterpret_cast<Ctrl<TF>*>(slot);
+    P.bodies_dev = reinterpret_cast<BodyDev<TF>*>(slot + L::bodies);
     Sk.bodies = P.bodies_dev;
-    Sk.rigid = A.rigid + size_t(k) * nbmax;
+    Sk.rigid = reinterpret_cast<RigidDev<TF>*>(slot + L::rigid);
+    P.flags = reinterpret_cast<uint32_t*>(slot + L::flag + 64);
     Sk.ft = A.ft + ft_off;
     Sk.grid = nblk;
     Sk.red = A.red + blk0;
     P.ftp = ftp + ftp_off;
-    P.base = o;
     ft_off += size_t(nblk) * nbk * 6;
     ftp_off += size_t(kRigidChunks) * nbk * 6;
-    tab[k] = FusedScene<TF>{o, n, blk0, nblk, nb, 0u, Sk.ctrl, Sk.bodies, Sk.rigid, Sk.ft, Sk.red};
+    tab[k] = FusedScene<TF>{o,        n,          blk0,  nblk,   nb,      0u,
+                            Sk.ctrl,  Sk.bodies,  Sk.rigid, Sk.ft, P.ftp, Sk.red, P.flags};
+    const auto* f = P.f;
+    hio[k] = FusedIo<TF>{f->particle_x,      f->particle_v,     f->particle_kappa,
+                         f->particle_kappa_v, f->particle_x,   f->particle_v,
+                         f->particle_a,     f->particle_density, f->particle_dfsph_factor,
+                         f->particle_kappa, f->particle_kappa_v, f->particle_density_adv};
+    hbuild[k] = BuildScene{P.g, cell_start + cell0[k], P.flags, o, n};
+    hbnd[k] = BoundaryScene<TF>{Sk.bodies, Sk.rigid, perm, f->particle_boundary,
+                                f->particle_boundary_kernel,
+                                &Sk.ctrl->rep.num_active_boundary_pairs, nb, o, n, 0u};
+    const uint32_t next = k + 1 < K ? s0[k + 1] : F.N;
+    hsort[k] = SortScene<TF>{f->particle_x, P.g, cell0[k], o, n, next - o - n, P.flags};
     for (uint32_t b = blk0; b < blk0 + nblk; ++b) hblk[b] = k;
   }
   A.n = F.N;
   A.ls = F.N;
   A.tpp = 1;
   A.grid = F.nblocks;
-  A.perm = nullptr;
+  A.perm = perm;
   A.blk_scene = blk;
   A.fused = table;
+  A.io = io;
   A.nscenes = K;
   F.S = A;
+  F.build = build;
+  F.bnd = bnd;
+  F.sort = sort;
+  F.ncells = uint32_t(C);
   F.hgo = plans[0].io.hflag;
+  F.nbmax = nbmax;
+  F.stage_host = plans[0].io.hc;  // slot 0 starts the pinned block
+  F.stage_dev = stage;
+  F.stage_bytes = L::bytes * K;
+  F.ft_words = ft_words;
   // upload the tables when they (or their buffers) changed
-  std::vector<unsigned char> bytes(sizeof(FusedScene<TF>) * K + sizeof(uint32_t) * F.nblocks +
-                                   2 * sizeof(void*));
-  std::memcpy(bytes.data(), tab.data(), sizeof(FusedScene<TF>) * K);
-  std::memcpy(bytes.data() + sizeof(FusedScene<TF>) * K, hblk.data(),
-              sizeof(uint32_t) * F.nblocks);
-  const void* where[2] = {table, blk};
-  std::memcpy(bytes.data() + bytes.size() - sizeof(where), where, sizeof(where));
+  struct Part {
+    void* dev;
+    const void* host;
+    size_t bytes;
+  };
+  const Part parts[] = {{table, tab.data(), sizeof(FusedScene<TF>) * K},
+                        {blk, hblk.data(), sizeof(uint32_t) * F.nblocks},
+                        {io, hio.data(), sizeof(FusedIo<TF>) * K},
+                        {build, hbuild.data(), sizeof(BuildScene) * K},
+                        {bnd, hbnd.data(), sizeof(BoundaryScene<TF>) * K},
+                        {sort, hsort.data(), sizeof(SortScene<TF>) * K}};
+  std::vector<unsigned char> bytes;
+  for (const Part& pt : parts) {
+    const unsigned char* h = static_cast<const unsigned char*>(pt.host);
+    const unsigned char* d = reinterpret_cast<const unsigned char*>(&pt.dev);
+    bytes.insert(bytes.end(), d, d + sizeof(pt.dev));
+    bytes.insert(bytes.end(), h, h + pt.bytes);
+  }
   if (bytes != e->fused_tables) {
-    ALB_CUDA(cudaMemcpyAsync(table, tab.data(), sizeof(FusedScene<TF>) * K,
-                             cudaMemcpyHostToDevice, st));
-    ALB_CUDA(cudaMemcpyAsync(blk, hblk.data(), sizeof(uint32_t) * F.nblocks,
-                             cudaMemcpyHostToDevice, st));
+    for (const Part& pt : parts)
+      ALB_CUDA(cudaMemcpyAsync(pt.dev, pt.host, pt.bytes, cudaMemcpyHostToDevice, st));
     ALB_CUDA(cudaStreamSynchronize(st));
     e->fused_tables.swap(bytes);
   }
+  return AL_OK;
+}
+
+// The fused passes of a batch after the scenes' grid sorts: gather,
+// boundary sampling and neighbor build (with the divergence warm start's
+// first pass), each one launch over the arena.
+template <class TF>
+int enqueue_fused_head(al_engine* e, const StepPlan<TF>& P0, FusedPlan<TF>& F, cudaStream_t st) {
+  const Cn<TF>& c = P0.c;
+  const StepState<TF>& S = F.S;
+  const uint32_t G = F.nblocks, B = kFusedBlock;
+  ALB_LAUNCH(e, "gather_state", 1, st,
+             (k_gather_state<TF, true, true><<<G, B, 0, st>>>(S, nullptr, nullptr, nullptr)));
+  ALB_LAUNCH(e, "boundary", 1, st,
+             ALB_TRY(sample_boundaries_fused<TF>(c, S.x, F.N, S.blk_scene, F.bnd, F.K, G, S.mask,
+                                                 S.bx, S.bk, st)));
+  const SortedBoundaryKernel<TF> sbk{S.mask, S.bk, F.N};
+  TF* rho_rec = reinterpret_cast<TF*>(S.rec) + 7;  // rec[2s + 1].w
+  const FusedBuild fb{S.blk_scene, F.build, F.K};
+  if (P0.div) {
+    const WarmDivergence<TF> wd{S, nullptr, nullptr, c.radius * TF(2), c.vol, nullptr};
+    ALB_LAUNCH(e, "neighbors", 1, st,
+               (k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, WarmDivergence<TF>, false,
+                                  true><<<G, B, 0, st>>>(c, GridDims{}, nullptr, S.x, 0u, F.N,
+                                                         sbk, S.nbr, S.ncount, S.rho, S.alpha,
+                                                         rho_rec, nullptr, wd, fb)));
+  } else {
+    ALB_LAUNCH(e, "neighbors", 1, st,
+               (k_build_neighbors<TF, SortedBoundaryKernel<TF>, true, NoExtra<TF>, false, true>
+                    <<<G, B, 0, st>>>(c, GridDims{}, nullptr, S.x, 0u, F.N, sbk, S.nbr, S.ncount,
+                                      S.rho, S.alpha, rho_rec, nullptr, NoExtra<TF>{}, fb)));
+  }
+  ALB_CUDA(cudaGetLastError());
   return AL_OK;
 }
 
@@ -2238,36 +2405,35 @@ int enqueue_fused_solve(al_engine* e, const StepPlan<TF>& P0, FusedPlan<TF>& F, 
 // condition).
 constexpr uint32_t kFusedIterationLaunches = 3;
 
-// Enqueues a fused batch on `st`; with `capture` (st capturing) the scenes'
-// heads and tails run in parallel branches.
+// Enqueues a fused batch on `st`: one upload of every scene's staging, one
+// counting sort over all scenes' cells, every other pass one launch over all
+// scenes, one readback.
 template <class TF>
 int enqueue_fused_batch(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPlan<TF>& F,
                         cudaStream_t st, bool capture, int* loops) {
   const uint32_t K = uint32_t(plans.size());
-  auto phase = [&](StepPhase ph) -> int {
-    if (!capture) {
-      for (uint32_t k = 0; k < K; ++k) {
-        e->ns = batch_ns(k);
-        ALB_TRY(enqueue_step<TF>(e, plans[k], st, false, nullptr, ph));
-      }
-      e->ns.clear();
-      return AL_OK;
-    }
-    ALB_CUDA(cudaEventRecord(e->fork_event, st));
-    for (uint32_t k = 0; k < K; ++k) {
-      cudaStream_t bs = e->branch_streams[k];
-      ALB_CUDA(cudaStreamWaitEvent(bs, e->fork_event, 0));
-      e->ns = batch_ns(k);
-      ALB_TRY(enqueue_step<TF>(e, plans[k], bs, true, loops, ph));
-      ALB_CUDA(cudaEventRecord(e->join_events[k], bs));
-      ALB_CUDA(cudaStreamWaitEvent(st, e->join_events[k], 0));
-    }
-    e->ns.clear();
-    return AL_OK;
-  };
-  ALB_TRY(phase(kStepHead));
+  const StepState<TF>& S = F.S;
+  ALB_CUDA(cudaMemcpyAsync(F.stage_dev, F.stage_host, F.stage_bytes, cudaMemcpyHostToDevice, st));
+  ALB_CUDA(cudaMemsetAsync(S.ft, 0, F.ft_words * sizeof(double), st));
+  ALB_LAUNCH(e, "step_init", 1, st, (k_fused_step_init<TF><<<K, 32, 0, st>>>(S.fused)));
+  GridState gs;
+  e->ns = "fused.";
+  ALB_LAUNCH(e, "grid_sort", grid_fused_kernels(F.ncells), st,
+             ALB_TRY(grid_build_fused<TF>(e, plans[0].c.h, S.blk_scene, F.sort, K, F.N, F.ncells,
+                                          gs, st)));
+  e->ns.clear();
+  ALB_TRY(enqueue_fused_head<TF>(e, plans[0], F, st));
   ALB_TRY(enqueue_fused_solve<TF>(e, plans[0], F, st, capture, loops));
-  return phase(kStepTail);
+  ALB_LAUNCH(e, "finish", 1, st,
+             (k_df_finish<TF, false, true><<<F.nblocks, kFusedBlock, 0, st>>>(
+                 plans[0].c, S, plans[0].den ? 1 : 0, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 nullptr, nullptr, nullptr, nullptr)));
+  ALB_LAUNCH(e, "rigid_finish", 2, st,
+             (k_fused_rigid_partial<TF><<<dim3(kRigidChunks, F.nbmax, K), 256, 0, st>>>(S.fused),
+              k_fused_rigid_finish<TF><<<dim3(F.nbmax, K), 256, 0, st>>>(S.fused)));
+  ALB_CUDA(cudaGetLastError());
+  ALB_CUDA(cudaMemcpyAsync(F.stage_host, F.stage_dev, F.stage_bytes, cudaMemcpyDeviceToHost, st));
+  return AL_OK;
 }
 
 template <class TF>
@@ -2275,7 +2441,6 @@ int capture_batch_fused(al_engine* e, std::vector<StepPlan<TF>>& plans, FusedPla
                         cudaGraphExec_t* exec, uint32_t* fixed) {
   *exec = nullptr;
   ALB_TRY(e->capture_streams());
-  ALB_TRY(e->branches(uint32_t(plans.size())));
   cudaStream_t cs = e->capture_stream;
   const uint64_t launches0 = e->launches;
   const uint64_t gen0 = e->generation;
@@ -2319,26 +2484,40 @@ int run_batch(al_engine* e, const std::vector<StepArgs<TF>>& args, std::vector<i
     nonempty = nonempty && plans[k].S.n > 0;
   }
   e->ns.clear();
+  // A fused batch's arena and tables follow from what the key holds (the
+  // scenes' buffers and sizes, the scratch generation): a replay of its
+  // captured graph needs them placed again only when another fused batch
+  // used the tables since.
   FusedPlan<TF> F;
-  if (fused) ALB_TRY(fused_prepare<TF>(e, plans, F, st));
+  bool placed = false;
   auto key = [&]() {
     std::vector<uint64_t> k = batch_key<TF>(e, args, plans);
-    if (fused) k.insert(k.end(), {0xF05EDull, uint64_t(F.N)});
+    if (fused) k.push_back(0xF05EDull);
     return k;
   };
+  auto place = [&]() -> int {
+    if (!placed) ALB_TRY(fused_prepare<TF>(e, plans, F, st));
+    placed = true;
+    e->fused_key = key();
+    return AL_OK;
+  };
   const bool use_graph = e->graph_mode && !e->profiling && nonempty;
+  const std::vector<uint64_t> key0 = key();
   al_engine::Graph* graph = nullptr;
   if (use_graph)
-    ALB_TRY(find_or_capture(e, key(),
-                            [&](cudaGraphExec_t* x, uint32_t* fl) {
-                              return fused ? capture_batch_fused<TF>(e, plans, F, x, fl)
-                                           : capture_batch<TF>(e, plans, x, fl);
+    ALB_TRY(find_or_capture(e, key0,
+                            [&](cudaGraphExec_t* x, uint32_t* fl) -> int {
+                              if (!fused) return capture_batch<TF>(e, plans, x, fl);
+                              ALB_TRY(place());
+                              return capture_batch_fused<TF>(e, plans, F, x, fl);
                             },
                             &graph));
   if (graph) {
+    if (fused && e->fused_key != key0) ALB_TRY(place());
     ALB_CUDA(cudaGraphLaunch(graph->exec, st));
     ++e->graph_replays;
   } else if (fused) {
+    ALB_TRY(place());
     ALB_TRY(enqueue_fused_batch<TF>(e, plans, F, st, false, nullptr));
   } else {
     for (uint32_t k = 0; k < K; ++k) {

@@ -48,6 +48,8 @@ struct Ctrl {
 
 template <class TF>
 struct FusedScene;
+template <class TF>
+struct FusedIo;
 
 template <class TF>
 struct StepState {
@@ -90,13 +92,15 @@ struct StepState {
   // block (nscenes for a block past every scene) and the scenes' ranges.
   const uint32_t* blk_scene = nullptr;
   const FusedScene<TF>* fused = nullptr;
+  const FusedIo<TF>* io = nullptr;
   uint32_t nscenes = 0;
 };
 
 // One scene of a fused batch: its particles [s0, s0 + n) of the shared
 // arena, its blocks [blk0, blk0 + nblk) of a pass launch (128 threads, one
 // per particle), and its control block, bodies, rigid state, rigid slots
-// ([nblk][nb][6]) and reduction partials ([nblk]).
+// ([nblk][nb][6]), their first-stage partials, reduction partials ([nblk])
+// and anomaly flags.
 template <class TF>
 struct FusedScene {
   uint32_t s0, n, blk0, nblk, nb, pad;
@@ -104,7 +108,27 @@ struct FusedScene {
   const BodyDev<TF>* bodies;
   RigidDev<TF>* rigid;
   double* ft;
+  double* ftp;
   double* red;
+  uint32_t* flags;
+};
+
+// The caller's buffers of one scene of a fused batch (original particle
+// order: read by the gather, written by the write-back).
+template <class TF>
+struct FusedIo {
+  const TF* x_in;
+  const TF* v_in;
+  const TF* kappa_in;
+  const TF* kappa_v_in;
+  TF* x_out;
+  TF* v_out;
+  TF* a_out;
+  TF* rho_out;
+  TF* alpha_out;
+  TF* kappa_out;
+  TF* kappa_v_out;
+  TF* rho_adv_out;
 };
 
 }  // namespace alb

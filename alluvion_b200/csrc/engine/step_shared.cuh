@@ -49,8 +49,9 @@ __device__ __forceinline__ bool grid_sum_last(double value, double* red, uint32_
   return grid_sum_last(value, red, ticket, total, blockIdx.x, gridDim.x);
 }
 
+// The step's control-block initialisation; thread 0 of the calling block.
 template <class TF>
-__global__ void k_step_init(StepState<TF> S) {
+__device__ __forceinline__ void step_init(const StepState<TF>& S) {
   Ctrl<TF>& C = *S.ctrl;
   if (threadIdx.x == 0) {
     C.ticket = 0;
@@ -77,6 +78,11 @@ __global__ void k_step_init(StepState<TF> S) {
     }
     r.pile_max_v2 = double(m);
   }
+}
+
+template <class TF>
+__global__ void k_step_init(StepState<TF> S) {
+  step_init(S);
 }
 
 // ------------------------------------------------------------ loop control
@@ -136,10 +142,11 @@ __device__ __forceinline__ void apply_update_dt(Ctrl<TF>& C, TF pmax) {
 // slots).  Deterministic: the chunking depends on `grid` only.
 constexpr uint32_t kRigidChunks = 128;
 
-__global__ void k_rigid_partial(const double* __restrict__ ft, uint32_t grid, uint32_t nb,
-                                double* __restrict__ part) {
-  const uint32_t b = blockIdx.y, c = blockIdx.x;
-  const uint32_t len = (grid + gridDim.x - 1) / gridDim.x;
+// Chunk c of body b (one block).
+__device__ __forceinline__ void rigid_partial(const double* __restrict__ ft, uint32_t grid,
+                                              uint32_t nb, double* __restrict__ part, uint32_t b,
+                                              uint32_t c) {
+  const uint32_t len = (grid + kRigidChunks - 1) / kRigidChunks;
   const uint32_t lo = c * len, hi = min(lo + len, grid);
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (uint32_t g = lo + threadIdx.x; g < hi; g += blockDim.x) {
@@ -156,13 +163,18 @@ __global__ void k_rigid_partial(const double* __restrict__ ft, uint32_t grid, ui
   }
 }
 
+__global__ void k_rigid_partial(const double* __restrict__ ft, uint32_t grid, uint32_t nb,
+                                double* __restrict__ part) {
+  rigid_partial(ft, grid, nb, part, blockIdx.y, blockIdx.x);
+}
+
 // Per-body totals of the rigid slots (solver_df.hpp:346-353) in double and
-// Pile::integrate_kinematics (pile.hpp:794-815).  One block per body, over
+// Pile::integrate_kinematics (pile.hpp:794-815) of body b (one block), over
 // `nslots` slots of `slots` ([nslots][nb][6]).
 template <class TF>
-__global__ void k_rigid_finish(StepState<TF> S, const double* __restrict__ slots,
-                               uint32_t nslots) {
-  const uint32_t b = blockIdx.x;
+__device__ __forceinline__ void rigid_finish(const StepState<TF>& S,
+                                             const double* __restrict__ slots, uint32_t nslots,
+                                             uint32_t b) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (uint32_t g = threadIdx.x; g < nslots; g += blockDim.x) {
     const double* slot = slots + (size_t(g) * S.nb + b) * 6;
@@ -228,6 +240,13 @@ __global__ void k_rigid_finish(StepState<TF> S, const double* __restrict__ slots
     r.v = (TF(1) / dt) * dx;
   }
   S.rigid[b] = r;
+}
+
+// One block per body.
+template <class TF>
+__global__ void k_rigid_finish(StepState<TF> S, const double* __restrict__ slots,
+                               uint32_t nslots) {
+  rigid_finish(S, slots, nslots, blockIdx.x);
 }
 
 // Host read of the loop flag of an eagerly launched solve.

@@ -163,7 +163,7 @@ def parse_args():
                    help="sweep the pass groups' launch shapes before timing (untimed; "
                         "alluvion_b200.autotune); auto: on for batched workloads run as "
                         "branches")
-    p.add_argument("--batch-form", choices=["fused", "branches"], default="branches",
+    p.add_argument("--batch-form", choices=["fused", "branches"], default="fused",
                    help="batched workloads: fused (one launch per solver pass over all "
                         "scenes) or one graph branch per scene; the line also times the "
                         "other form for comparison")

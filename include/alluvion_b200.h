@@ -764,19 +764,21 @@ AL_API int al_solve_contacts_f32(al_engine* engine, const al_body_f32* bodies,
  * second call with the same configuration on, the whole batch is one
  * captured CUDA graph: one launch and one synchronisation for all scenes.
  *
- * Fused (after al_engine_set_batch_fused(engine, 1), when every scene has
- * particles, the same constants `cn`, the same solves enabled and no
- * periodic wrap): the scenes' particles
+ * Fused (the default, when every scene has particles, the same constants
+ * `cn`, the same solves enabled and no periodic wrap): the scenes' particles
  * share one device arena and every solver pass is ONE kernel launch over
- * all scenes, each block finding its scene in a block -> scene table; the
+ * all scenes, each block finding its scene in a block -> scene table: one
+ * counting sort over all scenes' cells, then gather, boundary sampling,
+ * neighbor build, every solver pass, write-back and rigid totals.  The
  * solver loops are one device-driven loop in which a scene whose solve has
  * converged sits out the remaining iterations, so each scene runs exactly
  * its own iterations.  Pair passes run one thread per particle in
- * 128-thread blocks.  The scenes' grid sorts, boundary sampling, neighbor
- * builds and write-backs run as concurrent graph branches.
- * Otherwise (the default): the graph's parallel branches are the scenes'
- * whole steps, each with its own scratch and launch shapes (the shape
- * table's batch context).
+ * 128-thread blocks.  The scenes' control blocks, bodies and rigid state are
+ * uploaded and read back in one copy each.  Out-of-grid particles (an
+ * AL_ERR_OUT_OF_GRID step) are ordered by index in their tail bucket.
+ * Otherwise (or after al_engine_set_batch_fused(engine, 0)): the graph's
+ * parallel branches are the scenes' whole steps, each with its own scratch
+ * and launch shapes (the shape table's batch context).
  * With 128-thread blocks and one thread per particle for every pair pass in
  * the batch context, both forms give bit-identical results.
  * Returns AL_OK, or the first scene's failure; every scene's own status is

@@ -1,15 +1,15 @@
 """Batched scenes (al_df_batch_step_f32).
 
-Branch form (one graph branch per scene): each branch runs the scene's own
-kernels; with the default launch-shape tables (the same shapes in the single
-and the batch context: threads per particle from the scene's own particle
-count) the results equal the same scenes stepped one at a time with
-al_df_step_f32 bit for bit, whether the batch runs eagerly (first call) or
-as one replayed graph.  Tuned tables that give a scene another shape in a
+Branch form (one graph branch per scene, al_engine_set_batch_fused(0)):
+each branch runs the scene's own kernels; with the default launch-shape
+tables (the same shapes in the single and the batch context: threads per
+particle from the scene's own particle count) the results equal the same
+scenes stepped one at a time with al_df_step_f32 bit for bit, whether the
+batch runs eagerly (first call) or as one replayed graph.  Tuned tables that give a scene another shape in a
 batch change its float results in the last bits
 (tests/test_gpu_launch_shapes.py covers that case against the oracle).
 
-Fused form (one launch per solver pass over all scenes): pair
+Fused form (one launch per solver pass over all scenes, the default): pair
 passes run one thread per particle in 128-thread blocks, so with those
 shapes in the batch context the two forms agree bit for bit, including
 scenes whose solves take different iteration counts; against the oracle
@@ -47,6 +47,14 @@ def _uniform_batch_shapes(engine, scene_list, block, tpp):
 
 
 def test_batch_matches_single_steps(engine):
+    engine.set_batch_fused(False)
+    try:
+        _batch_matches_single_steps(engine)
+    finally:
+        engine.set_batch_fused(True)
+
+
+def _batch_matches_single_steps(engine):
     sp = scenes.solver_params()
     batch = _scenes(engine)
     single = _scenes(engine)
@@ -120,8 +128,33 @@ def test_fused_batch_matches_branch_batch(engine):
         for f, b in zip(fused, branch):
             _states_equal(f, b)
     finally:
-        engine.set_batch_fused(False)
+        engine.set_batch_fused(True)
         _uniform_batch_shapes(engine, fused, 0, 0)
+
+
+def test_two_fused_batches_alternate(engine):
+    """Two fused batches of different scenes, stepped in turn (each replays
+    its own graph over the shared arena tables): each equals its branch-form
+    twin bit for bit."""
+    mk = lambda seed0: [scenes.dam_break(engine, np.float32, lat, 0.01, (0.5, 0.4, 0.4), [],
+                                         seed=seed0 + k, volume_resolution=16)
+                        for k, lat in enumerate(SIZES[:3])]
+    a_f, a_b, b_f, b_b = mk(10), mk(10), mk(20), mk(20)
+    b_f, b_b = b_f[:2], b_b[:2]
+    sp = scenes.solver_params()
+    _uniform_batch_shapes(engine, a_f + b_f, 128, 1)
+    try:
+        dts = {id(x): [2e-4] * len(x) for x in (a_f, a_b, b_f, b_b)}
+        for step in range(3):
+            for fused, batch in ((True, a_f), (True, b_f), (False, a_b), (False, b_b)):
+                engine.set_batch_fused(fused)
+                dts[id(batch)], _, st = scenes.batch_step(engine, batch, sp, dts[id(batch)])
+                assert st == [0] * len(batch)
+        for f, b in zip(a_f + b_f, a_b + b_b):
+            _states_equal(f, b)
+    finally:
+        engine.set_batch_fused(True)
+        _uniform_batch_shapes(engine, a_f + b_f, 0, 0)
 
 
 def test_fused_batch_falls_back_for_mixed_constants(engine):
@@ -137,7 +170,7 @@ def test_fused_batch_falls_back_for_mixed_constants(engine):
     try:
         dts_b, reps_b, status = scenes.batch_step(engine, batch, sp, [2e-4, 2e-4])
     finally:
-        engine.set_batch_fused(False)
+        engine.set_batch_fused(True)
     assert status == [0, 0]
     for k, sc in enumerate(single):
         dt, rep = sc.step("df", sp, 2e-4)
@@ -190,7 +223,7 @@ def test_batch_of_benchmark_scenes_matches_oracle(engine, fused, shape):
             _close(g["v"], ostate["v"], tol["v"], "v")
             _close(g["density"], ostate["density"], tol["density"], "density")
     finally:
-        engine.set_batch_fused(False)
+        engine.set_batch_fused(True)
         for b in buckets:
             for name, _ in groups:
                 engine.set_launch_shape(name, b, 1, 0, 0)

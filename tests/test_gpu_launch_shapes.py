@@ -119,7 +119,7 @@ def test_batch_equals_single_steps_with_the_same_shapes(engine, fused, shape):
             for key in ("x", "v", "kappa", "kappa_v", "density"):
                 np.testing.assert_array_equal(sa[key], ss[key], err_msg=key)
     finally:
-        engine.set_batch_fused(False)
+        engine.set_batch_fused(True)
         for b in buckets:
             for name, _ in groups:
                 for ctx in (0, 1):
