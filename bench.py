@@ -648,10 +648,9 @@ def batch_arm(args):
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > 126 MB L2 (inputs larger than L2, no flush)",
                    "launch": ("eager" if args.eager else "batch graph") + (
-                       ": fused, one launch per solver pass over all scenes (pair passes "
-                       "one thread per particle, 128-thread blocks), per-scene grid sort, "
-                       "boundary sampling, neighbor build and write-back in concurrent "
-                       "branches" if fused else ": one branch per scene"),
+                       ": fused, every pass one launch over all scenes (one counting sort "
+                       "over all scenes' cells; pair passes one thread per particle in "
+                       "128-thread blocks)" if fused else ": one branch per scene"),
                    "autotune": tuning,
                    "graph_replays_timed": graphs1[1] - graphs0[1],
                    "mean_divergence_iterations": round(float(its[:, :, 0].mean()), 3),
