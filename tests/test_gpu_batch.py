@@ -157,6 +157,41 @@ def test_two_fused_batches_alternate(engine):
         _uniform_batch_shapes(engine, a_f + b_f, 0, 0)
 
 
+def test_fused_batch_reports_each_scenes_anomalies(engine):
+    """Anomalies stay with their scene in the fused form: a particle outside
+    one scene's grid (AL_ERR_OUT_OF_GRID) and a cell cap of 4 in another
+    (AL_ERR_CELL_OVERFLOW) give the same per-scene statuses, reports and
+    states as the branch form (128-thread blocks, one thread per particle),
+    and the other scenes AL_OK."""
+    def mk():
+        out = _scenes(engine)[:3]
+        out[1].x[0] = out[1].x.new_tensor([50.0, 50.0, 50.0])
+        out[2].cni.max_num_particles_per_cell = 4
+        return out
+    fused, branch = mk(), mk()
+    sp = scenes.solver_params()
+    _uniform_batch_shapes(engine, fused, 128, 1)
+    try:
+        dts_f, dts_b = [2e-4] * 3, [2e-4] * 3
+        for step in range(2):
+            engine.set_batch_fused(True)
+            dts_f, reps_f, st_f = scenes.batch_step(engine, fused, sp, dts_f,
+                                                    allow=_capi.ANOMALY_STATUSES)
+            engine.set_batch_fused(False)
+            dts_b, reps_b, st_b = scenes.batch_step(engine, branch, sp, dts_b,
+                                                    allow=_capi.ANOMALY_STATUSES)
+            assert st_f == st_b == [0, _capi.AL_ERR_OUT_OF_GRID, _capi.AL_ERR_CELL_OVERFLOW]
+            assert dts_f == dts_b
+            for rf, rb in zip(reps_f, reps_b):
+                assert list(rf.grid_anomaly) == list(rb.grid_anomaly)
+                assert rf.num_density_solve == rb.num_density_solve
+        for f, b in zip(fused, branch):
+            _states_equal(f, b)
+    finally:
+        engine.set_batch_fused(True)
+        _uniform_batch_shapes(engine, fused, 0, 0)
+
+
 def test_fused_batch_falls_back_for_mixed_constants(engine):
     """A batch whose scenes have different constants (particle radii) runs as
     branches: equal to the same scenes stepped alone, bit for bit."""
