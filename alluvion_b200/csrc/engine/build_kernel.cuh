@@ -40,7 +40,12 @@ struct NoExtra {
   static constexpr bool kOn = false;
   __device__ __forceinline__ void narrow(uint32_t) {}
   __device__ __forceinline__ vec3<TF> self_v(uint32_t) const { return vec3<TF>{0, 0, 0}; }
-  __device__ __forceinline__ vec3<TF> vj(uint32_t) const { return vec3<TF>{0, 0, 0}; }
+  // neighbor t's position and velocity for phase 2 (the velocity unused)
+  __device__ __forceinline__ void xv(const vec4<TF>* __restrict__ xs, uint32_t t, vec3<TF>& x,
+                                     vec3<TF>& v) const {
+    x = xyz(__ldg(xs + t));
+    v = vec3<TF>{0, 0, 0};
+  }
   __device__ __forceinline__ void finish(uint32_t, const BuildOut<TF>&) const {}
 };
 
@@ -64,9 +69,10 @@ static_assert(32 % kScan == 0 && kScan <= kSortedPad,
 // d and |d|^2 with the same rounded operations, so phase 2 sees the
 // distances phase 1 accepted.
 //
-// `EX` adds one more sum over the list to phase 2 (EX::kOn): it supplies
-// the particle's and the neighbors' velocities and receives
-// sum_j V (v_i - v_j) . grad W_ij, in list order, at the end.
+// `EX` supplies the neighbors' positions (and velocities) for phase 2 and
+// may add one more sum over the list (EX::kOn): it supplies the particle's
+// and the neighbors' velocities and receives sum_j V (v_i - v_j) . grad W_ij,
+// in list order, at the end.
 //
 // The list is slot-major with row stride `stride` (n for one scene).  With
 // BT the launch covers every scene of a fused batch (fb): xs, the outputs
@@ -168,10 +174,7 @@ __global__ void __launch_bounds__(kMaxBlock)
       t[q] = k0 + q < cnt ? nbr[size_t(k0 + q) * stride + s] : s;
     vec3<TF> xj[kB], vj[kB];
 #pragma unroll
-    for (uint32_t q = 0; q < kB; ++q) {
-      xj[q] = xyz(__ldg(xs + t[q]));
-      vj[q] = ex.vj(t[q]);
-    }
+    for (uint32_t q = 0; q < kB; ++q) ex.xv(xs, t[q], xj[q], vj[q]);
 #pragma unroll
     for (uint32_t q = 0; q < kB; ++q) {
       if (k0 + q >= cnt) break;

@@ -354,7 +354,14 @@ struct WarmDivergence {
     S.rigid = S.fused[k].rigid;
   }
   __device__ __forceinline__ vec3<TF> self_v(uint32_t s) const { return xyz(RV(S, s)); }
-  __device__ __forceinline__ vec3<TF> vj(uint32_t t) const { return xyz(gV(S, t)); }
+  // neighbor t's position and velocity in one load of its 32-byte record
+  // (the record's position is the sorted position the scan used)
+  __device__ __forceinline__ void xv(const vec4<TF>*, uint32_t t, vec3<TF>& x, vec3<TF>& v) const {
+    vec4<TF> x4, v4;
+    gXV(S, t, x4, v4);
+    x = xyz(x4);
+    v = xyz(v4);
+  }
   __device__ __forceinline__ void finish(uint32_t s, const BuildOut<TF>& o) const {
     TF acc = o.div, bvol = 0, bden = 0;
     for (uint32_t m = S.mask[s]; m; m &= m - 1) {
