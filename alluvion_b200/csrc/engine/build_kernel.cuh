@@ -65,7 +65,7 @@ static_assert(32 % kScan == 0 && kScan <= kSortedPad,
 // accepted, so the tests run without a branch per candidate and only the
 // accepted ones pay for a store.  Phase 2 walks the compact list in
 // the same order and evaluates W (and grad W for the DFSPH factor) only
-// for neighbors, four list entries in flight at a time.  Both phases form
+// for neighbors, two list entries in flight at a time.  Both phases form
 // d and |d|^2 with the same rounded operations, so phase 2 sees the
 // distances phase 1 accepted.
 //
@@ -166,7 +166,10 @@ __global__ void __launch_bounds__(kMaxBlock)
   vec3<TF> grad_i{0, 0, 0};
   TF div = 0;
   const vec3<TF> vi = ex.self_v(s);
-  constexpr uint32_t kB = 4;
+  // list entries per round (measured on B200 with the 256-bit record loads,
+  // per build at 1,048,576 / 8,388,608 particles: 0.334 / 2.66 ms at 2,
+  // 0.338 / 2.71 at 4, 0.367 / 2.90 at 8)
+  constexpr uint32_t kB = 2;
   for (uint32_t k0 = 0; k0 < cnt; k0 += kB) {
     uint32_t t[kB];
 #pragma unroll
