@@ -320,10 +320,16 @@ int scan_with_flags(al_engine* e, const uint32_t* count, uint32_t* start, uint32
 template <class TF>
 int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* particle_x,
                uint32_t n, vec4<TF>* xs, uint32_t* flags, GridState& gs, cudaStream_t st) {
+  gs.n = n;
+  gs.ncells = g.ncells;
   gs.flags = flags;
-  ALB_TRY(grid_buffers(e, g, n, gs));
   uint32_t* rank = nullptr;
+  ALB_TRY(e->buf("grid.cell", n, &gs.cell));
   ALB_TRY(e->buf("grid.rank", n, &rank));
+  ALB_TRY(e->buf("grid.perm", n, &gs.perm));
+  ALB_TRY(e->buf("grid.inv", n, &gs.inv));
+  ALB_TRY(e->buf("grid.count", size_t(g.ncells) + 1, &gs.count));
+  ALB_TRY(e->buf("grid.start", size_t(g.ncells) + 2, &gs.cell_start));
   ALB_CUDA(cudaMemsetAsync(gs.count, 0, (size_t(g.ncells) + 1) * sizeof(uint32_t), st));
   if (n == 0) {
     ALB_CUDA(cudaMemsetAsync(gs.cell_start, 0, (size_t(g.ncells) + 2) * sizeof(uint32_t), st));
@@ -341,17 +347,6 @@ int grid_build(al_engine* e, const Cn<TF>& c, const GridDims& g, const TF* parti
                                                                         gs.perm);
   k_gather_x<TF><<<blocks_for(n, kBlock), kBlock, 0, st>>>(particle_x, gs.perm, n, xs, gs.inv);
   ALB_CUDA(cudaGetLastError());
-  return AL_OK;
-}
-
-int grid_buffers(al_engine* e, const GridDims& g, uint32_t n, GridState& gs) {
-  gs.n = n;
-  gs.ncells = g.ncells;
-  ALB_TRY(e->buf("grid.cell", n, &gs.cell));
-  ALB_TRY(e->buf("grid.perm", n, &gs.perm));
-  ALB_TRY(e->buf("grid.inv", n, &gs.inv));
-  ALB_TRY(e->buf("grid.count", size_t(g.ncells) + 1, &gs.count));
-  ALB_TRY(e->buf("grid.start", size_t(g.ncells) + 2, &gs.cell_start));
   return AL_OK;
 }
 

@@ -31,11 +31,6 @@ struct GridState {
 // per-cell orderings, gather).
 constexpr int kGridBuildKernels = 8;
 
-// The scratch grid_build uses for a sort of n particles on grid g, under the
-// engine's current buffer namespace (cell, perm, inv, count, cell_start of
-// gs): a later grid_build with the same sizes uses the same buffers.
-int grid_buffers(al_engine* e, const GridDims& g, uint32_t n, GridState& gs);
-
 // Hashes, sorts and gathers positions into `xs` (sorted order, w = 0).
 // particle_x is the caller's [n][3] array.  `flags` must be zeroed by the
 // caller (it is also used by later passes).
