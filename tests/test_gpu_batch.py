@@ -96,10 +96,13 @@ def test_fused_batch_matches_branch_batch(engine):
     particle in the batch context: equal dts, iteration counts, reports and
     states bit for bit over four steps (the first eager, then captured).
     The second scene is held to at least five density iterations, so the
-    others sit out iterations of the fused loop."""
+    others sit out iterations of the fused loop; the third runs a smaller
+    time-step cap and the fourth keeps its rigid body fixed."""
     fused, branch = _scenes(engine), _scenes(engine)
     sps = [scenes.solver_params() for _ in fused]
     sps[1] = scenes.solver_params(min_density_solve=5)
+    sps[2] = scenes.solver_params(max_dt=1e-4)
+    sps[3] = scenes.solver_params(integrate_rigids=0)
     _uniform_batch_shapes(engine, fused, 128, 1)
     try:
         c0, r0 = engine.graph_stats()
