@@ -2003,22 +2003,25 @@ std::vector<uint64_t> batch_key(al_engine* e, const std::vector<StepArgs<TF>>& a
 }
 
 // ------------------------------------------------------------ fused batches
-// A fused batch runs each solver pass of all its scenes as one launch.  The
+// A fused batch runs each pass of all its scenes as one launch.  The
 // scenes' cell-sorted particles share one arena (scene k at slots
-// [s0_k, s0_k + n_k), s0_k a multiple of kFusedAlign), the neighbor lists
-// and boundary terms are slot-major over the whole arena (the lists hold
-// arena slots), and each block of a pass finds its scene in a block -> scene
+// [s0_k, s0_k + n_k), s0_k a multiple of kFusedAlign, so every
+// kFusedBlock-slot block belongs to one scene), the neighbor lists and
+// boundary terms are slot-major over the whole arena (the lists hold arena
+// slots), and each block of a pass finds its scene in a block -> scene
 // table (block_scene) for the scene's dt, control block, bodies and
-// reductions.  Grid sort, boundary sampling and the neighbor build (the
-// scenes' grids differ) and the write-back stay per scene, in concurrent
-// graph branches.  The solver loops are one WHILE loop over all scenes: a
-// scene whose solve has converged sits out the remaining iterations and
-// the loop ends when no scene iterates again, so each scene runs exactly
-// its own iterations.  Pair passes run one thread per particle in
-// kFusedBlock-thread blocks; every reduction of a scene covers its own
-// blocks in the order a single step's 128-thread launch would, so with
-// those shapes in the shape table's batch context the branch and the
-// fused batch give bit-identical results.
+// reductions.  The sort is one counting sort over all scenes' cells
+// (grid_build_fused); gather, boundary sampling and the neighbor build take
+// each block's scene grid and buffers from per-scene tables; the write-back
+// goes to each scene's own buffers; the control blocks, bodies and rigid
+// state travel in one device copy of the batch's staging.  The solver
+// loops are one WHILE loop over all scenes: a scene whose solve has
+// converged sits out the remaining iterations and the loop ends when no
+// scene iterates again, so each scene runs exactly its own iterations.
+// Pair passes run one thread per particle in kFusedBlock-thread blocks;
+// every reduction of a scene covers its own blocks in the order a single
+// step's 128-thread launch would, so with those shapes in the shape table's
+// batch context the branch and the fused batch give bit-identical results.
 constexpr uint32_t kFusedBlock = 128;
 constexpr uint32_t kFusedAlign = 256;
 
