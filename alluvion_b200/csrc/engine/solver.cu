@@ -1707,9 +1707,9 @@ struct StepArgs {
 };
 
 // Validates the arguments, sizes the scene's scratch (under the engine's
-// current buffer namespace; with `alloc` false only its anomaly flags: a
-// fused batch places the particle state in its shared arena) and fills
-// staging slot `slot` of `nslots`.
+// current buffer namespace; with `alloc` false none: a fused batch places
+// the scene's state in its shared arena and staging copy) and fills staging
+// slot `slot` of `nslots`.
 template <class TF>
 int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t slot,
                  uint32_t nslots, bool alloc = true) {
@@ -1747,8 +1747,8 @@ int prepare_step(al_engine* e, const StepArgs<TF>& A, StepPlan<TF>& P, uint32_t 
   }
   if (S.grid == 0) S.grid = 1;
   // ---- buffers
-  ALB_TRY(e->buf("flags", 4, &P.flags));
   if (alloc) {
+    ALB_TRY(e->buf("flags", 4, &P.flags));
     ALB_TRY(e->buf("sorted.x", size_t(n) + kSortedPad, &S.x));
     ALB_TRY(e->buf("sorted.rec", size_t(n) * 2, &S.rec));
     ALB_TRY(e->buf("sorted.a", n, &S.a));
