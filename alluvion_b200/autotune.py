@@ -89,10 +89,33 @@ def _group_ms(engine, steps):
     return {name: tot / cnt for name, (tot, cnt) in engine.kernel_stats().items() if cnt}
 
 
-def tune_scene(engine, scene, sp, method="df", steps=3, warm=None):
+def _graph_step_ms(scene, sp, method, snap, steps, warm):
+    """ms per step of `steps` captured steps from the restored state (two
+    untimed steps first: the eager one and the capture)."""
+    import torch
+    scene.restore(snap)
+    dt = float(sp.max_dt)
+    for _ in range(2):
+        dt, _ = scene.step(method, sp, dt, warm=warm)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        dt, _ = scene.step(method, sp, dt, warm=warm)
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / steps
+
+
+def tune_scene(engine, scene, sp, method="df", steps=3, warm=None, check_steps=10):
     """Sweeps every tunable group's shape on `scene` (its state is put back
-    after each trial and at the end); applies and returns the table of the
-    fastest shape per group for the scene's bucket, single-step context."""
+    after each trial and at the end), timing each group per launch; then
+    times whole captured steps with the fastest shape per group and with the
+    defaults, and keeps the faster of the two (per-launch times of small
+    scenes do not show how the launches overlap in the step graph).  Applies
+    and returns the table for the scene's bucket, single-step context; its
+    "graph_ms" records both step times and "kept" which won."""
     import torch
     groups = _capi.tunable_groups()
     b = bucket_of(scene.n)
@@ -129,9 +152,16 @@ def tune_scene(engine, scene, sp, method="df", steps=3, warm=None):
                         "ms": round(best_ms, 5),
                         "default_ms": round(dict((c, t) for t, c in trials[name]).get(
                             engine.launch_shape(name, scene.n, 0), float("nan")), 5)})
-    scene.restore(snap)
     table = {"device": torch.cuda.get_device_name(), "entries": entries}
+    default_ms = _graph_step_ms(scene, sp, method, snap, check_steps, warm)
     apply(engine, table)
+    tuned_ms = _graph_step_ms(scene, sp, method, snap, check_steps, warm)
+    table["graph_ms"] = {"default": round(default_ms, 4), "tuned": round(tuned_ms, 4)}
+    table["kept"] = "tuned" if tuned_ms < default_ms else "default"
+    if table["kept"] == "default":
+        clear(engine, table)
+        table["entries"] = []
+    scene.restore(snap)
     return table
 
 

@@ -161,8 +161,9 @@ def parse_args():
                         "default workload, else 0)")
     p.add_argument("--autotune", choices=["auto", "on", "off"], default="auto",
                    help="sweep the pass groups' launch shapes before timing (untimed; "
-                        "alluvion_b200.autotune); auto: on for single scenes of 2^20 particles "
-                        "or more and for batched workloads run as branches")
+                        "alluvion_b200.autotune); auto: on for single scenes (the sweep keeps "
+                        "the defaults when its table is slower in the step graph) and for "
+                        "batched workloads run as branches")
     p.add_argument("--batch-form", choices=["fused", "branches"], default="fused",
                    help="batched workloads: fused (one launch per solver pass over all "
                         "scenes) or one graph branch per scene; the line also times the "
@@ -889,10 +890,7 @@ def engine_arm(args):
     host_state = scene.state() if rank == 0 and world == 1 else None
     host_bodies = scene.host_bodies() if host_state is not None else None
     tuning = None
-    # measured on B200: tuned shapes save 1.3 % of the 8.4M-particle step and
-    # 0.3-2.6 % at 1M particles; at 32,768 particles the per-launch timing of
-    # the sweep picks shapes that run 3 % slower in the step graph
-    if args.autotune == "on" or (args.autotune == "auto" and n >= 1 << 20 and not args.eager):
+    if args.autotune == "on" or (args.autotune == "auto" and not args.eager):
         from alluvion_b200 import autotune
         t0 = time.perf_counter()
         tuning = autotune.tune_scene(engine, scene, sp, method=args.method)
@@ -936,7 +934,8 @@ def engine_arm(args):
                              "an iteration")
         config["learned_warm_start"] = warm_info
     if tuning is not None:
-        config["autotune"] = {"seconds": tuning["seconds"], "shapes": {
+        config["autotune"] = {"seconds": tuning["seconds"], "kept": tuning["kept"],
+                              "graph_ms_per_step": tuning["graph_ms"], "shapes": {
             e["group"]: [e["block"], e["tpp"]] for e in tuning["entries"]}}
     if args.fp64_steps and rank == 0:
         config["error_vs_fp64_plain"] = fp64_error(engine, args, sp, args.fp64_steps)
