@@ -548,6 +548,28 @@ def batch_scene_specs(spec, seed=SEED):
     return out
 
 
+def pack_scenes(scene_list, keys, torch):
+    """Rebinds each scene's per-particle arrays `keys` to views into one
+    device tensor per key (the scenes' data copied in, every view starting on
+    a 256-byte boundary), as a host that owns many scenes would lay them out:
+    its host copies then move each array of the whole batch at once.
+    Returns {key: tensor}."""
+    out = {}
+    for k in keys:
+        parts = [getattr(sc, k) for sc in scene_list]
+        offs, off = [], 0
+        for p in parts:
+            offs.append(off)
+            off += (p.numel() + 63) // 64 * 64
+        big = torch.zeros(off, dtype=parts[0].dtype, device=parts[0].device)
+        for sc, p, o in zip(scene_list, parts, offs):
+            view = big[o:o + p.numel()].view(p.shape)
+            view.copy_(p)
+            setattr(sc, k, view)
+        out[k] = big
+    return out
+
+
 def batch_arm(args):
     """Config-3 style batch: every step advances all scenes with one
     al_df_batch_step_f32 call (one graph launch from the second step on),
@@ -565,6 +587,7 @@ def batch_arm(args):
     engine = _capi.Engine(local)
     engine.set_graph_mode(not args.eager)
     sl = batch_scene_list(engine, spec)
+    packed = pack_scenes(sl, ("x", "v", "kappa", "kappa_v"), torch)
     sp = scenes.solver_params()
     if args.max_dt:
         sp.max_dt = args.max_dt
@@ -618,10 +641,12 @@ def batch_arm(args):
     barrier(world)
     ms = max_over_ranks(ms, world, torch)
     value = job_throughput(total_n, world, args.steps, ms)
+    # host copies of all scenes' x, v, kappa, kappa_v (one pinned buffer per
+    # array): uploaded before and x, v read back after every batched step
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    dev_in = [t for sc in sl for t in (sc.x, sc.v, sc.kappa, sc.kappa_v)]
+    dev_in = [packed[k] for k in ("x", "v", "kappa", "kappa_v")]
     host_in = [pin(t.cpu().numpy()) for t in dev_in]
-    dev_out = [t for sc in sl for t in (sc.x, sc.v)]
+    dev_out = [packed["x"], packed["v"]]
     host_out = [pin(t.cpu().numpy()) for t in dev_out]
     h2d = sum(t.numel() * t.element_size() for t in host_in)
     d2h = sum(t.numel() * t.element_size() for t in host_out)
