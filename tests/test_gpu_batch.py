@@ -162,20 +162,23 @@ def test_two_fused_batches_alternate(engine):
 
 def test_fused_batch_reports_each_scenes_anomalies(engine):
     """Anomalies stay with their scene in the fused form: a particle outside
-    one scene's grid (AL_ERR_OUT_OF_GRID) and a cell cap of 4 in another
-    (AL_ERR_CELL_OVERFLOW) give the same per-scene statuses, reports and
-    states as the branch form (128-thread blocks, one thread per particle),
-    and the other scenes AL_OK."""
+    one scene's grid (AL_ERR_OUT_OF_GRID), a cell cap of 4 in another
+    (AL_ERR_CELL_OVERFLOW) and a neighbor cap of 16 in a third
+    (AL_ERR_NEIGHBOR_OVERFLOW: its lists keep the first 16 canonical
+    neighbors) give the same per-scene statuses, reports and states as the
+    branch form (128-thread blocks, one thread per particle), and the other
+    scene AL_OK."""
     def mk():
-        out = _scenes(engine)[:3]
+        out = _scenes(engine)[:4]
         out[1].x[0] = out[1].x.new_tensor([50.0, 50.0, 50.0])
         out[2].cni.max_num_particles_per_cell = 4
+        out[3].cni.max_num_neighbors_per_particle = 16
         return out
     fused, branch = mk(), mk()
     sp = scenes.solver_params()
     _uniform_batch_shapes(engine, fused, 128, 1)
     try:
-        dts_f, dts_b = [2e-4] * 3, [2e-4] * 3
+        dts_f, dts_b = [2e-4] * 4, [2e-4] * 4
         for step in range(2):
             engine.set_batch_fused(True)
             dts_f, reps_f, st_f = scenes.batch_step(engine, fused, sp, dts_f,
@@ -183,7 +186,8 @@ def test_fused_batch_reports_each_scenes_anomalies(engine):
             engine.set_batch_fused(False)
             dts_b, reps_b, st_b = scenes.batch_step(engine, branch, sp, dts_b,
                                                     allow=_capi.ANOMALY_STATUSES)
-            assert st_f == st_b == [0, _capi.AL_ERR_OUT_OF_GRID, _capi.AL_ERR_CELL_OVERFLOW]
+            assert st_f == st_b == [0, _capi.AL_ERR_OUT_OF_GRID, _capi.AL_ERR_CELL_OVERFLOW,
+                                    _capi.AL_ERR_NEIGHBOR_OVERFLOW]
             assert dts_f == dts_b
             for rf, rb in zip(reps_f, reps_b):
                 assert list(rf.grid_anomaly) == list(rb.grid_anomaly)
